@@ -1,0 +1,302 @@
+"""ctypes mirrors of the C ABI in include/tj_b200.h and a numpy-side data model.
+
+The reference (code/tjsq/common.f90:65-149) keeps its block-sparse objects in
+Fortran derived types.  This module holds the same objects as plain Python
+classes backed by numpy arrays (column-major sub-matrices, as in Fortran) and
+packs them into the flat C structs the library takes.  A packed object keeps
+references to every numpy buffer it points into, so the pointers stay valid
+for as long as the packed object lives.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Optional, Tuple
+
+import numpy as np
+
+c_int32_p = C.POINTER(C.c_int32)
+c_double_p = C.POINTER(C.c_double)
+
+
+class TjBlockSub(C.Structure):
+    _fields_ = [("num_up", C.c_int32), ("num_down", C.c_int32), ("down_dif", C.c_int32),
+                ("row_dim", C.c_int32), ("sdim", C.c_int32), ("pad_", C.c_int32),
+                ("off", C.c_int64)]
+
+
+class TjBlock(C.Structure):
+    _fields_ = [("len", C.c_int32), ("num", C.c_int32), ("dim", C.c_int32),
+                ("up_dif", C.c_int32), ("down_dif", C.c_int32), ("pad_", C.c_int32),
+                ("sub", C.POINTER(TjBlockSub)), ("data", c_double_p)]
+
+
+class TjBlockSet(C.Structure):
+    _fields_ = [("elec_up", TjBlock), ("elec_down", TjBlock), ("spin_sd", TjBlock),
+                ("spin_sz", TjBlock), ("num_sn", TjBlock)]
+
+
+class TjModel(C.Structure):
+    _fields_ = [("len", C.c_int32), ("nsub", C.c_int32), ("ham", TjBlock),
+                ("sub", C.POINTER(TjBlockSet))]
+
+
+class TjBasisSub(C.Structure):
+    _fields_ = [("spos", C.c_int32), ("sdim", C.c_int32), ("bl_num_up", C.c_int32),
+                ("bl_num_down", C.c_int32), ("st_num_up", C.c_int32), ("st_num_down", C.c_int32)]
+
+
+class TjBasisMap(C.Structure):
+    _fields_ = [("idx", C.c_int32), ("num", C.c_int32), ("dim", C.c_int32),
+                ("new_num_up", C.c_int32), ("new_num_down", C.c_int32), ("first", C.c_int32)]
+
+
+class TjBasis(C.Structure):
+    _fields_ = [("len", C.c_int32), ("num", C.c_int32), ("dim", C.c_int32), ("pad_", C.c_int32),
+                ("sub", C.POINTER(TjBasisMap)), ("maps", C.POINTER(TjBasisSub))]
+
+
+class TjWaveSub(C.Structure):
+    _fields_ = [("sys_num_up", C.c_int32), ("sys_num_down", C.c_int32),
+                ("env_num_up", C.c_int32), ("env_num_down", C.c_int32),
+                ("sys_dim", C.c_int32), ("env_dim", C.c_int32), ("off", C.c_int64)]
+
+
+class TjWave(C.Structure):
+    _fields_ = [("sys_len", C.c_int32), ("env_len", C.c_int32), ("num", C.c_int32),
+                ("pad_", C.c_int32), ("dim", C.c_int64), ("sub", C.POINTER(TjWaveSub)),
+                ("data", c_double_p)]
+
+
+class TjLattice(C.Structure):
+    _fields_ = [("num_site", C.c_int32), ("neibt", C.c_int32), ("up_bias", C.c_int32),
+                ("pad_", C.c_int32),
+                ("neib", c_int32_p), ("neiba", c_int32_p), ("inb1", c_int32_p),
+                ("nleg11", c_int32_p), ("nposi", c_int32_p), ("nposi_dm", c_int32_p),
+                ("nposi_lat", c_int32_p),
+                ("jt", c_double_p), ("jz", c_double_p), ("jd", c_double_p), ("jn", c_double_p),
+                ("esite", c_double_p)]
+
+
+class TjTruncResult(C.Structure):
+    _fields_ = [("num_state", C.c_int32), ("num", C.c_int32), ("data_len", C.c_int64),
+                ("trunc_err", C.c_double), ("entropy1", C.c_double), ("entropy2", C.c_double),
+                ("entropys", C.c_double), ("sub", C.POINTER(TjBlockSub)), ("data", c_double_p)]
+
+
+class TjHpsiStats(C.Structure):
+    _fields_ = [("flops", C.c_double), ("flops_ref", C.c_double), ("bytes", C.c_double),
+                ("n_products", C.c_int64), ("n_tasks", C.c_int64), ("n_tiles_p1", C.c_int64),
+                ("n_tiles_p2", C.c_int64), ("scratch_doubles", C.c_int64),
+                ("last_ms", C.c_double), ("last_ms_phase1", C.c_double),
+                ("last_ms_phase2", C.c_double)]
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(c_double_p)
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(c_int32_p)
+
+
+# --------------------------------------------------------------------------
+# numpy-side objects
+# --------------------------------------------------------------------------
+@dataclass
+class SubBlock:
+    """Sub_Block: maps sector (num_up, num_down) by down_dif; mat is (row_dim, sdim)."""
+    num_up: int
+    num_down: int
+    down_dif: int
+    mat: np.ndarray
+
+
+@dataclass
+class Block:
+    """Total_Block (common.f90:119-122)."""
+    len: int
+    up_dif: int
+    down_dif: int
+    subs: List[SubBlock] = field(default_factory=list)
+
+    @property
+    def dim(self) -> int:
+        return int(sum(s.mat.shape[1] for s in self.subs))
+
+    def pack(self) -> "PackedBlock":
+        return PackedBlock(self)
+
+
+class PackedBlock:
+    def __init__(self, b: Block):
+        n = len(b.subs)
+        self.subs = (TjBlockSub * max(n, 1))()
+        total = int(sum(s.mat.size for s in b.subs))
+        self.data = np.zeros(max(total, 1), dtype=np.float64)
+        off = 0
+        for i, s in enumerate(b.subs):
+            r, c = s.mat.shape
+            self.subs[i] = TjBlockSub(s.num_up, s.num_down, s.down_dif, r, c, 0, off)
+            self.data[off:off + r * c] = np.asarray(s.mat, dtype=np.float64).reshape(-1, order="F")
+            off += r * c
+        self.c = TjBlock(b.len, n, b.dim, b.up_dif, b.down_dif, 0,
+                         C.cast(self.subs, C.POINTER(TjBlockSub)), _dptr(self.data))
+
+
+OPS = ("elec_up", "elec_down", "spin_sd", "spin_sz", "num_sn")
+
+
+@dataclass
+class BlockSet:
+    elec_up: Block
+    elec_down: Block
+    spin_sd: Block
+    spin_sz: Block
+    num_sn: Block
+
+
+@dataclass
+class Model:
+    """Total_Model inputs (common.f90:144-149): ham and sub(1:nsub)."""
+    len: int
+    ham: Block
+    sub: List[BlockSet]
+
+    def pack(self) -> "PackedModel":
+        return PackedModel(self)
+
+
+class PackedModel:
+    def __init__(self, m: Model):
+        self.ham = m.ham.pack()
+        self.sets = []
+        n = len(m.sub)
+        self.sub = (TjBlockSet * max(n, 1))()
+        for i, bs in enumerate(m.sub):
+            ps = [getattr(bs, k).pack() for k in OPS]
+            self.sets.append(ps)
+            self.sub[i] = TjBlockSet(*[p.c for p in ps])
+        self.c = TjModel(m.len, n, self.ham.c, C.cast(self.sub, C.POINTER(TjBlockSet)))
+
+
+@dataclass
+class BasisMap:
+    new_num_up: int
+    new_num_down: int
+    # (spos, sdim, bl_num_up, bl_num_down, st_num_up, st_num_down)
+    subs: List[Tuple[int, int, int, int, int, int]]
+
+    @property
+    def dim(self) -> int:
+        return int(sum(s[1] for s in self.subs))
+
+
+@dataclass
+class Basis:
+    """Total_Basis (common.f90:79-82)."""
+    len: int
+    maps: List[BasisMap]
+
+    @property
+    def dim(self) -> int:
+        return int(sum(m.dim for m in self.maps))
+
+    def pack(self) -> "PackedBasis":
+        return PackedBasis(self)
+
+
+class PackedBasis:
+    def __init__(self, b: Basis):
+        n = len(b.maps)
+        nm = sum(len(m.subs) for m in b.maps)
+        self.sub = (TjBasisMap * max(n, 1))()
+        self.maps = (TjBasisSub * max(nm, 1))()
+        k = 0
+        for i, m in enumerate(b.maps):
+            self.sub[i] = TjBasisMap(0, len(m.subs), m.dim, m.new_num_up, m.new_num_down, k)
+            for s in m.subs:
+                self.maps[k] = TjBasisSub(*s)
+                k += 1
+        self.c = TjBasis(b.len, n, b.dim, 0, C.cast(self.sub, C.POINTER(TjBasisMap)),
+                         C.cast(self.maps, C.POINTER(TjBasisSub)))
+
+
+@dataclass
+class WaveSector:
+    sys_num_up: int
+    sys_num_down: int
+    env_num_up: int
+    env_num_down: int
+    sys_dim: int
+    env_dim: int
+
+
+class Wave:
+    """Wavefunction (common.f90:100-110): sector matrices stored back to back."""
+
+    def __init__(self, sys_len: int, env_len: int, sectors: List[WaveSector],
+                 data: Optional[np.ndarray] = None):
+        self.sys_len = sys_len
+        self.env_len = env_len
+        self.sectors = list(sectors)
+        self.offsets = np.zeros(len(sectors) + 1, dtype=np.int64)
+        for i, s in enumerate(sectors):
+            self.offsets[i + 1] = self.offsets[i] + s.sys_dim * s.env_dim
+        self.dim = int(self.offsets[-1])
+        self.data = np.zeros(max(self.dim, 1), dtype=np.float64) if data is None else data
+        assert self.data.dtype == np.float64 and self.data.flags.c_contiguous
+        self.sub = (TjWaveSub * max(len(sectors), 1))()
+        for i, s in enumerate(sectors):
+            self.sub[i] = TjWaveSub(s.sys_num_up, s.sys_num_down, s.env_num_up, s.env_num_down,
+                                    s.sys_dim, s.env_dim, int(self.offsets[i]))
+        self.c = TjWave(sys_len, env_len, len(sectors), 0, self.dim,
+                        C.cast(self.sub, C.POINTER(TjWaveSub)), _dptr(self.data))
+
+    def like(self, data: Optional[np.ndarray] = None) -> "Wave":
+        return Wave(self.sys_len, self.env_len, self.sectors,
+                    np.zeros_like(self.data) if data is None else data)
+
+    def copy(self) -> "Wave":
+        return self.like(self.data.copy())
+
+    def sector(self, i: int) -> np.ndarray:
+        s = self.sectors[i]
+        a = self.data[self.offsets[i]:self.offsets[i + 1]]
+        return a.reshape((s.sys_dim, s.env_dim), order="F")
+
+
+class Lattice:
+    """Module pubdata globals read on the hot path, in the layouts of tj_lattice."""
+
+    def __init__(self, num_site: int, neibt: int, up_bias: int, neib, neiba, inb1, nleg11,
+                 nposi, nposi_dm, nposi_lat, jt, jz, jd, jn, esite):
+        self.num_site, self.neibt, self.up_bias = num_site, neibt, up_bias
+        ns1 = num_site + 1
+        f = lambda a, shape: np.ascontiguousarray(np.asarray(a, dtype=np.int32).reshape(-1, order="F"))
+        self.neib = f(neib, (ns1, neibt))
+        self.neiba = f(neiba, (ns1, ns1))
+        self.inb1 = f(inb1, (ns1, ns1))
+        self.nleg11 = np.ascontiguousarray(np.asarray(nleg11, dtype=np.int32))
+        self.nposi = np.ascontiguousarray(np.asarray(nposi, dtype=np.int32))
+        self.nposi_dm = np.ascontiguousarray(np.asarray(nposi_dm, dtype=np.int32))
+        self.nposi_lat = np.ascontiguousarray(np.asarray(nposi_lat, dtype=np.int32))
+        d = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1, order="F"))
+        self.jt, self.jz, self.jd = d(jt), d(jz), d(jd)
+        self.jn = d(jn)
+        self.esite = d(esite)
+        self.c = TjLattice(num_site, neibt, up_bias, 0, _iptr(self.neib), _iptr(self.neiba),
+                           _iptr(self.inb1), _iptr(self.nleg11), _iptr(self.nposi),
+                           _iptr(self.nposi_dm), _iptr(self.nposi_lat), _dptr(self.jt),
+                           _dptr(self.jz), _dptr(self.jd), _dptr(self.jn), _dptr(self.esite))
+
+
+def block_from_c_result(res: TjTruncResult, length: int) -> Block:
+    """Turns a filled tj_trunc_result into a Block (trun_op)."""
+    subs = []
+    for i in range(res.num):
+        s = res.sub[i]
+        n = s.row_dim * s.sdim
+        buf = np.ctypeslib.as_array(res.data, shape=(res.data_len,))[s.off:s.off + n]
+        subs.append(SubBlock(s.num_up, s.num_down, 0, buf.reshape((s.row_dim, s.sdim), order="F").copy()))
+    return Block(length, 0, 0, subs)

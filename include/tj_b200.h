@@ -1,0 +1,243 @@
+/*
+ * tj_b200.h -- C ABI of the B200 implementation of the tjsq SU(2) t-J DMRG hot path.
+ *
+ * The reference (DongNingSheng/Grand_SQL_tJ, code/tjsq, Fortran 90) keeps its
+ * block-sparse tensors in derived types with allocatable components, which are
+ * not C-interoperable.  This header gives flat mirrors of those types and one
+ * entry point per reference routine on the hot path.  A Fortran caller fills
+ * the structs from its derived types (see INTEGRATION.md for the
+ * ISO_C_BINDING shim) and calls these functions in place of the Fortran ones.
+ *
+ * Conventions shared by every struct below:
+ *   - quantum numbers are the reference's integer labels: num_up (particle
+ *     number, or 0 when up_bias = 0) and num_down (twice the total spin, 2S);
+ *   - every dense matrix is column-major (Fortran order) and addressed as
+ *     data + off, with off counted in doubles;
+ *   - all pointers are host pointers owned by the caller;
+ *   - every function returns 0 on success or a TJ_ERR_* code; the message of
+ *     the last error on the calling thread is returned by tj_last_error().
+ */
+#ifndef TJ_B200_H
+#define TJ_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ errors */
+enum {
+  TJ_OK = 0,
+  TJ_ERR_ARG = 1,         /* null pointer, negative or inconsistent size            */
+  TJ_ERR_QN = 2,          /* quantum-number mismatch (the reference calls `stop`)   */
+  TJ_ERR_CUDA = 3,        /* a CUDA runtime call failed                             */
+  TJ_ERR_NOMEM = 4,       /* device allocation failed                               */
+  TJ_ERR_NODEV = 5,       /* no CUDA device, or the device is not sm_100            */
+  TJ_ERR_TIMEOUT = 6,     /* a bounded device-side wait gave up                     */
+  TJ_ERR_NUMERIC = 7,     /* NaN/Inf met, or an eigen-solver did not converge       */
+  TJ_ERR_LIMIT = 8        /* a size exceeds a documented fixed limit                */
+};
+
+/* -------------------------------------------------------------- data types */
+
+/* Sub_Block + its mat(row_dim, sdim)  (code/tjsq/common.f90:114-117).
+ * The sub-block maps the sector (num_up, num_down) to
+ * (num_up + up_dif, num_down + down_dif); mat has row_dim rows (the target
+ * sector's dimension) and sdim columns (the source sector's dimension). */
+typedef struct tj_block_sub {
+  int32_t num_up, num_down, down_dif, row_dim, sdim, pad_;
+  int64_t off;
+} tj_block_sub;
+
+/* Total_Block  (code/tjsq/common.f90:119-122).  sub(1:num) = sub[0..num-1]. */
+typedef struct tj_block {
+  int32_t len, num, dim, up_dif, down_dif, pad_;
+  const tj_block_sub *sub;
+  const double *data;
+} tj_block;
+
+/* Block_Set  (code/tjsq/common.f90:139-141). */
+typedef struct tj_block_set {
+  tj_block elec_up, elec_down, spin_sd, spin_sz, num_sn;
+} tj_block_set;
+
+/* Total_Model  (code/tjsq/common.f90:144-149).  Only ham and sub(1:nsub) are
+ * inputs; snc(2) and sub_s(nxx) are produced by hmerge inside the library
+ * (code/tjsq/get_sys.f90:4383-4593). */
+typedef struct tj_model {
+  int32_t len, nsub;
+  tj_block ham;
+  const tj_block_set *sub;       /* sub(1:nsub) */
+} tj_model;
+
+/* Sub_Basis_Map  (code/tjsq/common.f90:65-69). */
+typedef struct tj_basis_sub {
+  int32_t spos, sdim, bl_num_up, bl_num_down, st_num_up, st_num_down;
+} tj_basis_sub;
+
+/* Basis_Map  (code/tjsq/common.f90:72-76); sub(1:num) = maps[first .. first+num-1]. */
+typedef struct tj_basis_map {
+  int32_t idx, num, dim, new_num_up, new_num_down, first;
+} tj_basis_map;
+
+/* Total_Basis  (code/tjsq/common.f90:79-82). */
+typedef struct tj_basis {
+  int32_t len, num, dim, pad_;
+  const tj_basis_map *sub;
+  const tj_basis_sub *maps;
+} tj_basis;
+
+/* Sub_Wave  (code/tjsq/common.f90:100-105); vec(sys_dim, env_dim) at data + off. */
+typedef struct tj_wave_sub {
+  int32_t sys_num_up, sys_num_down, env_num_up, env_num_down, sys_dim, env_dim;
+  int64_t off;
+} tj_wave_sub;
+
+/* Wavefunction  (code/tjsq/common.f90:107-110).  dim = sum sys_dim*env_dim. */
+typedef struct tj_wave {
+  int32_t sys_len, env_len, num, pad_;
+  int64_t dim;
+  const tj_wave_sub *sub;
+  double *data;
+} tj_wave;
+
+/* Module pubdata globals read on the hot path (code/tjsq/common.f90:10-45),
+ * passed with their Fortran shapes and lower bounds:
+ *   neib (0:num_site, neibt)      neib [(k-1)*(num_site+1) + i]
+ *   neiba(0:num_site, 0:num_site) neiba[j*(num_site+1) + i]
+ *   inb1 (0:num_site, 0:num_site) inb1 [j*(num_site+1) + i]
+ *   nleg11(1:num_site)            nleg11[i-1]
+ *   nposi, nposi_dm, nposi_lat (0:num_site)  x[i]
+ *   jt, jz, jd (neibt, 0:num_site)           x[i*neibt + (k-1)]
+ *   jn (neibt)                                jn[k-1]
+ *   esite (0:num_site)                        esite[i]
+ * up_bias is the parameter of common.f90:12 (0: grand-canonical labels).
+ * The site operators st_elec_up, st_sd, num_elec, st_si of
+ * Get_site_operator_su2_U0 (code/tjsq/dmrg_sub.f90:370-473) are rebuilt
+ * from up_bias inside the library. */
+typedef struct tj_lattice {
+  int32_t num_site, neibt, up_bias, pad_;
+  const int32_t *neib, *neiba, *inb1, *nleg11, *nposi, *nposi_dm, *nposi_lat;
+  const double *jt, *jz, *jd, *jn, *esite;
+} tj_lattice;
+
+/* Output of Get_truncation_operator (code/tjsq/den_mat.f90:141-383).
+ * Two-call pattern: call tj_truncation with data == NULL to learn num and
+ * the total number of doubles (data_len); allocate sub[num] and
+ * data[data_len]; call again to fill them.  trun_op sub-blocks have
+ * down_dif = 0, row_dim = sector dimension, sdim = kept columns. */
+typedef struct tj_trunc_result {
+  int32_t num_state;         /* kept states (Num_state)                             */
+  int32_t num;               /* kept sectors (trun_op%num)                          */
+  int64_t data_len;          /* doubles needed for all trun_op mats                 */
+  double trunc_err;          /* discarded weight of the renormalised spectrum       */
+  double entropy1, entropy2, entropys;  /* entropies of den_mat.f90:222-297         */
+  tj_block_sub *sub;         /* caller-allocated, num entries (or NULL)             */
+  double *data;              /* caller-allocated, data_len doubles (or NULL)        */
+} tj_trunc_result;
+
+/* -------------------------------------------------------------- context */
+typedef struct tj_ctx tj_ctx;
+
+enum { TJ_PREC_FP64 = 0, TJ_PREC_OZAKI = 1 };
+
+/* Creates a context bound to one CUDA device (one context per host thread). */
+int tj_ctx_create(tj_ctx **ctx, int device);
+int tj_ctx_destroy(tj_ctx *ctx);
+/* Arithmetic of the block GEMMs of H*psi: TJ_PREC_FP64, or TJ_PREC_OZAKI with
+ * `slices` int8 slices per operand (3..8). */
+int tj_set_precision(tj_ctx *ctx, int mode, int slices);
+/* Invalidates the operators and task lists cached for the current DMRG step. */
+int tj_step_begin(tj_ctx *ctx);
+const char *tj_last_error(void);
+
+/* ------------------------------------------------------- hot-path calls */
+
+/* model_wave(sys,env,sys_bs,env_bs,invec,outvec)  (code/tjsq/get_sys.f90:4127-4381),
+ * add_op = 1 branch, preceded by hmerge(sys,env,sys_bs,env_bs)
+ * (code/tjsq/get_sys.f90:4383-4593) as lanczos_memo_new does
+ * (code/tjsq/eigen.f90:53-56).  outvec must have invec's sector layout; it
+ * is overwritten. */
+int tj_model_wave(tj_ctx *ctx, const tj_lattice *lat,
+                  const tj_model *sys, const tj_model *env,
+                  const tj_basis *sys_bs, const tj_basis *env_bs,
+                  const tj_wave *invec, tj_wave *outvec);
+
+/* lanczos_memo_new(sys,env,sys_bs,env_bs,super,eigvec,levels,num_idx)
+ * (code/tjsq/eigen.f90:2-175) for levels = 1: eigvec is the start vector on
+ * entry and the normalised Ritz vector on return; energies[0] = Energys(1);
+ * iters = Lanczos vectors used.  lanzero is the module global Lanzero. */
+int tj_lanczos_memo_new(tj_ctx *ctx, const tj_lattice *lat,
+                        const tj_model *sys, const tj_model *env,
+                        const tj_basis *sys_bs, const tj_basis *env_bs,
+                        tj_wave *eigvec, int levels, double lanzero,
+                        double *energies, int *iters);
+
+/* Get_density_matrix_{sys,env}_new + Get_truncation_operator
+ * (code/tjsq/den_mat.f90:84-134, 141-383) for levels = 1.
+ * side = 0: system block (rho = psi psi^T), side = 1: environment block
+ * (rho = psi^T psi).  The block length written to the result's sub-blocks is
+ * wave->sys_len or wave->env_len. */
+int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side,
+                  int kept_min, int kept_max, double trun_err,
+                  tj_trunc_result *out);
+
+/* Correlator contractions value = <psi| O |psi> (code/tjsq/measure.f90).
+ * flag is 'B' (boson) or 'F' (fermion) as FlagSign in the reference. */
+int tj_measure_sys_block(tj_ctx *ctx, const tj_block *sys_bl, const tj_basis *sys_bs,
+                         const tj_wave *wave, double *value);              /* :1241-1295 */
+int tj_measure_env_block(tj_ctx *ctx, const tj_block *env_bl, const tj_basis *env_bs,
+                         const tj_wave *wave, double *value);              /* :1359-1414 */
+int tj_sys_block_env_block_cor_dia(tj_ctx *ctx, const tj_block *sys_bl, const tj_block *env_bl,
+                                   const tj_basis *sys_bs, const tj_basis *env_bs,
+                                   const tj_wave *wave, double *value);    /* :1638-1732 */
+int tj_sys_block_env_block_cor_ndia(tj_ctx *ctx, const tj_block *sys_bl, const tj_block *env_bl,
+                                    const tj_basis *sys_bs, const tj_basis *env_bs,
+                                    const tj_wave *wave, char flag, double *value); /* :5241-5480 */
+int tj_sys_block_site_cor_ndia(tj_ctx *ctx, const tj_block *sys_bl, const tj_block *sys_st,
+                               const tj_basis *sys_bs, const tj_wave *wave,
+                               char flag, double *value);                  /* :4939-5083 */
+int tj_env_block_site_cor_ndia(tj_ctx *ctx, const tj_block *env_bl, const tj_block *env_st,
+                               const tj_basis *env_bs, const tj_wave *wave,
+                               char flag, double *value);                  /* :5085-5238 */
+int tj_sys_block_env_site_cor_ndia(tj_ctx *ctx, const tj_block *sys_bl, const tj_block *env_st,
+                                   const tj_basis *sys_bs, const tj_basis *env_bs,
+                                   const tj_wave *wave, char flag, double *value); /* :5482-5706 */
+int tj_sys_site_env_block_cor_ndia(tj_ctx *ctx, const tj_block *sys_st, const tj_block *env_bl,
+                                   const tj_basis *sys_bs, const tj_basis *env_bs,
+                                   const tj_wave *wave, char flag, double *value); /* :5926-6154 */
+int tj_sys_site_env_site_cor_ndia(tj_ctx *ctx, const tj_block *sys_st, const tj_block *env_st,
+                                  const tj_basis *sys_bs, const tj_basis *env_bs,
+                                  const tj_wave *wave, char flag, double *value); /* :5709-5924 */
+
+/* --------------------------------------------------- measurement support */
+
+/* Statistics of the H*psi task list compiled for the last tj_model_wave /
+ * tj_lanczos_memo_new call: flops and bytes per H*psi (the algorithmic work
+ * used for the roofline), task and tile counts, and the device time of the
+ * last H*psi in milliseconds (CUDA events on the context's stream). */
+typedef struct tj_hpsi_stats {
+  double flops;            /* executed FP64-equivalent flops per H*psi           */
+  double flops_ref;        /* flops of the reference's DGEMM sequence           */
+  double bytes;            /* algorithmic HBM bytes per H*psi                    */
+  int64_t n_products, n_tasks, n_tiles_p1, n_tiles_p2, scratch_doubles;
+  double last_ms;          /* device time of the last H*psi                      */
+  double last_ms_phase1, last_ms_phase2;
+} tj_hpsi_stats;
+int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st);
+
+/* Device-resident benchmarking helper: uploads invec once, then runs `reps`
+ * H*psi products back to back on the device (inputs resident in HBM), with
+ * CUDA events around the whole loop; *ms is the mean device time per H*psi.
+ * The result of the last product is copied to outvec. */
+int tj_model_wave_bench(tj_ctx *ctx, const tj_lattice *lat,
+                        const tj_model *sys, const tj_model *env,
+                        const tj_basis *sys_bs, const tj_basis *env_bs,
+                        const tj_wave *invec, tj_wave *outvec, int reps, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TJ_B200_H */
