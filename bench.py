@@ -1,0 +1,291 @@
+#!/usr/bin/env python
+"""Benchmark of the tjsq hot path on B200: H*psi per second on a 4x24 t-J
+cylinder superblock at m = 2000 multiplets (mid-chain, 12 holes, S = 0).
+
+One "step" is one H*psi (hmerge'd model_wave) over the whole superblock with
+operators and psi resident in HBM.  The superblock is synthetic (seeded):
+sector tables, bases and operator blocks with the reference's quantum-number
+structure at the sizes of that configuration (no DMRG run of the reference
+can be reproduced here).  Its operators (about 0.2 GB) and phase-1 products
+(about 0.14 GB) exceed the 126 MB L2, so no explicit L2 flush is done.
+
+  python bench.py [--gpus N --steps K --warmup W --impl b200|reference]
+
+--impl reference times the oracle (the C restatement of the reference's
+Fortran routines, FP64, OpenBLAS with every host thread) on the same
+workload; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "H·ψ/s & sweep time, 4×24 t-J m=2000: mixed vs FP64 GPU at ΔE/site≤1e-9"
+UNIT = "H*psi/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="cyl4x24_m2000")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "ozaki"])
+    ap.add_argument("--slices", type=int, default=6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--seed", type=int, default=1234)
+    return ap.parse_args()
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, n in enumerate(names):
+                    if r[4 + k].lower().startswith("active"):
+                        reasons.add(n)
+            except Exception:
+                pass
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "b200" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def allmax(pg, x: float, impl: str) -> float:
+    if pg is None:
+        return x
+    import torch
+    dev = "cuda" if impl == "b200" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, impl):
+    if pg is not None:
+        if impl == "b200":
+            import torch
+            pg.barrier(device_ids=[torch.cuda.current_device()])
+        else:
+            pg.barrier()
+
+
+def fp64_peak_tflops(device: int) -> float:
+    """cuBLAS DGEMM throughput on this GPU (best of a few 8192^3 products)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda:%d" % device)
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda:%d" % device)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2.0 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def cpu_reference(sb, steps: int, warmup: int, threads: int):
+    """Times the oracle's model_wave (hmerge included) on the host."""
+    from oracle import oracle
+    oracle.lib(threads)
+    oracle.set_threads(threads)
+    for _ in range(warmup):
+        oracle.model_wave(sb)
+    t = time.perf_counter()
+    for _ in range(steps):
+        oracle.model_wave(sb)
+    dt = time.perf_counter() - t
+    return steps / dt, dt / steps
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def profile_traffic(workload: str, precision: str):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "roofline_inputs.json")) as f:
+            d = json.load(f)
+        return d.get(workload, {}).get(precision, {}).get("traffic_bytes_per_hpsi")
+    except Exception:
+        return None
+
+
+def main():
+    args = parse()
+    ws, rank, local, pg = dist_init(args)
+    from grand_sql_tj_b200 import synth
+    sb = synth.workload(args.workload, seed=args.seed + (rank if args.impl == "b200" else 0))
+    cfg = {"workload": args.workload, "lattice": "4x24 cylinder (y periodic, x open)" if "4x24" in args.workload else args.workload,
+           "m": 2000 if "m2000" in args.workload else None, "t": 1.0, "J": 1.0 / 3.0, "holes": 12,
+           "sys_len": sb.sys.len, "env_len": sb.env.len, "psi_dim": sb.wave.dim,
+           "sectors": len(sb.wave.sectors), "l2": "inputs larger than L2 (no flush)",
+           "parallelism": "replicas" if ws > 1 else "single"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            barrier(pg, args.impl)
+            return
+        threads = os.cpu_count() or 1
+        steps = max(1, min(args.steps, 8))
+        warm = min(args.warmup, 1)
+        rate, sec = cpu_reference(sb, steps, warm, threads)
+        line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": ws,
+                "steps": steps, "warmup": warm, "ms_per_step": sec * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": cfg,
+                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                 "sample": "%d model_wave calls of the oracle (C restatement of get_sys.f90 "
+                                           "model_wave + hmerge, OpenBLAS dgemm)" % steps},
+                "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        barrier(pg, args.impl)
+        return
+
+    from grand_sql_tj_b200 import build as B
+    B.build()
+    from grand_sql_tj_b200.lib import Context, TJ_PREC_FP64, TJ_PREC_OZAKI
+    ctx = Context(local)
+    if args.precision == "ozaki":
+        ctx.set_precision(TJ_PREC_OZAKI, args.slices)
+    # warm-up (compiles the plan, uploads operators and psi)
+    ms_w, _ = ctx.model_wave_bench(sb, max(args.warmup, 3))
+    barrier(pg, args.impl)
+    with Clocks(local) as clk:
+        barrier(pg, args.impl)
+        t0 = time.perf_counter()
+        ms, out = ctx.model_wave_bench(sb, args.steps)
+        wall = time.perf_counter() - t0
+        barrier(pg, args.impl)
+    st = ctx.stats()
+    ms_max = allmax(pg, ms, args.impl)
+    value = ws * 1000.0 / ms_max
+
+    # end to end through the reference-facing call: lanczos_memo_new with host buffers
+    ctx.step_begin()
+    lz = 20.0e-6
+    t0 = time.perf_counter()
+    e0, iters, _ = ctx.lanczos_memo_new(sb, lz)
+    e2e_wall = time.perf_counter() - t0
+    st2 = ctx.stats()
+    nh = max(int(st2.lanczos_hpsi), 1)
+    e2e_wall = allmax(pg, e2e_wall, args.impl)
+    ops_bytes = 0
+    for m in (sb.sys, sb.env):
+        ops_bytes += sum(s.mat.size for s in m.ham.subs) * 8
+        for bs in m.sub:
+            for k in ("elec_up", "elec_down", "spin_sd", "num_sn"):
+                ops_bytes += sum(s.mat.size for s in getattr(bs, k).subs) * 8
+    e2e = {"value": ws * nh / e2e_wall, "unit": UNIT, "via": "tj_lanczos_memo_new (plan + operator upload + "
+           "%d H*psi + Ritz vector download)" % nh,
+           "h2d_bytes_per_step": int((ops_bytes + 8 * sb.wave.dim) / nh),
+           "d2h_bytes_per_step": int(8 * sb.wave.dim / nh), "lanczos_iters": iters, "E0": e0}
+
+    peaks = measured_peaks()
+    if rank == 0:
+        fp64 = fp64_peak_tflops(local)
+    else:
+        fp64 = None
+    achieved = st.flops / (ms * 1e-3) / 1e12
+    roof = {"bound": "tensor", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
+            "frac": (achieved / fp64) if fp64 else None, "traffic": profile_traffic(args.workload, args.precision),
+            "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU (FP64; not in MEASURED_PEAKS.json)",
+            "flops_per_hpsi": st.flops, "flops_ref_per_hpsi": st.flops_ref, "bytes_per_hpsi": st.bytes,
+            "hbm_frac": (st.bytes / (ms * 1e-3) / 1e9) / peaks.get("hbm_gbs", 6555.8),
+            "phase1_ms": st.last_ms_phase1, "phase2_ms": st.last_ms_phase2}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, sec = cpu_reference(sb, 2, 0, threads)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": "2 model_wave calls of the oracle on the same superblock"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": max(args.warmup, 3), "ms_per_step": ms_max, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "int8-ozaki",
+                "data": "synthetic", "config": cfg, "precision": args.precision,
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+                "gpu_launches": 2 * args.steps, "wall_s_timed": wall}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

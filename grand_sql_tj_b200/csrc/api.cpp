@@ -1,0 +1,428 @@
+// extern "C" entry points of include/tj_b200.h: context, H*psi and Lanczos.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "ctx.h"
+
+using namespace tjb;
+
+static thread_local std::string g_err;
+const char *tj_last_error(void) { return g_err.c_str(); }
+int tjb::set_err(int code, const std::string &m) {
+  g_err = m;
+  return code;
+}
+int tjb_set_err(int code, const std::string &m) { return tjb::set_err(code, m); }
+
+#define CK(call)                                                                                \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) return set_err(TJ_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ------------------------------------------------------------ device arrays
+int tjb::dev_reserve(void **p, size_t *cap, size_t bytes) {
+  if (bytes <= *cap && *p) return TJ_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  size_t want = bytes + bytes / 8 + 256;
+  cudaError_t e = cudaMalloc(p, want);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return set_err(TJ_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  *cap = want;
+  return TJ_OK;
+}
+
+tj_ctx::~tj_ctx() {
+  cudaSetDevice(device);
+  for (DevBuf *b : all_bufs()) b->release();
+  for (auto &e : ev)
+    if (e) cudaEventDestroy(e);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+extern "C" int tj_ctx_create(tj_ctx **out, int device) {
+  if (!out) return set_err(TJ_ERR_ARG, "tj_ctx_create: null output");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return set_err(TJ_ERR_NODEV, "no CUDA device");
+  if (device < 0 || device >= n) return set_err(TJ_ERR_ARG, "device index out of range");
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) return set_err(TJ_ERR_NODEV, "this library is built for sm_100a (B200) only");
+  std::unique_ptr<tj_ctx> c(new tj_ctx());
+  c->device = device;
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  for (auto &e : c->ev) CK(cudaEventCreate(&e));
+  *out = c.release();
+  return TJ_OK;
+}
+
+extern "C" int tj_ctx_destroy(tj_ctx *ctx) {
+  delete ctx;
+  return TJ_OK;
+}
+
+extern "C" int tj_set_precision(tj_ctx *ctx, int mode, int slices) {
+  if (!ctx) return set_err(TJ_ERR_ARG, "null context");
+  if (mode != TJ_PREC_FP64 && mode != TJ_PREC_OZAKI) return set_err(TJ_ERR_ARG, "unknown precision mode");
+  if (mode == TJ_PREC_OZAKI && (slices < 3 || slices > 8)) return set_err(TJ_ERR_ARG, "slices must be 3..8");
+  ctx->prec_mode = mode;
+  ctx->slices = slices;
+  ctx->plan_valid = false;
+  return TJ_OK;
+}
+
+extern "C" int tj_step_begin(tj_ctx *ctx) {
+  if (!ctx) return set_err(TJ_ERR_ARG, "null context");
+  ctx->plan_valid = false;
+  return TJ_OK;
+}
+
+extern "C" int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st) {
+  if (!ctx || !st) return set_err(TJ_ERR_ARG, "null argument");
+  *st = ctx->stats;
+  return TJ_OK;
+}
+
+// ------------------------------------------------------------ plan upload
+template <class T>
+static int upload_vec(tj_ctx *ctx, DevBuf &b, const std::vector<T> &v) {
+  int rc = b.reserve(v.size() * sizeof(T) + sizeof(T));
+  if (rc) return rc;
+  if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  return TJ_OK;
+}
+
+static uint64_t fnv(uint64_t h, const void *p, size_t n) {
+  const unsigned char *c = (const unsigned char *)p;
+  for (size_t i = 0; i < n; ++i) {
+    h ^= c[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+static uint64_t key_block(uint64_t h, const tj_block &b) {
+  h = fnv(h, &b, sizeof b);
+  if (b.num > 0 && b.sub) h = fnv(h, b.sub, sizeof(tj_block_sub) * b.num);
+  return h;
+}
+static uint64_t key_model(uint64_t h, const tj_model *m) {
+  h = fnv(h, m, sizeof *m);
+  h = key_block(h, m->ham);
+  for (int i = 0; i < m->nsub; ++i) {
+    const tj_block_set &s = m->sub[i];
+    h = key_block(key_block(key_block(key_block(key_block(h, s.elec_up), s.elec_down), s.spin_sd), s.spin_sz), s.num_sn);
+  }
+  return h;
+}
+static uint64_t key_basis(uint64_t h, const tj_basis *b) {
+  h = fnv(h, b, sizeof *b);
+  h = fnv(h, b->sub, sizeof(tj_basis_map) * b->num);
+  int nm = 0;
+  for (int i = 0; i < b->num; ++i) nm = std::max(nm, b->sub[i].first + b->sub[i].num);
+  return fnv(h, b->maps, sizeof(tj_basis_sub) * nm);
+}
+static uint64_t key_lattice(uint64_t h, const tj_lattice *L) {
+  const size_t ns1 = L->num_site + 1;
+  h = fnv(h, L, sizeof *L);
+  h = fnv(h, L->neib, sizeof(int32_t) * ns1 * L->neibt);
+  h = fnv(h, L->neiba, sizeof(int32_t) * ns1 * ns1);
+  h = fnv(h, L->inb1, sizeof(int32_t) * ns1 * ns1);
+  h = fnv(h, L->nleg11, sizeof(int32_t) * L->num_site);
+  h = fnv(h, L->nposi, sizeof(int32_t) * ns1);
+  h = fnv(h, L->nposi_dm, sizeof(int32_t) * ns1);
+  h = fnv(h, L->nposi_lat, sizeof(int32_t) * ns1);
+  h = fnv(h, L->jt, sizeof(double) * ns1 * L->neibt);
+  h = fnv(h, L->jz, sizeof(double) * ns1 * L->neibt);
+  h = fnv(h, L->jd, sizeof(double) * ns1 * L->neibt);
+  h = fnv(h, L->jn, sizeof(double) * L->neibt);
+  return fnv(h, L->esite, sizeof(double) * ns1);
+}
+
+// Compiles (or reuses) the plan of H*psi and uploads operators and work lists.
+int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const tj_model *env,
+                      const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave) {
+  if (!ctx || !lat || !sys || !env || !sys_bs || !env_bs || !wave) return set_err(TJ_ERR_ARG, "null argument");
+  if (!lat->neib || !lat->nleg11 || !lat->jt || !sys->sub || !env->sub || !sys_bs->sub || !env_bs->sub || !wave->sub)
+    return set_err(TJ_ERR_ARG, "null table in the inputs");
+  uint64_t h = 1469598103934665603ull;
+  h = key_lattice(h, lat);
+  h = key_model(h, sys);
+  h = key_model(h, env);
+  h = key_basis(h, sys_bs);
+  h = key_basis(h, env_bs);
+  h = fnv(h, wave->sub, sizeof(tj_wave_sub) * wave->num);
+  h = fnv(h, &ctx->prec_mode, sizeof ctx->prec_mode);
+  if (ctx->plan_valid && ctx->plan_key == h) return TJ_OK;
+  ctx->plan_valid = false;
+  CK(cudaSetDevice(ctx->device));
+  std::unique_ptr<HpsiPlan> P(new HpsiPlan());
+  std::string msg;
+  int rc = build_hpsi_plan(lat, sys, env, sys_bs, env_bs, wave, *P, msg);
+  if (rc) return set_err(rc, "H*psi plan: " + msg);
+  // operators: one copy per input block, then the merged sums on the device
+  if ((rc = ctx->ops.reserve(sizeof(double) * (P->ops_len + 4)))) return rc;
+  for (const auto &u : P->uploads)
+    if (u.n > 0)
+      CK(cudaMemcpyAsync(ctx->ops.d() + u.dst, u.src, sizeof(double) * u.n, cudaMemcpyHostToDevice, ctx->stream));
+  {
+    std::vector<int64_t> dst, n;
+    std::vector<int32_t> sb, se;
+    for (const auto &m : P->merges) {
+      dst.push_back(m.dst);
+      n.push_back(m.n);
+      sb.push_back(m.s_begin);
+      se.push_back(m.s_end);
+    }
+    if ((rc = upload_vec(ctx, ctx->m_dst, dst)) || (rc = upload_vec(ctx, ctx->m_n, n)) ||
+        (rc = upload_vec(ctx, ctx->m_sb, sb)) || (rc = upload_vec(ctx, ctx->m_se, se)) ||
+        (rc = upload_vec(ctx, ctx->m_src, P->merge_src)) || (rc = upload_vec(ctx, ctx->m_coef, P->merge_coef)))
+      return rc;
+    launch_merge(ctx->ops.d(), (const int64_t *)ctx->m_dst.p, (const int64_t *)ctx->m_n.p,
+                 (const int32_t *)ctx->m_sb.p, (const int32_t *)ctx->m_se.p, (const int64_t *)ctx->m_src.p,
+                 (const double *)ctx->m_coef.p, (int)P->merges.size(), ctx->stream);
+    CK(cudaGetLastError());
+  }
+  if ((rc = upload_vec(ctx, ctx->cells1, P->cells1)) || (rc = upload_vec(ctx, ctx->cells2, P->cells2)) ||
+      (rc = upload_vec(ctx, ctx->tasks1, P->tasks1)) || (rc = upload_vec(ctx, ctx->tasks2, P->tasks2)) ||
+      (rc = upload_vec(ctx, ctx->tiles1, P->tiles1)) || (rc = upload_vec(ctx, ctx->tiles2, P->tiles2)))
+    return rc;
+  if ((rc = ctx->scr.reserve(sizeof(double) * (P->scratch_len + 4)))) return rc;
+  if ((rc = ctx->counters.reserve(64))) return rc;
+  if ((rc = ctx->partials.reserve(sizeof(double) * (std::max(P->tiles2.size(), P->tiles1.size()) + 4096))))
+    return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->stats = tj_hpsi_stats();
+  ctx->stats.flops = P->flops;
+  ctx->stats.flops_ref = P->flops_ref;
+  ctx->stats.bytes = P->bytes;
+  ctx->stats.n_products = (int64_t)P->cells1.size();
+  ctx->stats.n_tasks = (int64_t)P->tasks2.size();
+  ctx->stats.n_tiles_p1 = (int64_t)P->tiles1.size();
+  ctx->stats.n_tiles_p2 = (int64_t)P->tiles2.size();
+  ctx->stats.scratch_doubles = P->scratch_len;
+  ctx->plan = std::move(P);
+  ctx->plan_key = h;
+  ctx->plan_valid = true;
+  return TJ_OK;
+}
+
+// out = H * in on the device (both device pointers in the plan's psi layout).
+int tjb::run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed) {
+  const HpsiPlan &P = *ctx->plan;
+  unsigned int *cnt = (unsigned int *)ctx->counters.p;
+  CK(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), ctx->stream));
+  if (timed) CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+  GemmParams g;
+  std::memset(&g, 0, sizeof g);
+  g.ops = ctx->ops.d();
+  g.psi = in;
+  g.scr = ctx->scr.d();
+  g.out = ctx->scr.d();
+  g.cells = (const Cell *)ctx->cells1.p;
+  g.tasks = (const Task *)ctx->tasks1.p;
+  g.tiles = (const Tile *)ctx->tiles1.p;
+  g.ntiles = (int)P.tiles1.size();
+  g.counter = cnt;
+  launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles), ctx->stream);
+  if (timed) CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+  g.out = out;
+  g.cells = (const Cell *)ctx->cells2.p;
+  g.tasks = (const Task *)ctx->tasks2.p;
+  g.tiles = (const Tile *)ctx->tiles2.p;
+  g.ntiles = (int)P.tiles2.size();
+  g.counter = cnt + 1;
+  launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles), ctx->stream);
+  if (timed) CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+  CK(cudaGetLastError());
+  ++ctx->n_hpsi;
+  return TJ_OK;
+}
+
+static int check_wave(const tj_wave *w) {
+  if (!w || w->num < 0 || (w->num > 0 && (!w->sub || !w->data)) || w->dim < 0)
+    return set_err(TJ_ERR_ARG, "bad wavefunction");
+  int64_t d = 0;
+  for (int i = 0; i < w->num; ++i) {
+    if (w->sub[i].sys_dim < 0 || w->sub[i].env_dim < 0 || w->sub[i].off < 0) return set_err(TJ_ERR_ARG, "bad sector");
+    d = std::max(d, w->sub[i].off + (int64_t)w->sub[i].sys_dim * w->sub[i].env_dim);
+  }
+  if (d > w->dim) return set_err(TJ_ERR_ARG, "sector extends past wave->dim");
+  return TJ_OK;
+}
+static bool same_layout(const tj_wave *a, const tj_wave *b) {
+  if (a->num != b->num || a->dim != b->dim) return false;
+  return std::memcmp(a->sub, b->sub, sizeof(tj_wave_sub) * a->num) == 0;
+}
+
+extern "C" int tj_model_wave(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const tj_model *env,
+                             const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *invec,
+                             tj_wave *outvec) {
+  int rc;
+  if (!ctx) return set_err(TJ_ERR_ARG, "null context");
+  if ((rc = check_wave(invec)) || (rc = check_wave(outvec))) return rc;
+  if (!same_layout(invec, outvec)) return set_err(TJ_ERR_ARG, "outvec must have invec's sector layout");
+  CK(cudaSetDevice(ctx->device));
+  if ((rc = prepare_hpsi(ctx, lat, sys, env, sys_bs, env_bs, invec))) return rc;
+  const int64_t D = invec->dim;
+  if ((rc = ctx->vin.reserve(sizeof(double) * (D + 4))) || (rc = ctx->vout.reserve(sizeof(double) * (D + 4))))
+    return rc;
+  CK(cudaMemcpyAsync(ctx->vin.d(), invec->data, sizeof(double) * D, cudaMemcpyHostToDevice, ctx->stream));
+  if ((rc = run_hpsi(ctx, ctx->vin.d(), ctx->vout.d(), true))) return rc;
+  CK(cudaMemcpyAsync(outvec->data, ctx->vout.d(), sizeof(double) * D, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  float a = 0, b = 0;
+  cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+  cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+  ctx->stats.last_ms_phase1 = a;
+  ctx->stats.last_ms_phase2 = b;
+  ctx->stats.last_ms = a + b;
+  return TJ_OK;
+}
+
+extern "C" int tj_model_wave_bench(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const tj_model *env,
+                                   const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *invec,
+                                   tj_wave *outvec, int reps, double *ms) {
+  int rc;
+  if (!ctx || !ms || reps < 1) return set_err(TJ_ERR_ARG, "bad argument");
+  if ((rc = check_wave(invec)) || (rc = check_wave(outvec))) return rc;
+  if (!same_layout(invec, outvec)) return set_err(TJ_ERR_ARG, "outvec must have invec's sector layout");
+  CK(cudaSetDevice(ctx->device));
+  if ((rc = prepare_hpsi(ctx, lat, sys, env, sys_bs, env_bs, invec))) return rc;
+  const int64_t D = invec->dim;
+  if ((rc = ctx->vin.reserve(sizeof(double) * (D + 4))) || (rc = ctx->vout.reserve(sizeof(double) * (D + 4))))
+    return rc;
+  CK(cudaMemcpyAsync(ctx->vin.d(), invec->data, sizeof(double) * D, cudaMemcpyHostToDevice, ctx->stream));
+  if ((rc = run_hpsi(ctx, ctx->vin.d(), ctx->vout.d(), false))) return rc;   // warm-up
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+  double p1 = 0, p2 = 0;
+  for (int r = 0; r < reps; ++r) {
+    if ((rc = run_hpsi(ctx, ctx->vin.d(), ctx->vout.d(), true))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+    p1 += a;
+    p2 += b;
+  }
+  *ms = (p1 + p2) / reps;
+  ctx->stats.last_ms_phase1 = p1 / reps;
+  ctx->stats.last_ms_phase2 = p2 / reps;
+  ctx->stats.last_ms = *ms;
+  CK(cudaMemcpyAsync(outvec->data, ctx->vout.d(), sizeof(double) * D, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return TJ_OK;
+}
+
+// ----------------------------------------------------------------- Lanczos
+// lanczos_memo_new (code/tjsq/eigen.f90:2-175) with levels = 1: three-term
+// recurrence, full classical Gram-Schmidt against all previous vectors, the
+// lowest Ritz value of the tridiagonal matrix after every step, stop when it
+// moves by <= lanzero (or when beta <= lanzero, or after 110 vectors), then
+// the Ritz vector.  All vectors live on the device; the host reads two
+// scalars per step (beta and the Ritz value) to take the stop decisions.
+extern "C" int tj_lanczos_memo_new(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const tj_model *env,
+                                   const tj_basis *sys_bs, const tj_basis *env_bs, tj_wave *eigvec, int levels,
+                                   double lanzero, double *energies, int *iters) {
+  const int LOOP_IN = 110;
+  int rc;
+  if (!ctx || !energies || !iters) return set_err(TJ_ERR_ARG, "null argument");
+  if (levels != 1) return set_err(TJ_ERR_ARG, "only levels = 1 is supported (main.f90 sets levels = 1)");
+  if ((rc = check_wave(eigvec))) return rc;
+  CK(cudaSetDevice(ctx->device));
+  if ((rc = prepare_hpsi(ctx, lat, sys, env, sys_bs, env_bs, eigvec))) return rc;
+  const int64_t D = eigvec->dim;
+  const int64_t ld = (D + 31) / 32 * 32;
+  if ((rc = ctx->lanV.reserve(sizeof(double) * ld * (LOOP_IN + 2)))) return rc;
+  const int nblk = dot_blocks(D);
+  const int mdb = (int)((D + 256 * 8 - 1) / (256 * 8));
+  if ((rc = ctx->lanScal.reserve(sizeof(double) * 1024))) return rc;
+  if ((rc = ctx->lanPart.reserve(sizeof(double) * ((size_t)std::max(nblk, 1) + (size_t)std::max(mdb, 1) * 128 + 256))))
+    return rc;
+  double *V = ctx->lanV.d();
+  double *S = ctx->lanScal.d();   // [0..127] alpha, [128..255] beta, [256..383] uu, [384..511] coef, [512] lam, [513] nrm, [600..727] dz
+  double *alpha = S, *beta = S + 128, *uu = S + 256, *coef = S + 384, *lam = S + 512, *nrm = S + 513, *dz = S + 600;
+  double *part = ctx->lanPart.d(), *mpart = part + nblk;
+  auto vec = [&](int j) { return V + (int64_t)(j - 1) * ld; };   // tempvec(j), 1-based
+  auto norm_into = [&](const double *x, double *res) {
+    launch_dot(x, x, D, part, nblk, ctx->stream);
+    launch_sum(part, nblk, res, 1, ctx->stream);
+  };
+  auto dot_into = [&](const double *x, const double *y, double *res) {
+    launch_dot(x, y, D, part, nblk, ctx->stream);
+    launch_sum(part, nblk, res, 0, ctx->stream);
+  };
+  auto fetch = [&](const double *d, double *h) -> int {
+    CK(cudaMemcpyAsync(h, d, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TJ_OK;
+  };
+  const auto t0 = std::chrono::steady_clock::now();
+  CK(cudaMemsetAsync(S, 0, sizeof(double) * 1024, ctx->stream));
+  CK(cudaMemcpyAsync(vec(1), eigvec->data, sizeof(double) * D, cudaMemcpyHostToDevice, ctx->stream));
+  norm_into(vec(1), nrm);
+  launch_scale_inv(vec(1), nrm, D, ctx->stream);
+  dot_into(vec(1), vec(1), uu + 1);
+  const int64_t h0 = ctx->n_hpsi;
+  if ((rc = run_hpsi(ctx, vec(1), vec(2), false))) return rc;
+  dot_into(vec(1), vec(2), alpha + 1);
+  double ritzmin = 0, hb = 0, hl = 0;
+  if ((rc = fetch(alpha + 1, &ritzmin))) return rc;
+  int last = 1;
+  while (last < LOOP_IN) {
+    launch_lanczos_update(vec(last + 1), vec(last), last >= 2 ? vec(last - 1) : nullptr, alpha + last,
+                          beta + last - 1, D, ctx->stream);
+    norm_into(vec(last + 1), beta + last);
+    if ((rc = fetch(beta + last, &hb))) return rc;
+    if (!std::isfinite(hb)) return set_err(TJ_ERR_NUMERIC, "Lanczos: non-finite beta");
+    if (std::fabs(hb) <= lanzero) break;
+    launch_scale_inv(vec(last + 1), beta + last, D, ctx->stream);
+    // Gram_Schmidt_process (block.f90:2515-2551)
+    launch_multi_dot(V, ld, last, vec(last + 1), D, mpart, mdb, 128, ctx->stream);
+    launch_multi_sum(mpart, mdb, last, 128, uu + 1, coef, ctx->stream);
+    launch_combine(V, ld, last, coef, vec(last + 1), D, 0, ctx->stream);
+    norm_into(vec(last + 1), nrm);
+    launch_scale_inv(vec(last + 1), nrm, D, ctx->stream);
+    ++last;
+    dot_into(vec(last), vec(last), uu + last);
+    if ((rc = run_hpsi(ctx, vec(last), vec(last + 1), false))) return rc;
+    dot_into(vec(last), vec(last + 1), alpha + last);
+    launch_tridiag_min(alpha + 1, beta + 1, last, lam, nullptr, 0, ctx->stream);
+    CK(cudaGetLastError());
+    if ((rc = fetch(lam, &hl))) return rc;
+    if (!std::isfinite(hl)) return set_err(TJ_ERR_NUMERIC, "Lanczos: non-finite Ritz value");
+    if (std::fabs(hl - ritzmin) <= lanzero || last == LOOP_IN) {
+      ritzmin = hl;
+      break;
+    }
+    ritzmin = hl;
+  }
+  // label 411: dstev('V') and the Ritz vector
+  launch_tridiag_min(alpha + 1, beta + 1, last, lam, dz, 1, ctx->stream);
+  if ((rc = ctx->vout.reserve(sizeof(double) * (D + 4)))) return rc;
+  launch_combine(V, ld, last, dz, ctx->vout.d(), D, 1, ctx->stream);
+  norm_into(ctx->vout.d(), nrm);
+  launch_scale_inv(ctx->vout.d(), nrm, D, ctx->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(eigvec->data, ctx->vout.d(), sizeof(double) * D, cudaMemcpyDeviceToHost, ctx->stream));
+  if ((rc = fetch(lam, &hl))) return rc;
+  energies[0] = hl;
+  *iters = last;
+  ctx->stats.lanczos_hpsi = ctx->n_hpsi - h0;
+  ctx->stats_lanczos_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return TJ_OK;
+}

@@ -1,0 +1,1215 @@
+// Host-side compiler of H*psi (model_wave + hmerge) into grouped-GEMM work lists.
+//
+// For every term kernel that model_wave calls (code/tjsq/get_sys.f90:4127-4240,
+// add_op = 1) this file walks the same loop nest over psi sectors, basis
+// sub-blocks, spin-transfer channels and target total spins, applies the same
+// look-up rules and the same recoupling coefficient (6j products, sqrt and
+// sign factors), and records each surviving DGEMM pair as a task instead of
+// executing it.  The operators that hmerge (get_sys.f90:4383-4593) pre-sums
+// become "merged" sub-blocks computed on the device.  Transposed environment
+// operators (block_transfer_trans, block.f90:1676-1706) are never copied: a
+// transposed view only flips the operand's transpose flag.
+#include <algorithm>
+#include <array>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <stdexcept>
+#include <tuple>
+#include <unordered_map>
+
+#include "tj_internal.h"
+
+int tjb_set_err(int code, const std::string &m);
+
+namespace tjb {
+
+// ----------------------------------------------------------------- 6j symbol
+// Racah's single-sum formula for {j1 j2 j3; l1 l2 l3} with doubled spins, as
+// in W6JS (block.f90:1564-1615): triangle and parity checks, then the
+// alternating sum over w with factorial weights.  The factorial table holds
+// 0!..142! like FACTRL (block.f90:1508-1516).
+static double g_fact[302];
+static bool g_fact_ready = false;
+static inline double fct(int i) { return (i >= 0 && i <= 301) ? g_fact[i] : 0.0; }
+
+double w6j(int j1, int j2, int j3, int l1, int l2, int l3) {
+  if (!g_fact_ready) {
+    std::fill(g_fact, g_fact + 302, 0.0);
+    g_fact[0] = 1.0;
+    for (int i = 1; i <= 142; ++i) g_fact[i] = g_fact[i - 1] * (double)(float)i;
+    g_fact_ready = true;
+  }
+  const int a = j1 + j2, b = j1 - j2, c = j1 + l2, d = j1 - l2;
+  const int e = l1 + j2, f = l1 - j2, g = l1 + l2, h = l1 - l2;
+  if (a < j3 || std::abs(b) > j3 || c < l3 || std::abs(d) > l3) return 0.0;
+  if (e < l3 || std::abs(f) > l3 || g < j3 || std::abs(h) > j3) return 0.0;
+  const int s1 = a + j3, s2 = c + l3, s3 = e + l3, s4 = g + j3;
+  if ((s1 | s2 | s3 | s4) & 1) return 0.0;
+  const int wmin = std::max(std::max(s1, s2), std::max(s3, s4));
+  const int ii = a + g, ij = j2 + j3 + l2 + l3, ik = j3 + j1 + l3 + l1;
+  const int wmax = std::min(ii, std::min(ij, ik));
+  double omega = 0.0;
+  for (int w = wmin; w <= wmax; w += 2) {
+    double den = fct((w - s1) / 2) * fct((w - s2) / 2) * fct((w - s3) / 2) * fct((w - s4) / 2) *
+                 fct((ii - w) / 2) * fct((ij - w) / 2) * fct((ik - w) / 2);
+    if (w % 4 != 0) den = -den;
+    omega += fct(w / 2 + 1) / den;
+  }
+  const double t1 = fct((a - j3) / 2) * fct((j3 + b) / 2) * fct((j3 - b) / 2) / fct(s1 / 2 + 1);
+  const double t2 = fct((c - l3) / 2) * fct((l3 + d) / 2) * fct((l3 - d) / 2) / fct(s2 / 2 + 1);
+  const double t3 = fct((e - l3) / 2) * fct((l3 + f) / 2) * fct((l3 - f) / 2) / fct(s3 / 2 + 1);
+  const double t4 = fct((g - j3) / 2) * fct((j3 + h) / 2) * fct((j3 - h) / 2) / fct(s4 / 2 + 1);
+  return omega * std::sqrt(t1 * t2 * t3 * t4);
+}
+
+namespace {
+
+struct PlanError : std::runtime_error {
+  int code;
+  PlanError(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+// ------------------------------------------------------------ operator view
+struct OSub {
+  int num_up, num_down, down_dif, row_dim, sdim;
+  int64_t off;   // device offset of the stored matrix
+  bool zero;     // structurally zero (merged sub-block without contributions)
+};
+struct OBlk {
+  int len = 0, up_dif = 0, down_dif = 0;
+  std::vector<OSub> sub;
+};
+// A block, or its transpose (block_transfer_trans) without copying.
+struct OView {
+  const OBlk *b;
+  bool tr;
+  int up_dif() const { return tr ? -b->up_dif : b->up_dif; }
+  int down_dif() const { return b->down_dif; }
+  int num() const { return (int)b->sub.size(); }
+  // labels of sub-block k as seen through the view
+  int nu(int k) const { const OSub &s = b->sub[k]; return tr ? s.num_up + b->up_dif : s.num_up; }
+  int nd(int k) const { const OSub &s = b->sub[k]; return tr ? s.num_down + s.down_dif : s.num_down; }
+  int dd(int k) const { const OSub &s = b->sub[k]; return tr ? -s.down_dif : s.down_dif; }
+  int rows(int k) const { const OSub &s = b->sub[k]; return tr ? s.sdim : s.row_dim; }
+  int cols(int k) const { const OSub &s = b->sub[k]; return tr ? s.row_dim : s.sdim; }
+  bool zero(int k) const { return b->sub[k].zero; }
+  // operand for (view matrix)^(extra ? T : N)
+  Operand mat(int k, bool extra_t) const {
+    const OSub &s = b->sub[k];
+    Operand o;
+    o.off = s.off;
+    o.ld = s.row_dim;
+    o.space = SP_OPS;
+    o.trans = (int8_t)((tr ? 1 : 0) ^ (extra_t ? 1 : 0));
+    o.pad = 0;
+    return o;
+  }
+  // first sub-block with the labels (num_up, num_down[, down_dif])
+  int find(int nu_, int nd_, int dd_, bool use_dd) const {
+    for (int k = 0; k < num(); ++k)
+      if (nu(k) == nu_ && nd(k) == nd_ && (!use_dd || dd(k) == dd_)) return k;
+    return -1;
+  }
+};
+
+// Site operators (Get_site_operator_su2_U0, dmrg_sub.f90:370-473) carry their
+// 1x1 values on the host.
+struct SiteOp {
+  OBlk b;
+  std::vector<double> val;
+};
+
+struct SiteOps {
+  SiteOp eu, sd, ne, si;
+};
+static SiteOp make_site(int up_dif, int down_dif, std::vector<std::tuple<int, int, int, double>> subs) {
+  SiteOp s;
+  s.b.len = 1;
+  s.b.up_dif = up_dif;
+  s.b.down_dif = down_dif;
+  for (auto &t : subs) {
+    s.b.sub.push_back(OSub{std::get<0>(t), std::get<1>(t), std::get<2>(t), 1, 1, -1, false});
+    s.val.push_back(std::get<3>(t));
+  }
+  return s;
+}
+static SiteOps make_site_ops(int ub) {
+  SiteOps o;
+  o.eu = make_site(ub, 1, {{0, 0, 1, -std::sqrt(2.0)}});                             // st_elec_up
+  o.sd = make_site(0, 2, {{ub, 1, 0, std::sqrt(1.5)}});                              // st_sd
+  o.ne = make_site(0, 0, {{0, 0, 0, 0.0}, {ub, 1, 0, std::sqrt(2.0)}});             // num_elec
+  o.si = make_site(0, 0, {{0, 0, 0, 1.0}, {ub, 1, 0, std::sqrt(2.0)}});             // st_si
+  return o;
+}
+static int site_find(const SiteOp &s, int nu, int nd, int dd, bool use_dd) {
+  for (size_t k = 0; k < s.b.sub.size(); ++k) {
+    const OSub &q = s.b.sub[k];
+    if (q.num_up == nu && q.num_down == nd && (!use_dd || q.down_dif == dd)) return (int)k;
+  }
+  return -1;
+}
+
+static inline double sgn(char flag, int n) {
+  if (flag == 'B') return 1.0;
+  if (flag == 'F') return (n % 2 == 0) ? 1.0 : -1.0;
+  return 0.0;
+}
+static inline double m1pow(int n) { return (n % 2) ? -1.0 : 1.0; }
+
+// ------------------------------------------------------------------ builder
+struct Builder {
+  const tj_basis *sbs, *ebs;
+  const tj_wave *wave;
+  HpsiPlan &plan;
+  // psi cells
+  std::vector<int> sec_x, sec_y, cell_base;   // per sector: sys map, env map, first cell id
+  std::vector<int64_t> cell_off;
+  std::vector<int> cell_ld, cell_M, cell_N;
+  int ncells = 0;
+  std::map<std::tuple<int, int, int, int>, int> sec_of;   // first sector with the labels
+  // tasks
+  std::vector<std::vector<Task>> cell_tasks;
+  std::unordered_map<std::string, int> prod_id;
+  std::vector<int64_t> op_touched;
+  bool dedup = true;
+
+  Builder(const tj_basis *s, const tj_basis *e, const tj_wave *w, HpsiPlan &p) : sbs(s), ebs(e), wave(w), plan(p) {}
+
+  const tj_basis_sub &SM(int x, int l) const { return sbs->maps[sbs->sub[x].first + l]; }
+  const tj_basis_sub &EM(int y, int l) const { return ebs->maps[ebs->sub[y].first + l]; }
+
+  static int find_map(const tj_basis *b, int nu, int nd) {
+    for (int x = 0; x < b->num; ++x)
+      if (b->sub[x].new_num_up == nu && b->sub[x].new_num_down == nd) return x;
+    return -1;
+  }
+
+  void init_cells() {
+    const int ns = wave->num;
+    sec_x.assign(ns, -1);
+    sec_y.assign(ns, -1);
+    cell_base.assign(ns + 1, 0);
+    for (int i = 0; i < ns; ++i) {
+      const tj_wave_sub &w = wave->sub[i];
+      auto key = std::make_tuple(w.sys_num_up, w.sys_num_down, w.env_num_up, w.env_num_down);
+      if (!sec_of.count(key)) sec_of[key] = i;
+      int x = find_map(sbs, w.sys_num_up, w.sys_num_down);
+      int y = find_map(ebs, w.env_num_up, w.env_num_down);
+      if (x < 0 || y < 0) throw PlanError(TJ_ERR_QN, "wave sector without a matching basis sector");
+      if (sbs->sub[x].dim != w.sys_dim || ebs->sub[y].dim != w.env_dim)
+        throw PlanError(TJ_ERR_ARG, "wave sector dimensions differ from the basis");
+      sec_x[i] = x;
+      sec_y[i] = y;
+      cell_base[i + 1] = cell_base[i] + sbs->sub[x].num * ebs->sub[y].num;
+    }
+    ncells = cell_base[ns];
+    cell_off.resize(ncells);
+    cell_ld.resize(ncells);
+    cell_M.resize(ncells);
+    cell_N.resize(ncells);
+    for (int i = 0; i < ns; ++i) {
+      const int x = sec_x[i], y = sec_y[i], ny = ebs->sub[y].num;
+      for (int m = 0; m < sbs->sub[x].num; ++m)
+        for (int n = 0; n < ny; ++n) {
+          const int c = cell_base[i] + m * ny + n;
+          const tj_basis_sub &a = SM(x, m), &b = EM(y, n);
+          cell_off[c] = wave->sub[i].off + (int64_t)b.spos * wave->sub[i].sys_dim + a.spos;
+          cell_ld[c] = wave->sub[i].sys_dim;
+          cell_M[c] = a.sdim;
+          cell_N[c] = b.sdim;
+        }
+    }
+    cell_tasks.assign(ncells, {});
+  }
+  int cell(int i, int m, int n) const { return cell_base[i] + m * ebs->sub[sec_y[i]].num + n; }
+  int find_sec(int su, int sd, int eu, int ed) const {
+    auto it = sec_of.find(std::make_tuple(su, sd, eu, ed));
+    return it == sec_of.end() ? -1 : it->second;
+  }
+  Operand xop(int c) const {
+    Operand o;
+    o.off = cell_off[c];
+    o.ld = cell_ld[c];
+    o.space = SP_PSI;
+    o.trans = 0;
+    o.pad = 0;
+    return o;
+  }
+  static Operand none() {
+    Operand o;
+    std::memset(&o, 0, sizeof o);
+    return o;
+  }
+  void touch(const Operand &o) {
+    if (o.space == SP_OPS) op_touched.push_back(o.off);
+  }
+
+  // out(oc) += coef * op(A) * X(xc); op(A) is (rows x K)
+  void emitL(int oc, const OView &A, int ka, bool at, int xc, double coef, double ref_extra = 0.0) {
+    if (A.zero(ka) || coef == 0.0) return;
+    const int rows = at ? A.cols(ka) : A.rows(ka), K = at ? A.rows(ka) : A.cols(ka);
+    if (rows != cell_M[oc] || K != cell_M[xc] || cell_N[xc] != cell_N[oc])
+      throw PlanError(TJ_ERR_ARG, "operator sub-block does not match the basis dimensions");
+    Task t;
+    t.L = A.mat(ka, at);
+    t.R = xop(xc);
+    t.coef = coef;
+    t.K = K;
+    t.pad = 0;
+    touch(t.L);
+    cell_tasks[oc].push_back(t);
+    const double f = 2.0 * rows * cell_N[oc] * (double)K;
+    plan.flops += f;
+    plan.flops_ref += f + ref_extra;
+  }
+  // out(oc) += coef * X(xc) * op(B); op(B) is (K x cols)
+  void emitR(int oc, int xc, const OView &B, int kb, bool bt, double coef) {
+    if (B.zero(kb) || coef == 0.0) return;
+    const int K = bt ? B.cols(kb) : B.rows(kb), cols = bt ? B.rows(kb) : B.cols(kb);
+    if (cols != cell_N[oc] || K != cell_N[xc] || cell_M[xc] != cell_M[oc])
+      throw PlanError(TJ_ERR_ARG, "operator sub-block does not match the basis dimensions");
+    Task t;
+    t.L = xop(xc);
+    t.R = B.mat(kb, bt);
+    t.coef = coef;
+    t.K = K;
+    t.pad = 0;
+    touch(t.R);
+    cell_tasks[oc].push_back(t);
+    const double f = 2.0 * cell_M[oc] * cols * (double)K;
+    plan.flops += f;
+    plan.flops_ref += f;
+  }
+  // out(oc) += coef * X(xc)
+  void emitAxpy(int oc, int xc, double coef) {
+    if (coef == 0.0) return;
+    if (cell_M[oc] != cell_M[xc] || cell_N[oc] != cell_N[xc])
+      throw PlanError(TJ_ERR_ARG, "site term between cells of different size");
+    Task t;
+    t.L = xop(xc);
+    t.R = none();
+    t.coef = coef;
+    t.K = 0;
+    t.pad = 0;
+    cell_tasks[oc].push_back(t);
+    plan.flops += 2.0 * cell_M[oc] * cell_N[oc];
+    plan.flops_ref += 2.0 * cell_M[oc] * cell_N[oc];
+  }
+  // out(oc) += coef * [op(A) * X(xc)] * op(B)   (phase-1 product, then phase-2 task)
+  void emit2(int oc, const OView &A, int ka, bool at, int xc, const OView &B, int kb, bool bt, double coef) {
+    if (A.zero(ka) || B.zero(kb) || coef == 0.0) return;
+    const int M = at ? A.cols(ka) : A.rows(ka), K1 = at ? A.rows(ka) : A.cols(ka);
+    const int K2 = bt ? B.cols(kb) : B.rows(kb), N = bt ? B.rows(kb) : B.cols(kb);
+    if (M != cell_M[oc] || N != cell_N[oc] || K1 != cell_M[xc] || K2 != cell_N[xc])
+      throw PlanError(TJ_ERR_ARG, "operator sub-block does not match the basis dimensions");
+    Operand a = A.mat(ka, at);
+    char key[64];
+    std::snprintf(key, sizeof key, "%lld:%d:%d", (long long)a.off, (int)a.trans, xc);
+    int pid;
+    auto it = dedup ? prod_id.find(key) : prod_id.end();
+    if (it != prod_id.end()) {
+      pid = it->second;
+    } else {
+      pid = (int)plan.cells1.size();
+      if (dedup) prod_id[key] = pid;
+      Cell c;
+      std::memset(&c, 0, sizeof c);
+      c.off = plan.scratch_len;
+      c.ld = M;
+      c.M = M;
+      c.N = K2;
+      c.space = SP_SCR;
+      c.t_begin = (int)plan.tasks1.size();
+      c.t_end = c.t_begin + 1;
+      plan.scratch_len += ((int64_t)M * K2 + 3) / 4 * 4;
+      plan.cells1.push_back(c);
+      Task t;
+      t.L = a;
+      t.R = xop(xc);
+      t.coef = 1.0;
+      t.K = K1;
+      t.pad = 0;
+      touch(t.L);
+      plan.tasks1.push_back(t);
+      plan.flops += 2.0 * M * K2 * (double)K1;
+    }
+    Task t;
+    t.L.off = plan.cells1[pid].off;
+    t.L.ld = M;
+    t.L.space = SP_SCR;
+    t.L.trans = 0;
+    t.L.pad = 0;
+    t.R = B.mat(kb, bt);
+    t.coef = coef;
+    t.K = K2;
+    t.pad = 0;
+    touch(t.R);
+    cell_tasks[oc].push_back(t);
+    plan.flops += 2.0 * M * N * (double)K2;
+    plan.flops_ref += 2.0 * M * K2 * (double)K1 + 2.0 * M * N * (double)K2;
+  }
+
+  // ============================================================ term kernels
+  // block_vec_dia (get_sys.f90:1242-1289)
+  void block_vec_dia(const OView &H, double coef) {
+    for (int i = 0; i < wave->num; ++i) {
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m) {
+        const tj_basis_sub &q = SM(x, m);
+        const double c1 = coef / std::sqrt(1.0 + q.bl_num_down);
+        const int k = H.find(q.bl_num_up, q.bl_num_down, 0, false);
+        if (k < 0) continue;
+        for (int n = 0; n < ebs->sub[y].num; ++n) emitL(cell(i, m, n), H, k, false, cell(i, m, n), c1);
+      }
+    }
+  }
+  // vec_block_dia (get_sys.f90:1293-1340)
+  void vec_block_dia(const OView &H, double coef) {
+    for (int i = 0; i < wave->num; ++i) {
+      const int x = sec_x[i], y = sec_y[i];
+      for (int n = 0; n < ebs->sub[y].num; ++n) {
+        const tj_basis_sub &q = EM(y, n);
+        const double c1 = coef / std::sqrt(1.0 + q.bl_num_down);
+        const int k = H.find(q.bl_num_up, q.bl_num_down, 0, false);
+        if (k < 0) continue;
+        for (int m = 0; m < sbs->sub[x].num; ++m) emitR(cell(i, m, n), cell(i, m, n), H, k, true, c1);
+      }
+    }
+  }
+  // site_vec_site_dia (get_sys.f90:1609-1705)
+  void site_vec_site_dia(const SiteOp &sst, const SiteOp &est, double coef) {
+    for (int i = 0; i < wave->num; ++i) {
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m) {
+        const tj_basis_sub &qs = SM(x, m);
+        const int ks = site_find(sst, qs.st_num_up, qs.st_num_down, 0, false);
+        for (int n = 0; n < ebs->sub[y].num; ++n) {
+          const tj_basis_sub &qe = EM(y, n);
+          const int ke = site_find(est, qe.st_num_up, qe.st_num_down, 0, false);
+          if (ks < 0 || ke < 0) continue;
+          double ct = coef * sst.val[ks] * est.val[ke];
+          ct = ct / std::sqrt((1.0 + qs.st_num_down) * (1.0 + qe.st_num_down));
+          emitAxpy(cell(i, m, n), cell(i, m, n), ct);
+        }
+      }
+    }
+  }
+  // locate the system sub-block of the sector with labels (nu, nd) satisfying pred
+  template <class P>
+  bool find_sys(int nu, int nd, P pred, int &xk, int &l) const {
+    for (int k = 0; k < sbs->num; ++k) {
+      if (sbs->sub[k].new_num_up != nu || sbs->sub[k].new_num_down != nd) continue;
+      for (int q = 0; q < sbs->sub[k].num; ++q)
+        if (pred(SM(k, q))) { xk = k; l = q; return true; }
+    }
+    return false;
+  }
+  template <class P>
+  bool find_env(int nu, int nd, P pred, int &yk, int &l) const {
+    for (int k = 0; k < ebs->num; ++k) {
+      if (ebs->sub[k].new_num_up != nu || ebs->sub[k].new_num_down != nd) continue;
+      for (int q = 0; q < ebs->sub[k].num; ++q)
+        if (pred(EM(k, q))) { yk = k; l = q; return true; }
+    }
+    return false;
+  }
+  // sub-block index l of map x, as a cell row/column index of sector ko
+  int sys_index_in(int ko, int xk, int l) const {
+    if (sec_x[ko] != xk) throw PlanError(TJ_ERR_QN, "basis sector mismatch");
+    return l;
+  }
+  int env_index_in(int ko, int yk, int l) const {
+    if (sec_y[ko] != yk) throw PlanError(TJ_ERR_QN, "basis sector mismatch");
+    return l;
+  }
+
+  // site_vec_site_ndia (get_sys.f90:3761-4124, live 3794-3994)
+  void site_vec_site_ndia(const SiteOp &sst, char fst, const SiteOp &est, char fet, double coef) {
+    const int up = sst.b.up_dif, d1 = sst.b.down_dif;
+    for (int i = 0; i < wave->num; ++i) {
+      const tj_wave_sub &w = wave->sub[i];
+      const int su = w.sys_num_up, sd = w.sys_num_down, eu = w.env_num_up, ed = w.env_num_down;
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m) {
+        const tj_basis_sub &ms = SM(x, m);
+        for (int n = 0; n < ebs->sub[y].num; ++n) {
+          const tj_basis_sub &me = EM(y, n);
+          for (int sdd1 = -sst.b.down_dif; sdd1 <= sst.b.down_dif; sdd1 += 2) {
+            const int ks = site_find(sst, ms.st_num_up, ms.st_num_down, sdd1, true);
+            const int nss_up = ms.st_num_up + up, nss_dn = ms.st_num_down + sdd1;
+            for (int sdd2 = -est.b.down_dif; sdd2 <= est.b.down_dif; sdd2 += 2) {
+              const int nes_up = me.st_num_up - up, nes_dn = me.st_num_down - sdd2;
+              const int ke = site_find(est, nes_up, nes_dn, sdd2, true);
+              if (ks < 0 || ke < 0) continue;
+              const int nsu = su + up, neu = eu - up;
+              for (int nsd = std::abs(sd - sst.b.down_dif); nsd <= sd + sst.b.down_dif; nsd += 2) {
+                const int ned = nsd;
+                int xk, ls, yk, le;
+                if (!find_sys(nsu, nsd, [&](const tj_basis_sub &q) {
+                      return q.st_num_up == nss_up && q.st_num_down == nss_dn && q.bl_num_down == ms.bl_num_down; }, xk, ls))
+                  continue;
+                if (!find_env(neu, ned, [&](const tj_basis_sub &q) {
+                      return q.st_num_up == nes_up && q.st_num_down == nes_dn && q.bl_num_down == me.bl_num_down; }, yk, le))
+                  continue;
+                const int ko = find_sec(nsu, nsd, neu, ned);
+                if (ko < 0) continue;
+                const double ct = sgn(fst, ms.bl_num_down) * sgn(fet, sd) * coef;
+                const int j1 = nsd, j2 = d1, j3 = sd, j4 = ms.st_num_down, j5 = ms.bl_num_down, j6 = nss_dn;
+                const int j11 = ned, j22 = d1, j33 = ed, j44 = me.st_num_down, j55 = me.bl_num_down, j66 = nes_dn;
+                double c1 = w6j(j1, j2, j3, j4, j5, j6);
+                if (c1 == 0.0) continue;
+                const double c11 = w6j(j11, j22, j33, j44, j55, j66);
+                if (c11 == 0.0) continue;
+                c1 *= c11;
+                if (c1 == 0.0) continue;
+                c1 *= std::sqrt((1.0 + j11) * (1.0 + j33) / (1.0 + d1));
+                if (((j55 + j44 + j11 + j22) / 2 + (j5 + j4 + j1 + j2) / 2) % 2 != 0) c1 = -c1;
+                c1 = ct * c1 * sst.val[ks] * est.val[ke];
+                const int oc = cell(ko, sys_index_in(ko, xk, ls), env_index_in(ko, yk, le));
+                emitAxpy(oc, cell(i, m, n), c1);
+                if (d1 == 1) emitAxpy(cell(i, m, n), oc, c1);
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  // block_site_vec_ndia (get_sys.f90:2016-2265, live 2047-2170)
+  void block_site_vec_ndia(const OView &bl, const SiteOp &st, char fst, double coef) {
+    const int up = bl.up_dif(), d1 = bl.down_dif();
+    if (up != st.b.up_dif || d1 != st.b.down_dif) throw PlanError(TJ_ERR_QN, "Quantum number error in block_site_vec");
+    for (int i = 0; i < wave->num; ++i) {
+      const int sd = wave->sub[i].sys_num_down;
+      const int k = sec_x[i], y = sec_y[i];
+      for (int x = 0; x < sbs->sub[k].num; ++x) {
+        const tj_basis_sub &q = SM(k, x);
+        for (int dd = -d1; dd <= d1; dd += 2)
+          for (int sdd = -d1; sdd <= d1; sdd += 2) {
+            const int kb = bl.find(q.bl_num_up, q.bl_num_down, dd, true);
+            const int nst_up = q.st_num_up - up, nst_dn = q.st_num_down - sdd;
+            const int ks = site_find(st, nst_up, nst_dn, sdd, true);
+            const int nbl_up = q.bl_num_up + up, nbl_dn = q.bl_num_down + dd;
+            if (kb < 0 || ks < 0) continue;
+            int np = -1;
+            for (int yy = 0; yy < sbs->sub[k].num; ++yy) {
+              const tj_basis_sub &r = SM(k, yy);
+              if (r.bl_num_up == nbl_up && r.bl_num_down == nbl_dn && r.st_num_up == nst_up && r.st_num_down == nst_dn) {
+                np = yy;
+                break;
+              }
+            }
+            if (np < 0) continue;
+            const int j1 = nbl_dn, j2 = q.bl_num_down, j3 = d1, j4 = q.st_num_down, j5 = nst_dn, j6 = sd;
+            double c1 = w6j(j1, j2, j3, j4, j5, j6);
+            if (c1 == 0.0) continue;
+            c1 = c1 * m1pow((j2 + j5 + j3 + j6) / 2) / std::sqrt(1.0 + d1);
+            const double ct = sgn(fst, q.bl_num_down) * c1 * coef * st.val[ks];
+            for (int n = 0; n < ebs->sub[y].num; ++n) {
+              emitL(cell(i, np, n), bl, kb, false, cell(i, x, n), ct);
+              if (d1 == 1) emitL(cell(i, x, n), bl, kb, true, cell(i, np, n), ct);
+            }
+          }
+      }
+    }
+  }
+  // block_site_vec_dia (get_sys.f90:1460-1530)
+  void block_site_vec_dia(const OView &bl, const SiteOp &st, double coef) {
+    for (int i = 0; i < wave->num; ++i) {
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m) {
+        const tj_basis_sub &q = SM(x, m);
+        const int kb = bl.find(q.bl_num_up, q.bl_num_down, 0, false);
+        const int ks = site_find(st, q.st_num_up, q.st_num_down, 0, false);
+        if (kb < 0 || ks < 0) continue;
+        double ct = coef * st.val[ks];
+        ct = ct / std::sqrt((1.0 + q.bl_num_down) * (1.0 + q.st_num_down));
+        for (int n = 0; n < ebs->sub[y].num; ++n) emitL(cell(i, m, n), bl, kb, false, cell(i, m, n), ct);
+      }
+    }
+  }
+  // vec_block_site_ndia (get_sys.f90:2269-2552, live 2301-2446)
+  void vec_block_site_ndia(const OView &bl, char fbl, const SiteOp &st, char fst, double coef) {
+    const int up = bl.up_dif(), d1 = bl.down_dif();
+    if (up != st.b.up_dif || d1 != st.b.down_dif) throw PlanError(TJ_ERR_QN, "Quantum number error in vec_block_site");
+    for (int i = 0; i < wave->num; ++i) {
+      const int sd = wave->sub[i].sys_num_down, ed = wave->sub[i].env_num_down;
+      const int xs = sec_x[i], k = sec_y[i];
+      for (int x = 0; x < ebs->sub[k].num; ++x) {
+        const tj_basis_sub &q = EM(k, x);
+        for (int bdd = -d1; bdd <= d1; bdd += 2) {
+          const int kb = bl.find(q.bl_num_up, q.bl_num_down, bdd, true);
+          for (int sdd = -d1; sdd <= d1; sdd += 2) {
+            const int nst_up = q.st_num_up - up, nst_dn = q.st_num_down - sdd;
+            const int ks = site_find(st, nst_up, nst_dn, sdd, true);
+            const int nbl_up = q.bl_num_up + up, nbl_dn = q.bl_num_down + bdd;
+            if (ks < 0 || kb < 0) continue;
+            int np = -1;
+            for (int yy = 0; yy < ebs->sub[k].num; ++yy) {
+              const tj_basis_sub &r = EM(k, yy);
+              if (r.bl_num_up == nbl_up && r.bl_num_down == nbl_dn && r.st_num_up == nst_up && r.st_num_down == nst_dn) {
+                np = yy;
+                break;
+              }
+            }
+            if (np < 0) continue;
+            const int j1 = nbl_dn, j2 = q.bl_num_down, j3 = d1, j4 = q.st_num_down, j5 = nst_dn, j6 = ed;
+            double c1 = w6j(j1, j2, j3, j4, j5, j6);
+            if (c1 == 0.0) continue;
+            c1 = c1 * m1pow((j2 + j5 + j3 + j6) / 2) / std::sqrt(1.0 + d1);
+            const double ct = sgn(fbl, sd + nst_dn) * sgn(fst, sd) * c1 * coef * st.val[ks];
+            for (int m = 0; m < sbs->sub[xs].num; ++m) {
+              emitR(cell(i, m, np), cell(i, m, x), bl, kb, true, ct);
+              if (d1 == 1) emitR(cell(i, m, x), cell(i, m, np), bl, kb, false, ct);
+            }
+          }
+        }
+      }
+    }
+  }
+  // vec_block_site_dia (get_sys.f90:1534-1605)
+  void vec_block_site_dia(const OView &bl, const SiteOp &st, double coef) {
+    for (int i = 0; i < wave->num; ++i) {
+      const int x = sec_x[i], y = sec_y[i];
+      for (int n = 0; n < ebs->sub[y].num; ++n) {
+        const tj_basis_sub &q = EM(y, n);
+        const int kb = bl.find(q.bl_num_up, q.bl_num_down, 0, false);
+        const int ks = site_find(st, q.st_num_up, q.st_num_down, 0, false);
+        if (kb < 0 || ks < 0) continue;
+        double ct = coef * st.val[ks];
+        ct = ct / std::sqrt((1.0 + q.bl_num_down) * (1.0 + q.st_num_down));
+        for (int m = 0; m < sbs->sub[x].num; ++m) emitR(cell(i, m, n), cell(i, m, n), bl, kb, true, ct);
+      }
+    }
+  }
+  // block_vec_site_ndia (get_sys.f90:2984-3351, live 3021-3209)
+  void block_vec_site_ndia(const OView &bl, const SiteOp &st, char fet, double coef) {
+    const int up = bl.up_dif(), d1 = bl.down_dif();
+    if (up != st.b.up_dif || d1 != st.b.down_dif) throw PlanError(TJ_ERR_QN, "Quantum number error in block_vec_site");
+    for (int i = 0; i < wave->num; ++i) {
+      const tj_wave_sub &w = wave->sub[i];
+      const int su = w.sys_num_up, sd = w.sys_num_down, eu = w.env_num_up, ed = w.env_num_down;
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m) {
+        const tj_basis_sub &ms = SM(x, m);
+        for (int n = 0; n < ebs->sub[y].num; ++n) {
+          const tj_basis_sub &me = EM(y, n);
+          for (int bdd = -d1; bdd <= d1; bdd += 2) {
+            const int nsb_up = ms.bl_num_up + up, nsb_dn = ms.bl_num_down + bdd;
+            const int kb = bl.find(ms.bl_num_up, ms.bl_num_down, bdd, true);
+            for (int sdd = -st.b.down_dif; sdd <= st.b.down_dif; sdd += 2) {
+              const int nes_up = me.st_num_up - up, nes_dn = me.st_num_down - sdd;
+              const int ks = site_find(st, nes_up, nes_dn, sdd, true);
+              if (kb < 0 || ks < 0) continue;
+              const int nsu = su + up, neu = eu - up;
+              for (int nsd = std::abs(sd - d1); nsd <= sd + d1; nsd += 2) {
+                const int ned = nsd;
+                int xk, ls, yk, le;
+                if (!find_sys(nsu, nsd, [&](const tj_basis_sub &q) {
+                      return q.bl_num_up == nsb_up && q.bl_num_down == nsb_dn && q.st_num_down == ms.st_num_down; }, xk, ls))
+                  continue;
+                if (!find_env(neu, ned, [&](const tj_basis_sub &q) {
+                      return q.st_num_up == nes_up && q.st_num_down == nes_dn && q.bl_num_down == me.bl_num_down; }, yk, le))
+                  continue;
+                const int ko = find_sec(nsu, nsd, neu, ned);
+                if (ko < 0) continue;
+                const int j1 = nsd, j2 = d1, j3 = sd, j4 = ms.bl_num_down, j5 = ms.st_num_down, j6 = nsb_dn;
+                const int j11 = ned, j22 = d1, j33 = ed, j44 = me.st_num_down, j55 = me.bl_num_down, j66 = nes_dn;
+                double c1 = w6j(j1, j2, j3, j4, j5, j6);
+                if (c1 == 0.0) continue;
+                const double c11 = w6j(j11, j22, j33, j44, j55, j66);
+                if (c11 == 0.0) continue;
+                c1 *= c11;
+                if (c1 == 0.0) continue;
+                c1 *= std::sqrt((1.0 + j11) * (1.0 + j33) / (1.0 + d1));
+                if (((j6 + j5 + j3 + j2) / 2 + (j55 + j44 + j11 + j22) / 2) % 2 != 0) c1 = -c1;
+                const double ct = sgn(fet, sd) * c1 * coef * st.val[ks];
+                const int oc = cell(ko, sys_index_in(ko, xk, ls), env_index_in(ko, yk, le));
+                emitL(oc, bl, kb, false, cell(i, m, n), ct);
+                if (d1 == 1) emitL(cell(i, m, n), bl, kb, true, oc, ct);
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  // block_vec_site_dia (get_sys.f90:1709-1805)
+  void block_vec_site_dia(const OView &bl, const SiteOp &st, double coef) {
+    for (int i = 0; i < wave->num; ++i) {
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m) {
+        const tj_basis_sub &ms = SM(x, m);
+        const int kb = bl.find(ms.bl_num_up, ms.bl_num_down, 0, false);
+        for (int n = 0; n < ebs->sub[y].num; ++n) {
+          const tj_basis_sub &me = EM(y, n);
+          const int ks = site_find(st, me.st_num_up, me.st_num_down, 0, false);
+          if (kb < 0 || ks < 0) continue;
+          double ct = coef * st.val[ks];
+          ct = ct / std::sqrt((1.0 + me.st_num_down) * (1.0 + ms.bl_num_down));
+          emitL(cell(i, m, n), bl, kb, false, cell(i, m, n), ct);
+        }
+      }
+    }
+  }
+  // site_vec_block_ndia (get_sys.f90:3355-3757, live 3391-3604); bl is a transposed view
+  void site_vec_block_ndia(const SiteOp &st, char fst, const OView &bl, char fel, double coef) {
+    const int up = st.b.up_dif, d1 = st.b.down_dif;
+    if (up != bl.up_dif() || d1 != bl.down_dif()) throw PlanError(TJ_ERR_QN, "Quantum number error in site_vec_block");
+    for (int i = 0; i < wave->num; ++i) {
+      const tj_wave_sub &w = wave->sub[i];
+      const int su = w.sys_num_up, sd = w.sys_num_down, eu = w.env_num_up, ed = w.env_num_down;
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m) {
+        const tj_basis_sub &ms = SM(x, m);
+        for (int n = 0; n < ebs->sub[y].num; ++n) {
+          const tj_basis_sub &me = EM(y, n);
+          for (int sdd = -d1; sdd <= d1; sdd += 2) {
+            const int nss_up = ms.st_num_up + up, nss_dn = ms.st_num_down + sdd;
+            const int ks = site_find(st, ms.st_num_up, ms.st_num_down, sdd, true);
+            for (int bdd = -bl.down_dif(); bdd <= bl.down_dif(); bdd += 2) {
+              const int neb_up = me.bl_num_up - up, neb_dn = me.bl_num_down - bdd;
+              const int kb = bl.find(neb_up, neb_dn, bdd, true);
+              if (ks < 0 || kb < 0) continue;
+              const int nsu = su + up, neu = eu - up;
+              for (int nsd = std::abs(sd - d1); nsd <= sd + d1; nsd += 2) {
+                const int ned = nsd;
+                int xk, ls, yk, le;
+                if (!find_sys(nsu, nsd, [&](const tj_basis_sub &q) {
+                      return q.st_num_up == nss_up && q.st_num_down == nss_dn && q.bl_num_down == ms.bl_num_down &&
+                             q.bl_num_up == ms.bl_num_up; }, xk, ls))
+                  continue;
+                if (!find_env(neu, ned, [&](const tj_basis_sub &q) {
+                      return q.bl_num_up == neb_up && q.bl_num_down == neb_dn && q.st_num_up == me.st_num_up &&
+                             q.st_num_down == me.st_num_down; }, yk, le))
+                  continue;
+                const int ko = find_sec(nsu, nsd, neu, ned);
+                if (ko < 0) continue;
+                const int j1 = nsd, j2 = d1, j3 = sd, j4 = ms.st_num_down, j5 = ms.bl_num_down, j6 = nss_dn;
+                const int j11 = ned, j22 = d1, j33 = ed, j44 = me.bl_num_down, j55 = me.st_num_down, j66 = neb_dn;
+                double c1 = w6j(j1, j2, j3, j4, j5, j6);
+                if (c1 == 0.0) continue;
+                const double c11 = w6j(j11, j22, j33, j44, j55, j66);
+                if (c11 == 0.0) continue;
+                c1 *= c11;
+                if (c1 == 0.0) continue;
+                c1 *= std::sqrt((1.0 + j11) * (j33 + 1.0) / (1.0 + d1));
+                if (((j66 + j55 + j33 + j22) / 2 + (j5 + j4 + j1 + j2) / 2) % 2 != 0) c1 = -c1;
+                const double ct = sgn(fst, ms.bl_num_down) * sgn(fel, sd + me.st_num_down) * c1 * coef * st.val[ks];
+                const int oc = cell(ko, sys_index_in(ko, xk, ls), env_index_in(ko, yk, le));
+                emitR(oc, cell(i, m, n), bl, kb, false, ct);
+                if (d1 == 1) emitR(cell(i, m, n), oc, bl, kb, true, ct);
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  // site_vec_block_dia (get_sys.f90:1809-1906)
+  void site_vec_block_dia(const SiteOp &st, const OView &bl, double coef) {
+    for (int i = 0; i < wave->num; ++i) {
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m) {
+        const tj_basis_sub &ms = SM(x, m);
+        const int ks = site_find(st, ms.st_num_up, ms.st_num_down, 0, false);
+        for (int n = 0; n < ebs->sub[y].num; ++n) {
+          const tj_basis_sub &me = EM(y, n);
+          const int kb = bl.find(me.bl_num_up, me.bl_num_down, 0, false);
+          if (ks < 0 || kb < 0) continue;
+          double ct = coef * st.val[ks];
+          ct = ct / std::sqrt((1.0 + me.bl_num_down) * (1.0 + ms.st_num_down));
+          emitR(cell(i, m, n), cell(i, m, n), bl, kb, true, ct);
+        }
+      }
+    }
+  }
+  // block_vec_block_ndia (get_sys.f90:2555-2981, live 2595-2834); ebl is a transposed view
+  void block_vec_block_ndia(const OView &sbl, const OView &ebl, char fel, double coef) {
+    const int up = sbl.up_dif(), d1 = sbl.down_dif();
+    if (up != ebl.up_dif() || d1 != ebl.down_dif()) throw PlanError(TJ_ERR_QN, "Quantum number error in block_vec_block");
+    for (int i = 0; i < wave->num; ++i) {
+      const tj_wave_sub &w = wave->sub[i];
+      const int su = w.sys_num_up, sd = w.sys_num_down, eu = w.env_num_up, ed = w.env_num_down;
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m)
+        for (int n = 0; n < ebs->sub[y].num; ++n) {
+          const tj_basis_sub &ms = SM(x, m), &me = EM(y, n);
+          for (int dd = -d1; dd <= d1; dd += 2) {
+            const int ks = sbl.find(ms.bl_num_up, ms.bl_num_down, dd, true);
+            const int nsb_up = ms.bl_num_up + up, nsb_dn = ms.bl_num_down + dd;
+            for (int edd = -d1; edd <= d1; edd += 2) {
+              const int neb_up = me.bl_num_up - up, neb_dn = me.bl_num_down - edd;
+              const int ke = ebl.find(neb_up, neb_dn, edd, true);
+              if (ks < 0 || ke < 0) continue;
+              for (int nsd = std::abs(sd - d1); nsd <= sd + d1; nsd += 2) {
+                const int nsu = su + up, neu = eu - up, ned = nsd;
+                int xk, ls, yk, le;
+                if (!find_sys(nsu, nsd, [&](const tj_basis_sub &q) {
+                      return q.bl_num_up == nsb_up && q.bl_num_down == nsb_dn && q.st_num_down == ms.st_num_down &&
+                             q.st_num_up == ms.st_num_up; }, xk, ls))
+                  continue;
+                if (!find_env(neu, ned, [&](const tj_basis_sub &q) {
+                      return q.bl_num_up == neb_up && q.bl_num_down == neb_dn && q.st_num_down == me.st_num_down &&
+                             q.st_num_up == me.st_num_up; }, yk, le))
+                  continue;
+                const int ko = find_sec(nsu, nsd, neu, ned);
+                if (ko < 0) continue;
+                const int j1 = nsd, j2 = d1, j3 = sd, j4 = ms.bl_num_down, j5 = ms.st_num_down, j6 = nsb_dn;
+                const int j11 = ned, j22 = d1, j33 = ed, j44 = me.bl_num_down, j55 = me.st_num_down, j66 = neb_dn;
+                double c1 = w6j(j1, j2, j3, j4, j5, j6);
+                if (c1 == 0.0) continue;
+                const double c11 = w6j(j11, j22, j33, j44, j55, j66);
+                if (c11 == 0.0) continue;
+                c1 *= c11;
+                if (c1 == 0.0) continue;
+                c1 *= std::sqrt((1.0 + j11) * (1.0 + j33) / (1.0 + d1));
+                if (((j6 + j5 + j3 + j2) / 2 + (j66 + j55 + j33 + j22) / 2) % 2 == 1) c1 = -c1;
+                const double ct = sgn(fel, sd + me.st_num_down) * coef * c1;
+                const int oc = cell(ko, sys_index_in(ko, xk, ls), env_index_in(ko, yk, le));
+                const int xc = cell(i, m, n);
+                emit2(oc, sbl, ks, false, xc, ebl, ke, false, ct);
+                if (d1 == 1) emit2(xc, sbl, ks, true, oc, ebl, ke, true, ct);
+              }
+            }
+          }
+        }
+    }
+  }
+  // block_vec_block_dia (get_sys.f90:1910-2012)
+  void block_vec_block_dia(const OView &sbl, const OView &ebl, double coef) {
+    for (int i = 0; i < wave->num; ++i) {
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m) {
+        const tj_basis_sub &ms = SM(x, m);
+        const int ks = sbl.find(ms.bl_num_up, ms.bl_num_down, 0, false);
+        for (int n = 0; n < ebs->sub[y].num; ++n) {
+          const tj_basis_sub &me = EM(y, n);
+          const int ke = ebl.find(me.bl_num_up, me.bl_num_down, 0, false);
+          if (ks < 0 || ke < 0) continue;
+          if (ms.sdim * me.sdim == 0) throw PlanError(TJ_ERR_ARG, "block_vec_block_dia: empty tile");
+          const double c1 = coef / std::sqrt((1.0 + me.bl_num_down) * (1.0 + ms.bl_num_down));
+          emit2(cell(i, m, n), sbl, ks, false, cell(i, m, n), ebl, ke, true, c1);
+        }
+      }
+    }
+  }
+
+  // -------------------------------------------------------------- finalise
+  void finalize() {
+    // phase-2 cells: every cell of the output vector
+    plan.cells2.clear();
+    plan.tasks2.clear();
+    for (int c = 0; c < ncells; ++c) {
+      Cell cl;
+      std::memset(&cl, 0, sizeof cl);
+      cl.off = cell_off[c];
+      cl.ld = cell_ld[c];
+      cl.M = cell_M[c];
+      cl.N = cell_N[c];
+      cl.space = SP_PSI;
+      cl.t_begin = (int)plan.tasks2.size();
+      // GEMM tasks first, axpy tasks last (the kernel applies axpys in its epilogue)
+      for (const Task &t : cell_tasks[c])
+        if (t.R.space != SP_NONE) plan.tasks2.push_back(t);
+      for (const Task &t : cell_tasks[c])
+        if (t.R.space == SP_NONE) plan.tasks2.push_back(t);
+      cl.t_end = (int)plan.tasks2.size();
+      plan.cells2.push_back(cl);
+    }
+    auto make_tiles = [](const std::vector<Cell> &cells, const std::vector<Task> &tasks, std::vector<Tile> &tiles) {
+      std::vector<std::pair<double, Tile>> w;
+      for (int c = 0; c < (int)cells.size(); ++c) {
+        const Cell &cl = cells[c];
+        double k = 0;
+        for (int t = cl.t_begin; t < cl.t_end; ++t) k += tasks[t].K + 1;
+        for (int r = 0; r < cl.M; r += BM)
+          for (int q = 0; q < cl.N; q += BN) {
+            Tile t{c, r, q, 0};
+            w.push_back({k, t});
+          }
+      }
+      std::stable_sort(w.begin(), w.end(), [](const std::pair<double, Tile> &a, const std::pair<double, Tile> &b) {
+        return a.first > b.first;
+      });
+      tiles.clear();
+      for (auto &p : w) tiles.push_back(p.second);
+    };
+    make_tiles(plan.cells1, plan.tasks1, plan.tiles1);
+    make_tiles(plan.cells2, plan.tasks2, plan.tiles2);
+    std::sort(op_touched.begin(), op_touched.end());
+    op_touched.erase(std::unique(op_touched.begin(), op_touched.end()), op_touched.end());
+  }
+};
+
+// ------------------------------------------------------------- model copy
+struct Model {
+  int len = 0;
+  OBlk ham;
+  std::vector<std::array<OBlk, 5>> sub;   // input slots
+  std::array<OBlk, 5> snc[2];             // merged (hmerge)
+  std::vector<std::array<OBlk, 5>> sub_s; // merged (hmerge)
+};
+enum { EU = 0, ED = 1, SD = 2, SZ = 3, SN = 4 };
+
+static int64_t align4(int64_t x) { return (x + 3) / 4 * 4; }
+
+static void load_block(const tj_block &b, OBlk &o, HpsiPlan &plan) {
+  o.len = b.len;
+  o.up_dif = b.up_dif;
+  o.down_dif = b.down_dif;
+  o.sub.clear();
+  if (b.num < 0 || (b.num > 0 && (!b.sub || !b.data))) throw PlanError(TJ_ERR_ARG, "block with null sub/data");
+  // one host-to-device copy per block: the span of its sub-block matrices
+  int64_t lo = LLONG_MAX, hi = 0;
+  for (int k = 0; k < b.num; ++k) {
+    const tj_block_sub &s = b.sub[k];
+    if (s.row_dim < 0 || s.sdim < 0 || s.off < 0) throw PlanError(TJ_ERR_ARG, "negative sub-block size");
+    lo = std::min(lo, (int64_t)s.off);
+    hi = std::max(hi, (int64_t)s.off + (int64_t)s.row_dim * s.sdim);
+  }
+  if (b.num == 0) return;
+  const int64_t base = plan.ops_len;
+  plan.uploads.push_back({b.data + lo, hi - lo, base});
+  plan.ops_len += align4(hi - lo);
+  for (int k = 0; k < b.num; ++k) {
+    const tj_block_sub &s = b.sub[k];
+    OSub q{s.num_up, s.num_down, s.down_dif, s.row_dim, s.sdim, base + (s.off - lo), false};
+    plan.sub_extent.push_back({q.off, (int64_t)s.row_dim * s.sdim});
+    o.sub.push_back(q);
+  }
+}
+static void load_model(const tj_model *m, Model &o, HpsiPlan &plan) {
+  if (!m || m->nsub < 1 || !m->sub) throw PlanError(TJ_ERR_ARG, "model needs sub(1:nsub), nsub >= 1");
+  o.len = m->len;
+  load_block(m->ham, o.ham, plan);
+  o.sub.resize(m->nsub);
+  for (int i = 0; i < m->nsub; ++i) {
+    load_block(m->sub[i].elec_up, o.sub[i][EU], plan);
+    load_block(m->sub[i].elec_down, o.sub[i][ED], plan);
+    load_block(m->sub[i].spin_sd, o.sub[i][SD], plan);
+    o.sub[i][SZ] = OBlk();
+    load_block(m->sub[i].num_sn, o.sub[i][SN], plan);
+  }
+}
+// block_pass_info (block.f90:1741-1768): zero block with the structure of `old`
+static void pass_info(const OBlk &old, OBlk &nw, HpsiPlan &plan) {
+  nw = old;
+  for (OSub &s : nw.sub) {
+    const int64_t n = (int64_t)s.row_dim * s.sdim;
+    s.off = plan.ops_len;
+    s.zero = true;
+    plan.sub_extent.push_back({s.off, n});
+    plan.merges.push_back({s.off, n, (int32_t)plan.merge_src.size(), (int32_t)plan.merge_src.size()});
+    plan.ops_len += align4(n);
+  }
+}
+// block_add_block_two (block.f90:1786-1822): the search restarts after the last match
+static void add_two(const OBlk &b1, double coef, OBlk &nw, HpsiPlan &plan) {
+  size_t x1 = 0;
+  for (OSub &s : nw.sub) {
+    for (size_t x = x1; x < b1.sub.size(); ++x) {
+      const OSub &q = b1.sub[x];
+      if (q.num_up == s.num_up && q.num_down == s.num_down && q.down_dif == s.down_dif) {
+        x1 = x + 1;
+        if ((int64_t)q.row_dim * q.sdim != (int64_t)s.row_dim * s.sdim)
+          throw PlanError(TJ_ERR_ARG, "hmerge: operator sub-blocks of different size");
+        // find the merge record of s (its destination offset)
+        for (auto it = plan.merges.rbegin(); it != plan.merges.rend(); ++it)
+          if (it->dst == s.off) {
+            // sources of one destination are contiguous: append by moving this record last
+            HpsiPlan::Merge m = *it;
+            std::vector<int64_t> src(plan.merge_src.begin() + m.s_begin, plan.merge_src.begin() + m.s_end);
+            std::vector<double> cf(plan.merge_coef.begin() + m.s_begin, plan.merge_coef.begin() + m.s_end);
+            src.push_back(q.off);
+            cf.push_back(coef);
+            it->s_begin = (int32_t)plan.merge_src.size();
+            plan.merge_src.insert(plan.merge_src.end(), src.begin(), src.end());
+            plan.merge_coef.insert(plan.merge_coef.end(), cf.begin(), cf.end());
+            it->s_end = (int32_t)plan.merge_src.size();
+            break;
+          }
+        s.zero = false;
+        break;
+      }
+    }
+  }
+}
+
+struct Geo {
+  const tj_lattice *L;
+  int ns1;
+  std::vector<int> inb;   // inb(-4:num_site) at [i+4]
+  int coup_bs[2][2] = {{0, 0}, {0, 0}}, coup_bb[2] = {0, 0};
+  int neib(int i, int k) const { return L->neib[(size_t)(k - 1) * ns1 + i]; }
+  int neiba(int i, int j) const { return L->neiba[(size_t)j * ns1 + i]; }
+  int inb1(int i, int j) const { return L->inb1[(size_t)j * ns1 + i]; }
+  int nleg11(int i) const { return L->nleg11[i - 1]; }
+  int nposi(int i) const { return L->nposi[i]; }
+  int nposi_dm(int i) const { return L->nposi_dm[i]; }
+  int nposi_lat(int i) const { return L->nposi_lat[i]; }
+  double jt(int k, int i) const { return L->jt[(size_t)i * L->neibt + k - 1]; }
+  double jd(int k, int i) const { return L->jd[(size_t)i * L->neibt + k - 1]; }
+  double jn(int k) const { return L->jn[k - 1]; }
+  double esite(int i) const { return L->esite[i]; }
+  int &INB(int i) { return inb[i + 4]; }
+  int npd(int j) const {   // nposi(nposi_dm(j)) with range checks
+    if (j < 0 || j >= ns1) throw PlanError(TJ_ERR_ARG, "lattice index out of range");
+    int p = nposi_dm(j);
+    if (p < 0 || p >= ns1) throw PlanError(TJ_ERR_ARG, "lattice index out of range");
+    return nposi(p);
+  }
+};
+
+static int slot(const Model &m, int i1) {
+  if (i1 < 1 || i1 > (int)m.sub.size()) {
+    char b[96];
+    std::snprintf(b, sizeof b, "operator slot %d outside 1..%d", i1, (int)m.sub.size());
+    throw PlanError(TJ_ERR_ARG, b);
+  }
+  return i1 - 1;
+}
+
+// hmerge (get_sys.f90:4383-4593)
+static void hmerge(Geo &g, Model &sys, Model &env, HpsiPlan &plan) {
+  const int neibt = g.L->neibt;
+  const int syssite = sys.len + 1, dmsite = sys.len + env.len + 2;
+  for (int k = 1; k <= neibt; ++k) {
+    int j = g.neib(syssite, k);
+    if (g.npd(j) == 3) g.coup_bs[1][0] = 1;
+    if (g.npd(j) == 1) g.coup_bs[0][0] = 1;
+    j = g.neib(g.nposi_lat(dmsite), k);
+    if (g.npd(j) == 3) g.coup_bs[1][1] = 1;
+    if (g.npd(j) == 1) g.coup_bs[0][1] = 1;
+  }
+  for (int ia = 0; ia < 2; ++ia) {
+    if (g.coup_bs[0][ia] == 1)
+      for (int op : {EU, SD, SN}) pass_info(sys.sub[0][op], sys.snc[ia][op], plan);
+    if (g.coup_bs[1][ia] == 1)
+      for (int op : {EU, ED, SD, SN}) pass_info(env.sub[0][op], env.snc[ia][op], plan);
+  }
+  for (int ia = 1; ia <= 2; ++ia) {
+    const int j = sys.len + 1 + (env.len + 1) * (ia - 1);
+    const int lj = g.nposi_lat(j);
+    for (int k1 = 1; k1 <= neibt; ++k1) {
+      const int ib = g.neib(lj, k1);
+      if (g.npd(ib) == 3 && g.coup_bs[1][ia - 1] != 0) {
+        const int s = slot(env, g.inb1(g.nposi_dm(ib) - sys.len - 1, env.len));
+        const double jd1 = g.jd(k1, lj), jt1 = g.jt(k1, lj), jn1 = g.jn(k1);
+        if (jt1 != 0.0) {
+          add_two(env.sub[s][EU], jt1, env.snc[ia - 1][EU], plan);
+          add_two(env.sub[s][ED], jt1, env.snc[ia - 1][ED], plan);
+        }
+        if (jd1 != 0.0) add_two(env.sub[s][SD], jd1, env.snc[ia - 1][SD], plan);
+        if (jn1 != 0.0) add_two(env.sub[s][SN], jn1, env.snc[ia - 1][SN], plan);
+      }
+      if (g.npd(ib) == 1 && g.coup_bs[0][ia - 1] == 1) {
+        const int s = slot(sys, g.inb1(g.nposi_dm(ib), sys.len));
+        const double jd1 = g.jd(k1, lj), jt1 = g.jt(k1, lj), jn1 = g.jn(k1);
+        if (jt1 != 0.0) add_two(sys.sub[s][EU], jt1, sys.snc[ia - 1][EU], plan);
+        if (jd1 != 0.0) add_two(sys.sub[s][SD], jd1, sys.snc[ia - 1][SD], plan);
+        if (jn1 != 0.0) add_two(sys.sub[s][SN], jn1, sys.snc[ia - 1][SN], plan);
+      }
+    }
+  }
+  int k11 = 0;
+  for (int I = 1; I <= sys.len; ++I) {
+    int k1 = 0;
+    for (int k = 1; k <= neibt; ++k)
+      if (g.npd(g.neib(I, k)) == 3) ++k1;
+    g.INB(I) = k1;
+    if (g.nleg11(env.len) < g.nleg11(sys.len)) g.INB(I) = 0;
+    if (g.INB(I) != 0) ++k11;
+  }
+  g.coup_bb[0] = k11;
+  g.INB(sys.len + 1) = 0;
+  g.INB(sys.len + 1 + env.len + 1) = 0;
+  for (int I = 1; I <= env.len; ++I) {
+    int k1 = 0;
+    g.INB(I + sys.len + 1) = 0;
+    for (int k = 1; k <= neibt; ++k) {
+      const int J = g.neib(g.nposi_lat(I + sys.len + 1), k);
+      if (g.npd(J) == 1 && g.INB(J) == 0) ++k1;
+    }
+    g.INB(I + sys.len + 1) = k1;
+    if (k1 != 0) ++k11;
+  }
+  g.coup_bb[1] = k11 - g.coup_bb[0];
+  env.sub_s.assign(g.coup_bb[0], {});
+  sys.sub_s.assign(g.coup_bb[1], {});
+  for (int i = 0; i < g.coup_bb[0]; ++i)
+    for (int op : {EU, ED, SD, SN}) pass_info(env.sub[0][op], env.sub_s[i][op], plan);
+  for (int i = 0; i < g.coup_bb[1]; ++i)
+    for (int op : {EU, SD, SN}) pass_info(sys.sub[0][op], sys.sub_s[i][op], plan);
+  int jc = 0;
+  for (int I = 1; I <= sys.len + env.len + 1; ++I) {
+    if (g.INB(I) == 0) continue;
+    const int Ia = g.nposi_lat(I);
+    ++jc;
+    for (int k1 = 1; k1 <= neibt; ++k1) {
+      const int ib = g.neib(Ia, k1);
+      if (g.npd(ib) == 3 && I <= sys.len) {
+        const int s = slot(env, g.inb1(g.nposi_dm(ib) - sys.len - 1, env.len));
+        const double jt1 = g.jt(k1, Ia), jd1 = g.jd(k1, Ia), jn1 = g.jn(k1);
+        if (jt1 != 0.0) {
+          add_two(env.sub[s][EU], jt1, env.sub_s[jc - 1][EU], plan);
+          add_two(env.sub[s][ED], jt1, env.sub_s[jc - 1][ED], plan);
+        }
+        if (jd1 != 0.0) add_two(env.sub[s][SD], jd1, env.sub_s[jc - 1][SD], plan);
+        if (jn1 != 0.0) add_two(env.sub[s][SN], jn1, env.sub_s[jc - 1][SN], plan);
+      }
+      if (g.npd(ib) == 1 && I > sys.len + 1 && g.INB(g.nposi_dm(ib)) == 0) {
+        const int s = slot(sys, g.inb1(ib, sys.len));
+        const int jc1 = jc - g.coup_bb[0];
+        const double jt1 = g.jt(k1, Ia), jd1 = g.jd(k1, Ia), jn1 = g.jn(k1);
+        if (jc1 < 1 || jc1 > (int)sys.sub_s.size()) throw PlanError(TJ_ERR_ARG, "hmerge: leg index out of range");
+        if (jt1 != 0.0) add_two(sys.sub[s][EU], jt1, sys.sub_s[jc1 - 1][EU], plan);
+        if (jd1 != 0.0) add_two(sys.sub[s][SD], jd1, sys.sub_s[jc1 - 1][SD], plan);
+        if (jn1 != 0.0) add_two(sys.sub[s][SN], jn1, sys.sub_s[jc1 - 1][SN], plan);
+      }
+    }
+  }
+}
+
+static void check_lattice(const tj_lattice *L) {
+  if (!L || !L->neib || !L->neiba || !L->inb1 || !L->nleg11 || !L->nposi || !L->nposi_dm || !L->nposi_lat ||
+      !L->jt || !L->jz || !L->jd || !L->jn || !L->esite)
+    throw PlanError(TJ_ERR_ARG, "lattice tables missing");
+  if (L->num_site < 2 || L->neibt < 1) throw PlanError(TJ_ERR_ARG, "bad lattice sizes");
+}
+
+}  // namespace
+
+int build_hpsi_plan(const tj_lattice *lat, const tj_model *sysm, const tj_model *envm, const tj_basis *sys_bs,
+                    const tj_basis *env_bs, const tj_wave *wave, HpsiPlan &plan, std::string &msg) {
+  try {
+    check_lattice(lat);
+    if (!sys_bs || !env_bs || !wave || !sys_bs->sub || !env_bs->sub || (wave->num > 0 && !wave->sub))
+      throw PlanError(TJ_ERR_ARG, "null basis or wave");
+    plan = HpsiPlan();
+    Model sys, env;
+    load_model(sysm, sys, plan);
+    load_model(envm, env, plan);
+    if (sys.len + env.len + 2 > lat->num_site) throw PlanError(TJ_ERR_ARG, "sys_len + env_len + 2 exceeds num_site");
+    Geo g;
+    g.L = lat;
+    g.ns1 = lat->num_site + 1;
+    g.inb.assign(lat->num_site + 8, 0);
+    hmerge(g, sys, env, plan);
+    const SiteOps so = make_site_ops(lat->up_bias);
+    Builder B(sys_bs, env_bs, wave, plan);
+    B.init_cells();
+    plan.psi_len = wave->dim;
+    // model_wave, add_op = 1 (get_sys.f90:4157-4239)
+    B.block_vec_dia(OView{&sys.ham, false}, 1.0);
+    B.vec_block_dia(OView{&env.ham, false}, 1.0);
+    const int is = g.nposi_lat(sys.len + 1), js = g.nposi_lat(sys.len + env.len + 2);
+    if (g.esite(is) != 0.0) B.site_vec_site_dia(so.ne, so.si, g.esite(is));
+    if (g.esite(js) != 0.0) B.site_vec_site_dia(so.si, so.ne, g.esite(js));
+    const int ii = g.neiba(is, js);
+    if (ii != 0) {
+      const double jd1 = g.jd(ii, is), coefx = g.jt(ii, is), jn1 = g.jn(ii);
+      if (coefx != 0.0) B.site_vec_site_ndia(so.eu, 'F', so.eu, 'F', coefx);
+      if (jd1 != 0.0) B.site_vec_site_ndia(so.sd, 'B', so.sd, 'B', jd1);
+      B.site_vec_site_dia(so.ne, so.ne, jn1);
+    }
+    if (g.coup_bs[0][0] == 1) {
+      B.block_site_vec_ndia(OView{&sys.snc[0][EU], false}, so.eu, 'F', 1.0);
+      B.block_site_vec_ndia(OView{&sys.snc[0][SD], false}, so.sd, 'B', 1.0);
+      B.block_site_vec_dia(OView{&sys.snc[0][SN], false}, so.ne, 1.0);
+    }
+    if (g.coup_bs[0][1] == 1) {
+      B.block_vec_site_ndia(OView{&sys.snc[1][EU], false}, so.eu, 'F', 1.0);
+      B.block_vec_site_ndia(OView{&sys.snc[1][SD], false}, so.sd, 'B', 1.0);
+      B.block_vec_site_dia(OView{&sys.snc[1][SN], false}, so.ne, 1.0);
+    }
+    if (g.coup_bs[1][0] == 1) {
+      B.site_vec_block_ndia(so.eu, 'F', OView{&env.snc[0][ED], true}, 'F', 1.0);
+      B.site_vec_block_ndia(so.sd, 'B', OView{&env.snc[0][SD], true}, 'B', 1.0);
+      B.site_vec_block_dia(so.ne, OView{&env.snc[0][SN], false}, 1.0);
+    }
+    if (g.coup_bs[1][1] == 1) {
+      B.vec_block_site_ndia(OView{&env.snc[1][EU], false}, 'F', so.eu, 'F', 1.0);
+      B.vec_block_site_ndia(OView{&env.snc[1][SD], false}, 'B', so.sd, 'B', 1.0);
+      B.vec_block_site_dia(OView{&env.snc[1][SN], false}, so.ne, 1.0);
+    }
+    int jc = 0;
+    for (int i = 1; i <= sys.len + 1 + env.len; ++i) {
+      if (g.INB(i) == 0) continue;
+      ++jc;
+      const std::array<OBlk, 5> *sa, *eb;
+      if (i <= sys.len) {
+        sa = &sys.sub[slot(sys, g.inb1(i, sys.len))];
+        if (jc > (int)env.sub_s.size()) throw PlanError(TJ_ERR_ARG, "leg index out of range");
+        eb = &env.sub_s[jc - 1];
+      } else {
+        eb = &env.sub[slot(env, g.inb1(i - sys.len - 1, env.len))];
+        const int jc1 = jc - g.coup_bb[0];
+        if (jc1 < 1 || jc1 > (int)sys.sub_s.size()) throw PlanError(TJ_ERR_ARG, "leg index out of range");
+        sa = &sys.sub_s[jc1 - 1];
+      }
+      B.block_vec_block_ndia(OView{&(*sa)[EU], false}, OView{&(*eb)[ED], true}, 'F', 1.0);
+      B.block_vec_block_ndia(OView{&(*sa)[SD], false}, OView{&(*eb)[SD], true}, 'B', 1.0);
+      B.block_vec_block_dia(OView{&(*sa)[SN], false}, OView{&(*eb)[SN], false}, 1.0);
+    }
+    B.finalize();
+    // algorithmic bytes: every operator sub-block touched once, psi read, output read-modify-write
+    double opb = 0;
+    {
+      std::unordered_map<int64_t, int64_t> sz;
+      for (const auto &e : plan.sub_extent) sz[e.first] = e.second;
+      for (int64_t off : B.op_touched) opb += (double)sz[off];
+    }
+    plan.bytes = 8.0 * (opb + 3.0 * (double)wave->dim);
+    return TJ_OK;
+  } catch (const PlanError &e) {
+    msg = e.what();
+    return e.code;
+  } catch (const std::exception &e) {
+    msg = e.what();
+    return TJ_ERR_ARG;
+  }
+}
+
+static_assert(sizeof(Task) == sizeof(tj_plan_task), "task layout");
+static_assert(sizeof(Cell) == sizeof(tj_plan_cell), "cell layout");
+static_assert(sizeof(HpsiPlan::Upload) == sizeof(tj_plan_upload), "upload layout");
+static_assert(sizeof(HpsiPlan::Merge) == sizeof(tj_plan_merge), "merge layout");
+
+}  // namespace tjb
+
+extern "C" int tj_hpsi_plan_export(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
+                                   const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave,
+                                   tj_plan_export *out) {
+  if (!out) return tjb_set_err(TJ_ERR_ARG, "null output");
+  tjb::HpsiPlan P;
+  std::string msg;
+  int rc = tjb::build_hpsi_plan(lat, sys, env, sys_bs, env_bs, wave, P, msg);
+  if (rc) return tjb_set_err(rc, "H*psi plan: " + msg);
+  out->ops_len = P.ops_len;
+  out->scratch_len = P.scratch_len;
+  out->psi_len = P.psi_len;
+  out->n_tasks1 = (int64_t)P.tasks1.size();
+  out->n_tasks2 = (int64_t)P.tasks2.size();
+  out->n_cells1 = (int64_t)P.cells1.size();
+  out->n_cells2 = (int64_t)P.cells2.size();
+  out->n_uploads = (int64_t)P.uploads.size();
+  out->n_merges = (int64_t)P.merges.size();
+  out->n_merge_src = (int64_t)P.merge_src.size();
+  out->flops = P.flops;
+  out->flops_ref = P.flops_ref;
+  out->bytes = P.bytes;
+  auto cp = [](void *dst, const void *src, size_t n) { if (dst && n) std::memcpy(dst, src, n); };
+  cp(out->tasks1, P.tasks1.data(), P.tasks1.size() * sizeof(tjb::Task));
+  cp(out->tasks2, P.tasks2.data(), P.tasks2.size() * sizeof(tjb::Task));
+  cp(out->cells1, P.cells1.data(), P.cells1.size() * sizeof(tjb::Cell));
+  cp(out->cells2, P.cells2.data(), P.cells2.size() * sizeof(tjb::Cell));
+  cp(out->uploads, P.uploads.data(), P.uploads.size() * sizeof(tjb::HpsiPlan::Upload));
+  cp(out->merges, P.merges.data(), P.merges.size() * sizeof(tjb::HpsiPlan::Merge));
+  cp(out->merge_src, P.merge_src.data(), P.merge_src.size() * sizeof(int64_t));
+  cp(out->merge_coef, P.merge_coef.data(), P.merge_coef.size() * sizeof(double));
+  return TJ_OK;
+}

@@ -1,0 +1,100 @@
+// Internal data structures of the B200 tjsq hot path.
+//
+// H*psi is compiled, once per DMRG step, into two grouped-GEMM work lists:
+//
+//   phase 1  (products)   P_p  = op(A_p) * X_p          one output per product
+//   phase 2  (cells)      Y_c  = sum_t coef_t * L_t * R_t  (+ sum coef * X  axpy terms)
+//
+// where every X is a "cell" of psi -- the rectangle of one sector matrix
+// spanned by one system sub-block (Sub_Basis_Map) and one environment
+// sub-block -- every Y is a cell of the output vector, A/R are operator
+// sub-blocks (possibly transposed), and L is a phase-1 product, an operator
+// sub-block or a psi cell.  Each output cell is owned by exactly one set of
+// CTAs, so accumulation needs no atomics and is deterministic.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/tj_b200.h"
+
+namespace tjb {
+
+// Memory space an operand lives in.
+enum Space : int8_t { SP_NONE = 0, SP_OPS = 1, SP_PSI = 2, SP_SCR = 3 };
+
+// A dense column-major matrix operand, used as op(M) (trans = 1 means M^T).
+struct Operand {
+  int64_t off;     // element offset into the space's base pointer
+  int32_t ld;      // leading dimension of the stored matrix
+  int8_t space;    // Space
+  int8_t trans;    // 0: M, 1: M^T
+  int16_t pad;
+};
+
+// One contribution to a cell: Y += coef * op(L) * op(R); R.space == SP_NONE is an axpy Y += coef * L.
+struct Task {
+  Operand L, R;
+  double coef;
+  int32_t K;       // inner dimension (ignored for axpy)
+  int32_t pad;
+};
+
+// An output rectangle and the tasks that accumulate into it.
+struct Cell {
+  int64_t off;     // element offset of Y(0,0) in the output space
+  int32_t ld, M, N;
+  int32_t t_begin, t_end;  // range in the task array
+  int8_t space;    // SP_SCR (phase 1) or SP_PSI (phase 2 output vector)
+  int8_t pad[7];
+};
+
+// One CTA work item: a BM x BN tile of a cell.
+struct Tile {
+  int32_t cell, row0, col0, pad;
+};
+
+// The compiled H*psi of one superblock.
+struct HpsiPlan {
+  // operator storage: every input sub-block, then every merged sub-block
+  int64_t ops_len = 0;                       // doubles
+  struct Upload { const double *src; int64_t n; int64_t dst; };
+  std::vector<Upload> uploads;               // host -> device op copies
+  struct Merge { int64_t dst, n; int32_t s_begin, s_end; };
+  std::vector<Merge> merges;                 // merged sub-blocks (hmerge)
+  std::vector<int64_t> merge_src;            // source offsets
+  std::vector<double> merge_coef;            // and coefficients
+  std::vector<std::pair<int64_t, int64_t>> sub_extent;   // (offset, doubles) of every sub-block
+
+  std::vector<Task> tasks1, tasks2;
+  std::vector<Cell> cells1, cells2;
+  std::vector<Tile> tiles1, tiles2;
+  int64_t scratch_len = 0;                   // doubles of phase-1 products
+  int64_t psi_len = 0;
+
+  // accounting
+  double flops = 0, flops_ref = 0, bytes = 0;
+  std::string key;                           // structural fingerprint
+};
+
+// Tile shape of the grouped FP64 kernel.
+constexpr int BM = 64, BN = 64, BK = 16;
+
+// Builds the plan (host).  Returns TJ_OK or an error code with msg set.
+int build_hpsi_plan(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
+                    const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave,
+                    HpsiPlan &plan, std::string &msg);
+
+// Racah 6j symbol on doubled spins (host); same formula as the reference's W6JS.
+double w6j(int j1, int j2, int j3, int l1, int l2, int l3);
+
+// Correlator plans: one cell list whose epilogue dots with psi instead of storing.
+enum CorKind {
+  COR_MEASURE_SYS_BLOCK, COR_MEASURE_ENV_BLOCK, COR_SBEB_DIA, COR_SBEB_NDIA, COR_SB_SITE_NDIA,
+  COR_EB_SITE_NDIA, COR_SB_ESITE_NDIA, COR_SSITE_EB_NDIA, COR_SSITE_ESITE_NDIA
+};
+int build_cor_plan(CorKind kind, const tj_block *a, const tj_block *b, const tj_basis *sys_bs,
+                   const tj_basis *env_bs, const tj_wave *wave, char flag, HpsiPlan &plan,
+                   std::string &msg);
+
+}  // namespace tjb

@@ -1,0 +1,262 @@
+"""Python mirror of the reference's routine interface, bound to libtjb200.so.
+
+Each function takes the same objects as the Fortran routine it replaces
+(models, bases, wavefunctions) and calls the corresponding C-ABI entry point
+of include/tj_b200.h.  There is no CPU path: when the compiled library is
+missing or no B200 is visible the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+from .structs import (Block, TjBasis, TjBlock, TjBlockSub, TjHpsiStats, TjLattice, TjModel,
+                      TjTruncResult, TjWave, Wave, block_from_c_result)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtjb200.so")
+
+TJ_PREC_FP64, TJ_PREC_OZAKI = 0, 1
+
+
+class TjError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("tj error %d: %s" % (code, msg))
+        self.code = code
+
+
+class PlanOperand(C.Structure):
+    _fields_ = [("off", C.c_int64), ("ld", C.c_int32), ("space", C.c_int8), ("trans", C.c_int8),
+                ("pad_", C.c_int16)]
+
+
+class PlanTask(C.Structure):
+    _fields_ = [("L", PlanOperand), ("R", PlanOperand), ("coef", C.c_double), ("K", C.c_int32),
+                ("pad_", C.c_int32)]
+
+
+class PlanCell(C.Structure):
+    _fields_ = [("off", C.c_int64), ("ld", C.c_int32), ("M", C.c_int32), ("N", C.c_int32),
+                ("t_begin", C.c_int32), ("t_end", C.c_int32), ("space", C.c_int8), ("pad_", C.c_int8 * 7)]
+
+
+class PlanUpload(C.Structure):
+    _fields_ = [("src", C.c_void_p), ("n", C.c_int64), ("dst", C.c_int64)]
+
+
+class PlanMerge(C.Structure):
+    _fields_ = [("dst", C.c_int64), ("n", C.c_int64), ("s_begin", C.c_int32), ("s_end", C.c_int32)]
+
+
+class PlanExport(C.Structure):
+    _fields_ = [("ops_len", C.c_int64), ("scratch_len", C.c_int64), ("psi_len", C.c_int64),
+                ("n_tasks1", C.c_int64), ("n_tasks2", C.c_int64), ("n_cells1", C.c_int64),
+                ("n_cells2", C.c_int64), ("n_uploads", C.c_int64), ("n_merges", C.c_int64),
+                ("n_merge_src", C.c_int64), ("flops", C.c_double), ("flops_ref", C.c_double),
+                ("bytes", C.c_double),
+                ("tasks1", C.POINTER(PlanTask)), ("tasks2", C.POINTER(PlanTask)),
+                ("cells1", C.POINTER(PlanCell)), ("cells2", C.POINTER(PlanCell)),
+                ("uploads", C.POINTER(PlanUpload)), ("merges", C.POINTER(PlanMerge)),
+                ("merge_src", C.POINTER(C.c_int64)), ("merge_coef", C.POINTER(C.c_double))]
+
+
+_lib = None
+
+
+class _Lib:
+    """Wraps the CDLL; argtypes of symbols the library does not export are skipped."""
+
+    def __init__(self, dll):
+        object.__setattr__(self, "_dll", dll)
+
+    def __getattr__(self, name):
+        try:
+            return getattr(self._dll, name)
+        except AttributeError:
+            return _Missing(name)
+
+
+class _Missing:
+    def __init__(self, name):
+        self.name = name
+
+    def __setattr__(self, k, v):
+        object.__setattr__(self, k, v)
+
+    def __call__(self, *a):
+        raise TjError(-1, "libtjb200.so does not export " + self.name)
+
+
+COR_NAMES = {
+    "measure_sys_block": 0, "measure_env_block": 1, "sys_block_env_block_cor_dia": 2,
+    "sys_block_env_block_cor_ndia": 3, "sys_block_site_cor_ndia": 4, "env_block_site_cor_ndia": 5,
+    "sys_block_env_site_cor_ndia": 6, "sys_site_env_block_cor_ndia": 7, "sys_site_env_site_cor_ndia": 8,
+}
+
+
+def lib():
+    """Loads libtjb200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError("libtjb200.so not built: run python -m grand_sql_tj_b200.build")
+        L = _Lib(C.CDLL(LIB_PATH))
+        P = C.POINTER
+        L.tj_last_error.restype = C.c_char_p
+        L.tj_ctx_create.argtypes = [P(C.c_void_p), C.c_int]
+        L.tj_ctx_destroy.argtypes = [C.c_void_p]
+        L.tj_set_precision.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.tj_step_begin.argtypes = [C.c_void_p]
+        hp = [C.c_void_p, P(TjLattice), P(TjModel), P(TjModel), P(TjBasis), P(TjBasis)]
+        L.tj_model_wave.argtypes = hp + [P(TjWave), P(TjWave)]
+        L.tj_model_wave_bench.argtypes = hp + [P(TjWave), P(TjWave), C.c_int, P(C.c_double)]
+        L.tj_lanczos_memo_new.argtypes = hp + [P(TjWave), C.c_int, C.c_double, P(C.c_double), P(C.c_int)]
+        L.tj_truncation.argtypes = [C.c_void_p, P(TjWave), C.c_int, C.c_int, C.c_int, C.c_double,
+                                    P(TjTruncResult)]
+        L.tj_hpsi_stats_get.argtypes = [C.c_void_p, P(TjHpsiStats)]
+        L.tj_hpsi_plan_export.argtypes = [P(TjLattice), P(TjModel), P(TjModel), P(TjBasis), P(TjBasis),
+                                          P(TjWave), P(PlanExport)]
+        for n in ("tj_measure_sys_block", "tj_measure_env_block"):
+            getattr(L, n).argtypes = [C.c_void_p, P(TjBlock), P(TjBasis), P(TjWave), P(C.c_double)]
+        L.tj_sys_block_env_block_cor_dia.argtypes = [C.c_void_p, P(TjBlock), P(TjBlock), P(TjBasis),
+                                                     P(TjBasis), P(TjWave), P(C.c_double)]
+        for n in ("tj_sys_block_env_block_cor_ndia", "tj_sys_block_env_site_cor_ndia",
+                  "tj_sys_site_env_block_cor_ndia", "tj_sys_site_env_site_cor_ndia"):
+            getattr(L, n).argtypes = [C.c_void_p, P(TjBlock), P(TjBlock), P(TjBasis), P(TjBasis),
+                                      P(TjWave), C.c_char, P(C.c_double)]
+        for n in ("tj_sys_block_site_cor_ndia", "tj_env_block_site_cor_ndia"):
+            getattr(L, n).argtypes = [C.c_void_p, P(TjBlock), P(TjBlock), P(TjBasis), P(TjWave),
+                                      C.c_char, P(C.c_double)]
+        _lib = L
+    return _lib
+
+
+def _chk(rc: int):
+    if rc:
+        raise TjError(rc, lib().tj_last_error().decode())
+
+
+class Context:
+    """One tj_ctx: a CUDA device, a stream and the cached plan of the current step."""
+
+    def __init__(self, device: int = 0):
+        self.h = C.c_void_p()
+        _chk(lib().tj_ctx_create(C.byref(self.h), device))
+
+    def close(self):
+        if self.h:
+            lib().tj_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_precision(self, mode: int, slices: int = 6):
+        _chk(lib().tj_set_precision(self.h, mode, slices))
+
+    def step_begin(self):
+        _chk(lib().tj_step_begin(self.h))
+
+    def stats(self) -> TjHpsiStats:
+        s = TjHpsiStats()
+        _chk(lib().tj_hpsi_stats_get(self.h, C.byref(s)))
+        return s
+
+    # --------------------------------------------------------- hot path
+    def model_wave(self, sb, invec: Optional[Wave] = None) -> Wave:
+        """model_wave (get_sys.f90:4127) with hmerge; host buffers in and out."""
+        invec = sb.wave if invec is None else invec
+        ps, pe, bs, be = sb.sys.pack(), sb.env.pack(), sb.sys_bs.pack(), sb.env_bs.pack()
+        out = invec.like()
+        _chk(lib().tj_model_wave(self.h, C.byref(sb.lat.c), C.byref(ps.c), C.byref(pe.c), C.byref(bs.c),
+                                 C.byref(be.c), C.byref(invec.c), C.byref(out.c)))
+        return out
+
+    def model_wave_bench(self, sb, reps: int, invec: Optional[Wave] = None) -> Tuple[float, Wave]:
+        invec = sb.wave if invec is None else invec
+        ps, pe, bs, be = sb.sys.pack(), sb.env.pack(), sb.sys_bs.pack(), sb.env_bs.pack()
+        out = invec.like()
+        ms = C.c_double()
+        _chk(lib().tj_model_wave_bench(self.h, C.byref(sb.lat.c), C.byref(ps.c), C.byref(pe.c), C.byref(bs.c),
+                                       C.byref(be.c), C.byref(invec.c), C.byref(out.c), reps, C.byref(ms)))
+        return ms.value, out
+
+    def lanczos_memo_new(self, sb, lanzero: float, start: Optional[Wave] = None):
+        """lanczos_memo_new (eigen.f90:2), levels = 1: returns (E0, iterations, Ritz vector)."""
+        w = (sb.wave if start is None else start).copy()
+        ps, pe, bs, be = sb.sys.pack(), sb.env.pack(), sb.sys_bs.pack(), sb.env_bs.pack()
+        e, it = (C.c_double * 1)(), C.c_int()
+        _chk(lib().tj_lanczos_memo_new(self.h, C.byref(sb.lat.c), C.byref(ps.c), C.byref(pe.c), C.byref(bs.c),
+                                       C.byref(be.c), C.byref(w.c), 1, lanzero, e, C.byref(it)))
+        return e[0], it.value, w
+
+    def truncation(self, wave: Wave, side: int, kept_min: int, kept_max: int, trun_err: float):
+        """Get_density_matrix_{sys,env}_new + Get_truncation_operator (den_mat.f90)."""
+        r = TjTruncResult()
+        _chk(lib().tj_truncation(self.h, C.byref(wave.c), side, kept_min, kept_max, trun_err, C.byref(r)))
+        subs = (TjBlockSub * max(r.num, 1))()
+        data = np.zeros(max(r.data_len, 1))
+        r.sub = C.cast(subs, C.POINTER(TjBlockSub))
+        r.data = data.ctypes.data_as(C.POINTER(C.c_double))
+        _chk(lib().tj_truncation(self.h, C.byref(wave.c), side, kept_min, kept_max, trun_err, C.byref(r)))
+        length = wave.sys_len if side == 0 else wave.env_len
+        return r, block_from_c_result(r, length)
+
+    def correlator(self, name: str, a: Block, b: Optional[Block], sys_bs, env_bs, wave: Wave,
+                   flag: str = "B") -> float:
+        """The measure.f90 contraction `name` (e.g. 'sys_block_env_block_cor_ndia')."""
+        L = lib()
+        v = C.c_double()
+        pa = a.pack()
+        pb = b.pack() if b is not None else None
+        ps = sys_bs.pack() if sys_bs is not None else None
+        pe = env_bs.pack() if env_bs is not None else None
+        fn = getattr(L, "tj_" + name)
+        f = flag.encode()
+        if name == "measure_sys_block":
+            _chk(fn(self.h, C.byref(pa.c), C.byref(ps.c), C.byref(wave.c), C.byref(v)))
+        elif name == "measure_env_block":
+            _chk(fn(self.h, C.byref(pa.c), C.byref(pe.c), C.byref(wave.c), C.byref(v)))
+        elif name == "sys_block_env_block_cor_dia":
+            _chk(fn(self.h, C.byref(pa.c), C.byref(pb.c), C.byref(ps.c), C.byref(pe.c), C.byref(wave.c),
+                    C.byref(v)))
+        elif name == "sys_block_site_cor_ndia":
+            _chk(fn(self.h, C.byref(pa.c), C.byref(pb.c), C.byref(ps.c), C.byref(wave.c), f, C.byref(v)))
+        elif name == "env_block_site_cor_ndia":
+            _chk(fn(self.h, C.byref(pa.c), C.byref(pb.c), C.byref(pe.c), C.byref(wave.c), f, C.byref(v)))
+        else:
+            _chk(fn(self.h, C.byref(pa.c), C.byref(pb.c), C.byref(ps.c), C.byref(pe.c), C.byref(wave.c), f,
+                    C.byref(v)))
+        return v.value
+
+
+def plan_export(sb, invec: Optional[Wave] = None) -> dict:
+    """Compiled task lists of H*psi for `sb` (no GPU needed)."""
+    L = lib()
+    invec = sb.wave if invec is None else invec
+    ps, pe, bs, be = sb.sys.pack(), sb.env.pack(), sb.sys_bs.pack(), sb.env_bs.pack()
+    ex = PlanExport()
+    args = (C.byref(sb.lat.c), C.byref(ps.c), C.byref(pe.c), C.byref(bs.c), C.byref(be.c), C.byref(invec.c))
+    _chk(L.tj_hpsi_plan_export(*args, C.byref(ex)))
+    arrs = {
+        "tasks1": (PlanTask * max(ex.n_tasks1, 1))(), "tasks2": (PlanTask * max(ex.n_tasks2, 1))(),
+        "cells1": (PlanCell * max(ex.n_cells1, 1))(), "cells2": (PlanCell * max(ex.n_cells2, 1))(),
+        "uploads": (PlanUpload * max(ex.n_uploads, 1))(), "merges": (PlanMerge * max(ex.n_merges, 1))(),
+        "merge_src": (C.c_int64 * max(ex.n_merge_src, 1))(), "merge_coef": (C.c_double * max(ex.n_merge_src, 1))(),
+    }
+    for k, a in arrs.items():
+        setattr(ex, k, C.cast(a, type(getattr(ex, k))))
+    _chk(L.tj_hpsi_plan_export(*args, C.byref(ex)))
+    # copy the operator data now, while the packed buffers are alive
+    ops = np.zeros(max(ex.ops_len, 1))
+    for i in range(ex.n_uploads):
+        u = arrs["uploads"][i]
+        src = np.ctypeslib.as_array(C.cast(u.src, C.POINTER(C.c_double)), shape=(u.n,))
+        ops[u.dst:u.dst + u.n] = src
+    return {"ex": ex, "ops": ops, **arrs}

@@ -225,6 +225,7 @@ typedef struct tj_hpsi_stats {
   int64_t n_products, n_tasks, n_tiles_p1, n_tiles_p2, scratch_doubles;
   double last_ms;          /* device time of the last H*psi                      */
   double last_ms_phase1, last_ms_phase2;
+  int64_t lanczos_hpsi;    /* H*psi products of the last tj_lanczos_memo_new      */
 } tj_hpsi_stats;
 int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st);
 
@@ -236,6 +237,34 @@ int tj_model_wave_bench(tj_ctx *ctx, const tj_lattice *lat,
                         const tj_model *sys, const tj_model *env,
                         const tj_basis *sys_bs, const tj_basis *env_bs,
                         const tj_wave *invec, tj_wave *outvec, int reps, double *ms);
+
+/* ------------------------------------------------------ plan introspection */
+/* The compiled form of one H*psi (hmerge + model_wave): phase-1 products
+ * P = op(A) * X and phase-2 cells Y = sum coef * op(L) * op(R) (R.space == 0:
+ * Y += coef * L).  Spaces: 1 operators, 2 input vector, 3 phase-1 products.
+ * op(M) = M (trans 0) or M^T (trans 1) of the column-major matrix at
+ * base + off with leading dimension ld.  This call needs no GPU and does no
+ * arithmetic; the test-suite uses it to check the compiler on the CPU.
+ * Two-call pattern: with every array pointer NULL the counts are filled. */
+typedef struct tj_plan_operand { int64_t off; int32_t ld; int8_t space, trans; int16_t pad_; } tj_plan_operand;
+typedef struct tj_plan_task { tj_plan_operand L, R; double coef; int32_t K, pad_; } tj_plan_task;
+typedef struct tj_plan_cell { int64_t off; int32_t ld, M, N, t_begin, t_end; int8_t space, pad_[7]; } tj_plan_cell;
+typedef struct tj_plan_upload { const double *src; int64_t n, dst; } tj_plan_upload;
+typedef struct tj_plan_merge { int64_t dst, n; int32_t s_begin, s_end; } tj_plan_merge;
+typedef struct tj_plan_export {
+  int64_t ops_len, scratch_len, psi_len;
+  int64_t n_tasks1, n_tasks2, n_cells1, n_cells2, n_uploads, n_merges, n_merge_src;
+  double flops, flops_ref, bytes;
+  tj_plan_task *tasks1, *tasks2;
+  tj_plan_cell *cells1, *cells2;
+  tj_plan_upload *uploads;
+  tj_plan_merge *merges;
+  int64_t *merge_src;
+  double *merge_coef;
+} tj_plan_export;
+int tj_hpsi_plan_export(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
+                        const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave,
+                        tj_plan_export *out);
 
 #ifdef __cplusplus
 }
