@@ -238,6 +238,28 @@ int tj_model_wave_bench(tj_ctx *ctx, const tj_lattice *lat,
                         const tj_basis *sys_bs, const tj_basis *env_bs,
                         const tj_wave *invec, tj_wave *outvec, int reps, double *ms);
 
+/* ------------------------------------------------ allocation-free H*psi */
+/* No counterpart in the reference.  model_wave (with hmerge) for callers that
+ * cannot allocate device memory while they run -- for example a Fortran sweep
+ * driver whose device memory belongs to its own pool, or a host program that
+ * forbids allocation inside a solve.  The caller passes every operator
+ * block's data and both wavefunctions' data as DEVICE pointers (8-byte
+ * aligned; the sector and sub-block tables stay in host memory).  Everything
+ * else -- hmerge'd operator sums, phase-1 products, work lists -- is placed
+ * in one fixed array of TJ_NOALLOC_SCRATCH_BYTES in device global memory
+ * that the library declares; every GPU that loads the library holds it until
+ * the process exits.  The call allocates nothing (no cudaMalloc/cudaFree),
+ * runs on `stream` (a cudaStream_t, NULL for the default stream) and returns
+ * after the stream has synchronised.  A superblock needing more scratch than
+ * the array holds is rejected with TJ_ERR_LIMIT.  The first call on a device
+ * looks up the array's device address, so make that first call before any
+ * stream capture.  All calls share the one array: calls that overlap on the
+ * GPU (other threads, other streams) race and must not be issued. */
+#define TJ_NOALLOC_SCRATCH_BYTES (64ull << 20)
+int tj_model_wave_noalloc(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
+                          const tj_basis *sys_bs, const tj_basis *env_bs,
+                          const tj_wave *invec, tj_wave *outvec, void *stream);
+
 /* ------------------------------------------------------ plan introspection */
 /* The compiled form of one H*psi (hmerge + model_wave): phase-1 products
  * P = op(A) * X and phase-2 cells Y = sum coef * op(L) * op(R) (R.space == 0:
