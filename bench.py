@@ -35,13 +35,14 @@ UNIT = "H*psi/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="cyl4x24_m2000")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "ozaki"])
     ap.add_argument("--slices", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end Lanczos leg (profiling runs)")
     ap.add_argument("--seed", type=int, default=1234)
     return ap.parse_args()
 
@@ -60,7 +61,7 @@ class Clocks:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -236,25 +237,27 @@ def main():
     ms_max = allmax(pg, ms, args.impl)
     value = ws * 1000.0 / ms_max
 
-    # end to end through the reference-facing call: lanczos_memo_new with host buffers
-    ctx.step_begin()
-    lz = 20.0e-6
-    t0 = time.perf_counter()
-    e0, iters, _ = ctx.lanczos_memo_new(sb, lz)
-    e2e_wall = time.perf_counter() - t0
-    st2 = ctx.stats()
-    nh = max(int(st2.lanczos_hpsi), 1)
-    e2e_wall = allmax(pg, e2e_wall, args.impl)
-    ops_bytes = 0
-    for m in (sb.sys, sb.env):
-        ops_bytes += sum(s.mat.size for s in m.ham.subs) * 8
-        for bs in m.sub:
-            for k in ("elec_up", "elec_down", "spin_sd", "num_sn"):
-                ops_bytes += sum(s.mat.size for s in getattr(bs, k).subs) * 8
-    e2e = {"value": ws * nh / e2e_wall, "unit": UNIT, "via": "tj_lanczos_memo_new (plan + operator upload + "
-           "%d H*psi + Ritz vector download)" % nh,
-           "h2d_bytes_per_step": int((ops_bytes + 8 * sb.wave.dim) / nh),
-           "d2h_bytes_per_step": int(8 * sb.wave.dim / nh), "lanczos_iters": iters, "E0": e0}
+    e2e = None
+    if not args.no_e2e:
+        # end to end through the reference-facing call: lanczos_memo_new with host buffers
+        ctx.step_begin()
+        lz = 20.0e-6
+        t0 = time.perf_counter()
+        e0, iters, _ = ctx.lanczos_memo_new(sb, lz)
+        e2e_wall = time.perf_counter() - t0
+        st2 = ctx.stats()
+        nh = max(int(st2.lanczos_hpsi), 1)
+        e2e_wall = allmax(pg, e2e_wall, args.impl)
+        ops_bytes = 0
+        for m in (sb.sys, sb.env):
+            ops_bytes += sum(s.mat.size for s in m.ham.subs) * 8
+            for bs in m.sub:
+                for k in ("elec_up", "elec_down", "spin_sd", "num_sn"):
+                    ops_bytes += sum(s.mat.size for s in getattr(bs, k).subs) * 8
+        e2e = {"value": ws * nh / e2e_wall, "unit": UNIT, "via": "tj_lanczos_memo_new (plan + operator upload + "
+               "%d H*psi + Ritz vector download)" % nh,
+               "h2d_bytes_per_step": int((ops_bytes + 8 * sb.wave.dim) / nh),
+               "d2h_bytes_per_step": int(8 * sb.wave.dim / nh), "lanczos_iters": iters, "E0": e0}
 
     peaks = measured_peaks()
     if rank == 0:

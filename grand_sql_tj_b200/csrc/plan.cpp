@@ -136,6 +136,20 @@ static SiteOp make_site(int up_dif, int down_dif, std::vector<std::tuple<int, in
   }
   return s;
 }
+static SiteOp site_from_block(const tj_block &b) {
+  if (b.num < 1 || !b.sub || !b.data) throw PlanError(TJ_ERR_ARG, "site operator block is empty");
+  SiteOp s;
+  s.b.len = b.len;
+  s.b.up_dif = b.up_dif;
+  s.b.down_dif = b.down_dif;
+  for (int k = 0; k < b.num; ++k) {
+    const tj_block_sub &q = b.sub[k];
+    if (q.row_dim != 1 || q.sdim != 1) throw PlanError(TJ_ERR_ARG, "site operator sub-blocks must be 1x1");
+    s.b.sub.push_back(OSub{q.num_up, q.num_down, q.down_dif, 1, 1, -1, false});
+    s.val.push_back(b.data[q.off]);
+  }
+  return s;
+}
 static SiteOps make_site_ops(int ub) {
   SiteOps o;
   o.eu = make_site(ub, 1, {{0, 0, 1, -std::sqrt(2.0)}});                             // st_elec_up
@@ -175,6 +189,7 @@ struct Builder {
   std::unordered_map<std::string, int> prod_id;
   std::vector<int64_t> op_touched;
   bool dedup = true;
+  bool cor_mode = false;   // correlators: keep only the cells that have tasks
 
   Builder(const tj_basis *s, const tj_basis *e, const tj_wave *w, HpsiPlan &p) : sbs(s), ebs(e), wave(w), plan(p) {}
 
@@ -804,6 +819,7 @@ struct Builder {
     plan.cells2.clear();
     plan.tasks2.clear();
     for (int c = 0; c < ncells; ++c) {
+      if (cor_mode && cell_tasks[c].empty()) continue;
       Cell cl;
       std::memset(&cl, 0, sizeof cl);
       cl.off = cell_off[c];
@@ -1174,6 +1190,411 @@ int build_hpsi_plan(const tj_lattice *lat, const tj_model *sysm, const tj_model 
   }
 }
 
+
+// ------------------------------------------------------------ correlators
+namespace {
+// A basis whose sectors are the wave's system (side 0) or environment labels,
+// each one sub-block spanning the whole sector: used when a contraction has
+// no operator on that side and the reference takes whole sector rows/columns.
+struct TrivialBasis {
+  std::vector<tj_basis_map> maps;
+  std::vector<tj_basis_sub> subs;
+  tj_basis b;
+  TrivialBasis(const tj_wave *w, int side) {
+    for (int i = 0; i < w->num; ++i) {
+      const int nu = side == 0 ? w->sub[i].sys_num_up : w->sub[i].env_num_up;
+      const int nd = side == 0 ? w->sub[i].sys_num_down : w->sub[i].env_num_down;
+      const int dim = side == 0 ? w->sub[i].sys_dim : w->sub[i].env_dim;
+      bool seen = false;
+      for (auto &m : maps)
+        if (m.new_num_up == nu && m.new_num_down == nd) seen = true;
+      if (seen) continue;
+      tj_basis_map m{0, 1, dim, nu, nd, (int32_t)subs.size()};
+      maps.push_back(m);
+      subs.push_back(tj_basis_sub{0, dim, -1000, -1000, -1000, -1000});
+    }
+    b.len = 0;
+    b.num = (int32_t)maps.size();
+    b.dim = 0;
+    b.pad_ = 0;
+    b.sub = maps.data();
+    b.maps = subs.data();
+  }
+};
+
+struct CorBuilder : Builder {
+  using Builder::Builder;
+  // measure_sys_block (measure.f90:1241-1295)
+  void measure_sys_block(const OView &A) {
+    for (int i = 0; i < wave->num; ++i) {
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m) {
+        const tj_basis_sub &q = SM(x, m);
+        const double c1 = 1.0 / std::sqrt(1.0 + q.bl_num_down);
+        const int k = A.find(q.bl_num_up, q.bl_num_down, 0, false);
+        if (k < 0) continue;
+        for (int n = 0; n < ebs->sub[y].num; ++n) emitL(cell(i, m, n), A, k, false, cell(i, m, n), c1);
+      }
+    }
+  }
+  // measure_env_block (measure.f90:1359-1414)
+  void measure_env_block(const OView &A) {
+    for (int i = 0; i < wave->num; ++i) {
+      const int x = sec_x[i], y = sec_y[i];
+      for (int n = 0; n < ebs->sub[y].num; ++n) {
+        const tj_basis_sub &q = EM(y, n);
+        const int k = A.find(q.bl_num_up, q.bl_num_down, 0, false);
+        if (k < 0) continue;
+        const double c1 = 1.0 / std::sqrt(1.0 + q.bl_num_down);
+        for (int m = 0; m < sbs->sub[x].num; ++m) emitR(cell(i, m, n), cell(i, m, n), A, k, false, c1);
+      }
+    }
+  }
+  // sys_block_env_block_cor_dia (measure.f90:1638-1732): <psi B, A psi> = <psi, A psi B^T>
+  void sbeb_dia(const OView &A, const OView &B) {
+    for (int i = 0; i < wave->num; ++i) {
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m) {
+        const tj_basis_sub &ms = SM(x, m);
+        const int ks = A.find(ms.bl_num_up, ms.bl_num_down, 0, false);
+        for (int n = 0; n < ebs->sub[y].num; ++n) {
+          const tj_basis_sub &me = EM(y, n);
+          const int ke = B.find(me.bl_num_up, me.bl_num_down, 0, false);
+          if (ks < 0 || ke < 0) continue;
+          const double c1 = 1.0 / std::sqrt((1.0 + me.bl_num_down) * (1.0 + ms.bl_num_down));
+          emit2(cell(i, m, n), A, ks, false, cell(i, m, n), B, ke, true, c1);
+        }
+      }
+    }
+  }
+  // sys_block_env_block_cor_ndia (measure.f90:5241-5480): <psi_k, c A psi_i B>
+  void sbeb_ndia(const OView &A, const OView &B, char flag) {
+    const int up = A.up_dif(), d1 = A.down_dif();
+    for (int i = 0; i < wave->num; ++i) {
+      const tj_wave_sub &w = wave->sub[i];
+      const int su = w.sys_num_up, sd = w.sys_num_down, eu = w.env_num_up, ed = w.env_num_down;
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m)
+        for (int n = 0; n < ebs->sub[y].num; ++n) {
+          const tj_basis_sub &ms = SM(x, m), &me = EM(y, n);
+          for (int dd = -d1; dd <= d1; dd += 2) {
+            const int nsb_up = ms.bl_num_up + up, nsb_dn = ms.bl_num_down + dd;
+            const int ks = A.find(ms.bl_num_up, ms.bl_num_down, dd, true);
+            for (int edd = -d1; edd <= d1; edd += 2) {
+              const int neb_up = me.bl_num_up - up, neb_dn = me.bl_num_down - edd;
+              const int ke = B.find(neb_up, neb_dn, edd, true);
+              for (int nsd = std::abs(sd - d1); nsd <= sd + d1; nsd += 2) {
+                const int nsu = su + up, neu = eu - up, ned = nsd;
+                int xk, ls, yk, le;
+                if (!find_sys(nsu, nsd, [&](const tj_basis_sub &q) {
+                      return q.bl_num_up == nsb_up && q.bl_num_down == nsb_dn && q.st_num_up == ms.st_num_up &&
+                             q.st_num_down == ms.st_num_down; }, xk, ls))
+                  continue;
+                if (!find_env(neu, ned, [&](const tj_basis_sub &q) {
+                      return q.bl_num_up == neb_up && q.bl_num_down == neb_dn && q.st_num_up == me.st_num_up &&
+                             q.st_num_down == me.st_num_down; }, yk, le))
+                  continue;
+                const int wid = find_sec(nsu, nsd, neu, ned);
+                if (ks < 0 || ke < 0 || wid < 0) continue;
+                const double signs = sgn(flag, sd + me.st_num_down);
+                const int j1 = nsd, j2 = d1, j3 = sd, j4 = ms.bl_num_down, j5 = ms.st_num_down, j6 = nsb_dn;
+                const int j11 = ned, j22 = d1, j33 = ed, j44 = me.bl_num_down, j55 = me.st_num_down, j66 = neb_dn;
+                double c1 = w6j(j1, j2, j3, j4, j5, j6);
+                if (c1 == 0.0) continue;
+                c1 = c1 * w6j(j11, j22, j33, j44, j55, j66);
+                if (c1 == 0.0) continue;
+                c1 = c1 * std::sqrt((1.0 + j11) * (1.0 + j33) / (1.0 + d1));
+                if (((j6 + j5 + j3 + j2) / 2 + (j66 + j55 + j33 + j22) / 2) % 2 == 1) c1 = -c1;
+                emit2(cell(wid, sys_index_in(wid, xk, ls), env_index_in(wid, yk, le)), A, ks, false, cell(i, m, n), B,
+                      ke, false, signs * c1);
+              }
+            }
+          }
+        }
+    }
+  }
+  // sys_block_site_cor_ndia (measure.f90:4939-5083)
+  void sb_site_ndia(const OView &A, const SiteOp &st, char flag) {
+    const int up = A.up_dif(), d1 = A.down_dif();
+    for (int i = 0; i < wave->num; ++i) {
+      const int sd = wave->sub[i].sys_num_down;
+      const int j = sec_x[i], y = sec_y[i];
+      for (int k = 0; k < sbs->sub[j].num; ++k) {
+        const tj_basis_sub &q = SM(j, k);
+        for (int dd = -d1; dd <= d1; dd += 2)
+          for (int sdd = -d1; sdd <= d1; sdd += 2) {
+            const int nbl_up = q.bl_num_up + up, nbl_dn = q.bl_num_down + dd;
+            const int nst_up = q.st_num_up - up, nst_dn = q.st_num_down - sdd;
+            const int kb = A.find(q.bl_num_up, q.bl_num_down, dd, true);
+            const int ks = site_find(st, nst_up, nst_dn, sdd, true);
+            int np = -1;
+            for (int x = 0; x < sbs->sub[j].num; ++x) {
+              const tj_basis_sub &r = SM(j, x);
+              if (r.bl_num_up == nbl_up && r.bl_num_down == nbl_dn && r.st_num_up == nst_up && r.st_num_down == nst_dn) {
+                np = x;
+                break;
+              }
+            }
+            if (kb < 0 || ks < 0 || np < 0) continue;
+            const double signs = sgn(flag, q.bl_num_down);
+            const int j1 = nbl_dn, j2 = q.bl_num_down, j3 = d1, j4 = q.st_num_down, j5 = nst_dn, j6 = sd;
+            double c1 = 1.0 / std::sqrt(1.0 + d1) * w6j(j1, j2, j3, j4, j5, j6);
+            if (c1 == 0.0) continue;
+            c1 = c1 * m1pow((j2 + j5 + j3 + j6) / 2);
+            const double coef = signs * st.val[ks] * c1;
+            for (int n = 0; n < ebs->sub[y].num; ++n) emitL(cell(i, np, n), A, kb, false, cell(i, k, n), coef);
+          }
+      }
+    }
+  }
+  // env_block_site_cor_ndia (measure.f90:5085-5238)
+  void eb_site_ndia(const OView &A, const SiteOp &st, char flag) {
+    const int up = A.up_dif(), d1 = A.down_dif();
+    for (int i = 0; i < wave->num; ++i) {
+      const int sd = wave->sub[i].sys_num_down, ed = wave->sub[i].env_num_down;
+      const int x0 = sec_x[i], j = sec_y[i];
+      for (int k = 0; k < ebs->sub[j].num; ++k) {
+        const tj_basis_sub &q = EM(j, k);
+        for (int bdd = -d1; bdd <= d1; bdd += 2) {
+          const int nbl_up = q.bl_num_up - up, nbl_dn = q.bl_num_down - bdd;
+          const int kb = A.find(nbl_up, nbl_dn, bdd, true);
+          for (int sdd = -d1; sdd <= d1; sdd += 2) {
+            const int nst_up = q.st_num_up + up, nst_dn = q.st_num_down + sdd;
+            const int ks = site_find(st, q.st_num_up, q.st_num_down, sdd, true);
+            int np = -1;
+            for (int x = 0; x < ebs->sub[j].num; ++x) {
+              const tj_basis_sub &r = EM(j, x);
+              if (r.bl_num_up == nbl_up && r.bl_num_down == nbl_dn && r.st_num_up == nst_up && r.st_num_down == nst_dn) {
+                np = x;
+                break;
+              }
+            }
+            if (kb < 0 || ks < 0 || np < 0) continue;
+            const double signs = sgn(flag, sd + q.st_num_down + sd);
+            const int j1 = nbl_dn, j2 = q.bl_num_down, j3 = d1, j4 = q.st_num_down, j5 = nst_dn, j6 = ed;
+            double c1 = 1.0 / std::sqrt(1.0 + d1) * w6j(j1, j2, j3, j4, j5, j6);
+            c1 = c1 * m1pow((j2 + j5 + j3 + j6) / 2);
+            if (c1 == 0.0) continue;
+            const double coef = signs * st.val[ks] * c1;
+            for (int m = 0; m < sbs->sub[x0].num; ++m) emitR(cell(i, m, np), cell(i, m, k), A, kb, false, coef);
+          }
+        }
+      }
+    }
+  }
+  // sys_block_env_site_cor_ndia (measure.f90:5482-5706)
+  void sb_esite_ndia(const OView &A, const SiteOp &st, char flag) {
+    const int up = A.up_dif(), d1 = A.down_dif();
+    for (int i = 0; i < wave->num; ++i) {
+      const tj_wave_sub &w = wave->sub[i];
+      const int su = w.sys_num_up, sd = w.sys_num_down, eu = w.env_num_up, ed = w.env_num_down;
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m)
+        for (int n = 0; n < ebs->sub[y].num; ++n) {
+          const tj_basis_sub &ms = SM(x, m), &me = EM(y, n);
+          for (int bdd = -d1; bdd <= d1; bdd += 2) {
+            const int nsb_up = ms.bl_num_up + up, nsb_dn = ms.bl_num_down + bdd;
+            const int kb = A.find(ms.bl_num_up, ms.bl_num_down, bdd, true);
+            for (int sdd = -st.b.down_dif; sdd <= st.b.down_dif; sdd += 2) {
+              const int nes_up = me.st_num_up - up, nes_dn = me.st_num_down - sdd;
+              const int ks = site_find(st, nes_up, nes_dn, sdd, true);
+              if (kb < 0 || ks < 0) continue;
+              for (int nsd = std::abs(sd - d1); nsd <= sd + d1; nsd += 2) {
+                const int nsu = su + up, neu = eu - up, ned = nsd;
+                int xk, ls, yk, le;
+                if (!find_sys(nsu, nsd, [&](const tj_basis_sub &q) {
+                      return q.bl_num_up == nsb_up && q.bl_num_down == nsb_dn && q.st_num_up == ms.st_num_up &&
+                             q.st_num_down == ms.st_num_down; }, xk, ls))
+                  continue;
+                if (!find_env(neu, ned, [&](const tj_basis_sub &q) {
+                      return q.st_num_up == nes_up && q.st_num_down == nes_dn && q.bl_num_down == me.bl_num_down; }, yk, le))
+                  continue;
+                const int wid = find_sec(nsu, nsd, neu, ned);
+                if (wid < 0) continue;
+                const double signs = sgn(flag, sd);
+                const int j1 = nsd, j2 = d1, j3 = sd, j4 = ms.bl_num_down, j5 = ms.st_num_down, j6 = nsb_dn;
+                const int j11 = ned, j22 = d1, j33 = ed, j44 = me.st_num_down, j55 = me.bl_num_down, j66 = nes_dn;
+                double c1 = w6j(j1, j2, j3, j4, j5, j6);
+                if (c1 == 0.0) continue;
+                c1 = c1 * w6j(j11, j22, j33, j44, j55, j66);
+                if (c1 == 0.0) continue;
+                c1 = c1 * std::sqrt((1.0 + j11) * (1.0 + j33) / (1.0 + d1));
+                if (((j6 + j5 + j3 + j2) / 2 + (j55 + j44 + j11 + j22) / 2) % 2 != 0) c1 = -c1;
+                const double coef = signs * st.val[ks] * c1;
+                emitL(cell(wid, sys_index_in(wid, xk, ls), env_index_in(wid, yk, le)), A, kb, false, cell(i, m, n), coef);
+              }
+            }
+          }
+        }
+    }
+  }
+  // sys_site_env_block_cor_ndia (measure.f90:5926-6154): <c psi_k B^T, psi_i>
+  void ssite_eb_ndia(const SiteOp &st, const OView &B, char flag) {
+    const int up = st.b.up_dif, d1 = st.b.down_dif;
+    for (int i = 0; i < wave->num; ++i) {
+      const tj_wave_sub &w = wave->sub[i];
+      const int su = w.sys_num_up, sd = w.sys_num_down, eu = w.env_num_up, ed = w.env_num_down;
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m)
+        for (int n = 0; n < ebs->sub[y].num; ++n) {
+          const tj_basis_sub &ms = SM(x, m), &me = EM(y, n);
+          for (int sdd = -d1; sdd <= d1; sdd += 2) {
+            const int nss_up = ms.st_num_up + up, nss_dn = ms.st_num_down + sdd;
+            const int ks = site_find(st, ms.st_num_up, ms.st_num_down, sdd, true);
+            for (int bdd = -B.down_dif(); bdd <= B.down_dif(); bdd += 2) {
+              const int neb_up = me.bl_num_up - up, neb_dn = me.bl_num_down - bdd;
+              const int kb = B.find(neb_up, neb_dn, bdd, true);
+              if (ks < 0 || kb < 0) continue;
+              for (int nsd = std::abs(sd - d1); nsd <= sd + d1; nsd += 2) {
+                const int nsu = su + up, neu = eu - up, ned = nsd;
+                int xk, ls, yk, le;
+                if (!find_sys(nsu, nsd, [&](const tj_basis_sub &q) {
+                      return q.st_num_up == nss_up && q.st_num_down == nss_dn && q.bl_num_down == ms.bl_num_down; }, xk, ls))
+                  continue;
+                if (!find_env(neu, ned, [&](const tj_basis_sub &q) {
+                      return q.bl_num_up == neb_up && q.bl_num_down == neb_dn && q.st_num_down == me.st_num_down; }, yk, le))
+                  continue;
+                const int wid = find_sec(nsu, nsd, neu, ned);
+                if (wid < 0) continue;
+                const double signs = sgn(flag, sd + me.st_num_down + ms.bl_num_down);
+                double coef = signs * st.val[ks];
+                if (coef == 0.0) continue;
+                const int j1 = nsd, j2 = d1, j3 = sd, j4 = ms.st_num_down, j5 = ms.bl_num_down, j6 = nss_dn;
+                const int j11 = ned, j22 = d1, j33 = ed, j44 = me.bl_num_down, j55 = me.st_num_down, j66 = neb_dn;
+                double c1 = w6j(j1, j2, j3, j4, j5, j6);
+                if (c1 == 0.0) continue;
+                c1 = c1 * w6j(j11, j22, j33, j44, j55, j66);
+                if (c1 == 0.0) continue;
+                c1 = c1 * std::sqrt((1.0 + j11) * (j33 + 1.0) / (1.0 + d1));
+                if (((j66 + j55 + j33 + j22) / 2 + (j5 + j4 + j1 + j2) / 2) % 2 != 0) c1 = -c1;
+                coef = coef * c1;
+                emitR(cell(i, m, n), cell(wid, sys_index_in(wid, xk, ls), env_index_in(wid, yk, le)), B, kb, true, coef);
+              }
+            }
+          }
+        }
+    }
+  }
+  // sys_site_env_site_cor_ndia (measure.f90:5709-5924)
+  void ssite_esite_ndia(const SiteOp &st, const SiteOp &et, char flag) {
+    const int up = st.b.up_dif, d1 = st.b.down_dif;
+    for (int i = 0; i < wave->num; ++i) {
+      const tj_wave_sub &w = wave->sub[i];
+      const int su = w.sys_num_up, sd = w.sys_num_down, eu = w.env_num_up, ed = w.env_num_down;
+      const int x = sec_x[i], y = sec_y[i];
+      for (int m = 0; m < sbs->sub[x].num; ++m)
+        for (int n = 0; n < ebs->sub[y].num; ++n) {
+          const tj_basis_sub &ms = SM(x, m), &me = EM(y, n);
+          for (int sdd1 = -d1; sdd1 <= d1; sdd1 += 2) {
+            const int nss_up = ms.st_num_up + up, nss_dn = ms.st_num_down + sdd1;
+            const int ks = site_find(st, ms.st_num_up, ms.st_num_down, sdd1, true);
+            for (int sdd2 = -d1; sdd2 <= d1; sdd2 += 2) {
+              const int nes_up = me.st_num_up - up, nes_dn = me.st_num_down - sdd2;
+              const int ke = site_find(et, nes_up, nes_dn, sdd2, true);
+              if (ks < 0 || ke < 0) continue;
+              for (int nsd = std::abs(sd - d1); nsd <= sd + d1; nsd += 2) {
+                const int nsu = su + up, neu = eu - up, ned = nsd;
+                int xk, ls, yk, le;
+                if (!find_sys(nsu, nsd, [&](const tj_basis_sub &q) {
+                      return q.st_num_up == nss_up && q.st_num_down == nss_dn && q.bl_num_down == ms.bl_num_down; }, xk, ls))
+                  continue;
+                if (!find_env(neu, ned, [&](const tj_basis_sub &q) {
+                      return q.st_num_up == nes_up && q.st_num_down == nes_dn && q.bl_num_down == me.bl_num_down; }, yk, le))
+                  continue;
+                const int wid = find_sec(nsu, nsd, neu, ned);
+                if (wid < 0) continue;
+                const double signs = sgn(flag, sd + ms.bl_num_down);
+                double coef = signs * st.val[ks] * et.val[ke];
+                if (coef == 0.0) continue;
+                const int j1 = nsd, j2 = d1, j3 = sd, j4 = ms.st_num_down, j5 = ms.bl_num_down, j6 = nss_dn;
+                const int j11 = ned, j22 = d1, j33 = ed, j44 = me.st_num_down, j55 = me.bl_num_down, j66 = nes_dn;
+                double c1 = w6j(j1, j2, j3, j4, j5, j6);
+                if (c1 == 0.0) continue;
+                c1 = c1 * w6j(j11, j22, j33, j44, j55, j66);
+                if (c1 == 0.0) continue;
+                c1 = c1 * std::sqrt((1.0 + j11) * (1.0 + j33) / (1.0 + d1));
+                if (((j55 + j44 + j11 + j22) / 2 + (j5 + j4 + j1 + j2) / 2) % 2 != 0) c1 = -c1;
+                coef = coef * c1;
+                emitAxpy(cell(i, m, n), cell(wid, sys_index_in(wid, xk, ls), env_index_in(wid, yk, le)), coef);
+              }
+            }
+          }
+        }
+    }
+  }
+};
+}  // namespace
+
+int build_cor_plan(CorKind kind, const tj_block *a, const tj_block *b, const tj_basis *sys_bs,
+                   const tj_basis *env_bs, const tj_wave *wave, char flag, HpsiPlan &plan, std::string &msg) {
+  try {
+    if (!a || !wave || wave->num < 0 || (wave->num > 0 && !wave->sub)) throw PlanError(TJ_ERR_ARG, "null argument");
+    if (flag != 'B' && flag != 'F') throw PlanError(TJ_ERR_ARG, "flag must be 'B' or 'F'");
+    plan = HpsiPlan();
+    TrivialBasis ts(wave, 0), te(wave, 1);
+    const tj_basis *sb = sys_bs ? sys_bs : &ts.b, *eb = env_bs ? env_bs : &te.b;
+    CorBuilder B(sb, eb, wave, plan);
+    B.cor_mode = true;
+    B.init_cells();
+    plan.psi_len = wave->dim;
+    OBlk ba, bb;
+    switch (kind) {
+      case COR_MEASURE_SYS_BLOCK:
+        load_block(*a, ba, plan);
+        B.measure_sys_block(OView{&ba, false});
+        break;
+      case COR_MEASURE_ENV_BLOCK:
+        load_block(*a, ba, plan);
+        B.measure_env_block(OView{&ba, false});
+        break;
+      case COR_SBEB_DIA:
+        if (!b) throw PlanError(TJ_ERR_ARG, "null operator");
+        load_block(*a, ba, plan);
+        load_block(*b, bb, plan);
+        B.sbeb_dia(OView{&ba, false}, OView{&bb, false});
+        break;
+      case COR_SBEB_NDIA:
+        if (!b) throw PlanError(TJ_ERR_ARG, "null operator");
+        load_block(*a, ba, plan);
+        load_block(*b, bb, plan);
+        B.sbeb_ndia(OView{&ba, false}, OView{&bb, false}, flag);
+        break;
+      case COR_SB_SITE_NDIA:
+        if (!b) throw PlanError(TJ_ERR_ARG, "null operator");
+        load_block(*a, ba, plan);
+        B.sb_site_ndia(OView{&ba, false}, site_from_block(*b), flag);
+        break;
+      case COR_EB_SITE_NDIA:
+        if (!b) throw PlanError(TJ_ERR_ARG, "null operator");
+        load_block(*a, ba, plan);
+        B.eb_site_ndia(OView{&ba, false}, site_from_block(*b), flag);
+        break;
+      case COR_SB_ESITE_NDIA:
+        if (!b) throw PlanError(TJ_ERR_ARG, "null operator");
+        load_block(*a, ba, plan);
+        B.sb_esite_ndia(OView{&ba, false}, site_from_block(*b), flag);
+        break;
+      case COR_SSITE_EB_NDIA:
+        if (!b) throw PlanError(TJ_ERR_ARG, "null operator");
+        load_block(*b, bb, plan);
+        B.ssite_eb_ndia(site_from_block(*a), OView{&bb, false}, flag);
+        break;
+      case COR_SSITE_ESITE_NDIA:
+        if (!b) throw PlanError(TJ_ERR_ARG, "null operator");
+        B.ssite_esite_ndia(site_from_block(*a), site_from_block(*b), flag);
+        break;
+    }
+    B.finalize();
+    return TJ_OK;
+  } catch (const PlanError &e) {
+    msg = e.what();
+    return e.code;
+  } catch (const std::exception &e) {
+    msg = e.what();
+    return TJ_ERR_ARG;
+  }
+}
+
 static_assert(sizeof(Task) == sizeof(tj_plan_task), "task layout");
 static_assert(sizeof(Cell) == sizeof(tj_plan_cell), "cell layout");
 static_assert(sizeof(HpsiPlan::Upload) == sizeof(tj_plan_upload), "upload layout");
@@ -1181,14 +1602,7 @@ static_assert(sizeof(HpsiPlan::Merge) == sizeof(tj_plan_merge), "merge layout");
 
 }  // namespace tjb
 
-extern "C" int tj_hpsi_plan_export(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
-                                   const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave,
-                                   tj_plan_export *out) {
-  if (!out) return tjb_set_err(TJ_ERR_ARG, "null output");
-  tjb::HpsiPlan P;
-  std::string msg;
-  int rc = tjb::build_hpsi_plan(lat, sys, env, sys_bs, env_bs, wave, P, msg);
-  if (rc) return tjb_set_err(rc, "H*psi plan: " + msg);
+static int export_plan(tjb::HpsiPlan &P, tj_plan_export *out) {
   out->ops_len = P.ops_len;
   out->scratch_len = P.scratch_len;
   out->psi_len = P.psi_len;
@@ -1202,7 +1616,7 @@ extern "C" int tj_hpsi_plan_export(const tj_lattice *lat, const tj_model *sys, c
   out->flops = P.flops;
   out->flops_ref = P.flops_ref;
   out->bytes = P.bytes;
-  auto cp = [](void *dst, const void *src, size_t n) { if (dst && n) std::memcpy(dst, src, n); };
+  auto cp = [](void *dst, const void *src, size_t n) { if (dst && src && n) std::memcpy(dst, src, n); };
   cp(out->tasks1, P.tasks1.data(), P.tasks1.size() * sizeof(tjb::Task));
   cp(out->tasks2, P.tasks2.data(), P.tasks2.size() * sizeof(tjb::Task));
   cp(out->cells1, P.cells1.data(), P.cells1.size() * sizeof(tjb::Cell));
@@ -1212,4 +1626,26 @@ extern "C" int tj_hpsi_plan_export(const tj_lattice *lat, const tj_model *sys, c
   cp(out->merge_src, P.merge_src.data(), P.merge_src.size() * sizeof(int64_t));
   cp(out->merge_coef, P.merge_coef.data(), P.merge_coef.size() * sizeof(double));
   return TJ_OK;
+}
+
+extern "C" int tj_hpsi_plan_export(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
+                                   const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave,
+                                   tj_plan_export *out) {
+  if (!out) return tjb_set_err(TJ_ERR_ARG, "null output");
+  tjb::HpsiPlan P;
+  std::string msg;
+  int rc = tjb::build_hpsi_plan(lat, sys, env, sys_bs, env_bs, wave, P, msg);
+  if (rc) return tjb_set_err(rc, "H*psi plan: " + msg);
+  return export_plan(P, out);
+}
+
+extern "C" int tj_cor_plan_export(int kind, const tj_block *a, const tj_block *b, const tj_basis *sys_bs,
+                                  const tj_basis *env_bs, const tj_wave *wave, char flag, tj_plan_export *out) {
+  if (!out) return tjb_set_err(TJ_ERR_ARG, "null output");
+  if (kind < 0 || kind > (int)tjb::COR_SSITE_ESITE_NDIA) return tjb_set_err(TJ_ERR_ARG, "unknown correlator kind");
+  tjb::HpsiPlan P;
+  std::string msg;
+  int rc = tjb::build_cor_plan((tjb::CorKind)kind, a, b, sys_bs, env_bs, wave, flag, P, msg);
+  if (rc) return tjb_set_err(rc, "correlator plan: " + msg);
+  return export_plan(P, out);
 }

@@ -119,6 +119,8 @@ def lib():
         L.tj_hpsi_stats_get.argtypes = [C.c_void_p, P(TjHpsiStats)]
         L.tj_hpsi_plan_export.argtypes = [P(TjLattice), P(TjModel), P(TjModel), P(TjBasis), P(TjBasis),
                                           P(TjWave), P(PlanExport)]
+        L.tj_cor_plan_export.argtypes = [C.c_int, P(TjBlock), P(TjBlock), P(TjBasis), P(TjBasis), P(TjWave),
+                                         C.c_char, P(PlanExport)]
         for n in ("tj_measure_sys_block", "tj_measure_env_block"):
             getattr(L, n).argtypes = [C.c_void_p, P(TjBlock), P(TjBasis), P(TjWave), P(C.c_double)]
         L.tj_sys_block_env_block_cor_dia.argtypes = [C.c_void_p, P(TjBlock), P(TjBlock), P(TjBasis),
@@ -236,14 +238,9 @@ class Context:
         return v.value
 
 
-def plan_export(sb, invec: Optional[Wave] = None) -> dict:
-    """Compiled task lists of H*psi for `sb` (no GPU needed)."""
-    L = lib()
-    invec = sb.wave if invec is None else invec
-    ps, pe, bs, be = sb.sys.pack(), sb.env.pack(), sb.sys_bs.pack(), sb.env_bs.pack()
+def _export(call) -> dict:
     ex = PlanExport()
-    args = (C.byref(sb.lat.c), C.byref(ps.c), C.byref(pe.c), C.byref(bs.c), C.byref(be.c), C.byref(invec.c))
-    _chk(L.tj_hpsi_plan_export(*args, C.byref(ex)))
+    _chk(call(C.byref(ex)))
     arrs = {
         "tasks1": (PlanTask * max(ex.n_tasks1, 1))(), "tasks2": (PlanTask * max(ex.n_tasks2, 1))(),
         "cells1": (PlanCell * max(ex.n_cells1, 1))(), "cells2": (PlanCell * max(ex.n_cells2, 1))(),
@@ -252,11 +249,32 @@ def plan_export(sb, invec: Optional[Wave] = None) -> dict:
     }
     for k, a in arrs.items():
         setattr(ex, k, C.cast(a, type(getattr(ex, k))))
-    _chk(L.tj_hpsi_plan_export(*args, C.byref(ex)))
-    # copy the operator data now, while the packed buffers are alive
+    _chk(call(C.byref(ex)))
+    # copy the operator data now, while the caller's packed buffers are alive
     ops = np.zeros(max(ex.ops_len, 1))
     for i in range(ex.n_uploads):
         u = arrs["uploads"][i]
         src = np.ctypeslib.as_array(C.cast(u.src, C.POINTER(C.c_double)), shape=(u.n,))
         ops[u.dst:u.dst + u.n] = src
     return {"ex": ex, "ops": ops, **arrs}
+
+
+def plan_export(sb, invec: Optional[Wave] = None) -> dict:
+    """Compiled task lists of H*psi for `sb` (no GPU needed)."""
+    L = lib()
+    invec = sb.wave if invec is None else invec
+    ps, pe, bs, be = sb.sys.pack(), sb.env.pack(), sb.sys_bs.pack(), sb.env_bs.pack()
+    return _export(lambda ex: L.tj_hpsi_plan_export(C.byref(sb.lat.c), C.byref(ps.c), C.byref(pe.c), C.byref(bs.c),
+                                                     C.byref(be.c), C.byref(invec.c), ex))
+
+
+def cor_plan_export(name: str, a: Block, b: Optional[Block], sys_bs, env_bs, wave: Wave, flag: str = "B") -> dict:
+    """Compiled task lists of the correlator contraction `name` (no GPU needed)."""
+    L = lib()
+    pa = a.pack()
+    pb = b.pack() if b is not None else None
+    ps = sys_bs.pack() if sys_bs is not None else None
+    pe = env_bs.pack() if env_bs is not None else None
+    ref = lambda p: C.byref(p.c) if p is not None else None
+    return _export(lambda ex: L.tj_cor_plan_export(COR_NAMES[name], ref(pa), ref(pb), ref(ps), ref(pe),
+                                                    C.byref(wave.c), flag.encode(), ex))

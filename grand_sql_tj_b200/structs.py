@@ -291,6 +291,13 @@ class Lattice:
                            _dptr(self.jz), _dptr(self.jd), _dptr(self.jn), _dptr(self.esite))
 
 
+def block_transfer_trans(b: Block) -> Block:
+    """block_transfer_trans (block.f90:1676-1706): the transposed operator."""
+    subs = [SubBlock(s.num_up + b.up_dif, s.num_down + s.down_dif, -s.down_dif, np.asfortranarray(s.mat.T))
+            for s in b.subs]
+    return Block(b.len, -b.up_dif, b.down_dif, subs)
+
+
 def block_from_c_result(res: TjTruncResult, length: int) -> Block:
     """Turns a filled tj_trunc_result into a Block (trun_op)."""
     subs = []

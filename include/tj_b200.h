@@ -287,6 +287,13 @@ typedef struct tj_plan_export {
 int tj_hpsi_plan_export(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
                         const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave,
                         tj_plan_export *out);
+/* The same for one correlator contraction: kind 0..8 in the order of the
+ * tj_measure_* / tj_*_cor_* declarations above (measure_sys_block = 0, ...,
+ * sys_site_env_site_cor_ndia = 8); the epilogue dots every phase-2 cell with
+ * psi, so value = sum over cells <psi_cell, Y_cell>.  Arguments as in the
+ * matching entry point (NULL for a basis or operator it does not take). */
+int tj_cor_plan_export(int kind, const tj_block *a, const tj_block *b, const tj_basis *sys_bs,
+                       const tj_basis *env_bs, const tj_wave *wave, char flag, tj_plan_export *out);
 
 #ifdef __cplusplus
 }
