@@ -197,8 +197,10 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   }
   if ((rc = upload_vec(ctx, ctx->cells1, P->cells1)) || (rc = upload_vec(ctx, ctx->cells2, P->cells2)) ||
       (rc = upload_vec(ctx, ctx->tasks1, P->tasks1)) || (rc = upload_vec(ctx, ctx->tasks2, P->tasks2)) ||
-      (rc = upload_vec(ctx, ctx->tiles1, P->tiles1)) || (rc = upload_vec(ctx, ctx->tiles2, P->tiles2)))
+      (rc = upload_vec(ctx, ctx->tiles1, P->tiles1)) || (rc = upload_vec(ctx, ctx->tiles2, P->tiles2)) ||
+      (rc = upload_vec(ctx, ctx->red1, P->red1)) || (rc = upload_vec(ctx, ctx->red2, P->red2)))
     return rc;
+  if ((rc = ctx->slots.reserve(sizeof(double) * (std::max(P->nslots1, P->nslots2) * BM * BN + 4)))) return rc;
   if ((rc = ctx->scr.reserve(sizeof(double) * (P->scratch_len + 4)))) return rc;
   if ((rc = ctx->counters.reserve(64))) return rc;
   if ((rc = ctx->partials.reserve(sizeof(double) * (std::max(P->tiles2.size(), P->tiles1.size()) + 4096))))
@@ -236,7 +238,9 @@ int tjb::run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed) {
   g.tiles = (const Tile *)ctx->tiles1.p;
   g.ntiles = (int)P.tiles1.size();
   g.counter = cnt;
+  g.slots = ctx->slots.d();
   launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles), ctx->stream);
+  launch_reduce(g, (const Reduce *)ctx->red1.p, (int)P.red1.size(), ctx->stream);
   if (timed) CK(cudaEventRecord(ctx->ev[1], ctx->stream));
   g.out = out;
   g.cells = (const Cell *)ctx->cells2.p;
@@ -245,6 +249,7 @@ int tjb::run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed) {
   g.ntiles = (int)P.tiles2.size();
   g.counter = cnt + 1;
   launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles), ctx->stream);
+  launch_reduce(g, (const Reduce *)ctx->red2.p, (int)P.red2.size(), ctx->stream);
   if (timed) CK(cudaEventRecord(ctx->ev[2], ctx->stream));
   CK(cudaGetLastError());
   ++ctx->n_hpsi;

@@ -44,14 +44,14 @@ struct tj_ctx {
   double stats_lanczos_ms = 0;
   // device buffers
   tjb::DevBuf ops, scr, vin, vout, counters, partials;
-  tjb::DevBuf cells1, cells2, tasks1, tasks2, tiles1, tiles2;
+  tjb::DevBuf cells1, cells2, tasks1, tasks2, tiles1, tiles2, red1, red2, slots;
   tjb::DevBuf m_dst, m_n, m_sb, m_se, m_src, m_coef;
   tjb::DevBuf lanV, lanScal, lanPart;
   tjb::DevBuf trA, trB, trC, trD, trE;          // truncation
   tjb::DevBuf corCells, corTasks, corTiles, corOps, corScr, corPsi;   // correlators
   std::vector<tjb::DevBuf *> all_bufs() {
     return {&ops, &scr, &vin, &vout, &counters, &partials, &cells1, &cells2, &tasks1, &tasks2, &tiles1,
-            &tiles2, &m_dst, &m_n, &m_sb, &m_se, &m_src, &m_coef, &lanV, &lanScal, &lanPart, &trA, &trB,
+            &tiles2, &red1, &red2, &slots, &m_dst, &m_n, &m_sb, &m_se, &m_src, &m_coef, &lanV, &lanScal, &lanPart, &trA, &trB,
             &trC, &trD, &trE, &corCells, &corTasks, &corTiles, &corOps, &corScr, &corPsi};
   }
   ~tj_ctx();

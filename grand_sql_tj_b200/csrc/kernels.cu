@@ -55,10 +55,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 4) grouped_gemm_f64(GemmParams p
 #pragma unroll
       for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-    int ti = c.t_begin;
-    for (; ti < c.t_end; ++ti) {
+    for (int ti = tl.tb; ti < tl.te; ++ti) {
       const Task tk = p.tasks[ti];
-      if (tk.R.space == SP_NONE) break;   // axpy tasks come last
       const double *__restrict__ Lb = space_base(p, tk.L.space) + tk.L.off;
       const double *__restrict__ Rb = space_base(p, tk.R.space) + tk.R.off;
       const int ldl = tk.L.ld, ldr = tk.R.ld, K = tk.K;
@@ -134,15 +132,17 @@ __global__ void __launch_bounds__(GEMM_THREADS, 4) grouped_gemm_f64(GemmParams p
           const int n = tl.col0 + wc * 32 + ni * 8 + 2 * (lane & 3) + e;
           if (r < c.M && n < c.N) {
             double v = acc[mi][ni][e];
-            for (int tj = ti; tj < c.t_end; ++tj) {
+            for (int tj = tl.ab; tj < tl.ae; ++tj) {
               const Task &ax = p.tasks[tj];
               v += ax.coef * space_base(p, ax.L.space)[ax.L.off + (int64_t)n * ax.L.ld + r];
             }
             const int64_t o = c.off + (int64_t)n * c.ld + r;
             if (p.dot_mode)
               local += v * p.dot_with[o];
-            else
+            else if (tl.slot < 0)
               p.out[o] = v;
+            else
+              p.slots[(int64_t)tl.slot * (BM * BN) + (n - tl.col0) * BM + (r - tl.row0)] = v;
           }
         }
     if (p.dot_mode) {
@@ -171,6 +171,29 @@ int grouped_gemm_grid(int ntiles) {
 void launch_grouped_gemm(const GemmParams &p, int grid, cudaStream_t s) {
   if (p.ntiles <= 0) return;
   grouped_gemm_f64<<<grid, GEMM_THREADS, 0, s>>>(p);
+}
+
+// One CTA per split tile: the slots are added in slot order, so the result
+// does not depend on which items finished first.
+__global__ void reduce_slots_kernel(GemmParams p, const Reduce *red) {
+  const Reduce rd = red[blockIdx.x];
+  const Cell c = p.cells[rd.cell];
+  const int rows = min(BM, c.M - rd.row0), cols = min(BN, c.N - rd.col0);
+  for (int idx = threadIdx.x; idx < rows * cols; idx += blockDim.x) {
+    const int r = idx % rows, n = idx / rows;
+    double v = 0.0;
+    for (int k = 0; k < rd.nslot; ++k) v += p.slots[(int64_t)(rd.slot0 + k) * (BM * BN) + n * BM + r];
+    const int gr = rd.row0 + r, gn = rd.col0 + n;
+    for (int tj = rd.ab; tj < rd.ae; ++tj) {
+      const Task &ax = p.tasks[tj];
+      v += ax.coef * space_base(p, ax.L.space)[ax.L.off + (int64_t)gn * ax.L.ld + gr];
+    }
+    p.out[c.off + (int64_t)gn * c.ld + gr] = v;
+  }
+}
+
+void launch_reduce(const GemmParams &p, const Reduce *red, int nred, cudaStream_t s) {
+  if (nred > 0) reduce_slots_kernel<<<nred, 256, 0, s>>>(p, red);
 }
 
 // ------------------------------------------------------------------ merges

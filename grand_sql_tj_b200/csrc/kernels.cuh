@@ -17,12 +17,15 @@ struct GemmParams {
   const Tile *tiles;
   int ntiles;
   unsigned int *counter;   // dynamic tile counter (zeroed before launch)
-  double *partials;        // dot mode: one partial sum per tile
+  double *partials;        // dot mode: one partial sum per work item
+  double *slots;           // partial tiles of split cells, BM*BN doubles per slot
   const double *dot_with;  // dot mode: vector the result is dotted with (same layout as out)
   int dot_mode;            // 0: store the tile, 1: write <dot_with, tile> to partials[tile]
 };
 
 void launch_grouped_gemm(const GemmParams &p, int grid, cudaStream_t s);
+// out tile = sum of its partial slots (in slot order) + its axpy tasks
+void launch_reduce(const GemmParams &p, const Reduce *red, int nred, cudaStream_t s);
 int grouped_gemm_grid(int ntiles);
 
 // merged operators: dst[e] = sum_j coef_j * src_j[e]

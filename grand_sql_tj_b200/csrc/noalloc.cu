@@ -120,17 +120,19 @@ extern "C" int tj_model_wave_noalloc(const tj_lattice *lat, const tj_model *sys,
   }
   for (int64_t &x : msrc) x = remap(x);
 
-  // scratch layout: merged operators | phase-1 products | work lists | counters
+  // scratch layout: merged operators | phase-1 products | partial tiles | work lists | counters
   int64_t cursor = up256(P.ops_len - merged0);
   const int64_t prod_off = cursor;
   cursor += up256(P.scratch_len);
+  const int64_t slot_off = cursor;
+  cursor += up256(std::max(P.nslots1, P.nslots2) * BM * BN);
   int64_t need = cursor;
   {
     auto b = [](size_t n, size_t sz) { return up256((int64_t)((n * sz + 7) / 8)); };
     need += b(P.cells1.size(), sizeof(Cell)) + b(P.cells2.size(), sizeof(Cell)) + b(P.tasks1.size(), sizeof(Task)) +
             b(P.tasks2.size(), sizeof(Task)) + b(P.tiles1.size(), sizeof(Tile)) + b(P.tiles2.size(), sizeof(Tile)) +
             b(mdst.size(), 8) + b(mn.size(), 8) + b(msb.size(), 4) + b(mse.size(), 4) + b(msrc.size(), 8) +
-            b(P.merge_coef.size(), 8) + 32;
+            b(P.merge_coef.size(), 8) + b(P.red1.size(), sizeof(Reduce)) + b(P.red2.size(), sizeof(Reduce)) + 32;
   }
   if (need > (int64_t)kScratchDoubles) {
     char b[256];
@@ -143,6 +145,7 @@ extern "C" int tj_model_wave_noalloc(const tj_lattice *lat, const tj_model *sys,
   Cell *c1, *c2;
   Task *t1, *t2;
   Tile *l1, *l2;
+  Reduce *r1, *r2;
   int64_t *d_mdst, *d_mn, *d_msrc;
   int32_t *d_msb, *d_mse;
   double *d_mcoef;
@@ -151,7 +154,8 @@ extern "C" int tj_model_wave_noalloc(const tj_lattice *lat, const tj_model *sys,
       (rc = put(s, base, cursor, P.tiles1, &l1)) || (rc = put(s, base, cursor, P.tiles2, &l2)) ||
       (rc = put(s, base, cursor, mdst, &d_mdst)) || (rc = put(s, base, cursor, mn, &d_mn)) ||
       (rc = put(s, base, cursor, msb, &d_msb)) || (rc = put(s, base, cursor, mse, &d_mse)) ||
-      (rc = put(s, base, cursor, msrc, &d_msrc)) || (rc = put(s, base, cursor, P.merge_coef, &d_mcoef)))
+      (rc = put(s, base, cursor, msrc, &d_msrc)) || (rc = put(s, base, cursor, P.merge_coef, &d_mcoef)) ||
+      (rc = put(s, base, cursor, P.red1, &r1)) || (rc = put(s, base, cursor, P.red2, &r2)))
     return rc;
   // the tile counters must start at zero on every call
   unsigned int *cnt = (unsigned int *)(base + cursor);
@@ -170,7 +174,9 @@ extern "C" int tj_model_wave_noalloc(const tj_lattice *lat, const tj_model *sys,
   g.tiles = l1;
   g.ntiles = (int)P.tiles1.size();
   g.counter = cnt;
+  g.slots = base + slot_off;
   launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles), s);
+  launch_reduce(g, r1, (int)P.red1.size(), s);
   g.out = outvec->data;
   g.cells = c2;
   g.tasks = t2;
@@ -178,6 +184,7 @@ extern "C" int tj_model_wave_noalloc(const tj_lattice *lat, const tj_model *sys,
   g.ntiles = (int)P.tiles2.size();
   g.counter = cnt + 1;
   launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles), s);
+  launch_reduce(g, r2, (int)P.red2.size(), s);
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return set_err(TJ_ERR_CUDA, std::string("tj_model_wave_noalloc: ") + cudaGetErrorString(e));

@@ -173,6 +173,81 @@ static inline double sgn(char flag, int n) {
 }
 static inline double m1pow(int n) { return (n % 2) ? -1.0 : 1.0; }
 
+}  // namespace
+
+// Work items of one grouped-GEMM pass.  Every BM x BN tile of every cell
+// becomes one or more items; a tile whose tasks carry more than `chunk`
+// inner-dimension steps is cut at task boundaries into several items whose
+// partial tiles a Reduce record adds up (dot mode needs no reduction: the
+// partial dot products are simply summed).  Items are ordered by decreasing
+// work so that the dynamic scheduler finishes with the small ones.
+void split_tiles(const std::vector<Cell> &cells, const std::vector<Task> &tasks, std::vector<Tile> &tiles,
+                 std::vector<Reduce> &red, int64_t &nslots, bool dot_mode) {
+  tiles.clear();
+  red.clear();
+  nslots = 0;
+  double total = 0;
+  int64_t ntile = 0;
+  for (const Cell &c : cells) {
+    double k = 0;
+    for (int t = c.t_begin; t < c.t_end; ++t) k += tasks[t].K;
+    const int64_t nt = (int64_t)((c.M + BM - 1) / BM) * ((c.N + BN - 1) / BN);
+    total += k * nt;
+    ntile += nt;
+  }
+  // aim at ~6 items per resident CTA (148 SMs x 4), never below 256 k-steps per item
+  const double target = std::max(256.0, total / (148.0 * 4 * 6));
+  std::vector<std::pair<double, Tile>> w;
+  for (int ci = 0; ci < (int)cells.size(); ++ci) {
+    const Cell &c = cells[ci];
+    int gb = c.t_begin, ge = c.t_begin;   // GEMM tasks [gb, ge), axpys [ge, t_end)
+    while (ge < c.t_end && tasks[ge].R.space != SP_NONE) ++ge;
+    std::vector<std::pair<int, int>> chunks;
+    double acc = 0;
+    int start = gb;
+    for (int t = gb; t < ge; ++t) {
+      acc += tasks[t].K;
+      if (acc >= target && t + 1 < ge) {
+        chunks.push_back({start, t + 1});
+        start = t + 1;
+        acc = 0;
+      }
+    }
+    chunks.push_back({start, ge});
+    const bool split = chunks.size() > 1 && !dot_mode;
+    for (int r = 0; r < c.M; r += BM)
+      for (int q = 0; q < c.N; q += BN) {
+        int slot0 = -1;
+        if (split) {
+          slot0 = (int)nslots;
+          nslots += (int64_t)chunks.size();
+          red.push_back(Reduce{ci, r, q, slot0, (int)chunks.size(), ge, c.t_end, 0});
+        }
+        for (size_t k = 0; k < chunks.size(); ++k) {
+          double kw = 1;
+          for (int t = chunks[k].first; t < chunks[k].second; ++t) kw += tasks[t].K;
+          Tile t;
+          t.cell = ci;
+          t.row0 = r;
+          t.col0 = q;
+          t.tb = chunks[k].first;
+          t.te = chunks[k].second;
+          // axpys: by the single owner, or (dot mode) by the first chunk; split tiles get them in the Reduce
+          t.ab = ge;
+          t.ae = (!split && k == 0) ? c.t_end : ge;
+          t.slot = split ? slot0 + (int)k : -1;
+          w.push_back({kw, t});
+        }
+      }
+  }
+  std::stable_sort(w.begin(), w.end(), [](const std::pair<double, Tile> &a, const std::pair<double, Tile> &b) {
+    return a.first > b.first;
+  });
+  for (auto &p : w) tiles.push_back(p.second);
+}
+
+namespace {
+
 // ------------------------------------------------------------------ builder
 struct Builder {
   const tj_basis *sbs, *ebs;
@@ -836,26 +911,12 @@ struct Builder {
       cl.t_end = (int)plan.tasks2.size();
       plan.cells2.push_back(cl);
     }
-    auto make_tiles = [](const std::vector<Cell> &cells, const std::vector<Task> &tasks, std::vector<Tile> &tiles) {
-      std::vector<std::pair<double, Tile>> w;
-      for (int c = 0; c < (int)cells.size(); ++c) {
-        const Cell &cl = cells[c];
-        double k = 0;
-        for (int t = cl.t_begin; t < cl.t_end; ++t) k += tasks[t].K + 1;
-        for (int r = 0; r < cl.M; r += BM)
-          for (int q = 0; q < cl.N; q += BN) {
-            Tile t{c, r, q, 0};
-            w.push_back({k, t});
-          }
-      }
-      std::stable_sort(w.begin(), w.end(), [](const std::pair<double, Tile> &a, const std::pair<double, Tile> &b) {
-        return a.first > b.first;
-      });
-      tiles.clear();
-      for (auto &p : w) tiles.push_back(p.second);
+    auto make_tiles = [&](const std::vector<Cell> &cells, const std::vector<Task> &tasks,
+                          std::vector<Tile> &tiles, std::vector<Reduce> &red, int64_t &nslots) {
+      split_tiles(cells, tasks, tiles, red, nslots, cor_mode);
     };
-    make_tiles(plan.cells1, plan.tasks1, plan.tiles1);
-    make_tiles(plan.cells2, plan.tasks2, plan.tiles2);
+    make_tiles(plan.cells1, plan.tasks1, plan.tiles1, plan.red1, plan.nslots1);
+    make_tiles(plan.cells2, plan.tasks2, plan.tiles2, plan.red2, plan.nslots2);
     std::sort(op_touched.begin(), op_touched.end());
     op_touched.erase(std::unique(op_touched.begin(), op_touched.end()), op_touched.end());
   }
@@ -1599,6 +1660,8 @@ static_assert(sizeof(Task) == sizeof(tj_plan_task), "task layout");
 static_assert(sizeof(Cell) == sizeof(tj_plan_cell), "cell layout");
 static_assert(sizeof(HpsiPlan::Upload) == sizeof(tj_plan_upload), "upload layout");
 static_assert(sizeof(HpsiPlan::Merge) == sizeof(tj_plan_merge), "merge layout");
+static_assert(sizeof(Tile) == sizeof(tj_plan_item), "item layout");
+static_assert(sizeof(Reduce) == sizeof(tj_plan_reduce), "reduce layout");
 
 }  // namespace tjb
 
@@ -1625,6 +1688,14 @@ static int export_plan(tjb::HpsiPlan &P, tj_plan_export *out) {
   cp(out->merges, P.merges.data(), P.merges.size() * sizeof(tjb::HpsiPlan::Merge));
   cp(out->merge_src, P.merge_src.data(), P.merge_src.size() * sizeof(int64_t));
   cp(out->merge_coef, P.merge_coef.data(), P.merge_coef.size() * sizeof(double));
+  out->n_items1 = (int64_t)P.tiles1.size();
+  out->n_items2 = (int64_t)P.tiles2.size();
+  out->n_red1 = (int64_t)P.red1.size();
+  out->n_red2 = (int64_t)P.red2.size();
+  cp(out->items1, P.tiles1.data(), P.tiles1.size() * sizeof(tjb::Tile));
+  cp(out->items2, P.tiles2.data(), P.tiles2.size() * sizeof(tjb::Tile));
+  cp(out->red1, P.red1.data(), P.red1.size() * sizeof(tjb::Reduce));
+  cp(out->red2, P.red2.data(), P.red2.size() * sizeof(tjb::Reduce));
   return TJ_OK;
 }
 

@@ -49,9 +49,19 @@ struct Cell {
   int8_t pad[7];
 };
 
-// One CTA work item: a BM x BN tile of a cell.
+// One CTA work item: a BM x BN tile of a cell and a contiguous range of the
+// cell's GEMM tasks [tb, te).  The axpy tasks [ab, ae) are applied by the
+// item that finishes the tile.  slot < 0: the item owns the whole tile and
+// writes it; slot >= 0: the item writes a partial tile to partial slot
+// `slot` and a Reduce record sums the slots of the tile in a fixed order.
 struct Tile {
-  int32_t cell, row0, col0, pad;
+  int32_t cell, row0, col0, tb, te, ab, ae, slot;
+};
+
+// Sums the partial slots [slot0, slot0 + nslot) of one tile, adds its axpy
+// tasks and stores it.
+struct Reduce {
+  int32_t cell, row0, col0, slot0, nslot, ab, ae, pad;
 };
 
 // The compiled H*psi of one superblock.
@@ -69,6 +79,8 @@ struct HpsiPlan {
   std::vector<Task> tasks1, tasks2;
   std::vector<Cell> cells1, cells2;
   std::vector<Tile> tiles1, tiles2;
+  std::vector<Reduce> red1, red2;
+  int64_t nslots1 = 0, nslots2 = 0;          // partial tiles of split cells
   int64_t scratch_len = 0;                   // doubles of phase-1 products
   int64_t psi_len = 0;
 
@@ -79,6 +91,10 @@ struct HpsiPlan {
 
 // Tile shape of the grouped FP64 kernel.
 constexpr int BM = 64, BN = 64, BK = 16;
+
+// Work items (and Reduce records) of one grouped-GEMM pass over `cells`.
+void split_tiles(const std::vector<Cell> &cells, const std::vector<Task> &tasks, std::vector<Tile> &tiles,
+                 std::vector<Reduce> &red, int64_t &nslots, bool dot_mode);
 
 // Builds the plan (host).  Returns TJ_OK or an error code with msg set.
 int build_hpsi_plan(const tj_lattice *lat, const tj_model *sys, const tj_model *env,

@@ -257,7 +257,7 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       const int ci = (int)cells.size();
       cells.push_back(c);
       for (int r0 = 0; r0 < n; r0 += BM)
-        for (int c0 = 0; c0 < n; c0 += BN) tiles.push_back(Tile{ci, r0, c0, 0});
+        for (int c0 = 0; c0 < n; c0 += BN) tiles.push_back(Tile{ci, r0, c0, c.t_begin, c.t_end, c.t_end, c.t_end, -1});
     }
     if ((rc = ctx->trB.reserve(sizeof(double) * (rlen + 4))) || (rc = ctx->trC.reserve(sizeof(double) * (rlen + 4))) ||
         (rc = ctx->trD.reserve(sizeof(double) * (etot + 4))))

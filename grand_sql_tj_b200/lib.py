@@ -51,6 +51,14 @@ class PlanMerge(C.Structure):
     _fields_ = [("dst", C.c_int64), ("n", C.c_int64), ("s_begin", C.c_int32), ("s_end", C.c_int32)]
 
 
+class PlanItem(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("cell", "row0", "col0", "tb", "te", "ab", "ae", "slot")]
+
+
+class PlanReduce(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("cell", "row0", "col0", "slot0", "nslot", "ab", "ae", "pad_")]
+
+
 class PlanExport(C.Structure):
     _fields_ = [("ops_len", C.c_int64), ("scratch_len", C.c_int64), ("psi_len", C.c_int64),
                 ("n_tasks1", C.c_int64), ("n_tasks2", C.c_int64), ("n_cells1", C.c_int64),
@@ -60,7 +68,10 @@ class PlanExport(C.Structure):
                 ("tasks1", C.POINTER(PlanTask)), ("tasks2", C.POINTER(PlanTask)),
                 ("cells1", C.POINTER(PlanCell)), ("cells2", C.POINTER(PlanCell)),
                 ("uploads", C.POINTER(PlanUpload)), ("merges", C.POINTER(PlanMerge)),
-                ("merge_src", C.POINTER(C.c_int64)), ("merge_coef", C.POINTER(C.c_double))]
+                ("merge_src", C.POINTER(C.c_int64)), ("merge_coef", C.POINTER(C.c_double)),
+                ("n_items1", C.c_int64), ("n_items2", C.c_int64), ("n_red1", C.c_int64), ("n_red2", C.c_int64),
+                ("items1", C.POINTER(PlanItem)), ("items2", C.POINTER(PlanItem)),
+                ("red1", C.POINTER(PlanReduce)), ("red2", C.POINTER(PlanReduce))]
 
 
 _lib = None
@@ -246,6 +257,8 @@ def _export(call) -> dict:
         "cells1": (PlanCell * max(ex.n_cells1, 1))(), "cells2": (PlanCell * max(ex.n_cells2, 1))(),
         "uploads": (PlanUpload * max(ex.n_uploads, 1))(), "merges": (PlanMerge * max(ex.n_merges, 1))(),
         "merge_src": (C.c_int64 * max(ex.n_merge_src, 1))(), "merge_coef": (C.c_double * max(ex.n_merge_src, 1))(),
+        "items1": (PlanItem * max(ex.n_items1, 1))(), "items2": (PlanItem * max(ex.n_items2, 1))(),
+        "red1": (PlanReduce * max(ex.n_red1, 1))(), "red2": (PlanReduce * max(ex.n_red2, 1))(),
     }
     for k, a in arrs.items():
         setattr(ex, k, C.cast(a, type(getattr(ex, k))))

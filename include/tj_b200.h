@@ -273,6 +273,12 @@ typedef struct tj_plan_task { tj_plan_operand L, R; double coef; int32_t K, pad_
 typedef struct tj_plan_cell { int64_t off; int32_t ld, M, N, t_begin, t_end; int8_t space, pad_[7]; } tj_plan_cell;
 typedef struct tj_plan_upload { const double *src; int64_t n, dst; } tj_plan_upload;
 typedef struct tj_plan_merge { int64_t dst, n; int32_t s_begin, s_end; } tj_plan_merge;
+/* A work item: BM x BN tile (row0, col0) of `cell`, GEMM tasks [tb, te), axpy
+ * tasks [ab, ae); slot < 0 stores the tile, slot >= 0 writes partial slot
+ * `slot`.  A reduce record sums slots [slot0, slot0 + nslot) of a tile and
+ * adds the axpy tasks [ab, ae).  Tile size: 64 x 64. */
+typedef struct tj_plan_item { int32_t cell, row0, col0, tb, te, ab, ae, slot; } tj_plan_item;
+typedef struct tj_plan_reduce { int32_t cell, row0, col0, slot0, nslot, ab, ae, pad_; } tj_plan_reduce;
 typedef struct tj_plan_export {
   int64_t ops_len, scratch_len, psi_len;
   int64_t n_tasks1, n_tasks2, n_cells1, n_cells2, n_uploads, n_merges, n_merge_src;
@@ -283,6 +289,9 @@ typedef struct tj_plan_export {
   tj_plan_merge *merges;
   int64_t *merge_src;
   double *merge_coef;
+  int64_t n_items1, n_items2, n_red1, n_red2;
+  tj_plan_item *items1, *items2;
+  tj_plan_reduce *red1, *red2;
 } tj_plan_export;
 int tj_hpsi_plan_export(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
                         const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave,
