@@ -9,6 +9,20 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libtjb200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+
+def cutlass_include() -> str:
+    """CUTLASS/CuTe headers (only the sm100 UMMA descriptor definitions are used)."""
+    import glob as _g
+    import site
+    for d in site.getsitepackages() + [os.path.join(os.path.dirname(os.__file__), "site-packages")]:
+        for cand in (os.path.join(d, "flashinfer", "data", "cutlass", "include"),):
+            if os.path.exists(os.path.join(cand, "cute", "arch", "mma_sm100_desc.hpp")):
+                return cand
+    hits = _g.glob("/opt/**/cutlass/include/cute/arch/mma_sm100_desc.hpp", recursive=True)
+    if hits:
+        return os.path.dirname(os.path.dirname(os.path.dirname(hits[0])))
+    raise RuntimeError("CUTLASS headers with sm100 UMMA descriptors not found")
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-gencode", "arch=compute_100a,code=sm_100a",
          "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-O3", "--expt-relaxed-constexpr"]
 
@@ -37,7 +51,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     objs = []
     for src in sources():
         obj = os.path.join(bdir, os.path.basename(src) + ".o")
-        cmd = [NVCC] + FLAGS + ["-I", os.path.join(HERE, "..", "include"), "-c", src, "-o", obj]
+        cmd = [NVCC] + FLAGS + ["-I", os.path.join(HERE, "..", "include"), "-I", cutlass_include(), "-c", src, "-o", obj]
         if src.endswith(".cpp"):
             cmd[1:1] = ["-x", "cu"]
         if verbose:

@@ -205,6 +205,32 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   if ((rc = ctx->counters.reserve(64))) return rc;
   if ((rc = ctx->partials.reserve(sizeof(double) * (std::max(P->tiles2.size(), P->tiles1.size()) + 4096))))
     return rc;
+  ctx->oz.reset();
+  if (ctx->prec_mode == TJ_PREC_OZAKI) {
+    // split-precision form: regroup the tasks, split the operators once for this step
+    std::unique_ptr<OzPlan> oz(new OzPlan());
+    try {
+      build_ozaki_plan(*P, ctx->slices, *oz);
+    } catch (const std::exception &e) {
+      return set_err(TJ_ERR_ARG, std::string("split-precision plan: ") + e.what());
+    }
+    if ((rc = upload_vec(ctx, ctx->ozSplitsS, oz->sta)) || (rc = upload_vec(ctx, ctx->ozSplitsA, oz->dyn_a)) ||
+        (rc = upload_vec(ctx, ctx->ozSplitsB, oz->dyn_b)) || (rc = upload_vec(ctx, ctx->ozGroupsA, oz->groups_a)) ||
+        (rc = upload_vec(ctx, ctx->ozGroupsB, oz->groups_b)) || (rc = upload_vec(ctx, ctx->ozRowsA, oz->rows_a)) ||
+        (rc = upload_vec(ctx, ctx->ozRowsB, oz->rows_b)) || (rc = upload_vec(ctx, ctx->ozItemsA, oz->items_a)) ||
+        (rc = upload_vec(ctx, ctx->ozItemsB, oz->items_b)) || (rc = upload_vec(ctx, ctx->ozSums, oz->sums)) ||
+        (rc = upload_vec(ctx, ctx->ozSlotOffs, oz->slot_offs)))
+      return rc;
+    if ((rc = ctx->ozStaPack.reserve(oz->sta_pack + 256)) || (rc = ctx->ozStaSig.reserve(8 * (oz->sta_sig + 4))) ||
+        (rc = ctx->ozDynPack.reserve(oz->dyn_pack + 256)) || (rc = ctx->ozDynSig.reserve(8 * (oz->dyn_sig + 4))) ||
+        (rc = ctx->ozSlots.reserve(8 * (oz->slots_len + 4))) || (rc = ctx->ozMisc.reserve(256)))
+      return rc;
+    CK(cudaMemsetAsync(ctx->ozMisc.p, 0, 256, ctx->stream));
+    launch_oz_split((const OzSplit *)ctx->ozSplitsS.p, (int)oz->sta.size(), ctx->ops.d(), nullptr, nullptr,
+                    (int8_t *)ctx->ozStaPack.p, ctx->ozStaSig.d(), oz->s, ctx->stream);
+    CK(cudaGetLastError());
+    ctx->oz = std::move(oz);
+  }
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->stats = tj_hpsi_stats();
   ctx->stats.flops = P->flops;
@@ -215,14 +241,58 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   ctx->stats.n_tiles_p1 = (int64_t)P->tiles1.size();
   ctx->stats.n_tiles_p2 = (int64_t)P->tiles2.size();
   ctx->stats.scratch_doubles = P->scratch_len;
+  if (ctx->oz) ctx->stats.int8_ops = ctx->oz->mma_ops;
   ctx->plan = std::move(P);
   ctx->plan_key = h;
   ctx->plan_valid = true;
   return TJ_OK;
 }
 
+// Split-precision H*psi: split psi, launch A (products, one-sided tasks),
+// split the products, launch B (two-sided tasks), sum the task results per cell.
+static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
+  const HpsiPlan &P = *ctx->plan;
+  const OzPlan &oz = *ctx->oz;
+  cudaStream_t st = ctx->stream;
+  unsigned int *cnt = (unsigned int *)ctx->ozMisc.p;
+  int *err = (int *)((char *)ctx->ozMisc.p + 64);
+  CK(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), st));
+  if (timed) CK(cudaEventRecord(ctx->ev[0], st));
+  int8_t *dp = (int8_t *)ctx->ozDynPack.p;
+  double *ds = ctx->ozDynSig.d();
+  launch_oz_split((const OzSplit *)ctx->ozSplitsA.p, (int)oz.dyn_a.size(), ctx->ops.d(), in, ctx->scr.d(), dp, ds,
+                  oz.s, st);
+  CK(launch_oz_gemm(dp, ds, (const int8_t *)ctx->ozStaPack.p, ctx->ozStaSig.d(), (const OzGroup *)ctx->ozGroupsA.p,
+                    (const OzRow *)ctx->ozRowsA.p, (const OzItem *)ctx->ozItemsA.p, (int)oz.items_a.size(),
+                    ctx->scr.d(), ctx->ozSlots.d(), cnt, err, oz.s, st));
+  if (timed) CK(cudaEventRecord(ctx->ev[1], st));
+  launch_oz_split((const OzSplit *)ctx->ozSplitsB.p, (int)oz.dyn_b.size(), ctx->ops.d(), in, ctx->scr.d(), dp, ds,
+                  oz.s, st);
+  CK(launch_oz_gemm(dp, ds, (const int8_t *)ctx->ozStaPack.p, ctx->ozStaSig.d(), (const OzGroup *)ctx->ozGroupsB.p,
+                    (const OzRow *)ctx->ozRowsB.p, (const OzItem *)ctx->ozItemsB.p, (int)oz.items_b.size(),
+                    ctx->scr.d(), ctx->ozSlots.d(), cnt + 1, err, oz.s, st));
+  launch_oz_sum((const OzCellSum *)ctx->ozSums.p, (int)oz.sums.size(), (const int64_t *)ctx->ozSlotOffs.p,
+                ctx->ozSlots.d(), (const Task *)ctx->tasks2.p, ctx->ops.d(), in, ctx->scr.d(), out, st);
+  if (timed) CK(cudaEventRecord(ctx->ev[2], st));
+  CK(cudaGetLastError());
+  (void)P;
+  ++ctx->n_hpsi;
+  return TJ_OK;
+}
+
+// Reads the device error flag of the split-precision kernels (bounded waits).
+int tjb::check_device_flags(tj_ctx *ctx) {
+  if (!ctx->oz) return TJ_OK;
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, (char *)ctx->ozMisc.p + 64, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (flag) return set_err(TJ_ERR_TIMEOUT, "split-precision GEMM: a bounded tensor-core wait timed out");
+  return TJ_OK;
+}
+
 // out = H * in on the device (both device pointers in the plan's psi layout).
 int tjb::run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed) {
+  if (ctx->oz) return run_hpsi_oz(ctx, in, out, timed);
   const HpsiPlan &P = *ctx->plan;
   unsigned int *cnt = (unsigned int *)ctx->counters.p;
   CK(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), ctx->stream));
@@ -288,6 +358,7 @@ extern "C" int tj_model_wave(tj_ctx *ctx, const tj_lattice *lat, const tj_model 
   if ((rc = run_hpsi(ctx, ctx->vin.d(), ctx->vout.d(), true))) return rc;
   CK(cudaMemcpyAsync(outvec->data, ctx->vout.d(), sizeof(double) * D, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  if ((rc = check_device_flags(ctx))) return rc;
   float a = 0, b = 0;
   cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
   cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
@@ -329,7 +400,7 @@ extern "C" int tj_model_wave_bench(tj_ctx *ctx, const tj_lattice *lat, const tj_
   ctx->stats.last_ms = *ms;
   CK(cudaMemcpyAsync(outvec->data, ctx->vout.d(), sizeof(double) * D, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  return TJ_OK;
+  return check_device_flags(ctx);
 }
 
 // ----------------------------------------------------------------- Lanczos
@@ -424,6 +495,7 @@ extern "C" int tj_lanczos_memo_new(tj_ctx *ctx, const tj_lattice *lat, const tj_
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(eigvec->data, ctx->vout.d(), sizeof(double) * D, cudaMemcpyDeviceToHost, ctx->stream));
   if ((rc = fetch(lam, &hl))) return rc;
+  if ((rc = check_device_flags(ctx))) return rc;
   energies[0] = hl;
   *iters = last;
   ctx->stats.lanczos_hpsi = ctx->n_hpsi - h0;

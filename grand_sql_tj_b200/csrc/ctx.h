@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "ozaki.h"
 #include "tj_internal.h"
 
 namespace tjb {
@@ -49,10 +50,16 @@ struct tj_ctx {
   tjb::DevBuf lanV, lanScal, lanPart;
   tjb::DevBuf trA, trB, trC, trD, trE;          // truncation
   tjb::DevBuf corCells, corTasks, corTiles, corOps, corScr, corPsi;   // correlators
+  // split-precision H*psi
+  std::unique_ptr<tjb::OzPlan> oz;
+  tjb::DevBuf ozStaPack, ozStaSig, ozDynPack, ozDynSig, ozSplitsA, ozSplitsB, ozGroupsA, ozGroupsB, ozRowsA,
+      ozRowsB, ozItemsA, ozItemsB, ozSums, ozSlotOffs, ozSlots, ozSplitsS, ozMisc;
   std::vector<tjb::DevBuf *> all_bufs() {
     return {&ops, &scr, &vin, &vout, &counters, &partials, &cells1, &cells2, &tasks1, &tasks2, &tiles1,
             &tiles2, &red1, &red2, &slots, &m_dst, &m_n, &m_sb, &m_se, &m_src, &m_coef, &lanV, &lanScal, &lanPart, &trA, &trB,
-            &trC, &trD, &trE, &corCells, &corTasks, &corTiles, &corOps, &corScr, &corPsi};
+            &trC, &trD, &trE, &corCells, &corTasks, &corTiles, &corOps, &corScr, &corPsi, &ozStaPack, &ozStaSig,
+            &ozDynPack, &ozDynSig, &ozSplitsA, &ozSplitsB, &ozGroupsA, &ozGroupsB, &ozRowsA, &ozRowsB, &ozItemsA,
+            &ozItemsB, &ozSums, &ozSlotOffs, &ozSlots, &ozSplitsS, &ozMisc};
   }
   ~tj_ctx();
 };
@@ -61,4 +68,5 @@ namespace tjb {
 int prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const tj_model *env,
                  const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave);
 int run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed);
+int check_device_flags(tj_ctx *ctx);
 }  // namespace tjb

@@ -74,6 +74,45 @@ class PlanExport(C.Structure):
                 ("red1", C.POINTER(PlanReduce)), ("red2", C.POINTER(PlanReduce))]
 
 
+class OzSplitC(C.Structure):
+    _fields_ = [("src_off", C.c_int64), ("pack_off", C.c_int64), ("sig_off", C.c_int64), ("rs", C.c_int32),
+                ("ks", C.c_int32), ("nrows", C.c_int32), ("K", C.c_int32), ("K_pad", C.c_int32),
+                ("space", C.c_int8), ("pad_", C.c_int8 * 3)]
+
+
+class OzGroupC(C.Structure):
+    _fields_ = [("s_pack_off", C.c_int64), ("tau_off", C.c_int64), ("N", C.c_int32), ("K_pad", C.c_int32),
+                ("row_begin", C.c_int32), ("row_end", C.c_int32)]
+
+
+class OzRowC(C.Structure):
+    _fields_ = [("pack_off", C.c_int64), ("sig_idx", C.c_int64), ("dst_off", C.c_int64), ("coef", C.c_double),
+                ("slice_stride", C.c_int32), ("dst_stride", C.c_int32), ("dst_space", C.c_int32),
+                ("pad_", C.c_int32)]
+
+
+class OzItemC(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("group", "row0", "n0", "pad_")]
+
+
+class OzCellSumC(C.Structure):
+    _fields_ = [("out_off", C.c_int64)] + [(n, C.c_int32) for n in ("ld", "M", "N", "s_begin", "s_end",
+                                                                     "a_begin", "a_end")]
+
+
+class OzExport(C.Structure):
+    _fields_ = ([(n, C.c_int32) for n in ("slices", "tile_m", "tile_n", "pad_")] +
+                [(n, C.c_int64) for n in ("sta_pack", "sta_sig", "dyn_pack", "dyn_sig", "slots_len")] +
+                [("int8_ops", C.c_double)] +
+                [(n, C.c_int64) for n in ("n_sta", "n_dyn_a", "n_dyn_b", "n_groups_a", "n_groups_b", "n_rows_a",
+                                          "n_rows_b", "n_items_a", "n_items_b", "n_sums", "n_slots")] +
+                [("sta", C.POINTER(OzSplitC)), ("dyn_a", C.POINTER(OzSplitC)), ("dyn_b", C.POINTER(OzSplitC)),
+                 ("groups_a", C.POINTER(OzGroupC)), ("groups_b", C.POINTER(OzGroupC)),
+                 ("rows_a", C.POINTER(OzRowC)), ("rows_b", C.POINTER(OzRowC)),
+                 ("items_a", C.POINTER(OzItemC)), ("items_b", C.POINTER(OzItemC)),
+                 ("sums", C.POINTER(OzCellSumC)), ("slot_offs", C.POINTER(C.c_int64))])
+
+
 _lib = None
 
 
@@ -132,6 +171,8 @@ def lib():
                                           P(TjWave), P(PlanExport)]
         L.tj_cor_plan_export.argtypes = [C.c_int, P(TjBlock), P(TjBlock), P(TjBasis), P(TjBasis), P(TjWave),
                                          C.c_char, P(PlanExport)]
+        L.tj_ozaki_plan_export.argtypes = [P(TjLattice), P(TjModel), P(TjModel), P(TjBasis), P(TjBasis),
+                                           P(TjWave), C.c_int, P(OzExport)]
         for n in ("tj_measure_sys_block", "tj_measure_env_block"):
             getattr(L, n).argtypes = [C.c_void_p, P(TjBlock), P(TjBasis), P(TjWave), P(C.c_double)]
         L.tj_sys_block_env_block_cor_dia.argtypes = [C.c_void_p, P(TjBlock), P(TjBlock), P(TjBasis),
@@ -291,3 +332,29 @@ def cor_plan_export(name: str, a: Block, b: Optional[Block], sys_bs, env_bs, wav
     ref = lambda p: C.byref(p.c) if p is not None else None
     return _export(lambda ex: L.tj_cor_plan_export(COR_NAMES[name], ref(pa), ref(pb), ref(ps), ref(pe),
                                                     C.byref(wave.c), flag.encode(), ex))
+
+
+def ozaki_plan_export(sb, slices: int = 5, invec: Optional[Wave] = None) -> dict:
+    """Split-precision tables of H*psi for `sb` (no GPU needed)."""
+    L = lib()
+    invec = sb.wave if invec is None else invec
+    ps, pe, bs, be = sb.sys.pack(), sb.env.pack(), sb.sys_bs.pack(), sb.env_bs.pack()
+
+    def call(ex):
+        return L.tj_ozaki_plan_export(C.byref(sb.lat.c), C.byref(ps.c), C.byref(pe.c), C.byref(bs.c),
+                                      C.byref(be.c), C.byref(invec.c), slices, ex)
+
+    ex = OzExport()
+    _chk(call(C.byref(ex)))
+    arrs = {
+        "sta": (OzSplitC * max(ex.n_sta, 1))(), "dyn_a": (OzSplitC * max(ex.n_dyn_a, 1))(),
+        "dyn_b": (OzSplitC * max(ex.n_dyn_b, 1))(), "groups_a": (OzGroupC * max(ex.n_groups_a, 1))(),
+        "groups_b": (OzGroupC * max(ex.n_groups_b, 1))(), "rows_a": (OzRowC * max(ex.n_rows_a, 1))(),
+        "rows_b": (OzRowC * max(ex.n_rows_b, 1))(), "items_a": (OzItemC * max(ex.n_items_a, 1))(),
+        "items_b": (OzItemC * max(ex.n_items_b, 1))(), "sums": (OzCellSumC * max(ex.n_sums, 1))(),
+        "slot_offs": (C.c_int64 * max(ex.n_slots, 1))(),
+    }
+    for k, a in arrs.items():
+        setattr(ex, k, C.cast(a, type(getattr(ex, k))))
+    _chk(call(C.byref(ex)))
+    return {"ex": ex, **arrs}

@@ -89,7 +89,8 @@ class TjHpsiStats(C.Structure):
                 ("n_products", C.c_int64), ("n_tasks", C.c_int64), ("n_tiles_p1", C.c_int64),
                 ("n_tiles_p2", C.c_int64), ("scratch_doubles", C.c_int64),
                 ("last_ms", C.c_double), ("last_ms_phase1", C.c_double),
-                ("last_ms_phase2", C.c_double), ("lanczos_hpsi", C.c_int64)]
+                ("last_ms_phase2", C.c_double), ("lanczos_hpsi", C.c_int64),
+                ("int8_ops", C.c_double)]
 
 
 def _dptr(a: np.ndarray):

@@ -226,6 +226,7 @@ typedef struct tj_hpsi_stats {
   double last_ms;          /* device time of the last H*psi                      */
   double last_ms_phase1, last_ms_phase2;
   int64_t lanczos_hpsi;    /* H*psi products of the last tj_lanczos_memo_new      */
+  double int8_ops;         /* split precision: 2 x int8 MACs issued per H*psi     */
 } tj_hpsi_stats;
 int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st);
 
@@ -303,6 +304,49 @@ int tj_hpsi_plan_export(const tj_lattice *lat, const tj_model *sys, const tj_mod
  * matching entry point (NULL for a basis or operator it does not take). */
 int tj_cor_plan_export(int kind, const tj_block *a, const tj_block *b, const tj_basis *sys_bs,
                        const tj_basis *env_bs, const tj_wave *wave, char flag, tj_plan_export *out);
+
+/* The split-precision form of the same H*psi (TJ_PREC_OZAKI with `slices`
+ * int8 slices), for CPU checks of its index tables.  A split cuts rows of a
+ * matrix (element (r, k) = base[src_off + r*rs + k*ks], space 1 operators,
+ * 2 input vector, 3 phase-1 products) into `slices` int8 rows of K_pad bytes
+ * (slice p of row r at pack_off + p*nrows*K_pad + r*K_pad) and a power-of-two
+ * scale (index sig_off + r).  A GEMM group pairs the rows [row_begin,
+ * row_end) of the row list with the N rows of one operator split; each row
+ * writes y[n] = coef * sum_k L[k] S[n][k] to dst_off + n*dst_stride in the
+ * phase-1 product space (dst_space 0) or the task slots (dst_space 1).
+ * Launch A holds the products and the one-sided tasks, launch B the
+ * two-sided tasks; a cell sum adds slots [s_begin, s_end) of the slot-offset
+ * list (each an M x N column-major task result) and the axpy tasks
+ * [a_begin, a_end) of the phase-2 task list.  Two-call pattern as above. */
+typedef struct tj_oz_split {
+  int64_t src_off, pack_off, sig_off;
+  int32_t rs, ks, nrows, K, K_pad;
+  int8_t space, pad_[3];
+} tj_oz_split;
+typedef struct tj_oz_group { int64_t s_pack_off, tau_off; int32_t N, K_pad, row_begin, row_end; } tj_oz_group;
+typedef struct tj_oz_row {
+  int64_t pack_off, sig_idx, dst_off;
+  double coef;
+  int32_t slice_stride, dst_stride, dst_space, pad_;
+} tj_oz_row;
+typedef struct tj_oz_item { int32_t group, row0, n0, pad_; } tj_oz_item;
+typedef struct tj_oz_cell_sum { int64_t out_off; int32_t ld, M, N, s_begin, s_end, a_begin, a_end; } tj_oz_cell_sum;
+typedef struct tj_ozaki_export {
+  int32_t slices, tile_m, tile_n, pad_;
+  int64_t sta_pack, sta_sig, dyn_pack, dyn_sig, slots_len;
+  double int8_ops;
+  int64_t n_sta, n_dyn_a, n_dyn_b, n_groups_a, n_groups_b, n_rows_a, n_rows_b, n_items_a, n_items_b, n_sums,
+      n_slots;
+  tj_oz_split *sta, *dyn_a, *dyn_b;
+  tj_oz_group *groups_a, *groups_b;
+  tj_oz_row *rows_a, *rows_b;
+  tj_oz_item *items_a, *items_b;
+  tj_oz_cell_sum *sums;
+  int64_t *slot_offs;
+} tj_ozaki_export;
+int tj_ozaki_plan_export(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
+                         const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave, int slices,
+                         tj_ozaki_export *out);
 
 #ifdef __cplusplus
 }

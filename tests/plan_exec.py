@@ -15,7 +15,8 @@ def _view(base, op, rows, cols):
     return as_strided(a, shape=(rows, cols), strides=(8 * op.ld, 8))
 
 
-def execute(plan, psi: np.ndarray) -> np.ndarray:
+def merged_ops(plan) -> np.ndarray:
+    """The operator space after the hmerge sums (what the device computes once per step)."""
     ex = plan["ex"]
     ops = plan["ops"].copy()
     for r in range(ex.n_merges):
@@ -25,6 +26,12 @@ def execute(plan, psi: np.ndarray) -> np.ndarray:
             s = plan["merge_src"][j]
             acc = acc + plan["merge_coef"][j] * ops[s:s + m.n]
         ops[m.dst:m.dst + m.n] = acc
+    return ops
+
+
+def execute(plan, psi: np.ndarray) -> np.ndarray:
+    ex = plan["ex"]
+    ops = merged_ops(plan)
     scr = np.zeros(ex.scratch_len + 8)
     out = np.zeros(max(ex.psi_len, 1))
     psi = np.concatenate([psi, np.zeros(8)])
@@ -51,14 +58,7 @@ def execute(plan, psi: np.ndarray) -> np.ndarray:
 def execute_items(plan, psi: np.ndarray, tile: int = 64) -> np.ndarray:
     """Like execute(), but through the work items and reduce records, as the device does."""
     ex = plan["ex"]
-    ops = plan["ops"].copy()
-    for r in range(ex.n_merges):
-        m = plan["merges"][r]
-        acc = np.zeros(m.n)
-        for j in range(m.s_begin, m.s_end):
-            s = plan["merge_src"][j]
-            acc = acc + plan["merge_coef"][j] * ops[s:s + m.n]
-        ops[m.dst:m.dst + m.n] = acc
+    ops = merged_ops(plan)
     scr = np.zeros(ex.scratch_len + 8)
     out = np.full(max(ex.psi_len, 1), np.nan)
     psi = np.concatenate([psi, np.zeros(8)])
