@@ -99,8 +99,17 @@ __host__ __device__ constexpr uint32_t oz_idesc() {
                                                cute::UMMA::Major::K>();
 }
 
+__device__ __forceinline__ uint64_t oz_now_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for the mbarrier phase with the given parity; gives up after about
+// two seconds of wall time (true: the phase completed).
 __device__ __forceinline__ bool oz_wait(uint32_t mbar, uint32_t parity) {
-  for (int it = 0; it < (1 << 24); ++it) {
+  const uint64_t t0 = oz_now_ns();
+  for (;;) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred P1;\n\t"
@@ -110,8 +119,8 @@ __device__ __forceinline__ bool oz_wait(uint32_t mbar, uint32_t parity) {
         : "r"(mbar), "r"(parity)
         : "memory");
     if (ok) return true;
+    if (oz_now_ns() - t0 > 2000000000ull) return false;
   }
-  return false;
 }
 
 template <int S, int BN>

@@ -5,8 +5,8 @@
  * block-sparse tensors in derived types with allocatable components, which are
  * not C-interoperable.  This header gives flat mirrors of those types and one
  * entry point per reference routine on the hot path.  A Fortran caller fills
- * the structs from its derived types (see INTEGRATION.md for the
- * ISO_C_BINDING shim) and calls these functions in place of the Fortran ones.
+ * the structs from its derived types through an ISO_C_BINDING shim module
+ * and calls these functions in place of the Fortran ones.
  *
  * Conventions shared by every struct below:
  *   - quantum numbers are the reference's integer labels: num_up (particle
