@@ -283,7 +283,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "int8-ozaki",
                 "data": "synthetic", "config": cfg, "precision": args.precision,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-                "gpu_launches": 2 * args.steps, "wall_s_timed": wall}
+                "gpu_launches": int(st.kernels_per_hpsi) * args.steps, "wall_s_timed": wall}
         print(json.dumps(line), flush=True)
     ctx.close()
     if pg is not None:

@@ -214,20 +214,22 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
     } catch (const std::exception &e) {
       return set_err(TJ_ERR_ARG, std::string("split-precision plan: ") + e.what());
     }
-    if ((rc = upload_vec(ctx, ctx->ozSplitsS, oz->sta)) || (rc = upload_vec(ctx, ctx->ozSplitsA, oz->dyn_a)) ||
-        (rc = upload_vec(ctx, ctx->ozSplitsB, oz->dyn_b)) || (rc = upload_vec(ctx, ctx->ozGroupsA, oz->groups_a)) ||
-        (rc = upload_vec(ctx, ctx->ozGroupsB, oz->groups_b)) || (rc = upload_vec(ctx, ctx->ozRowsA, oz->rows_a)) ||
-        (rc = upload_vec(ctx, ctx->ozRowsB, oz->rows_b)) || (rc = upload_vec(ctx, ctx->ozItemsA, oz->items_a)) ||
-        (rc = upload_vec(ctx, ctx->ozItemsB, oz->items_b)) || (rc = upload_vec(ctx, ctx->ozSums, oz->sums)) ||
-        (rc = upload_vec(ctx, ctx->ozSlotOffs, oz->slot_offs)))
+    if ((rc = upload_vec(ctx, ctx->ozStaJobs, oz->sta_jobs)) || (rc = upload_vec(ctx, ctx->ozPsiJobs, oz->psi_jobs)) ||
+        (rc = upload_vec(ctx, ctx->ozProdJobs, oz->prod_jobs)) || (rc = upload_vec(ctx, ctx->ozSegs, oz->segs)) ||
+        (rc = upload_vec(ctx, ctx->ozFams, oz->fams)) || (rc = upload_vec(ctx, ctx->ozStacks, oz->stacks)) ||
+        (rc = upload_vec(ctx, ctx->ozCells, oz->cells)) || (rc = upload_vec(ctx, ctx->ozItems1, oz->items1)) ||
+        (rc = upload_vec(ctx, ctx->ozItems2, oz->items2)))
       return rc;
-    if ((rc = ctx->ozStaPack.reserve(oz->sta_pack + 256)) || (rc = ctx->ozStaSig.reserve(8 * (oz->sta_sig + 4))) ||
-        (rc = ctx->ozDynPack.reserve(oz->dyn_pack + 256)) || (rc = ctx->ozDynSig.reserve(8 * (oz->dyn_sig + 4))) ||
-        (rc = ctx->ozSlots.reserve(8 * (oz->slots_len + 4))) || (rc = ctx->ozMisc.reserve(256)))
+    if ((rc = ctx->ozPack.reserve(oz->sta_pack + oz->dyn_pack + 256)) ||
+        (rc = ctx->ozScales.reserve(sizeof(double) * (oz->n_scales + 4))) || (rc = ctx->ozMisc.reserve(256)))
       return rc;
     CK(cudaMemsetAsync(ctx->ozMisc.p, 0, 256, ctx->stream));
-    launch_oz_split((const OzSplit *)ctx->ozSplitsS.p, (int)oz->sta.size(), ctx->ops.d(), nullptr, nullptr,
-                    (int8_t *)ctx->ozStaPack.p, ctx->ozStaSig.d(), oz->s, ctx->stream);
+    CK(cudaMemsetAsync(ctx->ozScales.p, 0, sizeof(double) * (oz->n_scales + 4), ctx->stream));
+    // operator splits: once per step
+    launch_oz_max((const OzJob *)ctx->ozStaJobs.p, (int)oz->sta_jobs.size(), ctx->ops.d(), nullptr, nullptr,
+                  ctx->ozScales.d(), ctx->stream);
+    launch_oz_split((const OzJob *)ctx->ozStaJobs.p, (int)oz->sta_jobs.size(), ctx->ops.d(), nullptr, nullptr,
+                    ctx->ozScales.d(), (uint8_t *)ctx->ozPack.p, oz->s, ctx->stream);
     CK(cudaGetLastError());
     ctx->oz = std::move(oz);
   }
@@ -241,41 +243,43 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   ctx->stats.n_tiles_p1 = (int64_t)P->tiles1.size();
   ctx->stats.n_tiles_p2 = (int64_t)P->tiles2.size();
   ctx->stats.scratch_doubles = P->scratch_len;
-  if (ctx->oz) ctx->stats.int8_ops = ctx->oz->mma_ops;
+  ctx->stats.kernels_per_hpsi = 2 + (P->red1.empty() ? 0 : 1) + (P->red2.empty() ? 0 : 1);
+  if (ctx->oz) {
+    const OzPlan &oz = *ctx->oz;
+    ctx->stats.int8_ops = oz.mma_ops;
+    ctx->stats.kernels_per_hpsi = (oz.psi_jobs.empty() ? 0 : 2) + (oz.items1.empty() ? 0 : 1) +
+                                  (oz.prod_jobs.empty() ? 0 : 1) + (oz.items2.empty() ? 0 : 1);
+  }
   ctx->plan = std::move(P);
   ctx->plan_key = h;
   ctx->plan_valid = true;
   return TJ_OK;
 }
 
-// Split-precision H*psi: split psi, launch A (products, one-sided tasks),
-// split the products, launch B (two-sided tasks), sum the task results per cell.
+// Split-precision H*psi: psi scales and splits, launch 1 (phase-1 products,
+// left and right families), product splits, launch 2 (two-sided families).
 static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
-  const HpsiPlan &P = *ctx->plan;
   const OzPlan &oz = *ctx->oz;
   cudaStream_t st = ctx->stream;
-  unsigned int *cnt = (unsigned int *)ctx->ozMisc.p;
   int *err = (int *)((char *)ctx->ozMisc.p + 64);
-  CK(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), st));
+  double *scales = ctx->ozScales.d();
+  uint8_t *pack = (uint8_t *)ctx->ozPack.p;
+  CK(cudaMemsetAsync(scales + oz.dyn_scale_begin, 0, sizeof(double) * (oz.n_scales - oz.dyn_scale_begin), st));
   if (timed) CK(cudaEventRecord(ctx->ev[0], st));
-  int8_t *dp = (int8_t *)ctx->ozDynPack.p;
-  double *ds = ctx->ozDynSig.d();
-  launch_oz_split((const OzSplit *)ctx->ozSplitsA.p, (int)oz.dyn_a.size(), ctx->ops.d(), in, ctx->scr.d(), dp, ds,
-                  oz.s, st);
-  CK(launch_oz_gemm(dp, ds, (const int8_t *)ctx->ozStaPack.p, ctx->ozStaSig.d(), (const OzGroup *)ctx->ozGroupsA.p,
-                    (const OzRow *)ctx->ozRowsA.p, (const OzItem *)ctx->ozItemsA.p, (int)oz.items_a.size(),
-                    ctx->scr.d(), ctx->ozSlots.d(), cnt, err, oz.s, st));
+  launch_oz_max((const OzJob *)ctx->ozPsiJobs.p, (int)oz.psi_jobs.size(), ctx->ops.d(), in, ctx->scr.d(), scales, st);
+  launch_oz_split((const OzJob *)ctx->ozPsiJobs.p, (int)oz.psi_jobs.size(), ctx->ops.d(), in, ctx->scr.d(), scales,
+                  pack, oz.s, st);
+  CK(launch_oz_gemm((const OzItem *)ctx->ozItems1.p, (int)oz.items1.size(), (const OzSeg *)ctx->ozSegs.p,
+                    (const OzFam *)ctx->ozFams.p, (const OzStack *)ctx->ozStacks.p, (const OzCell *)ctx->ozCells.p,
+                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, st));
   if (timed) CK(cudaEventRecord(ctx->ev[1], st));
-  launch_oz_split((const OzSplit *)ctx->ozSplitsB.p, (int)oz.dyn_b.size(), ctx->ops.d(), in, ctx->scr.d(), dp, ds,
-                  oz.s, st);
-  CK(launch_oz_gemm(dp, ds, (const int8_t *)ctx->ozStaPack.p, ctx->ozStaSig.d(), (const OzGroup *)ctx->ozGroupsB.p,
-                    (const OzRow *)ctx->ozRowsB.p, (const OzItem *)ctx->ozItemsB.p, (int)oz.items_b.size(),
-                    ctx->scr.d(), ctx->ozSlots.d(), cnt + 1, err, oz.s, st));
-  launch_oz_sum((const OzCellSum *)ctx->ozSums.p, (int)oz.sums.size(), (const int64_t *)ctx->ozSlotOffs.p,
-                ctx->ozSlots.d(), (const Task *)ctx->tasks2.p, ctx->ops.d(), in, ctx->scr.d(), out, st);
+  launch_oz_split((const OzJob *)ctx->ozProdJobs.p, (int)oz.prod_jobs.size(), ctx->ops.d(), in, ctx->scr.d(), scales,
+                  pack, oz.s, st);
+  CK(launch_oz_gemm((const OzItem *)ctx->ozItems2.p, (int)oz.items2.size(), (const OzSeg *)ctx->ozSegs.p,
+                    (const OzFam *)ctx->ozFams.p, (const OzStack *)ctx->ozStacks.p, (const OzCell *)ctx->ozCells.p,
+                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, st));
   if (timed) CK(cudaEventRecord(ctx->ev[2], st));
   CK(cudaGetLastError());
-  (void)P;
   ++ctx->n_hpsi;
   return TJ_OK;
 }

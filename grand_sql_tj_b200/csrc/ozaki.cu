@@ -1,19 +1,23 @@
-// Device side of the split-precision H*psi (see ozaki.h for the scheme).
+// Device side of the split-precision H*psi (the scheme and the split layout
+// are described in ozaki.h).
 //
-// oz_split:  one warp per row: row max -> power-of-two scale 2^e with
-//            |x| / 2^e < 1 -> s truncated radix-128 digits, each in [-127, 127].
-// oz_gemm:   persistent CTAs (4 warps).  Per work item (group, 128 stacked
-//            rows, BN shared-operand rows) the A slices (gathered rows) and B
-//            slices are staged in shared memory in the UMMA K-major,
-//            no-swizzle layout (8-row x 16-byte core matrices), one thread
-//            issues tcgen05.mma kind::i8 for every slice pair (p, q) with
-//            p + q <= s + 1 into the TMEM accumulator of diagonal p + q, a
-//            tcgen05.commit arrives on an mbarrier, and all four warps read
-//            the diagonals back (tcgen05.ld 32x32b), weight them by 128^-d in
-//            FP64 and store the scaled rows.  Every wait is bounded: on
-//            timeout the kernel raises an error flag, frees its TMEM and
-//            returns.
-// oz_sum:    output cell = sum of its tasks' results + axpy terms.
+// oz_max_kernel    row maxima of the split jobs (atomic max on the scale pool)
+// oz_split_kernel  scaled, truncated radix-128 digits in the tile-ready layout
+// oz_gemm_kernel   persistent, warp-specialised tcgen05 kind::i8 GEMM:
+//                    warp 4 (one lane)  bulk-copies the A and B digit blocks of
+//                                       each k-block into a ring of smem stages
+//                    warp 5 (one lane)  issues, per stage, the MMAs of every slice
+//                                       pair p + q <= s + 1 into the TMEM
+//                                       accumulator of diagonal p + q (two TMEM
+//                                       buffers, one family each)
+//                    warps 0-3          read the diagonals back (tcgen05.ld),
+//                                       weight them by 128^-d, scale by the row
+//                                       and column scales and add into the FP64
+//                                       output tile (products: store P and raise
+//                                       the pi scales)
+//                  Every wait is bounded by wall time: on timeout the kernel
+//                  raises *err, lets the other roles drop out, waits (bounded)
+//                  for its copies and MMAs in flight, frees TMEM and returns.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -25,60 +29,155 @@
 
 namespace tjb {
 
-struct OzSplitParams {
-  const OzSplit *jobs;
-  const double *ops, *psi, *scr;
-  int8_t *pack;
-  double *sig;
-  int s;
-};
+__device__ __forceinline__ double oz_pow2_of(double m) {
+  if (!(m > 0.0)) return 0.0;
+  int e;
+  frexp(m, &e);   // m = f 2^e, f in [0.5, 1): every |x| <= m has |x| 2^-e < 1
+  return ldexp(1.0, e);
+}
 
-__global__ void __launch_bounds__(256) oz_split_kernel(OzSplitParams p) {
-  const OzSplit J = p.jobs[blockIdx.x];
-  const double *base = J.space == SP_OPS ? p.ops : (J.space == SP_PSI ? p.psi : p.scr);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int r = warp; r < J.nrows; r += nw) {
-    const double *row = base + J.src_off + (int64_t)r * J.rs;
-    double mx = 0.0;
-    for (int k = lane; k < J.K; k += 32) mx = fmax(mx, fabs(row[(int64_t)k * J.ks]));
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    int e = 0;
-    if (mx > 0.0) frexp(mx, &e);   // mx = f 2^e, f in [0.5, 1): |x| 2^-e < 1
-    if (lane == 0) p.sig[J.sig_off + r] = mx > 0.0 ? ldexp(1.0, e) : 0.0;
-    int8_t *dst = p.pack + J.pack_off + (int64_t)r * J.K_pad;
-    const int64_t sstride = (int64_t)J.nrows * J.K_pad;
-    for (int k = lane; k < J.K_pad; k += 32) {
-      double t = (k < J.K && mx > 0.0) ? ldexp(row[(int64_t)k * J.ks], -e) : 0.0;
-      for (int q = 0; q < p.s; ++q) {
-        t *= 128.0;
-        const double a = trunc(t);
-        t -= a;
-        dst[q * sstride + k] = (int8_t)(int)a;
+__device__ __forceinline__ const double *oz_space(int8_t sp, const double *ops, const double *psi,
+                                                  const double *scr) {
+  return sp == SP_OPS ? ops : (sp == SP_PSI ? psi : scr);
+}
+
+// ------------------------------------------------------------ row maxima
+// One CTA (256 threads) per job.  rs == 1: 32 consecutive rows x 8 k lanes;
+// otherwise 32 consecutive k x 8 rows (the unit-stride index runs across lanes).
+__global__ void __launch_bounds__(256) oz_max_kernel(const OzJob *jobs, const double *ops, const double *psi,
+                                                     const double *scr, double *scales) {
+  const OzJob J = jobs[blockIdx.x];
+  if (!J.want_max) return;
+  const double *base = oz_space(J.space, ops, psi, scr) + J.src_off;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  __shared__ double red[8][33];
+  if (J.rs == 1) {
+    for (int r0 = 0; r0 < J.nrows; r0 += 32) {
+      const int r = r0 + tx;
+      double m = 0.0;
+      if (r < J.nrows)
+        for (int k = ty; k < J.K; k += 8) m = fmax(m, fabs(J.coef * base[(int64_t)r + (int64_t)k * J.ks]));
+      red[ty][tx] = m;
+      __syncthreads();
+      if (ty == 0 && r < J.nrows) {
+        for (int y = 1; y < 8; ++y) m = fmax(m, red[y][tx]);
+        if (m > 0.0)
+          atomicMax((unsigned long long *)&scales[J.scale_idx + r], (unsigned long long)__double_as_longlong(m));
+      }
+      __syncthreads();
+    }
+  } else {
+    for (int r = ty; r < J.nrows; r += 8) {
+      double m = 0.0;
+      for (int k = tx; k < J.K; k += 32) m = fmax(m, fabs(J.coef * base[(int64_t)r * J.rs + k]));
+      for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if (tx == 0 && m > 0.0)
+        atomicMax((unsigned long long *)&scales[J.scale_idx + r], (unsigned long long)__double_as_longlong(m));
+    }
+  }
+}
+
+// ------------------------------------------------------------ digits
+// One unit = (row r, 16 consecutive k): s 16-byte digit rows.
+template <int S>
+__global__ void __launch_bounds__(256) oz_split_kernel(const OzJob *jobs, const double *ops, const double *psi,
+                                                       const double *scr, const double *scales, uint8_t *pack) {
+  const OzJob J = jobs[blockIdx.x];
+  const double *base = oz_space(J.space, ops, psi, scr) + J.src_off;
+  const int rows = J.gtot * 8;
+  const int nk16 = (J.K + 31) / 32 * 2;
+  const int64_t units = (int64_t)rows * nk16;
+  for (int64_t u = threadIdx.x; u < units; u += blockDim.x) {
+    int r, c16;
+    if (J.rs == 1) {   // consecutive threads: consecutive rows
+      r = (int)(u % rows);
+      c16 = (int)(u / rows);
+    } else {           // consecutive threads: consecutive k chunks
+      r = (int)(u / nk16);
+      c16 = (int)(u % nk16);
+    }
+    uint32_t dig[S][4];
+#pragma unroll
+    for (int q = 0; q < S; ++q) dig[q][0] = dig[q][1] = dig[q][2] = dig[q][3] = 0u;
+    if (r < J.nrows) {
+      const double sc = oz_pow2_of(scales[J.scale_idx + r]);
+      if (sc > 0.0) {
+        const double inv = 1.0 / sc;   // exact: sc is a power of two
+        const double *row = base + (int64_t)r * J.rs;
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+          const int k = c16 * 16 + kk;
+          double t = k < J.K ? (J.coef * row[(int64_t)k * J.ks]) * inv : 0.0;
+#pragma unroll
+          for (int q = 0; q < S; ++q) {
+            t *= 128.0;
+            const double a = trunc(t);
+            t -= a;
+            dig[q][kk >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)a) << (8 * (kk & 3));
+          }
+        }
       }
     }
+    const int kb = c16 >> 1, c = c16 & 1, g = r >> 3, r8 = r & 7;
+    uint8_t *dst = pack + J.dst + ((int64_t)(J.kb0 + kb) * J.gtot + g) * (S * 256) + c * 128 + r8 * 16;
+#pragma unroll
+    for (int q = 0; q < S; ++q)
+      *reinterpret_cast<uint4 *>(dst + q * 256) = make_uint4(dig[q][0], dig[q][1], dig[q][2], dig[q][3]);
   }
 }
 
 // ------------------------------------------------------------ tcgen05 GEMM
 struct OzGemmParams {
-  const int8_t *dyn_pack;
-  const double *dyn_sig;
-  const int8_t *sta_pack;
-  const double *sta_sig;
-  const OzGroup *groups;
-  const OzRow *rows;
   const OzItem *items;
   int nitems;
-  double *out_scr, *out_slots;
-  unsigned int *counter;
+  const OzSeg *segs;
+  const OzFam *fams;
+  const OzStack *stacks;
+  const OzCell *cells;
+  const Task *tasks;
+  const uint8_t *pack;
+  double *scales;
+  const double *psi;
+  double *scr, *out;
   int *err;
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint32_t oz_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// K-major, no-swizzle UMMA shared-memory descriptor: core matrices of 8 rows
-// x 16 bytes stored contiguously; lbo = bytes between the two 16-byte halves
-// of a k32 step, sbo = bytes between consecutive 8-row groups.
+__device__ __forceinline__ uint64_t oz_now_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+constexpr uint64_t OZ_WAIT_NS = 2000000000ull;
+
+// Waits for the phase of the given parity; false after ~2 s or when another
+// role has aborted (*abort != 0).
+__device__ __forceinline__ bool oz_wait(uint32_t mbar, uint32_t parity, volatile int *abort) {
+  const uint64_t t0 = oz_now_ns();
+  for (;;) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(ok)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (abort && *abort) return false;
+    if (oz_now_ns() - t0 > OZ_WAIT_NS) return false;
+  }
+}
+
+__device__ __forceinline__ void oz_fail(volatile int *abort, int *err) {
+  *abort = 1;
+  atomicExch(err, 1);
+}
+
+// K-major, no-swizzle UMMA shared-memory descriptor (core matrices of 8 rows x
+// 16 bytes; lbo = bytes between the two K halves, sbo = bytes between groups).
 __device__ __forceinline__ uint64_t oz_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   cute::UMMA::SmemDescriptor d;
   d.desc_ = 0;
@@ -92,262 +191,410 @@ __device__ __forceinline__ uint64_t oz_desc(uint32_t saddr, uint32_t lbo, uint32
   return d.desc_;
 }
 
-template <int BN>
-__host__ __device__ constexpr uint32_t oz_idesc() {
-  // kind::i8: signed int8 A and B (K-major), int32 accumulator, M = 128, N = BN
-  return (uint32_t)cute::UMMA::make_instr_desc<int8_t, int8_t, int32_t, OZ_BM, BN, cute::UMMA::Major::K,
-                                               cute::UMMA::Major::K>();
+// kind::i8 instruction descriptor: signed int8 A and B (K-major), int32 D, M x N.
+__device__ __forceinline__ uint32_t oz_idesc(int M, int N) {
+  cute::UMMA::InstrDescriptor d =
+      cute::UMMA::make_instr_desc<int8_t, int8_t, int32_t, 128, 64, cute::UMMA::Major::K, cute::UMMA::Major::K>();
+  d.m_dim_ = (uint8_t)(M >> 4);
+  d.n_dim_ = (uint8_t)(N >> 3);
+  return (uint32_t)d;
 }
 
-__device__ __forceinline__ uint64_t oz_now_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
+__device__ __forceinline__ void oz_bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
 }
 
-// Waits for the mbarrier phase with the given parity; gives up after about
-// two seconds of wall time (true: the phase completed).
-__device__ __forceinline__ bool oz_wait(uint32_t mbar, uint32_t parity) {
-  const uint64_t t0 = oz_now_ns();
-  for (;;) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, P1;\n\t}"
-        : "=r"(ok)
-        : "r"(mbar), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if (oz_now_ns() - t0 > 2000000000ull) return false;
-  }
+__device__ __forceinline__ void oz_arrive_expect(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void oz_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void oz_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
 }
 
 template <int S, int BN>
-__global__ void __launch_bounds__(128, 1) oz_gemm_kernel(OzGemmParams p) {
+struct OzCfg {
+  static constexpr int A_BYTES = S * 16 * 256;          // 128 rows x 32 k, s slices
+  static constexpr int B_BYTES = S * (BN / 8) * 256;
+  static constexpr int STAGE = A_BYTES + B_BYTES;
+  static constexpr int STAGES_RAW = (200 * 1024) / STAGE;
+  static constexpr int STAGES = STAGES_RAW > 8 ? 8 : STAGES_RAW;
+  static constexpr int SMEM = STAGES * STAGE;
+  static_assert(S * BN <= 256, "diagonal accumulators exceed one TMEM buffer");
+  static_assert(STAGES >= 2, "too few pipeline stages");
+};
+
+template <int S, int BN>
+__global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
+  using C = OzCfg<S, BN>;
+  constexpr int ST = C::STAGES;
   extern __shared__ __align__(1024) uint8_t smem[];
-  constexpr int A_CHUNK = OZ_BM * 16;          // bytes of one 16-byte K column of A (128 rows)
-  constexpr int B_CHUNK = BN * 16;
-  constexpr int A_SLICE = A_CHUNK * (OZ_KC / 16);
-  constexpr int B_SLICE = B_CHUNK * (OZ_KC / 16);
-  constexpr int TMEM_COLS = 256;
-  static_assert(S * BN <= TMEM_COLS, "diagonal accumulators exceed the TMEM allocation");
-  uint8_t *As = smem;
-  uint8_t *Bs = smem + S * A_SLICE;
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t full_bar[ST], empty_bar[ST], tfull_bar[2], tempty_bar[2], drain_bar;
   __shared__ uint32_t tmem_sh;
-  __shared__ int item_sh, bad_sh;
+  __shared__ volatile int abort_sh;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
+  if (tid == 0) {
+    for (int i = 0; i < ST; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(&full_bar[i])), "r"(1));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(&empty_bar[i])), "r"(1));
+    }
+    for (int i = 0; i < 2; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(&tfull_bar[i])), "r"(1));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(&tempty_bar[i])), "r"(128));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(&drain_bar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_sh = 0;
+  }
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
-                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(oz_smem(&tmem_sh)),
+                 "r"(512));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     asm volatile("tcgen05.fence::before_thread_sync;");
-  }
-  if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
-    asm volatile("fence.mbarrier_init.release.cluster;");
-    bad_sh = 0;
   }
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = tmem_sh;
-  const uint32_t mb = smem_u32(&mbar);
-  const uint32_t idesc = oz_idesc<BN>();
-  uint32_t phase = 0;
+  const uint32_t smem0 = oz_smem(smem);
 
-  for (;;) {
-    if (tid == 0) item_sh = (int)atomicAdd(p.counter, 1u);
-    __syncthreads();
-    const int it = item_sh;
-    if (it >= p.nitems || bad_sh) break;
-    const OzItem item = p.items[it];
-    const OzGroup g = p.groups[item.group];
-    const int nrows = min(OZ_BM, g.row_end - g.row_begin - item.row0);
-    const int ncols = min(BN, g.N - item.n0);
-    for (int kc = 0; kc < g.K_pad; kc += OZ_KC) {
-      const int kb = min(OZ_KC, g.K_pad - kc), nch = kb / 16;
-      for (int idx = tid; idx < S * OZ_BM * nch; idx += blockDim.x) {
-        const int c = idx % nch, r = (idx / nch) % OZ_BM, sl = idx / (nch * OZ_BM);
-        const uint32_t dst = smem_u32(As) + sl * A_SLICE + c * A_CHUNK + (r >> 3) * 128 + (r & 7) * 16;
-        const int8_t *src = p.dyn_pack;
-        uint32_t bytes = 0;
-        if (r < nrows) {
-          const OzRow &R = p.rows[g.row_begin + item.row0 + r];
-          src = p.dyn_pack + R.pack_off + (int64_t)sl * R.slice_stride + kc + c * 16;
-          bytes = 16;
-        }
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
-      }
-      for (int idx = tid; idx < S * BN * nch; idx += blockDim.x) {
-        const int c = idx % nch, n = (idx / nch) % BN, sl = idx / (nch * BN);
-        const uint32_t dst = smem_u32(Bs) + sl * B_SLICE + c * B_CHUNK + (n >> 3) * 128 + (n & 7) * 16;
-        const int8_t *src = p.sta_pack;
-        uint32_t bytes = 0;
-        if (n < ncols) {
-          src = p.sta_pack + g.s_pack_off + ((int64_t)sl * g.N + item.n0 + n) * g.K_pad + kc + c * 16;
-          bytes = 16;
-        }
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
-      }
-      asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      __syncthreads();
-      if (tid == 0) {
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        for (int ks = 0; ks < kb / 32; ++ks) {
-#pragma unroll
-          for (int pa = 1; pa <= S; ++pa)
-#pragma unroll
-            for (int qb = 1; pa + qb <= S + 1; ++qb) {
-              const int d = pa + qb;
-              const uint64_t da = oz_desc(smem_u32(As) + (pa - 1) * A_SLICE + ks * 2 * A_CHUNK, A_CHUNK, 128);
-              const uint64_t db = oz_desc(smem_u32(Bs) + (qb - 1) * B_SLICE + ks * 2 * B_CHUNK, B_CHUNK, 128);
-              const uint32_t dt = tmem + (uint32_t)((d - 2) * BN);
-              // the first product of each diagonal in an item overwrites the accumulator
-              const uint32_t acc = (kc > 0 || ks > 0 || pa > 1) ? 1u : 0u;
-              asm volatile(
-                  "{\n\t.reg .pred p;\n\t"
-                  "setp.ne.b32 p, %4, 0;\n\t"
-                  "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-                  :
-                  : "r"(dt), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+  if (warp == 4) {
+    // ------------------------------------------------ producer
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t ph = 0;
+      int armed[ST];
+      uint32_t armed_ph[ST];
+      for (int i = 0; i < ST; ++i) armed[i] = 0, armed_ph[i] = 0;
+      bool ok = true;
+      for (int ii = blockIdx.x; ii < p.nitems && ok; ii += gridDim.x) {
+        const OzItem it = p.items[ii];
+        const uint32_t gb = (uint32_t)((it.ncols + 7) >> 3), b_g0 = (uint32_t)(it.col0 >> 3);
+        if (it.kind == 1) {
+          const OzSeg sg = p.segs[it.seg];
+          for (int kb = 0; kb < sg.nkb && ok; ++kb) {
+            if (!oz_wait(oz_smem(&empty_bar[stage]), ph ^ 1u, &abort_sh)) {
+              if (!abort_sh) oz_fail(&abort_sh, p.err);
+              ok = false;
+              break;
             }
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mb)
-                     : "memory");
-      }
-      if (!oz_wait(mb, phase)) {
-        if (tid == 0) {
-          bad_sh = 1;
-          atomicExch(p.err, 1);
-        }
-        oz_wait(mb, phase);   // give the MMAs in flight one more bounded chance before TMEM is freed
-      }
-      phase ^= 1u;
-      asm volatile("tcgen05.fence::after_thread_sync;");
-      __syncthreads();
-      if (bad_sh) break;
-    }
-    if (bad_sh) break;
-    // epilogue: warp w reads TMEM lanes 32w..32w+31 = stacked rows 32w..32w+31
-    const int r = warp * 32 + lane;
-    const bool rv = r < nrows;
-    double rscale = 0.0;
-    double *dst = nullptr;
-    int32_t dstride = 0;
-    if (rv) {
-      const OzRow &R = p.rows[g.row_begin + item.row0 + r];
-      rscale = R.coef * p.dyn_sig[R.sig_idx];
-      dst = (R.dst_space == 0 ? p.out_scr : p.out_slots) + R.dst_off;
-      dstride = R.dst_stride;
-    }
-#pragma unroll
-    for (int j0 = 0; j0 < BN; j0 += 16) {
-      uint32_t v[S][16];
-#pragma unroll
-      for (int d = 0; d < S; ++d) {
-        const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(d * BN + j0);
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(v[d][0]), "=r"(v[d][1]), "=r"(v[d][2]), "=r"(v[d][3]), "=r"(v[d][4]), "=r"(v[d][5]),
-              "=r"(v[d][6]), "=r"(v[d][7]), "=r"(v[d][8]), "=r"(v[d][9]), "=r"(v[d][10]), "=r"(v[d][11]),
-              "=r"(v[d][12]), "=r"(v[d][13]), "=r"(v[d][14]), "=r"(v[d][15])
-            : "r"(ta));
-      }
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (rv) {
-#pragma unroll
-        for (int jj = 0; jj < 16; ++jj) {
-          const int n = j0 + jj;
-          if (n < ncols) {
-            double acc = 0.0;
-#pragma unroll
-            for (int d = S - 1; d >= 0; --d) acc = acc + ldexp((double)(int32_t)v[d][jj], -7 * (d + 2));
-            dst[(int64_t)(item.n0 + n) * dstride] = acc * rscale * p.sta_sig[g.tau_off + item.n0 + n];
+            const uint32_t fb = oz_smem(&full_bar[stage]);
+            const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE), sbb = sa + C::A_BYTES;
+            uint32_t bytes = gb * S * 256;
+            for (int si = it.fam_begin; si < it.fam_end; ++si) bytes += (uint32_t)p.stacks[si].a_ng * S * 256;
+            oz_arrive_expect(fb, bytes);
+            armed[stage] = 1;
+            armed_ph[stage] = ph;
+            uint32_t aoff = 0;
+            for (int si = it.fam_begin; si < it.fam_end; ++si) {
+              const OzStack sk = p.stacks[si];
+              const uint8_t *src = p.pack + sk.a_base + ((int64_t)kb * sk.a_gtot + sk.a_g0) * (S * 256);
+              oz_bulk_g2s(sa + aoff, src, (uint32_t)sk.a_ng * S * 256, fb);
+              aoff += (uint32_t)sk.a_ng * S * 256;
+            }
+            const uint8_t *bsrc = p.pack + sg.b_base + ((int64_t)(sg.b_kb0 + kb) * sg.b_gtot + b_g0) * (S * 256);
+            oz_bulk_g2s(sbb, bsrc, gb * S * 256, fb);
+            if (++stage == ST) stage = 0, ph ^= 1u;
+          }
+        } else {
+          const uint32_t ga = (uint32_t)((it.mrows + 7) >> 3), a_g0 = (uint32_t)(it.row0 >> 3);
+          for (int f = it.fam_begin; f < it.fam_end && ok; ++f) {
+            const OzFam fm = p.fams[f];
+            for (int sgi = fm.seg_begin; sgi < fm.seg_end && ok; ++sgi) {
+              const OzSeg sg = p.segs[sgi];
+              for (int kb = 0; kb < sg.nkb; ++kb) {
+                if (!oz_wait(oz_smem(&empty_bar[stage]), ph ^ 1u, &abort_sh)) {
+                  if (!abort_sh) oz_fail(&abort_sh, p.err);
+                  ok = false;
+                  break;
+                }
+                const uint32_t fb = oz_smem(&full_bar[stage]);
+                const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE), sbb = sa + C::A_BYTES;
+                oz_arrive_expect(fb, (ga + gb) * S * 256);
+                armed[stage] = 1;
+                armed_ph[stage] = ph;
+                const uint8_t *asrc =
+                    p.pack + sg.a_base + ((int64_t)(sg.a_kb0 + kb) * sg.a_gtot + a_g0) * (S * 256);
+                const uint8_t *bsrc =
+                    p.pack + sg.b_base + ((int64_t)(sg.b_kb0 + kb) * sg.b_gtot + b_g0) * (S * 256);
+                oz_bulk_g2s(sa, asrc, ga * S * 256, fb);
+                oz_bulk_g2s(sbb, bsrc, gb * S * 256, fb);
+                if (++stage == ST) stage = 0, ph ^= 1u;
+              }
+            }
           }
         }
       }
+      // copies still in flight land before the CTA exits
+      for (int i = 0; i < ST; ++i)
+        if (armed[i]) oz_wait(oz_smem(&full_bar[i]), armed_ph[i], nullptr);
     }
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
+    __syncwarp();
+  } else if (warp == 5) {
+    // ------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t ph = 0;
+      uint32_t famc = 0;
+      bool ok = true, issued = false;
+      for (int ii = blockIdx.x; ii < p.nitems && ok; ii += gridDim.x) {
+        const OzItem it = p.items[ii];
+        const uint32_t idesc = oz_idesc(it.M, it.N);
+        const int nf = it.kind == 1 ? 1 : it.fam_end - it.fam_begin;
+        for (int f = 0; f < nf && ok; ++f) {
+          const uint32_t buf = famc & 1u, use = famc >> 1;
+          if (!oz_wait(oz_smem(&tempty_bar[buf]), (use & 1u) ^ 1u, &abort_sh)) {
+            if (!abort_sh) oz_fail(&abort_sh, p.err);
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          const uint32_t dt = tmem + buf * 256u;
+          int sb, se;
+          if (it.kind == 1) {
+            sb = it.seg;
+            se = it.seg + 1;
+          } else {
+            const OzFam fm = p.fams[it.fam_begin + f];
+            sb = fm.seg_begin;
+            se = fm.seg_end;
+          }
+          bool first = true;
+          for (int sgi = sb; sgi < se && ok; ++sgi) {
+            const int nkb = p.segs[sgi].nkb;
+            for (int kb = 0; kb < nkb; ++kb) {
+              if (!oz_wait(oz_smem(&full_bar[stage]), ph, &abort_sh)) {
+                if (!abort_sh) oz_fail(&abort_sh, p.err);
+                ok = false;
+                break;
+              }
+              asm volatile("tcgen05.fence::after_thread_sync;");
+              const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE), sbb = sa + C::A_BYTES;
+#pragma unroll
+              for (int pa = 1; pa <= S; ++pa) {
+#pragma unroll
+                for (int qb = 1; pa + qb <= S + 1; ++qb) {
+                  const uint64_t da = oz_desc(sa + (uint32_t)(pa - 1) * 256u, 128u, S * 256u);
+                  const uint64_t db = oz_desc(sbb + (uint32_t)(qb - 1) * 256u, 128u, S * 256u);
+                  const uint32_t d = dt + (uint32_t)((pa + qb - 2) * BN);
+                  const uint32_t acc = (first && pa == 1) ? 0u : 1u;
+                  asm volatile(
+                      "{\n\t.reg .pred p;\n\t"
+                      "setp.ne.b32 p, %4, 0;\n\t"
+                      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                      :
+                      : "r"(d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+                }
+              }
+              issued = true;
+              oz_commit(oz_smem(&empty_bar[stage]));   // frees the stage when these MMAs finish
+              first = false;
+              if (++stage == ST) stage = 0, ph ^= 1u;
+            }
+          }
+          if (!ok) break;
+          oz_commit(oz_smem(&tfull_bar[buf]));
+          ++famc;
+        }
+      }
+      if (issued) {
+        // every MMA issued so far has finished before TMEM is released
+        oz_commit(oz_smem(&drain_bar));
+        oz_wait(oz_smem(&drain_bar), 0u, nullptr);
+      }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------ epilogue (warps 0-3)
+    uint32_t famc = 0;
+    double w[S];
+    {
+      double x = 1.0 / 16384.0;   // 128^-2
+#pragma unroll
+      for (int d = 0; d < S; ++d) {
+        w[d] = x;
+        x *= 1.0 / 128.0;
+      }
+    }
+    bool ok = true;
+    for (int ii = blockIdx.x; ii < p.nitems && ok; ii += gridDim.x) {
+      const OzItem it = p.items[ii];
+      // TMEM lane of this thread = 32*warp + lane; the tile row it holds:
+      //   M = 128: row = 32*warp + lane; M = 64: rows 16w..16w+15 in lanes 32w..32w+15
+      int r;
+      bool rv;
+      if (it.M == 128) {
+        r = tid;
+        rv = r < it.mrows;
+      } else {
+        r = warp * 16 + lane;
+        rv = lane < 16 && r < it.mrows;
+      }
+      const int nf = it.kind == 1 ? 1 : it.fam_end - it.fam_begin;
+      double *dst = nullptr;
+      int64_t cstride = 0;
+      double rscale_stack = 0.0;
+      int64_t pib = -1;   // kind 1: pi index of this row's product row `col0`
+      if (it.kind == 0) {
+        const OzCell c = p.cells[it.cell];
+        dst = p.out + c.off + (int64_t)(it.row0 + r) + (int64_t)it.col0 * c.ld;
+        cstride = c.ld;
+        if (it.init && rv) {
+          for (int n = 0; n < it.ncols; ++n) {
+            double v = 0.0;
+            for (int a = c.a_begin; a < c.a_end; ++a) {
+              const Task &t = p.tasks[a];
+              const double *b = t.L.space == SP_PSI ? p.psi : (t.L.space == SP_SCR ? p.scr : nullptr);
+              if (b) v += t.coef * b[t.L.off + (int64_t)(it.col0 + n) * t.L.ld + it.row0 + r];
+            }
+            dst[(int64_t)n * cstride] = v;
+          }
+        }
+      } else {
+        // stacked products: the run holding this row
+        int start = 0;
+        bool found = false;
+        for (int si = it.fam_begin; si < it.fam_end; ++si) {
+          const OzStack sk = p.stacks[si];
+          const int len = sk.a_ng * 8;
+          if (!found && r < start + len) {
+            const int jl = r - start;
+            found = true;
+            pib = sk.pi_idx + it.col0;
+            if (jl < sk.ncols) {
+              dst = p.scr + sk.dst_off + (int64_t)jl * sk.dst_ld + it.col0;
+              rscale_stack = oz_pow2_of(p.scales[sk.rs_idx + jl]);
+            } else {
+              rv = false;
+            }
+          }
+          start += len;
+        }
+        if (!found) rv = false;
+        cstride = 1;
+      }
+      for (int f = 0; f < nf; ++f) {
+        const uint32_t buf = famc & 1u, use = famc >> 1;
+        if (!oz_wait(oz_smem(&tfull_bar[buf]), use & 1u, &abort_sh)) {
+          if (!abort_sh) oz_fail(&abort_sh, p.err);
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        double rscale;
+        int64_t cs_idx;
+        if (it.kind == 0) {
+          const OzFam fm = p.fams[it.fam_begin + f];
+          rscale = rv ? oz_pow2_of(p.scales[fm.rs_idx + it.row0 + r]) : 0.0;
+          cs_idx = fm.cs_idx + it.col0;
+        } else {
+          rscale = rscale_stack;
+          cs_idx = it.cs_idx;
+        }
+        for (int j0 = 0; j0 < it.N; j0 += 16) {
+          uint32_t v[S][16];
+#pragma unroll
+          for (int d = 0; d < S; ++d) {
+            const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + buf * 256u + (uint32_t)(d * BN + j0);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(v[d][0]), "=r"(v[d][1]), "=r"(v[d][2]), "=r"(v[d][3]), "=r"(v[d][4]), "=r"(v[d][5]),
+                  "=r"(v[d][6]), "=r"(v[d][7]), "=r"(v[d][8]), "=r"(v[d][9]), "=r"(v[d][10]), "=r"(v[d][11]),
+                  "=r"(v[d][12]), "=r"(v[d][13]), "=r"(v[d][14]), "=r"(v[d][15])
+                : "r"(ta));
+          }
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int jj = 0; jj < 16; ++jj) {
+            const int n = j0 + jj;
+            double val = 0.0;
+            if (rv && n < it.ncols) {
+              double acc = 0.0;
+#pragma unroll
+              for (int d = S - 1; d >= 0; --d) acc += (double)(int32_t)v[d][jj] * w[d];
+              val = acc * rscale * oz_pow2_of(p.scales[cs_idx + n]);
+              if (it.kind == 0)
+                dst[(int64_t)n * cstride] += val;
+              else
+                dst[n] = val;
+            }
+            if (it.kind == 1) {
+              // pi: max |P(i, .)| over each 8-row group (one product), one atomic per group and column
+              double m = fabs(val);
+              for (int o = 1; o < 8; o <<= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+              if ((lane & 7) == 0 && pib >= 0 && n < it.ncols && m > 0.0)
+                atomicMax((unsigned long long *)&p.scales[pib + n], (unsigned long long)__double_as_longlong(m));
+            }
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        oz_arrive(oz_smem(&tempty_bar[buf]));
+        ++famc;
+      }
+    }
   }
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
-}
-
-// output cell = sum of task slots (in task order) + axpy terms
-struct OzSumParams {
-  const OzCellSum *sums;
-  const int64_t *slot_offs;
-  const double *slots;
-  const Task *tasks;
-  const double *ops, *psi, *scr;
-  double *out;
-};
-__global__ void oz_sum_kernel(OzSumParams p) {
-  const OzCellSum c = p.sums[blockIdx.x];
-  for (int idx = threadIdx.x; idx < c.M * c.N; idx += blockDim.x) {
-    const int i = idx % c.M, n = idx / c.M;
-    double v = 0.0;
-    for (int s = c.s_begin; s < c.s_end; ++s) v += p.slots[p.slot_offs[s] + (int64_t)n * c.M + i];
-    for (int a = c.a_begin; a < c.a_end; ++a) {
-      const Task &t = p.tasks[a];
-      const double *b = t.L.space == SP_OPS ? p.ops : (t.L.space == SP_PSI ? p.psi : p.scr);
-      v += t.coef * b[t.L.off + (int64_t)n * t.L.ld + i];
-    }
-    p.out[c.out_off + (int64_t)n * c.ld + i] = v;
-  }
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
 }
 
 // ------------------------------------------------------------ host launches
-void launch_oz_split(const OzSplit *jobs, int njobs, const double *ops, const double *psi, const double *scr,
-                     int8_t *pack, double *sig, int s, cudaStream_t st) {
+void launch_oz_max(const OzJob *jobs, int njobs, const double *ops, const double *psi, const double *scr,
+                   double *scales, cudaStream_t st) {
   if (njobs <= 0) return;
-  OzSplitParams p{jobs, ops, psi, scr, pack, sig, s};
-  oz_split_kernel<<<njobs, 256, 0, st>>>(p);
+  oz_max_kernel<<<njobs, 256, 0, st>>>(jobs, ops, psi, scr, scales);
 }
 
-template <int S, int BN>
-static cudaError_t launch_gemm_t(const OzGemmParams &p, int grid, cudaStream_t st) {
-  // at least 100 KB per CTA keeps two CTAs per SM, so their 2 x 256 TMEM
-  // columns never exceed the SM's 512 and no allocation has to wait
-  size_t smem = (size_t)S * (OZ_BM + BN) * OZ_KC;
-  if (smem < (100u << 10)) smem = 100u << 10;
-  cudaError_t e = cudaFuncSetAttribute(oz_gemm_kernel<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  oz_gemm_kernel<S, BN><<<grid, 128, smem, st>>>(p);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_oz_gemm(const int8_t *dyn_pack, const double *dyn_sig, const int8_t *sta_pack,
-                           const double *sta_sig, const OzGroup *groups, const OzRow *rows, const OzItem *items,
-                           int nitems, double *out_scr, double *out_slots, unsigned int *counter, int *err, int s,
-                           cudaStream_t st) {
-  if (nitems <= 0) return cudaSuccess;
-  OzGemmParams p{dyn_pack, dyn_sig, sta_pack, sta_sig, groups, rows, items, nitems, out_scr, out_slots, counter, err};
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = nitems < 2 * sms ? nitems : 2 * sms;
+void launch_oz_split(const OzJob *jobs, int njobs, const double *ops, const double *psi, const double *scr,
+                     const double *scales, uint8_t *pack, int s, cudaStream_t st) {
+  if (njobs <= 0) return;
   switch (s) {
-    case 3: return launch_gemm_t<3, 48>(p, grid, st);
-    case 4: return launch_gemm_t<4, 48>(p, grid, st);
-    case 5: return launch_gemm_t<5, 48>(p, grid, st);
-    case 6: return launch_gemm_t<6, 32>(p, grid, st);
-    case 7: return launch_gemm_t<7, 32>(p, grid, st);
-    case 8: return launch_gemm_t<8, 32>(p, grid, st);
-    default: return cudaErrorInvalidValue;
+    case 3: oz_split_kernel<3><<<njobs, 256, 0, st>>>(jobs, ops, psi, scr, scales, pack); break;
+    case 4: oz_split_kernel<4><<<njobs, 256, 0, st>>>(jobs, ops, psi, scr, scales, pack); break;
+    case 5: oz_split_kernel<5><<<njobs, 256, 0, st>>>(jobs, ops, psi, scr, scales, pack); break;
+    case 6: oz_split_kernel<6><<<njobs, 256, 0, st>>>(jobs, ops, psi, scr, scales, pack); break;
+    case 7: oz_split_kernel<7><<<njobs, 256, 0, st>>>(jobs, ops, psi, scr, scales, pack); break;
+    case 8: oz_split_kernel<8><<<njobs, 256, 0, st>>>(jobs, ops, psi, scr, scales, pack); break;
+    default: break;
   }
 }
 
-void launch_oz_sum(const OzCellSum *sums, int nsums, const int64_t *slot_offs, const double *slots,
-                   const Task *tasks, const double *ops, const double *psi, const double *scr, double *out,
-                   cudaStream_t st) {
-  if (nsums <= 0) return;
-  OzSumParams p{sums, slot_offs, slots, tasks, ops, psi, scr, out};
-  oz_sum_kernel<<<nsums, 256, 0, st>>>(p);
+template <int S, int BN>
+static cudaError_t launch_gemm_t(const OzGemmParams &p, cudaStream_t st) {
+  using Cf = OzCfg<S, BN>;
+  cudaError_t e = cudaFuncSetAttribute(oz_gemm_kernel<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cf::SMEM);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = p.nitems < sms ? p.nitems : sms;
+  oz_gemm_kernel<S, BN><<<grid, 192, Cf::SMEM, st>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_oz_gemm(const OzItem *items, int nitems, const OzSeg *segs, const OzFam *fams,
+                           const OzStack *stacks, const OzCell *cells, const Task *tasks, const uint8_t *pack,
+                           double *scales, const double *psi, double *scr, double *out, int *err, int s,
+                           cudaStream_t st) {
+  if (nitems <= 0) return cudaSuccess;
+  OzGemmParams p{items, nitems, segs, fams, stacks, cells, tasks, pack, scales, psi, scr, out, err};
+  switch (s) {
+    case 3: return launch_gemm_t<3, 48>(p, st);
+    case 4: return launch_gemm_t<4, 48>(p, st);
+    case 5: return launch_gemm_t<5, 48>(p, st);
+    case 6: return launch_gemm_t<6, 32>(p, st);
+    case 7: return launch_gemm_t<7, 32>(p, st);
+    case 8: return launch_gemm_t<8, 32>(p, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace tjb

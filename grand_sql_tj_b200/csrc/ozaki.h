@@ -1,18 +1,40 @@
 // Split-precision H*psi: Ozaki-style int8 slicing on the tcgen05 tensor cores.
 //
-// Every GEMM task Y = coef * op(L) * op(R) of the compiled H*psi is recast as
-// rows of one "group": a shared operand S (the operator sub-block the tasks
-// have in common, N rows x K) and a stack of rows of varying operands L_i
-// (each a length-K vector), so that a 128-row tcgen05 tile holds rows of many
-// small tasks:
+// Every matrix that enters a block GEMM is scaled row by row by a power of
+// two, x = 2^e * sum_{p=1..s} a_p 128^-p + tail, with truncated radix-128
+// digits a_p in [-127, 127] (the "slices").  The tensor cores form the exact
+// int32 sums D_d = sum_{p+q=d} A_p B_q^T for d <= s + 1, one TMEM accumulator
+// per diagonal d, and the epilogue forms 2^(e_row + e_col) sum_d 128^-d D_d
+// in FP64.
 //
-//   y_i[n] = coef_i * sum_k L_i[k] * S[n][k]
+// A sum of GEMMs sum_t L_t R_t becomes ONE integer accumulation over the
+// concatenated inner dimension when every L_t shares the row scales and every
+// R_t the column scales.  The tasks of an output cell fall into three
+// families that allow this:
 //
-// Each L_i and each S row is scaled by a power of two so that |x| < 1 and cut
-// into s int8 slices (truncating radix-128 digits), x = 2^e sum_p a_p 128^-p.
-// The tensor cores form the exact int32 products of slice pairs with
-// p + q <= s + 1, one TMEM accumulator per diagonal d = p + q; the epilogue
-// adds the diagonals with weights 128^-d in FP64 and applies the scales.
+//   left   Y += sum_t coef_t op(A_t) X_t   A: per-cell concat of coef_t op(A_t)
+//                                             (static, own row scales)
+//                                          B: columns of the psi cells X_t, scaled
+//                                             per env basis state (tau)
+//   right  Y += sum_t X_t coef_t op(R_t)   A: rows of psi cells, scaled per sys
+//                                             basis state (rho)
+//                                          B: per-cell concat of coef_t op(R_t)
+//   two    Y += sum_t P_t coef_t op(R_t)   A: rows of the phase-1 products P_t,
+//                                             scaled per sys basis state (pi)
+//                                          B: per-cell concat (static)
+//
+// Phase-1 products P_t = op(A_t) X_t are computed first with the rows of
+// P_t^T (columns of X_t, scale tau) stacked across products that share
+// op(A_t); their epilogue stores P in FP64 and raises pi.
+//
+// Split storage ("pack" pools, bytes): a split of R rows x K has
+// G = ceil(R / 8) row groups and nkb = ceil(K / 32) k-blocks, laid out
+//   [kb][g][slice p][c (2)][row r8 (8)][16 bytes]
+// so that any run of row groups of one k-block is one contiguous block of
+// (groups * s * 256) bytes, which lands in shared memory as the canonical
+// UMMA K-major, no-swizzle layout (core matrices of 8 rows x 16 bytes,
+// leading-byte offset 128 between the two K halves, stride-byte offset
+// s * 256 between row groups, slice p at +p * 256).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -23,83 +45,117 @@
 
 namespace tjb {
 
-constexpr int OZ_BM = 128;   // stacked rows per tile (tcgen05 M)
-// shared-operand rows per tile (tcgen05 N): s diagonal accumulators of BN
-// int32 columns must fit the 256 TMEM columns a CTA allocates
-inline int oz_bn(int s) { return s <= 5 ? 48 : 32; }
-constexpr int OZ_KC = 64;    // K bytes staged in shared memory per step (two k32 MMAs)
 constexpr int OZ_MAX_S = 8;
+// N tile (shared-operand rows): s diagonal accumulators of <= 256 int32
+// columns each, two TMEM buffers of 256 columns per CTA
+inline int oz_bn(int s) { return s <= 5 ? 48 : 32; }
 
-// A matrix cut into row slices: element (r, k) = src[off + r*rs + k*ks].
-struct OzSplit {
+// One split job: rows [0, nrows) x k [0, K) of coef * M, M(r, k) =
+// base[src_off + r*rs + k*ks], written to k-blocks [kb0, kb0 + ceil(K/32))
+// of the split at pack offset `dst` (gtot row groups); rows up to gtot*8 and
+// k up to the k-block boundary are written as zero digits.  The row scale is
+// scales[scale_idx + r] (max |value| of the row, made a power of two by the
+// kernels); want_max: this job contributes to that maximum.
+struct OzJob {
   int64_t src_off;
-  int64_t pack_off;   // byte offset of slice 0, row 0 in the pack pool
-  int64_t sig_off;    // index of row 0's scale in the scale pool
-  int32_t rs, ks;
-  int32_t nrows, K, K_pad;
-  int8_t space;       // SP_OPS / SP_PSI / SP_SCR
-  int8_t pad[3];
-};
-
-// A shared operand and its range of stacked rows in one GEMM launch.
-struct OzGroup {
-  int64_t s_pack_off;   // static pool: slice p, row n at s_pack_off + (p*N + n)*K_pad
-  int64_t tau_off;      // static scale pool index of row 0
-  int32_t N, K_pad;
-  int32_t row_begin, row_end;
-};
-
-// One stacked row: a row of a dynamic split and where its output goes.
-struct OzRow {
-  int64_t pack_off;     // dynamic pool byte offset of this row's slice 0
-  int64_t sig_idx;      // dynamic scale pool index
-  int64_t dst_off;      // output element offset
+  int64_t dst;
+  int64_t scale_idx;
   double coef;
-  int32_t slice_stride; // bytes between slices of this row
-  int32_t dst_stride;   // output element stride along n
-  int32_t dst_space;    // 0: phase-1 products (scratch), 1: task slots
+  int32_t rs, ks, nrows, K;
+  int32_t gtot, kb0;
+  int8_t space, want_max;
+  int8_t pad[6];
+};
+
+// One k-range of an operand pair: k-blocks [a_kb0, a_kb0 + nkb) of the A
+// split and [b_kb0, b_kb0 + nkb) of the B split.
+struct OzSeg {
+  int64_t a_base, b_base;   // pack offsets of the splits
+  int32_t a_gtot, b_gtot;   // their row-group counts
+  int32_t a_kb0, b_kb0, nkb;
   int32_t pad;
 };
 
-struct OzItem {
-  int32_t group, row0, n0, pad;
+// A family: segments accumulated in one TMEM buffer, then scaled by
+// scales[rs_idx + row] * scales[cs_idx + col].
+struct OzFam {
+  int32_t seg_begin, seg_end;
+  int64_t rs_idx, cs_idx;
 };
 
-// Output cell = sum of its tasks' slots (in task order) + axpy terms.
-struct OzCellSum {
-  int64_t out_off;
+// A run of stacked rows of a product tile: rows of P^T = columns
+// [8*a_g0, 8*a_g0 + ncols) of X_t, i.e. row groups [a_g0, a_g0 + a_ng) of
+// X_t's column split.
+struct OzStack {
+  int64_t a_base;           // psi column split of X_t
+  int64_t dst_off;          // P_t(0, 8*a_g0) in the product space
+  int64_t rs_idx;           // tau index of X_t's column 8*a_g0
+  int64_t pi_idx;           // pi index of P_t's row 0
+  int32_t a_gtot, a_g0, a_ng;
+  int32_t dst_ld;
+  int32_t ncols;            // valid rows of this run
+  int32_t pad;
+};
+
+// A work item: the output tile rows [row0, row0 + M) x cols [col0, col0 + N)
+//   kind 0 (cell):  of phase-2 cell `cell`; families [fam_begin, fam_end);
+//                   init = 1: the tile is written (axpy terms or zero), then
+//                   every family is added; init = 0: families are added
+//   kind 1 (stack): of the products stacked in [fam_begin, fam_end) of the
+//                   stack list, sharing the operator split `seg` (B side)
+struct OzItem {
+  int32_t kind, cell;
+  int32_t row0, col0;
+  int32_t M, N;             // M in {64, 128}; N multiple of 16, <= oz_bn(s)
+  int32_t mrows, ncols;     // valid rows / columns
+  int32_t fam_begin, fam_end;
+  int32_t seg;              // kind 1: the segment of the shared operator
+  int32_t init;
+  int64_t cs_idx;           // kind 1: scale index of the operator's row 0
+  int64_t pad2;
+  int64_t cost;             // issued int8 MACs (for ordering)
+};
+
+// Output cell of kind-0 items (phase-2 cell) with its axpy tasks.
+struct OzCell {
+  int64_t off;
   int32_t ld, M, N;
-  int32_t s_begin, s_end;   // range in the slot-offset list
-  int32_t a_begin, a_end;   // axpy tasks (indices into the H*psi phase-2 task list)
+  int32_t a_begin, a_end;   // axpy tasks in the phase-2 task list
+  int32_t pad;
 };
 
 struct OzPlan {
   int s = 5;
-  std::vector<OzSplit> sta;          // operator splits (once per DMRG step)
-  std::vector<OzSplit> dyn_a;        // psi splits for launch A
-  std::vector<OzSplit> dyn_b;        // product splits for launch B
-  int64_t sta_pack = 0, sta_sig = 0, dyn_pack = 0, dyn_sig = 0;
-  std::vector<OzGroup> groups_a, groups_b;
-  std::vector<OzRow> rows_a, rows_b;
-  std::vector<OzItem> items_a, items_b;
-  std::vector<OzCellSum> sums;
-  std::vector<int64_t> slot_offs;
-  int64_t slots_len = 0;             // doubles of task slots
-  double mma_ops = 0;                // int8 MACs * 2 per H*psi
+  int bn = 48;
+  // pools
+  int64_t sta_pack = 0, dyn_pack = 0;      // bytes (static part first in one buffer)
+  int64_t n_scales = 0;                    // doubles: static scales, then rho, tau, pi
+  int64_t dyn_scale_begin = 0;             // first dynamic scale (zeroed per H*psi)
+  int64_t rho0 = 0, tau0 = 0, pi0 = 0;
+  // jobs
+  std::vector<OzJob> sta_jobs;             // once per step
+  std::vector<OzJob> psi_jobs;             // per H*psi, before launch 1
+  std::vector<OzJob> prod_jobs;            // per H*psi, between the launches
+  // GEMM tables
+  std::vector<OzSeg> segs;
+  std::vector<OzFam> fams;
+  std::vector<OzStack> stacks;
+  std::vector<OzCell> cells;
+  std::vector<OzItem> items1, items2;      // launch 1 (products, left, right), launch 2 (two-sided)
+  double mma_ops = 0;                      // 2 x int8 MACs issued per H*psi
 };
 
 // Builds the split-precision form of an H*psi plan (host).
 void build_ozaki_plan(const HpsiPlan &hp, int s, OzPlan &oz);
 
 // device launches (ozaki.cu)
-void launch_oz_split(const OzSplit *jobs, int njobs, const double *ops, const double *psi, const double *scr,
-                     int8_t *pack, double *sig, int s, cudaStream_t st);
-cudaError_t launch_oz_gemm(const int8_t *dyn_pack, const double *dyn_sig, const int8_t *sta_pack,
-                           const double *sta_sig, const OzGroup *groups, const OzRow *rows, const OzItem *items,
-                           int nitems, double *out_scr, double *out_slots, unsigned int *counter, int *err, int s,
+void launch_oz_max(const OzJob *jobs, int njobs, const double *ops, const double *psi, const double *scr,
+                   double *scales, cudaStream_t st);
+void launch_oz_split(const OzJob *jobs, int njobs, const double *ops, const double *psi, const double *scr,
+                     const double *scales, uint8_t *pack, int s, cudaStream_t st);
+cudaError_t launch_oz_gemm(const OzItem *items, int nitems, const OzSeg *segs, const OzFam *fams,
+                           const OzStack *stacks, const OzCell *cells, const Task *tasks, const uint8_t *pack,
+                           double *scales, const double *psi, double *scr, double *out, int *err, int s,
                            cudaStream_t st);
-void launch_oz_sum(const OzCellSum *sums, int nsums, const int64_t *slot_offs, const double *slots,
-                   const Task *tasks, const double *ops, const double *psi, const double *scr, double *out,
-                   cudaStream_t st);
 
 }  // namespace tjb

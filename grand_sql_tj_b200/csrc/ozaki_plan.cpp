@@ -1,19 +1,19 @@
-// Host side of the split-precision H*psi: regroups the compiled tasks by the
-// operator sub-block they share and lays out the int8 slice pools.
+// Host side of the split-precision H*psi: turns the compiled FP64 task lists
+// into split jobs, per-cell K-concatenated families and tcgen05 work items
+// (the scheme and the storage layout are described in ozaki.h).
 //
-//   launch A  phase-1 products  P^T = X^T op(A)^T   rows: columns of X   S: rows of op(A)
-//             left-only tasks   Y^T = X^T op(A)^T   rows: columns of X   S: rows of op(A)
-//             right-only tasks  Y   = X op(R)       rows: rows of X      S: columns of op(R)
-//   (split the products P)
-//   launch B  two-sided tasks   Y   = P op(R)       rows: rows of P      S: columns of op(R)
-//   reduce    out(cell) = sum of the cell's task outputs + axpy terms
+//   once per step   sta_jobs: operator splits (phase-1 operators, per-cell
+//                   concatenations of coef * op(.)), with their own row scales
+//   per H*psi       zero rho/tau/pi; psi_jobs (max, then split): psi column
+//                   splits (tau) and row splits (rho); launch 1 (products,
+//                   left and right families); prod_jobs: product row splits
+//                   (pi, raised by launch 1); launch 2 (two-sided families)
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <stdexcept>
-#include <tuple>
-
-#include <cstring>
 #include <string>
+#include <unordered_map>
 
 #include "ozaki.h"
 #include "tj_b200.h"
@@ -22,190 +22,422 @@ namespace tjb {
 
 namespace {
 
-inline int32_t pad32(int32_t k) { return (k + 31) / 32 * 32; }
+inline int32_t cdiv(int64_t a, int64_t b) { return (int32_t)((a + b - 1) / b); }
+
+// Which dynamic scale pool an index is relative to while building.
+enum { REL_NONE = -1, REL_RHO = 0, REL_TAU = 1, REL_PI = 2 };
 
 struct Builder {
   const HpsiPlan &hp;
   OzPlan &oz;
-  std::map<std::tuple<int64_t, int, int>, int> sta_idx;   // (off, trans, role) -> static split
-  std::map<std::pair<int64_t, int>, int> dyn_a_idx;       // (cell offset, kind) -> dynamic split
-  std::map<int64_t, int> dyn_b_idx;                        // product offset -> dynamic split
+  int S;
+  int64_t sta_bytes = 0, dyn_bytes = 0;
+  std::vector<OzJob> dyn_psi, dyn_prod;
+  std::vector<int> dyn_psi_rel;                 // REL_RHO / REL_TAU per psi job
+  std::unordered_map<int64_t, int> psi_cell;    // psi offset -> phase-2 cell
+  std::unordered_map<int64_t, int> prod_of;     // scratch offset -> product
+  std::vector<int64_t> colsplit, rowsplit;      // per psi cell: dynamic pack offset or -1
+  std::vector<int64_t> prodsplit;               // per product
+  std::vector<int> seg_dyn_a, seg_dyn_b;        // segments with a dynamic A / B split
+  struct FamRel { int fam, rs_rel, cs_rel; };
+  std::vector<FamRel> famrel;
 
-  Builder(const HpsiPlan &h, OzPlan &o) : hp(h), oz(o) {}
+  Builder(const HpsiPlan &h, OzPlan &o, int s) : hp(h), oz(o), S(s) {}
 
-  int add_split(std::vector<OzSplit> &v, int64_t &pack, int64_t &sig, int8_t space, int64_t off, int32_t rs,
-                int32_t ks, int32_t nrows, int32_t K) {
-    if (K < 1 || nrows < 1) throw std::runtime_error("empty split");
-    OzSplit s;
-    s.src_off = off;
-    s.rs = rs;
-    s.ks = ks;
-    s.nrows = nrows;
-    s.K = K;
-    s.K_pad = pad32(K);
-    s.space = space;
-    s.pad[0] = s.pad[1] = s.pad[2] = 0;
-    s.pack_off = pack;
-    s.sig_off = sig;
-    pack += (int64_t)oz.s * nrows * s.K_pad;
-    sig += nrows;
-    v.push_back(s);
-    return (int)v.size() - 1;
+  int64_t split_bytes(int32_t rows, int32_t K) const { return (int64_t)cdiv(K, 32) * cdiv(rows, 8) * S * 256; }
+  static int64_t align256(int64_t x) { return (x + 255) / 256 * 256; }
+  int64_t alloc_sta(int32_t rows, int32_t K) {
+    const int64_t o = sta_bytes;
+    sta_bytes = align256(sta_bytes + split_bytes(rows, K));
+    return o;
   }
-  // Shared operand from op(M): role 0 = rows of op(M), role 1 = columns of op(M).
-  int static_split(const Operand &o, int rows, int cols, int role) {
-    auto key = std::make_tuple(o.off, (int)o.trans, role);
-    auto it = sta_idx.find(key);
-    if (it != sta_idx.end()) return it->second;
-    int32_t rs, ks, nr, K;
-    if (role == 0) {   // row r of op(M), k along the row
-      rs = o.trans ? o.ld : 1;
-      ks = o.trans ? 1 : o.ld;
-      nr = rows;
-      K = cols;
-    } else {           // column n of op(M), k down the column
-      rs = o.trans ? 1 : o.ld;
-      ks = o.trans ? o.ld : 1;
-      nr = cols;
-      K = rows;
-    }
-    int id = add_split(oz.sta, oz.sta_pack, oz.sta_sig, SP_OPS, o.off, rs, ks, nr, K);
-    sta_idx[key] = id;
-    return id;
+  int64_t alloc_dyn(int32_t rows, int32_t K) {
+    const int64_t o = dyn_bytes;
+    dyn_bytes = align256(dyn_bytes + split_bytes(rows, K));
+    return o;
   }
-  // psi cell as the varying operand: kind 0 = its columns (X^T rows), kind 1 = its rows.
-  int psi_split(const Operand &x, int M, int N, int kind) {
+  int64_t alloc_scales(int64_t n) {
+    const int64_t o = oz.n_scales;
+    oz.n_scales += n;
+    return o;
+  }
+
+  static OzJob job(int8_t space, int64_t src_off, int32_t rs, int32_t ks, int32_t nrows, int32_t K, double coef,
+                   int64_t dst, int32_t gtot, int32_t kb0, int64_t scale_idx, bool want_max) {
+    if (nrows < 1 || K < 1) throw std::runtime_error("empty split");
+    OzJob j;
+    std::memset(&j, 0, sizeof j);
+    j.src_off = src_off;
+    j.dst = dst;
+    j.scale_idx = scale_idx;
+    j.coef = coef;
+    j.rs = rs;
+    j.ks = ks;
+    j.nrows = nrows;
+    j.K = K;
+    j.gtot = gtot;
+    j.kb0 = kb0;
+    j.space = space;
+    j.want_max = want_max ? 1 : 0;
+    return j;
+  }
+  // Split rows of op(M) (role 0) or of op(M)^T (role 1): element (r, k) at
+  // src + r*rs + k*ks.
+  static void strides(const Operand &o, int role, int32_t &rs, int32_t &ks) {
+    const bool t = (o.trans != 0) ^ (role == 1);
+    rs = t ? o.ld : 1;
+    ks = t ? 1 : o.ld;
+  }
+
+  int psi_index(const Operand &x) const {
     if (x.space != SP_PSI || x.trans) throw std::runtime_error("psi operand is not a plain cell");
-    auto key = std::make_pair(x.off, kind);
-    auto it = dyn_a_idx.find(key);
-    if (it != dyn_a_idx.end()) return it->second;
-    int id = kind == 0 ? add_split(oz.dyn_a, oz.dyn_pack, oz.dyn_sig, SP_PSI, x.off, x.ld, 1, N, M)
-                       : add_split(oz.dyn_a, oz.dyn_pack, oz.dyn_sig, SP_PSI, x.off, 1, x.ld, M, N);
-    dyn_a_idx[key] = id;
-    return id;
+    auto it = psi_cell.find(x.off);
+    if (it == psi_cell.end()) throw std::runtime_error("psi operand is not a cell");
+    return it->second;
   }
-  int prod_split(const Operand &p, int M, int N) {
-    if (p.space != SP_SCR || p.trans) throw std::runtime_error("product operand is not a plain scratch cell");
-    auto it = dyn_b_idx.find(p.off);
-    if (it != dyn_b_idx.end()) return it->second;
-    int id = add_split(oz.dyn_b, oz.dyn_pack, oz.dyn_sig, SP_SCR, p.off, 1, p.ld, M, N);
-    dyn_b_idx[p.off] = id;
-    return id;
-  }
-
-  // rows of one launch, grouped by their static split
-  struct PendingRow {
-    int dyn;          // dynamic split
-    int row;          // row within it
-    int64_t dst_off;
-    int32_t dst_stride, dst_space;
-    double coef;
-  };
-  std::map<int, std::vector<PendingRow>> pend_a, pend_b;
-
-  void emit_rows(std::map<int, std::vector<PendingRow>> &pend, int sta, int dyn, int nrows, int64_t dst_base,
-                 int32_t row_step, int32_t dst_stride, int32_t dst_space, double coef) {
-    auto &v = pend[sta];
-    for (int r = 0; r < nrows; ++r) v.push_back(PendingRow{dyn, r, dst_base + (int64_t)r * row_step, dst_stride, dst_space, coef});
-  }
-
-  void finish(std::map<int, std::vector<PendingRow>> &pend, const std::vector<OzSplit> &dyn, std::vector<OzGroup> &groups,
-              std::vector<OzRow> &rows, std::vector<OzItem> &items) {
-    for (auto &kv : pend) {
-      const OzSplit &S = oz.sta[kv.first];
-      OzGroup g;
-      g.s_pack_off = S.pack_off;
-      g.tau_off = S.sig_off;
-      g.N = S.nrows;
-      g.K_pad = S.K_pad;
-      g.row_begin = (int32_t)rows.size();
-      for (const PendingRow &p : kv.second) {
-        const OzSplit &D = dyn[p.dyn];
-        if (D.K_pad != S.K_pad) throw std::runtime_error("inner dimensions differ");
-        // exact int32 accumulation: every diagonal sums at most s slice products of 127^2 per k
-        if ((double)S.K_pad * oz.s * 127.0 * 127.0 >= 2147483647.0)
-          throw std::runtime_error("inner dimension too large for int32 accumulation");
-        OzRow r;
-        r.pack_off = D.pack_off + (int64_t)p.row * D.K_pad;
-        r.sig_idx = D.sig_off + p.row;
-        r.dst_off = p.dst_off;
-        r.coef = p.coef;
-        r.slice_stride = D.nrows * D.K_pad;
-        r.dst_stride = p.dst_stride;
-        r.dst_space = p.dst_space;
-        r.pad = 0;
-        rows.push_back(r);
-      }
-      g.row_end = (int32_t)rows.size();
-      const int gi = (int)groups.size();
-      groups.push_back(g);
-      const int bn = oz_bn(oz.s);
-      for (int r0 = 0; r0 < g.row_end - g.row_begin; r0 += OZ_BM)
-        for (int n0 = 0; n0 < g.N; n0 += bn) {
-          items.push_back(OzItem{gi, r0, n0, 0});
-          oz.mma_ops += 2.0 * OZ_BM * bn * (double)g.K_pad * (oz.s * (oz.s + 1) / 2);
-        }
+  // psi cell c as a B operand: rows = its columns (scale tau), K = its rows
+  int64_t psi_col(int c) {
+    if (colsplit[c] < 0) {
+      const Cell &x = hp.cells2[c];
+      colsplit[c] = alloc_dyn(x.N, x.M);
+      dyn_psi.push_back(job(SP_PSI, x.off, x.ld, 1, x.N, x.M, 1.0, colsplit[c], cdiv(x.N, 8), 0,
+                            hp.cell2_col_state[c], true));
+      dyn_psi_rel.push_back(REL_TAU);
     }
+    return colsplit[c];
+  }
+  // psi cell c as an A operand: rows = its rows (scale rho), K = its columns
+  int64_t psi_row(int c) {
+    if (rowsplit[c] < 0) {
+      const Cell &x = hp.cells2[c];
+      rowsplit[c] = alloc_dyn(x.M, x.N);
+      dyn_psi.push_back(job(SP_PSI, x.off, 1, x.ld, x.M, x.N, 1.0, rowsplit[c], cdiv(x.M, 8), 0,
+                            hp.cell2_row_state[c], true));
+      dyn_psi_rel.push_back(REL_RHO);
+    }
+    return rowsplit[c];
+  }
+  // phase-1 product p as an A operand: rows = its rows (scale pi), K = its columns
+  int64_t prod_row(int p) {
+    if (prodsplit[p] < 0) {
+      const Cell &P = hp.cells1[p];
+      prodsplit[p] = alloc_dyn(P.M, P.N);
+      dyn_prod.push_back(job(SP_SCR, P.off, 1, P.ld, P.M, P.N, 1.0, prodsplit[p], cdiv(P.M, 8), 0,
+                             hp.cell1_row_state[p], false));
+    }
+    return prodsplit[p];
   }
 
-  void build() {
-    // launch A: phase-1 products
+  int64_t item_cost(const OzItem &it, int64_t kbs) const {
+    return (int64_t)it.M * it.N * 32 * kbs * (S * (S + 1) / 2);
+  }
+
+  void products() {
+    const int BN = oz.bn;
+    std::map<std::pair<int64_t, int>, std::vector<int>> by_op;
     for (size_t p = 0; p < hp.cells1.size(); ++p) {
       const Cell &c = hp.cells1[p];
       if (c.t_end != c.t_begin + 1) throw std::runtime_error("phase-1 cell with more than one task");
       const Task &t = hp.tasks1[c.t_begin];
-      if (t.L.space != SP_OPS) throw std::runtime_error("phase-1 task without an operator");
-      const int sta = static_split(t.L, c.M, t.K, 0);       // rows of op(A): M x K
-      const int dyn = psi_split(t.R, t.K, c.N, 0);          // columns of X (K x N)
-      // row n of P^T (= column n of P) -> P(a, n) at off + n*ld + a
-      emit_rows(pend_a, sta, dyn, c.N, c.off, c.ld, 1, 0, t.coef);
+      if (t.L.space != SP_OPS || t.coef != 1.0) throw std::runtime_error("unexpected phase-1 task");
+      by_op[{t.L.off, (int)t.L.trans}].push_back((int)p);
     }
-    // phase-2 tasks: slots and rows
-    for (size_t ci = 0; ci < hp.cells2.size(); ++ci) {
+    for (auto &kv : by_op) {
+      const std::vector<int> &prods = kv.second;
+      const Cell &c0 = hp.cells1[prods[0]];
+      const Task &t0 = hp.tasks1[c0.t_begin];
+      const int32_t Mop = c0.M, K = t0.K;
+      int32_t rs, ks;
+      strides(t0.L, 0, rs, ks);
+      const int64_t pk = alloc_sta(Mop, K);
+      const int64_t sc = alloc_scales(Mop);
+      oz.sta_jobs.push_back(job(SP_OPS, t0.L.off, rs, ks, Mop, K, 1.0, pk, cdiv(Mop, 8), 0, sc, true));
+      OzSeg sg;
+      std::memset(&sg, 0, sizeof sg);
+      sg.a_base = -1;   // the stacks carry the A side
+      sg.b_base = pk;
+      sg.b_gtot = cdiv(Mop, 8);
+      sg.nkb = cdiv(K, 32);
+      const int seg = (int)oz.segs.size();
+      oz.segs.push_back(sg);
+      // runs of <= 16 row groups of the operands' column splits
+      std::vector<OzStack> runs;
+      for (int p : prods) {
+        const Cell &c = hp.cells1[p];
+        const Task &t = hp.tasks1[c.t_begin];
+        if (c.M != Mop || t.K != K) throw std::runtime_error("products of one operator differ in shape");
+        const int x = psi_index(t.R);
+        const Cell &X = hp.cells2[x];
+        if (X.M != K || X.N != c.N) throw std::runtime_error("product operand shape");
+        const int64_t cs = psi_col(x);
+        const int32_t G = cdiv(X.N, 8);
+        for (int32_t g0 = 0; g0 < G; g0 += 16) {
+          OzStack r;
+          std::memset(&r, 0, sizeof r);
+          r.a_base = cs;   // dynamic-relative
+          r.a_gtot = G;
+          r.a_g0 = g0;
+          r.a_ng = std::min(16, G - g0);
+          r.dst_off = c.off + (int64_t)8 * g0 * c.ld;
+          r.dst_ld = c.ld;
+          r.ncols = std::min(8 * r.a_ng, X.N - 8 * g0);
+          r.rs_idx = hp.cell2_col_state[x] + 8 * g0;   // tau-relative
+          r.pi_idx = hp.cell1_row_state[p];             // pi-relative
+          runs.push_back(r);
+        }
+      }
+      size_t i = 0;
+      while (i < runs.size()) {
+        int32_t groups = 0;
+        const int fb = (int)oz.stacks.size();
+        while (i < runs.size() && groups + runs[i].a_ng <= 16) {
+          groups += runs[i].a_ng;
+          oz.stacks.push_back(runs[i]);
+          ++i;
+        }
+        const int fe = (int)oz.stacks.size();
+        for (int32_t n0 = 0; n0 < Mop; n0 += BN) {
+          OzItem it;
+          std::memset(&it, 0, sizeof it);
+          it.kind = 1;
+          it.cell = -1;
+          it.row0 = 0;
+          it.col0 = n0;
+          it.mrows = groups * 8;
+          it.M = it.mrows <= 64 ? 64 : 128;
+          it.ncols = std::min(BN, Mop - n0);
+          it.N = std::min(BN, (it.ncols + 15) / 16 * 16);
+          it.fam_begin = fb;
+          it.fam_end = fe;
+          it.seg = seg;
+          it.init = 1;
+          it.cs_idx = sc + n0;
+          it.cost = item_cost(it, sg.nkb);
+          oz.items1.push_back(it);
+        }
+      }
+    }
+  }
+
+  // A family of tasks that share the B side's concatenation (right: psi rows,
+  // two-sided: product rows).
+  int right_family(const Cell &c, int64_t ci, const std::vector<int> &tl, bool prods) {
+    const int32_t GM = cdiv(c.M, 8), GN = cdiv(c.N, 8);
+    int32_t kbt = 0;
+    for (int ti : tl) kbt += cdiv(hp.tasks2[ti].K, 32);
+    const int64_t pk = alloc_sta(c.N, 32 * kbt);
+    const int64_t sc = alloc_scales(c.N);
+    OzFam f;
+    f.seg_begin = (int)oz.segs.size();
+    int32_t kb = 0;
+    for (int ti : tl) {
+      const Task &t = hp.tasks2[ti];
+      int32_t rs, ks;
+      strides(t.R, 1, rs, ks);
+      oz.sta_jobs.push_back(job(SP_OPS, t.R.off, rs, ks, c.N, t.K, t.coef, pk, GN, kb, sc, true));
+      OzSeg sg;
+      std::memset(&sg, 0, sizeof sg);
+      if (!prods) {
+        const int x = psi_index(t.L);
+        const Cell &X = hp.cells2[x];
+        if (X.M != c.M || X.N != t.K || hp.cell2_row_state[x] != hp.cell2_row_state[ci])
+          throw std::runtime_error("right task operand shape");
+        sg.a_base = psi_row(x);
+      } else {
+        if (t.L.trans || t.L.space != SP_SCR) throw std::runtime_error("product operand is not a plain product");
+        auto it = prod_of.find(t.L.off);
+        if (it == prod_of.end()) throw std::runtime_error("product operand is not a product");
+        const int p = it->second;
+        const Cell &P = hp.cells1[p];
+        if (P.M != c.M || P.N != t.K || hp.cell1_row_state[p] != hp.cell2_row_state[ci])
+          throw std::runtime_error("two-sided task operand shape");
+        sg.a_base = prod_row(p);
+      }
+      sg.a_gtot = GM;
+      sg.a_kb0 = 0;
+      sg.b_base = pk;
+      sg.b_gtot = GN;
+      sg.b_kb0 = kb;
+      sg.nkb = cdiv(t.K, 32);
+      seg_dyn_a.push_back((int)oz.segs.size());
+      oz.segs.push_back(sg);
+      kb += sg.nkb;
+    }
+    f.seg_end = (int)oz.segs.size();
+    f.rs_idx = hp.cell2_row_state[ci];
+    f.cs_idx = sc;
+    const int fi = (int)oz.fams.size();
+    famrel.push_back({fi, prods ? REL_PI : REL_RHO, REL_NONE});
+    oz.fams.push_back(f);
+    return fi;
+  }
+
+  int left_family(const Cell &c, int64_t ci, const std::vector<int> &tl) {
+    const int32_t GM = cdiv(c.M, 8), GN = cdiv(c.N, 8);
+    int32_t kbt = 0;
+    for (int ti : tl) kbt += cdiv(hp.tasks2[ti].K, 32);
+    const int64_t pk = alloc_sta(c.M, 32 * kbt);
+    const int64_t sc = alloc_scales(c.M);
+    OzFam f;
+    f.seg_begin = (int)oz.segs.size();
+    int32_t kb = 0;
+    for (int ti : tl) {
+      const Task &t = hp.tasks2[ti];
+      int32_t rs, ks;
+      strides(t.L, 0, rs, ks);
+      oz.sta_jobs.push_back(job(SP_OPS, t.L.off, rs, ks, c.M, t.K, t.coef, pk, GM, kb, sc, true));
+      const int x = psi_index(t.R);
+      const Cell &X = hp.cells2[x];
+      if (X.M != t.K || X.N != c.N || hp.cell2_col_state[x] != hp.cell2_col_state[ci])
+        throw std::runtime_error("left task operand shape");
+      OzSeg sg;
+      std::memset(&sg, 0, sizeof sg);
+      sg.a_base = pk;
+      sg.a_gtot = GM;
+      sg.a_kb0 = kb;
+      sg.b_base = psi_col(x);
+      sg.b_gtot = GN;
+      sg.b_kb0 = 0;
+      sg.nkb = cdiv(t.K, 32);
+      seg_dyn_b.push_back((int)oz.segs.size());
+      oz.segs.push_back(sg);
+      kb += sg.nkb;
+    }
+    f.seg_end = (int)oz.segs.size();
+    f.rs_idx = sc;
+    f.cs_idx = hp.cell2_col_state[ci];
+    const int fi = (int)oz.fams.size();
+    famrel.push_back({fi, REL_NONE, REL_TAU});
+    oz.fams.push_back(f);
+    return fi;
+  }
+
+  void add_items(std::vector<OzItem> &dst, const Cell &c, int cell_idx, int fb, int fe, int init) {
+    const int BN = oz.bn;
+    int64_t kbs = 0;
+    for (int f = fb; f < fe; ++f)
+      for (int sgi = oz.fams[f].seg_begin; sgi < oz.fams[f].seg_end; ++sgi) kbs += oz.segs[sgi].nkb;
+    for (int32_t r0 = 0; r0 < c.M; r0 += 128)
+      for (int32_t n0 = 0; n0 < c.N; n0 += BN) {
+        OzItem it;
+        std::memset(&it, 0, sizeof it);
+        it.kind = 0;
+        it.cell = cell_idx;
+        it.row0 = r0;
+        it.col0 = n0;
+        it.mrows = std::min(128, c.M - r0);
+        it.M = it.mrows <= 64 ? 64 : 128;
+        it.ncols = std::min(BN, c.N - n0);
+        it.N = std::min(BN, (it.ncols + 15) / 16 * 16);
+        it.fam_begin = fb;
+        it.fam_end = fe;
+        it.seg = -1;
+        it.init = init;
+        it.cost = item_cost(it, kbs);
+        dst.push_back(it);
+      }
+  }
+
+  void cells() {
+    const int64_t npsi = (int64_t)hp.cells2.size();
+    for (int64_t ci = 0; ci < npsi; ++ci) {
       const Cell &c = hp.cells2[ci];
-      OzCellSum cs;
-      cs.out_off = c.off;
-      cs.ld = c.ld;
-      cs.M = c.M;
-      cs.N = c.N;
-      cs.s_begin = (int32_t)oz.slot_offs.size();
-      cs.a_begin = cs.a_end = c.t_end;
+      OzCell oc;
+      std::memset(&oc, 0, sizeof oc);
+      oc.off = c.off;
+      oc.ld = c.ld;
+      oc.M = c.M;
+      oc.N = c.N;
+      oc.a_begin = oc.a_end = c.t_end;
+      std::vector<int> left, right, two;
       for (int ti = c.t_begin; ti < c.t_end; ++ti) {
         const Task &t = hp.tasks2[ti];
         if (t.R.space == SP_NONE) {
-          if (t.L.trans) throw std::runtime_error("transposed axpy operand");
-          if (cs.a_begin == c.t_end) cs.a_begin = ti;
+          if (t.L.trans || t.L.space != SP_PSI) throw std::runtime_error("axpy operand is not a psi cell");
+          if (oc.a_begin == c.t_end) oc.a_begin = ti;
           continue;
         }
-        const int64_t slot = oz.slots_len;
-        oz.slots_len += ((int64_t)c.M * c.N + 3) / 4 * 4;
-        oz.slot_offs.push_back(slot);
-        if (t.L.space == SP_OPS) {            // op(A) X: Y^T = X^T op(A)^T
-          const int sta = static_split(t.L, c.M, t.K, 0);
-          const int dyn = psi_split(t.R, t.K, c.N, 0);
-          emit_rows(pend_a, sta, dyn, c.N, slot, c.M, 1, 1, t.coef);
-        } else if (t.L.space == SP_PSI) {     // X op(R)
-          const int sta = static_split(t.R, t.K, c.N, 1);
-          const int dyn = psi_split(t.L, c.M, t.K, 1);
-          emit_rows(pend_a, sta, dyn, c.M, slot, 1, c.M, 1, t.coef);
-        } else {                              // P op(R)
-          const int sta = static_split(t.R, t.K, c.N, 1);
-          const int dyn = prod_split(t.L, c.M, t.K);
-          emit_rows(pend_b, sta, dyn, c.M, slot, 1, c.M, 1, t.coef);
-        }
+        if (t.L.space == SP_OPS) left.push_back(ti);
+        else if (t.L.space == SP_PSI) right.push_back(ti);
+        else if (t.L.space == SP_SCR) two.push_back(ti);
+        else throw std::runtime_error("unknown task form");
       }
-      cs.s_end = (int32_t)oz.slot_offs.size();
-      cs.a_end = c.t_end;
-      oz.sums.push_back(cs);
+      if (oc.a_begin != c.t_end) oc.a_end = c.t_end;
+      const int cell_idx = (int)oz.cells.size();
+      oz.cells.push_back(oc);
+      if (c.M <= 0 || c.N <= 0) continue;
+      const int fl = left.empty() ? -1 : left_family(c, ci, left);
+      const int fr = right.empty() ? -1 : right_family(c, ci, right, false);
+      const int f2 = two.empty() ? -1 : right_family(c, ci, two, true);
+      // launch 1: the left and right families (adjacent in the list) or none
+      int fb = 0, fe = 0;
+      if (fl >= 0 || fr >= 0) {
+        fb = fl >= 0 ? fl : fr;
+        fe = (fr >= 0 ? fr : fl) + 1;
+      }
+      add_items(oz.items1, c, cell_idx, fb, fe, 1);
+      if (f2 >= 0) add_items(oz.items2, c, cell_idx, f2, f2 + 1, 0);
     }
-    finish(pend_a, oz.dyn_a, oz.groups_a, oz.rows_a, oz.items_a);
-    finish(pend_b, oz.dyn_b, oz.groups_b, oz.rows_b, oz.items_b);
-    auto by_k = [&](std::vector<OzItem> &items, const std::vector<OzGroup> &g) {
-      std::stable_sort(items.begin(), items.end(),
-                       [&](const OzItem &a, const OzItem &b) { return g[a.group].K_pad > g[b.group].K_pad; });
+  }
+
+  void finish() {
+    oz.sta_pack = sta_bytes;
+    oz.dyn_pack = dyn_bytes;
+    const int64_t dbase = sta_bytes;
+    for (OzJob &j : dyn_psi) j.dst += dbase;
+    for (OzJob &j : dyn_prod) j.dst += dbase;
+    for (OzStack &r : oz.stacks) r.a_base += dbase;
+    for (int i : seg_dyn_a) oz.segs[i].a_base += dbase;
+    for (int i : seg_dyn_b) oz.segs[i].b_base += dbase;
+    // scale pool: static scales, then rho, tau, pi
+    oz.dyn_scale_begin = oz.n_scales;
+    oz.rho0 = oz.n_scales;
+    oz.tau0 = oz.rho0 + hp.n_sys_states;
+    oz.pi0 = oz.tau0 + hp.n_env_states;
+    oz.n_scales = oz.pi0 + hp.n_sys_states;
+    const int64_t base[3] = {oz.rho0, oz.tau0, oz.pi0};
+    for (size_t i = 0; i < dyn_psi.size(); ++i) dyn_psi[i].scale_idx += base[dyn_psi_rel[i]];
+    for (OzJob &j : dyn_prod) j.scale_idx += oz.pi0;
+    for (OzStack &r : oz.stacks) {
+      r.rs_idx += oz.tau0;
+      r.pi_idx += oz.pi0;
+    }
+    for (const FamRel &fr : famrel) {
+      OzFam &f = oz.fams[fr.fam];
+      if (fr.rs_rel != REL_NONE) f.rs_idx += base[fr.rs_rel];
+      if (fr.cs_rel != REL_NONE) f.cs_idx += base[fr.cs_rel];
+    }
+    oz.psi_jobs = std::move(dyn_psi);
+    oz.prod_jobs = std::move(dyn_prod);
+    auto by_cost = [](std::vector<OzItem> &v) {
+      std::stable_sort(v.begin(), v.end(), [](const OzItem &a, const OzItem &b) { return a.cost > b.cost; });
     };
-    by_k(oz.items_a, oz.groups_a);
-    by_k(oz.items_b, oz.groups_b);
+    by_cost(oz.items1);
+    by_cost(oz.items2);
+    oz.mma_ops = 0;
+    int64_t kmax = 0;
+    for (const std::vector<OzItem> *v : {&oz.items1, &oz.items2})
+      for (const OzItem &it : *v) {
+        oz.mma_ops += 2.0 * it.cost;
+        kmax = std::max<int64_t>(kmax, it.cost / ((int64_t)it.M * it.N * (S * (S + 1) / 2)));
+      }
+    // exact int32 accumulation: a diagonal sums <= s slice products of 127^2 per k
+    if ((double)kmax * S * 127.0 * 127.0 >= 2147483647.0)
+      throw std::runtime_error("inner dimension too large for int32 accumulation");
+  }
+
+  void build() {
+    const int64_t npsi = (int64_t)hp.cells2.size();
+    if (hp.cell2_row_state.size() != hp.cells2.size() || hp.cell1_row_state.size() != hp.cells1.size())
+      throw std::runtime_error("plan without basis-state tables");
+    for (int64_t c = 0; c < npsi; ++c) psi_cell[hp.cells2[c].off] = (int)c;
+    for (size_t p = 0; p < hp.cells1.size(); ++p) prod_of[hp.cells1[p].off] = (int)p;
+    colsplit.assign(npsi, -1);
+    rowsplit.assign(npsi, -1);
+    prodsplit.assign(hp.cells1.size(), -1);
+    products();
+    cells();
+    finish();
   }
 };
 
@@ -215,15 +447,17 @@ void build_ozaki_plan(const HpsiPlan &hp, int s, OzPlan &oz) {
   if (s < 3 || s > OZ_MAX_S) throw std::runtime_error("slices must be in 3..8");
   oz = OzPlan();
   oz.s = s;
-  Builder b(hp, oz);
+  oz.bn = oz_bn(s);
+  Builder b(hp, oz, s);
   b.build();
 }
 
-static_assert(sizeof(OzSplit) == sizeof(tj_oz_split), "split layout");
-static_assert(sizeof(OzGroup) == sizeof(tj_oz_group), "group layout");
-static_assert(sizeof(OzRow) == sizeof(tj_oz_row), "row layout");
+static_assert(sizeof(OzJob) == sizeof(tj_oz_job), "job layout");
+static_assert(sizeof(OzSeg) == sizeof(tj_oz_seg), "segment layout");
+static_assert(sizeof(OzFam) == sizeof(tj_oz_fam), "family layout");
+static_assert(sizeof(OzStack) == sizeof(tj_oz_stack), "stack layout");
 static_assert(sizeof(OzItem) == sizeof(tj_oz_item), "item layout");
-static_assert(sizeof(OzCellSum) == sizeof(tj_oz_cell_sum), "cell-sum layout");
+static_assert(sizeof(OzCell) == sizeof(tj_oz_cell), "cell layout");
 
 }  // namespace tjb
 
@@ -244,29 +478,26 @@ extern "C" int tj_ozaki_plan_export(const tj_lattice *lat, const tj_model *sys, 
     return tjb_set_err(TJ_ERR_ARG, std::string("split-precision plan: ") + e.what());
   }
   out->slices = oz.s;
-  out->tile_m = tjb::OZ_BM;
-  out->tile_n = tjb::oz_bn(oz.s);
-  out->pad_ = 0;
+  out->tile_n = oz.bn;
   out->sta_pack = oz.sta_pack;
-  out->sta_sig = oz.sta_sig;
   out->dyn_pack = oz.dyn_pack;
-  out->dyn_sig = oz.dyn_sig;
-  out->slots_len = oz.slots_len;
+  out->n_scales = oz.n_scales;
+  out->rho0 = oz.rho0;
+  out->tau0 = oz.tau0;
+  out->pi0 = oz.pi0;
   out->int8_ops = oz.mma_ops;
   auto put = [](auto *dst, const auto &v, int64_t &n) {
     n = (int64_t)v.size();
     if (dst && !v.empty()) std::memcpy((void *)dst, v.data(), v.size() * sizeof(v[0]));
   };
-  put(out->sta, oz.sta, out->n_sta);
-  put(out->dyn_a, oz.dyn_a, out->n_dyn_a);
-  put(out->dyn_b, oz.dyn_b, out->n_dyn_b);
-  put(out->groups_a, oz.groups_a, out->n_groups_a);
-  put(out->groups_b, oz.groups_b, out->n_groups_b);
-  put(out->rows_a, oz.rows_a, out->n_rows_a);
-  put(out->rows_b, oz.rows_b, out->n_rows_b);
-  put(out->items_a, oz.items_a, out->n_items_a);
-  put(out->items_b, oz.items_b, out->n_items_b);
-  put(out->sums, oz.sums, out->n_sums);
-  put(out->slot_offs, oz.slot_offs, out->n_slots);
+  put(out->sta_jobs, oz.sta_jobs, out->n_sta_jobs);
+  put(out->psi_jobs, oz.psi_jobs, out->n_psi_jobs);
+  put(out->prod_jobs, oz.prod_jobs, out->n_prod_jobs);
+  put(out->segs, oz.segs, out->n_segs);
+  put(out->fams, oz.fams, out->n_fams);
+  put(out->stacks, oz.stacks, out->n_stacks);
+  put(out->cells, oz.cells, out->n_cells);
+  put(out->items1, oz.items1, out->n_items1);
+  put(out->items2, oz.items2, out->n_items2);
   return TJ_OK;
 }

@@ -257,6 +257,7 @@ struct Builder {
   std::vector<int> sec_x, sec_y, cell_base;   // per sector: sys map, env map, first cell id
   std::vector<int64_t> cell_off;
   std::vector<int> cell_ld, cell_M, cell_N;
+  std::vector<int32_t> cell_rs, cell_cs;       // basis-state index of row 0 / column 0
   int ncells = 0;
   std::map<std::tuple<int, int, int, int>, int> sec_of;   // first sector with the labels
   // tasks
@@ -300,6 +301,28 @@ struct Builder {
     cell_ld.resize(ncells);
     cell_M.resize(ncells);
     cell_N.resize(ncells);
+    cell_rs.resize(ncells);
+    cell_cs.resize(ncells);
+    // basis states of the (unenlarged) block: every sub-block (bl, st) of an
+    // enlarged sector spans all states of its block sector bl (site sectors
+    // are one-dimensional), so row i of any cell with block label bl is block
+    // state first(bl) + i
+    auto block_states = [](const tj_basis *b, std::map<std::pair<int, int>, int32_t> &first) {
+      int32_t n = 0;
+      for (int x = 0; x < b->num; ++x)
+        for (int l = 0; l < b->sub[x].num; ++l) {
+          const tj_basis_sub &m = b->maps[b->sub[x].first + l];
+          auto key = std::make_pair(m.bl_num_up, m.bl_num_down);
+          if (!first.count(key)) {
+            first[key] = n;
+            n += m.sdim;
+          }
+        }
+      return n;
+    };
+    std::map<std::pair<int, int>, int32_t> sys_first, env_first;
+    plan.n_sys_states = block_states(sbs, sys_first);
+    plan.n_env_states = block_states(ebs, env_first);
     for (int i = 0; i < ns; ++i) {
       const int x = sec_x[i], y = sec_y[i], ny = ebs->sub[y].num;
       for (int m = 0; m < sbs->sub[x].num; ++m)
@@ -309,6 +332,8 @@ struct Builder {
           cell_off[c] = wave->sub[i].off + (int64_t)b.spos * wave->sub[i].sys_dim + a.spos;
           cell_ld[c] = wave->sub[i].sys_dim;
           cell_M[c] = a.sdim;
+          cell_rs[c] = sys_first[std::make_pair(a.bl_num_up, a.bl_num_down)];
+          cell_cs[c] = env_first[std::make_pair(b.bl_num_up, b.bl_num_down)];
           cell_N[c] = b.sdim;
         }
     }
@@ -416,6 +441,7 @@ struct Builder {
       c.t_end = c.t_begin + 1;
       plan.scratch_len += ((int64_t)M * K2 + 3) / 4 * 4;
       plan.cells1.push_back(c);
+      plan.cell1_row_state.push_back(cell_rs[oc]);
       Task t;
       t.L = a;
       t.R = xop(xc);
@@ -910,6 +936,8 @@ struct Builder {
         if (t.R.space == SP_NONE) plan.tasks2.push_back(t);
       cl.t_end = (int)plan.tasks2.size();
       plan.cells2.push_back(cl);
+      plan.cell2_row_state.push_back(cell_rs[c]);
+      plan.cell2_col_state.push_back(cell_cs[c]);
     }
     auto make_tiles = [&](const std::vector<Cell> &cells, const std::vector<Task> &tasks,
                           std::vector<Tile> &tiles, std::vector<Reduce> &red, int64_t &nslots) {

@@ -84,6 +84,13 @@ struct HpsiPlan {
   int64_t scratch_len = 0;                   // doubles of phase-1 products
   int64_t psi_len = 0;
 
+  // Block-state index (over all block sectors of the sys / env block, before
+  // the site is added) of row 0 and column 0 of every phase-2 cell, and of
+  // row 0 of every phase-1 product (its rows are states of the target sys
+  // sub-block).
+  std::vector<int32_t> cell2_row_state, cell2_col_state, cell1_row_state;
+  int32_t n_sys_states = 0, n_env_states = 0;
+
   // accounting
   double flops = 0, flops_ref = 0, bytes = 0;
   std::string key;                           // structural fingerprint

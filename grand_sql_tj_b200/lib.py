@@ -74,43 +74,46 @@ class PlanExport(C.Structure):
                 ("red1", C.POINTER(PlanReduce)), ("red2", C.POINTER(PlanReduce))]
 
 
-class OzSplitC(C.Structure):
-    _fields_ = [("src_off", C.c_int64), ("pack_off", C.c_int64), ("sig_off", C.c_int64), ("rs", C.c_int32),
-                ("ks", C.c_int32), ("nrows", C.c_int32), ("K", C.c_int32), ("K_pad", C.c_int32),
-                ("space", C.c_int8), ("pad_", C.c_int8 * 3)]
+class OzJobC(C.Structure):
+    _fields_ = [("src_off", C.c_int64), ("dst", C.c_int64), ("scale_idx", C.c_int64), ("coef", C.c_double)] + \
+               [(n, C.c_int32) for n in ("rs", "ks", "nrows", "K", "gtot", "kb0")] + \
+               [("space", C.c_int8), ("want_max", C.c_int8), ("pad_", C.c_int8 * 6)]
 
 
-class OzGroupC(C.Structure):
-    _fields_ = [("s_pack_off", C.c_int64), ("tau_off", C.c_int64), ("N", C.c_int32), ("K_pad", C.c_int32),
-                ("row_begin", C.c_int32), ("row_end", C.c_int32)]
+class OzSegC(C.Structure):
+    _fields_ = [("a_base", C.c_int64), ("b_base", C.c_int64)] + \
+               [(n, C.c_int32) for n in ("a_gtot", "b_gtot", "a_kb0", "b_kb0", "nkb", "pad_")]
 
 
-class OzRowC(C.Structure):
-    _fields_ = [("pack_off", C.c_int64), ("sig_idx", C.c_int64), ("dst_off", C.c_int64), ("coef", C.c_double),
-                ("slice_stride", C.c_int32), ("dst_stride", C.c_int32), ("dst_space", C.c_int32),
-                ("pad_", C.c_int32)]
+class OzFamC(C.Structure):
+    _fields_ = [("seg_begin", C.c_int32), ("seg_end", C.c_int32), ("rs_idx", C.c_int64), ("cs_idx", C.c_int64)]
+
+
+class OzStackC(C.Structure):
+    _fields_ = [("a_base", C.c_int64), ("dst_off", C.c_int64), ("rs_idx", C.c_int64), ("pi_idx", C.c_int64)] + \
+               [(n, C.c_int32) for n in ("a_gtot", "a_g0", "a_ng", "dst_ld", "ncols", "pad_")]
 
 
 class OzItemC(C.Structure):
-    _fields_ = [(n, C.c_int32) for n in ("group", "row0", "n0", "pad_")]
+    _fields_ = [(n, C.c_int32) for n in ("kind", "cell", "row0", "col0", "M", "N", "mrows", "ncols", "fam_begin",
+                                         "fam_end", "seg", "init")] + \
+               [("cs_idx", C.c_int64), ("pad2_", C.c_int64), ("cost", C.c_int64)]
 
 
-class OzCellSumC(C.Structure):
-    _fields_ = [("out_off", C.c_int64)] + [(n, C.c_int32) for n in ("ld", "M", "N", "s_begin", "s_end",
-                                                                     "a_begin", "a_end")]
+class OzCellC(C.Structure):
+    _fields_ = [("off", C.c_int64)] + [(n, C.c_int32) for n in ("ld", "M", "N", "a_begin", "a_end", "pad_")]
+
+
+_OZ_ARRAYS = [("sta_jobs", OzJobC), ("psi_jobs", OzJobC), ("prod_jobs", OzJobC), ("segs", OzSegC),
+              ("fams", OzFamC), ("stacks", OzStackC), ("cells", OzCellC), ("items1", OzItemC), ("items2", OzItemC)]
 
 
 class OzExport(C.Structure):
-    _fields_ = ([(n, C.c_int32) for n in ("slices", "tile_m", "tile_n", "pad_")] +
-                [(n, C.c_int64) for n in ("sta_pack", "sta_sig", "dyn_pack", "dyn_sig", "slots_len")] +
+    _fields_ = ([("slices", C.c_int32), ("tile_n", C.c_int32)] +
+                [(n, C.c_int64) for n in ("sta_pack", "dyn_pack", "n_scales", "rho0", "tau0", "pi0")] +
                 [("int8_ops", C.c_double)] +
-                [(n, C.c_int64) for n in ("n_sta", "n_dyn_a", "n_dyn_b", "n_groups_a", "n_groups_b", "n_rows_a",
-                                          "n_rows_b", "n_items_a", "n_items_b", "n_sums", "n_slots")] +
-                [("sta", C.POINTER(OzSplitC)), ("dyn_a", C.POINTER(OzSplitC)), ("dyn_b", C.POINTER(OzSplitC)),
-                 ("groups_a", C.POINTER(OzGroupC)), ("groups_b", C.POINTER(OzGroupC)),
-                 ("rows_a", C.POINTER(OzRowC)), ("rows_b", C.POINTER(OzRowC)),
-                 ("items_a", C.POINTER(OzItemC)), ("items_b", C.POINTER(OzItemC)),
-                 ("sums", C.POINTER(OzCellSumC)), ("slot_offs", C.POINTER(C.c_int64))])
+                [("n_" + n, C.c_int64) for n, _ in _OZ_ARRAYS] +
+                [(n, C.POINTER(t)) for n, t in _OZ_ARRAYS])
 
 
 _lib = None
@@ -346,14 +349,7 @@ def ozaki_plan_export(sb, slices: int = 5, invec: Optional[Wave] = None) -> dict
 
     ex = OzExport()
     _chk(call(C.byref(ex)))
-    arrs = {
-        "sta": (OzSplitC * max(ex.n_sta, 1))(), "dyn_a": (OzSplitC * max(ex.n_dyn_a, 1))(),
-        "dyn_b": (OzSplitC * max(ex.n_dyn_b, 1))(), "groups_a": (OzGroupC * max(ex.n_groups_a, 1))(),
-        "groups_b": (OzGroupC * max(ex.n_groups_b, 1))(), "rows_a": (OzRowC * max(ex.n_rows_a, 1))(),
-        "rows_b": (OzRowC * max(ex.n_rows_b, 1))(), "items_a": (OzItemC * max(ex.n_items_a, 1))(),
-        "items_b": (OzItemC * max(ex.n_items_b, 1))(), "sums": (OzCellSumC * max(ex.n_sums, 1))(),
-        "slot_offs": (C.c_int64 * max(ex.n_slots, 1))(),
-    }
+    arrs = {n: (t * max(getattr(ex, "n_" + n), 1))() for n, t in _OZ_ARRAYS}
     for k, a in arrs.items():
         setattr(ex, k, C.cast(a, type(getattr(ex, k))))
     _chk(call(C.byref(ex)))

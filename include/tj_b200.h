@@ -227,6 +227,7 @@ typedef struct tj_hpsi_stats {
   double last_ms_phase1, last_ms_phase2;
   int64_t lanczos_hpsi;    /* H*psi products of the last tj_lanczos_memo_new      */
   double int8_ops;         /* split precision: 2 x int8 MACs issued per H*psi     */
+  int64_t kernels_per_hpsi; /* kernel launches of one H*psi                        */
 } tj_hpsi_stats;
 int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st);
 
@@ -306,43 +307,48 @@ int tj_cor_plan_export(int kind, const tj_block *a, const tj_block *b, const tj_
                        const tj_basis *env_bs, const tj_wave *wave, char flag, tj_plan_export *out);
 
 /* The split-precision form of the same H*psi (TJ_PREC_OZAKI with `slices`
- * int8 slices), for CPU checks of its index tables.  A split cuts rows of a
- * matrix (element (r, k) = base[src_off + r*rs + k*ks], space 1 operators,
- * 2 input vector, 3 phase-1 products) into `slices` int8 rows of K_pad bytes
- * (slice p of row r at pack_off + p*nrows*K_pad + r*K_pad) and a power-of-two
- * scale (index sig_off + r).  A GEMM group pairs the rows [row_begin,
- * row_end) of the row list with the N rows of one operator split; each row
- * writes y[n] = coef * sum_k L[k] S[n][k] to dst_off + n*dst_stride in the
- * phase-1 product space (dst_space 0) or the task slots (dst_space 1).
- * Launch A holds the products and the one-sided tasks, launch B the
- * two-sided tasks; a cell sum adds slots [s_begin, s_end) of the slot-offset
- * list (each an M x N column-major task result) and the axpy tasks
- * [a_begin, a_end) of the phase-2 task list.  Two-call pattern as above. */
-typedef struct tj_oz_split {
-  int64_t src_off, pack_off, sig_off;
-  int32_t rs, ks, nrows, K, K_pad;
-  int8_t space, pad_[3];
-} tj_oz_split;
-typedef struct tj_oz_group { int64_t s_pack_off, tau_off; int32_t N, K_pad, row_begin, row_end; } tj_oz_group;
-typedef struct tj_oz_row {
-  int64_t pack_off, sig_idx, dst_off;
+ * int8 slices), for CPU checks of its tables.  A split stores R rows x K of
+ * a matrix as G = ceil(R/8) row groups and ceil(K/32) k-blocks of `slices`
+ * int8 digit planes, byte (kb, g, p, c, r8, b) at
+ *   base + ((kb*G + g)*slices + p)*256 + c*128 + r8*16 + b
+ * for row 8g + r8 and k = 32kb + 16c + b.  A job writes coef*M(r, k) =
+ * coef*src[src_off + r*rs + k*ks] (space 1 operators, 2 input vector, 3
+ * phase-1 products) for r < nrows, k < K into k-blocks kb0.. of the split at
+ * pack offset dst, with the row scale held in scales[scale_idx + r] (the
+ * row's max |value|; want_max: the job raises it).  A segment pairs k-blocks
+ * of an A split and a B split; a family sums its segments and scales by
+ * scales[rs_idx + row] * scales[cs_idx + col]; an item is one output tile
+ * (kind 0: of cell `cell`, families [fam_begin, fam_end); kind 1: phase-1
+ * products stacked in [fam_begin, fam_end) of the stack list against the
+ * operator split of segment `seg`).  Two-call pattern as above. */
+typedef struct tj_oz_job {
+  int64_t src_off, dst, scale_idx;
   double coef;
-  int32_t slice_stride, dst_stride, dst_space, pad_;
-} tj_oz_row;
-typedef struct tj_oz_item { int32_t group, row0, n0, pad_; } tj_oz_item;
-typedef struct tj_oz_cell_sum { int64_t out_off; int32_t ld, M, N, s_begin, s_end, a_begin, a_end; } tj_oz_cell_sum;
+  int32_t rs, ks, nrows, K, gtot, kb0;
+  int8_t space, want_max, pad_[6];
+} tj_oz_job;
+typedef struct tj_oz_seg { int64_t a_base, b_base; int32_t a_gtot, b_gtot, a_kb0, b_kb0, nkb, pad_; } tj_oz_seg;
+typedef struct tj_oz_fam { int32_t seg_begin, seg_end; int64_t rs_idx, cs_idx; } tj_oz_fam;
+typedef struct tj_oz_stack {
+  int64_t a_base, dst_off, rs_idx, pi_idx;
+  int32_t a_gtot, a_g0, a_ng, dst_ld, ncols, pad_;
+} tj_oz_stack;
+typedef struct tj_oz_item {
+  int32_t kind, cell, row0, col0, M, N, mrows, ncols, fam_begin, fam_end, seg, init;
+  int64_t cs_idx, pad2_, cost;
+} tj_oz_item;
+typedef struct tj_oz_cell { int64_t off; int32_t ld, M, N, a_begin, a_end, pad_; } tj_oz_cell;
 typedef struct tj_ozaki_export {
-  int32_t slices, tile_m, tile_n, pad_;
-  int64_t sta_pack, sta_sig, dyn_pack, dyn_sig, slots_len;
+  int32_t slices, tile_n;
+  int64_t sta_pack, dyn_pack, n_scales, rho0, tau0, pi0;
   double int8_ops;
-  int64_t n_sta, n_dyn_a, n_dyn_b, n_groups_a, n_groups_b, n_rows_a, n_rows_b, n_items_a, n_items_b, n_sums,
-      n_slots;
-  tj_oz_split *sta, *dyn_a, *dyn_b;
-  tj_oz_group *groups_a, *groups_b;
-  tj_oz_row *rows_a, *rows_b;
-  tj_oz_item *items_a, *items_b;
-  tj_oz_cell_sum *sums;
-  int64_t *slot_offs;
+  int64_t n_sta_jobs, n_psi_jobs, n_prod_jobs, n_segs, n_fams, n_stacks, n_cells, n_items1, n_items2;
+  tj_oz_job *sta_jobs, *psi_jobs, *prod_jobs;
+  tj_oz_seg *segs;
+  tj_oz_fam *fams;
+  tj_oz_stack *stacks;
+  tj_oz_cell *cells;
+  tj_oz_item *items1, *items2;
 } tj_ozaki_export;
 int tj_ozaki_plan_export(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
                          const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave, int slices,

@@ -1,10 +1,12 @@
 """numpy executor of the split-precision H*psi tables (test helper, CPU only).
 
-It repeats the device arithmetic step by step -- row scales, truncated int8
-slices, exact integer slice products per diagonal, the FP64 epilogue in the
-kernel's order, the per-cell sums -- and checks every table index on the way
-(pack offsets inside their pools, each product and slot entry written exactly
-once), so that the split-precision plan can be verified without a GPU.
+It repeats the device arithmetic step by step -- row maxima, power-of-two
+scales, truncated radix-128 digits in the tile-ready layout, exact integer
+slice products per diagonal over each family's concatenated k-blocks, the
+FP64 epilogue in the kernel's order, the products' pi maxima -- and checks
+the table indices on the way (every split inside its pool, every output tile
+covered once per launch), so that the split-precision plan can be verified
+without a GPU.
 """
 import math
 
@@ -13,137 +15,175 @@ import numpy as np
 from tests.plan_exec import merged_ops
 
 
-def _rows(base, sp, nrows, K):
-    """Matrix (nrows x K) of a split: element (r, k) = base[src_off + r*rs + k*ks]."""
-    r = np.arange(nrows, dtype=np.int64)[:, None]
-    k = np.arange(K, dtype=np.int64)[None, :]
-    return base[sp.src_off + r * sp.rs + k * sp.ks]
+def _pow2_of(m):
+    m = np.asarray(m, dtype=np.float64)
+    out = np.zeros_like(m)
+    nz = m > 0
+    out[nz] = np.ldexp(1.0, np.frexp(m[nz])[1])
+    return out
 
 
-def _split(base, sp, s, pack, sig):
-    """oz_split_kernel: per-row power-of-two scale and s truncated radix-128 digits."""
-    X = _rows(base, sp, sp.nrows, sp.K)
-    out = np.zeros((s, sp.nrows, sp.K_pad), dtype=np.int64)
-    for r in range(sp.nrows):
-        mx = float(np.max(np.abs(X[r]))) if sp.K else 0.0
-        if mx > 0.0:
-            e = math.frexp(mx)[1]
-            sig[sp.sig_off + r] = math.ldexp(1.0, e)
-            t = np.ldexp(X[r], -e)
-            for q in range(s):
+class _Machine:
+    def __init__(self, plan, oz, psi):
+        ex, oe = plan["ex"], oz["ex"]
+        self.plan, self.oz, self.ex, self.oe = plan, oz, ex, oe
+        self.S, self.BN = oe.slices, oe.tile_n
+        self.ops = merged_ops(plan)
+        self.psi = np.concatenate([psi, np.zeros(8)])
+        self.scr = np.full(ex.scratch_len + 8, np.nan)
+        self.out = np.full(max(ex.psi_len, 1), np.nan)
+        self.pack = np.zeros(oe.sta_pack + oe.dyn_pack, dtype=np.int8)
+        self.scales = np.zeros(oe.n_scales)
+        self.spaces = {1: self.ops, 2: self.psi, 3: self.scr}
+
+    def _matrix(self, j):
+        base = self.spaces[j.space]
+        r = np.arange(j.nrows, dtype=np.int64)[:, None]
+        k = np.arange(j.K, dtype=np.int64)[None, :]
+        return j.coef * base[j.src_off + r * j.rs + k * j.ks]
+
+    def run_max(self, jobs, n):
+        for i in range(n):
+            j = jobs[i]
+            if not j.want_max:
+                continue
+            m = np.max(np.abs(self._matrix(j)), axis=1)
+            idx = j.scale_idx + np.arange(j.nrows)
+            self.scales[idx] = np.maximum(self.scales[idx], m)
+
+    def run_split(self, jobs, n):
+        S = self.S
+        for i in range(n):
+            j = jobs[i]
+            nkb = -(-j.K // 32)
+            rows = j.gtot * 8
+            X = np.zeros((rows, nkb * 32))
+            X[:j.nrows, :j.K] = self._matrix(j)
+            sc = np.zeros(rows)
+            sc[:j.nrows] = _pow2_of(self.scales[j.scale_idx:j.scale_idx + j.nrows])
+            with np.errstate(divide="ignore", invalid="ignore"):
+                t = np.where(sc[:, None] > 0, X * np.where(sc > 0, 1.0 / np.where(sc > 0, sc, 1.0), 0.0)[:, None], 0.0)
+            dig = np.zeros((S, rows, nkb * 32), dtype=np.int64)
+            for q in range(S):
                 t = t * 128.0
                 a = np.trunc(t)
                 t = t - a
-                out[q, r, :sp.K] = a.astype(np.int64)
-        else:
-            sig[sp.sig_off + r] = 0.0
-    assert np.all(np.abs(out) <= 127)
-    end = sp.pack_off + s * sp.nrows * sp.K_pad
-    assert 0 <= sp.pack_off and end <= len(pack)
-    pack[sp.pack_off:end] = out.reshape(-1)
+                dig[q] = a.astype(np.int64)
+            assert np.all(np.abs(dig) <= 127)
+            # [kb][g][p][c][r8][16]
+            blk = dig.reshape(S, j.gtot, 8, nkb, 2, 16).transpose(3, 1, 0, 4, 2, 5)
+            start = j.dst + j.kb0 * j.gtot * S * 256
+            size = nkb * j.gtot * S * 256
+            assert 0 <= start and start + size <= len(self.pack)
+            self.pack[start:start + size] = blk.reshape(-1).astype(np.int8)
 
+    def digits(self, base, gtot, g0, ng, kb0, nkb):
+        """Slices (S, 8*ng, 32*nkb) of row groups [g0, g0+ng), k-blocks [kb0, kb0+nkb) of a split."""
+        S = self.S
+        out = np.zeros((S, ng * 8, nkb * 32), dtype=np.int64)
+        for kb in range(nkb):
+            o = base + ((kb0 + kb) * gtot + g0) * S * 256
+            assert 0 <= o and o + ng * S * 256 <= len(self.pack)
+            b = self.pack[o:o + ng * S * 256].astype(np.int64).reshape(ng, S, 2, 8, 16)
+            out[:, :, kb * 32:(kb + 1) * 32] = b.transpose(1, 0, 3, 2, 4).reshape(S, ng * 8, 32)
+        return out
 
-def _gemm(groups, ngroups, rows, items, nitems, s, bn, dyn_pack, dyn_sig, sta_pack, sta_sig, dst, written):
-    # every (group, row tile, n tile) exactly once
-    seen = set()
-    for i in range(nitems):
-        it = items[i]
-        key = (it.group, it.row0, it.n0)
-        assert key not in seen
-        seen.add(key)
-    expect = set()
-    for gi in range(ngroups):
-        g = groups[gi]
-        for r0 in range(0, g.row_end - g.row_begin, 128):
-            for n0 in range(0, g.N, bn):
-                expect.add((gi, r0, n0))
-    assert seen == expect
-    w = 2.0 ** (-7 * np.arange(2, s + 2))
-    for gi in range(ngroups):
-        g = groups[gi]
-        B = sta_pack[g.s_pack_off:g.s_pack_off + s * g.N * g.K_pad].reshape(s, g.N, g.K_pad)
-        tau = sta_sig[g.tau_off:g.tau_off + g.N]
-        nr = g.row_end - g.row_begin
-        A = np.zeros((s, nr, g.K_pad), dtype=np.int64)
-        for j in range(nr):
-            R = rows[g.row_begin + j]
-            for p in range(s):
-                o = R.pack_off + p * R.slice_stride
-                assert 0 <= o and o + g.K_pad <= len(dyn_pack)
-                A[p, j] = dyn_pack[o:o + g.K_pad]
-        diag = np.zeros((s, nr, g.N), dtype=np.int64)
-        for p in range(1, s + 1):
-            for q in range(1, s + 2 - p):
-                diag[p + q - 2] += A[p - 1] @ B[q - 1].T
-        assert np.max(np.abs(diag)) < 2 ** 31
-        acc = np.zeros((nr, g.N))
-        for d in range(s - 1, -1, -1):
-            acc = acc + diag[d].astype(np.float64) * w[d]
-        for j in range(nr):
-            R = rows[g.row_begin + j]
-            vals = acc[j] * (R.coef * dyn_sig[R.sig_idx]) * tau
-            idx = R.dst_off + np.arange(g.N, dtype=np.int64) * R.dst_stride
-            space = dst[R.dst_space]
-            assert idx.min() >= 0 and idx.max() < len(space)
-            space[idx] = vals
-            written[R.dst_space][idx] += 1
+    def accum(self, A, B):
+        """sum_d 128^-(d+2) D_d, D_d = sum_{p+q=d+2} A_p B_q^T, summed from the last diagonal down."""
+        S = self.S
+        D = [0] * S
+        for pa in range(1, S + 1):
+            for qb in range(1, S + 2 - pa):
+                D[pa + qb - 2] = D[pa + qb - 2] + A[pa - 1] @ B[qb - 1].T
+        acc = np.zeros((A.shape[1], B.shape[1]))
+        for d in range(S - 1, -1, -1):
+            if not isinstance(D[d], int):
+                assert np.max(np.abs(D[d])) < 2 ** 31
+                acc = acc + D[d].astype(np.float64) * (2.0 ** (-7 * (d + 2)))
+        return acc
+
+    def run_items(self, items, n, covered):
+        oz = self.oz
+        S = self.S
+        for ii in range(n):
+            it = items[ii]
+            ga, gb = -(-it.mrows // 8), -(-it.ncols // 8)
+            assert it.M in (64, 128) and it.mrows <= it.M and it.N % 16 == 0 and it.ncols <= it.N <= self.BN
+            if it.kind == 0:
+                c = oz["cells"][it.cell]
+                key = (it.cell, it.row0, it.col0)
+                assert key not in covered
+                covered.add(key)
+                rows = it.row0 + np.arange(it.mrows)
+                cols = it.col0 + np.arange(it.ncols)
+                idx = c.off + rows[:, None] + cols[None, :] * c.ld
+                if it.init:
+                    v = np.zeros((it.mrows, it.ncols))
+                    tasks = self.plan["tasks2"]
+                    for a in range(c.a_begin, c.a_end):
+                        t = tasks[a]
+                        b = self.spaces[t.L.space]
+                        v = v + t.coef * b[t.L.off + cols[None, :] * t.L.ld + rows[:, None]]
+                    self.out[idx] = v
+                for f in range(it.fam_begin, it.fam_end):
+                    fm = oz["fams"][f]
+                    acc = 0
+                    A_all, B_all = [], []
+                    for sgi in range(fm.seg_begin, fm.seg_end):
+                        sg = oz["segs"][sgi]
+                        A_all.append(self.digits(sg.a_base, sg.a_gtot, it.row0 // 8, ga, sg.a_kb0, sg.nkb))
+                        B_all.append(self.digits(sg.b_base, sg.b_gtot, it.col0 // 8, gb, sg.b_kb0, sg.nkb))
+                    A = np.concatenate(A_all, axis=2)[:, :it.mrows]
+                    B = np.concatenate(B_all, axis=2)[:, :it.ncols]
+                    acc = self.accum(A, B)
+                    rs = _pow2_of(self.scales[fm.rs_idx + rows])
+                    cs = _pow2_of(self.scales[fm.cs_idx + cols])
+                    self.out[idx] = self.out[idx] + (acc * rs[:, None]) * cs[None, :]
+            else:
+                sg = oz["segs"][it.seg]
+                pieces = [oz["stacks"][si] for si in range(it.fam_begin, it.fam_end)]
+                A = np.concatenate([self.digits(sk.a_base, sk.a_gtot, sk.a_g0, sk.a_ng, 0, sg.nkb) for sk in pieces],
+                                   axis=1)
+                B = self.digits(sg.b_base, sg.b_gtot, it.col0 // 8, gb, sg.b_kb0, sg.nkb)[:, :it.ncols]
+                acc = self.accum(A, B)
+                cs = _pow2_of(self.scales[it.cs_idx + np.arange(it.ncols)])
+                r0 = 0
+                for sk in pieces:
+                    jl = np.arange(sk.ncols)
+                    rs = _pow2_of(self.scales[sk.rs_idx + jl])
+                    val = (acc[r0:r0 + sk.ncols] * rs[:, None]) * cs[None, :]
+                    # P(i = col0 + n, j = 8*a_g0 + jl)
+                    idx = sk.dst_off + jl[:, None] * sk.dst_ld + it.col0 + np.arange(it.ncols)[None, :]
+                    key = ("p", int(sk.dst_off), it.col0)
+                    assert key not in covered
+                    covered.add(key)
+                    self.scr[idx] = val
+                    pidx = sk.pi_idx + it.col0 + np.arange(it.ncols)
+                    if sk.ncols:
+                        self.scales[pidx] = np.maximum(self.scales[pidx], np.max(np.abs(val), axis=0))
+                    r0 += sk.a_ng * 8
 
 
 def execute_ozaki(plan, oz, psi):
-    """H*psi through the split-precision tables; returns (out, checks dict)."""
-    ex, oe = plan["ex"], oz["ex"]
-    s, bn = oe.slices, oe.tile_n
-    ops = merged_ops(plan)
-    psi = np.concatenate([psi, np.zeros(8)])
-    scr = np.full(ex.scratch_len + 8, np.nan)
-    slots = np.full(max(oe.slots_len, 1), np.nan)
-    sta_pack = np.zeros(oe.sta_pack, dtype=np.int64)
-    sta_sig = np.full(oe.sta_sig, np.nan)
-    dyn_pack = np.zeros(oe.dyn_pack, dtype=np.int64)
-    dyn_sig = np.full(oe.dyn_sig, np.nan)
-    for i in range(oe.n_sta):
-        assert oz["sta"][i].space == 1
-        _split(ops, oz["sta"][i], s, sta_pack, sta_sig)
-    for i in range(oe.n_dyn_a):
-        assert oz["dyn_a"][i].space == 2
-        _split(psi, oz["dyn_a"][i], s, dyn_pack, dyn_sig)
-    written = {0: np.zeros(len(scr), dtype=np.int64), 1: np.zeros(len(slots), dtype=np.int64)}
-    dst = {0: scr, 1: slots}
-    _gemm(oz["groups_a"], oe.n_groups_a, oz["rows_a"], oz["items_a"], oe.n_items_a, s, bn, dyn_pack, dyn_sig,
-          sta_pack, sta_sig, dst, written)
-    for i in range(oe.n_dyn_b):
-        assert oz["dyn_b"][i].space == 3
-        _split(scr, oz["dyn_b"][i], s, dyn_pack, dyn_sig)
-    _gemm(oz["groups_b"], oe.n_groups_b, oz["rows_b"], oz["items_b"], oe.n_items_b, s, bn, dyn_pack, dyn_sig,
-          sta_pack, sta_sig, dst, written)
-    # cell sums
-    out = np.full(max(ex.psi_len, 1), np.nan)
-    spaces = {1: ops, 2: psi, 3: scr}
-    tasks = plan["tasks2"]
-    for ci in range(oe.n_sums):
-        c = oz["sums"][ci]
-        v = np.zeros((c.N, c.M))
-        for j in range(c.s_begin, c.s_end):
-            o = oz["slot_offs"][j]
-            v = v + slots[o:o + c.M * c.N].reshape(c.N, c.M)
-        for a in range(c.a_begin, c.a_end):
-            t = tasks[a]
-            b = spaces[t.L.space]
-            idx = t.L.off + np.arange(c.N)[:, None] * t.L.ld + np.arange(c.M)[None, :]
-            v = v + t.coef * b[idx]
-        idx = c.out_off + np.arange(c.N)[:, None] * c.ld + np.arange(c.M)[None, :]
-        out[idx] = v
-    # phase-1 products and task slots: written exactly once where read
-    cells1 = plan["cells1"]
+    """H*psi through the split-precision tables, as the device runs them."""
+    m = _Machine(plan, oz, psi)
+    oe = m.oe
+    # once per step
+    m.run_max(oz["sta_jobs"], oe.n_sta_jobs)
+    m.run_split(oz["sta_jobs"], oe.n_sta_jobs)
+    # per H*psi
+    m.scales[oe.rho0:] = 0.0
+    m.run_max(oz["psi_jobs"], oe.n_psi_jobs)
+    m.run_split(oz["psi_jobs"], oe.n_psi_jobs)
+    cov1 = set()
+    m.run_items(oz["items1"], oe.n_items1, cov1)
+    m.run_split(oz["prod_jobs"], oe.n_prod_jobs)
+    cov2 = set()
+    m.run_items(oz["items2"], oe.n_items2, cov2)
+    # every phase-1 product was written where it is read
+    ex = plan["ex"]
     for ci in range(ex.n_cells1):
-        c = cells1[ci]
+        c = plan["cells1"][ci]
         idx = c.off + np.arange(c.N)[:, None] * c.ld + np.arange(c.M)[None, :]
-        assert np.all(written[0][idx] == 1)
-    used = np.zeros(len(slots), dtype=bool)
-    for ci in range(oe.n_sums):
-        c = oz["sums"][ci]
-        for j in range(c.s_begin, c.s_end):
-            o = oz["slot_offs"][j]
-            used[o:o + c.M * c.N] = True
-    assert np.all(written[1][used] == 1)
-    return out[:ex.psi_len]
+        assert np.all(np.isfinite(m.scr[idx])), "product %d not fully written" % ci
+    return m.out[:ex.psi_len]

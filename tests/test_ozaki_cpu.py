@@ -13,8 +13,8 @@ from grand_sql_tj_b200.lib import TjError, ozaki_plan_export, plan_export
 from tests.oz_exec import execute_ozaki
 
 
-@pytest.mark.parametrize("name,slices,tol", [("tiny", 5, 1e-9), ("small", 5, 1e-9), ("small_gc", 4, 1e-7),
-                                             ("cyl4", 5, 1e-9), ("cyl4", 7, 1e-13)])
+@pytest.mark.parametrize("name,slices,tol", [("tiny", 5, 2e-9), ("small", 5, 2e-9), ("small_gc", 4, 3e-7),
+                                             ("cyl4", 5, 2e-9), ("cyl4", 6, 2e-11), ("cyl4", 8, 1e-13)])
 def test_ozaki_tables_match_oracle(name, slices, tol, product_lib, oracle_lib):
     from oracle import oracle
     sb = synth.workload(name, seed=11)
@@ -42,10 +42,11 @@ def test_ozaki_accounting(product_lib):
     sb = synth.workload("cyl4", seed=5)
     oz5 = ozaki_plan_export(sb, 5)["ex"]
     oz6 = ozaki_plan_export(sb, 6)["ex"]
-    assert oz5.tile_m == 128 and oz5.tile_n == 48 and oz6.tile_n == 32
+    assert oz5.tile_n == 48 and oz6.tile_n == 32
     assert oz5.int8_ops > plan_export(sb)["ex"].flops   # padded int8 work exceeds the FP64 flops
     assert oz6.int8_ops > plan_export(sb)["ex"].flops
-    assert oz5.n_items_a > 0 and oz5.n_items_b > 0 and oz5.n_sums > 0
+    assert oz5.n_items1 > 0 and oz5.n_items2 > 0 and oz5.n_sta_jobs > 0 and oz5.n_psi_jobs > 0
+    assert oz5.rho0 < oz5.tau0 < oz5.pi0 < oz5.n_scales
 
 
 def test_ozaki_rejects_bad_slice_count(product_lib):
