@@ -29,11 +29,13 @@
 
 namespace tjb {
 
+// The power of two just above the row maximum m: 2^(E+1) for m = 1.f * 2^E
+// (so every |x| <= m has |x| / 2^(E+1) < 1); 0 for m = 0.  Read off the
+// exponent bits; m is finite and non-negative.
 __device__ __forceinline__ double oz_pow2_of(double m) {
   if (!(m > 0.0)) return 0.0;
-  int e;
-  frexp(m, &e);   // m = f 2^e, f in [0.5, 1): every |x| <= m has |x| 2^-e < 1
-  return ldexp(1.0, e);
+  const unsigned long long e = ((unsigned long long)__double_as_longlong(m) >> 52) & 0x7FFull;
+  return __longlong_as_double((long long)((e == 0 ? 1ull : e + 1ull) << 52));
 }
 
 __device__ __forceinline__ const double *oz_space(int8_t sp, const double *ops, const double *psi,
@@ -235,10 +237,16 @@ template <int S, int BN>
 __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
   using C = OzCfg<S, BN>;
   constexpr int ST = C::STAGES;
+  constexpr uint32_t GB = S * 256;   // bytes of one row group (all slices) of one k-block
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ __align__(8) uint64_t full_bar[ST], empty_bar[ST], tfull_bar[2], tempty_bar[2], drain_bar;
   __shared__ uint32_t tmem_sh;
   __shared__ volatile int abort_sh;
+  __shared__ volatile int tfull_ok_sh;
+  __shared__ double cscale_sh[BN];           // epilogue: column scales of the current family
+  __shared__ int32_t stk_start[17];          // epilogue: first tile row of each stacked run
+  __shared__ int64_t stk_dst[16], stk_rs[16], stk_pi[16];
+  __shared__ int32_t stk_ld[16], stk_nc[16];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (tid == 0) {
@@ -266,76 +274,105 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
   const uint32_t smem0 = oz_smem(smem);
 
   if (warp == 4) {
-    // ------------------------------------------------ producer
-    if (lane == 0) {
-      int stage = 0;
-      uint32_t ph = 0;
-      int armed[ST];
-      uint32_t armed_ph[ST];
-      for (int i = 0; i < ST; ++i) armed[i] = 0, armed_ph[i] = 0;
-      bool ok = true;
-      for (int ii = blockIdx.x; ii < p.nitems && ok; ii += gridDim.x) {
-        const OzItem it = p.items[ii];
-        const uint32_t gb = (uint32_t)((it.ncols + 7) >> 3), b_g0 = (uint32_t)(it.col0 >> 3);
-        if (it.kind == 1) {
-          const OzSeg sg = p.segs[it.seg];
-          for (int kb = 0; kb < sg.nkb && ok; ++kb) {
-            if (!oz_wait(oz_smem(&empty_bar[stage]), ph ^ 1u, &abort_sh)) {
-              if (!abort_sh) oz_fail(&abort_sh, p.err);
-              ok = false;
-              break;
-            }
-            const uint32_t fb = oz_smem(&full_bar[stage]);
-            const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE), sbb = sa + C::A_BYTES;
-            uint32_t bytes = gb * S * 256;
-            for (int si = it.fam_begin; si < it.fam_end; ++si) bytes += (uint32_t)p.stacks[si].a_ng * S * 256;
-            oz_arrive_expect(fb, bytes);
-            armed[stage] = 1;
-            armed_ph[stage] = ph;
-            uint32_t aoff = 0;
-            for (int si = it.fam_begin; si < it.fam_end; ++si) {
-              const OzStack sk = p.stacks[si];
-              const uint8_t *src = p.pack + sk.a_base + ((int64_t)kb * sk.a_gtot + sk.a_g0) * (S * 256);
-              oz_bulk_g2s(sa + aoff, src, (uint32_t)sk.a_ng * S * 256, fb);
-              aoff += (uint32_t)sk.a_ng * S * 256;
-            }
-            const uint8_t *bsrc = p.pack + sg.b_base + ((int64_t)(sg.b_kb0 + kb) * sg.b_gtot + b_g0) * (S * 256);
-            oz_bulk_g2s(sbb, bsrc, gb * S * 256, fb);
-            if (++stage == ST) stage = 0, ph ^= 1u;
-          }
+    // ------------------------------------------------ producer (whole warp; lane 0 owns the barriers)
+    int stage = 0;
+    uint32_t ph = 0;
+    uint32_t armed = 0, armed_ph = 0;   // bit i: stage i armed, and the parity of its last arming
+    bool ok = true;
+    // lane 0 waits for a free stage and arms it with `bytes`; every lane learns the outcome
+    auto acquire = [&](uint32_t bytes) -> bool {
+      int good = 1;
+      if (lane == 0) {
+        if (!oz_wait(oz_smem(&empty_bar[stage]), ph ^ 1u, &abort_sh)) {
+          if (!abort_sh) oz_fail(&abort_sh, p.err);
+          good = 0;
         } else {
-          const uint32_t ga = (uint32_t)((it.mrows + 7) >> 3), a_g0 = (uint32_t)(it.row0 >> 3);
-          for (int f = it.fam_begin; f < it.fam_end && ok; ++f) {
-            const OzFam fm = p.fams[f];
-            for (int sgi = fm.seg_begin; sgi < fm.seg_end && ok; ++sgi) {
-              const OzSeg sg = p.segs[sgi];
-              for (int kb = 0; kb < sg.nkb; ++kb) {
-                if (!oz_wait(oz_smem(&empty_bar[stage]), ph ^ 1u, &abort_sh)) {
-                  if (!abort_sh) oz_fail(&abort_sh, p.err);
+          oz_arrive_expect(oz_smem(&full_bar[stage]), bytes);
+        }
+      }
+      good = __shfl_sync(0xffffffffu, good, 0);
+      if (good) {
+        armed |= 1u << stage;
+        armed_ph = (armed_ph & ~(1u << stage)) | (ph << stage);
+      }
+      __syncwarp();
+      return good != 0;
+    };
+    for (int ii = blockIdx.x; ii < p.nitems && ok; ii += gridDim.x) {
+      const OzItem it = p.items[ii];
+      const uint32_t gb = (uint32_t)((it.ncols + 7) >> 3), b_g0 = (uint32_t)(it.col0 >> 3);
+      if (it.kind == 1) {
+        const OzSeg sg = p.segs[it.seg];
+        const int np = it.fam_end - it.fam_begin;   // <= 16 stacked runs, one per lane
+        int64_t abase = 0;
+        int32_t agtot = 0, ag0 = 0, ang = 0;
+        if (lane < np) {
+          const OzStack sk = p.stacks[it.fam_begin + lane];
+          abase = sk.a_base;
+          agtot = sk.a_gtot;
+          ag0 = sk.a_g0;
+          ang = sk.a_ng;
+        }
+        int32_t off = ang;   // exclusive prefix of the runs' groups
+        for (int o = 1; o < 32; o <<= 1) {
+          const int32_t v = __shfl_up_sync(0xffffffffu, off, o);
+          if (lane >= o) off += v;
+        }
+        const int32_t tot = __shfl_sync(0xffffffffu, off, 31);
+        off -= ang;
+        for (int kb = 0; kb < sg.nkb; ++kb) {
+          if (!acquire(((uint32_t)tot + gb) * GB)) {
+            ok = false;
+            break;
+          }
+          const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE), sbb = sa + C::A_BYTES;
+          const uint32_t fb = oz_smem(&full_bar[stage]);
+          if (lane < np)
+            oz_bulk_g2s(sa + (uint32_t)off * GB, p.pack + abase + ((int64_t)kb * agtot + ag0) * GB,
+                        (uint32_t)ang * GB, fb);
+          if (lane == 31)
+            oz_bulk_g2s(sbb, p.pack + sg.b_base + ((int64_t)(sg.b_kb0 + kb) * sg.b_gtot + b_g0) * GB, gb * GB, fb);
+          if (++stage == ST) stage = 0, ph ^= 1u;
+        }
+      } else {
+        const uint32_t ga = (uint32_t)((it.mrows + 7) >> 3), a_g0 = (uint32_t)(it.row0 >> 3);
+        for (int f = it.fam_begin; f < it.fam_end && ok; ++f) {
+          const OzFam fm = p.fams[f];
+          for (int s0 = fm.seg_begin; s0 < fm.seg_end && ok; s0 += 32) {
+            // the next <= 32 segments, one per lane
+            OzSeg mine;
+            if (s0 + lane < fm.seg_end) mine = p.segs[s0 + lane];
+            const int cnt = min(32, fm.seg_end - s0);
+            for (int j = 0; j < cnt && ok; ++j) {
+              const int64_t a_base = __shfl_sync(0xffffffffu, mine.a_base, j);
+              const int64_t b_base = __shfl_sync(0xffffffffu, mine.b_base, j);
+              const int32_t a_gtot = __shfl_sync(0xffffffffu, mine.a_gtot, j);
+              const int32_t b_gtot = __shfl_sync(0xffffffffu, mine.b_gtot, j);
+              const int32_t a_kb0 = __shfl_sync(0xffffffffu, mine.a_kb0, j);
+              const int32_t b_kb0 = __shfl_sync(0xffffffffu, mine.b_kb0, j);
+              const int32_t nkb = __shfl_sync(0xffffffffu, mine.nkb, j);
+              for (int kb = 0; kb < nkb; ++kb) {
+                if (!acquire((ga + gb) * GB)) {
                   ok = false;
                   break;
                 }
-                const uint32_t fb = oz_smem(&full_bar[stage]);
                 const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE), sbb = sa + C::A_BYTES;
-                oz_arrive_expect(fb, (ga + gb) * S * 256);
-                armed[stage] = 1;
-                armed_ph[stage] = ph;
-                const uint8_t *asrc =
-                    p.pack + sg.a_base + ((int64_t)(sg.a_kb0 + kb) * sg.a_gtot + a_g0) * (S * 256);
-                const uint8_t *bsrc =
-                    p.pack + sg.b_base + ((int64_t)(sg.b_kb0 + kb) * sg.b_gtot + b_g0) * (S * 256);
-                oz_bulk_g2s(sa, asrc, ga * S * 256, fb);
-                oz_bulk_g2s(sbb, bsrc, gb * S * 256, fb);
+                const uint32_t fb = oz_smem(&full_bar[stage]);
+                if (lane == 0)
+                  oz_bulk_g2s(sa, p.pack + a_base + ((int64_t)(a_kb0 + kb) * a_gtot + a_g0) * GB, ga * GB, fb);
+                if (lane == 1)
+                  oz_bulk_g2s(sbb, p.pack + b_base + ((int64_t)(b_kb0 + kb) * b_gtot + b_g0) * GB, gb * GB, fb);
                 if (++stage == ST) stage = 0, ph ^= 1u;
               }
             }
           }
         }
       }
-      // copies still in flight land before the CTA exits
-      for (int i = 0; i < ST; ++i)
-        if (armed[i]) oz_wait(oz_smem(&full_bar[i]), armed_ph[i], nullptr);
     }
+    // copies still in flight land before the CTA exits
+    if (lane == 0)
+      for (int i = 0; i < ST; ++i)
+        if (armed & (1u << i)) oz_wait(oz_smem(&full_bar[i]), (armed_ph >> i) & 1u, nullptr);
     __syncwarp();
   } else if (warp == 5) {
     // ------------------------------------------------ MMA issuer
@@ -344,11 +381,13 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
       uint32_t ph = 0;
       uint32_t famc = 0;
       bool ok = true, issued = false;
+      const uint64_t dbase = oz_desc(0u, 128u, S * 256u);   // start address added per stage
       for (int ii = blockIdx.x; ii < p.nitems && ok; ii += gridDim.x) {
         const OzItem it = p.items[ii];
         const uint32_t idesc = oz_idesc(it.M, it.N);
         const int nf = it.kind == 1 ? 1 : it.fam_end - it.fam_begin;
         for (int f = 0; f < nf && ok; ++f) {
+          const int nkb = it.kind == 1 ? it.nkb : p.fams[it.fam_begin + f].nkb;
           const uint32_t buf = famc & 1u, use = famc >> 1;
           if (!oz_wait(oz_smem(&tempty_bar[buf]), (use & 1u) ^ 1u, &abort_sh)) {
             if (!abort_sh) oz_fail(&abort_sh, p.err);
@@ -357,47 +396,36 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
           }
           asm volatile("tcgen05.fence::after_thread_sync;");
           const uint32_t dt = tmem + buf * 256u;
-          int sb, se;
-          if (it.kind == 1) {
-            sb = it.seg;
-            se = it.seg + 1;
-          } else {
-            const OzFam fm = p.fams[it.fam_begin + f];
-            sb = fm.seg_begin;
-            se = fm.seg_end;
-          }
-          bool first = true;
-          for (int sgi = sb; sgi < se && ok; ++sgi) {
-            const int nkb = p.segs[sgi].nkb;
-            for (int kb = 0; kb < nkb; ++kb) {
-              if (!oz_wait(oz_smem(&full_bar[stage]), ph, &abort_sh)) {
-                if (!abort_sh) oz_fail(&abort_sh, p.err);
-                ok = false;
-                break;
-              }
-              asm volatile("tcgen05.fence::after_thread_sync;");
-              const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE), sbb = sa + C::A_BYTES;
-#pragma unroll
-              for (int pa = 1; pa <= S; ++pa) {
-#pragma unroll
-                for (int qb = 1; pa + qb <= S + 1; ++qb) {
-                  const uint64_t da = oz_desc(sa + (uint32_t)(pa - 1) * 256u, 128u, S * 256u);
-                  const uint64_t db = oz_desc(sbb + (uint32_t)(qb - 1) * 256u, 128u, S * 256u);
-                  const uint32_t d = dt + (uint32_t)((pa + qb - 2) * BN);
-                  const uint32_t acc = (first && pa == 1) ? 0u : 1u;
-                  asm volatile(
-                      "{\n\t.reg .pred p;\n\t"
-                      "setp.ne.b32 p, %4, 0;\n\t"
-                      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-                      :
-                      : "r"(d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
-                }
-              }
-              issued = true;
-              oz_commit(oz_smem(&empty_bar[stage]));   // frees the stage when these MMAs finish
-              first = false;
-              if (++stage == ST) stage = 0, ph ^= 1u;
+          for (int kb = 0; kb < nkb; ++kb) {
+            if (!oz_wait(oz_smem(&full_bar[stage]), ph, &abort_sh)) {
+              if (!abort_sh) oz_fail(&abort_sh, p.err);
+              ok = false;
+              break;
             }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE);
+            const uint64_t da0 = dbase + (uint64_t)(sa >> 4);
+            const uint64_t db0 = dbase + (uint64_t)((sa + C::A_BYTES) >> 4);
+            const uint32_t acc0 = kb == 0 ? 0u : 1u;
+#pragma unroll
+            for (int pa = 1; pa <= S; ++pa) {
+#pragma unroll
+              for (int qb = 1; pa + qb <= S + 1; ++qb) {
+                const uint64_t da = da0 + (uint64_t)((pa - 1) * 16);   // +256 bytes per slice
+                const uint64_t db = db0 + (uint64_t)((qb - 1) * 16);
+                const uint32_t d = dt + (uint32_t)((pa + qb - 2) * BN);
+                const uint32_t acc = pa == 1 ? acc0 : 1u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                    :
+                    : "r"(d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+              }
+            }
+            issued = true;
+            oz_commit(oz_smem(&empty_bar[stage]));   // frees the stage when these MMAs finish
+            if (++stage == ST) stage = 0, ph ^= 1u;
           }
           if (!ok) break;
           oz_commit(oz_smem(&tfull_bar[buf]));
@@ -412,7 +440,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
     }
     __syncwarp();
   } else {
-    // ------------------------------------------------ epilogue (warps 0-3)
+    // ------------------------------------------------ epilogue (warps 0-3, named barrier 1)
     uint32_t famc = 0;
     double w[S];
     {
@@ -441,7 +469,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
       double *dst = nullptr;
       int64_t cstride = 0;
       double rscale_stack = 0.0;
-      int64_t pib = -1;   // kind 1: pi index of this row's product row `col0`
+      int64_t pib = -1;   // kind 1: pi index of this row's product, row col0
       if (it.kind == 0) {
         const OzCell c = p.cells[it.cell];
         dst = p.out + c.off + (int64_t)(it.row0 + r) + (int64_t)it.col0 * c.ld;
@@ -451,43 +479,46 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
             double v = 0.0;
             for (int a = c.a_begin; a < c.a_end; ++a) {
               const Task &t = p.tasks[a];
-              const double *b = t.L.space == SP_PSI ? p.psi : (t.L.space == SP_SCR ? p.scr : nullptr);
-              if (b) v += t.coef * b[t.L.off + (int64_t)(it.col0 + n) * t.L.ld + it.row0 + r];
+              v += t.coef * p.psi[t.L.off + (int64_t)(it.col0 + n) * t.L.ld + it.row0 + r];
             }
             dst[(int64_t)n * cstride] = v;
           }
         }
       } else {
-        // stacked products: the run holding this row
-        int start = 0;
-        bool found = false;
-        for (int si = it.fam_begin; si < it.fam_end; ++si) {
-          const OzStack sk = p.stacks[si];
-          const int len = sk.a_ng * 8;
-          if (!found && r < start + len) {
-            const int jl = r - start;
-            found = true;
-            pib = sk.pi_idx + it.col0;
-            if (jl < sk.ncols) {
-              dst = p.scr + sk.dst_off + (int64_t)jl * sk.dst_ld + it.col0;
-              rscale_stack = oz_pow2_of(p.scales[sk.rs_idx + jl]);
-            } else {
-              rv = false;
-            }
-          }
-          start += len;
+        // stacked products: the runs of this tile, then the run holding this row
+        const int np = it.fam_end - it.fam_begin;
+        if (tid < np) {
+          const OzStack sk = p.stacks[it.fam_begin + tid];
+          stk_dst[tid] = sk.dst_off;
+          stk_rs[tid] = sk.rs_idx;
+          stk_pi[tid] = sk.pi_idx;
+          stk_ld[tid] = sk.dst_ld;
+          stk_nc[tid] = sk.ncols;
+          stk_start[tid + 1] = sk.a_ng * 8;
         }
-        if (!found) rv = false;
+        if (tid == 0) stk_start[0] = 0;
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        if (tid == 0)
+          for (int i = 0; i < np; ++i) stk_start[i + 1] += stk_start[i];
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        int piece = -1;
+        for (int i = 0; i < np; ++i)
+          if (r >= stk_start[i] && r < stk_start[i + 1]) piece = i;
+        rv = rv && piece >= 0;
+        if (piece >= 0) {
+          const int jl = r - stk_start[piece];
+          pib = stk_pi[piece] + it.col0;
+          if (jl < stk_nc[piece]) {
+            dst = p.scr + stk_dst[piece] + (int64_t)jl * stk_ld[piece] + it.col0;
+            rscale_stack = oz_pow2_of(p.scales[stk_rs[piece] + jl]);
+          } else {
+            rv = false;
+          }
+        }
         cstride = 1;
       }
       for (int f = 0; f < nf; ++f) {
         const uint32_t buf = famc & 1u, use = famc >> 1;
-        if (!oz_wait(oz_smem(&tfull_bar[buf]), use & 1u, &abort_sh)) {
-          if (!abort_sh) oz_fail(&abort_sh, p.err);
-          ok = false;
-          break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;");
         double rscale;
         int64_t cs_idx;
         if (it.kind == 0) {
@@ -498,6 +529,21 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
           rscale = rscale_stack;
           cs_idx = it.cs_idx;
         }
+        // column scales of this family (once per tile); thread 0 waits for the
+        // accumulators and the named barrier hands its verdict to all 128 threads
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        if (tid < it.ncols) cscale_sh[tid] = oz_pow2_of(p.scales[cs_idx + tid]);
+        if (tid == 0) {
+          const bool got = oz_wait(oz_smem(&tfull_bar[buf]), use & 1u, &abort_sh);
+          if (!got && !abort_sh) oz_fail(&abort_sh, p.err);
+          tfull_ok_sh = got ? 1 : 0;
+        }
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        if (!tfull_ok_sh) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
         for (int j0 = 0; j0 < it.N; j0 += 16) {
           uint32_t v[S][16];
 #pragma unroll
@@ -520,7 +566,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
               double acc = 0.0;
 #pragma unroll
               for (int d = S - 1; d >= 0; --d) acc += (double)(int32_t)v[d][jj] * w[d];
-              val = acc * rscale * oz_pow2_of(p.scales[cs_idx + n]);
+              val = acc * rscale * cscale_sh[n];
               if (it.kind == 0)
                 dst[(int64_t)n * cstride] += val;
               else

@@ -81,6 +81,8 @@ struct OzSeg {
 struct OzFam {
   int32_t seg_begin, seg_end;
   int64_t rs_idx, cs_idx;
+  int32_t nkb;              // k-blocks of all its segments
+  int32_t pad;
 };
 
 // A run of stacked rows of a product tile: rows of P^T = columns
@@ -112,7 +114,8 @@ struct OzItem {
   int32_t seg;              // kind 1: the segment of the shared operator
   int32_t init;
   int64_t cs_idx;           // kind 1: scale index of the operator's row 0
-  int64_t pad2;
+  int32_t nkb;              // k-blocks of all its families
+  int32_t pad2;
   int64_t cost;             // issued int8 MACs (for ordering)
 };
 

@@ -407,6 +407,18 @@ struct Builder {
       if (fr.rs_rel != REL_NONE) f.rs_idx += base[fr.rs_rel];
       if (fr.cs_rel != REL_NONE) f.cs_idx += base[fr.cs_rel];
     }
+    for (OzFam &f : oz.fams) {
+      f.nkb = 0;
+      f.pad = 0;
+      for (int i = f.seg_begin; i < f.seg_end; ++i) f.nkb += oz.segs[i].nkb;
+    }
+    for (std::vector<OzItem> *v : {&oz.items1, &oz.items2})
+      for (OzItem &it : *v) {
+        it.nkb = 0;
+        if (it.kind == 1) it.nkb = oz.segs[it.seg].nkb;
+        else
+          for (int f = it.fam_begin; f < it.fam_end; ++f) it.nkb += oz.fams[f].nkb;
+      }
     oz.psi_jobs = std::move(dyn_psi);
     oz.prod_jobs = std::move(dyn_prod);
     auto by_cost = [](std::vector<OzItem> &v) {

@@ -86,7 +86,8 @@ class OzSegC(C.Structure):
 
 
 class OzFamC(C.Structure):
-    _fields_ = [("seg_begin", C.c_int32), ("seg_end", C.c_int32), ("rs_idx", C.c_int64), ("cs_idx", C.c_int64)]
+    _fields_ = [("seg_begin", C.c_int32), ("seg_end", C.c_int32), ("rs_idx", C.c_int64), ("cs_idx", C.c_int64),
+                ("nkb", C.c_int32), ("pad_", C.c_int32)]
 
 
 class OzStackC(C.Structure):
@@ -97,7 +98,7 @@ class OzStackC(C.Structure):
 class OzItemC(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("kind", "cell", "row0", "col0", "M", "N", "mrows", "ncols", "fam_begin",
                                          "fam_end", "seg", "init")] + \
-               [("cs_idx", C.c_int64), ("pad2_", C.c_int64), ("cost", C.c_int64)]
+               [("cs_idx", C.c_int64), ("nkb", C.c_int32), ("pad2_", C.c_int32), ("cost", C.c_int64)]
 
 
 class OzCellC(C.Structure):

@@ -328,14 +328,16 @@ typedef struct tj_oz_job {
   int8_t space, want_max, pad_[6];
 } tj_oz_job;
 typedef struct tj_oz_seg { int64_t a_base, b_base; int32_t a_gtot, b_gtot, a_kb0, b_kb0, nkb, pad_; } tj_oz_seg;
-typedef struct tj_oz_fam { int32_t seg_begin, seg_end; int64_t rs_idx, cs_idx; } tj_oz_fam;
+typedef struct tj_oz_fam { int32_t seg_begin, seg_end; int64_t rs_idx, cs_idx; int32_t nkb, pad_; } tj_oz_fam;
 typedef struct tj_oz_stack {
   int64_t a_base, dst_off, rs_idx, pi_idx;
   int32_t a_gtot, a_g0, a_ng, dst_ld, ncols, pad_;
 } tj_oz_stack;
 typedef struct tj_oz_item {
   int32_t kind, cell, row0, col0, M, N, mrows, ncols, fam_begin, fam_end, seg, init;
-  int64_t cs_idx, pad2_, cost;
+  int64_t cs_idx;
+  int32_t nkb, pad2_;
+  int64_t cost;
 } tj_oz_item;
 typedef struct tj_oz_cell { int64_t off; int32_t ld, M, N, a_begin, a_end, pad_; } tj_oz_cell;
 typedef struct tj_ozaki_export {

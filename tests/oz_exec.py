@@ -16,10 +16,11 @@ from tests.plan_exec import merged_ops
 
 
 def _pow2_of(m):
+    """2^(E+1) for m = 1.f * 2^E (the device reads it off the exponent bits); 0 for m = 0."""
     m = np.asarray(m, dtype=np.float64)
     out = np.zeros_like(m)
     nz = m > 0
-    out[nz] = np.ldexp(1.0, np.frexp(m[nz])[1])
+    out[nz] = np.ldexp(1.0, np.maximum(np.frexp(m[nz])[1], -1022))
     return out
 
 
