@@ -244,9 +244,16 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   ctx->stats.n_tiles_p2 = (int64_t)P->tiles2.size();
   ctx->stats.scratch_doubles = P->scratch_len;
   ctx->stats.kernels_per_hpsi = 2 + (P->red1.empty() ? 0 : 1) + (P->red2.empty() ? 0 : 1);
+  ctx->stats.flops_launch1 = 0;
+  for (const Cell &c : P->cells1) ctx->stats.flops_launch1 += 2.0 * c.M * c.N * (double)P->tasks1[c.t_begin].K;
+  ctx->stats.flops_launch2 = P->flops - ctx->stats.flops_launch1;
   if (ctx->oz) {
     const OzPlan &oz = *ctx->oz;
     ctx->stats.int8_ops = oz.mma_ops;
+    ctx->stats.int8_ops_launch1 = oz.issued1;
+    ctx->stats.int8_ops_launch2 = oz.issued2;
+    ctx->stats.flops_launch1 = oz.flops1;
+    ctx->stats.flops_launch2 = oz.flops2;
     ctx->stats.kernels_per_hpsi = (oz.psi_jobs.empty() ? 0 : 2) + (oz.items1.empty() ? 0 : 1) +
                                   (oz.prod_jobs.empty() ? 0 : 1) + (oz.items2.empty() ? 0 : 1);
   }
@@ -269,16 +276,18 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
   launch_oz_max((const OzJob *)ctx->ozPsiJobs.p, (int)oz.psi_jobs.size(), ctx->ops.d(), in, ctx->scr.d(), scales, st);
   launch_oz_split((const OzJob *)ctx->ozPsiJobs.p, (int)oz.psi_jobs.size(), ctx->ops.d(), in, ctx->scr.d(), scales,
                   pack, oz.s, st);
+  if (timed) CK(cudaEventRecord(ctx->ev[1], st));
   CK(launch_oz_gemm((const OzItem *)ctx->ozItems1.p, (int)oz.items1.size(), (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzStack *)ctx->ozStacks.p, (const OzCell *)ctx->ozCells.p,
                     (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, st));
-  if (timed) CK(cudaEventRecord(ctx->ev[1], st));
+  if (timed) CK(cudaEventRecord(ctx->ev[2], st));
   launch_oz_split((const OzJob *)ctx->ozProdJobs.p, (int)oz.prod_jobs.size(), ctx->ops.d(), in, ctx->scr.d(), scales,
                   pack, oz.s, st);
+  if (timed) CK(cudaEventRecord(ctx->ev[3], st));
   CK(launch_oz_gemm((const OzItem *)ctx->ozItems2.p, (int)oz.items2.size(), (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzStack *)ctx->ozStacks.p, (const OzCell *)ctx->ozCells.p,
                     (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, st));
-  if (timed) CK(cudaEventRecord(ctx->ev[2], st));
+  if (timed) CK(cudaEventRecord(ctx->ev[4], st));
   CK(cudaGetLastError());
   ++ctx->n_hpsi;
   return TJ_OK;
@@ -300,7 +309,10 @@ int tjb::run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed) {
   const HpsiPlan &P = *ctx->plan;
   unsigned int *cnt = (unsigned int *)ctx->counters.p;
   CK(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), ctx->stream));
-  if (timed) CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+  if (timed) {
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+  }
   GemmParams g;
   std::memset(&g, 0, sizeof g);
   g.ops = ctx->ops.d();
@@ -315,7 +327,10 @@ int tjb::run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed) {
   g.slots = ctx->slots.d();
   launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles), ctx->stream);
   launch_reduce(g, (const Reduce *)ctx->red1.p, (int)P.red1.size(), ctx->stream);
-  if (timed) CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+  if (timed) {
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+  }
   g.out = out;
   g.cells = (const Cell *)ctx->cells2.p;
   g.tasks = (const Task *)ctx->tasks2.p;
@@ -324,7 +339,7 @@ int tjb::run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed) {
   g.counter = cnt + 1;
   launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles), ctx->stream);
   launch_reduce(g, (const Reduce *)ctx->red2.p, (int)P.red2.size(), ctx->stream);
-  if (timed) CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+  if (timed) CK(cudaEventRecord(ctx->ev[4], ctx->stream));
   CK(cudaGetLastError());
   ++ctx->n_hpsi;
   return TJ_OK;
@@ -346,6 +361,17 @@ static bool same_layout(const tj_wave *a, const tj_wave *b) {
   return std::memcmp(a->sub, b->sub, sizeof(tj_wave_sub) * a->num) == 0;
 }
 
+// Device times of the last timed H*psi: splits, first GEMM launch, second
+// GEMM launch (with its splits excluded), total.
+static void read_phases(tj_ctx *ctx, double t[4]) {
+  float e[4] = {0, 0, 0, 0};
+  for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&e[i], ctx->ev[i], ctx->ev[i + 1]);
+  t[0] = (double)e[0] + e[2];
+  t[1] = e[1];
+  t[2] = e[3];
+  t[3] = (double)e[0] + e[1] + e[2] + e[3];
+}
+
 extern "C" int tj_model_wave(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const tj_model *env,
                              const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *invec,
                              tj_wave *outvec) {
@@ -363,12 +389,12 @@ extern "C" int tj_model_wave(tj_ctx *ctx, const tj_lattice *lat, const tj_model 
   CK(cudaMemcpyAsync(outvec->data, ctx->vout.d(), sizeof(double) * D, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   if ((rc = check_device_flags(ctx))) return rc;
-  float a = 0, b = 0;
-  cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
-  cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
-  ctx->stats.last_ms_phase1 = a;
-  ctx->stats.last_ms_phase2 = b;
-  ctx->stats.last_ms = a + b;
+  double t[4];
+  read_phases(ctx, t);
+  ctx->stats.last_ms_split = t[0];
+  ctx->stats.last_ms_phase1 = t[1];
+  ctx->stats.last_ms_phase2 = t[2];
+  ctx->stats.last_ms = t[3];
   return TJ_OK;
 }
 
@@ -387,20 +413,18 @@ extern "C" int tj_model_wave_bench(tj_ctx *ctx, const tj_lattice *lat, const tj_
   CK(cudaMemcpyAsync(ctx->vin.d(), invec->data, sizeof(double) * D, cudaMemcpyHostToDevice, ctx->stream));
   if ((rc = run_hpsi(ctx, ctx->vin.d(), ctx->vout.d(), false))) return rc;   // warm-up
   CK(cudaStreamSynchronize(ctx->stream));
-  CK(cudaEventRecord(ctx->ev[3], ctx->stream));
-  double p1 = 0, p2 = 0;
+  double acc[4] = {0, 0, 0, 0};
   for (int r = 0; r < reps; ++r) {
     if ((rc = run_hpsi(ctx, ctx->vin.d(), ctx->vout.d(), true))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
-    float a = 0, b = 0;
-    cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
-    cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
-    p1 += a;
-    p2 += b;
+    double t[4];
+    read_phases(ctx, t);
+    for (int i = 0; i < 4; ++i) acc[i] += t[i];
   }
-  *ms = (p1 + p2) / reps;
-  ctx->stats.last_ms_phase1 = p1 / reps;
-  ctx->stats.last_ms_phase2 = p2 / reps;
+  *ms = acc[3] / reps;
+  ctx->stats.last_ms_split = acc[0] / reps;
+  ctx->stats.last_ms_phase1 = acc[1] / reps;
+  ctx->stats.last_ms_phase2 = acc[2] / reps;
   ctx->stats.last_ms = *ms;
   CK(cudaMemcpyAsync(outvec->data, ctx->vout.d(), sizeof(double) * D, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));

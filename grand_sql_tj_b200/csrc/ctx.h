@@ -34,7 +34,9 @@ struct DevBuf {
 struct tj_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // H*psi timing: 0 start, 1 after the splits of psi, 2 after the first GEMM
+  // launch, 3 after the product splits, 4 end (FP64: 1 = 0 and 3 = 2)
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   int prec_mode = TJ_PREC_FP64, slices = 6;
   // compiled H*psi of the current step
   std::unique_ptr<tjb::HpsiPlan> plan;

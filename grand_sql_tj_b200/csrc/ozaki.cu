@@ -470,20 +470,11 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
       int64_t cstride = 0;
       double rscale_stack = 0.0;
       int64_t pib = -1;   // kind 1: pi index of this row's product, row col0
+      OzCell c{};
       if (it.kind == 0) {
-        const OzCell c = p.cells[it.cell];
+        c = p.cells[it.cell];
         dst = p.out + c.off + (int64_t)(it.row0 + r) + (int64_t)it.col0 * c.ld;
         cstride = c.ld;
-        if (it.init && rv) {
-          for (int n = 0; n < it.ncols; ++n) {
-            double v = 0.0;
-            for (int a = c.a_begin; a < c.a_end; ++a) {
-              const Task &t = p.tasks[a];
-              v += t.coef * p.psi[t.L.off + (int64_t)(it.col0 + n) * t.L.ld + it.row0 + r];
-            }
-            dst[(int64_t)n * cstride] = v;
-          }
-        }
       } else {
         // stacked products: the runs of this tile, then the run holding this row
         const int np = it.fam_end - it.fam_begin;
@@ -517,6 +508,10 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
         }
         cstride = 1;
       }
+      // the tile row of this thread, summed over the item's families
+      double accv[BN];
+#pragma unroll
+      for (int j = 0; j < BN; ++j) accv[j] = 0.0;
       for (int f = 0; f < nf; ++f) {
         const uint32_t buf = famc & 1u, use = famc >> 1;
         double rscale;
@@ -544,35 +539,73 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;");
-        for (int j0 = 0; j0 < it.N; j0 += 16) {
-          uint32_t v[S][16];
 #pragma unroll
-          for (int d = 0; d < S; ++d) {
-            const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + buf * 256u + (uint32_t)(d * BN + j0);
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-                "[%16];"
-                : "=r"(v[d][0]), "=r"(v[d][1]), "=r"(v[d][2]), "=r"(v[d][3]), "=r"(v[d][4]), "=r"(v[d][5]),
-                  "=r"(v[d][6]), "=r"(v[d][7]), "=r"(v[d][8]), "=r"(v[d][9]), "=r"(v[d][10]), "=r"(v[d][11]),
-                  "=r"(v[d][12]), "=r"(v[d][13]), "=r"(v[d][14]), "=r"(v[d][15])
-                : "r"(ta));
-          }
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        for (int ch = 0; ch < BN / 16; ++ch) {
+          if (ch * 16 < it.N) {
+            uint32_t v[S][16];
 #pragma unroll
-          for (int jj = 0; jj < 16; ++jj) {
-            const int n = j0 + jj;
-            double val = 0.0;
-            if (rv && n < it.ncols) {
+            for (int d = 0; d < S; ++d) {
+              const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + buf * 256u + (uint32_t)(d * BN + ch * 16);
+              asm volatile(
+                  "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                  "[%16];"
+                  : "=r"(v[d][0]), "=r"(v[d][1]), "=r"(v[d][2]), "=r"(v[d][3]), "=r"(v[d][4]), "=r"(v[d][5]),
+                    "=r"(v[d][6]), "=r"(v[d][7]), "=r"(v[d][8]), "=r"(v[d][9]), "=r"(v[d][10]), "=r"(v[d][11]),
+                    "=r"(v[d][12]), "=r"(v[d][13]), "=r"(v[d][14]), "=r"(v[d][15])
+                  : "r"(ta));
+            }
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int jj = 0; jj < 16; ++jj) {
               double acc = 0.0;
 #pragma unroll
               for (int d = S - 1; d >= 0; --d) acc += (double)(int32_t)v[d][jj] * w[d];
-              val = acc * rscale * cscale_sh[n];
-              if (it.kind == 0)
-                dst[(int64_t)n * cstride] += val;
-              else
-                dst[n] = val;
+              accv[ch * 16 + jj] += acc * rscale * cscale_sh[ch * 16 + jj];
             }
-            if (it.kind == 1) {
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        oz_arrive(oz_smem(&tempty_bar[buf]));
+        ++famc;
+      }
+      if (!ok) break;
+      // store the tile row once: loads of a 16-column chunk first, then the stores
+      if (it.kind == 0) {
+#pragma unroll
+        for (int ch = 0; ch < BN / 16; ++ch) {
+          if (rv && ch * 16 < it.ncols) {
+            double old[16];
+#pragma unroll
+            for (int jj = 0; jj < 16; ++jj) {
+              const int n = ch * 16 + jj;
+              old[jj] = 0.0;
+              if (n < it.ncols) {
+                if (it.init) {
+                  for (int a = c.a_begin; a < c.a_end; ++a) {
+                    const Task &t = p.tasks[a];
+                    old[jj] += t.coef * p.psi[t.L.off + (int64_t)(it.col0 + n) * t.L.ld + it.row0 + r];
+                  }
+                } else {
+                  old[jj] = dst[(int64_t)n * cstride];
+                }
+              }
+            }
+#pragma unroll
+            for (int jj = 0; jj < 16; ++jj) {
+              const int n = ch * 16 + jj;
+              if (n < it.ncols) dst[(int64_t)n * cstride] = old[jj] + accv[n];
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int ch = 0; ch < BN / 16; ++ch) {
+          if (ch * 16 < it.N) {
+#pragma unroll
+            for (int jj = 0; jj < 16; ++jj) {
+              const int n = ch * 16 + jj;
+              const double val = (rv && n < it.ncols) ? accv[n] : 0.0;
+              if (rv && n < it.ncols) dst[n] = val;
               // pi: max |P(i, .)| over each 8-row group (one product), one atomic per group and column
               double m = fabs(val);
               for (int o = 1; o < 8; o <<= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -581,9 +614,6 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
             }
           }
         }
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        oz_arrive(oz_smem(&tempty_bar[buf]));
-        ++famc;
       }
     }
   }

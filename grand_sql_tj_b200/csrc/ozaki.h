@@ -146,6 +146,8 @@ struct OzPlan {
   std::vector<OzCell> cells;
   std::vector<OzItem> items1, items2;      // launch 1 (products, left, right), launch 2 (two-sided)
   double mma_ops = 0;                      // 2 x int8 MACs issued per H*psi
+  double issued1 = 0, issued2 = 0;         // ... per launch
+  double flops1 = 0, flops2 = 0;           // FP64-equivalent flops of each launch
 };
 
 // Builds the split-precision form of an H*psi plan (host).

@@ -431,7 +431,17 @@ struct Builder {
     for (const std::vector<OzItem> *v : {&oz.items1, &oz.items2})
       for (const OzItem &it : *v) {
         oz.mma_ops += 2.0 * it.cost;
+        (v == &oz.items1 ? oz.issued1 : oz.issued2) += 2.0 * it.cost;
         kmax = std::max<int64_t>(kmax, it.cost / ((int64_t)it.M * it.N * (S * (S + 1) / 2)));
+      }
+    // FP64-equivalent work: products and one-sided tasks in launch 1, two-sided tasks in launch 2
+    oz.flops1 = oz.flops2 = 0;
+    for (const Cell &c : hp.cells1) oz.flops1 += 2.0 * c.M * c.N * (double)hp.tasks1[c.t_begin].K;
+    for (const Cell &c : hp.cells2)
+      for (int ti = c.t_begin; ti < c.t_end; ++ti) {
+        const Task &t = hp.tasks2[ti];
+        if (t.R.space == SP_NONE) continue;
+        (t.L.space == SP_SCR ? oz.flops2 : oz.flops1) += 2.0 * c.M * c.N * (double)t.K;
       }
     // exact int32 accumulation: a diagonal sums <= s slice products of 127^2 per k
     if ((double)kmax * S * 127.0 * 127.0 >= 2147483647.0)

@@ -90,7 +90,9 @@ class TjHpsiStats(C.Structure):
                 ("n_tiles_p2", C.c_int64), ("scratch_doubles", C.c_int64),
                 ("last_ms", C.c_double), ("last_ms_phase1", C.c_double),
                 ("last_ms_phase2", C.c_double), ("lanczos_hpsi", C.c_int64),
-                ("int8_ops", C.c_double), ("kernels_per_hpsi", C.c_int64)]
+                ("int8_ops", C.c_double), ("kernels_per_hpsi", C.c_int64), ("last_ms_split", C.c_double),
+                ("flops_launch1", C.c_double), ("flops_launch2", C.c_double),
+                ("int8_ops_launch1", C.c_double), ("int8_ops_launch2", C.c_double)]
 
 
 def _dptr(a: np.ndarray):

@@ -224,10 +224,13 @@ typedef struct tj_hpsi_stats {
   double bytes;            /* algorithmic HBM bytes per H*psi                    */
   int64_t n_products, n_tasks, n_tiles_p1, n_tiles_p2, scratch_doubles;
   double last_ms;          /* device time of the last H*psi                      */
-  double last_ms_phase1, last_ms_phase2;
+  double last_ms_phase1, last_ms_phase2;  /* its first / second GEMM launch          */
   int64_t lanczos_hpsi;    /* H*psi products of the last tj_lanczos_memo_new      */
   double int8_ops;         /* split precision: 2 x int8 MACs issued per H*psi     */
   int64_t kernels_per_hpsi; /* kernel launches of one H*psi                        */
+  double last_ms_split;    /* split precision: its max/split kernels             */
+  double flops_launch1, flops_launch2;  /* FP64-equivalent flops of each launch    */
+  double int8_ops_launch1, int8_ops_launch2;  /* split precision: issued per launch */
 } tj_hpsi_stats;
 int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st);
 

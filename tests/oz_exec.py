@@ -119,13 +119,15 @@ class _Machine:
                 cols = it.col0 + np.arange(it.ncols)
                 idx = c.off + rows[:, None] + cols[None, :] * c.ld
                 if it.init:
-                    v = np.zeros((it.mrows, it.ncols))
+                    old = np.zeros((it.mrows, it.ncols))
                     tasks = self.plan["tasks2"]
                     for a in range(c.a_begin, c.a_end):
                         t = tasks[a]
                         b = self.spaces[t.L.space]
-                        v = v + t.coef * b[t.L.off + cols[None, :] * t.L.ld + rows[:, None]]
-                    self.out[idx] = v
+                        old = old + t.coef * b[t.L.off + cols[None, :] * t.L.ld + rows[:, None]]
+                else:
+                    old = self.out[idx]
+                tot = np.zeros((it.mrows, it.ncols))
                 for f in range(it.fam_begin, it.fam_end):
                     fm = oz["fams"][f]
                     acc = 0
@@ -139,7 +141,8 @@ class _Machine:
                     acc = self.accum(A, B)
                     rs = _pow2_of(self.scales[fm.rs_idx + rows])
                     cs = _pow2_of(self.scales[fm.cs_idx + cols])
-                    self.out[idx] = self.out[idx] + (acc * rs[:, None]) * cs[None, :]
+                    tot = tot + (acc * rs[:, None]) * cs[None, :]
+                self.out[idx] = old + tot
             else:
                 sg = oz["segs"][it.seg]
                 pieces = [oz["stacks"][si] for si in range(it.fam_begin, it.fam_end)]
