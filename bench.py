@@ -1,15 +1,25 @@
 #!/usr/bin/env python
 """Benchmark of the tjsq hot path on B200: H*psi per second on a 4x24 t-J
-cylinder superblock at m = 2000 multiplets (mid-chain, 12 holes, S = 0).
+cylinder superblock at m = 2000 multiplets (mid-chain, 12 holes, S = 0),
+split-precision ("mixed": int8 slices on the tensor cores, FP64 elsewhere)
+against the plain FP64 GPU path.
 
 One "step" is one H*psi (hmerge'd model_wave) over the whole superblock with
 operators and psi resident in HBM.  The superblock is synthetic (seeded):
 sector tables, bases and operator blocks with the reference's quantum-number
 structure at the sizes of that configuration (no DMRG run of the reference
-can be reproduced here).  Its operators (about 0.2 GB) and phase-1 products
-(about 0.14 GB) exceed the 126 MB L2, so no explicit L2 flush is done.
+can be reproduced here).  Its operators (about 0.2 GB), slice pools (about
+0.5 GB) and phase-1 products (about 0.14 GB) exceed the 126 MB L2, so no
+explicit L2 flush is done.
 
-  python bench.py [--gpus N --steps K --warmup W --impl b200|reference]
+  python bench.py [--gpus N --steps K --warmup W --impl b200|reference
+                   --precision mixed|fp64|ozaki --slices S]
+
+mixed (default): the split-precision H*psi is the timed value; an FP64 leg
+gives the speed-up, and Lanczos in both precisions from the same start
+vector gives |dE|/site and ||psi - psi_FP64||.  The end-to-end leg is
+tj_lanczos_memo_new through the C ABI with host buffers, followed by the
+system-block truncation (one DMRG step of the hot path).
 
 --impl reference times the oracle (the C restatement of the reference's
 Fortran routines, FP64, OpenBLAS with every host thread) on the same
@@ -39,8 +49,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="cyl4x24_m2000")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "ozaki"])
-    ap.add_argument("--slices", type=int, default=6)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "ozaki"],
+                    help="mixed: split-precision H*psi timed, FP64 leg for the speed-up and the accuracy check")
+    ap.add_argument("--slices", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end Lanczos leg (profiling runs)")
     ap.add_argument("--seed", type=int, default=1234)
@@ -187,6 +198,43 @@ def profile_traffic(workload: str, precision: str):
         return None
 
 
+def int8_peak_tops(device: int) -> float:
+    """cuBLASLt int8 GEMM throughput on this GPU (torch._int_mm, best of a few 8192^3 products)."""
+    import torch
+    n = 8192
+    a = torch.randint(-127, 127, (n, n), dtype=torch.int8, device="cuda:%d" % device)
+    b = torch.randint(-127, 127, (n, n), dtype=torch.int8, device="cuda:%d" % device)
+    torch._int_mm(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch._int_mm(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2.0 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def run_leg(ctx, sb, steps: int, warmup: int):
+    """Device-timed H*psi on a resident superblock: (ms per H*psi, stats)."""
+    ctx.model_wave_bench(sb, max(warmup, 3))
+    ms, _ = ctx.model_wave_bench(sb, steps)
+    return ms, ctx.stats()
+
+
+def lanczos_leg(ctx, sb, lanzero: float):
+    """tj_lanczos_memo_new through the C ABI with host buffers (plan, uploads, iterations, Ritz vector)."""
+    ctx.step_begin()
+    t0 = time.perf_counter()
+    e0, iters, w = ctx.lanczos_memo_new(sb, lanzero)
+    wall = time.perf_counter() - t0
+    return e0, iters, w, wall, ctx.stats()
+
+
 def main():
     args = parse()
     ws, rank, local, pg = dist_init(args)
@@ -220,32 +268,37 @@ def main():
 
     from grand_sql_tj_b200 import build as B
     B.build()
-    from grand_sql_tj_b200.lib import Context, TJ_PREC_FP64, TJ_PREC_OZAKI
-    ctx = Context(local)
-    if args.precision == "ozaki":
-        ctx.set_precision(TJ_PREC_OZAKI, args.slices)
-    # warm-up (compiles the plan, uploads operators and psi)
-    ms_w, _ = ctx.model_wave_bench(sb, max(args.warmup, 3))
+    import numpy as np
+    from grand_sql_tj_b200.lib import Context, TJ_PREC_OZAKI
+    mixed = args.precision in ("mixed", "ozaki")
+    ctx64 = Context(local)
+    ctxoz = None
+    if mixed:
+        ctxoz = Context(local)
+        ctxoz.set_precision(TJ_PREC_OZAKI, args.slices)
+    head = ctxoz if mixed else ctx64
+    # untimed legs first: the other precision (for the speed-up) and warm-up
+    ms64 = st64 = None
+    if args.precision == "mixed":
+        ms64, st64 = run_leg(ctx64, sb, max(20, args.steps // 4), args.warmup)
+    head.model_wave_bench(sb, max(args.warmup, 3))
     barrier(pg, args.impl)
     with Clocks(local) as clk:
         barrier(pg, args.impl)
         t0 = time.perf_counter()
-        ms, out = ctx.model_wave_bench(sb, args.steps)
+        ms, _ = head.model_wave_bench(sb, args.steps)
         wall = time.perf_counter() - t0
         barrier(pg, args.impl)
-    st = ctx.stats()
+    st = head.stats()
     ms_max = allmax(pg, ms, args.impl)
     value = ws * 1000.0 / ms_max
 
-    e2e = None
+    e2e = accuracy = step = None
     if not args.no_e2e:
-        # end to end through the reference-facing call: lanczos_memo_new with host buffers
-        ctx.step_begin()
+        # end to end through the reference-facing call (host buffers), at the
+        # reference's sweep threshold lanzero = 2e-5
         lz = 20.0e-6
-        t0 = time.perf_counter()
-        e0, iters, _ = ctx.lanczos_memo_new(sb, lz)
-        e2e_wall = time.perf_counter() - t0
-        st2 = ctx.stats()
+        e0, iters, w, e2e_wall, st2 = lanczos_leg(head, sb, lz)
         nh = max(int(st2.lanczos_hpsi), 1)
         e2e_wall = allmax(pg, e2e_wall, args.impl)
         ops_bytes = 0
@@ -258,19 +311,54 @@ def main():
                "%d H*psi + Ritz vector download)" % nh,
                "h2d_bytes_per_step": int((ops_bytes + 8 * sb.wave.dim) / nh),
                "d2h_bytes_per_step": int(8 * sb.wave.dim / nh), "lanczos_iters": iters, "E0": e0}
+        # one DMRG step of the hot path: Lanczos + truncation of the system block
+        t0 = time.perf_counter()
+        kept = head.truncation(w, 0, 2000, 2000, 1e-12)
+        trunc_s = time.perf_counter() - t0
+        nsite = sb.geo.num_site
+        step = {"lanczos_s": e2e_wall, "truncation_s": trunc_s, "dmrg_step_s": e2e_wall + trunc_s,
+                "sweep_s_upper": 2 * (nsite - 3) * (e2e_wall + trunc_s),
+                "note": "mid-chain step; a sweep has 2*(N_site-3) steps, most of them on smaller superblocks"}
+        if mixed:
+            # the split-precision result against FP64 on the same start vector and threshold
+            e64, it64, w64, wall64, _ = lanczos_leg(ctx64, sb, lz)
+            ov = float(np.dot(w.data, w64.data))
+            dpsi = float(np.linalg.norm(w.data - np.sign(ov) * w64.data))
+            de = abs(e0 - e64) / nsite
+            accuracy = {"E0_mixed": e0, "E0_fp64": e64, "dE_per_site": de, "psi_diff_norm": dpsi,
+                        "iters_mixed": iters, "iters_fp64": it64, "ok": bool(de <= 1e-9),
+                        "fp64_lanczos_s": wall64}
+        del kept
 
     peaks = measured_peaks()
-    if rank == 0:
-        fp64 = fp64_peak_tflops(local)
+    fp64 = fp64_peak_tflops(local) if rank == 0 else None
+    if mixed:
+        i8 = int8_peak_tops(local) if rank == 0 else None
+        t1, t2 = st.last_ms_phase1, st.last_ms_phase2
+        dom = 1 if t1 >= t2 else 2
+        tdom = max(t1, t2)
+        s_ = args.slices
+        alg = (st.flops_launch1 if dom == 1 else st.flops_launch2) * s_ * (s_ + 1) / 2
+        issued = st.int8_ops_launch1 if dom == 1 else st.int8_ops_launch2
+        achieved = alg / (tdom * 1e-3) / 1e12
+        roof = {"bound": "tensor", "kernel": "oz_gemm_kernel (launch %d)" % dom, "achieved": achieved,
+                "peak": i8, "unit": "TFLOP/s", "frac": (achieved / i8) if i8 else None,
+                "traffic": profile_traffic(args.workload, "ozaki"),
+                "peak_source": "measured cuBLASLt int8 GEMM 8192^3 (torch._int_mm) on this GPU; int8 ops",
+                "work": "algorithmic int8 ops = FP64-equivalent flops of the launch x s(s+1)/2 slice products",
+                "issued_int8_ops": issued, "launch_ms": tdom,
+                "launch1_ms": t1, "launch2_ms": t2, "splits_ms": st.last_ms_split,
+                "fp64_equiv_tflops": st.flops / (ms * 1e-3) / 1e12,
+                "fp64_dgemm_peak_tflops": fp64}
     else:
-        fp64 = None
-    achieved = st.flops / (ms * 1e-3) / 1e12
-    roof = {"bound": "tensor", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
-            "frac": (achieved / fp64) if fp64 else None, "traffic": profile_traffic(args.workload, args.precision),
-            "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU (FP64; not in MEASURED_PEAKS.json)",
-            "flops_per_hpsi": st.flops, "flops_ref_per_hpsi": st.flops_ref, "bytes_per_hpsi": st.bytes,
-            "hbm_frac": (st.bytes / (ms * 1e-3) / 1e9) / peaks.get("hbm_gbs", 6555.8),
-            "phase1_ms": st.last_ms_phase1, "phase2_ms": st.last_ms_phase2}
+        achieved = st.flops / (ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "kernel": "grouped_gemm_kernel (both phases)", "achieved": achieved,
+                "peak": fp64, "unit": "TFLOP/s", "frac": (achieved / fp64) if fp64 else None,
+                "traffic": profile_traffic(args.workload, "fp64"),
+                "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU (FP64; not in MEASURED_PEAKS.json)",
+                "phase1_ms": st.last_ms_phase1, "phase2_ms": st.last_ms_phase2}
+    roof.update({"flops_per_hpsi": st.flops, "flops_ref_per_hpsi": st.flops_ref, "bytes_per_hpsi": st.bytes,
+                 "hbm_frac": (st.bytes / (ms * 1e-3) / 1e9) / peaks.get("hbm_gbs", 6555.8)})
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -280,12 +368,24 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": max(args.warmup, 3), "ms_per_step": ms_max, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "int8-ozaki",
-                "data": "synthetic", "config": cfg, "precision": args.precision,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "int8 slices (s=%d) + f64" % args.slices if mixed else "f64",
+                "data": "synthetic", "config": cfg,
+                "precision": "mixed" if mixed else "fp64",
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
                 "gpu_launches": int(st.kernels_per_hpsi) * args.steps, "wall_s_timed": wall}
+        if ms64 is not None:
+            line["fp64"] = {"value": ws * 1000.0 / ms64, "ms_per_step": ms64, "unit": UNIT,
+                            "phase1_ms": st64.last_ms_phase1, "phase2_ms": st64.last_ms_phase2}
+            line["speedup_vs_fp64"] = ms64 / ms
+        if accuracy is not None:
+            line["accuracy"] = accuracy
+        if step is not None:
+            line["sweep"] = step
         print(json.dumps(line), flush=True)
-    ctx.close()
+    ctx64.close()
+    if ctxoz is not None:
+        ctxoz.close()
     if pg is not None:
         pg.destroy_process_group()
 

@@ -210,7 +210,9 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
     // split-precision form: regroup the tasks, split the operators once for this step
     std::unique_ptr<OzPlan> oz(new OzPlan());
     try {
-      build_ozaki_plan(*P, ctx->slices, *oz);
+      int nsm = 148;
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+      build_ozaki_plan(*P, ctx->slices, nsm, *oz);
     } catch (const std::exception &e) {
       return set_err(TJ_ERR_ARG, std::string("split-precision plan: ") + e.what());
     }
@@ -218,7 +220,8 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
         (rc = upload_vec(ctx, ctx->ozProdJobs, oz->prod_jobs)) || (rc = upload_vec(ctx, ctx->ozSegs, oz->segs)) ||
         (rc = upload_vec(ctx, ctx->ozFams, oz->fams)) || (rc = upload_vec(ctx, ctx->ozStacks, oz->stacks)) ||
         (rc = upload_vec(ctx, ctx->ozCells, oz->cells)) || (rc = upload_vec(ctx, ctx->ozItems1, oz->items1)) ||
-        (rc = upload_vec(ctx, ctx->ozItems2, oz->items2)))
+        (rc = upload_vec(ctx, ctx->ozItems2, oz->items2)) || (rc = upload_vec(ctx, ctx->ozCta1, oz->cta1)) ||
+        (rc = upload_vec(ctx, ctx->ozCta2, oz->cta2)))
       return rc;
     if ((rc = ctx->ozPack.reserve(oz->sta_pack + oz->dyn_pack + 256)) ||
         (rc = ctx->ozScales.reserve(sizeof(double) * (oz->n_scales + 4))) || (rc = ctx->ozMisc.reserve(256)))
@@ -277,14 +280,16 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
   launch_oz_split((const OzJob *)ctx->ozPsiJobs.p, (int)oz.psi_jobs.size(), ctx->ops.d(), in, ctx->scr.d(), scales,
                   pack, oz.s, st);
   if (timed) CK(cudaEventRecord(ctx->ev[1], st));
-  CK(launch_oz_gemm((const OzItem *)ctx->ozItems1.p, (int)oz.items1.size(), (const OzSeg *)ctx->ozSegs.p,
+  CK(launch_oz_gemm((const OzItem *)ctx->ozItems1.p, (const int32_t *)ctx->ozCta1.p, (int)oz.cta1.size() - 1,
+                    (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzStack *)ctx->ozStacks.p, (const OzCell *)ctx->ozCells.p,
                     (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, st));
   if (timed) CK(cudaEventRecord(ctx->ev[2], st));
   launch_oz_split((const OzJob *)ctx->ozProdJobs.p, (int)oz.prod_jobs.size(), ctx->ops.d(), in, ctx->scr.d(), scales,
                   pack, oz.s, st);
   if (timed) CK(cudaEventRecord(ctx->ev[3], st));
-  CK(launch_oz_gemm((const OzItem *)ctx->ozItems2.p, (int)oz.items2.size(), (const OzSeg *)ctx->ozSegs.p,
+  CK(launch_oz_gemm((const OzItem *)ctx->ozItems2.p, (const int32_t *)ctx->ozCta2.p, (int)oz.cta2.size() - 1,
+                    (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzStack *)ctx->ozStacks.p, (const OzCell *)ctx->ozCells.p,
                     (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, st));
   if (timed) CK(cudaEventRecord(ctx->ev[4], st));

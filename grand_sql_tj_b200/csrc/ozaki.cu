@@ -121,17 +121,18 @@ __global__ void __launch_bounds__(256) oz_split_kernel(const OzJob *jobs, const 
       }
     }
     const int kb = c16 >> 1, c = c16 & 1, g = r >> 3, r8 = r & 7;
-    uint8_t *dst = pack + J.dst + ((int64_t)(J.kb0 + kb) * J.gtot + g) * (S * 256) + c * 128 + r8 * 16;
+    uint8_t *dst = pack + J.dst + ((int64_t)(J.kb0 + kb) * S * J.gtot + g) * 256 + c * 128 + r8 * 16;
+    const int64_t plane = (int64_t)J.gtot * 256;   // bytes of one slice of one k-block
 #pragma unroll
     for (int q = 0; q < S; ++q)
-      *reinterpret_cast<uint4 *>(dst + q * 256) = make_uint4(dig[q][0], dig[q][1], dig[q][2], dig[q][3]);
+      *reinterpret_cast<uint4 *>(dst + q * plane) = make_uint4(dig[q][0], dig[q][1], dig[q][2], dig[q][3]);
   }
 }
 
 // ------------------------------------------------------------ tcgen05 GEMM
 struct OzGemmParams {
   const OzItem *items;
-  int nitems;
+  const int32_t *cta;   // CTA b runs items [cta[b], cta[b+1])
   const OzSeg *segs;
   const OzFam *fams;
   const OzStack *stacks;
@@ -298,7 +299,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
       __syncwarp();
       return good != 0;
     };
-    for (int ii = blockIdx.x; ii < p.nitems && ok; ii += gridDim.x) {
+    for (int ii = p.cta[blockIdx.x], ie = p.cta[blockIdx.x + 1]; ii < ie && ok; ++ii) {
       const OzItem it = p.items[ii];
       const uint32_t gb = (uint32_t)((it.ncols + 7) >> 3), b_g0 = (uint32_t)(it.col0 >> 3);
       if (it.kind == 1) {
@@ -320,6 +321,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
         }
         const int32_t tot = __shfl_sync(0xffffffffu, off, 31);
         off -= ang;
+        const uint32_t bslice = (uint32_t)(it.N >> 3) * 256u;   // smem bytes of one B slice
         for (int kb = 0; kb < sg.nkb; ++kb) {
           if (!acquire(((uint32_t)tot + gb) * GB)) {
             ok = false;
@@ -327,15 +329,23 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
           }
           const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE), sbb = sa + C::A_BYTES;
           const uint32_t fb = oz_smem(&full_bar[stage]);
+          // A: lane i (< np) copies its run, slice by slice, to the run's group offset in each slice
           if (lane < np)
-            oz_bulk_g2s(sa + (uint32_t)off * GB, p.pack + abase + ((int64_t)kb * agtot + ag0) * GB,
-                        (uint32_t)ang * GB, fb);
-          if (lane == 31)
-            oz_bulk_g2s(sbb, p.pack + sg.b_base + ((int64_t)(sg.b_kb0 + kb) * sg.b_gtot + b_g0) * GB, gb * GB, fb);
+            for (int q = 0; q < S; ++q)
+              oz_bulk_g2s(sa + (uint32_t)q * 4096u + (uint32_t)off * 256u,
+                          p.pack + abase + (((int64_t)kb * S + q) * agtot + ag0) * 256, (uint32_t)ang * 256u, fb);
+          // B: lanes 16.. copy one slice each
+          if (lane >= 16 && lane < 16 + S) {
+            const int q = lane - 16;
+            oz_bulk_g2s(sbb + (uint32_t)q * bslice,
+                        p.pack + sg.b_base + (((int64_t)(sg.b_kb0 + kb) * S + q) * sg.b_gtot + b_g0) * 256,
+                        gb * 256u, fb);
+          }
           if (++stage == ST) stage = 0, ph ^= 1u;
         }
       } else {
         const uint32_t ga = (uint32_t)((it.mrows + 7) >> 3), a_g0 = (uint32_t)(it.row0 >> 3);
+        const uint32_t bslice = (uint32_t)(it.N >> 3) * 256u;
         for (int f = it.fam_begin; f < it.fam_end && ok; ++f) {
           const OzFam fm = p.fams[f];
           for (int s0 = fm.seg_begin; s0 < fm.seg_end && ok; s0 += 32) {
@@ -358,10 +368,17 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
                 }
                 const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE), sbb = sa + C::A_BYTES;
                 const uint32_t fb = oz_smem(&full_bar[stage]);
-                if (lane == 0)
-                  oz_bulk_g2s(sa, p.pack + a_base + ((int64_t)(a_kb0 + kb) * a_gtot + a_g0) * GB, ga * GB, fb);
-                if (lane == 1)
-                  oz_bulk_g2s(sbb, p.pack + b_base + ((int64_t)(b_kb0 + kb) * b_gtot + b_g0) * GB, gb * GB, fb);
+                // lanes 0..S-1: A slices; lanes 16..16+S-1: B slices
+                if (lane < S)
+                  oz_bulk_g2s(sa + (uint32_t)lane * 4096u,
+                              p.pack + a_base + (((int64_t)(a_kb0 + kb) * S + lane) * a_gtot + a_g0) * 256,
+                              ga * 256u, fb);
+                if (lane >= 16 && lane < 16 + S) {
+                  const int q = lane - 16;
+                  oz_bulk_g2s(sbb + (uint32_t)q * bslice,
+                              p.pack + b_base + (((int64_t)(b_kb0 + kb) * S + q) * b_gtot + b_g0) * 256, gb * 256u,
+                              fb);
+                }
                 if (++stage == ST) stage = 0, ph ^= 1u;
               }
             }
@@ -381,10 +398,14 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
       uint32_t ph = 0;
       uint32_t famc = 0;
       bool ok = true, issued = false;
-      const uint64_t dbase = oz_desc(0u, 128u, S * 256u);   // start address added per stage
-      for (int ii = blockIdx.x; ii < p.nitems && ok; ii += gridDim.x) {
+      const uint64_t dbase = oz_desc(0u, 128u, 256u);   // start address added per stage
+      for (int ii = p.cta[blockIdx.x], ie = p.cta[blockIdx.x + 1]; ii < ie && ok; ++ii) {
         const OzItem it = p.items[ii];
-        const uint32_t idesc = oz_idesc(it.M, it.N);
+        // MMA pa multiplies A slice pa with B slices 1..S+1-pa (N' = (S+1-pa) N):
+        // its column block q lands on the accumulator of diagonal pa+q at column (pa+q-2) N
+        uint32_t idesc[S];
+#pragma unroll
+        for (int pa = 1; pa <= S; ++pa) idesc[pa - 1] = oz_idesc(it.M, (S + 1 - pa) * it.N);
         const int nf = it.kind == 1 ? 1 : it.fam_end - it.fam_begin;
         for (int f = 0; f < nf && ok; ++f) {
           const int nkb = it.kind == 1 ? it.nkb : p.fams[it.fam_begin + f].nkb;
@@ -405,23 +426,18 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
             asm volatile("tcgen05.fence::after_thread_sync;");
             const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE);
             const uint64_t da0 = dbase + (uint64_t)(sa >> 4);
-            const uint64_t db0 = dbase + (uint64_t)((sa + C::A_BYTES) >> 4);
-            const uint32_t acc0 = kb == 0 ? 0u : 1u;
+            const uint64_t db = dbase + (uint64_t)((sa + C::A_BYTES) >> 4);
 #pragma unroll
             for (int pa = 1; pa <= S; ++pa) {
-#pragma unroll
-              for (int qb = 1; pa + qb <= S + 1; ++qb) {
-                const uint64_t da = da0 + (uint64_t)((pa - 1) * 16);   // +256 bytes per slice
-                const uint64_t db = db0 + (uint64_t)((qb - 1) * 16);
-                const uint32_t d = dt + (uint32_t)((pa + qb - 2) * BN);
-                const uint32_t acc = pa == 1 ? acc0 : 1u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "setp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-                    :
-                    : "r"(d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
-              }
+              const uint64_t da = da0 + (uint64_t)((pa - 1) * 256);   // +4096 bytes per A slice
+              const uint32_t d = dt + (uint32_t)((pa - 1) * it.N);
+              const uint32_t acc = (kb == 0 && pa == 1) ? 0u : 1u;
+              asm volatile(
+                  "{\n\t.reg .pred p;\n\t"
+                  "setp.ne.b32 p, %4, 0;\n\t"
+                  "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                  :
+                  : "r"(d), "l"(da), "l"(db), "r"(idesc[pa - 1]), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
             }
             issued = true;
             oz_commit(oz_smem(&empty_bar[stage]));   // frees the stage when these MMAs finish
@@ -452,7 +468,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
       }
     }
     bool ok = true;
-    for (int ii = blockIdx.x; ii < p.nitems && ok; ii += gridDim.x) {
+    for (int ii = p.cta[blockIdx.x], ie = p.cta[blockIdx.x + 1]; ii < ie && ok; ++ii) {
       const OzItem it = p.items[ii];
       // TMEM lane of this thread = 32*warp + lane; the tile row it holds:
       //   M = 128: row = 32*warp + lane; M = 64: rows 16w..16w+15 in lanes 32w..32w+15
@@ -545,7 +561,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
             uint32_t v[S][16];
 #pragma unroll
             for (int d = 0; d < S; ++d) {
-              const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + buf * 256u + (uint32_t)(d * BN + ch * 16);
+              const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + buf * 256u + (uint32_t)(d * it.N + ch * 16);
               asm volatile(
                   "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
                   "[%16];"
@@ -644,31 +660,27 @@ void launch_oz_split(const OzJob *jobs, int njobs, const double *ops, const doub
 }
 
 template <int S, int BN>
-static cudaError_t launch_gemm_t(const OzGemmParams &p, cudaStream_t st) {
+static cudaError_t launch_gemm_t(const OzGemmParams &p, int ncta, cudaStream_t st) {
   using Cf = OzCfg<S, BN>;
   cudaError_t e = cudaFuncSetAttribute(oz_gemm_kernel<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cf::SMEM);
   if (e != cudaSuccess) return e;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = p.nitems < sms ? p.nitems : sms;
-  oz_gemm_kernel<S, BN><<<grid, 192, Cf::SMEM, st>>>(p);
+  oz_gemm_kernel<S, BN><<<ncta, 192, Cf::SMEM, st>>>(p);
   return cudaGetLastError();
 }
 
-cudaError_t launch_oz_gemm(const OzItem *items, int nitems, const OzSeg *segs, const OzFam *fams,
+cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
                            const OzStack *stacks, const OzCell *cells, const Task *tasks, const uint8_t *pack,
                            double *scales, const double *psi, double *scr, double *out, int *err, int s,
                            cudaStream_t st) {
-  if (nitems <= 0) return cudaSuccess;
-  OzGemmParams p{items, nitems, segs, fams, stacks, cells, tasks, pack, scales, psi, scr, out, err};
+  if (ncta <= 0) return cudaSuccess;
+  OzGemmParams p{items, cta, segs, fams, stacks, cells, tasks, pack, scales, psi, scr, out, err};
   switch (s) {
-    case 3: return launch_gemm_t<3, 48>(p, st);
-    case 4: return launch_gemm_t<4, 48>(p, st);
-    case 5: return launch_gemm_t<5, 48>(p, st);
-    case 6: return launch_gemm_t<6, 32>(p, st);
-    case 7: return launch_gemm_t<7, 32>(p, st);
-    case 8: return launch_gemm_t<8, 32>(p, st);
+    case 3: return launch_gemm_t<3, 48>(p, ncta, st);
+    case 4: return launch_gemm_t<4, 48>(p, ncta, st);
+    case 5: return launch_gemm_t<5, 48>(p, ncta, st);
+    case 6: return launch_gemm_t<6, 32>(p, ncta, st);
+    case 7: return launch_gemm_t<7, 32>(p, ncta, st);
+    case 8: return launch_gemm_t<8, 32>(p, ncta, st);
     default: return cudaErrorInvalidValue;
   }
 }

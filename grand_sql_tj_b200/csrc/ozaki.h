@@ -145,20 +145,24 @@ struct OzPlan {
   std::vector<OzStack> stacks;
   std::vector<OzCell> cells;
   std::vector<OzItem> items1, items2;      // launch 1 (products, left, right), launch 2 (two-sided)
+  // static schedule: CTA b of a launch runs items [cta[b], cta[b+1]) in order
+  // (longest-processing-time-first assignment over nsm CTAs)
+  std::vector<int32_t> cta1, cta2;
+  int nsm = 148;
   double mma_ops = 0;                      // 2 x int8 MACs issued per H*psi
   double issued1 = 0, issued2 = 0;         // ... per launch
   double flops1 = 0, flops2 = 0;           // FP64-equivalent flops of each launch
 };
 
 // Builds the split-precision form of an H*psi plan (host).
-void build_ozaki_plan(const HpsiPlan &hp, int s, OzPlan &oz);
+void build_ozaki_plan(const HpsiPlan &hp, int s, int nsm, OzPlan &oz);
 
 // device launches (ozaki.cu)
 void launch_oz_max(const OzJob *jobs, int njobs, const double *ops, const double *psi, const double *scr,
                    double *scales, cudaStream_t st);
 void launch_oz_split(const OzJob *jobs, int njobs, const double *ops, const double *psi, const double *scr,
                      const double *scales, uint8_t *pack, int s, cudaStream_t st);
-cudaError_t launch_oz_gemm(const OzItem *items, int nitems, const OzSeg *segs, const OzFam *fams,
+cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
                            const OzStack *stacks, const OzCell *cells, const Task *tasks, const uint8_t *pack,
                            double *scales, const double *psi, double *scr, double *out, int *err, int s,
                            cudaStream_t st);

@@ -421,11 +421,8 @@ struct Builder {
       }
     oz.psi_jobs = std::move(dyn_psi);
     oz.prod_jobs = std::move(dyn_prod);
-    auto by_cost = [](std::vector<OzItem> &v) {
-      std::stable_sort(v.begin(), v.end(), [](const OzItem &a, const OzItem &b) { return a.cost > b.cost; });
-    };
-    by_cost(oz.items1);
-    by_cost(oz.items2);
+    schedule(oz.items1, oz.cta1);
+    schedule(oz.items2, oz.cta2);
     oz.mma_ops = 0;
     int64_t kmax = 0;
     for (const std::vector<OzItem> *v : {&oz.items1, &oz.items2})
@@ -448,6 +445,38 @@ struct Builder {
       throw std::runtime_error("inner dimension too large for int32 accumulation");
   }
 
+  // Longest-processing-time-first: items by decreasing estimated time, each
+  // to the least loaded CTA; then each CTA's items are made contiguous.
+  // Estimated time of an item: bytes it streams through shared memory
+  // (row groups of A and B per k-block) plus a fixed epilogue share.
+  void schedule(std::vector<OzItem> &v, std::vector<int32_t> &cta) {
+    const int n = (int)v.size();
+    if (n == 0) {
+      cta.assign(1, 0);
+      return;
+    }
+    const int nb = std::min(oz.nsm, n);
+    auto est = [](const OzItem &it) {
+      return (int64_t)it.nkb * ((it.mrows + 7) / 8 + (it.ncols + 7) / 8) + 24;
+    };
+    std::stable_sort(v.begin(), v.end(), [&](const OzItem &a, const OzItem &b) { return est(a) > est(b); });
+    std::vector<int64_t> load(nb, 0);
+    std::vector<std::vector<int>> bins(nb);
+    for (int i = 0; i < n; ++i) {
+      int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      load[b] += est(v[i]);
+      bins[b].push_back(i);
+    }
+    std::vector<OzItem> out;
+    out.reserve(n);
+    cta.assign(nb + 1, 0);
+    for (int b = 0; b < nb; ++b) {
+      for (int i : bins[b]) out.push_back(v[i]);
+      cta[b + 1] = (int32_t)out.size();
+    }
+    v.swap(out);
+  }
+
   void build() {
     const int64_t npsi = (int64_t)hp.cells2.size();
     if (hp.cell2_row_state.size() != hp.cells2.size() || hp.cell1_row_state.size() != hp.cells1.size())
@@ -465,10 +494,11 @@ struct Builder {
 
 }  // namespace
 
-void build_ozaki_plan(const HpsiPlan &hp, int s, OzPlan &oz) {
+void build_ozaki_plan(const HpsiPlan &hp, int s, int nsm, OzPlan &oz) {
   if (s < 3 || s > OZ_MAX_S) throw std::runtime_error("slices must be in 3..8");
   oz = OzPlan();
   oz.s = s;
+  oz.nsm = std::max(1, nsm);
   oz.bn = oz_bn(s);
   Builder b(hp, oz, s);
   b.build();
@@ -495,7 +525,7 @@ extern "C" int tj_ozaki_plan_export(const tj_lattice *lat, const tj_model *sys, 
   if (rc) return tjb_set_err(rc, "H*psi plan: " + msg);
   tjb::OzPlan oz;
   try {
-    tjb::build_ozaki_plan(P, slices, oz);
+    tjb::build_ozaki_plan(P, slices, 148, oz);
   } catch (const std::exception &e) {
     return tjb_set_err(TJ_ERR_ARG, std::string("split-precision plan: ") + e.what());
   }
@@ -521,5 +551,7 @@ extern "C" int tj_ozaki_plan_export(const tj_lattice *lat, const tj_model *sys, 
   put(out->cells, oz.cells, out->n_cells);
   put(out->items1, oz.items1, out->n_items1);
   put(out->items2, oz.items2, out->n_items2);
+  put(out->cta1, oz.cta1, out->n_cta1);
+  put(out->cta2, oz.cta2, out->n_cta2);
   return TJ_OK;
 }

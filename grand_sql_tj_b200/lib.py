@@ -114,7 +114,9 @@ class OzExport(C.Structure):
                 [(n, C.c_int64) for n in ("sta_pack", "dyn_pack", "n_scales", "rho0", "tau0", "pi0")] +
                 [("int8_ops", C.c_double)] +
                 [("n_" + n, C.c_int64) for n, _ in _OZ_ARRAYS] +
-                [(n, C.POINTER(t)) for n, t in _OZ_ARRAYS])
+                [(n, C.POINTER(t)) for n, t in _OZ_ARRAYS] +
+                [("n_cta1", C.c_int64), ("n_cta2", C.c_int64), ("cta1", C.POINTER(C.c_int32)),
+                 ("cta2", C.POINTER(C.c_int32))])
 
 
 _lib = None
@@ -351,6 +353,8 @@ def ozaki_plan_export(sb, slices: int = 5, invec: Optional[Wave] = None) -> dict
     ex = OzExport()
     _chk(call(C.byref(ex)))
     arrs = {n: (t * max(getattr(ex, "n_" + n), 1))() for n, t in _OZ_ARRAYS}
+    arrs["cta1"] = (C.c_int32 * max(ex.n_cta1, 1))()
+    arrs["cta2"] = (C.c_int32 * max(ex.n_cta2, 1))()
     for k, a in arrs.items():
         setattr(ex, k, C.cast(a, type(getattr(ex, k))))
     _chk(call(C.byref(ex)))

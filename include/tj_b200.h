@@ -323,7 +323,9 @@ int tj_cor_plan_export(int kind, const tj_block *a, const tj_block *b, const tj_
  * scales[rs_idx + row] * scales[cs_idx + col]; an item is one output tile
  * (kind 0: of cell `cell`, families [fam_begin, fam_end); kind 1: phase-1
  * products stacked in [fam_begin, fam_end) of the stack list against the
- * operator split of segment `seg`).  Two-call pattern as above. */
+ * operator split of segment `seg`).  The plan schedules the items of each
+ * launch statically over 148 CTAs (the export's device-independent choice).
+ * Two-call pattern as above. */
 typedef struct tj_oz_job {
   int64_t src_off, dst, scale_idx;
   double coef;
@@ -354,6 +356,8 @@ typedef struct tj_ozaki_export {
   tj_oz_stack *stacks;
   tj_oz_cell *cells;
   tj_oz_item *items1, *items2;
+  int64_t n_cta1, n_cta2;     /* CTA b of launch k runs items [cta_k[b], cta_k[b+1]) */
+  int32_t *cta1, *cta2;
 } tj_ozaki_export;
 int tj_ozaki_plan_export(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
                          const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave, int slices,

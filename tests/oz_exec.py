@@ -71,8 +71,8 @@ class _Machine:
                 t = t - a
                 dig[q] = a.astype(np.int64)
             assert np.all(np.abs(dig) <= 127)
-            # [kb][g][p][c][r8][16]
-            blk = dig.reshape(S, j.gtot, 8, nkb, 2, 16).transpose(3, 1, 0, 4, 2, 5)
+            # [kb][p][g][c][r8][16]
+            blk = dig.reshape(S, j.gtot, 8, nkb, 2, 16).transpose(3, 0, 1, 4, 2, 5)
             start = j.dst + j.kb0 * j.gtot * S * 256
             size = nkb * j.gtot * S * 256
             assert 0 <= start and start + size <= len(self.pack)
@@ -83,10 +83,11 @@ class _Machine:
         S = self.S
         out = np.zeros((S, ng * 8, nkb * 32), dtype=np.int64)
         for kb in range(nkb):
-            o = base + ((kb0 + kb) * gtot + g0) * S * 256
-            assert 0 <= o and o + ng * S * 256 <= len(self.pack)
-            b = self.pack[o:o + ng * S * 256].astype(np.int64).reshape(ng, S, 2, 8, 16)
-            out[:, :, kb * 32:(kb + 1) * 32] = b.transpose(1, 0, 3, 2, 4).reshape(S, ng * 8, 32)
+            for q in range(S):
+                o = base + (((kb0 + kb) * S + q) * gtot + g0) * 256
+                assert 0 <= o and o + ng * 256 <= len(self.pack)
+                b = self.pack[o:o + ng * 256].astype(np.int64).reshape(ng, 2, 8, 16)
+                out[q, :, kb * 32:(kb + 1) * 32] = b.transpose(0, 2, 1, 3).reshape(ng * 8, 32)
         return out
 
     def accum(self, A, B):
@@ -179,6 +180,9 @@ def execute_ozaki(plan, oz, psi):
     m.scales[oe.rho0:] = 0.0
     m.run_max(oz["psi_jobs"], oe.n_psi_jobs)
     m.run_split(oz["psi_jobs"], oe.n_psi_jobs)
+    for n_items, cta, n_cta in ((oe.n_items1, oz["cta1"], oe.n_cta1), (oe.n_items2, oz["cta2"], oe.n_cta2)):
+        b = [cta[i] for i in range(n_cta)]
+        assert b[0] == 0 and b[-1] == n_items and all(x <= y for x, y in zip(b, b[1:])) and len(b) <= 149
     cov1 = set()
     m.run_items(oz["items1"], oe.n_items1, cov1)
     m.run_split(oz["prod_jobs"], oe.n_prod_jobs)
