@@ -43,90 +43,122 @@ __device__ __forceinline__ const double *oz_space(int8_t sp, const double *ops, 
   return sp == SP_OPS ? ops : (sp == SP_PSI ? psi : scr);
 }
 
-// ------------------------------------------------------------ row maxima
-// One CTA (256 threads) per job.  rs == 1: 32 consecutive rows x 8 k lanes;
-// otherwise 32 consecutive k x 8 rows (the unit-stride index runs across lanes).
-__global__ void __launch_bounds__(256) oz_max_kernel(const OzJob *jobs, const double *ops, const double *psi,
-                                                     const double *scr, double *scales) {
-  const OzJob J = jobs[blockIdx.x];
-  if (!J.want_max) return;
-  const double *base = oz_space(J.space, ops, psi, scr) + J.src_off;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  __shared__ double red[8][33];
-  if (J.rs == 1) {
-    for (int r0 = 0; r0 < J.nrows; r0 += 32) {
-      const int r = r0 + tx;
-      double m = 0.0;
-      if (r < J.nrows)
-        for (int k = ty; k < J.K; k += 8) m = fmax(m, fabs(J.coef * base[(int64_t)r + (int64_t)k * J.ks]));
-      red[ty][tx] = m;
-      __syncthreads();
-      if (ty == 0 && r < J.nrows) {
-        for (int y = 1; y < 8; ++y) m = fmax(m, red[y][tx]);
-        if (m > 0.0)
-          atomicMax((unsigned long long *)&scales[J.scale_idx + r], (unsigned long long)__double_as_longlong(m));
+// ------------------------------------------------------------ split jobs
+// The units of a job list (one unit = one row x 16 consecutive k of a job,
+// rows padded to whole groups) are laid end to end and cut into CTAs of
+// OZ_SPLIT_THREADS threads, one unit per thread.  Within a job the unit order
+// puts the unit-stride source index across consecutive threads.
+struct OzUnit {
+  int job, r, c16;
+};
+
+__device__ __forceinline__ bool oz_unit(const OzJob *jobs, int njobs, const OzSpan *spans, OzUnit &u, OzJob &J) {
+  const OzSpan sp = spans[blockIdx.x];
+  int j = sp.job;
+  int64_t k = (int64_t)sp.u0 + threadIdx.x;
+  for (; j < njobs; ++j) {
+    J = jobs[j];
+    const int rows = J.gtot * 8, nk16 = (J.K + 31) / 32 * 2;
+    const int64_t units = (int64_t)rows * nk16;
+    if (k < units) {
+      u.job = j;
+      if (J.rs == 1) {
+        u.r = (int)(k % rows);
+        u.c16 = (int)(k / rows);
+      } else {
+        u.r = (int)(k / nk16);
+        u.c16 = (int)(k % nk16);
       }
-      __syncthreads();
+      return true;
     }
-  } else {
-    for (int r = ty; r < J.nrows; r += 8) {
-      double m = 0.0;
-      for (int k = tx; k < J.K; k += 32) m = fmax(m, fabs(J.coef * base[(int64_t)r * J.rs + k]));
-      for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-      if (tx == 0 && m > 0.0)
-        atomicMax((unsigned long long *)&scales[J.scale_idx + r], (unsigned long long)__double_as_longlong(m));
-    }
+    k -= units;
   }
+  return false;
 }
 
-// ------------------------------------------------------------ digits
-// One unit = (row r, 16 consecutive k): s 16-byte digit rows.
-template <int S>
-__global__ void __launch_bounds__(256) oz_split_kernel(const OzJob *jobs, const double *ops, const double *psi,
-                                                       const double *scr, const double *scales, uint8_t *pack) {
-  const OzJob J = jobs[blockIdx.x];
-  const double *base = oz_space(J.space, ops, psi, scr) + J.src_off;
-  const int rows = J.gtot * 8;
-  const int nk16 = (J.K + 31) / 32 * 2;
-  const int64_t units = (int64_t)rows * nk16;
-  for (int64_t u = threadIdx.x; u < units; u += blockDim.x) {
-    int r, c16;
-    if (J.rs == 1) {   // consecutive threads: consecutive rows
-      r = (int)(u % rows);
-      c16 = (int)(u / rows);
-    } else {           // consecutive threads: consecutive k chunks
-      r = (int)(u / nk16);
-      c16 = (int)(u % nk16);
+// Row maxima of |coef * M| over the jobs with want_max: one unit = one row x
+// OZ_MAX_CHUNK k, one atomic max per unit.
+__global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_max_kernel(const OzJob *jobs, int njobs, const OzSpan *spans,
+                                                                  const double *ops, const double *psi,
+                                                                  const double *scr, double *scales) {
+  const OzSpan sp = spans[blockIdx.x];
+  int64_t k = (int64_t)sp.u0 + threadIdx.x;
+  OzJob J;
+  int r = -1, c = 0;
+  for (int j = sp.job; j < njobs; ++j) {
+    J = jobs[j];
+    if (!J.want_max) continue;
+    const int nc = (J.K + OZ_MAX_CHUNK - 1) / OZ_MAX_CHUNK;
+    const int64_t units = (int64_t)J.nrows * nc;
+    if (k < units) {
+      if (J.rs == 1) {   // consecutive threads: consecutive rows
+        r = (int)(k % J.nrows);
+        c = (int)(k / J.nrows);
+      } else {
+        r = (int)(k / nc);
+        c = (int)(k % nc);
+      }
+      break;
     }
-    uint32_t dig[S][4];
+    k -= units;
+  }
+  if (r < 0) return;
+  const double *row = oz_space(J.space, ops, psi, scr) + J.src_off + (int64_t)r * J.rs;
+  const int k0 = c * OZ_MAX_CHUNK, k1 = min(J.K, k0 + OZ_MAX_CHUNK);
+  double m = 0.0;
+  for (int kk = k0; kk < k1; ++kk) m = fmax(m, fabs(J.coef * row[(int64_t)kk * J.ks]));
+  if (m > 0.0)
+    atomicMax((unsigned long long *)&scales[J.scale_idx + r], (unsigned long long)__double_as_longlong(m));
+}
+
+// Scaled, truncated radix-128 digits: s 16-byte digit rows per unit.
+template <int S>
+__global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_split_kernel(const OzJob *jobs, int njobs, const OzSpan *spans,
+                                                                    const double *ops, const double *psi,
+                                                                    const double *scr, const double *scales,
+                                                                    uint8_t *pack) {
+  OzUnit u;
+  OzJob J;
+  if (!oz_unit(jobs, njobs, spans, u, J)) return;
+  const int r = u.r, c16 = u.c16;
+  uint32_t dig[S][4];
 #pragma unroll
-    for (int q = 0; q < S; ++q) dig[q][0] = dig[q][1] = dig[q][2] = dig[q][3] = 0u;
-    if (r < J.nrows) {
-      const double sc = oz_pow2_of(scales[J.scale_idx + r]);
-      if (sc > 0.0) {
-        const double inv = 1.0 / sc;   // exact: sc is a power of two
-        const double *row = base + (int64_t)r * J.rs;
+  for (int q = 0; q < S; ++q) dig[q][0] = dig[q][1] = dig[q][2] = dig[q][3] = 0u;
+  if (r < J.nrows) {
+    const double sc = oz_pow2_of(scales[J.scale_idx + r]);
+    if (sc > 0.0) {
+      const double inv = 1.0 / sc;   // exact: sc is a power of two
+      const double *row = oz_space(J.space, ops, psi, scr) + J.src_off + (int64_t)r * J.rs;
+      double x[16];
 #pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-          const int k = c16 * 16 + kk;
-          double t = k < J.K ? (J.coef * row[(int64_t)k * J.ks]) * inv : 0.0;
+      for (int kk = 0; kk < 16; ++kk) {
+        const int k = c16 * 16 + kk;
+        x[kk] = k < J.K ? row[(int64_t)k * J.ks] : 0.0;
+      }
 #pragma unroll
-          for (int q = 0; q < S; ++q) {
-            t *= 128.0;
-            const double a = trunc(t);
-            t -= a;
-            dig[q][kk >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)a) << (8 * (kk & 3));
-          }
+      for (int kk = 0; kk < 16; ++kk) {
+        double t = (J.coef * x[kk]) * inv;
+#pragma unroll
+        for (int q = 0; q < S; ++q) {
+          t *= 128.0;
+          const double a = trunc(t);
+          t -= a;
+          dig[q][kk >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)a) << (8 * (kk & 3));
         }
       }
     }
-    const int kb = c16 >> 1, c = c16 & 1, g = r >> 3, r8 = r & 7;
-    uint8_t *dst = pack + J.dst + ((int64_t)(J.kb0 + kb) * S * J.gtot + g) * 256 + c * 128 + r8 * 16;
-    const int64_t plane = (int64_t)J.gtot * 256;   // bytes of one slice of one k-block
-#pragma unroll
-    for (int q = 0; q < S; ++q)
-      *reinterpret_cast<uint4 *>(dst + q * plane) = make_uint4(dig[q][0], dig[q][1], dig[q][2], dig[q][3]);
   }
+  // split row -> tile, group within the tile
+  const int sr = J.row0 + r;
+  const int t = sr / J.R, rl = sr - t * J.R;
+  const int gt = t < J.ntiles - 1 ? J.R / 8 : J.gt_last;
+  const int kb = c16 >> 1, c = c16 & 1, g = rl >> 3, r8 = rl & 7;
+  const int64_t plane = (int64_t)gt * 256;   // bytes of one slice of one k-block of the tile
+  uint8_t *dst = pack + J.dst + (int64_t)t * J.nkb * S * (J.R / 8) * 256 + ((int64_t)(J.kb0 + kb) * S * gt + g) * 256 +
+                 c * 128 + r8 * 16;
+#pragma unroll
+  for (int q = 0; q < S; ++q)
+    *reinterpret_cast<uint4 *>(dst + q * plane) = make_uint4(dig[q][0], dig[q][1], dig[q][2], dig[q][3]);
 }
 
 // ------------------------------------------------------------ tcgen05 GEMM
@@ -246,7 +278,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
   __shared__ volatile int tfull_ok_sh;
   __shared__ double cscale_sh[BN];           // epilogue: column scales of the current family
   __shared__ int32_t stk_start[17];          // epilogue: first tile row of each stacked run
-  __shared__ int64_t stk_dst[16], stk_rs[16], stk_pi[16];
+  __shared__ int64_t stk_dst[16], stk_rs[16];
   __shared__ int32_t stk_ld[16], stk_nc[16];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
@@ -301,89 +333,56 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
     };
     for (int ii = p.cta[blockIdx.x], ie = p.cta[blockIdx.x + 1]; ii < ie && ok; ++ii) {
       const OzItem it = p.items[ii];
-      const uint32_t gb = (uint32_t)((it.ncols + 7) >> 3), b_g0 = (uint32_t)(it.col0 >> 3);
+      // tiles of this item: A row tile ta (ga groups), B column tile tb (gb groups)
+      const uint32_t ga = (uint32_t)((it.mrows + 7) >> 3), gb = (uint32_t)(it.N >> 3);
+      const int64_t ta = it.row0 / 128, tb = it.col0 / BN;
+      const uint32_t bytes = (ga + gb) * GB;
+      int fb0, fe0;
       if (it.kind == 1) {
-        const OzSeg sg = p.segs[it.seg];
-        const int np = it.fam_end - it.fam_begin;   // <= 16 stacked runs, one per lane
-        int64_t abase = 0;
-        int32_t agtot = 0, ag0 = 0, ang = 0;
-        if (lane < np) {
-          const OzStack sk = p.stacks[it.fam_begin + lane];
-          abase = sk.a_base;
-          agtot = sk.a_gtot;
-          ag0 = sk.a_g0;
-          ang = sk.a_ng;
-        }
-        int32_t off = ang;   // exclusive prefix of the runs' groups
-        for (int o = 1; o < 32; o <<= 1) {
-          const int32_t v = __shfl_up_sync(0xffffffffu, off, o);
-          if (lane >= o) off += v;
-        }
-        const int32_t tot = __shfl_sync(0xffffffffu, off, 31);
-        off -= ang;
-        const uint32_t bslice = (uint32_t)(it.N >> 3) * 256u;   // smem bytes of one B slice
-        for (int kb = 0; kb < sg.nkb; ++kb) {
-          if (!acquire(((uint32_t)tot + gb) * GB)) {
-            ok = false;
-            break;
-          }
-          const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE), sbb = sa + C::A_BYTES;
-          const uint32_t fb = oz_smem(&full_bar[stage]);
-          // A: lane i (< np) copies its run, slice by slice, to the run's group offset in each slice
-          if (lane < np)
-            for (int q = 0; q < S; ++q)
-              oz_bulk_g2s(sa + (uint32_t)q * 4096u + (uint32_t)off * 256u,
-                          p.pack + abase + (((int64_t)kb * S + q) * agtot + ag0) * 256, (uint32_t)ang * 256u, fb);
-          // B: lanes 16.. copy one slice each
-          if (lane >= 16 && lane < 16 + S) {
-            const int q = lane - 16;
-            oz_bulk_g2s(sbb + (uint32_t)q * bslice,
-                        p.pack + sg.b_base + (((int64_t)(sg.b_kb0 + kb) * S + q) * sg.b_gtot + b_g0) * 256,
-                        gb * 256u, fb);
-          }
-          if (++stage == ST) stage = 0, ph ^= 1u;
-        }
+        fb0 = fe0 = -1;
       } else {
-        const uint32_t ga = (uint32_t)((it.mrows + 7) >> 3), a_g0 = (uint32_t)(it.row0 >> 3);
-        const uint32_t bslice = (uint32_t)(it.N >> 3) * 256u;
-        for (int f = it.fam_begin; f < it.fam_end && ok; ++f) {
+        fb0 = it.fam_begin;
+        fe0 = it.fam_end;
+      }
+      for (int f = fb0; (it.kind == 1 ? f == -1 : f < fe0) && ok; ++f) {
+        int sb, se;
+        if (it.kind == 1) {
+          sb = it.seg;
+          se = it.seg + 1;
+        } else {
           const OzFam fm = p.fams[f];
-          for (int s0 = fm.seg_begin; s0 < fm.seg_end && ok; s0 += 32) {
-            // the next <= 32 segments, one per lane
-            OzSeg mine;
-            if (s0 + lane < fm.seg_end) mine = p.segs[s0 + lane];
-            const int cnt = min(32, fm.seg_end - s0);
-            for (int j = 0; j < cnt && ok; ++j) {
-              const int64_t a_base = __shfl_sync(0xffffffffu, mine.a_base, j);
-              const int64_t b_base = __shfl_sync(0xffffffffu, mine.b_base, j);
-              const int32_t a_gtot = __shfl_sync(0xffffffffu, mine.a_gtot, j);
-              const int32_t b_gtot = __shfl_sync(0xffffffffu, mine.b_gtot, j);
-              const int32_t a_kb0 = __shfl_sync(0xffffffffu, mine.a_kb0, j);
-              const int32_t b_kb0 = __shfl_sync(0xffffffffu, mine.b_kb0, j);
-              const int32_t nkb = __shfl_sync(0xffffffffu, mine.nkb, j);
-              for (int kb = 0; kb < nkb; ++kb) {
-                if (!acquire((ga + gb) * GB)) {
-                  ok = false;
-                  break;
-                }
-                const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE), sbb = sa + C::A_BYTES;
-                const uint32_t fb = oz_smem(&full_bar[stage]);
-                // lanes 0..S-1: A slices; lanes 16..16+S-1: B slices
-                if (lane < S)
-                  oz_bulk_g2s(sa + (uint32_t)lane * 4096u,
-                              p.pack + a_base + (((int64_t)(a_kb0 + kb) * S + lane) * a_gtot + a_g0) * 256,
-                              ga * 256u, fb);
-                if (lane >= 16 && lane < 16 + S) {
-                  const int q = lane - 16;
-                  oz_bulk_g2s(sbb + (uint32_t)q * bslice,
-                              p.pack + b_base + (((int64_t)(b_kb0 + kb) * S + q) * b_gtot + b_g0) * 256, gb * 256u,
-                              fb);
-                }
-                if (++stage == ST) stage = 0, ph ^= 1u;
+          sb = fm.seg_begin;
+          se = fm.seg_end;
+        }
+        for (int s0 = sb; s0 < se && ok; s0 += 32) {
+          // the next <= 32 segments, one per lane
+          OzSeg mine;
+          if (s0 + lane < se) mine = p.segs[s0 + lane];
+          const int cnt = min(32, se - s0);
+          for (int j = 0; j < cnt && ok; ++j) {
+            const int64_t a_base = __shfl_sync(0xffffffffu, mine.a_base, j);
+            const int64_t b_base = __shfl_sync(0xffffffffu, mine.b_base, j);
+            const int32_t a_nkb = __shfl_sync(0xffffffffu, mine.a_nkb, j);
+            const int32_t b_nkb = __shfl_sync(0xffffffffu, mine.b_nkb, j);
+            const int32_t a_kb0 = __shfl_sync(0xffffffffu, mine.a_kb0, j);
+            const int32_t b_kb0 = __shfl_sync(0xffffffffu, mine.b_kb0, j);
+            const int32_t nkb = __shfl_sync(0xffffffffu, mine.nkb, j);
+            const uint8_t *asrc = p.pack + a_base + ta * a_nkb * (int64_t)(16 * GB) + (int64_t)a_kb0 * ga * GB;
+            const uint8_t *bsrc = p.pack + b_base + tb * b_nkb * (int64_t)((BN / 8) * GB) + (int64_t)b_kb0 * gb * GB;
+            for (int kb = 0; kb < nkb; ++kb) {
+              if (!acquire(bytes)) {
+                ok = false;
+                break;
               }
+              const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE), sbb = sa + C::A_BYTES;
+              const uint32_t fbar = oz_smem(&full_bar[stage]);
+              if (lane == 0) oz_bulk_g2s(sa, asrc + (int64_t)kb * ga * GB, ga * GB, fbar);
+              if (lane == 1) oz_bulk_g2s(sbb, bsrc + (int64_t)kb * gb * GB, gb * GB, fbar);
+              if (++stage == ST) stage = 0, ph ^= 1u;
             }
           }
         }
+        if (it.kind == 1) break;
       }
     }
     // copies still in flight land before the CTA exits
@@ -406,6 +405,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
         uint32_t idesc[S];
 #pragma unroll
         for (int pa = 1; pa <= S; ++pa) idesc[pa - 1] = oz_idesc(it.M, (S + 1 - pa) * it.N);
+        const uint32_t aslice16 = (uint32_t)((it.mrows + 7) >> 3) * 16u;   // A slice stride in 16-byte units
         const int nf = it.kind == 1 ? 1 : it.fam_end - it.fam_begin;
         for (int f = 0; f < nf && ok; ++f) {
           const int nkb = it.kind == 1 ? it.nkb : p.fams[it.fam_begin + f].nkb;
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
             const uint64_t db = dbase + (uint64_t)((sa + C::A_BYTES) >> 4);
 #pragma unroll
             for (int pa = 1; pa <= S; ++pa) {
-              const uint64_t da = da0 + (uint64_t)((pa - 1) * 256);   // +4096 bytes per A slice
+              const uint64_t da = da0 + (uint64_t)((pa - 1) * aslice16);   // A slices ga groups apart
               const uint32_t d = dt + (uint32_t)((pa - 1) * it.N);
               const uint32_t acc = (kb == 0 && pa == 1) ? 0u : 1u;
               asm volatile(
@@ -485,7 +485,6 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
       double *dst = nullptr;
       int64_t cstride = 0;
       double rscale_stack = 0.0;
-      int64_t pib = -1;   // kind 1: pi index of this row's product, row col0
       OzCell c{};
       if (it.kind == 0) {
         c = p.cells[it.cell];
@@ -498,7 +497,6 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
           const OzStack sk = p.stacks[it.fam_begin + tid];
           stk_dst[tid] = sk.dst_off;
           stk_rs[tid] = sk.rs_idx;
-          stk_pi[tid] = sk.pi_idx;
           stk_ld[tid] = sk.dst_ld;
           stk_nc[tid] = sk.ncols;
           stk_start[tid + 1] = sk.a_ng * 8;
@@ -514,7 +512,6 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
         rv = rv && piece >= 0;
         if (piece >= 0) {
           const int jl = r - stk_start[piece];
-          pib = stk_pi[piece] + it.col0;
           if (jl < stk_nc[piece]) {
             dst = p.scr + stk_dst[piece] + (int64_t)jl * stk_ld[piece] + it.col0;
             rscale_stack = oz_pow2_of(p.scales[stk_rs[piece] + jl]);
@@ -620,13 +617,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
 #pragma unroll
             for (int jj = 0; jj < 16; ++jj) {
               const int n = ch * 16 + jj;
-              const double val = (rv && n < it.ncols) ? accv[n] : 0.0;
-              if (rv && n < it.ncols) dst[n] = val;
-              // pi: max |P(i, .)| over each 8-row group (one product), one atomic per group and column
-              double m = fabs(val);
-              for (int o = 1; o < 8; o <<= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-              if ((lane & 7) == 0 && pib >= 0 && n < it.ncols && m > 0.0)
-                atomicMax((unsigned long long *)&p.scales[pib + n], (unsigned long long)__double_as_longlong(m));
+              if (rv && n < it.ncols) dst[n] = accv[n];
             }
           }
         }
@@ -639,24 +630,26 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
 }
 
 // ------------------------------------------------------------ host launches
-void launch_oz_max(const OzJob *jobs, int njobs, const double *ops, const double *psi, const double *scr,
-                   double *scales, cudaStream_t st) {
-  if (njobs <= 0) return;
-  oz_max_kernel<<<njobs, 256, 0, st>>>(jobs, ops, psi, scr, scales);
+void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
+                   const double *psi, const double *scr, double *scales, cudaStream_t st) {
+  if (njobs <= 0 || nspans <= 0) return;
+  oz_max_kernel<<<nspans, OZ_SPLIT_THREADS, 0, st>>>(jobs, njobs, spans, ops, psi, scr, scales);
 }
 
-void launch_oz_split(const OzJob *jobs, int njobs, const double *ops, const double *psi, const double *scr,
-                     const double *scales, uint8_t *pack, int s, cudaStream_t st) {
-  if (njobs <= 0) return;
+void launch_oz_split(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
+                     const double *psi, const double *scr, const double *scales, uint8_t *pack, int s, cudaStream_t st) {
+  if (njobs <= 0 || nspans <= 0) return;
+#define OZ_SPLIT(SS) oz_split_kernel<SS><<<nspans, OZ_SPLIT_THREADS, 0, st>>>(jobs, njobs, spans, ops, psi, scr, scales, pack)
   switch (s) {
-    case 3: oz_split_kernel<3><<<njobs, 256, 0, st>>>(jobs, ops, psi, scr, scales, pack); break;
-    case 4: oz_split_kernel<4><<<njobs, 256, 0, st>>>(jobs, ops, psi, scr, scales, pack); break;
-    case 5: oz_split_kernel<5><<<njobs, 256, 0, st>>>(jobs, ops, psi, scr, scales, pack); break;
-    case 6: oz_split_kernel<6><<<njobs, 256, 0, st>>>(jobs, ops, psi, scr, scales, pack); break;
-    case 7: oz_split_kernel<7><<<njobs, 256, 0, st>>>(jobs, ops, psi, scr, scales, pack); break;
-    case 8: oz_split_kernel<8><<<njobs, 256, 0, st>>>(jobs, ops, psi, scr, scales, pack); break;
+    case 3: OZ_SPLIT(3); break;
+    case 4: OZ_SPLIT(4); break;
+    case 5: OZ_SPLIT(5); break;
+    case 6: OZ_SPLIT(6); break;
+    case 7: OZ_SPLIT(7); break;
+    case 8: OZ_SPLIT(8); break;
     default: break;
   }
+#undef OZ_SPLIT
 }
 
 template <int S, int BN>

@@ -27,14 +27,17 @@
 // P_t^T (columns of X_t, scale tau) stacked across products that share
 // op(A_t); their epilogue stores P in FP64 and raises pi.
 //
-// Split storage ("pack" pools, bytes): a split of R rows x K has
-// G = ceil(R / 8) row groups and nkb = ceil(K / 32) k-blocks, laid out
-//   [kb][g][slice p][c (2)][row r8 (8)][16 bytes]
-// so that any run of row groups of one k-block is one contiguous block of
-// (groups * s * 256) bytes, which lands in shared memory as the canonical
-// UMMA K-major, no-swizzle layout (core matrices of 8 rows x 16 bytes,
-// leading-byte offset 128 between the two K halves, stride-byte offset
-// s * 256 between row groups, slice p at +p * 256).
+// Split storage ("pack" pools, bytes): a split of `rows` x K is cut into
+// tiles of R rows (R = 128 for an A operand, R = BN for a B operand) and
+// ceil(K / 32) k-blocks.  Tile t holds G_t row groups of 8 rows (R/8 for all
+// but the last; the last holds ceil(rem/8) for A, round16(rem)/8 for B, so a
+// B tile is a whole number of 16-row MMA columns), laid out
+//   [tile][kb][slice p][group g < G_t][c (2)][row r8 (8)][16 bytes]
+// so that one k-block of one tile, all slices, is ONE contiguous block of
+// s * G_t * 256 bytes: it lands in shared memory as s consecutive slices in
+// the canonical UMMA K-major, no-swizzle layout (core matrices of 8 rows x
+// 16 bytes, leading-byte offset 128 between the two K halves, stride-byte
+// offset 256 between row groups).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -51,11 +54,13 @@ constexpr int OZ_MAX_S = 8;
 inline int oz_bn(int s) { return s <= 5 ? 48 : 32; }
 
 // One split job: rows [0, nrows) x k [0, K) of coef * M, M(r, k) =
-// base[src_off + r*rs + k*ks], written to k-blocks [kb0, kb0 + ceil(K/32))
-// of the split at pack offset `dst` (gtot row groups); rows up to gtot*8 and
-// k up to the k-block boundary are written as zero digits.  The row scale is
-// scales[scale_idx + r] (max |value| of the row, made a power of two by the
-// kernels); want_max: this job contributes to that maximum.
+// base[src_off + r*rs + k*ks], written as split rows row0 + r, k-blocks
+// [kb0, kb0 + ceil(K/32)) of the split at pack offset `dst` (tiles of R
+// rows, nkb k-blocks in all, ntiles tiles, the last of gt_last groups).  The
+// job writes gtot groups (rows up to row0 + 8*gtot; rows past nrows and k
+// past K as zero digits).  The row scale is scales[scale_idx + r] (max
+// |value| of the row, made a power of two by the kernels); want_max: the job
+// contributes to that maximum.
 struct OzJob {
   int64_t src_off;
   int64_t dst;
@@ -63,15 +68,16 @@ struct OzJob {
   double coef;
   int32_t rs, ks, nrows, K;
   int32_t gtot, kb0;
+  int32_t R, nkb, ntiles, gt_last, row0;
   int8_t space, want_max;
-  int8_t pad[6];
+  int8_t pad[2];
 };
 
 // One k-range of an operand pair: k-blocks [a_kb0, a_kb0 + nkb) of the A
 // split and [b_kb0, b_kb0 + nkb) of the B split.
 struct OzSeg {
   int64_t a_base, b_base;   // pack offsets of the splits
-  int32_t a_gtot, b_gtot;   // their row-group counts
+  int32_t a_nkb, b_nkb;     // their k-block counts (tile strides)
   int32_t a_kb0, b_kb0, nkb;
   int32_t pad;
 };
@@ -86,17 +92,14 @@ struct OzFam {
 };
 
 // A run of stacked rows of a product tile: rows of P^T = columns
-// [8*a_g0, 8*a_g0 + ncols) of X_t, i.e. row groups [a_g0, a_g0 + a_ng) of
-// X_t's column split.
+// [8*a_g0, 8*a_g0 + ncols) of X_t, held as a_ng row groups of the tile's
+// stack split (written there by a split job of X_t's columns).
 struct OzStack {
-  int64_t a_base;           // psi column split of X_t
   int64_t dst_off;          // P_t(0, 8*a_g0) in the product space
   int64_t rs_idx;           // tau index of X_t's column 8*a_g0
-  int64_t pi_idx;           // pi index of P_t's row 0
-  int32_t a_gtot, a_g0, a_ng;
+  int32_t a_g0, a_ng;
   int32_t dst_ld;
   int32_t ncols;            // valid rows of this run
-  int32_t pad;
 };
 
 // A work item: the output tile rows [row0, row0 + M) x cols [col0, col0 + N)
@@ -104,7 +107,8 @@ struct OzStack {
 //                   init = 1: the tile is written (axpy terms or zero), then
 //                   every family is added; init = 0: families are added
 //   kind 1 (stack): of the products stacked in [fam_begin, fam_end) of the
-//                   stack list, sharing the operator split `seg` (B side)
+//                   stack list; segment `seg` pairs the tile's stack split
+//                   (A) with the shared operator's split (B)
 struct OzItem {
   int32_t kind, cell;
   int32_t row0, col0;
@@ -127,6 +131,15 @@ struct OzCell {
   int32_t pad;
 };
 
+// Work split of a job list over 128-thread CTAs: CTA b starts at unit u0 of
+// job `job`.  Split units: one row (rows padded to whole groups) x 16 k;
+// maximum units: one row x OZ_MAX_CHUNK k.
+struct OzSpan {
+  int32_t job, u0;
+};
+constexpr int OZ_SPLIT_THREADS = 128;
+constexpr int OZ_MAX_CHUNK = 64;
+
 struct OzPlan {
   int s = 5;
   int bn = 48;
@@ -139,6 +152,8 @@ struct OzPlan {
   std::vector<OzJob> sta_jobs;             // once per step
   std::vector<OzJob> psi_jobs;             // per H*psi, before launch 1
   std::vector<OzJob> prod_jobs;            // per H*psi, between the launches
+  std::vector<OzSpan> sta_spans, psi_spans, prod_spans;            // split units
+  std::vector<OzSpan> sta_mspans, psi_mspans, prod_mspans;         // maximum units
   // GEMM tables
   std::vector<OzSeg> segs;
   std::vector<OzFam> fams;
@@ -158,10 +173,10 @@ struct OzPlan {
 void build_ozaki_plan(const HpsiPlan &hp, int s, int nsm, OzPlan &oz);
 
 // device launches (ozaki.cu)
-void launch_oz_max(const OzJob *jobs, int njobs, const double *ops, const double *psi, const double *scr,
-                   double *scales, cudaStream_t st);
-void launch_oz_split(const OzJob *jobs, int njobs, const double *ops, const double *psi, const double *scr,
-                     const double *scales, uint8_t *pack, int s, cudaStream_t st);
+void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
+                   const double *psi, const double *scr, double *scales, cudaStream_t st);
+void launch_oz_split(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
+                     const double *psi, const double *scr, const double *scales, uint8_t *pack, int s, cudaStream_t st);
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
                            const OzStack *stacks, const OzCell *cells, const Task *tasks, const uint8_t *pack,
                            double *scales, const double *psi, double *scr, double *out, int *err, int s,

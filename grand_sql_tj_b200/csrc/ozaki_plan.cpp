@@ -27,6 +27,11 @@ inline int32_t cdiv(int64_t a, int64_t b) { return (int32_t)((a + b - 1) / b); }
 // Which dynamic scale pool an index is relative to while building.
 enum { REL_NONE = -1, REL_RHO = 0, REL_TAU = 1, REL_PI = 2 };
 
+// Tiling of a split: tiles of R rows; the last one of gt_last groups.
+struct Tiling {
+  int32_t rows, R, nkb, ntiles, gt_last, gsum;
+};
+
 struct Builder {
   const HpsiPlan &hp;
   OzPlan &oz;
@@ -44,16 +49,29 @@ struct Builder {
 
   Builder(const HpsiPlan &h, OzPlan &o, int s) : hp(h), oz(o), S(s) {}
 
-  int64_t split_bytes(int32_t rows, int32_t K) const { return (int64_t)cdiv(K, 32) * cdiv(rows, 8) * S * 256; }
+  // A operands are tiled by 128 rows; B operands by the N tile, each tile a
+  // whole number of 16-row MMA columns.
+  Tiling tiling(int32_t rows, int32_t K, bool b_role) const {
+    Tiling t;
+    t.rows = rows;
+    t.R = b_role ? oz.bn : 128;
+    t.nkb = cdiv(K, 32);
+    t.ntiles = cdiv(rows, t.R);
+    const int32_t rem = rows - (t.ntiles - 1) * t.R;
+    t.gt_last = b_role ? (rem + 15) / 16 * 2 : cdiv(rem, 8);
+    t.gsum = (t.ntiles - 1) * (t.R / 8) + t.gt_last;
+    return t;
+  }
+  int64_t split_bytes(const Tiling &t) const { return (int64_t)t.nkb * S * t.gsum * 256; }
   static int64_t align256(int64_t x) { return (x + 255) / 256 * 256; }
-  int64_t alloc_sta(int32_t rows, int32_t K) {
+  int64_t alloc_sta(const Tiling &t) {
     const int64_t o = sta_bytes;
-    sta_bytes = align256(sta_bytes + split_bytes(rows, K));
+    sta_bytes = align256(sta_bytes + split_bytes(t));
     return o;
   }
-  int64_t alloc_dyn(int32_t rows, int32_t K) {
+  int64_t alloc_dyn(const Tiling &t) {
     const int64_t o = dyn_bytes;
-    dyn_bytes = align256(dyn_bytes + split_bytes(rows, K));
+    dyn_bytes = align256(dyn_bytes + split_bytes(t));
     return o;
   }
   int64_t alloc_scales(int64_t n) {
@@ -62,9 +80,12 @@ struct Builder {
     return o;
   }
 
+  // A job writing rows [row0, row0 + 8*gtot) (gtot groups; the first nrows
+  // from the source) and k-blocks from kb0 of the split at dst.
   static OzJob job(int8_t space, int64_t src_off, int32_t rs, int32_t ks, int32_t nrows, int32_t K, double coef,
-                   int64_t dst, int32_t gtot, int32_t kb0, int64_t scale_idx, bool want_max) {
-    if (nrows < 1 || K < 1) throw std::runtime_error("empty split");
+                   int64_t dst, const Tiling &t, int32_t row0, int32_t gtot, int32_t kb0, int64_t scale_idx,
+                   bool want_max) {
+    if (nrows < 1 || K < 1 || gtot < 1) throw std::runtime_error("empty split");
     OzJob j;
     std::memset(&j, 0, sizeof j);
     j.src_off = src_off;
@@ -77,6 +98,11 @@ struct Builder {
     j.K = K;
     j.gtot = gtot;
     j.kb0 = kb0;
+    j.R = t.R;
+    j.nkb = t.nkb;
+    j.ntiles = t.ntiles;
+    j.gt_last = t.gt_last;
+    j.row0 = row0;
     j.space = space;
     j.want_max = want_max ? 1 : 0;
     return j;
@@ -99,8 +125,9 @@ struct Builder {
   int64_t psi_col(int c) {
     if (colsplit[c] < 0) {
       const Cell &x = hp.cells2[c];
-      colsplit[c] = alloc_dyn(x.N, x.M);
-      dyn_psi.push_back(job(SP_PSI, x.off, x.ld, 1, x.N, x.M, 1.0, colsplit[c], cdiv(x.N, 8), 0,
+      const Tiling t = tiling(x.N, x.M, true);
+      colsplit[c] = alloc_dyn(t);
+      dyn_psi.push_back(job(SP_PSI, x.off, x.ld, 1, x.N, x.M, 1.0, colsplit[c], t, 0, t.gsum, 0,
                             hp.cell2_col_state[c], true));
       dyn_psi_rel.push_back(REL_TAU);
     }
@@ -110,8 +137,9 @@ struct Builder {
   int64_t psi_row(int c) {
     if (rowsplit[c] < 0) {
       const Cell &x = hp.cells2[c];
-      rowsplit[c] = alloc_dyn(x.M, x.N);
-      dyn_psi.push_back(job(SP_PSI, x.off, 1, x.ld, x.M, x.N, 1.0, rowsplit[c], cdiv(x.M, 8), 0,
+      const Tiling t = tiling(x.M, x.N, false);
+      rowsplit[c] = alloc_dyn(t);
+      dyn_psi.push_back(job(SP_PSI, x.off, 1, x.ld, x.M, x.N, 1.0, rowsplit[c], t, 0, t.gsum, 0,
                             hp.cell2_row_state[c], true));
       dyn_psi_rel.push_back(REL_RHO);
     }
@@ -121,9 +149,10 @@ struct Builder {
   int64_t prod_row(int p) {
     if (prodsplit[p] < 0) {
       const Cell &P = hp.cells1[p];
-      prodsplit[p] = alloc_dyn(P.M, P.N);
-      dyn_prod.push_back(job(SP_SCR, P.off, 1, P.ld, P.M, P.N, 1.0, prodsplit[p], cdiv(P.M, 8), 0,
-                             hp.cell1_row_state[p], false));
+      const Tiling t = tiling(P.M, P.N, false);
+      prodsplit[p] = alloc_dyn(t);
+      dyn_prod.push_back(job(SP_SCR, P.off, 1, P.ld, P.M, P.N, 1.0, prodsplit[p], t, 0, t.gsum, 0,
+                             hp.cell1_row_state[p], true));
     }
     return prodsplit[p];
   }
@@ -132,6 +161,9 @@ struct Builder {
     return (int64_t)it.M * it.N * 32 * kbs * (S * (S + 1) / 2);
   }
 
+  // Phase-1 products P_t = op(A_t) X_t, grouped by operator: the columns of
+  // the X_t (rows of P_t^T, scale tau) are stacked into 128-row tiles, each
+  // tile a split of its own written by one job per run.
   void products() {
     const int BN = oz.bn;
     std::map<std::pair<int64_t, int>, std::vector<int>> by_op;
@@ -149,19 +181,16 @@ struct Builder {
       const int32_t Mop = c0.M, K = t0.K;
       int32_t rs, ks;
       strides(t0.L, 0, rs, ks);
-      const int64_t pk = alloc_sta(Mop, K);
+      const Tiling tb = tiling(Mop, K, true);
+      const int64_t pk = alloc_sta(tb);
       const int64_t sc = alloc_scales(Mop);
-      oz.sta_jobs.push_back(job(SP_OPS, t0.L.off, rs, ks, Mop, K, 1.0, pk, cdiv(Mop, 8), 0, sc, true));
-      OzSeg sg;
-      std::memset(&sg, 0, sizeof sg);
-      sg.a_base = -1;   // the stacks carry the A side
-      sg.b_base = pk;
-      sg.b_gtot = cdiv(Mop, 8);
-      sg.nkb = cdiv(K, 32);
-      const int seg = (int)oz.segs.size();
-      oz.segs.push_back(sg);
-      // runs of <= 16 row groups of the operands' column splits
-      std::vector<OzStack> runs;
+      oz.sta_jobs.push_back(job(SP_OPS, t0.L.off, rs, ks, Mop, K, 1.0, pk, tb, 0, tb.gsum, 0, sc, true));
+      // runs of <= 16 row groups: columns of the operands
+      struct Run {
+        OzStack st;
+        int x;   // psi cell
+      };
+      std::vector<Run> runs;
       for (int p : prods) {
         const Cell &c = hp.cells1[p];
         const Task &t = hp.tasks1[c.t_begin];
@@ -169,33 +198,51 @@ struct Builder {
         const int x = psi_index(t.R);
         const Cell &X = hp.cells2[x];
         if (X.M != K || X.N != c.N) throw std::runtime_error("product operand shape");
-        const int64_t cs = psi_col(x);
         const int32_t G = cdiv(X.N, 8);
         for (int32_t g0 = 0; g0 < G; g0 += 16) {
-          OzStack r;
-          std::memset(&r, 0, sizeof r);
-          r.a_base = cs;   // dynamic-relative
-          r.a_gtot = G;
-          r.a_g0 = g0;
-          r.a_ng = std::min(16, G - g0);
-          r.dst_off = c.off + (int64_t)8 * g0 * c.ld;
-          r.dst_ld = c.ld;
-          r.ncols = std::min(8 * r.a_ng, X.N - 8 * g0);
-          r.rs_idx = hp.cell2_col_state[x] + 8 * g0;   // tau-relative
-          r.pi_idx = hp.cell1_row_state[p];             // pi-relative
+          Run r;
+          std::memset(&r.st, 0, sizeof r.st);
+          r.x = x;
+          r.st.a_g0 = g0;
+          r.st.a_ng = std::min(16, G - g0);
+          r.st.dst_off = c.off + (int64_t)8 * g0 * c.ld;
+          r.st.dst_ld = c.ld;
+          r.st.ncols = std::min(8 * r.st.a_ng, X.N - 8 * g0);
+          r.st.rs_idx = hp.cell2_col_state[x] + 8 * g0;   // tau-relative
           runs.push_back(r);
         }
       }
       size_t i = 0;
       while (i < runs.size()) {
         int32_t groups = 0;
+        size_t e = i;
+        while (e < runs.size() && groups + runs[e].st.a_ng <= 16) groups += runs[e++].st.a_ng;
+        // the tile's stack split (one 128-row tile) and the jobs that fill it
+        const Tiling ta = tiling(8 * groups, K, false);
+        const int64_t sk = alloc_dyn(ta);
         const int fb = (int)oz.stacks.size();
-        while (i < runs.size() && groups + runs[i].a_ng <= 16) {
-          groups += runs[i].a_ng;
-          oz.stacks.push_back(runs[i]);
-          ++i;
+        int32_t off = 0;
+        for (size_t q = i; q < e; ++q) {
+          const Run &r = runs[q];
+          const Cell &X = hp.cells2[r.x];
+          oz.stacks.push_back(r.st);
+          dyn_psi.push_back(job(SP_PSI, X.off + (int64_t)8 * r.st.a_g0 * X.ld, X.ld, 1, r.st.ncols, K, 1.0, sk, ta,
+                                8 * off, r.st.a_ng, 0, hp.cell2_col_state[r.x] + 8 * r.st.a_g0, true));
+          dyn_psi_rel.push_back(REL_TAU);
+          off += r.st.a_ng;
         }
         const int fe = (int)oz.stacks.size();
+        i = e;
+        OzSeg sg;
+        std::memset(&sg, 0, sizeof sg);
+        sg.a_base = sk;
+        sg.a_nkb = ta.nkb;
+        sg.b_base = pk;
+        sg.b_nkb = tb.nkb;
+        sg.nkb = tb.nkb;
+        const int seg = (int)oz.segs.size();
+        seg_dyn_a.push_back(seg);
+        oz.segs.push_back(sg);
         for (int32_t n0 = 0; n0 < Mop; n0 += BN) {
           OzItem it;
           std::memset(&it, 0, sizeof it);
@@ -222,10 +269,10 @@ struct Builder {
   // A family of tasks that share the B side's concatenation (right: psi rows,
   // two-sided: product rows).
   int right_family(const Cell &c, int64_t ci, const std::vector<int> &tl, bool prods) {
-    const int32_t GM = cdiv(c.M, 8), GN = cdiv(c.N, 8);
     int32_t kbt = 0;
     for (int ti : tl) kbt += cdiv(hp.tasks2[ti].K, 32);
-    const int64_t pk = alloc_sta(c.N, 32 * kbt);
+    const Tiling tb = tiling(c.N, 32 * kbt, true);
+    const int64_t pk = alloc_sta(tb);
     const int64_t sc = alloc_scales(c.N);
     OzFam f;
     f.seg_begin = (int)oz.segs.size();
@@ -234,7 +281,7 @@ struct Builder {
       const Task &t = hp.tasks2[ti];
       int32_t rs, ks;
       strides(t.R, 1, rs, ks);
-      oz.sta_jobs.push_back(job(SP_OPS, t.R.off, rs, ks, c.N, t.K, t.coef, pk, GN, kb, sc, true));
+      oz.sta_jobs.push_back(job(SP_OPS, t.R.off, rs, ks, c.N, t.K, t.coef, pk, tb, 0, tb.gsum, kb, sc, true));
       OzSeg sg;
       std::memset(&sg, 0, sizeof sg);
       if (!prods) {
@@ -253,10 +300,10 @@ struct Builder {
           throw std::runtime_error("two-sided task operand shape");
         sg.a_base = prod_row(p);
       }
-      sg.a_gtot = GM;
+      sg.a_nkb = cdiv(t.K, 32);
       sg.a_kb0 = 0;
       sg.b_base = pk;
-      sg.b_gtot = GN;
+      sg.b_nkb = tb.nkb;
       sg.b_kb0 = kb;
       sg.nkb = cdiv(t.K, 32);
       seg_dyn_a.push_back((int)oz.segs.size());
@@ -273,10 +320,10 @@ struct Builder {
   }
 
   int left_family(const Cell &c, int64_t ci, const std::vector<int> &tl) {
-    const int32_t GM = cdiv(c.M, 8), GN = cdiv(c.N, 8);
     int32_t kbt = 0;
     for (int ti : tl) kbt += cdiv(hp.tasks2[ti].K, 32);
-    const int64_t pk = alloc_sta(c.M, 32 * kbt);
+    const Tiling ta = tiling(c.M, 32 * kbt, false);
+    const int64_t pk = alloc_sta(ta);
     const int64_t sc = alloc_scales(c.M);
     OzFam f;
     f.seg_begin = (int)oz.segs.size();
@@ -285,7 +332,7 @@ struct Builder {
       const Task &t = hp.tasks2[ti];
       int32_t rs, ks;
       strides(t.L, 0, rs, ks);
-      oz.sta_jobs.push_back(job(SP_OPS, t.L.off, rs, ks, c.M, t.K, t.coef, pk, GM, kb, sc, true));
+      oz.sta_jobs.push_back(job(SP_OPS, t.L.off, rs, ks, c.M, t.K, t.coef, pk, ta, 0, ta.gsum, kb, sc, true));
       const int x = psi_index(t.R);
       const Cell &X = hp.cells2[x];
       if (X.M != t.K || X.N != c.N || hp.cell2_col_state[x] != hp.cell2_col_state[ci])
@@ -293,10 +340,10 @@ struct Builder {
       OzSeg sg;
       std::memset(&sg, 0, sizeof sg);
       sg.a_base = pk;
-      sg.a_gtot = GM;
+      sg.a_nkb = ta.nkb;
       sg.a_kb0 = kb;
       sg.b_base = psi_col(x);
-      sg.b_gtot = GN;
+      sg.b_nkb = cdiv(t.K, 32);
       sg.b_kb0 = 0;
       sg.nkb = cdiv(t.K, 32);
       seg_dyn_b.push_back((int)oz.segs.size());
@@ -386,7 +433,6 @@ struct Builder {
     const int64_t dbase = sta_bytes;
     for (OzJob &j : dyn_psi) j.dst += dbase;
     for (OzJob &j : dyn_prod) j.dst += dbase;
-    for (OzStack &r : oz.stacks) r.a_base += dbase;
     for (int i : seg_dyn_a) oz.segs[i].a_base += dbase;
     for (int i : seg_dyn_b) oz.segs[i].b_base += dbase;
     // scale pool: static scales, then rho, tau, pi
@@ -398,10 +444,7 @@ struct Builder {
     const int64_t base[3] = {oz.rho0, oz.tau0, oz.pi0};
     for (size_t i = 0; i < dyn_psi.size(); ++i) dyn_psi[i].scale_idx += base[dyn_psi_rel[i]];
     for (OzJob &j : dyn_prod) j.scale_idx += oz.pi0;
-    for (OzStack &r : oz.stacks) {
-      r.rs_idx += oz.tau0;
-      r.pi_idx += oz.pi0;
-    }
+    for (OzStack &r : oz.stacks) r.rs_idx += oz.tau0;
     for (const FamRel &fr : famrel) {
       OzFam &f = oz.fams[fr.fam];
       if (fr.rs_rel != REL_NONE) f.rs_idx += base[fr.rs_rel];
@@ -421,6 +464,12 @@ struct Builder {
       }
     oz.psi_jobs = std::move(dyn_psi);
     oz.prod_jobs = std::move(dyn_prod);
+    make_spans(oz.sta_jobs, oz.sta_spans, false);
+    make_spans(oz.psi_jobs, oz.psi_spans, false);
+    make_spans(oz.prod_jobs, oz.prod_spans, false);
+    make_spans(oz.sta_jobs, oz.sta_mspans, true);
+    make_spans(oz.psi_jobs, oz.psi_mspans, true);
+    make_spans(oz.prod_jobs, oz.prod_mspans, true);
     schedule(oz.items1, oz.cta1);
     schedule(oz.items2, oz.cta2);
     oz.mma_ops = 0;
@@ -443,6 +492,24 @@ struct Builder {
     // exact int32 accumulation: a diagonal sums <= s slice products of 127^2 per k
     if ((double)kmax * S * 127.0 * 127.0 >= 2147483647.0)
       throw std::runtime_error("inner dimension too large for int32 accumulation");
+  }
+
+  // CTA start points over the concatenated units of a job list: CTA b takes
+  // global units [b*T, (b+1)*T), starting inside job `job` at unit u0.
+  // Split units cover gtot*8 rows x K/16; maximum units nrows x K/OZ_MAX_CHUNK.
+  static int64_t job_units(const OzJob &j, bool max_units) {
+    if (max_units) return j.want_max ? (int64_t)j.nrows * cdiv(j.K, OZ_MAX_CHUNK) : 0;
+    return (int64_t)j.gtot * 8 * (cdiv(j.K, 32) * 2);
+  }
+  static void make_spans(const std::vector<OzJob> &jobs, std::vector<OzSpan> &spans, bool max_units) {
+    spans.clear();
+    std::vector<int64_t> st(jobs.size() + 1, 0);
+    for (size_t j = 0; j < jobs.size(); ++j) st[j + 1] = st[j] + job_units(jobs[j], max_units);
+    size_t j = 0;
+    for (int64_t g = 0; g < st.back(); g += OZ_SPLIT_THREADS) {
+      while (st[j + 1] <= g) ++j;
+      spans.push_back(OzSpan{(int32_t)j, (int32_t)(g - st[j])});
+    }
   }
 
   // Longest-processing-time-first: items by decreasing estimated time, each

@@ -76,13 +76,14 @@ class PlanExport(C.Structure):
 
 class OzJobC(C.Structure):
     _fields_ = [("src_off", C.c_int64), ("dst", C.c_int64), ("scale_idx", C.c_int64), ("coef", C.c_double)] + \
-               [(n, C.c_int32) for n in ("rs", "ks", "nrows", "K", "gtot", "kb0")] + \
-               [("space", C.c_int8), ("want_max", C.c_int8), ("pad_", C.c_int8 * 6)]
+               [(n, C.c_int32) for n in ("rs", "ks", "nrows", "K", "gtot", "kb0", "R", "nkb", "ntiles", "gt_last",
+                                         "row0")] + \
+               [("space", C.c_int8), ("want_max", C.c_int8), ("pad_", C.c_int8 * 2)]
 
 
 class OzSegC(C.Structure):
     _fields_ = [("a_base", C.c_int64), ("b_base", C.c_int64)] + \
-               [(n, C.c_int32) for n in ("a_gtot", "b_gtot", "a_kb0", "b_kb0", "nkb", "pad_")]
+               [(n, C.c_int32) for n in ("a_nkb", "b_nkb", "a_kb0", "b_kb0", "nkb", "pad_")]
 
 
 class OzFamC(C.Structure):
@@ -91,8 +92,8 @@ class OzFamC(C.Structure):
 
 
 class OzStackC(C.Structure):
-    _fields_ = [("a_base", C.c_int64), ("dst_off", C.c_int64), ("rs_idx", C.c_int64), ("pi_idx", C.c_int64)] + \
-               [(n, C.c_int32) for n in ("a_gtot", "a_g0", "a_ng", "dst_ld", "ncols", "pad_")]
+    _fields_ = [("dst_off", C.c_int64), ("rs_idx", C.c_int64)] + \
+               [(n, C.c_int32) for n in ("a_g0", "a_ng", "dst_ld", "ncols")]
 
 
 class OzItemC(C.Structure):

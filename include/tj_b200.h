@@ -310,33 +310,35 @@ int tj_cor_plan_export(int kind, const tj_block *a, const tj_block *b, const tj_
                        const tj_basis *env_bs, const tj_wave *wave, char flag, tj_plan_export *out);
 
 /* The split-precision form of the same H*psi (TJ_PREC_OZAKI with `slices`
- * int8 slices), for CPU checks of its tables.  A split stores R rows x K of
- * a matrix as G = ceil(R/8) row groups and ceil(K/32) k-blocks of `slices`
- * int8 digit planes, byte (kb, g, p, c, r8, b) at
- *   base + ((kb*G + g)*slices + p)*256 + c*128 + r8*16 + b
- * for row 8g + r8 and k = 32kb + 16c + b.  A job writes coef*M(r, k) =
+ * int8 slices), for CPU checks of its tables.  A split stores `rows` x K of
+ * a matrix in tiles of R rows (R = 128 for an A operand, the N tile for a B
+ * operand) and ceil(K/32) k-blocks of `slices` int8 digit planes; tile t
+ * (G_t row groups of 8: R/8, the last one gt_last) holds byte
+ * (kb, p, g, c, r8, b) at
+ *   base + t*nkb*slices*(R/8)*256 + ((kb*slices + p)*G_t + g)*256 + c*128 + r8*16 + b
+ * for tile row 8g + r8 and k = 32kb + 16c + b.  A job writes coef*M(r, k) =
  * coef*src[src_off + r*rs + k*ks] (space 1 operators, 2 input vector, 3
- * phase-1 products) for r < nrows, k < K into k-blocks kb0.. of the split at
- * pack offset dst, with the row scale held in scales[scale_idx + r] (the
- * row's max |value|; want_max: the job raises it).  A segment pairs k-blocks
- * of an A split and a B split; a family sums its segments and scales by
+ * phase-1 products) for r < nrows, k < K to split rows row0 + r, k-blocks
+ * kb0.., with the row scale held in scales[scale_idx + r] (the row's max
+ * |value|; want_max: the job raises it).  A segment pairs k-blocks of an A
+ * split and a B split; a family sums its segments and scales by
  * scales[rs_idx + row] * scales[cs_idx + col]; an item is one output tile
  * (kind 0: of cell `cell`, families [fam_begin, fam_end); kind 1: phase-1
- * products stacked in [fam_begin, fam_end) of the stack list against the
- * operator split of segment `seg`).  The plan schedules the items of each
- * launch statically over 148 CTAs (the export's device-independent choice).
- * Two-call pattern as above. */
+ * products stacked in [fam_begin, fam_end) of the stack list, segment
+ * `seg`).  The plan schedules the items of each launch statically over 148
+ * CTAs (the export's device-independent choice).  Two-call pattern as
+ * above. */
 typedef struct tj_oz_job {
   int64_t src_off, dst, scale_idx;
   double coef;
-  int32_t rs, ks, nrows, K, gtot, kb0;
-  int8_t space, want_max, pad_[6];
+  int32_t rs, ks, nrows, K, gtot, kb0, R, nkb, ntiles, gt_last, row0;
+  int8_t space, want_max, pad_[2];
 } tj_oz_job;
-typedef struct tj_oz_seg { int64_t a_base, b_base; int32_t a_gtot, b_gtot, a_kb0, b_kb0, nkb, pad_; } tj_oz_seg;
+typedef struct tj_oz_seg { int64_t a_base, b_base; int32_t a_nkb, b_nkb, a_kb0, b_kb0, nkb, pad_; } tj_oz_seg;
 typedef struct tj_oz_fam { int32_t seg_begin, seg_end; int64_t rs_idx, cs_idx; int32_t nkb, pad_; } tj_oz_fam;
 typedef struct tj_oz_stack {
-  int64_t a_base, dst_off, rs_idx, pi_idx;
-  int32_t a_gtot, a_g0, a_ng, dst_ld, ncols, pad_;
+  int64_t dst_off, rs_idx;
+  int32_t a_g0, a_ng, dst_ld, ncols;
 } tj_oz_stack;
 typedef struct tj_oz_item {
   int32_t kind, cell, row0, col0, M, N, mrows, ncols, fam_begin, fam_end, seg, init;

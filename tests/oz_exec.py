@@ -71,23 +71,31 @@ class _Machine:
                 t = t - a
                 dig[q] = a.astype(np.int64)
             assert np.all(np.abs(dig) <= 127)
-            # [kb][p][g][c][r8][16]
-            blk = dig.reshape(S, j.gtot, 8, nkb, 2, 16).transpose(3, 0, 1, 4, 2, 5)
-            start = j.dst + j.kb0 * j.gtot * S * 256
-            size = nkb * j.gtot * S * 256
-            assert 0 <= start and start + size <= len(self.pack)
-            self.pack[start:start + size] = blk.reshape(-1).astype(np.int8)
+            # split row sr -> tile, group; [tile][kb][p][g][c][r8][16]
+            for jr in range(0, rows, 8):
+                sr = j.row0 + jr
+                tt, rl = divmod(sr, j.R)
+                gt = j.R // 8 if tt < j.ntiles - 1 else j.gt_last
+                g = rl // 8
+                assert g < gt
+                tile = j.dst + tt * j.nkb * S * (j.R // 8) * 256
+                for kb in range(nkb):
+                    for q in range(S):
+                        o = tile + ((j.kb0 + kb) * S + q) * gt * 256 + g * 256
+                        assert 0 <= o and o + 256 <= len(self.pack)
+                        blk = dig[q, jr:jr + 8, kb * 32:(kb + 1) * 32].reshape(8, 2, 16).transpose(1, 0, 2)
+                        self.pack[o:o + 256] = blk.reshape(-1).astype(np.int8)
 
-    def digits(self, base, gtot, g0, ng, kb0, nkb):
-        """Slices (S, 8*ng, 32*nkb) of row groups [g0, g0+ng), k-blocks [kb0, kb0+nkb) of a split."""
+    def tile_digits(self, base, nkb_tot, tile_groups, t, g, kb0, nkb):
+        """Slices (S, 8*g, 32*nkb) of tile t (g groups; full tiles have tile_groups) of a split."""
         S = self.S
-        out = np.zeros((S, ng * 8, nkb * 32), dtype=np.int64)
+        out = np.zeros((S, g * 8, nkb * 32), dtype=np.int64)
+        tb = base + t * nkb_tot * S * tile_groups * 256
         for kb in range(nkb):
-            for q in range(S):
-                o = base + (((kb0 + kb) * S + q) * gtot + g0) * 256
-                assert 0 <= o and o + ng * 256 <= len(self.pack)
-                b = self.pack[o:o + ng * 256].astype(np.int64).reshape(ng, 2, 8, 16)
-                out[q, :, kb * 32:(kb + 1) * 32] = b.transpose(0, 2, 1, 3).reshape(ng * 8, 32)
+            o = tb + (kb0 + kb) * S * g * 256
+            assert 0 <= o and o + S * g * 256 <= len(self.pack)
+            b = self.pack[o:o + S * g * 256].astype(np.int64).reshape(S, g, 2, 8, 16)
+            out[:, :, kb * 32:(kb + 1) * 32] = b.transpose(0, 1, 3, 2, 4).reshape(S, g * 8, 32)
         return out
 
     def accum(self, A, B):
@@ -109,8 +117,15 @@ class _Machine:
         S = self.S
         for ii in range(n):
             it = items[ii]
-            ga, gb = -(-it.mrows // 8), -(-it.ncols // 8)
+            ga, gb = -(-it.mrows // 8), it.N // 8
             assert it.M in (64, 128) and it.mrows <= it.M and it.N % 16 == 0 and it.ncols <= it.N <= self.BN
+            ta, tb = it.row0 // 128, it.col0 // self.BN
+
+            def operands(sg):
+                A = self.tile_digits(sg.a_base, sg.a_nkb, 16, ta, ga, sg.a_kb0, sg.nkb)
+                B = self.tile_digits(sg.b_base, sg.b_nkb, self.BN // 8, tb, gb, sg.b_kb0, sg.nkb)
+                return A, B
+
             if it.kind == 0:
                 c = oz["cells"][it.cell]
                 key = (it.cell, it.row0, it.col0)
@@ -131,29 +146,22 @@ class _Machine:
                 tot = np.zeros((it.mrows, it.ncols))
                 for f in range(it.fam_begin, it.fam_end):
                     fm = oz["fams"][f]
-                    acc = 0
-                    A_all, B_all = [], []
-                    for sgi in range(fm.seg_begin, fm.seg_end):
-                        sg = oz["segs"][sgi]
-                        A_all.append(self.digits(sg.a_base, sg.a_gtot, it.row0 // 8, ga, sg.a_kb0, sg.nkb))
-                        B_all.append(self.digits(sg.b_base, sg.b_gtot, it.col0 // 8, gb, sg.b_kb0, sg.nkb))
-                    A = np.concatenate(A_all, axis=2)[:, :it.mrows]
-                    B = np.concatenate(B_all, axis=2)[:, :it.ncols]
+                    As, Bs = zip(*[operands(oz["segs"][sgi]) for sgi in range(fm.seg_begin, fm.seg_end)])
+                    A = np.concatenate(As, axis=2)[:, :it.mrows]
+                    B = np.concatenate(Bs, axis=2)[:, :it.ncols]
                     acc = self.accum(A, B)
                     rs = _pow2_of(self.scales[fm.rs_idx + rows])
                     cs = _pow2_of(self.scales[fm.cs_idx + cols])
                     tot = tot + (acc * rs[:, None]) * cs[None, :]
                 self.out[idx] = old + tot
             else:
-                sg = oz["segs"][it.seg]
-                pieces = [oz["stacks"][si] for si in range(it.fam_begin, it.fam_end)]
-                A = np.concatenate([self.digits(sk.a_base, sk.a_gtot, sk.a_g0, sk.a_ng, 0, sg.nkb) for sk in pieces],
-                                   axis=1)
-                B = self.digits(sg.b_base, sg.b_gtot, it.col0 // 8, gb, sg.b_kb0, sg.nkb)[:, :it.ncols]
+                A, B = operands(oz["segs"][it.seg])
+                B = B[:, :it.ncols]
                 acc = self.accum(A, B)
                 cs = _pow2_of(self.scales[it.cs_idx + np.arange(it.ncols)])
                 r0 = 0
-                for sk in pieces:
+                for si in range(it.fam_begin, it.fam_end):
+                    sk = oz["stacks"][si]
                     jl = np.arange(sk.ncols)
                     rs = _pow2_of(self.scales[sk.rs_idx + jl])
                     val = (acc[r0:r0 + sk.ncols] * rs[:, None]) * cs[None, :]
@@ -163,9 +171,6 @@ class _Machine:
                     assert key not in covered
                     covered.add(key)
                     self.scr[idx] = val
-                    pidx = sk.pi_idx + it.col0 + np.arange(it.ncols)
-                    if sk.ncols:
-                        self.scales[pidx] = np.maximum(self.scales[pidx], np.max(np.abs(val), axis=0))
                     r0 += sk.a_ng * 8
 
 
@@ -185,6 +190,7 @@ def execute_ozaki(plan, oz, psi):
         assert b[0] == 0 and b[-1] == n_items and all(x <= y for x, y in zip(b, b[1:])) and len(b) <= 149
     cov1 = set()
     m.run_items(oz["items1"], oe.n_items1, cov1)
+    m.run_max(oz["prod_jobs"], oe.n_prod_jobs)
     m.run_split(oz["prod_jobs"], oe.n_prod_jobs)
     cov2 = set()
     m.run_items(oz["items2"], oe.n_items2, cov2)
