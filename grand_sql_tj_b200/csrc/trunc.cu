@@ -29,9 +29,9 @@ constexpr int JAC_MAX_N = 4096;
 
 // Two-sided cyclic Jacobi on the symmetric matrix A (n x n, column-major).
 // Each round applies n/2 disjoint plane rotations chosen by the circle
-// method, so every pair (p, q) is visited once per sweep.  On return the
-// diagonal of A holds the eigenvalues and V the eigenvectors.  status[s] = 1
-// if max_sweeps were not enough.
+// method, so every pair (p, q) is visited once per sweep; a sweep that
+// rotates nothing ends it.  On return the diagonal of A holds the eigenvalues
+// and V the eigenvectors.  status[s] = 1 if max_sweeps were not enough.
 __global__ void __launch_bounds__(JAC_THREADS) jacobi_kernel(double *Aall, double *Vall, const int64_t *off,
                                                             const int *dims, double *evals, const int64_t *eoff,
                                                             int max_sweeps, int *status) {
@@ -41,38 +41,17 @@ __global__ void __launch_bounds__(JAC_THREADS) jacobi_kernel(double *Aall, doubl
   const int m = n + (n & 1), half = m / 2;
   double *cs = (double *)sm_raw, *sn = cs + half;
   int *pp = (int *)(sn + half), *qq = pp + half;
-  __shared__ double red[JAC_THREADS / 32], red2[JAC_THREADS / 32];
-  __shared__ int done;
+  __shared__ int rotated;
   for (int64_t i = tid; i < (int64_t)n * n; i += blockDim.x) V[i] = (i % (n + 1) == 0) ? 1.0 : 0.0;
   __syncthreads();
   int sweep = 0;
-  for (; sweep < max_sweeps && n > 1; ++sweep) {
-    // convergence: sum of squared off-diagonal entries vs squared diagonal
-    double o = 0.0, d = 0.0;
-    for (int64_t i = tid; i < (int64_t)n * n; i += blockDim.x) {
-      const int r = (int)(i % n), c = (int)(i / n);
-      const double v = A[i];
-      if (r == c) d += v * v; else o += v * v;
-    }
-    for (int k = 16; k > 0; k >>= 1) {
-      o += __shfl_down_sync(0xffffffffu, o, k);
-      d += __shfl_down_sync(0xffffffffu, d, k);
-    }
-    if ((tid & 31) == 0) {
-      red[tid >> 5] = o;
-      red2[tid >> 5] = d;
-    }
+  bool converged = n <= 1;
+  for (; sweep < max_sweeps && !converged; ++sweep) {
+    // a sweep that needs no rotation ends the iteration: every off-diagonal
+    // entry is below the FP64 rounding level of its diagonal pair,
+    // |a_pq| <= 2^-53 sqrt(|a_pp a_qq|) (the classical relative threshold)
+    if (tid == 0) rotated = 0;
     __syncthreads();
-    if (tid == 0) {
-      double so = 0, sd = 0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-        so += red[w];
-        sd += red2[w];
-      }
-      done = (so <= 1e-30 * sd) ? 1 : 0;
-    }
-    __syncthreads();
-    if (done) break;
     for (int r = 0; r < m - 1; ++r) {
       for (int i = tid; i < half; i += blockDim.x) {
         int p, q;
@@ -92,11 +71,12 @@ __global__ void __launch_bounds__(JAC_THREADS) jacobi_kernel(double *Aall, doubl
         if (q < n) {
           const double apq = A[(int64_t)q * n + p];
           const double app = A[(int64_t)p * n + p], aqq = A[(int64_t)q * n + q];
-          if (apq != 0.0 && fabs(apq) > 1e-300) {
+          if (fabs(apq) > 1e-300 && fabs(apq) > 1.1102230246251565e-16 * sqrt(fabs(app * aqq))) {
             const double tau = (aqq - app) / (2.0 * apq);
             const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
             c = 1.0 / sqrt(1.0 + t * t);
             sv = t * c;
+            rotated = 1;
           }
         } else {
           q = -1;   // pair with the padding index: no rotation
@@ -138,8 +118,10 @@ __global__ void __launch_bounds__(JAC_THREADS) jacobi_kernel(double *Aall, doubl
       }
       __syncthreads();
     }
+    converged = rotated == 0;
+    __syncthreads();
   }
-  if (tid == 0) status[s] = (sweep >= max_sweeps && n > 1) ? 1 : 0;
+  if (tid == 0) status[s] = converged ? 0 : 1;
   for (int i = tid; i < n; i += blockDim.x) evals[eoff[s] + i] = A[(int64_t)i * n + i];
 }
 
