@@ -42,14 +42,28 @@ __global__ void __launch_bounds__(JAC_THREADS) jacobi_kernel(double *Aall, doubl
   double *cs = (double *)sm_raw, *sn = cs + half;
   int *pp = (int *)(sn + half), *qq = pp + half;
   __shared__ int rotated;
+  __shared__ double dmax_sh[JAC_THREADS / 32];
   for (int64_t i = tid; i < (int64_t)n * n; i += blockDim.x) V[i] = (i % (n + 1) == 0) ? 1.0 : 0.0;
+  // sum of |diagonal| entries (the trace of a density matrix, a bound on its
+  // norm): off-diagonal entries below 8 eps of it are at the rounding level of
+  // the rotations themselves and are left alone (density matrices of
+  // truncated states have many exactly-zero eigenvalues, whose block would
+  // otherwise keep rotating on rounding noise)
+  double dm = 0.0;
+  for (int i = tid; i < n; i += blockDim.x) dm += fabs(A[(int64_t)i * n + i]);
+  for (int k = 16; k > 0; k >>= 1) dm += __shfl_xor_sync(0xffffffffu, dm, k);
+  if ((tid & 31) == 0) dmax_sh[tid >> 5] = dm;
   __syncthreads();
+  double dsum = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) dsum += dmax_sh[w];
+  const double floor_abs = fmax(8.0 * 2.220446049250313e-16 * dsum, 1e-300);
   int sweep = 0;
   bool converged = n <= 1;
   for (; sweep < max_sweeps && !converged; ++sweep) {
     // a sweep that needs no rotation ends the iteration: every off-diagonal
     // entry is below the FP64 rounding level of its diagonal pair,
-    // |a_pq| <= 2^-53 sqrt(|a_pp a_qq|) (the classical relative threshold)
+    // |a_pq| <= 2^-53 sqrt(|a_pp a_qq|) (the classical relative threshold),
+    // or below the absolute floor above
     if (tid == 0) rotated = 0;
     __syncthreads();
     for (int r = 0; r < m - 1; ++r) {
@@ -71,7 +85,7 @@ __global__ void __launch_bounds__(JAC_THREADS) jacobi_kernel(double *Aall, doubl
         if (q < n) {
           const double apq = A[(int64_t)q * n + p];
           const double app = A[(int64_t)p * n + p], aqq = A[(int64_t)q * n + q];
-          if (fabs(apq) > 1e-300 && fabs(apq) > 1.1102230246251565e-16 * sqrt(fabs(app * aqq))) {
+          if (fabs(apq) > floor_abs && fabs(apq) > 1.1102230246251565e-16 * sqrt(fabs(app * aqq))) {
             const double tau = (aqq - app) / (2.0 * apq);
             const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
             c = 1.0 / sqrt(1.0 + t * t);
