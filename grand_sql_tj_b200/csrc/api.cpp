@@ -224,7 +224,9 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
         (rc = upload_vec(ctx, ctx->ozCta2, oz->cta2)) || (rc = upload_vec(ctx, ctx->ozStaSpans, oz->sta_spans)) ||
         (rc = upload_vec(ctx, ctx->ozPsiSpans, oz->psi_spans)) || (rc = upload_vec(ctx, ctx->ozProdSpans, oz->prod_spans)) ||
         (rc = upload_vec(ctx, ctx->ozStaMSpans, oz->sta_mspans)) || (rc = upload_vec(ctx, ctx->ozPsiMSpans, oz->psi_mspans)) ||
-        (rc = upload_vec(ctx, ctx->ozProdMSpans, oz->prod_mspans)))
+        (rc = upload_vec(ctx, ctx->ozProdMSpans, oz->prod_mspans)) ||
+        (rc = upload_vec(ctx, ctx->ozPiBegin, oz->pi_begin)) || (rc = upload_vec(ctx, ctx->ozPiList, oz->pi_list)) ||
+        (rc = ctx->ozPslots.reserve(sizeof(double) * (oz->n_pslots + 4))))
       return rc;
     if ((rc = ctx->ozPack.reserve(oz->sta_pack + oz->dyn_pack + 256)) ||
         (rc = ctx->ozScales.reserve(sizeof(double) * (oz->n_scales + 4))) || (rc = ctx->ozMisc.reserve(256)))
@@ -261,8 +263,8 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
     ctx->stats.int8_ops_launch2 = oz.issued2;
     ctx->stats.flops_launch1 = oz.flops1;
     ctx->stats.flops_launch2 = oz.flops2;
-    ctx->stats.kernels_per_hpsi = (oz.psi_jobs.empty() ? 0 : 2) + (oz.items1.empty() ? 0 : 1) +
-                                  (oz.prod_jobs.empty() ? 0 : 2) + (oz.items2.empty() ? 0 : 1);
+    ctx->stats.kernels_per_hpsi = (oz.psi_jobs.empty() ? 0 : 2) + (oz.items1.empty() ? 0 : 1) + (oz.n_pi > 0 ? 1 : 0) +
+                                  (oz.prod_jobs.empty() ? 0 : 1) + (oz.items2.empty() ? 0 : 1);
   }
   ctx->plan = std::move(P);
   ctx->plan_key = h;
@@ -288,17 +290,17 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
   CK(launch_oz_gemm((const OzItem *)ctx->ozItems1.p, (const int32_t *)ctx->ozCta1.p, (int)oz.cta1.size() - 1,
                     (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzStack *)ctx->ozStacks.p, (const OzCell *)ctx->ozCells.p,
-                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, st));
+                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, ctx->ozPslots.d(), err, oz.s, st));
   if (timed) CK(cudaEventRecord(ctx->ev[2], st));
-  launch_oz_max((const OzJob *)ctx->ozProdJobs.p, (int)oz.prod_jobs.size(), (const OzSpan *)ctx->ozProdMSpans.p,
-                (int)oz.prod_mspans.size(), ctx->ops.d(), in, ctx->scr.d(), scales, st);
+  launch_oz_pi(ctx->ozPslots.d(), (const int32_t *)ctx->ozPiBegin.p, (const int64_t *)ctx->ozPiList.p, oz.n_pi,
+               scales + oz.pi0, st);
   launch_oz_split((const OzJob *)ctx->ozProdJobs.p, (int)oz.prod_jobs.size(), (const OzSpan *)ctx->ozProdSpans.p,
                   (int)oz.prod_spans.size(), ctx->ops.d(), in, ctx->scr.d(), scales, pack, oz.s, st);
   if (timed) CK(cudaEventRecord(ctx->ev[3], st));
   CK(launch_oz_gemm((const OzItem *)ctx->ozItems2.p, (const int32_t *)ctx->ozCta2.p, (int)oz.cta2.size() - 1,
                     (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzStack *)ctx->ozStacks.p, (const OzCell *)ctx->ozCells.p,
-                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, st));
+                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, ctx->ozPslots.d(), err, oz.s, st));
   if (timed) CK(cudaEventRecord(ctx->ev[4], st));
   CK(cudaGetLastError());
   ++ctx->n_hpsi;

@@ -46,8 +46,8 @@ __device__ __forceinline__ const double *oz_space(int8_t sp, const double *ops, 
 // ------------------------------------------------------------ split jobs
 // The units of a job list (one unit = one row x 16 consecutive k of a job,
 // rows padded to whole groups) are laid end to end and cut into CTAs of
-// OZ_SPLIT_THREADS threads, one unit per thread.  Within a job the unit order
-// puts the unit-stride source index across consecutive threads.
+// OZ_SPLIT_THREADS threads, one unit per thread.  Within a job consecutive
+// threads take consecutive rows.
 struct OzUnit {
   int job, r, c16;
 };
@@ -59,16 +59,13 @@ __device__ __forceinline__ bool oz_unit(const OzJob *jobs, int njobs, const OzSp
   for (; j < njobs; ++j) {
     J = jobs[j];
     const int rows = J.gtot * 8, nk16 = (J.K + 31) / 32 * 2;
-    const int64_t units = (int64_t)rows * nk16;
+    const int64_t units = J.want_split ? (int64_t)rows * nk16 : 0;
     if (k < units) {
+      // consecutive threads: consecutive rows, so that the 16-byte digit rows
+      // of a group land as whole 128-byte lines
       u.job = j;
-      if (J.rs == 1) {
-        u.r = (int)(k % rows);
-        u.c16 = (int)(k / rows);
-      } else {
-        u.r = (int)(k / nk16);
-        u.c16 = (int)(k % nk16);
-      }
+      u.r = (int)(k % rows);
+      u.c16 = (int)(k / rows);
       return true;
     }
     k -= units;
@@ -174,6 +171,7 @@ struct OzGemmParams {
   double *scales;
   const double *psi;
   double *scr, *out;
+  double *pslots;       // products: partial row maxima, one per (stacked run, row)
   int *err;
 };
 
@@ -266,8 +264,12 @@ struct OzCfg {
   static_assert(STAGES >= 2, "too few pipeline stages");
 };
 
+// 8 epilogue warps (two column halves of the tile x four TMEM lane quarters),
+// then the producer warp and the MMA warp
+constexpr int OZ_EPI_THREADS = 256, OZ_GEMM_THREADS = OZ_EPI_THREADS + 64;
+
 template <int S, int BN>
-__global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
+__global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParams p) {
   using C = OzCfg<S, BN>;
   constexpr int ST = C::STAGES;
   constexpr uint32_t GB = S * 256;   // bytes of one row group (all slices) of one k-block
@@ -278,7 +280,8 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
   __shared__ volatile int tfull_ok_sh;
   __shared__ double cscale_sh[BN];           // epilogue: column scales of the current family
   __shared__ int32_t stk_start[17];          // epilogue: first tile row of each stacked run
-  __shared__ int64_t stk_dst[16], stk_rs[16];
+  __shared__ int64_t stk_dst[16], stk_rs[16], stk_slot[16];
+  __shared__ unsigned long long pmax_sh[16][BN];   // products: |P| maxima per (run, tile column)
   __shared__ int32_t stk_ld[16], stk_nc[16];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
@@ -289,7 +292,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
     }
     for (int i = 0; i < 2; ++i) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(&tfull_bar[i])), "r"(1));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(&tempty_bar[i])), "r"(128));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(&tempty_bar[i])), "r"(OZ_EPI_THREADS));
     }
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(&drain_bar)), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -306,7 +309,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
   const uint32_t tmem = tmem_sh;
   const uint32_t smem0 = oz_smem(smem);
 
-  if (warp == 4) {
+  if (warp == OZ_EPI_THREADS / 32) {
     // ------------------------------------------------ producer (whole warp; lane 0 owns the barriers)
     int stage = 0;
     uint32_t ph = 0;
@@ -390,7 +393,7 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
       for (int i = 0; i < ST; ++i)
         if (armed & (1u << i)) oz_wait(oz_smem(&full_bar[i]), (armed_ph >> i) & 1u, nullptr);
     __syncwarp();
-  } else if (warp == 5) {
+  } else if (warp == OZ_EPI_THREADS / 32 + 1) {
     // ------------------------------------------------ MMA issuer
     if (lane == 0) {
       int stage = 0;
@@ -470,21 +473,27 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
     bool ok = true;
     for (int ii = p.cta[blockIdx.x], ie = p.cta[blockIdx.x + 1]; ii < ie && ok; ++ii) {
       const OzItem it = p.items[ii];
-      // TMEM lane of this thread = 32*warp + lane; the tile row it holds:
-      //   M = 128: row = 32*warp + lane; M = 64: rows 16w..16w+15 in lanes 32w..32w+15
+      // warp w reads TMEM lane quarter q = w % 4 (lanes 32q..32q+31) and
+      // column half h = w / 4 of the tile; the tile row it holds:
+      //   M = 128: row = 32q + lane; M = 64: rows 16q..16q+15 in lanes 32q..32q+15
+      const int quarter = warp & 3, half = warp >> 2;
       int r;
       bool rv;
       if (it.M == 128) {
-        r = tid;
+        r = quarter * 32 + lane;
         rv = r < it.mrows;
       } else {
-        r = warp * 16 + lane;
+        r = quarter * 16 + lane;
         rv = lane < 16 && r < it.mrows;
       }
+      // this half's 8-column chunks: [c0, c0 + nchh)
+      const int nch = it.N >> 3, hch = (nch + 1) >> 1;
+      const int c0 = half * hch, nchh = min(hch, nch - c0);
       const int nf = it.kind == 1 ? 1 : it.fam_end - it.fam_begin;
       double *dst = nullptr;
       int64_t cstride = 0;
       double rscale_stack = 0.0;
+      int piece = -1;   // kind 1: this row's stacked run
       OzCell c{};
       if (it.kind == 0) {
         c = p.cells[it.cell];
@@ -497,16 +506,18 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
           const OzStack sk = p.stacks[it.fam_begin + tid];
           stk_dst[tid] = sk.dst_off;
           stk_rs[tid] = sk.rs_idx;
+          stk_slot[tid] = sk.slot;
           stk_ld[tid] = sk.dst_ld;
           stk_nc[tid] = sk.ncols;
           stk_start[tid + 1] = sk.a_ng * 8;
         }
         if (tid == 0) stk_start[0] = 0;
-        asm volatile("bar.sync 1, 128;" ::: "memory");
+        for (int i = tid; i < 16 * BN; i += OZ_EPI_THREADS) pmax_sh[i / BN][i % BN] = 0ull;
+        asm volatile("bar.sync 1, 256;" ::: "memory");
         if (tid == 0)
           for (int i = 0; i < np; ++i) stk_start[i + 1] += stk_start[i];
-        asm volatile("bar.sync 1, 128;" ::: "memory");
-        int piece = -1;
+        asm volatile("bar.sync 1, 256;" ::: "memory");
+        piece = -1;
         for (int i = 0; i < np; ++i)
           if (r >= stk_start[i] && r < stk_start[i + 1]) piece = i;
         rv = rv && piece >= 0;
@@ -521,10 +532,11 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
         }
         cstride = 1;
       }
-      // the tile row of this thread, summed over the item's families
-      double accv[BN];
+      // this half of the tile row, summed over the item's families
+      constexpr int HCH = (BN / 8 + 1) / 2;   // most 8-column chunks of a half
+      double accv[HCH * 8];
 #pragma unroll
-      for (int j = 0; j < BN; ++j) accv[j] = 0.0;
+      for (int j = 0; j < HCH * 8; ++j) accv[j] = 0.0;
       for (int f = 0; f < nf; ++f) {
         const uint32_t buf = famc & 1u, use = famc >> 1;
         double rscale;
@@ -538,42 +550,40 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
           cs_idx = it.cs_idx;
         }
         // column scales of this family (once per tile); thread 0 waits for the
-        // accumulators and the named barrier hands its verdict to all 128 threads
-        asm volatile("bar.sync 1, 128;" ::: "memory");
+        // accumulators and the named barrier hands its verdict to all epilogue threads
+        asm volatile("bar.sync 1, 256;" ::: "memory");
         if (tid < it.ncols) cscale_sh[tid] = oz_pow2_of(p.scales[cs_idx + tid]);
         if (tid == 0) {
           const bool got = oz_wait(oz_smem(&tfull_bar[buf]), use & 1u, &abort_sh);
           if (!got && !abort_sh) oz_fail(&abort_sh, p.err);
           tfull_ok_sh = got ? 1 : 0;
         }
-        asm volatile("bar.sync 1, 128;" ::: "memory");
+        asm volatile("bar.sync 1, 256;" ::: "memory");
         if (!tfull_ok_sh) {
           ok = false;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;");
 #pragma unroll
-        for (int ch = 0; ch < BN / 16; ++ch) {
-          if (ch * 16 < it.N) {
-            uint32_t v[S][16];
+        for (int cl = 0; cl < HCH; ++cl) {
+          if (cl < nchh) {
+            const int col = (c0 + cl) * 8;
+            uint32_t v[S][8];
 #pragma unroll
             for (int d = 0; d < S; ++d) {
-              const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + buf * 256u + (uint32_t)(d * it.N + ch * 16);
-              asm volatile(
-                  "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-                  "[%16];"
-                  : "=r"(v[d][0]), "=r"(v[d][1]), "=r"(v[d][2]), "=r"(v[d][3]), "=r"(v[d][4]), "=r"(v[d][5]),
-                    "=r"(v[d][6]), "=r"(v[d][7]), "=r"(v[d][8]), "=r"(v[d][9]), "=r"(v[d][10]), "=r"(v[d][11]),
-                    "=r"(v[d][12]), "=r"(v[d][13]), "=r"(v[d][14]), "=r"(v[d][15])
-                  : "r"(ta));
+              const uint32_t ta = tmem + ((uint32_t)(quarter * 32) << 16) + buf * 256u + (uint32_t)(d * it.N + col);
+              asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                           : "=r"(v[d][0]), "=r"(v[d][1]), "=r"(v[d][2]), "=r"(v[d][3]), "=r"(v[d][4]),
+                             "=r"(v[d][5]), "=r"(v[d][6]), "=r"(v[d][7])
+                           : "r"(ta));
             }
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-            for (int jj = 0; jj < 16; ++jj) {
+            for (int jj = 0; jj < 8; ++jj) {
               double acc = 0.0;
 #pragma unroll
               for (int d = S - 1; d >= 0; --d) acc += (double)(int32_t)v[d][jj] * w[d];
-              accv[ch * 16 + jj] += acc * rscale * cscale_sh[ch * 16 + jj];
+              accv[cl * 8 + jj] += acc * rscale * cscale_sh[col + jj];
             }
           }
         }
@@ -582,15 +592,16 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
         ++famc;
       }
       if (!ok) break;
-      // store the tile row once: loads of a 16-column chunk first, then the stores
+      // store this half of the tile row once: loads of an 8-column chunk first, then the stores
       if (it.kind == 0) {
 #pragma unroll
-        for (int ch = 0; ch < BN / 16; ++ch) {
-          if (rv && ch * 16 < it.ncols) {
-            double old[16];
+        for (int cl = 0; cl < HCH; ++cl) {
+          const int col = (c0 + cl) * 8;
+          if (rv && cl < nchh && col < it.ncols) {
+            double old[8];
 #pragma unroll
-            for (int jj = 0; jj < 16; ++jj) {
-              const int n = ch * 16 + jj;
+            for (int jj = 0; jj < 8; ++jj) {
+              const int n = col + jj;
               old[jj] = 0.0;
               if (n < it.ncols) {
                 if (it.init) {
@@ -604,23 +615,38 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
               }
             }
 #pragma unroll
-            for (int jj = 0; jj < 16; ++jj) {
-              const int n = ch * 16 + jj;
-              if (n < it.ncols) dst[(int64_t)n * cstride] = old[jj] + accv[n];
+            for (int jj = 0; jj < 8; ++jj) {
+              const int n = col + jj;
+              if (n < it.ncols) dst[(int64_t)n * cstride] = old[jj] + accv[cl * 8 + jj];
             }
           }
         }
       } else {
+        // store P, and reduce |P| over each 8-row group (one run) into the
+        // run's shared maxima; the item then writes one partial maximum per
+        // (run, product row) and a later kernel forms pi from them
 #pragma unroll
-        for (int ch = 0; ch < BN / 16; ++ch) {
-          if (ch * 16 < it.N) {
+        for (int cl = 0; cl < HCH; ++cl) {
+          const int col = (c0 + cl) * 8;
+          if (cl < nchh) {
 #pragma unroll
-            for (int jj = 0; jj < 16; ++jj) {
-              const int n = ch * 16 + jj;
-              if (rv && n < it.ncols) dst[n] = accv[n];
+            for (int jj = 0; jj < 8; ++jj) {
+              const bool cv = col + jj < it.ncols;
+              if (rv && cv) dst[col + jj] = accv[cl * 8 + jj];
+              double m = (rv && cv) ? fabs(accv[cl * 8 + jj]) : 0.0;
+              for (int o = 1; o < 8; o <<= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+              if ((lane & 7) == 0 && piece >= 0 && cv && m > 0.0)
+                atomicMax(&pmax_sh[piece][col + jj], (unsigned long long)__double_as_longlong(m));
             }
           }
         }
+        asm volatile("bar.sync 1, 256;" ::: "memory");
+        const int np = it.fam_end - it.fam_begin;
+        for (int i = tid; i < np * it.ncols; i += OZ_EPI_THREADS) {
+          const int run = i / it.ncols, n = i - run * it.ncols;
+          p.pslots[stk_slot[run] + it.col0 + n] = __longlong_as_double((long long)pmax_sh[run][n]);
+        }
+        asm volatile("bar.sync 1, 256;" ::: "memory");
       }
     }
   }
@@ -629,7 +655,22 @@ __global__ void __launch_bounds__(192, 1) oz_gemm_kernel(OzGemmParams p) {
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
 }
 
+// pi[e] = max of the products' partial row maxima listed for entry e
+__global__ void oz_pi_kernel(const double *pslots, const int32_t *begin, const int64_t *list, int n, double *pi) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  double m = 0.0;
+  for (int k = begin[e]; k < begin[e + 1]; ++k) m = fmax(m, pslots[list[k]]);
+  pi[e] = m;
+}
+
 // ------------------------------------------------------------ host launches
+void launch_oz_pi(const double *pslots, const int32_t *pi_begin, const int64_t *pi_list, int n_pi, double *pi,
+                  cudaStream_t st) {
+  if (n_pi <= 0) return;
+  oz_pi_kernel<<<(n_pi + 255) / 256, 256, 0, st>>>(pslots, pi_begin, pi_list, n_pi, pi);
+}
+
 void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
                    const double *psi, const double *scr, double *scales, cudaStream_t st) {
   if (njobs <= 0 || nspans <= 0) return;
@@ -657,16 +698,16 @@ static cudaError_t launch_gemm_t(const OzGemmParams &p, int ncta, cudaStream_t s
   using Cf = OzCfg<S, BN>;
   cudaError_t e = cudaFuncSetAttribute(oz_gemm_kernel<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cf::SMEM);
   if (e != cudaSuccess) return e;
-  oz_gemm_kernel<S, BN><<<ncta, 192, Cf::SMEM, st>>>(p);
+  oz_gemm_kernel<S, BN><<<ncta, OZ_GEMM_THREADS, Cf::SMEM, st>>>(p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
                            const OzStack *stacks, const OzCell *cells, const Task *tasks, const uint8_t *pack,
-                           double *scales, const double *psi, double *scr, double *out, int *err, int s,
-                           cudaStream_t st) {
+                           double *scales, const double *psi, double *scr, double *out, double *pslots, int *err,
+                           int s, cudaStream_t st) {
   if (ncta <= 0) return cudaSuccess;
-  OzGemmParams p{items, cta, segs, fams, stacks, cells, tasks, pack, scales, psi, scr, out, err};
+  OzGemmParams p{items, cta, segs, fams, stacks, cells, tasks, pack, scales, psi, scr, out, pslots, err};
   switch (s) {
     case 3: return launch_gemm_t<3, 48>(p, ncta, st);
     case 4: return launch_gemm_t<4, 48>(p, ncta, st);

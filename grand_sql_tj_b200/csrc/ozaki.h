@@ -60,7 +60,8 @@ inline int oz_bn(int s) { return s <= 5 ? 48 : 32; }
 // job writes gtot groups (rows up to row0 + 8*gtot; rows past nrows and k
 // past K as zero digits).  The row scale is scales[scale_idx + r] (max
 // |value| of the row, made a power of two by the kernels); want_max: the job
-// contributes to that maximum.
+// contributes to that maximum; want_split: the job writes digits (a job
+// with only want_max computes a maximum shared by other jobs).
 struct OzJob {
   int64_t src_off;
   int64_t dst;
@@ -69,8 +70,8 @@ struct OzJob {
   int32_t rs, ks, nrows, K;
   int32_t gtot, kb0;
   int32_t R, nkb, ntiles, gt_last, row0;
-  int8_t space, want_max;
-  int8_t pad[2];
+  int8_t space, want_max, want_split;
+  int8_t pad;
 };
 
 // One k-range of an operand pair: k-blocks [a_kb0, a_kb0 + nkb) of the A
@@ -97,6 +98,7 @@ struct OzFam {
 struct OzStack {
   int64_t dst_off;          // P_t(0, 8*a_g0) in the product space
   int64_t rs_idx;           // tau index of X_t's column 8*a_g0
+  int64_t slot;             // partial row maxima of this run: slot + i for P_t row i
   int32_t a_g0, a_ng;
   int32_t dst_ld;
   int32_t ncols;            // valid rows of this run
@@ -154,6 +156,13 @@ struct OzPlan {
   std::vector<OzJob> prod_jobs;            // per H*psi, between the launches
   std::vector<OzSpan> sta_spans, psi_spans, prod_spans;            // split units
   std::vector<OzSpan> sta_mspans, psi_mspans, prod_mspans;         // maximum units
+  // pi = row maxima of the products: launch 1 leaves one partial maximum per
+  // (stacked run, product row) in n_pslots slots; pi entry e (e < n_pi) is
+  // the maximum of slots pi_list[pi_begin[e] .. pi_begin[e+1])
+  int64_t n_pslots = 0;
+  int32_t n_pi = 0;
+  std::vector<int32_t> pi_begin;
+  std::vector<int64_t> pi_list;
   // GEMM tables
   std::vector<OzSeg> segs;
   std::vector<OzFam> fams;
@@ -177,9 +186,11 @@ void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans
                    const double *psi, const double *scr, double *scales, cudaStream_t st);
 void launch_oz_split(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
                      const double *psi, const double *scr, const double *scales, uint8_t *pack, int s, cudaStream_t st);
+void launch_oz_pi(const double *pslots, const int32_t *pi_begin, const int64_t *pi_list, int n_pi, double *pi,
+                  cudaStream_t st);
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
                            const OzStack *stacks, const OzCell *cells, const Task *tasks, const uint8_t *pack,
-                           double *scales, const double *psi, double *scr, double *out, int *err, int s,
-                           cudaStream_t st);
+                           double *scales, const double *psi, double *scr, double *out, double *pslots, int *err,
+                           int s, cudaStream_t st);
 
 }  // namespace tjb

@@ -105,6 +105,7 @@ struct Builder {
     j.row0 = row0;
     j.space = space;
     j.want_max = want_max ? 1 : 0;
+    j.want_split = 1;
     return j;
   }
   // Split rows of op(M) (role 0) or of op(M)^T (role 1): element (r, k) at
@@ -121,6 +122,20 @@ struct Builder {
     if (it == psi_cell.end()) throw std::runtime_error("psi operand is not a cell");
     return it->second;
   }
+  // tau of psi cell c's columns: from its column split's job, or from a
+  // maximum-only job when the cell is only stacked (one job per cell)
+  std::vector<char> tau_job;
+  std::vector<std::pair<int64_t, int64_t>> pi_slots;   // (pi entry, slot), pi-relative entries
+  void tau_of(int c) {
+    if (tau_job[c]) return;
+    tau_job[c] = 1;
+    const Cell &x = hp.cells2[c];
+    const Tiling t = tiling(x.N, x.M, true);
+    OzJob j = job(SP_PSI, x.off, x.ld, 1, x.N, x.M, 1.0, 0, t, 0, t.gsum, 0, hp.cell2_col_state[c], true);
+    j.want_split = 0;
+    dyn_psi.push_back(j);
+    dyn_psi_rel.push_back(REL_TAU);
+  }
   // psi cell c as a B operand: rows = its columns (scale tau), K = its rows
   int64_t psi_col(int c) {
     if (colsplit[c] < 0) {
@@ -128,8 +143,9 @@ struct Builder {
       const Tiling t = tiling(x.N, x.M, true);
       colsplit[c] = alloc_dyn(t);
       dyn_psi.push_back(job(SP_PSI, x.off, x.ld, 1, x.N, x.M, 1.0, colsplit[c], t, 0, t.gsum, 0,
-                            hp.cell2_col_state[c], true));
+                            hp.cell2_col_state[c], !tau_job[c]));
       dyn_psi_rel.push_back(REL_TAU);
+      tau_job[c] = 1;
     }
     return colsplit[c];
   }
@@ -151,8 +167,9 @@ struct Builder {
       const Cell &P = hp.cells1[p];
       const Tiling t = tiling(P.M, P.N, false);
       prodsplit[p] = alloc_dyn(t);
+      // pi comes from launch 1's partial maxima, not from a pass over P
       dyn_prod.push_back(job(SP_SCR, P.off, 1, P.ld, P.M, P.N, 1.0, prodsplit[p], t, 0, t.gsum, 0,
-                             hp.cell1_row_state[p], true));
+                             hp.cell1_row_state[p], false));
     }
     return prodsplit[p];
   }
@@ -189,6 +206,7 @@ struct Builder {
       struct Run {
         OzStack st;
         int x;   // psi cell
+        int p;   // product
       };
       std::vector<Run> runs;
       for (int p : prods) {
@@ -203,6 +221,7 @@ struct Builder {
           Run r;
           std::memset(&r.st, 0, sizeof r.st);
           r.x = x;
+          r.p = p;
           r.st.a_g0 = g0;
           r.st.a_ng = std::min(16, G - g0);
           r.st.dst_off = c.off + (int64_t)8 * g0 * c.ld;
@@ -225,10 +244,16 @@ struct Builder {
         for (size_t q = i; q < e; ++q) {
           const Run &r = runs[q];
           const Cell &X = hp.cells2[r.x];
-          oz.stacks.push_back(r.st);
+          OzStack st = r.st;
+          st.slot = oz.n_pslots;
+          oz.n_pslots += Mop;
+          for (int32_t i = 0; i < Mop; ++i) pi_slots.push_back({hp.cell1_row_state[r.p] + i, st.slot + i});
+          oz.stacks.push_back(st);
+          // tau of X's columns comes from X's own maximum job (tau_of)
           dyn_psi.push_back(job(SP_PSI, X.off + (int64_t)8 * r.st.a_g0 * X.ld, X.ld, 1, r.st.ncols, K, 1.0, sk, ta,
-                                8 * off, r.st.a_ng, 0, hp.cell2_col_state[r.x] + 8 * r.st.a_g0, true));
+                                8 * off, r.st.a_ng, 0, hp.cell2_col_state[r.x] + 8 * r.st.a_g0, false));
           dyn_psi_rel.push_back(REL_TAU);
+          tau_of(r.x);
           off += r.st.a_ng;
         }
         const int fe = (int)oz.stacks.size();
@@ -462,6 +487,21 @@ struct Builder {
         else
           for (int f = it.fam_begin; f < it.fam_end; ++f) it.nkb += oz.fams[f].nkb;
       }
+    // pi lists: entries are pi-relative row states
+    oz.n_pi = hp.n_sys_states;
+    std::sort(pi_slots.begin(), pi_slots.end());
+    oz.pi_begin.assign(oz.n_pi + 1, 0);
+    oz.pi_list.clear();
+    oz.pi_list.reserve(pi_slots.size());
+    {
+      size_t k = 0;
+      for (int32_t e = 0; e < oz.n_pi; ++e) {
+        oz.pi_begin[e] = (int32_t)oz.pi_list.size();
+        while (k < pi_slots.size() && pi_slots[k].first == e) oz.pi_list.push_back(pi_slots[k++].second);
+      }
+      oz.pi_begin[oz.n_pi] = (int32_t)oz.pi_list.size();
+      if (k != pi_slots.size()) throw std::runtime_error("product row outside the sys states");
+    }
     oz.psi_jobs = std::move(dyn_psi);
     oz.prod_jobs = std::move(dyn_prod);
     make_spans(oz.sta_jobs, oz.sta_spans, false);
@@ -499,7 +539,7 @@ struct Builder {
   // Split units cover gtot*8 rows x K/16; maximum units nrows x K/OZ_MAX_CHUNK.
   static int64_t job_units(const OzJob &j, bool max_units) {
     if (max_units) return j.want_max ? (int64_t)j.nrows * cdiv(j.K, OZ_MAX_CHUNK) : 0;
-    return (int64_t)j.gtot * 8 * (cdiv(j.K, 32) * 2);
+    return j.want_split ? (int64_t)j.gtot * 8 * (cdiv(j.K, 32) * 2) : 0;
   }
   static void make_spans(const std::vector<OzJob> &jobs, std::vector<OzSpan> &spans, bool max_units) {
     spans.clear();
@@ -552,6 +592,7 @@ struct Builder {
     for (size_t p = 0; p < hp.cells1.size(); ++p) prod_of[hp.cells1[p].off] = (int)p;
     colsplit.assign(npsi, -1);
     rowsplit.assign(npsi, -1);
+    tau_job.assign(npsi, 0);
     prodsplit.assign(hp.cells1.size(), -1);
     products();
     cells();
@@ -620,5 +661,12 @@ extern "C" int tj_ozaki_plan_export(const tj_lattice *lat, const tj_model *sys, 
   put(out->items2, oz.items2, out->n_items2);
   put(out->cta1, oz.cta1, out->n_cta1);
   put(out->cta2, oz.cta2, out->n_cta2);
+  out->n_pslots = oz.n_pslots;
+  out->n_pi = oz.n_pi;
+  {
+    int64_t dummy = 0;
+    put(out->pi_begin, oz.pi_begin, dummy);
+  }
+  put(out->pi_list, oz.pi_list, out->n_pi_list);
   return TJ_OK;
 }

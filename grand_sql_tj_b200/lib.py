@@ -78,7 +78,7 @@ class OzJobC(C.Structure):
     _fields_ = [("src_off", C.c_int64), ("dst", C.c_int64), ("scale_idx", C.c_int64), ("coef", C.c_double)] + \
                [(n, C.c_int32) for n in ("rs", "ks", "nrows", "K", "gtot", "kb0", "R", "nkb", "ntiles", "gt_last",
                                          "row0")] + \
-               [("space", C.c_int8), ("want_max", C.c_int8), ("pad_", C.c_int8 * 2)]
+               [("space", C.c_int8), ("want_max", C.c_int8), ("want_split", C.c_int8), ("pad_", C.c_int8)]
 
 
 class OzSegC(C.Structure):
@@ -92,7 +92,7 @@ class OzFamC(C.Structure):
 
 
 class OzStackC(C.Structure):
-    _fields_ = [("dst_off", C.c_int64), ("rs_idx", C.c_int64)] + \
+    _fields_ = [("dst_off", C.c_int64), ("rs_idx", C.c_int64), ("slot", C.c_int64)] + \
                [(n, C.c_int32) for n in ("a_g0", "a_ng", "dst_ld", "ncols")]
 
 
@@ -117,7 +117,8 @@ class OzExport(C.Structure):
                 [("n_" + n, C.c_int64) for n, _ in _OZ_ARRAYS] +
                 [(n, C.POINTER(t)) for n, t in _OZ_ARRAYS] +
                 [("n_cta1", C.c_int64), ("n_cta2", C.c_int64), ("cta1", C.POINTER(C.c_int32)),
-                 ("cta2", C.POINTER(C.c_int32))])
+                 ("cta2", C.POINTER(C.c_int32)), ("n_pslots", C.c_int64), ("n_pi", C.c_int64),
+                 ("n_pi_list", C.c_int64), ("pi_begin", C.POINTER(C.c_int32)), ("pi_list", C.POINTER(C.c_int64))])
 
 
 _lib = None
@@ -356,6 +357,8 @@ def ozaki_plan_export(sb, slices: int = 5, invec: Optional[Wave] = None) -> dict
     arrs = {n: (t * max(getattr(ex, "n_" + n), 1))() for n, t in _OZ_ARRAYS}
     arrs["cta1"] = (C.c_int32 * max(ex.n_cta1, 1))()
     arrs["cta2"] = (C.c_int32 * max(ex.n_cta2, 1))()
+    arrs["pi_begin"] = (C.c_int32 * max(ex.n_pi + 1, 1))()
+    arrs["pi_list"] = (C.c_int64 * max(ex.n_pi_list, 1))()
     for k, a in arrs.items():
         setattr(ex, k, C.cast(a, type(getattr(ex, k))))
     _chk(call(C.byref(ex)))

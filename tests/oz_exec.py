@@ -35,6 +35,7 @@ class _Machine:
         self.out = np.full(max(ex.psi_len, 1), np.nan)
         self.pack = np.zeros(oe.sta_pack + oe.dyn_pack, dtype=np.int8)
         self.scales = np.zeros(oe.n_scales)
+        self.pslots = np.full(max(oe.n_pslots, 1), np.nan)
         self.spaces = {1: self.ops, 2: self.psi, 3: self.scr}
 
     def _matrix(self, j):
@@ -56,6 +57,8 @@ class _Machine:
         S = self.S
         for i in range(n):
             j = jobs[i]
+            if not j.want_split:
+                continue
             nkb = -(-j.K // 32)
             rows = j.gtot * 8
             X = np.zeros((rows, nkb * 32))
@@ -171,6 +174,8 @@ class _Machine:
                     assert key not in covered
                     covered.add(key)
                     self.scr[idx] = val
+                    # partial row maxima of this run's product rows col0 .. col0 + ncols
+                    self.pslots[sk.slot + it.col0 + np.arange(it.ncols)] = np.max(np.abs(val), axis=0)
                     r0 += sk.a_ng * 8
 
 
@@ -190,6 +195,13 @@ def execute_ozaki(plan, oz, psi):
         assert b[0] == 0 and b[-1] == n_items and all(x <= y for x, y in zip(b, b[1:])) and len(b) <= 149
     cov1 = set()
     m.run_items(oz["items1"], oe.n_items1, cov1)
+    # pi from the partial maxima (every slot written by launch 1)
+    assert oe.n_pslots == 0 or np.all(np.isfinite(m.pslots))
+    pb = [oz["pi_begin"][e] for e in range(oe.n_pi + 1)]
+    pl = np.array([oz["pi_list"][k] for k in range(oe.n_pi_list)], dtype=np.int64)
+    for e in range(oe.n_pi):
+        if pb[e + 1] > pb[e]:
+            m.scales[oe.pi0 + e] = np.max(m.pslots[pl[pb[e]:pb[e + 1]]])
     m.run_max(oz["prod_jobs"], oe.n_prod_jobs)
     m.run_split(oz["prod_jobs"], oe.n_prod_jobs)
     cov2 = set()
