@@ -655,20 +655,22 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
 }
 
-// pi[e] = max of the products' partial row maxima listed for entry e
+// pi[e] = max of the products' partial row maxima listed for entry e; one
+// warp per entry (lists run to thousands of slots for the busiest states)
 __global__ void oz_pi_kernel(const double *pslots, const int32_t *begin, const int64_t *list, int n, double *pi) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (e >= n) return;
   double m = 0.0;
-  for (int k = begin[e]; k < begin[e + 1]; ++k) m = fmax(m, pslots[list[k]]);
-  pi[e] = m;
+  for (int k = begin[e] + lane; k < begin[e + 1]; k += 32) m = fmax(m, pslots[list[k]]);
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) pi[e] = m;
 }
 
 // ------------------------------------------------------------ host launches
 void launch_oz_pi(const double *pslots, const int32_t *pi_begin, const int64_t *pi_list, int n_pi, double *pi,
                   cudaStream_t st) {
   if (n_pi <= 0) return;
-  oz_pi_kernel<<<(n_pi + 255) / 256, 256, 0, st>>>(pslots, pi_begin, pi_list, n_pi, pi);
+  oz_pi_kernel<<<(n_pi + 7) / 8, 256, 0, st>>>(pslots, pi_begin, pi_list, n_pi, pi);
 }
 
 void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
