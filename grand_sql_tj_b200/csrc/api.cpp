@@ -225,8 +225,8 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
         (rc = upload_vec(ctx, ctx->ozPsiSpans, oz->psi_spans)) || (rc = upload_vec(ctx, ctx->ozProdSpans, oz->prod_spans)) ||
         (rc = upload_vec(ctx, ctx->ozStaMSpans, oz->sta_mspans)) || (rc = upload_vec(ctx, ctx->ozPsiMSpans, oz->psi_mspans)) ||
         (rc = upload_vec(ctx, ctx->ozProdMSpans, oz->prod_mspans)) ||
-        (rc = upload_vec(ctx, ctx->ozPiBegin, oz->pi_begin)) || (rc = upload_vec(ctx, ctx->ozPiList, oz->pi_list)) ||
-        (rc = ctx->ozPslots.reserve(sizeof(double) * (oz->n_pslots + 4))))
+        (rc = upload_vec(ctx, ctx->ozStaMJobs, oz->sta_mjobs)) || (rc = upload_vec(ctx, ctx->ozPsiMJobs, oz->psi_mjobs)) ||
+        (rc = upload_vec(ctx, ctx->ozProdMJobs, oz->prod_mjobs)))
       return rc;
     if ((rc = ctx->ozPack.reserve(oz->sta_pack + oz->dyn_pack + 256)) ||
         (rc = ctx->ozScales.reserve(sizeof(double) * (oz->n_scales + 4))) || (rc = ctx->ozMisc.reserve(256)))
@@ -234,7 +234,7 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
     CK(cudaMemsetAsync(ctx->ozMisc.p, 0, 256, ctx->stream));
     CK(cudaMemsetAsync(ctx->ozScales.p, 0, sizeof(double) * (oz->n_scales + 4), ctx->stream));
     // operator splits: once per step
-    launch_oz_max((const OzJob *)ctx->ozStaJobs.p, (int)oz->sta_jobs.size(), (const OzSpan *)ctx->ozStaMSpans.p,
+    launch_oz_max((const OzJob *)ctx->ozStaMJobs.p, (int)oz->sta_mjobs.size(), (const OzSpan *)ctx->ozStaMSpans.p,
                   (int)oz->sta_mspans.size(), ctx->ops.d(), nullptr, nullptr, ctx->ozScales.d(), ctx->stream);
     launch_oz_split((const OzJob *)ctx->ozStaJobs.p, (int)oz->sta_jobs.size(), (const OzSpan *)ctx->ozStaSpans.p,
                     (int)oz->sta_spans.size(), ctx->ops.d(), nullptr, nullptr, ctx->ozScales.d(),
@@ -263,8 +263,9 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
     ctx->stats.int8_ops_launch2 = oz.issued2;
     ctx->stats.flops_launch1 = oz.flops1;
     ctx->stats.flops_launch2 = oz.flops2;
-    ctx->stats.kernels_per_hpsi = (oz.psi_jobs.empty() ? 0 : 2) + (oz.items1.empty() ? 0 : 1) + (oz.n_pi > 0 ? 1 : 0) +
-                                  (oz.prod_jobs.empty() ? 0 : 1) + (oz.items2.empty() ? 0 : 1);
+    ctx->stats.kernels_per_hpsi = (oz.psi_mspans.empty() ? 0 : 1) + (oz.psi_spans.empty() ? 0 : 1) +
+                                  (oz.items1.empty() ? 0 : 1) + (oz.prod_mspans.empty() ? 0 : 1) +
+                                  (oz.prod_spans.empty() ? 0 : 1) + (oz.items2.empty() ? 0 : 1);
   }
   ctx->plan = std::move(P);
   ctx->plan_key = h;
@@ -282,7 +283,7 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
   uint8_t *pack = (uint8_t *)ctx->ozPack.p;
   CK(cudaMemsetAsync(scales + oz.dyn_scale_begin, 0, sizeof(double) * (oz.n_scales - oz.dyn_scale_begin), st));
   if (timed) CK(cudaEventRecord(ctx->ev[0], st));
-  launch_oz_max((const OzJob *)ctx->ozPsiJobs.p, (int)oz.psi_jobs.size(), (const OzSpan *)ctx->ozPsiMSpans.p,
+  launch_oz_max((const OzJob *)ctx->ozPsiMJobs.p, (int)oz.psi_mjobs.size(), (const OzSpan *)ctx->ozPsiMSpans.p,
                 (int)oz.psi_mspans.size(), ctx->ops.d(), in, ctx->scr.d(), scales, st);
   launch_oz_split((const OzJob *)ctx->ozPsiJobs.p, (int)oz.psi_jobs.size(), (const OzSpan *)ctx->ozPsiSpans.p,
                   (int)oz.psi_spans.size(), ctx->ops.d(), in, ctx->scr.d(), scales, pack, oz.s, st);
@@ -290,17 +291,17 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
   CK(launch_oz_gemm((const OzItem *)ctx->ozItems1.p, (const int32_t *)ctx->ozCta1.p, (int)oz.cta1.size() - 1,
                     (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzStack *)ctx->ozStacks.p, (const OzCell *)ctx->ozCells.p,
-                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, ctx->ozPslots.d(), err, oz.s, st));
+                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, st));
   if (timed) CK(cudaEventRecord(ctx->ev[2], st));
-  launch_oz_pi(ctx->ozPslots.d(), (const int32_t *)ctx->ozPiBegin.p, (const int64_t *)ctx->ozPiList.p, oz.n_pi,
-               scales + oz.pi0, st);
+  launch_oz_max((const OzJob *)ctx->ozProdMJobs.p, (int)oz.prod_mjobs.size(), (const OzSpan *)ctx->ozProdMSpans.p,
+                (int)oz.prod_mspans.size(), ctx->ops.d(), in, ctx->scr.d(), scales, st);
   launch_oz_split((const OzJob *)ctx->ozProdJobs.p, (int)oz.prod_jobs.size(), (const OzSpan *)ctx->ozProdSpans.p,
                   (int)oz.prod_spans.size(), ctx->ops.d(), in, ctx->scr.d(), scales, pack, oz.s, st);
   if (timed) CK(cudaEventRecord(ctx->ev[3], st));
   CK(launch_oz_gemm((const OzItem *)ctx->ozItems2.p, (const int32_t *)ctx->ozCta2.p, (int)oz.cta2.size() - 1,
                     (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzStack *)ctx->ozStacks.p, (const OzCell *)ctx->ozCells.p,
-                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, ctx->ozPslots.d(), err, oz.s, st));
+                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, st));
   if (timed) CK(cudaEventRecord(ctx->ev[4], st));
   CK(cudaGetLastError());
   ++ctx->n_hpsi;

@@ -59,7 +59,7 @@ __device__ __forceinline__ bool oz_unit(const OzJob *jobs, int njobs, const OzSp
   for (; j < njobs; ++j) {
     J = jobs[j];
     const int rows = J.gtot * 8, nk16 = (J.K + 31) / 32 * 2;
-    const int64_t units = J.want_split ? (int64_t)rows * nk16 : 0;
+    const int64_t units = (int64_t)rows * nk16;
     if (k < units) {
       // consecutive threads: consecutive rows, so that the 16-byte digit rows
       // of a group land as whole 128-byte lines
@@ -73,8 +73,9 @@ __device__ __forceinline__ bool oz_unit(const OzJob *jobs, int njobs, const OzSp
   return false;
 }
 
-// Row maxima of |coef * M| over the jobs with want_max: one unit = one row x
-// OZ_MAX_CHUNK k, one atomic max per unit.
+// Row maxima of |coef * M| (a list of maximum jobs): one unit = one row x
+// OZ_MAX_CHUNK k, consecutive threads on consecutive rows, one atomic max
+// per unit.
 __global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_max_kernel(const OzJob *jobs, int njobs, const OzSpan *spans,
                                                                   const double *ops, const double *psi,
                                                                   const double *scr, double *scales) {
@@ -84,17 +85,11 @@ __global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_max_kernel(const OzJob *j
   int r = -1, c = 0;
   for (int j = sp.job; j < njobs; ++j) {
     J = jobs[j];
-    if (!J.want_max) continue;
     const int nc = (J.K + OZ_MAX_CHUNK - 1) / OZ_MAX_CHUNK;
     const int64_t units = (int64_t)J.nrows * nc;
     if (k < units) {
-      if (J.rs == 1) {   // consecutive threads: consecutive rows
-        r = (int)(k % J.nrows);
-        c = (int)(k / J.nrows);
-      } else {
-        r = (int)(k / nc);
-        c = (int)(k % nc);
-      }
+      r = (int)(k % J.nrows);
+      c = (int)(k / J.nrows);
       break;
     }
     k -= units;
@@ -102,8 +97,16 @@ __global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_max_kernel(const OzJob *j
   if (r < 0) return;
   const double *row = oz_space(J.space, ops, psi, scr) + J.src_off + (int64_t)r * J.rs;
   const int k0 = c * OZ_MAX_CHUNK, k1 = min(J.K, k0 + OZ_MAX_CHUNK);
-  double m = 0.0;
-  for (int kk = k0; kk < k1; ++kk) m = fmax(m, fabs(J.coef * row[(int64_t)kk * J.ks]));
+  double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+  int kk = k0;
+  for (; kk + 4 <= k1; kk += 4) {
+    m0 = fmax(m0, fabs(row[(int64_t)kk * J.ks]));
+    m1 = fmax(m1, fabs(row[(int64_t)(kk + 1) * J.ks]));
+    m2 = fmax(m2, fabs(row[(int64_t)(kk + 2) * J.ks]));
+    m3 = fmax(m3, fabs(row[(int64_t)(kk + 3) * J.ks]));
+  }
+  for (; kk < k1; ++kk) m0 = fmax(m0, fabs(row[(int64_t)kk * J.ks]));
+  const double m = fabs(J.coef) * fmax(fmax(m0, m1), fmax(m2, m3));
   if (m > 0.0)
     atomicMax((unsigned long long *)&scales[J.scale_idx + r], (unsigned long long)__double_as_longlong(m));
 }
@@ -171,7 +174,6 @@ struct OzGemmParams {
   double *scales;
   const double *psi;
   double *scr, *out;
-  double *pslots;       // products: partial row maxima, one per (stacked run, row)
   int *err;
 };
 
@@ -280,8 +282,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
   __shared__ volatile int tfull_ok_sh;
   __shared__ double cscale_sh[BN];           // epilogue: column scales of the current family
   __shared__ int32_t stk_start[17];          // epilogue: first tile row of each stacked run
-  __shared__ int64_t stk_dst[16], stk_rs[16], stk_slot[16];
-  __shared__ unsigned long long pmax_sh[16][BN];   // products: |P| maxima per (run, tile column)
+  __shared__ int64_t stk_dst[16], stk_rs[16];
   __shared__ int32_t stk_ld[16], stk_nc[16];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
@@ -493,7 +494,6 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       double *dst = nullptr;
       int64_t cstride = 0;
       double rscale_stack = 0.0;
-      int piece = -1;   // kind 1: this row's stacked run
       OzCell c{};
       if (it.kind == 0) {
         c = p.cells[it.cell];
@@ -506,18 +506,16 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
           const OzStack sk = p.stacks[it.fam_begin + tid];
           stk_dst[tid] = sk.dst_off;
           stk_rs[tid] = sk.rs_idx;
-          stk_slot[tid] = sk.slot;
           stk_ld[tid] = sk.dst_ld;
           stk_nc[tid] = sk.ncols;
           stk_start[tid + 1] = sk.a_ng * 8;
         }
         if (tid == 0) stk_start[0] = 0;
-        for (int i = tid; i < 16 * BN; i += OZ_EPI_THREADS) pmax_sh[i / BN][i % BN] = 0ull;
         asm volatile("bar.sync 1, 256;" ::: "memory");
         if (tid == 0)
           for (int i = 0; i < np; ++i) stk_start[i + 1] += stk_start[i];
         asm volatile("bar.sync 1, 256;" ::: "memory");
-        piece = -1;
+        int piece = -1;
         for (int i = 0; i < np; ++i)
           if (r >= stk_start[i] && r < stk_start[i + 1]) piece = i;
         rv = rv && piece >= 0;
@@ -622,31 +620,15 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
           }
         }
       } else {
-        // store P, and reduce |P| over each 8-row group (one run) into the
-        // run's shared maxima; the item then writes one partial maximum per
-        // (run, product row) and a later kernel forms pi from them
 #pragma unroll
         for (int cl = 0; cl < HCH; ++cl) {
           const int col = (c0 + cl) * 8;
-          if (cl < nchh) {
+          if (rv && cl < nchh) {
 #pragma unroll
-            for (int jj = 0; jj < 8; ++jj) {
-              const bool cv = col + jj < it.ncols;
-              if (rv && cv) dst[col + jj] = accv[cl * 8 + jj];
-              double m = (rv && cv) ? fabs(accv[cl * 8 + jj]) : 0.0;
-              for (int o = 1; o < 8; o <<= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-              if ((lane & 7) == 0 && piece >= 0 && cv && m > 0.0)
-                atomicMax(&pmax_sh[piece][col + jj], (unsigned long long)__double_as_longlong(m));
-            }
+            for (int jj = 0; jj < 8; ++jj)
+              if (col + jj < it.ncols) dst[col + jj] = accv[cl * 8 + jj];
           }
         }
-        asm volatile("bar.sync 1, 256;" ::: "memory");
-        const int np = it.fam_end - it.fam_begin;
-        for (int i = tid; i < np * it.ncols; i += OZ_EPI_THREADS) {
-          const int run = i / it.ncols, n = i - run * it.ncols;
-          p.pslots[stk_slot[run] + it.col0 + n] = __longlong_as_double((long long)pmax_sh[run][n]);
-        }
-        asm volatile("bar.sync 1, 256;" ::: "memory");
       }
     }
   }
@@ -655,24 +637,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
 }
 
-// pi[e] = max of the products' partial row maxima listed for entry e; one
-// warp per entry (lists run to thousands of slots for the busiest states)
-__global__ void oz_pi_kernel(const double *pslots, const int32_t *begin, const int64_t *list, int n, double *pi) {
-  const int e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (e >= n) return;
-  double m = 0.0;
-  for (int k = begin[e] + lane; k < begin[e + 1]; k += 32) m = fmax(m, pslots[list[k]]);
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if (lane == 0) pi[e] = m;
-}
-
 // ------------------------------------------------------------ host launches
-void launch_oz_pi(const double *pslots, const int32_t *pi_begin, const int64_t *pi_list, int n_pi, double *pi,
-                  cudaStream_t st) {
-  if (n_pi <= 0) return;
-  oz_pi_kernel<<<(n_pi + 7) / 8, 256, 0, st>>>(pslots, pi_begin, pi_list, n_pi, pi);
-}
-
 void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
                    const double *psi, const double *scr, double *scales, cudaStream_t st) {
   if (njobs <= 0 || nspans <= 0) return;
@@ -706,10 +671,10 @@ static cudaError_t launch_gemm_t(const OzGemmParams &p, int ncta, cudaStream_t s
 
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
                            const OzStack *stacks, const OzCell *cells, const Task *tasks, const uint8_t *pack,
-                           double *scales, const double *psi, double *scr, double *out, double *pslots, int *err,
-                           int s, cudaStream_t st) {
+                           double *scales, const double *psi, double *scr, double *out, int *err, int s,
+                           cudaStream_t st) {
   if (ncta <= 0) return cudaSuccess;
-  OzGemmParams p{items, cta, segs, fams, stacks, cells, tasks, pack, scales, psi, scr, out, pslots, err};
+  OzGemmParams p{items, cta, segs, fams, stacks, cells, tasks, pack, scales, psi, scr, out, err};
   switch (s) {
     case 3: return launch_gemm_t<3, 48>(p, ncta, st);
     case 4: return launch_gemm_t<4, 48>(p, ncta, st);

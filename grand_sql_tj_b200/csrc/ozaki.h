@@ -98,7 +98,6 @@ struct OzFam {
 struct OzStack {
   int64_t dst_off;          // P_t(0, 8*a_g0) in the product space
   int64_t rs_idx;           // tau index of X_t's column 8*a_g0
-  int64_t slot;             // partial row maxima of this run: slot + i for P_t row i
   int32_t a_g0, a_ng;
   int32_t dst_ld;
   int32_t ncols;            // valid rows of this run
@@ -151,18 +150,13 @@ struct OzPlan {
   int64_t dyn_scale_begin = 0;             // first dynamic scale (zeroed per H*psi)
   int64_t rho0 = 0, tau0 = 0, pi0 = 0;
   // jobs
-  std::vector<OzJob> sta_jobs;             // once per step
-  std::vector<OzJob> psi_jobs;             // per H*psi, before launch 1
-  std::vector<OzJob> prod_jobs;            // per H*psi, between the launches
+  std::vector<OzJob> sta_jobs;             // splits once per step
+  std::vector<OzJob> psi_jobs;             // splits per H*psi, before launch 1
+  std::vector<OzJob> prod_jobs;            // splits per H*psi, between the launches
   std::vector<OzSpan> sta_spans, psi_spans, prod_spans;            // split units
   std::vector<OzSpan> sta_mspans, psi_mspans, prod_mspans;         // maximum units
-  // pi = row maxima of the products: launch 1 leaves one partial maximum per
-  // (stacked run, product row) in n_pslots slots; pi entry e (e < n_pi) is
-  // the maximum of slots pi_list[pi_begin[e] .. pi_begin[e+1])
-  int64_t n_pslots = 0;
-  int32_t n_pi = 0;
-  std::vector<int32_t> pi_begin;
-  std::vector<int64_t> pi_list;
+  // maximum jobs (the jobs with want_max, in their own lists)
+  std::vector<OzJob> sta_mjobs, psi_mjobs, prod_mjobs;
   // GEMM tables
   std::vector<OzSeg> segs;
   std::vector<OzFam> fams;
@@ -186,11 +180,9 @@ void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans
                    const double *psi, const double *scr, double *scales, cudaStream_t st);
 void launch_oz_split(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
                      const double *psi, const double *scr, const double *scales, uint8_t *pack, int s, cudaStream_t st);
-void launch_oz_pi(const double *pslots, const int32_t *pi_begin, const int64_t *pi_list, int n_pi, double *pi,
-                  cudaStream_t st);
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
                            const OzStack *stacks, const OzCell *cells, const Task *tasks, const uint8_t *pack,
-                           double *scales, const double *psi, double *scr, double *out, double *pslots, int *err,
-                           int s, cudaStream_t st);
+                           double *scales, const double *psi, double *scr, double *out, int *err, int s,
+                           cudaStream_t st);
 
 }  // namespace tjb

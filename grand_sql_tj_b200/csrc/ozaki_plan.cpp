@@ -125,7 +125,6 @@ struct Builder {
   // tau of psi cell c's columns: from its column split's job, or from a
   // maximum-only job when the cell is only stacked (one job per cell)
   std::vector<char> tau_job;
-  std::vector<std::pair<int64_t, int64_t>> pi_slots;   // (pi entry, slot), pi-relative entries
   void tau_of(int c) {
     if (tau_job[c]) return;
     tau_job[c] = 1;
@@ -167,9 +166,8 @@ struct Builder {
       const Cell &P = hp.cells1[p];
       const Tiling t = tiling(P.M, P.N, false);
       prodsplit[p] = alloc_dyn(t);
-      // pi comes from launch 1's partial maxima, not from a pass over P
       dyn_prod.push_back(job(SP_SCR, P.off, 1, P.ld, P.M, P.N, 1.0, prodsplit[p], t, 0, t.gsum, 0,
-                             hp.cell1_row_state[p], false));
+                             hp.cell1_row_state[p], true));
     }
     return prodsplit[p];
   }
@@ -244,11 +242,7 @@ struct Builder {
         for (size_t q = i; q < e; ++q) {
           const Run &r = runs[q];
           const Cell &X = hp.cells2[r.x];
-          OzStack st = r.st;
-          st.slot = oz.n_pslots;
-          oz.n_pslots += Mop;
-          for (int32_t i = 0; i < Mop; ++i) pi_slots.push_back({hp.cell1_row_state[r.p] + i, st.slot + i});
-          oz.stacks.push_back(st);
+          oz.stacks.push_back(r.st);
           // tau of X's columns comes from X's own maximum job (tau_of)
           dyn_psi.push_back(job(SP_PSI, X.off + (int64_t)8 * r.st.a_g0 * X.ld, X.ld, 1, r.st.ncols, K, 1.0, sk, ta,
                                 8 * off, r.st.a_ng, 0, hp.cell2_col_state[r.x] + 8 * r.st.a_g0, false));
@@ -487,29 +481,28 @@ struct Builder {
         else
           for (int f = it.fam_begin; f < it.fam_end; ++f) it.nkb += oz.fams[f].nkb;
       }
-    // pi lists: entries are pi-relative row states
-    oz.n_pi = hp.n_sys_states;
-    std::sort(pi_slots.begin(), pi_slots.end());
-    oz.pi_begin.assign(oz.n_pi + 1, 0);
-    oz.pi_list.clear();
-    oz.pi_list.reserve(pi_slots.size());
-    {
-      size_t k = 0;
-      for (int32_t e = 0; e < oz.n_pi; ++e) {
-        oz.pi_begin[e] = (int32_t)oz.pi_list.size();
-        while (k < pi_slots.size() && pi_slots[k].first == e) oz.pi_list.push_back(pi_slots[k++].second);
+    // maximum jobs and split jobs in lists of their own, so that no kernel
+    // walks over jobs it has nothing to do for
+    auto part = [](std::vector<OzJob> &all, std::vector<OzJob> &mx) {
+      mx.clear();
+      std::vector<OzJob> sp;
+      for (const OzJob &j : all) {
+        if (j.want_max) mx.push_back(j);
+        if (j.want_split) sp.push_back(j);
       }
-      oz.pi_begin[oz.n_pi] = (int32_t)oz.pi_list.size();
-      if (k != pi_slots.size()) throw std::runtime_error("product row outside the sys states");
-    }
+      all.swap(sp);
+    };
+    part(oz.sta_jobs, oz.sta_mjobs);
+    part(dyn_psi, oz.psi_mjobs);
+    part(dyn_prod, oz.prod_mjobs);
     oz.psi_jobs = std::move(dyn_psi);
     oz.prod_jobs = std::move(dyn_prod);
     make_spans(oz.sta_jobs, oz.sta_spans, false);
     make_spans(oz.psi_jobs, oz.psi_spans, false);
     make_spans(oz.prod_jobs, oz.prod_spans, false);
-    make_spans(oz.sta_jobs, oz.sta_mspans, true);
-    make_spans(oz.psi_jobs, oz.psi_mspans, true);
-    make_spans(oz.prod_jobs, oz.prod_mspans, true);
+    make_spans(oz.sta_mjobs, oz.sta_mspans, true);
+    make_spans(oz.psi_mjobs, oz.psi_mspans, true);
+    make_spans(oz.prod_mjobs, oz.prod_mspans, true);
     schedule(oz.items1, oz.cta1);
     schedule(oz.items2, oz.cta2);
     oz.mma_ops = 0;
@@ -538,8 +531,8 @@ struct Builder {
   // global units [b*T, (b+1)*T), starting inside job `job` at unit u0.
   // Split units cover gtot*8 rows x K/16; maximum units nrows x K/OZ_MAX_CHUNK.
   static int64_t job_units(const OzJob &j, bool max_units) {
-    if (max_units) return j.want_max ? (int64_t)j.nrows * cdiv(j.K, OZ_MAX_CHUNK) : 0;
-    return j.want_split ? (int64_t)j.gtot * 8 * (cdiv(j.K, 32) * 2) : 0;
+    if (max_units) return (int64_t)j.nrows * cdiv(j.K, OZ_MAX_CHUNK);
+    return (int64_t)j.gtot * 8 * (cdiv(j.K, 32) * 2);
   }
   static void make_spans(const std::vector<OzJob> &jobs, std::vector<OzSpan> &spans, bool max_units) {
     spans.clear();
@@ -661,12 +654,8 @@ extern "C" int tj_ozaki_plan_export(const tj_lattice *lat, const tj_model *sys, 
   put(out->items2, oz.items2, out->n_items2);
   put(out->cta1, oz.cta1, out->n_cta1);
   put(out->cta2, oz.cta2, out->n_cta2);
-  out->n_pslots = oz.n_pslots;
-  out->n_pi = oz.n_pi;
-  {
-    int64_t dummy = 0;
-    put(out->pi_begin, oz.pi_begin, dummy);
-  }
-  put(out->pi_list, oz.pi_list, out->n_pi_list);
+  put(out->sta_mjobs, oz.sta_mjobs, out->n_sta_mjobs);
+  put(out->psi_mjobs, oz.psi_mjobs, out->n_psi_mjobs);
+  put(out->prod_mjobs, oz.prod_mjobs, out->n_prod_mjobs);
   return TJ_OK;
 }

@@ -92,7 +92,7 @@ class OzFamC(C.Structure):
 
 
 class OzStackC(C.Structure):
-    _fields_ = [("dst_off", C.c_int64), ("rs_idx", C.c_int64), ("slot", C.c_int64)] + \
+    _fields_ = [("dst_off", C.c_int64), ("rs_idx", C.c_int64)] + \
                [(n, C.c_int32) for n in ("a_g0", "a_ng", "dst_ld", "ncols")]
 
 
@@ -117,8 +117,9 @@ class OzExport(C.Structure):
                 [("n_" + n, C.c_int64) for n, _ in _OZ_ARRAYS] +
                 [(n, C.POINTER(t)) for n, t in _OZ_ARRAYS] +
                 [("n_cta1", C.c_int64), ("n_cta2", C.c_int64), ("cta1", C.POINTER(C.c_int32)),
-                 ("cta2", C.POINTER(C.c_int32)), ("n_pslots", C.c_int64), ("n_pi", C.c_int64),
-                 ("n_pi_list", C.c_int64), ("pi_begin", C.POINTER(C.c_int32)), ("pi_list", C.POINTER(C.c_int64))])
+                 ("cta2", C.POINTER(C.c_int32)), ("n_sta_mjobs", C.c_int64), ("n_psi_mjobs", C.c_int64),
+                 ("n_prod_mjobs", C.c_int64), ("sta_mjobs", C.POINTER(OzJobC)), ("psi_mjobs", C.POINTER(OzJobC)),
+                 ("prod_mjobs", C.POINTER(OzJobC))])
 
 
 _lib = None
@@ -357,8 +358,8 @@ def ozaki_plan_export(sb, slices: int = 5, invec: Optional[Wave] = None) -> dict
     arrs = {n: (t * max(getattr(ex, "n_" + n), 1))() for n, t in _OZ_ARRAYS}
     arrs["cta1"] = (C.c_int32 * max(ex.n_cta1, 1))()
     arrs["cta2"] = (C.c_int32 * max(ex.n_cta2, 1))()
-    arrs["pi_begin"] = (C.c_int32 * max(ex.n_pi + 1, 1))()
-    arrs["pi_list"] = (C.c_int64 * max(ex.n_pi_list, 1))()
+    for n in ("sta_mjobs", "psi_mjobs", "prod_mjobs"):
+        arrs[n] = (OzJobC * max(getattr(ex, "n_" + n), 1))()
     for k, a in arrs.items():
         setattr(ex, k, C.cast(a, type(getattr(ex, k))))
     _chk(call(C.byref(ex)))

@@ -337,7 +337,7 @@ typedef struct tj_oz_job {
 typedef struct tj_oz_seg { int64_t a_base, b_base; int32_t a_nkb, b_nkb, a_kb0, b_kb0, nkb, pad_; } tj_oz_seg;
 typedef struct tj_oz_fam { int32_t seg_begin, seg_end; int64_t rs_idx, cs_idx; int32_t nkb, pad_; } tj_oz_fam;
 typedef struct tj_oz_stack {
-  int64_t dst_off, rs_idx, slot;
+  int64_t dst_off, rs_idx;
   int32_t a_g0, a_ng, dst_ld, ncols;
 } tj_oz_stack;
 typedef struct tj_oz_item {
@@ -360,12 +360,9 @@ typedef struct tj_ozaki_export {
   tj_oz_item *items1, *items2;
   int64_t n_cta1, n_cta2;     /* CTA b of launch k runs items [cta_k[b], cta_k[b+1]) */
   int32_t *cta1, *cta2;
-  /* pi entry e (row maximum of the products) = max of partial-maximum slots
-   * pi_list[pi_begin[e] .. pi_begin[e+1]); launch 1 writes slot stack.slot + i
-   * for row i of a stacked run's product */
-  int64_t n_pslots, n_pi, n_pi_list;
-  int32_t *pi_begin;
-  int64_t *pi_list;
+  /* the maximum jobs (row scales) of the three lists, run before their splits */
+  int64_t n_sta_mjobs, n_psi_mjobs, n_prod_mjobs;
+  tj_oz_job *sta_mjobs, *psi_mjobs, *prod_mjobs;
 } tj_ozaki_export;
 int tj_ozaki_plan_export(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
                          const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave, int slices,

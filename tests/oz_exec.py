@@ -35,7 +35,6 @@ class _Machine:
         self.out = np.full(max(ex.psi_len, 1), np.nan)
         self.pack = np.zeros(oe.sta_pack + oe.dyn_pack, dtype=np.int8)
         self.scales = np.zeros(oe.n_scales)
-        self.pslots = np.full(max(oe.n_pslots, 1), np.nan)
         self.spaces = {1: self.ops, 2: self.psi, 3: self.scr}
 
     def _matrix(self, j):
@@ -174,8 +173,6 @@ class _Machine:
                     assert key not in covered
                     covered.add(key)
                     self.scr[idx] = val
-                    # partial row maxima of this run's product rows col0 .. col0 + ncols
-                    self.pslots[sk.slot + it.col0 + np.arange(it.ncols)] = np.max(np.abs(val), axis=0)
                     r0 += sk.a_ng * 8
 
 
@@ -184,25 +181,18 @@ def execute_ozaki(plan, oz, psi):
     m = _Machine(plan, oz, psi)
     oe = m.oe
     # once per step
-    m.run_max(oz["sta_jobs"], oe.n_sta_jobs)
+    m.run_max(oz["sta_mjobs"], oe.n_sta_mjobs)
     m.run_split(oz["sta_jobs"], oe.n_sta_jobs)
     # per H*psi
     m.scales[oe.rho0:] = 0.0
-    m.run_max(oz["psi_jobs"], oe.n_psi_jobs)
+    m.run_max(oz["psi_mjobs"], oe.n_psi_mjobs)
     m.run_split(oz["psi_jobs"], oe.n_psi_jobs)
     for n_items, cta, n_cta in ((oe.n_items1, oz["cta1"], oe.n_cta1), (oe.n_items2, oz["cta2"], oe.n_cta2)):
         b = [cta[i] for i in range(n_cta)]
         assert b[0] == 0 and b[-1] == n_items and all(x <= y for x, y in zip(b, b[1:])) and len(b) <= 149
     cov1 = set()
     m.run_items(oz["items1"], oe.n_items1, cov1)
-    # pi from the partial maxima (every slot written by launch 1)
-    assert oe.n_pslots == 0 or np.all(np.isfinite(m.pslots))
-    pb = [oz["pi_begin"][e] for e in range(oe.n_pi + 1)]
-    pl = np.array([oz["pi_list"][k] for k in range(oe.n_pi_list)], dtype=np.int64)
-    for e in range(oe.n_pi):
-        if pb[e + 1] > pb[e]:
-            m.scales[oe.pi0 + e] = np.max(m.pslots[pl[pb[e]:pb[e + 1]]])
-    m.run_max(oz["prod_jobs"], oe.n_prod_jobs)
+    m.run_max(oz["prod_mjobs"], oe.n_prod_mjobs)
     m.run_split(oz["prod_jobs"], oe.n_prod_jobs)
     cov2 = set()
     m.run_items(oz["items2"], oe.n_items2, cov2)

@@ -57,3 +57,18 @@ def test_plan_items_cover_every_cell(name, product_lib, oracle_lib):
     got = execute_items(plan, sb.wave.data)
     assert np.all(np.isfinite(got))
     assert np.max(np.abs(got - ref)) <= 1e-13 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("name", ["tiny", "small", "small_gc", "cyl4"])
+def test_oracle_hpsi_is_symmetric(name, oracle_lib):
+    """<x, H y> = <H x, y>: the synthetic operators obey the reduced Hermiticity
+    rules, so every term's 6j weights and phases must pair up with those of
+    its transposed partner (a wrong phase or 6j argument breaks the symmetry)."""
+    from oracle import oracle
+    sb = synth.workload(name, seed=4)
+    rng = np.random.default_rng(0)
+    x = sb.wave.like(rng.standard_normal(sb.wave.dim))
+    y = sb.wave.like(rng.standard_normal(sb.wave.dim))
+    hx, hy = oracle.model_wave(sb, x).data, oracle.model_wave(sb, y).data
+    a, b = float(x.data @ hy), float(hx @ y.data)
+    assert abs(a - b) <= 1e-14 * np.linalg.norm(hx) * np.linalg.norm(y.data)
