@@ -280,6 +280,11 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
   __shared__ uint32_t tmem_sh;
   __shared__ volatile int abort_sh;
   __shared__ volatile int tfull_ok_sh;
+  // this CTA's first OZ_ICACHE items (and the segment of each product item),
+  // so that no role waits on a global load at an item boundary
+  constexpr int OZ_ICACHE = 64;
+  __shared__ OzItem item_sh[OZ_ICACHE];
+  __shared__ OzSeg seg1_sh[OZ_ICACHE];
   __shared__ double cscale_sh[BN];           // epilogue: column scales of the current family
   __shared__ int32_t stk_start[17];          // epilogue: first tile row of each stacked run
   __shared__ int64_t stk_dst[16], stk_rs[16];
@@ -299,6 +304,12 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     abort_sh = 0;
   }
+  const int ib = p.cta[blockIdx.x], ie_cta = p.cta[blockIdx.x + 1];
+  for (int i = tid; i < min(ie_cta - ib, OZ_ICACHE); i += blockDim.x) {
+    item_sh[i] = p.items[ib + i];
+    if (item_sh[i].kind == 1) seg1_sh[i] = p.segs[item_sh[i].seg];
+  }
+  auto get_item = [&](int ii) -> OzItem { return ii - ib < OZ_ICACHE ? item_sh[ii - ib] : p.items[ii]; };
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(oz_smem(&tmem_sh)),
                  "r"(512));
@@ -336,7 +347,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       return good != 0;
     };
     for (int ii = p.cta[blockIdx.x], ie = p.cta[blockIdx.x + 1]; ii < ie && ok; ++ii) {
-      const OzItem it = p.items[ii];
+      const OzItem it = get_item(ii);
       // tiles of this item: A row tile ta (ga groups), B column tile tb (gb groups)
       const uint32_t ga = (uint32_t)((it.mrows + 7) >> 3), gb = (uint32_t)(it.N >> 3);
       const int64_t ta = it.row0 / 128, tb = it.col0 / BN;
@@ -361,7 +372,10 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
         for (int s0 = sb; s0 < se && ok; s0 += 32) {
           // the next <= 32 segments, one per lane
           OzSeg mine;
-          if (s0 + lane < se) mine = p.segs[s0 + lane];
+          if (it.kind == 1 && ii - ib < OZ_ICACHE)
+            mine = seg1_sh[ii - ib];
+          else if (s0 + lane < se)
+            mine = p.segs[s0 + lane];
           const int cnt = min(32, se - s0);
           for (int j = 0; j < cnt && ok; ++j) {
             const int64_t a_base = __shfl_sync(0xffffffffu, mine.a_base, j);
@@ -403,7 +417,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       bool ok = true, issued = false;
       const uint64_t dbase = oz_desc(0u, 128u, 256u);   // start address added per stage
       for (int ii = p.cta[blockIdx.x], ie = p.cta[blockIdx.x + 1]; ii < ie && ok; ++ii) {
-        const OzItem it = p.items[ii];
+        const OzItem it = get_item(ii);
         // MMA pa multiplies A slice pa with B slices 1..S+1-pa (N' = (S+1-pa) N):
         // its column block q lands on the accumulator of diagonal pa+q at column (pa+q-2) N
         uint32_t idesc[S];
@@ -473,7 +487,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
     }
     bool ok = true;
     for (int ii = p.cta[blockIdx.x], ie = p.cta[blockIdx.x + 1]; ii < ie && ok; ++ii) {
-      const OzItem it = p.items[ii];
+      const OzItem it = get_item(ii);
       // warp w reads TMEM lane quarter q = w % 4 (lanes 32q..32q+31) and
       // column half h = w / 4 of the tile; the tile row it holds:
       //   M = 128: row = 32q + lane; M = 64: rows 16q..16q+15 in lanes 32q..32q+15

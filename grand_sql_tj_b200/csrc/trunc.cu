@@ -118,9 +118,10 @@ __global__ void __launch_bounds__(JAC_THREADS) jacobi_kernel(double *Aall, doubl
         vq[k] = sv * vx + c * vy;
       }
       __syncthreads();
-      // A <- J^T A (rows p, q)
+      // A <- J^T A (rows p, q): consecutive threads take consecutive pairs of
+      // the same column, so a warp stays inside one column (8n bytes)
       for (int64_t idx = tid; idx < (int64_t)half * n; idx += blockDim.x) {
-        const int i = (int)(idx / n), k = (int)(idx % n);
+        const int i = (int)(idx % half), k = (int)(idx / half);
         const int q = qq[i];
         if (q < 0 || sn[i] == 0.0) continue;
         const int p = pp[i];
