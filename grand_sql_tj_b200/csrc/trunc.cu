@@ -7,10 +7,16 @@
 // degeneracy 2S+1 for the entropies, sorts it, keeps kept_min..kept_max
 // states by the discarded-weight rule and returns the kept eigenvectors.
 //
-// Here rho is one more grouped-GEMM pass (one cell per sector), the
-// eigen-decomposition is a batched two-sided cyclic Jacobi (one CTA per
-// sector, round-robin parallel ordering, FP64), and the selection -- a sort
-// of at most a few 10^4 eigenvalues -- runs on the host in FP64.
+// Here rho is one more grouped-GEMM pass (one cell per sector).  The
+// eigen-decomposition follows the direct route of DSYEV's first stage and
+// replaces its second: every sector is reduced to tridiagonal form by
+// Householder reflections (one CTA per sector), all eigenvalues come from
+// Sturm-count multisection (one thread per eigenvalue), the host selects the
+// kept states exactly as den_mat.f90 does, and only the kept eigenvectors
+// are computed: inverse iteration on the tridiagonal matrix (one thread per
+// vector), Gram-Schmidt orthonormalisation inside each kept block, and the
+// back-transformation by the stored reflectors, written straight into the
+// truncation operator's layout.  Everything is FP64.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -24,130 +30,400 @@
 
 namespace tjb {
 
-constexpr int JAC_THREADS = 1024;
-constexpr int JAC_MAX_N = 4096;
+constexpr int EIG_THREADS = 1024;
+constexpr int EIG_MAX_N = 4096;
+constexpr double EIG_EPS = 2.220446049250313e-16;        // 2^-52
+constexpr double EIG_SAFMIN = 2.2250738585072014e-308;   // smallest normal FP64
+constexpr int ORTH_THREADS = 512;
 
-// Two-sided cyclic Jacobi on the symmetric matrix A (n x n, column-major).
-// Each round applies n/2 disjoint plane rotations chosen by the circle
-// method, so every pair (p, q) is visited once per sweep; a sweep that
-// rotates nothing ends it.  On return the diagonal of A holds the eigenvalues
-// and V the eigenvectors.  status[s] = 1 if max_sweeps were not enough.
-__global__ void __launch_bounds__(JAC_THREADS) jacobi_kernel(double *Aall, double *Vall, const int64_t *off,
-                                                            const int *dims, double *evals, const int64_t *eoff,
-                                                            int max_sweeps, int *status) {
-  extern __shared__ unsigned char sm_raw[];
-  const int s = blockIdx.x, n = dims[s], tid = threadIdx.x;
-  double *A = Aall + off[s], *V = Vall + off[s];
-  const int m = n + (n & 1), half = m / 2;
-  double *cs = (double *)sm_raw, *sn = cs + half;
-  int *pp = (int *)(sn + half), *qq = pp + half;
-  __shared__ int rotated;
-  __shared__ double dmax_sh[JAC_THREADS / 32];
-  for (int64_t i = tid; i < (int64_t)n * n; i += blockDim.x) V[i] = (i % (n + 1) == 0) ? 1.0 : 0.0;
-  // sum of |diagonal| entries (the trace of a density matrix, a bound on its
-  // norm): off-diagonal entries below 8 eps of it are at the rounding level of
-  // the rotations themselves and are left alone (density matrices of
-  // truncated states have many exactly-zero eigenvalues, whose block would
-  // otherwise keep rotating on rounding noise)
-  double dm = 0.0;
-  for (int i = tid; i < n; i += blockDim.x) dm += fabs(A[(int64_t)i * n + i]);
-  for (int k = 16; k > 0; k >>= 1) dm += __shfl_xor_sync(0xffffffffu, dm, k);
-  if ((tid & 31) == 0) dmax_sh[tid >> 5] = dm;
+// Sum of one value per thread over the block, in a fixed order; every thread
+// receives it.  red holds 32 doubles of shared memory.
+__device__ __forceinline__ double block_sum(double x, double *red) {
+  for (int k = 16; k > 0; k >>= 1) x += __shfl_xor_sync(0xffffffffu, x, k);
   __syncthreads();
-  double dsum = 0.0;
-  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) dsum += dmax_sh[w];
-  const double floor_abs = fmax(8.0 * 2.220446049250313e-16 * dsum, 1e-300);
-  int sweep = 0;
-  bool converged = n <= 1;
-  for (; sweep < max_sweeps && !converged; ++sweep) {
-    // a sweep that needs no rotation ends the iteration: every off-diagonal
-    // entry is below the FP64 rounding level of its diagonal pair,
-    // |a_pq| <= 2^-53 sqrt(|a_pp a_qq|) (the classical relative threshold),
-    // or below the absolute floor above
-    if (tid == 0) rotated = 0;
-    __syncthreads();
-    for (int r = 0; r < m - 1; ++r) {
-      for (int i = tid; i < half; i += blockDim.x) {
-        int p, q;
-        if (i == 0) {
-          p = m - 1;
-          q = r;
-        } else {
-          p = (r + i) % (m - 1);
-          q = (r - i + (m - 1)) % (m - 1);
-        }
-        if (p > q) {
-          const int t = p;
-          p = q;
-          q = t;
-        }
-        double c = 1.0, sv = 0.0;
-        if (q < n) {
-          const double apq = A[(int64_t)q * n + p];
-          const double app = A[(int64_t)p * n + p], aqq = A[(int64_t)q * n + q];
-          if (fabs(apq) > floor_abs && fabs(apq) > 1.1102230246251565e-16 * sqrt(fabs(app * aqq))) {
-            const double tau = (aqq - app) / (2.0 * apq);
-            const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-            c = 1.0 / sqrt(1.0 + t * t);
-            sv = t * c;
-            rotated = 1;
-          }
-        } else {
-          q = -1;   // pair with the padding index: no rotation
-        }
-        pp[i] = p;
-        qq[i] = q;
-        cs[i] = c;
-        sn[i] = sv;
-      }
-      __syncthreads();
-      // A <- A J (columns p, q) and V <- V J
-      for (int64_t idx = tid; idx < (int64_t)half * n; idx += blockDim.x) {
-        const int i = (int)(idx / n), k = (int)(idx % n);
-        const int q = qq[i];
-        if (q < 0 || sn[i] == 0.0) continue;
-        const int p = pp[i];
-        const double c = cs[i], sv = sn[i];
-        double *ap = A + (int64_t)p * n, *aq = A + (int64_t)q * n;
-        const double x = ap[k], y = aq[k];
-        ap[k] = c * x - sv * y;
-        aq[k] = sv * x + c * y;
-        double *vp = V + (int64_t)p * n, *vq = V + (int64_t)q * n;
-        const double vx = vp[k], vy = vq[k];
-        vp[k] = c * vx - sv * vy;
-        vq[k] = sv * vx + c * vy;
-      }
-      __syncthreads();
-      // A <- J^T A (rows p, q): consecutive threads take consecutive pairs of
-      // the same column, so a warp stays inside one column (8n bytes)
-      for (int64_t idx = tid; idx < (int64_t)half * n; idx += blockDim.x) {
-        const int i = (int)(idx % half), k = (int)(idx / half);
-        const int q = qq[i];
-        if (q < 0 || sn[i] == 0.0) continue;
-        const int p = pp[i];
-        const double c = cs[i], sv = sn[i];
-        double *col = A + (int64_t)k * n;
-        const double x = col[p], y = col[q];
-        col[p] = c * x - sv * y;
-        col[q] = sv * x + c * y;
-      }
-      __syncthreads();
-    }
-    converged = rotated == 0;
-    __syncthreads();
-  }
-  if (tid == 0) status[s] = converged ? 0 : 1;
-  for (int i = tid; i < n; i += blockDim.x) evals[eoff[s] + i] = A[(int64_t)i * n + i];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
+  __syncthreads();
+  double s = 0.0;
+  const int nw = blockDim.x >> 5;
+  for (int w = 0; w < nw; ++w) s += red[w];
+  return s;
 }
 
-// out[j] gathers column src_col[j] (length rows[j]) of the matrix at src_off[j].
-__global__ void gather_cols_kernel(const double *V, const int64_t *src_off, const int *rows, const int64_t *dst_off,
-                                   double *out, int ncols) {
-  const int j = blockIdx.x;
-  if (j >= ncols) return;
-  const double *s = V + src_off[j];
-  double *d = out + dst_off[j];
-  for (int i = threadIdx.x; i < rows[j]; i += blockDim.x) d[i] = s[i];
+// Householder reduction of one symmetric sector matrix A (n x n,
+// column-major, both triangles) to tridiagonal form T = Q^T A Q with
+// Q = H_0 H_1 ... H_{n-2}, H_k = I - tau_k v_k v_k^T acting on the indices
+// k+1..n-1 and v_k(k+1) = 1 (the lower-triangle scheme of LAPACK's dsytd2).
+// v_k overwrites A(k+1:n, k); d and e receive the diagonal and the
+// off-diagonal of T, info[4s..4s+3] its Gershgorin interval, max row sum and
+// the Sturm-count pivot floor.  The rank-2 update of step k,
+// A <- A - v w^T - w v^T, is applied lazily inside the matrix-vector product
+// p = A v of step k+1, so each step reads and writes the trailing block once.
+// One CTA per sector; order[] lists the sectors largest first.
+__global__ void __launch_bounds__(EIG_THREADS) tridiag_kernel(double *Aall, const int64_t *off, const int *dims,
+                                                             const int64_t *eoff, const int *order, double *dall,
+                                                             double *eall, double *tauall, double *info) {
+  extern __shared__ double sm[];
+  __shared__ double red[32];
+  __shared__ double sh_tau, sh_scl;
+  const int s = order[blockIdx.x], n = dims[s], tid = threadIdx.x, nt = blockDim.x;
+  double *A = Aall + off[s];
+  double *d = dall + eoff[s], *e = eall + eoff[s], *tau = tauall + eoff[s];
+  double *vp = sm, *wp = vp + n, *v = wp + n, *part = v + n;   // part: max(n, nt) entries
+  if (n == 0) return;
+  bool pending = false;
+  for (int k = 0; k + 1 < n; ++k) {
+    const int k1 = k + 1, m = n - k1;
+    double *colk = A + (int64_t)k * n;
+    // column k (rows k..n-1) with the pending update applied
+    double ss = 0.0;
+    for (int i = k + tid; i < n; i += nt) {
+      double a = colk[i];
+      if (pending) a -= vp[i] * wp[k] + wp[i] * vp[k];
+      v[i] = a;
+      if (i > k1) ss += a * a;
+    }
+    const double sigma2 = block_sum(ss, red);
+    if (tid == 0) {
+      d[k] = v[k];
+      const double alpha = v[k1];
+      double beta = alpha, t = 0.0, scl = 0.0;
+      if (sigma2 > 0.0) {
+        const double nr = sqrt(alpha * alpha + sigma2);
+        beta = alpha >= 0.0 ? -nr : nr;
+        t = (beta - alpha) / beta;
+        scl = 1.0 / (alpha - beta);
+      }
+      e[k] = beta;
+      tau[k] = t;
+      sh_tau = t;
+      sh_scl = scl;
+    }
+    __syncthreads();
+    const double t = sh_tau, scl = sh_scl;
+    for (int i = k1 + tid; i < n; i += nt) {
+      const double x = i == k1 ? 1.0 : v[i] * scl;
+      v[i] = x;
+      colk[i] = x;
+    }
+    __syncthreads();
+    // trailing block: apply the pending rank-2 update, p = A v
+    const int R = min((m + 31) & ~31, nt), G = nt / R;
+    const int g = tid / R, r = tid - g * R;
+    if (g < G) {
+      for (int ii = r; ii < m; ii += R) {
+        const int i = k1 + ii;
+        const double vpi = pending ? vp[i] : 0.0, wpi = pending ? wp[i] : 0.0;
+        double acc = 0.0;
+        double *a = A + (int64_t)(k1 + g) * n + i;
+        if (pending) {
+#pragma unroll 4
+          for (int jj = g; jj < m; jj += G, a += (int64_t)G * n) {
+            const int j = k1 + jj;
+            const double x = *a - (vpi * wp[j] + wpi * vp[j]);
+            *a = x;
+            acc += x * v[j];
+          }
+        } else {
+#pragma unroll 4
+          for (int jj = g; jj < m; jj += G, a += (int64_t)G * n) acc += *a * v[k1 + jj];
+        }
+        part[g * m + ii] = acc;
+      }
+    }
+    __syncthreads();
+    // p = tau A v, w = p - (tau/2)(p.v) v
+    double pv = 0.0;
+    for (int ii = tid; ii < m; ii += nt) {
+      double p = 0.0;
+      for (int q = 0; q < G; ++q) p += part[q * m + ii];
+      p *= t;
+      part[ii] = p;   // own entry only: q = 0 slot of the same ii
+      pv += p * v[k1 + ii];
+    }
+    const double K = 0.5 * t * block_sum(pv, red);
+    for (int ii = tid; ii < m; ii += nt) {
+      const int i = k1 + ii;
+      wp[i] = part[ii] - K * v[i];
+      vp[i] = v[i];
+    }
+    pending = true;
+    __syncthreads();
+  }
+  if (tid == 0) {
+    d[n - 1] = A[(int64_t)(n - 1) * n + (n - 1)];
+    if (n >= 1) tau[n - 1] = 0.0;
+    double gl = 1e308, gu = -1e308, emax2 = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double el = i > 0 ? fabs(e[i - 1]) : 0.0, er = i + 1 < n ? fabs(e[i]) : 0.0;
+      gl = fmin(gl, d[i] - el - er);
+      gu = fmax(gu, d[i] + el + er);
+      if (i + 1 < n) emax2 = fmax(emax2, e[i] * e[i]);
+    }
+    info[4 * s + 0] = gl;
+    info[4 * s + 1] = gu;
+    info[4 * s + 2] = fmax(fabs(gl), fabs(gu));
+    info[4 * s + 3] = EIG_SAFMIN * fmax(1.0, emax2);
+  }
+}
+
+// Number of eigenvalues of T below x0, x1, x2 (three Sturm sequences of the
+// LDL^T pivots of T - x I run side by side; pivots below pivmin in size are
+// replaced by -pivmin, as LAPACK's dstebz does).
+__device__ __forceinline__ void sturm3(const double *d, const double *e, int n, double pivmin, double x0, double x1,
+                                       double x2, int &c0, int &c1, int &c2) {
+  double q0 = d[0] - x0, q1 = d[0] - x1, q2 = d[0] - x2;
+  if (fabs(q0) < pivmin) q0 = -pivmin;
+  if (fabs(q1) < pivmin) q1 = -pivmin;
+  if (fabs(q2) < pivmin) q2 = -pivmin;
+  c0 = q0 < 0.0;
+  c1 = q1 < 0.0;
+  c2 = q2 < 0.0;
+  for (int i = 1; i < n; ++i) {
+    const double di = d[i], ee = e[i - 1] * e[i - 1];
+    q0 = (di - x0) - ee / q0;
+    q1 = (di - x1) - ee / q1;
+    q2 = (di - x2) - ee / q2;
+    if (fabs(q0) < pivmin) q0 = -pivmin;
+    if (fabs(q1) < pivmin) q1 = -pivmin;
+    if (fabs(q2) < pivmin) q2 = -pivmin;
+    c0 += q0 < 0.0;
+    c1 += q1 < 0.0;
+    c2 += q2 < 0.0;
+  }
+}
+
+// Eigenvalue k (ascending) of every sector, one thread each: the interval
+// [lo, hi) with count(lo) <= k < count(hi) starts at the Gershgorin bounds
+// and is cut into four per pass until it is below 2 eps max(|lo|, |hi|) or
+// eps ||T|| (the absolute accuracy of any backward-stable solver).
+__global__ void bisect_kernel(const double *dall, const double *eall, const int64_t *eoff, const int *dims,
+                              const double *info, const int *esec, int etot, double *evals) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= etot) return;
+  const int s = esec[idx], n = dims[s];
+  const int k = (int)(idx - eoff[s]);
+  const double *d = dall + eoff[s], *e = eall + eoff[s];
+  const double tnorm = info[4 * s + 2], pivmin = info[4 * s + 3];
+  const double pad = 2.0 * EIG_EPS * tnorm + 2.0 * pivmin;
+  double lo = info[4 * s + 0] - pad, hi = info[4 * s + 1] + pad;
+  for (int it = 0; it < 80; ++it) {
+    const double tol = fmax(fmax(2.0 * EIG_EPS * fmax(fabs(lo), fabs(hi)), EIG_EPS * tnorm), pivmin);
+    if (hi - lo <= tol) break;
+    const double h = 0.25 * (hi - lo);
+    const double x0 = lo + h, x1 = lo + 2.0 * h, x2 = hi - h;
+    int c0, c1, c2;
+    sturm3(d, e, n, pivmin, x0, x1, x2, c0, c1, c2);
+    if (c0 > k) {
+      hi = x0;
+    } else if (c1 > k) {
+      lo = x0;
+      hi = x1;
+    } else if (c2 > k) {
+      lo = x1;
+      hi = x2;
+    } else {
+      lo = x2;
+    }
+  }
+  evals[idx] = 0.5 * (lo + hi);
+}
+
+// Pseudo-random start vector entry in [-1, 1) (splitmix64 of the indices).
+__device__ __forceinline__ double start_entry(int s, int k, int i) {
+  uint64_t z = ((uint64_t)(uint32_t)s << 40) ^ ((uint64_t)(uint32_t)k << 20) ^ (uint64_t)(uint32_t)i;
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  z ^= z >> 31;
+  return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+// Eigenvector of T (sector job_sec[j]) for its eigenvalue job_k[j] by
+// inverse iteration, one thread per vector: LU factorisation of T - lam I
+// with partial pivoting (pivots below eps ||T|| raised to it, so that the
+// nearly singular factor stays finite), three solves from a fixed
+// pseudo-random start, each result rescaled.  The per-thread factors live in
+// work[] with element i of job j at i * njobs + j (coalesced across a warp);
+// the unit vector goes to Y[j * ldy + i].  status bit 0: a non-finite value.
+__global__ void inverse_iter_kernel(const double *dall, const double *eall, const int64_t *eoff, const int *dims,
+                                    const double *info, const double *evals, const int *job_sec, const int *job_k,
+                                    int njobs, int nmax, double *work, unsigned char *piv, double *Y, int ldy,
+                                    int *status) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= njobs) return;
+  const int s = job_sec[j], k = job_k[j], n = dims[s];
+  const double *d = dall + eoff[s], *e = eall + eoff[s];
+  const double lam = evals[eoff[s] + k];
+  const double pert = fmax(EIG_EPS * info[4 * s + 2], 1e-290);
+  const size_t st = (size_t)njobs, pl = (size_t)nmax * st;
+  double *U = work, *DU = work + pl, *DU2 = work + 2 * pl, *DL = work + 3 * pl, *X = work + 4 * pl;
+#define AT(arr, i) arr[(size_t)(i) * st + j]
+  // LU = P (T - lam I): row i of U is (U_i, DU_i, DU2_i) at columns i, i+1, i+2
+  double di = d[0] - lam, dui = n > 1 ? e[0] : 0.0;
+  for (int i = 0; i + 1 < n; ++i) {
+    const double sub = e[i];
+    double dn = d[i + 1] - lam, dun = i + 2 < n ? e[i + 1] : 0.0;
+    if (fabs(di) >= fabs(sub) || fabs(sub) < pert) {
+      const double u = fabs(di) < pert ? copysign(pert, di) : di;
+      const double l = sub / u;
+      AT(U, i) = u;
+      AT(DU, i) = dui;
+      AT(DU2, i) = 0.0;
+      AT(DL, i) = l;
+      piv[(size_t)i * st + j] = 0;
+      dn -= l * dui;
+    } else {   // rows i and i+1 exchanged
+      const double l = di / sub;
+      AT(U, i) = sub;
+      AT(DU, i) = dn;
+      AT(DU2, i) = dun;
+      AT(DL, i) = l;
+      piv[(size_t)i * st + j] = 1;
+      dn = dui - l * dn;
+      dun = -l * dun;
+    }
+    di = dn;
+    dui = dun;
+  }
+  AT(U, n - 1) = fabs(di) < pert ? copysign(pert, di) : di;
+  for (int i = 0; i < n; ++i) AT(X, i) = start_entry(s, k, i);
+  bool bad = false;
+  for (int sweep = 0; sweep < 3; ++sweep) {
+    // forward: P and L
+    for (int i = 0; i + 1 < n; ++i) {
+      const double l = AT(DL, i);
+      if (piv[(size_t)i * st + j]) {
+        const double t = AT(X, i);
+        const double xi = AT(X, i + 1);
+        AT(X, i) = xi;
+        AT(X, i + 1) = t - l * xi;
+      } else {
+        AT(X, i + 1) -= l * AT(X, i);
+      }
+    }
+    // backward: U, with a rescale of the whole vector if it nears overflow
+    double x1 = 0.0, x2 = 0.0;   // x_{i+1}, x_{i+2}
+    for (int i = n - 1; i >= 0; --i) {
+      double xi = (AT(X, i) - AT(DU, i) * x1 - AT(DU2, i) * x2) / AT(U, i);
+      if (fabs(xi) > 1e250) {
+        const double f = 1e-250;
+        for (int q = 0; q < n; ++q) AT(X, q) *= f;
+        xi *= f;
+        x1 *= f;
+        x2 *= f;
+      }
+      AT(X, i) = xi;
+      x2 = x1;
+      x1 = xi;
+    }
+    double mx = 0.0;
+    for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(AT(X, i)));
+    if (!(mx > 0.0) || !isfinite(mx)) {
+      bad = true;
+      break;
+    }
+    const double inv = 1.0 / mx;
+    for (int i = 0; i < n; ++i) AT(X, i) *= inv;
+  }
+  double nrm = 0.0;
+  for (int i = 0; i < n; ++i) nrm += AT(X, i) * AT(X, i);
+  if (bad || !(nrm > 0.0) || !isfinite(nrm)) {
+    atomicOr(status, 1);
+    nrm = 1.0;
+  }
+  const double inv = 1.0 / sqrt(nrm);
+  double *y = Y + (size_t)j * ldy;
+  for (int i = 0; i < n; ++i) y[i] = AT(X, i) * inv;
+  for (int i = n; i < nmax; ++i) y[i] = 0.0;
+#undef AT
+}
+
+// One kept block (grp = {sector, first job, count}): classical Gram-Schmidt
+// applied twice to its vectors in descending eigenvalue order, so that the
+// dominant states are the least changed; inverse iteration leaves vectors of
+// close eigenvalues only approximately orthogonal (to about eps ||T|| / gap).
+// status bit 1: a vector lost more than 0.999 of its norm to the projection.
+__global__ void __launch_bounds__(ORTH_THREADS) orthonormalize_kernel(const int *grp, const int *dims, double *Y,
+                                                                      int ldy, int *status) {
+  extern __shared__ double h[];
+  __shared__ double red[32];
+  const int s = grp[4 * blockIdx.x], j0 = grp[4 * blockIdx.x + 1], cnt = grp[4 * blockIdx.x + 2];
+  const int n = dims[s], tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  for (int t = 1; t < cnt; ++t) {
+    double *y = Y + (size_t)(j0 + cnt - 1 - t) * ldy;
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int q = warp; q < t; q += nw) {
+        const double *z = Y + (size_t)(j0 + cnt - 1 - q) * ldy;
+        double acc = 0.0;
+        for (int i = lane; i < n; i += 32) acc += z[i] * y[i];
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) h[q] = acc;
+      }
+      __syncthreads();
+      double ss = 0.0;
+      for (int i = tid; i < n; i += blockDim.x) {
+        double acc = y[i];
+        for (int q = 0; q < t; ++q) acc -= h[q] * Y[(size_t)(j0 + cnt - 1 - q) * ldy + i];
+        y[i] = acc;
+        ss += acc * acc;
+      }
+      const double nrm = sqrt(block_sum(ss, red));
+      if (pass == 0 && nrm < 1e-3 && tid == 0) atomicOr(status, 2);
+      const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+      for (int i = tid; i < n; i += blockDim.x) y[i] *= inv;
+      __syncthreads();
+    }
+  }
+}
+
+// Back-transformation of the kept vectors, one warp per vector and the
+// vector in shared memory: y <- H_0 (H_1 (... H_{n-2} y)), reflector k read
+// from A(k+1:n, k) of its sector.  The sign is fixed so that the entry of
+// largest magnitude (the first of equal ones) is positive, and the column is
+// written to the truncation operator at job_dst[j].  slab[2b], slab[2b+1]:
+// the block (grp index) and its first column handled by CTA b.
+__global__ void backtransform_kernel(const double *Aall, const int64_t *off, const double *tauall,
+                                     const int64_t *eoff, const int *dims, const int *grp, const int *slab,
+                                     const double *Y, int ldy, const int64_t *job_dst, double *out) {
+  extern __shared__ double colsm[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = slab[2 * blockIdx.x], c = slab[2 * blockIdx.x + 1] + warp;
+  const int s = grp[4 * g], j0 = grp[4 * g + 1], cnt = grp[4 * g + 2];
+  if (c >= cnt) return;
+  const int n = dims[s], j = j0 + c;
+  const double *A = Aall + off[s], *tau = tauall + eoff[s];
+  double *col = colsm + (size_t)warp * ldy;
+  for (int i = lane; i < n; i += 32) col[i] = Y[(size_t)j * ldy + i];
+  __syncwarp();
+  for (int k = n - 2; k >= 0; --k) {
+    const double t = tau[k];
+    if (t == 0.0) continue;
+    const double *v = A + (int64_t)k * n;
+    double acc = 0.0;
+    for (int i = k + 1 + lane; i < n; i += 32) acc += v[i] * col[i];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    const double f = t * acc;
+    for (int i = k + 1 + lane; i < n; i += 32) col[i] -= f * v[i];
+    __syncwarp();
+  }
+  double best = -1.0;
+  int bi = 0;
+  for (int i = lane; i < n; i += 32)
+    if (fabs(col[i]) > best) {
+      best = fabs(col[i]);
+      bi = i;
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ob > best || (ob == best && oi < bi)) {
+      best = ob;
+      bi = oi;
+    }
+  }
+  const double sg = col[bi] < 0.0 ? -1.0 : 1.0;
+  double *dst = out + job_dst[j];
+  for (int i = lane; i < n; i += 32) dst[i] = sg * col[i];
 }
 
 }  // namespace tjb
@@ -185,6 +461,8 @@ uint64_t hash_data(const double *p, int64_t n) {
   return h;
 }
 
+size_t al256(size_t x) { return (x + 255) / 256 * 256; }
+
 }  // namespace
 
 extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kept_min, int kept_max,
@@ -199,7 +477,7 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     if (w.sys_dim < 0 || w.env_dim < 0 || w.off < 0 || w.off + (int64_t)w.sys_dim * w.env_dim > D)
       return set_err(TJ_ERR_ARG, "tj_truncation: bad sector table");
     const int n = side == 0 ? w.sys_dim : w.env_dim;
-    if (n > JAC_MAX_N) return set_err(TJ_ERR_LIMIT, "tj_truncation: a density-matrix sector exceeds 4096 states");
+    if (n > EIG_MAX_N) return set_err(TJ_ERR_LIMIT, "tj_truncation: a density-matrix sector exceeds 4096 states");
   }
   const uint64_t h = hash_data(wave->data, D);
   TruncCache &tc = g_tc;
@@ -221,7 +499,7 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     std::vector<Task> tasks;
     std::vector<Tile> tiles;
     std::vector<int64_t> roff(nsec), eoff(nsec);
-    std::vector<int> dims(nsec);
+    std::vector<int> dims(nsec), esec;
     int64_t rlen = 0, etot = 0;
     for (int i = 0; i < nsec; ++i) {
       const tj_wave_sub &w = wave->sub[i];
@@ -231,6 +509,7 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       eoff[i] = etot;
       rlen += ((int64_t)n * n + 31) / 32 * 32;
       etot += n;
+      esec.insert(esec.end(), n, i);
       Cell c;
       std::memset(&c, 0, sizeof c);
       c.off = roff[i];
@@ -256,21 +535,28 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       for (int r0 = 0; r0 < n; r0 += BM)
         for (int c0 = 0; c0 < n; c0 += BN) tiles.push_back(Tile{ci, r0, c0, c.t_begin, c.t_end, c.t_end, c.t_end, -1});
     }
-    if ((rc = ctx->trB.reserve(sizeof(double) * (rlen + 4))) || (rc = ctx->trC.reserve(sizeof(double) * (rlen + 4))) ||
-        (rc = ctx->trD.reserve(sizeof(double) * (etot + 4))))
+    const int maxn = std::max(1, *std::max_element(dims.begin(), dims.end()));
+    // sectors largest first for the one-CTA-per-sector reduction
+    std::vector<int> order(nsec);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return dims[a] > dims[b]; });
+    // trD: d, e, tau, eigenvalues (etot each), then 4 per sector
+    if ((rc = ctx->trB.reserve(sizeof(double) * (rlen + 4))) ||
+        (rc = ctx->trD.reserve(sizeof(double) * (4 * etot + 4 * nsec + 8))))
       return rc;
+    double *dd = ctx->trD.d(), *de = dd + etot, *dtau = de + etot, *dev = dtau + etot, *dinfo = dev + etot;
     // small tables packed into one buffer
     const size_t tb = cells.size() * sizeof(Cell), kb = tasks.size() * sizeof(Task), lb = tiles.size() * sizeof(Tile);
     const size_t ob = nsec * sizeof(int64_t), db = nsec * sizeof(int);
     size_t pos = 0;
-    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-    const size_t p_cells = pos; pos += al(tb);
-    const size_t p_tasks = pos; pos += al(kb);
-    const size_t p_tiles = pos; pos += al(lb);
-    const size_t p_roff = pos; pos += al(ob);
-    const size_t p_eoff = pos; pos += al(ob);
-    const size_t p_dims = pos; pos += al(db);
-    const size_t p_stat = pos; pos += al(db);
+    const size_t p_cells = pos; pos += al256(tb);
+    const size_t p_tasks = pos; pos += al256(kb);
+    const size_t p_tiles = pos; pos += al256(lb);
+    const size_t p_roff = pos; pos += al256(ob);
+    const size_t p_eoff = pos; pos += al256(ob);
+    const size_t p_dims = pos; pos += al256(db);
+    const size_t p_order = pos; pos += al256(db);
+    const size_t p_esec = pos; pos += al256(sizeof(int) * (size_t)std::max<int64_t>(etot, 1));
     const size_t p_cnt = pos; pos += 256;
     if ((rc = ctx->trE.reserve(pos))) return rc;
     char *tbase = (char *)ctx->trE.p;
@@ -280,7 +566,12 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     CKT(cudaMemcpyAsync(tbase + p_roff, roff.data(), ob, cudaMemcpyHostToDevice, st));
     CKT(cudaMemcpyAsync(tbase + p_eoff, eoff.data(), ob, cudaMemcpyHostToDevice, st));
     CKT(cudaMemcpyAsync(tbase + p_dims, dims.data(), db, cudaMemcpyHostToDevice, st));
-    CKT(cudaMemsetAsync(tbase + p_cnt, 0, 16, st));
+    CKT(cudaMemcpyAsync(tbase + p_order, order.data(), db, cudaMemcpyHostToDevice, st));
+    if (etot) CKT(cudaMemcpyAsync(tbase + p_esec, esec.data(), sizeof(int) * etot, cudaMemcpyHostToDevice, st));
+    CKT(cudaMemsetAsync(tbase + p_cnt, 0, 32, st));
+    const int64_t *d_roff = (const int64_t *)(tbase + p_roff), *d_eoff = (const int64_t *)(tbase + p_eoff);
+    const int *d_dims = (const int *)(tbase + p_dims);
+    int *d_status = (int *)(tbase + p_cnt + 16);
     GemmParams g;
     std::memset(&g, 0, sizeof g);
     g.psi = psi;
@@ -293,20 +584,20 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     g.counter = (unsigned int *)(tbase + p_cnt);
     launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles), st);
     CKT(cudaGetLastError());
-    // batched Jacobi
-    int maxn = *std::max_element(dims.begin(), dims.end());
-    const size_t smem = (size_t)((maxn + 1) / 2 + 1) * (2 * sizeof(double) + 2 * sizeof(int));
-    jacobi_kernel<<<nsec, JAC_THREADS, smem, st>>>(ctx->trB.d(), ctx->trC.d(), (const int64_t *)(tbase + p_roff),
-                                                  (const int *)(tbase + p_dims), ctx->trD.d(),
-                                                  (const int64_t *)(tbase + p_eoff), 60, (int *)(tbase + p_stat));
+    // tridiagonal reduction, then all eigenvalues
+    const size_t tsm = sizeof(double) * (3 * (size_t)maxn + std::max(maxn, EIG_THREADS));
+    CKT(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+    tridiag_kernel<<<nsec, EIG_THREADS, tsm, st>>>(ctx->trB.d(), d_roff, d_dims, d_eoff,
+                                                   (const int *)(tbase + p_order), dd, de, dtau, dinfo);
     CKT(cudaGetLastError());
+    if (etot) {
+      bisect_kernel<<<(unsigned)((etot + 127) / 128), 128, 0, st>>>(dd, de, d_eoff, d_dims, dinfo,
+                                                                    (const int *)(tbase + p_esec), (int)etot, dev);
+      CKT(cudaGetLastError());
+    }
     std::vector<double> ev(etot);
-    std::vector<int> status(nsec);
-    CKT(cudaMemcpyAsync(ev.data(), ctx->trD.d(), sizeof(double) * etot, cudaMemcpyDeviceToHost, st));
-    CKT(cudaMemcpyAsync(status.data(), tbase + p_stat, sizeof(int) * nsec, cudaMemcpyDeviceToHost, st));
+    CKT(cudaMemcpyAsync(ev.data(), dev, sizeof(double) * etot, cudaMemcpyDeviceToHost, st));
     CKT(cudaStreamSynchronize(st));
-    for (int i = 0; i < nsec; ++i)
-      if (status[i]) return set_err(TJ_ERR_NUMERIC, "tj_truncation: Jacobi eigen-solver did not converge");
 
     // ---- selection (den_mat.f90:201-330) ----
     std::vector<int> qnu(nsec), qnd(nsec);
@@ -370,8 +661,8 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     std::vector<int> cnt(nsec, 0);
     for (int k = 0; k < num_state; ++k) ++cnt[owner[ord[k]]];
     // kept eigenvectors: the cnt largest of each sector, in ascending order
-    std::vector<int64_t> src_off, dst_off;
-    std::vector<int> rows;
+    std::vector<int> job_sec, job_k, grp, slab;
+    std::vector<int64_t> job_dst;
     tc.sub.clear();
     int64_t dpos = 0;
     for (int i = 0; i < nsec; ++i) {
@@ -388,31 +679,63 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       sb.sdim = col;
       sb.off = dpos;
       tc.sub.push_back(sb);
+      grp.insert(grp.end(), {x, (int)job_sec.size(), col, 0});
       for (int c = 0; c < col; ++c) {
-        const int k = asc[x][dims[x] - col + c];
-        src_off.push_back(roff[x] + (int64_t)k * dims[x]);
-        dst_off.push_back(dpos + (int64_t)c * row);
-        rows.push_back(row);
+        job_sec.push_back(x);
+        job_k.push_back(asc[x][dims[x] - col + c]);
+        job_dst.push_back(dpos + (int64_t)c * row);
       }
       dpos += (int64_t)row * col;
     }
     tc.mats.assign(dpos, 0.0);
-    const int ncols = (int)rows.size();
-    if (ncols > 0) {
-      // gather tables and output reuse trD / trE (sized above for eigenvalues and tables)
-      const size_t need = al(ncols * 8) * 2 + al(ncols * 4) + (size_t)dpos * 8 + 256;
-      if ((rc = ctx->trA.reserve(std::max((size_t)(D + 4) * 8, need)))) return rc;
-      char *gb = (char *)ctx->trA.p;   // psi is no longer needed
-      int64_t *d_src = (int64_t *)gb, *d_dst = (int64_t *)(gb + al(ncols * 8));
-      int *d_rows = (int *)(gb + 2 * al(ncols * 8));
-      double *d_out = (double *)(gb + 2 * al(ncols * 8) + al(ncols * 4));
-      CKT(cudaMemcpyAsync(d_src, src_off.data(), ncols * 8, cudaMemcpyHostToDevice, st));
-      CKT(cudaMemcpyAsync(d_dst, dst_off.data(), ncols * 8, cudaMemcpyHostToDevice, st));
-      CKT(cudaMemcpyAsync(d_rows, rows.data(), ncols * 4, cudaMemcpyHostToDevice, st));
-      gather_cols_kernel<<<ncols, 128, 0, st>>>(ctx->trC.d(), d_src, d_rows, d_dst, d_out, ncols);
+    const int njobs = (int)job_sec.size(), ngrp = (int)grp.size() / 4;
+    if (njobs > 0) {
+      // vectors in shared memory: W warps of one column each per CTA
+      const int W = std::max(1, std::min(32, (int)(196608 / (sizeof(double) * maxn))));
+      for (int b = 0; b < ngrp; ++b)
+        for (int c0 = 0; c0 < grp[4 * b + 2]; c0 += W) slab.insert(slab.end(), {b, c0});
+      const int nslab = (int)slab.size() / 2;
+      const int ldy = (maxn + 3) / 4 * 4;
+      // trC: inverse-iteration factors and vectors; trA: job tables and the operator
+      const size_t wpl = (size_t)maxn * njobs;
+      const size_t p_work = 0, p_y = p_work + al256(5 * wpl * 8), p_piv = p_y + al256((size_t)njobs * ldy * 8);
+      if ((rc = ctx->trC.reserve(p_piv + al256(wpl)))) return rc;
+      size_t q = 0;
+      const size_t q_sec = q; q += al256((size_t)njobs * 4);
+      const size_t q_k = q; q += al256((size_t)njobs * 4);
+      const size_t q_dst = q; q += al256((size_t)njobs * 8);
+      const size_t q_grp = q; q += al256(grp.size() * 4);
+      const size_t q_slab = q; q += al256(slab.size() * 4);
+      const size_t q_out = q; q += al256((size_t)dpos * 8);
+      if ((rc = ctx->trA.reserve(q))) return rc;   // psi is no longer needed
+      char *ab = (char *)ctx->trA.p, *cb = (char *)ctx->trC.p;
+      CKT(cudaMemcpyAsync(ab + q_sec, job_sec.data(), (size_t)njobs * 4, cudaMemcpyHostToDevice, st));
+      CKT(cudaMemcpyAsync(ab + q_k, job_k.data(), (size_t)njobs * 4, cudaMemcpyHostToDevice, st));
+      CKT(cudaMemcpyAsync(ab + q_dst, job_dst.data(), (size_t)njobs * 8, cudaMemcpyHostToDevice, st));
+      CKT(cudaMemcpyAsync(ab + q_grp, grp.data(), grp.size() * 4, cudaMemcpyHostToDevice, st));
+      CKT(cudaMemcpyAsync(ab + q_slab, slab.data(), slab.size() * 4, cudaMemcpyHostToDevice, st));
+      double *Y = (double *)(cb + p_y), *d_out = (double *)(ab + q_out);
+      inverse_iter_kernel<<<(njobs + 63) / 64, 64, 0, st>>>(dd, de, d_eoff, d_dims, dinfo, dev,
+                                                            (const int *)(ab + q_sec), (const int *)(ab + q_k), njobs,
+                                                            maxn, (double *)(cb + p_work),
+                                                            (unsigned char *)(cb + p_piv), Y, ldy, d_status);
       CKT(cudaGetLastError());
+      orthonormalize_kernel<<<ngrp, ORTH_THREADS, sizeof(double) * maxn, st>>>((const int *)(ab + q_grp), d_dims, Y,
+                                                                               ldy, d_status);
+      CKT(cudaGetLastError());
+      const size_t bsm = sizeof(double) * (size_t)W * ldy;
+      CKT(cudaFuncSetAttribute(backtransform_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
+      backtransform_kernel<<<nslab, 32 * W, bsm, st>>>(ctx->trB.d(), d_roff, dtau, d_eoff, d_dims,
+                                                       (const int *)(ab + q_grp), (const int *)(ab + q_slab), Y, ldy,
+                                                       (const int64_t *)(ab + q_dst), d_out);
+      CKT(cudaGetLastError());
+      int status = 0;
       CKT(cudaMemcpyAsync(tc.mats.data(), d_out, sizeof(double) * dpos, cudaMemcpyDeviceToHost, st));
+      CKT(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
       CKT(cudaStreamSynchronize(st));
+      if (status & 1) return set_err(TJ_ERR_NUMERIC, "tj_truncation: inverse iteration produced a non-finite vector");
+      if (status & 2)
+        return set_err(TJ_ERR_NUMERIC, "tj_truncation: inverse iteration gave linearly dependent eigenvectors");
     }
     std::memset(&tc.res, 0, sizeof tc.res);
     tc.res.num_state = num_state;

@@ -1,14 +1,15 @@
 """Truncation (den_mat.f90) and correlator contractions (measure.f90) on the
 B200 against the oracle.
 
-Truncation: per-sector eigenvalues from the device Jacobi solver against
-LAPACK dsyev in the oracle (absolute 1e-13 of the largest), identical kept
-count, truncation error and entropies to 1e-10, and the kept eigenvectors
-spanning the same space: projector difference <= max(1e-8, 1e-15 / gap),
-gap = the sector's distance between its smallest kept and largest dropped
-eigenvalue (a subspace is determined by FP64 data only to about eps ||rho||
-/ gap, for LAPACK and Jacobi alike; eigenvector signs and degenerate bases
-are free).  Correlators: relative 1e-12.
+Truncation: identical kept count, truncation error and entropies to 1e-10
+against LAPACK dsyev in the oracle (the device eigenvalues come from
+Householder tridiagonalisation and Sturm multisection), kept eigenvectors
+orthonormal to 1e-12 and spanning the same space: projector difference
+<= max(1e-8, 1e-15 / gap), gap = the sector's distance between its smallest
+kept and largest dropped eigenvalue (a subspace is determined by FP64 data
+only to about eps ||rho|| / gap, for any backward-stable solver;
+eigenvector signs and degenerate bases are free).  Correlators: relative
+1e-12.
 """
 import numpy as np
 import pytest
@@ -67,6 +68,9 @@ def test_truncation(ctx, oracle_lib, wl, side, kmin, kmax):
     assert abs(r1.trunc_err - r0.trunc_err) <= 1e-10
     for k in ("entropy1", "entropy2", "entropys"):
         assert abs(getattr(r1, k) - getattr(r0, k)) <= 1e-10, k
+    for sb1 in t1.subs:
+        q = sb1.mat
+        assert np.max(np.abs(q.T @ q - np.eye(q.shape[1]))) <= 1e-12
     p0, p1 = _projectors(t0), _projectors(t1)
     assert p0.keys() == p1.keys()
     gaps = _sector_gaps(psi, side, t0)
