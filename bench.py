@@ -188,12 +188,12 @@ def measured_peaks():
         return {}
 
 
-def profile_traffic(workload: str, precision: str):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if any."""
+def profile_traffic(workload: str, precision: str, launch: str):
+    """DRAM bytes (read + write) of one launch from the committed ncu capture summary, if any."""
     try:
         with open(os.path.join(ROOT, "profiles", "roofline_inputs.json")) as f:
             d = json.load(f)
-        return d.get(workload, {}).get(precision, {}).get("traffic_bytes_per_hpsi")
+        return d.get(workload, {}).get(precision, {}).get(launch)
     except Exception:
         return None
 
@@ -343,7 +343,8 @@ def main():
         achieved = alg / (tdom * 1e-3) / 1e12
         roof = {"bound": "tensor", "kernel": "oz_gemm_kernel (launch %d)" % dom, "achieved": achieved,
                 "peak": i8, "unit": "TFLOP/s", "frac": (achieved / i8) if i8 else None,
-                "traffic": profile_traffic(args.workload, "ozaki"),
+                "traffic": profile_traffic(args.workload, "ozaki", "launch%d" % dom),
+                "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
                 "peak_source": "measured cuBLASLt int8 GEMM 8192^3 (torch._int_mm) on this GPU; int8 ops",
                 "work": "algorithmic int8 ops = FP64-equivalent flops of the launch x s(s+1)/2 slice products",
                 "issued_int8_ops": issued, "launch_ms": tdom,
@@ -354,7 +355,8 @@ def main():
         achieved = st.flops / (ms * 1e-3) / 1e12
         roof = {"bound": "tensor", "kernel": "grouped_gemm_kernel (both phases)", "achieved": achieved,
                 "peak": fp64, "unit": "TFLOP/s", "frac": (achieved / fp64) if fp64 else None,
-                "traffic": profile_traffic(args.workload, "fp64"),
+                "traffic": profile_traffic(args.workload, "fp64", "per_hpsi"),
+                "traffic_unit": "bytes per H*psi, both launches (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
                 "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU (FP64; not in MEASURED_PEAKS.json)",
                 "phase1_ms": st.last_ms_phase1, "phase2_ms": st.last_ms_phase2}
     roof.update({"flops_per_hpsi": st.flops, "flops_ref_per_hpsi": st.flops_ref, "bytes_per_hpsi": st.bytes,
