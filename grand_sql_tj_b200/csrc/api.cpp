@@ -90,6 +90,18 @@ extern "C" int tj_step_begin(tj_ctx *ctx) {
   return TJ_OK;
 }
 
+extern "C" int tj_host_register(void *p, size_t bytes) {
+  if (!p || bytes == 0) return set_err(TJ_ERR_ARG, "tj_host_register: null pointer or zero size");
+  CK(cudaHostRegister(p, bytes, cudaHostRegisterDefault));
+  return TJ_OK;
+}
+
+extern "C" int tj_host_unregister(void *p) {
+  if (!p) return set_err(TJ_ERR_ARG, "tj_host_unregister: null pointer");
+  CK(cudaHostUnregister(p));
+  return TJ_OK;
+}
+
 extern "C" int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st) {
   if (!ctx || !st) return set_err(TJ_ERR_ARG, "null argument");
   *st = ctx->stats;
@@ -168,10 +180,15 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   if (ctx->plan_valid && ctx->plan_key == h) return TJ_OK;
   ctx->plan_valid = false;
   CK(cudaSetDevice(ctx->device));
+  using clk = std::chrono::steady_clock;
+  auto ms_since = [](clk::time_point a) { return std::chrono::duration<double, std::milli>(clk::now() - a).count(); };
+  const auto t_start = clk::now();
   std::unique_ptr<HpsiPlan> P(new HpsiPlan());
   std::string msg;
   int rc = build_hpsi_plan(lat, sys, env, sys_bs, env_bs, wave, *P, msg);
   if (rc) return set_err(rc, "H*psi plan: " + msg);
+  const double plan_ms = ms_since(t_start);
+  const auto t_up = clk::now();
   // operators: one copy per input block, then the merged sums on the device
   if ((rc = ctx->ops.reserve(sizeof(double) * (P->ops_len + 4)))) return rc;
   for (const auto &u : P->uploads)
@@ -205,9 +222,12 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   if ((rc = ctx->counters.reserve(64))) return rc;
   if ((rc = ctx->partials.reserve(sizeof(double) * (std::max(P->tiles2.size(), P->tiles1.size()) + 4096))))
     return rc;
+  const double upload_ms = ms_since(t_up);
+  double ozplan_ms = 0;
   ctx->oz.reset();
   if (ctx->prec_mode == TJ_PREC_OZAKI) {
     // split-precision form: regroup the tasks, split the operators once for this step
+    const auto t_oz = clk::now();
     std::unique_ptr<OzPlan> oz(new OzPlan());
     try {
       int nsm = 148;
@@ -216,6 +236,7 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
     } catch (const std::exception &e) {
       return set_err(TJ_ERR_ARG, std::string("split-precision plan: ") + e.what());
     }
+    ozplan_ms = ms_since(t_oz);
     if ((rc = upload_vec(ctx, ctx->ozStaJobs, oz->sta_jobs)) || (rc = upload_vec(ctx, ctx->ozPsiJobs, oz->psi_jobs)) ||
         (rc = upload_vec(ctx, ctx->ozProdJobs, oz->prod_jobs)) || (rc = upload_vec(ctx, ctx->ozSegs, oz->segs)) ||
         (rc = upload_vec(ctx, ctx->ozFams, oz->fams)) || (rc = upload_vec(ctx, ctx->ozStacks, oz->stacks)) ||
@@ -244,6 +265,10 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   }
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->stats = tj_hpsi_stats();
+  ctx->stats.prepare_ms = ms_since(t_start);
+  ctx->stats.plan_ms = plan_ms;
+  ctx->stats.upload_ms = upload_ms;
+  ctx->stats.ozplan_ms = ozplan_ms;
   ctx->stats.flops = P->flops;
   ctx->stats.flops_ref = P->flops_ref;
   ctx->stats.bytes = P->bytes;
@@ -542,7 +567,6 @@ extern "C" int tj_lanczos_memo_new(tj_ctx *ctx, const tj_lattice *lat, const tj_
   energies[0] = hl;
   *iters = last;
   ctx->stats.lanczos_hpsi = ctx->n_hpsi - h0;
-  ctx->stats_lanczos_ms =
-      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  ctx->stats.lanczos_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return TJ_OK;
 }

@@ -44,7 +44,6 @@ struct tj_ctx {
   bool plan_valid = false;
   int64_t n_hpsi = 0;
   tj_hpsi_stats stats{};
-  double stats_lanczos_ms = 0;
   // device buffers
   tjb::DevBuf ops, scr, vin, vout, counters, partials;
   tjb::DevBuf cells1, cells2, tasks1, tasks2, tiles1, tiles2, red1, red2, slots;

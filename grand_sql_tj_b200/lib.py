@@ -169,6 +169,8 @@ def lib():
         L.tj_ctx_destroy.argtypes = [C.c_void_p]
         L.tj_set_precision.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.tj_step_begin.argtypes = [C.c_void_p]
+        L.tj_host_register.argtypes = [C.c_void_p, C.c_size_t]
+        L.tj_host_unregister.argtypes = [C.c_void_p]
         hp = [C.c_void_p, P(TjLattice), P(TjModel), P(TjModel), P(TjBasis), P(TjBasis)]
         L.tj_model_wave.argtypes = hp + [P(TjWave), P(TjWave)]
         L.tj_model_wave_bench.argtypes = hp + [P(TjWave), P(TjWave), C.c_int, P(C.c_double)]
@@ -250,10 +252,17 @@ class Context:
                                        C.byref(be.c), C.byref(invec.c), C.byref(out.c), reps, C.byref(ms)))
         return ms.value, out
 
-    def lanczos_memo_new(self, sb, lanzero: float, start: Optional[Wave] = None):
-        """lanczos_memo_new (eigen.f90:2), levels = 1: returns (E0, iterations, Ritz vector)."""
-        w = (sb.wave if start is None else start).copy()
-        ps, pe, bs, be = sb.sys.pack(), sb.env.pack(), sb.sys_bs.pack(), sb.env_bs.pack()
+    def lanczos_memo_new(self, sb, lanzero: float, start: Optional[Wave] = None, packed=None,
+                         in_place: bool = False):
+        """lanczos_memo_new (eigen.f90:2), levels = 1: returns (E0, iterations, Ritz vector).
+
+        packed: (sys, env, sys_bs, env_bs) from pack_superblock, reused across
+        calls; in_place: `start` is overwritten by the Ritz vector (as the
+        reference's eigvec argument is) instead of being copied first."""
+        w = sb.wave if start is None else start
+        if not in_place:
+            w = w.copy()
+        ps, pe, bs, be = packed if packed is not None else pack_superblock(sb)
         e, it = (C.c_double * 1)(), C.c_int()
         _chk(lib().tj_lanczos_memo_new(self.h, C.byref(sb.lat.c), C.byref(ps.c), C.byref(pe.c), C.byref(bs.c),
                                        C.byref(be.c), C.byref(w.c), 1, lanzero, e, C.byref(it)))
@@ -320,6 +329,43 @@ def _export(call) -> dict:
         src = np.ctypeslib.as_array(C.cast(u.src, C.POINTER(C.c_double)), shape=(u.n,))
         ops[u.dst:u.dst + u.n] = src
     return {"ex": ex, "ops": ops, **arrs}
+
+
+def pack_superblock(sb):
+    """The C views (sys, env, sys_bs, env_bs) of a superblock's models and bases."""
+    return sb.sys.pack(), sb.env.pack(), sb.sys_bs.pack(), sb.env_bs.pack()
+
+
+def packed_arrays(packed):
+    """Every operator data array of pack_superblock's models."""
+    out = []
+    for m in packed[:2]:
+        out.append(m.ham.data)
+        for sets in m.sets:
+            out.extend(p.data for p in sets)
+    return out
+
+
+class PinnedHost:
+    """Page-locks host arrays through tj_host_register for the life of the object."""
+
+    def __init__(self, arrays):
+        self.ptrs = []
+        for a in arrays:
+            if a.nbytes:
+                _chk(lib().tj_host_register(a.ctypes.data, a.nbytes))
+                self.ptrs.append(a.ctypes.data)
+
+    def close(self):
+        for p in self.ptrs:
+            lib().tj_host_unregister(p)
+        self.ptrs = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def plan_export(sb, invec: Optional[Wave] = None) -> dict:

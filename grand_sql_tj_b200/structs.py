@@ -92,7 +92,9 @@ class TjHpsiStats(C.Structure):
                 ("last_ms_phase2", C.c_double), ("lanczos_hpsi", C.c_int64),
                 ("int8_ops", C.c_double), ("kernels_per_hpsi", C.c_int64), ("last_ms_split", C.c_double),
                 ("flops_launch1", C.c_double), ("flops_launch2", C.c_double),
-                ("int8_ops_launch1", C.c_double), ("int8_ops_launch2", C.c_double)]
+                ("int8_ops_launch1", C.c_double), ("int8_ops_launch2", C.c_double),
+                ("prepare_ms", C.c_double), ("plan_ms", C.c_double), ("upload_ms", C.c_double),
+                ("ozplan_ms", C.c_double), ("lanczos_ms", C.c_double)]
 
 
 def _dptr(a: np.ndarray):

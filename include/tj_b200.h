@@ -152,6 +152,14 @@ int tj_set_precision(tj_ctx *ctx, int mode, int slices);
 /* Invalidates the operators and task lists cached for the current DMRG step. */
 int tj_step_begin(tj_ctx *ctx);
 const char *tj_last_error(void);
+/* No counterpart in the reference.  Page-locks (pins) `bytes` of the caller's
+ * host memory at `p` for the lifetime of the registration, so that the
+ * per-step operator upload of tj_model_wave / tj_lanczos_memo_new runs as
+ * asynchronous DMA that overlaps the plan compilation on the host.  Optional:
+ * unpinned memory works, with the upload copied through the driver's staging
+ * buffers.  tj_host_unregister releases a registration made here. */
+int tj_host_register(void *p, size_t bytes);
+int tj_host_unregister(void *p);
 
 /* ------------------------------------------------------- hot-path calls */
 
@@ -231,6 +239,10 @@ typedef struct tj_hpsi_stats {
   double last_ms_split;    /* split precision: its max/split kernels             */
   double flops_launch1, flops_launch2;  /* FP64-equivalent flops of each launch    */
   double int8_ops_launch1, int8_ops_launch2;  /* split precision: issued per launch */
+  /* host wall time (ms) of the last plan preparation: all of it, the H*psi
+   * plan compile, operator upload + hmerge + work-list upload, the
+   * split-precision plan, and the last tj_lanczos_memo_new after it */
+  double prepare_ms, plan_ms, upload_ms, ozplan_ms, lanczos_ms;
 } tj_hpsi_stats;
 int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st);
 
