@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -244,7 +245,8 @@ __device__ __forceinline__ double start_entry(int s, int k, int i) {
 // nearly singular factor stays finite), three solves from a fixed
 // pseudo-random start, each result rescaled.  The per-thread factors live in
 // work[] with element i of job j at i * njobs + j (coalesced across a warp);
-// the unit vector goes to Y[j * ldy + i].  status bit 0: a non-finite value.
+// the unit vector goes to Y[j * ldy + i].  status[0] bit 0: a non-finite
+// value; the first such vector is described at status + 4 (six doubles).
 __global__ void inverse_iter_kernel(const double *dall, const double *eall, const int64_t *eoff, const int *dims,
                                     const double *info, const double *evals, const int *job_sec, const int *job_k,
                                     int njobs, int nmax, double *work, unsigned char *piv, double *Y, int ldy,
@@ -286,6 +288,9 @@ __global__ void inverse_iter_kernel(const double *dall, const double *eall, cons
     dui = dun;
   }
   AT(U, n - 1) = fabs(di) < pert ? copysign(pert, di) : di;
+  AT(DU, n - 1) = 0.0;   // read (times zero) by the first back-substitution row
+  AT(DU2, n - 1) = 0.0;
+  if (n >= 2) AT(DU2, n - 2) = 0.0;
   for (int i = 0; i < n; ++i) AT(X, i) = start_entry(s, k, i);
   bool bad = false;
   for (int sweep = 0; sweep < 3; ++sweep) {
@@ -329,6 +334,16 @@ __global__ void inverse_iter_kernel(const double *dall, const double *eall, cons
   for (int i = 0; i < n; ++i) nrm += AT(X, i) * AT(X, i);
   if (bad || !(nrm > 0.0) || !isfinite(nrm)) {
     atomicOr(status, 1);
+    // the first failing vector: sector, eigenvalue index, lam, pivot floor, n
+    if (atomicCAS(status + 1, 0, j + 1) == 0) {
+      double *diag = (double *)(status + 4);
+      diag[0] = s;
+      diag[1] = k;
+      diag[2] = lam;
+      diag[3] = pert;
+      diag[4] = n;
+      diag[5] = nrm;
+    }
     nrm = 1.0;
   }
   const double inv = 1.0 / sqrt(nrm);
@@ -568,7 +583,7 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     CKT(cudaMemcpyAsync(tbase + p_dims, dims.data(), db, cudaMemcpyHostToDevice, st));
     CKT(cudaMemcpyAsync(tbase + p_order, order.data(), db, cudaMemcpyHostToDevice, st));
     if (etot) CKT(cudaMemcpyAsync(tbase + p_esec, esec.data(), sizeof(int) * etot, cudaMemcpyHostToDevice, st));
-    CKT(cudaMemsetAsync(tbase + p_cnt, 0, 32, st));
+    CKT(cudaMemsetAsync(tbase + p_cnt, 0, 256, st));
     const int64_t *d_roff = (const int64_t *)(tbase + p_roff), *d_eoff = (const int64_t *)(tbase + p_eoff);
     const int *d_dims = (const int *)(tbase + p_dims);
     int *d_status = (int *)(tbase + p_cnt + 16);
@@ -729,12 +744,21 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
                                                        (const int *)(ab + q_grp), (const int *)(ab + q_slab), Y, ldy,
                                                        (const int64_t *)(ab + q_dst), d_out);
       CKT(cudaGetLastError());
-      int status = 0;
+      int status[16] = {0};
       CKT(cudaMemcpyAsync(tc.mats.data(), d_out, sizeof(double) * dpos, cudaMemcpyDeviceToHost, st));
-      CKT(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CKT(cudaMemcpyAsync(status, d_status, sizeof status, cudaMemcpyDeviceToHost, st));
       CKT(cudaStreamSynchronize(st));
-      if (status & 1) return set_err(TJ_ERR_NUMERIC, "tj_truncation: inverse iteration produced a non-finite vector");
-      if (status & 2)
+      if (status[0] & 1) {
+        double dg[6];
+        std::memcpy(dg, status + 4, sizeof dg);
+        char buf[256];
+        std::snprintf(buf, sizeof buf,
+                      "tj_truncation: inverse iteration produced a non-finite vector (sector %d, eigenvalue %d of "
+                      "%d, lambda %.17g, pivot floor %.3g, norm %g)",
+                      (int)dg[0], (int)dg[1], (int)dg[4], dg[2], dg[3], dg[5]);
+        return set_err(TJ_ERR_NUMERIC, buf);
+      }
+      if (status[0] & 2)
         return set_err(TJ_ERR_NUMERIC, "tj_truncation: inverse iteration gave linearly dependent eigenvectors");
     }
     std::memset(&tc.res, 0, sizeof tc.res);
