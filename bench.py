@@ -375,8 +375,11 @@ def main():
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, sec = cpu_reference(sb, 2, 0, threads)
+        rate1, sec1 = cpu_reference(sb, 1, 0, 1)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": "2 model_wave calls of the oracle on the same superblock"}
+               "sample": "2 model_wave calls of the oracle on the same superblock",
+               "single_thread": {"value": rate1, "unit": UNIT, "cores": 1,
+                                 "sample": "1 model_wave call of the oracle, OPENBLAS 1 thread"}}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": max(args.warmup, 3), "ms_per_step": ms_max, "higher_is_better": True,

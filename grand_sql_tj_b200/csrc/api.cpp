@@ -49,6 +49,7 @@ tj_ctx::~tj_ctx() {
   for (auto &e : ev)
     if (e) cudaEventDestroy(e);
   if (stream) cudaStreamDestroy(stream);
+  if (pinned) cudaFreeHost(pinned);
 }
 
 extern "C" int tj_ctx_create(tj_ctx **out, int device) {
@@ -64,6 +65,7 @@ extern "C" int tj_ctx_create(tj_ctx **out, int device) {
   c->device = device;
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CK(cudaMallocHost((void **)&c->pinned, 32 * sizeof(double)));
   for (auto &e : c->ev) CK(cudaEventCreate(&e));
   *out = c.release();
   return TJ_OK;
@@ -526,13 +528,16 @@ extern "C" int tj_lanczos_memo_new(tj_ctx *ctx, const tj_lattice *lat, const tj_
   double ritzmin = 0, hb = 0, hl = 0;
   if ((rc = fetch(alpha + 1, &ritzmin))) return rc;
   int last = 1;
+  // One host synchronisation per iteration: beta(last) and the new Ritz value
+  // are read together at its end.  The reference stops before normalising
+  // the next vector when |beta| <= lanzero (eigen.f90); here that vector and
+  // its H*psi are computed speculatively and dropped, with `last` restored,
+  // so the result is the same.
   while (last < LOOP_IN) {
     launch_lanczos_update(vec(last + 1), vec(last), last >= 2 ? vec(last - 1) : nullptr, alpha + last,
                           beta + last - 1, D, ctx->stream);
     norm_into(vec(last + 1), beta + last);
-    if ((rc = fetch(beta + last, &hb))) return rc;
-    if (!std::isfinite(hb)) return set_err(TJ_ERR_NUMERIC, "Lanczos: non-finite beta");
-    if (std::fabs(hb) <= lanzero) break;
+    CK(cudaMemcpyAsync(ctx->pinned, beta + last, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     launch_scale_inv(vec(last + 1), beta + last, D, ctx->stream);
     // Gram_Schmidt_process (block.f90:2515-2551)
     launch_multi_dot(V, ld, last, vec(last + 1), D, mpart, mdb, 128, ctx->stream);
@@ -546,7 +551,15 @@ extern "C" int tj_lanczos_memo_new(tj_ctx *ctx, const tj_lattice *lat, const tj_
     dot_into(vec(last), vec(last + 1), alpha + last);
     launch_tridiag_min(alpha + 1, beta + 1, last, lam, nullptr, 0, ctx->stream);
     CK(cudaGetLastError());
-    if ((rc = fetch(lam, &hl))) return rc;
+    CK(cudaMemcpyAsync(ctx->pinned + 1, lam, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    hb = ctx->pinned[0];
+    hl = ctx->pinned[1];
+    if (!std::isfinite(hb)) return set_err(TJ_ERR_NUMERIC, "Lanczos: non-finite beta");
+    if (std::fabs(hb) <= lanzero) {
+      --last;
+      break;
+    }
     if (!std::isfinite(hl)) return set_err(TJ_ERR_NUMERIC, "Lanczos: non-finite Ritz value");
     if (std::fabs(hl - ritzmin) <= lanzero || last == LOOP_IN) {
       ritzmin = hl;

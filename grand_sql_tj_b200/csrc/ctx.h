@@ -34,6 +34,7 @@ struct DevBuf {
 struct tj_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  double *pinned = nullptr;   // 32 doubles of page-locked host memory for scalar read-backs
   // H*psi timing: 0 start, 1 after the splits of psi, 2 after the first GEMM
   // launch, 3 after the product splits, 4 end (FP64: 1 = 0 and 3 = 2)
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};

@@ -348,11 +348,29 @@ void launch_combine(const double *V, int64_t ld, int k, const double *coef, doub
   combine_kernel<<<vgrid(n), VT, 0, s>>>(V, ld, k, coef, w, n, assign);
 }
 
-// Lowest eigenpair of a symmetric tridiagonal matrix (n <= 128): Sturm-count
-// bisection to full precision, then inverse iteration with a pivoted
-// tridiagonal solve.  One thread; n is at most the Lanczos depth.
+// Number of eigenvalues of the tridiagonal (a, b) below x (Sturm count).
+__device__ __forceinline__ int sturm_count(const double *a, const double *b, int n, double x) {
+  const double tiny = 1e-300;
+  int cnt = 0;
+  double q = a[0] - x;
+  if (q < 0) ++cnt;
+  for (int i = 1; i < n; ++i) {
+    if (fabs(q) < tiny) q = -tiny;
+    q = (a[i] - x) - b[i - 1] * b[i - 1] / q;
+    if (q < 0) ++cnt;
+  }
+  return cnt;
+}
+
+// Lowest eigenpair of a symmetric tridiagonal matrix (n <= 128): the lowest
+// eigenvalue to full precision -- the pair of adjacent doubles where the
+// Sturm count turns from 0 to 1 -- by 32-point multisection (one warp, one
+// point per lane: five bits per pass) finished by bisection, then inverse
+// iteration with a pivoted tridiagonal solve on one thread.  n is at most the
+// Lanczos depth.
 __global__ void tridiag_min_kernel(const double *a, const double *b, int n, double *lam, double *vec, int want_vec) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
   double lo = 0.0, hi = 0.0;
   for (int i = 0; i < n; ++i) {
     const double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i < n - 1 ? fabs(b[i]) : 0.0);
@@ -360,21 +378,31 @@ __global__ void tridiag_min_kernel(const double *a, const double *b, int n, doub
     if (i == 0 || l < lo) lo = l;
     if (i == 0 || h > hi) hi = h;
   }
-  const double tiny = 1e-300;
+  // invariant: count(lo) = 0 < count(hi) (Gershgorin bounds)
+  for (int pass = 0; pass < 64; ++pass) {
+    const double x = lo + (hi - lo) * ((double)(lane + 1) / 33.0);
+    const bool valid = x > lo && x < hi;
+    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+    if (vmask == 0) break;
+    const int cnt = valid ? sturm_count(a, b, n, x) : 0;
+    const unsigned up = __ballot_sync(0xffffffffu, valid && cnt >= 1);
+    if (up == 0) {
+      lo = __shfl_sync(0xffffffffu, x, 31 - __clz(vmask));   // the highest valid point
+    } else {
+      const int f = __ffs(up) - 1;
+      const double xf = __shfl_sync(0xffffffffu, x, f);
+      const double xp = __shfl_sync(0xffffffffu, x, f > 0 ? f - 1 : 0);
+      if (f > 0 && ((vmask >> (f - 1)) & 1u)) lo = xp;
+      hi = xf;
+    }
+  }
   for (int it = 0; it < 200; ++it) {
     const double mid = 0.5 * (lo + hi);
     if (mid <= lo || mid >= hi) break;
-    int cnt = 0;
-    double q = a[0] - mid;
-    if (q < 0) ++cnt;
-    for (int i = 1; i < n; ++i) {
-      if (fabs(q) < tiny) q = -tiny;
-      q = (a[i] - mid) - b[i - 1] * b[i - 1] / q;
-      if (q < 0) ++cnt;
-    }
-    if (cnt >= 1) hi = mid; else lo = mid;
+    if (sturm_count(a, b, n, mid) >= 1) hi = mid; else lo = mid;
   }
   const double l = 0.5 * (lo + hi);
+  if (lane != 0) return;
   *lam = l;
   if (!want_vec) return;
   // inverse iteration on (T - l I) with partial pivoting
