@@ -266,9 +266,26 @@ struct OzCfg {
   static_assert(STAGES >= 2, "too few pipeline stages");
 };
 
+// Per-item data of the epilogue, staged in shared memory by the metadata warp
+// ahead of the item's accumulators: power-of-two column scales and row scales
+// of each family (at most two per item), and where each tile row goes.
+constexpr int OZ_META = 4;       // ring slots
+constexpr int OZ_META_AX = 4;    // axpy terms held per cell (more are read from global memory)
+template <int BN>
+struct OzMeta {
+  double cs[2][BN];
+  double rs[2][128];
+  int64_t dst[128];              // products: offset of P(row's column, col0) in scr; -1: nothing to store
+  int64_t c_off;                 // cells: offset of (row0, col0) in out
+  int32_t c_ld, na;              // cells: leading dimension; axpy terms (init items)
+  double ax_coef[OZ_META_AX];
+  int64_t ax_off[OZ_META_AX];    // psi offset of the axpy operand's (row0, col0)
+  int32_t ax_ld[OZ_META_AX];
+};
+
 // 8 epilogue warps (two column halves of the tile x four TMEM lane quarters),
-// then the producer warp and the MMA warp
-constexpr int OZ_EPI_THREADS = 256, OZ_GEMM_THREADS = OZ_EPI_THREADS + 64;
+// then the producer warp, the MMA warp and the metadata warp
+constexpr int OZ_EPI_THREADS = 256, OZ_GEMM_THREADS = OZ_EPI_THREADS + 96;
 
 template <int S, int BN>
 __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParams p) {
@@ -285,10 +302,11 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
   constexpr int OZ_ICACHE = 64;
   __shared__ OzItem item_sh[OZ_ICACHE];
   __shared__ OzSeg seg1_sh[OZ_ICACHE];
-  __shared__ double cscale_sh[BN];           // epilogue: column scales of the current family
-  __shared__ int32_t stk_start[17];          // epilogue: first tile row of each stacked run
-  __shared__ int64_t stk_dst[16], stk_rs[16];
-  __shared__ int32_t stk_ld[16], stk_nc[16];
+  __shared__ OzMeta<BN> meta[OZ_META];
+  __shared__ __align__(8) uint64_t meta_full[OZ_META], meta_empty[OZ_META];
+  static_assert(C::SMEM + sizeof(OzMeta<BN>) * OZ_META + OZ_ICACHE * (sizeof(OzItem) + sizeof(OzSeg)) + 2048 <=
+                    232448,
+                "shared memory above 227 KB");
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (tid == 0) {
@@ -301,6 +319,10 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(&tempty_bar[i])), "r"(OZ_EPI_THREADS));
     }
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(&drain_bar)), "r"(1));
+    for (int i = 0; i < OZ_META; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(&meta_full[i])), "r"(32));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(oz_smem(&meta_empty[i])), "r"(OZ_EPI_THREADS));
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     abort_sh = 0;
   }
@@ -473,9 +495,86 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       }
     }
     __syncwarp();
+  } else if (warp == OZ_EPI_THREADS / 32 + 2) {
+    // ------------------------------------------------ metadata (whole warp): one ring slot per item
+    uint32_t icount = 0;
+    for (int ii = ib; ii < ie_cta; ++ii, ++icount) {
+      const OzItem it = get_item(ii);
+      const int slot = (int)(icount % OZ_META);
+      int good = 1;
+      if (lane == 0 && !oz_wait(oz_smem(&meta_empty[slot]), ((icount / OZ_META) & 1u) ^ 1u, &abort_sh)) {
+        if (!abort_sh) oz_fail(&abort_sh, p.err);
+        good = 0;
+      }
+      if (!__shfl_sync(0xffffffffu, good, 0)) break;
+      OzMeta<BN> &m = meta[slot];
+      if (it.kind == 1) {
+        // stacked runs (at most 16): the run holding each tile row, its P
+        // destination and the tau scale of the X column it came from
+        const int np = it.fam_end - it.fam_begin;
+        OzStack sk{};
+        int ng = 0;
+        if (lane < np) {
+          sk = p.stacks[it.fam_begin + lane];
+          ng = sk.a_ng;
+        }
+        int incl = ng * 8;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t;
+        }
+        const int start = incl - ng * 8;
+        for (int j = lane; j < it.ncols; j += 32) m.cs[0][j] = oz_pow2_of(p.scales[it.cs_idx + j]);
+        int64_t rdst[4] = {-1, -1, -1, -1}, ridx[4] = {0, 0, 0, 0};
+        for (int q = 0; q < np; ++q) {
+          const int s0 = __shfl_sync(0xffffffffu, start, q);
+          const int e0 = s0 + 8 * __shfl_sync(0xffffffffu, ng, q);
+          const int64_t d0 = __shfl_sync(0xffffffffu, sk.dst_off, q);
+          const int64_t x0 = __shfl_sync(0xffffffffu, sk.rs_idx, q);
+          const int ld = __shfl_sync(0xffffffffu, sk.dst_ld, q);
+          const int nc = __shfl_sync(0xffffffffu, sk.ncols, q);
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const int r = lane + 32 * t;
+            if (r >= s0 && r < e0 && r - s0 < nc) {
+              rdst[t] = d0 + (int64_t)(r - s0) * ld + it.col0;
+              ridx[t] = x0 + (r - s0);
+            }
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int r = lane + 32 * t;
+          m.dst[r] = rdst[t];
+          m.rs[0][r] = rdst[t] >= 0 ? oz_pow2_of(p.scales[ridx[t]]) : 0.0;
+        }
+      } else {
+        const int nf = it.fam_end - it.fam_begin;   // at most 2 (checked by the plan)
+        for (int f = 0; f < nf; ++f) {
+          const OzFam fm = p.fams[it.fam_begin + f];
+          for (int j = lane; j < it.ncols; j += 32) m.cs[f][j] = oz_pow2_of(p.scales[fm.cs_idx + it.col0 + j]);
+          for (int r = lane; r < it.mrows; r += 32) m.rs[f][r] = oz_pow2_of(p.scales[fm.rs_idx + it.row0 + r]);
+        }
+        const OzCell c = p.cells[it.cell];
+        const int na = it.init ? c.a_end - c.a_begin : 0;
+        if (lane == 0) {
+          m.c_off = c.off + it.row0 + (int64_t)it.col0 * c.ld;
+          m.c_ld = c.ld;
+          m.na = na;
+        }
+        if (lane < min(na, OZ_META_AX)) {
+          const Task t = p.tasks[c.a_begin + lane];
+          m.ax_coef[lane] = t.coef;
+          m.ax_off[lane] = t.L.off + (int64_t)it.col0 * t.L.ld + it.row0;
+          m.ax_ld[lane] = t.L.ld;
+        }
+      }
+      oz_arrive(oz_smem(&meta_full[slot]));   // every lane: release of its own writes
+    }
+    __syncwarp();
   } else {
-    // ------------------------------------------------ epilogue (warps 0-3, named barrier 1)
-    uint32_t famc = 0;
+    // ------------------------------------------------ epilogue (warps 0-7, named barrier 1)
+    uint32_t famc = 0, icount = 0;
     double w[S];
     {
       double x = 1.0 / 16384.0;   // 128^-2
@@ -486,7 +585,8 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       }
     }
     bool ok = true;
-    for (int ii = p.cta[blockIdx.x], ie = p.cta[blockIdx.x + 1]; ii < ie && ok; ++ii) {
+    constexpr int HCH = (BN / 8 + 1) / 2;   // most 8-column chunks of a half
+    for (int ii = ib; ii < ie_cta && ok; ++ii, ++icount) {
       const OzItem it = get_item(ii);
       // warp w reads TMEM lane quarter q = w % 4 (lanes 32q..32q+31) and
       // column half h = w / 4 of the tile; the tile row it holds:
@@ -501,77 +601,81 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
         r = quarter * 16 + lane;
         rv = lane < 16 && r < it.mrows;
       }
+      const int rr = min(r, 127);
       // this half's 8-column chunks: [c0, c0 + nchh)
       const int nch = it.N >> 3, hch = (nch + 1) >> 1;
       const int c0 = half * hch, nchh = min(hch, nch - c0);
       const int nf = it.kind == 1 ? 1 : it.fam_end - it.fam_begin;
+      const int slot = (int)(icount % OZ_META);
+      if (!oz_wait(oz_smem(&meta_full[slot]), (icount / OZ_META) & 1u, &abort_sh)) {
+        if (!abort_sh) oz_fail(&abort_sh, p.err);
+        ok = false;
+        break;
+      }
+      const OzMeta<BN> &m = meta[slot];
       double *dst = nullptr;
-      int64_t cstride = 0;
-      double rscale_stack = 0.0;
-      OzCell c{};
+      int64_t cstride = 1;
+      // the values the tile is added to, loaded before the accumulators are
+      // waited for: the old H*psi (cells of launch 2) or the axpy terms (init)
+      double old[HCH * 8];
+#pragma unroll
+      for (int j = 0; j < HCH * 8; ++j) old[j] = 0.0;
       if (it.kind == 0) {
-        c = p.cells[it.cell];
-        dst = p.out + c.off + (int64_t)(it.row0 + r) + (int64_t)it.col0 * c.ld;
-        cstride = c.ld;
-      } else {
-        // stacked products: the runs of this tile, then the run holding this row
-        const int np = it.fam_end - it.fam_begin;
-        if (tid < np) {
-          const OzStack sk = p.stacks[it.fam_begin + tid];
-          stk_dst[tid] = sk.dst_off;
-          stk_rs[tid] = sk.rs_idx;
-          stk_ld[tid] = sk.dst_ld;
-          stk_nc[tid] = sk.ncols;
-          stk_start[tid + 1] = sk.a_ng * 8;
-        }
-        if (tid == 0) stk_start[0] = 0;
-        asm volatile("bar.sync 1, 256;" ::: "memory");
-        if (tid == 0)
-          for (int i = 0; i < np; ++i) stk_start[i + 1] += stk_start[i];
-        asm volatile("bar.sync 1, 256;" ::: "memory");
-        int piece = -1;
-        for (int i = 0; i < np; ++i)
-          if (r >= stk_start[i] && r < stk_start[i + 1]) piece = i;
-        rv = rv && piece >= 0;
-        if (piece >= 0) {
-          const int jl = r - stk_start[piece];
-          if (jl < stk_nc[piece]) {
-            dst = p.scr + stk_dst[piece] + (int64_t)jl * stk_ld[piece] + it.col0;
-            rscale_stack = oz_pow2_of(p.scales[stk_rs[piece] + jl]);
-          } else {
-            rv = false;
+        dst = p.out + m.c_off + r;
+        cstride = m.c_ld;
+        const int na = m.na;
+        if (rv) {
+#pragma unroll
+          for (int cl = 0; cl < HCH; ++cl) {
+            const int col = (c0 + cl) * 8;
+            if (cl < nchh) {
+#pragma unroll
+              for (int jj = 0; jj < 8; ++jj) {
+                const int n = col + jj;
+                if (n < it.ncols) {
+                  if (!it.init) {
+                    old[cl * 8 + jj] = dst[(int64_t)n * cstride];
+                  } else {
+                    double a0 = 0.0;
+                    for (int a = 0; a < min(na, OZ_META_AX); ++a)
+                      a0 += m.ax_coef[a] * p.psi[m.ax_off[a] + (int64_t)n * m.ax_ld[a] + r];
+                    old[cl * 8 + jj] = a0;
+                  }
+                }
+              }
+            }
+          }
+          if (it.init && na > OZ_META_AX) {
+            const OzCell c = p.cells[it.cell];
+            for (int a = c.a_begin + OZ_META_AX; a < c.a_end; ++a) {
+              const Task t = p.tasks[a];
+#pragma unroll
+              for (int cl = 0; cl < HCH; ++cl) {
+                const int col = (c0 + cl) * 8;
+                if (cl < nchh)
+#pragma unroll
+                  for (int jj = 0; jj < 8; ++jj)
+                    if (col + jj < it.ncols)
+                      old[cl * 8 + jj] +=
+                          t.coef * p.psi[t.L.off + (int64_t)(it.col0 + col + jj) * t.L.ld + it.row0 + r];
+              }
+            }
           }
         }
-        cstride = 1;
+      } else {
+        const int64_t d = m.dst[rr];
+        rv = rv && d >= 0;
+        dst = rv ? p.scr + d : nullptr;
       }
       // this half of the tile row, summed over the item's families
-      constexpr int HCH = (BN / 8 + 1) / 2;   // most 8-column chunks of a half
       double accv[HCH * 8];
 #pragma unroll
       for (int j = 0; j < HCH * 8; ++j) accv[j] = 0.0;
       for (int f = 0; f < nf; ++f) {
         const uint32_t buf = famc & 1u, use = famc >> 1;
-        double rscale;
-        int64_t cs_idx;
-        if (it.kind == 0) {
-          const OzFam fm = p.fams[it.fam_begin + f];
-          rscale = rv ? oz_pow2_of(p.scales[fm.rs_idx + it.row0 + r]) : 0.0;
-          cs_idx = fm.cs_idx + it.col0;
-        } else {
-          rscale = rscale_stack;
-          cs_idx = it.cs_idx;
-        }
-        // column scales of this family (once per tile); thread 0 waits for the
-        // accumulators and the named barrier hands its verdict to all epilogue threads
-        asm volatile("bar.sync 1, 256;" ::: "memory");
-        if (tid < it.ncols) cscale_sh[tid] = oz_pow2_of(p.scales[cs_idx + tid]);
-        if (tid == 0) {
-          const bool got = oz_wait(oz_smem(&tfull_bar[buf]), use & 1u, &abort_sh);
-          if (!got && !abort_sh) oz_fail(&abort_sh, p.err);
-          tfull_ok_sh = got ? 1 : 0;
-        }
-        asm volatile("bar.sync 1, 256;" ::: "memory");
-        if (!tfull_ok_sh) {
+        const double rscale = rv ? m.rs[f][rr] : 0.0;
+        if (!oz_wait(oz_smem(&tfull_bar[buf]), use & 1u, &abort_sh)) {
+          if (!abort_sh) oz_fail(&abort_sh, p.err);
           ok = false;
           break;
         }
@@ -595,7 +699,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
               double acc = 0.0;
 #pragma unroll
               for (int d = S - 1; d >= 0; --d) acc += (double)(int32_t)v[d][jj] * w[d];
-              accv[cl * 8 + jj] += acc * rscale * cscale_sh[col + jj];
+              accv[cl * 8 + jj] += acc * rscale * m.cs[f][min(col + jj, BN - 1)];
             }
           }
         }
@@ -604,43 +708,21 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
         ++famc;
       }
       if (!ok) break;
-      // store this half of the tile row once: loads of an 8-column chunk first, then the stores
-      if (it.kind == 0) {
+      oz_arrive(oz_smem(&meta_empty[slot]));   // the slot's data is in registers now
+      // store this half of the tile row
 #pragma unroll
-        for (int cl = 0; cl < HCH; ++cl) {
-          const int col = (c0 + cl) * 8;
-          if (rv && cl < nchh && col < it.ncols) {
-            double old[8];
+      for (int cl = 0; cl < HCH; ++cl) {
+        const int col = (c0 + cl) * 8;
+        if (rv && cl < nchh) {
 #pragma unroll
-            for (int jj = 0; jj < 8; ++jj) {
-              const int n = col + jj;
-              old[jj] = 0.0;
-              if (n < it.ncols) {
-                if (it.init) {
-                  for (int a = c.a_begin; a < c.a_end; ++a) {
-                    const Task &t = p.tasks[a];
-                    old[jj] += t.coef * p.psi[t.L.off + (int64_t)(it.col0 + n) * t.L.ld + it.row0 + r];
-                  }
-                } else {
-                  old[jj] = dst[(int64_t)n * cstride];
-                }
-              }
+          for (int jj = 0; jj < 8; ++jj) {
+            const int n = col + jj;
+            if (n < it.ncols) {
+              if (it.kind == 0)
+                dst[(int64_t)n * cstride] = old[cl * 8 + jj] + accv[cl * 8 + jj];
+              else
+                dst[n] = accv[cl * 8 + jj];
             }
-#pragma unroll
-            for (int jj = 0; jj < 8; ++jj) {
-              const int n = col + jj;
-              if (n < it.ncols) dst[(int64_t)n * cstride] = old[jj] + accv[cl * 8 + jj];
-            }
-          }
-        }
-      } else {
-#pragma unroll
-        for (int cl = 0; cl < HCH; ++cl) {
-          const int col = (c0 + cl) * 8;
-          if (rv && cl < nchh) {
-#pragma unroll
-            for (int jj = 0; jj < 8; ++jj)
-              if (col + jj < it.ncols) dst[col + jj] = accv[cl * 8 + jj];
           }
         }
       }

@@ -522,6 +522,12 @@ struct Builder {
         if (t.R.space == SP_NONE) continue;
         (t.L.space == SP_SCR ? oz.flops2 : oz.flops1) += 2.0 * c.M * c.N * (double)t.K;
       }
+    // the epilogue stages at most two families of a cell item and 16 stacked
+    // runs of a product item
+    for (const std::vector<OzItem> *v : {&oz.items1, &oz.items2})
+      for (const OzItem &it : *v)
+        if ((it.kind == 0 && it.fam_end - it.fam_begin > 2) || (it.kind == 1 && it.fam_end - it.fam_begin > 16))
+          throw std::runtime_error("work item with too many families or stacked runs");
     // exact int32 accumulation: a diagonal sums <= s slice products of 127^2 per k
     if ((double)kmax * S * 127.0 * 127.0 >= 2147483647.0)
       throw std::runtime_error("inner dimension too large for int32 accumulation");
