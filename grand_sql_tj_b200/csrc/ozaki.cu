@@ -575,14 +575,20 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
   } else {
     // ------------------------------------------------ epilogue (warps 0-7, named barrier 1)
     uint32_t famc = 0, icount = 0;
-    double w[S];
-    {
-      double x = 1.0 / 16384.0;   // 128^-2
+    // diagonal d carries weight 128^-(d+2).  The diagonals are combined
+    // exactly in 64-bit integers, in groups of at most five (|D_d| < 2^31, so
+    // a group sum_d D_d 128^(g1-1-d) stays below 2^59), and each group is
+    // converted once: weight of the group ending at g1 is 128^-(g1+1)
+    constexpr int NG = (S + 4) / 5;
+    double wg[NG];
 #pragma unroll
-      for (int d = 0; d < S; ++d) {
-        w[d] = x;
-        x *= 1.0 / 128.0;
-      }
+    for (int g = 0; g < NG; ++g) {
+      const int g1 = min(S, 5 * g + 5);
+      double x = 1.0;
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        if (i <= g1) x *= 1.0 / 128.0;
+      wg[g] = x;
     }
     bool ok = true;
     constexpr int HCH = (BN / 8 + 1) / 2;   // most 8-column chunks of a half
@@ -698,7 +704,12 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
             for (int jj = 0; jj < 8; ++jj) {
               double acc = 0.0;
 #pragma unroll
-              for (int d = S - 1; d >= 0; --d) acc += (double)(int32_t)v[d][jj] * w[d];
+              for (int g = 0; g < NG; ++g) {
+                long long q = 0;
+#pragma unroll
+                for (int d = 5 * g; d < min(S, 5 * g + 5); ++d) q = q * 128 + (long long)(int32_t)v[d][jj];
+                acc += (double)q * wg[g];
+              }
               accv[cl * 8 + jj] += acc * rscale * m.cs[f][min(col + jj, BN - 1)];
             }
           }

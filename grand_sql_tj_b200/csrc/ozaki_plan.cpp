@@ -553,8 +553,10 @@ struct Builder {
 
   // Longest-processing-time-first: items by decreasing estimated time, each
   // to the least loaded CTA; then each CTA's items are made contiguous.
-  // Estimated time of an item: bytes it streams through shared memory
-  // (row groups of A and B per k-block) plus a fixed epilogue share.
+  // Estimated time of an item: a fixed cost per k-block (the ring of stages is
+  // latency-bound, not byte-bound: measured on the B200, an item takes about
+  // 0.42 us per k-block whatever its tile size) plus about four k-blocks'
+  // worth per item (pipeline hand-over and epilogue).
   void schedule(std::vector<OzItem> &v, std::vector<int32_t> &cta) {
     const int n = (int)v.size();
     if (n == 0) {
@@ -562,9 +564,7 @@ struct Builder {
       return;
     }
     const int nb = std::min(oz.nsm, n);
-    auto est = [](const OzItem &it) {
-      return (int64_t)it.nkb * ((it.mrows + 7) / 8 + (it.ncols + 7) / 8) + 24;
-    };
+    auto est = [](const OzItem &it) { return (int64_t)it.nkb + 4; };
     std::stable_sort(v.begin(), v.end(), [&](const OzItem &a, const OzItem &b) { return est(a) > est(b); });
     std::vector<int64_t> load(nb, 0);
     std::vector<std::vector<int>> bins(nb);
