@@ -54,14 +54,14 @@ struct tj_ctx {
   tjb::DevBuf corCells, corTasks, corTiles, corOps, corScr, corPsi;   // correlators
   // split-precision H*psi
   std::unique_ptr<tjb::OzPlan> oz;
-  tjb::DevBuf ozPack, ozScales, ozStaJobs, ozPsiJobs, ozProdJobs, ozSegs, ozFams, ozStacks, ozCells, ozItems1,
+  tjb::DevBuf ozPack, ozScales, ozStaJobs, ozPsiJobs, ozProdJobs, ozSegs, ozFams, ozCells, ozItems1,
       ozItems2, ozCta1, ozCta2, ozStaSpans, ozPsiSpans, ozProdSpans, ozStaMSpans,
       ozPsiMSpans, ozProdMSpans, ozStaMJobs, ozPsiMJobs, ozProdMJobs, ozMisc;
   std::vector<tjb::DevBuf *> all_bufs() {
     return {&ops, &scr, &vin, &vout, &counters, &partials, &cells1, &cells2, &tasks1, &tasks2, &tiles1,
             &tiles2, &red1, &red2, &slots, &m_dst, &m_n, &m_sb, &m_se, &m_src, &m_coef, &lanV, &lanScal, &lanPart, &trA, &trB,
             &trC, &trD, &trE, &corCells, &corTasks, &corTiles, &corOps, &corScr, &corPsi, &ozPack, &ozScales,
-            &ozStaJobs, &ozPsiJobs, &ozProdJobs, &ozSegs, &ozFams, &ozStacks, &ozCells, &ozItems1, &ozItems2,
+            &ozStaJobs, &ozPsiJobs, &ozProdJobs, &ozSegs, &ozFams, &ozCells, &ozItems1, &ozItems2,
             &ozCta1, &ozCta2, &ozStaSpans, &ozPsiSpans, &ozProdSpans, &ozStaMSpans,
             &ozPsiMSpans, &ozProdMSpans, &ozStaMJobs, &ozPsiMJobs, &ozProdMJobs, &ozMisc};
   }

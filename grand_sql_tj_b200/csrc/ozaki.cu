@@ -10,7 +10,9 @@
 //                                       pair p + q <= s + 1 into the TMEM
 //                                       accumulator of diagonal p + q (two TMEM
 //                                       buffers, one family each)
-//                    warps 0-3          read the diagonals back (tcgen05.ld),
+//                    warp 10            stages each item's scales and output
+//                                       addresses in shared memory ahead of it
+//                    warps 0-7          read the diagonals back (tcgen05.ld),
 //                                       weight them by 128^-d, scale by the row
 //                                       and column scales and add into the FP64
 //                                       output tile (products: store P and raise
@@ -167,7 +169,6 @@ struct OzGemmParams {
   const int32_t *cta;   // CTA b runs items [cta[b], cta[b+1])
   const OzSeg *segs;
   const OzFam *fams;
-  const OzStack *stacks;
   const OzCell *cells;
   const Task *tasks;
   const uint8_t *pack;
@@ -268,15 +269,14 @@ struct OzCfg {
 
 // Per-item data of the epilogue, staged in shared memory by the metadata warp
 // ahead of the item's accumulators: power-of-two column scales and row scales
-// of each family (at most two per item), and where each tile row goes.
+// of each family (at most two per item), the output tile and the axpy terms.
 constexpr int OZ_META = 4;       // ring slots
 constexpr int OZ_META_AX = 4;    // axpy terms held per cell (more are read from global memory)
 template <int BN>
 struct OzMeta {
   double cs[2][BN];
   double rs[2][128];
-  int64_t dst[128];              // products: offset of P(row's column, col0) in scr; -1: nothing to store
-  int64_t c_off;                 // cells: offset of (row0, col0) in out
+  int64_t c_off;                 // offset of the tile's (row0, col0) in out (cells) or scr (products)
   int32_t c_ld, na;              // cells: leading dimension; axpy terms (init items)
   double ax_coef[OZ_META_AX];
   int64_t ax_off[OZ_META_AX];    // psi offset of the axpy operand's (row0, col0)
@@ -301,10 +301,9 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
   // so that no role waits on a global load at an item boundary
   constexpr int OZ_ICACHE = 64;
   __shared__ OzItem item_sh[OZ_ICACHE];
-  __shared__ OzSeg seg1_sh[OZ_ICACHE];
   __shared__ OzMeta<BN> meta[OZ_META];
   __shared__ __align__(8) uint64_t meta_full[OZ_META], meta_empty[OZ_META];
-  static_assert(C::SMEM + sizeof(OzMeta<BN>) * OZ_META + OZ_ICACHE * (sizeof(OzItem) + sizeof(OzSeg)) + 2048 <=
+  static_assert(C::SMEM + sizeof(OzMeta<BN>) * OZ_META + OZ_ICACHE * sizeof(OzItem) + 2048 <=
                     232448,
                 "shared memory above 227 KB");
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -327,10 +326,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
     abort_sh = 0;
   }
   const int ib = p.cta[blockIdx.x], ie_cta = p.cta[blockIdx.x + 1];
-  for (int i = tid; i < min(ie_cta - ib, OZ_ICACHE); i += blockDim.x) {
-    item_sh[i] = p.items[ib + i];
-    if (item_sh[i].kind == 1) seg1_sh[i] = p.segs[item_sh[i].seg];
-  }
+  for (int i = tid; i < min(ie_cta - ib, OZ_ICACHE); i += blockDim.x) item_sh[i] = p.items[ib + i];
   auto get_item = [&](int ii) -> OzItem { return ii - ib < OZ_ICACHE ? item_sh[ii - ib] : p.items[ii]; };
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(oz_smem(&tmem_sh)),
@@ -374,30 +370,13 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       const uint32_t ga = (uint32_t)((it.mrows + 7) >> 3), gb = (uint32_t)(it.N >> 3);
       const int64_t ta = it.row0 / 128, tb = it.col0 / BN;
       const uint32_t bytes = (ga + gb) * GB;
-      int fb0, fe0;
-      if (it.kind == 1) {
-        fb0 = fe0 = -1;
-      } else {
-        fb0 = it.fam_begin;
-        fe0 = it.fam_end;
-      }
-      for (int f = fb0; (it.kind == 1 ? f == -1 : f < fe0) && ok; ++f) {
-        int sb, se;
-        if (it.kind == 1) {
-          sb = it.seg;
-          se = it.seg + 1;
-        } else {
-          const OzFam fm = p.fams[f];
-          sb = fm.seg_begin;
-          se = fm.seg_end;
-        }
+      for (int f = it.fam_begin; f < it.fam_end && ok; ++f) {
+        const OzFam fm = p.fams[f];
+        const int sb = fm.seg_begin, se = fm.seg_end;
         for (int s0 = sb; s0 < se && ok; s0 += 32) {
           // the next <= 32 segments, one per lane
           OzSeg mine;
-          if (it.kind == 1 && ii - ib < OZ_ICACHE)
-            mine = seg1_sh[ii - ib];
-          else if (s0 + lane < se)
-            mine = p.segs[s0 + lane];
+          if (s0 + lane < se) mine = p.segs[s0 + lane];
           const int cnt = min(32, se - s0);
           for (int j = 0; j < cnt && ok; ++j) {
             const int64_t a_base = __shfl_sync(0xffffffffu, mine.a_base, j);
@@ -422,7 +401,6 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
             }
           }
         }
-        if (it.kind == 1) break;
       }
     }
     // copies still in flight land before the CTA exits
@@ -446,9 +424,9 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
 #pragma unroll
         for (int pa = 1; pa <= S; ++pa) idesc[pa - 1] = oz_idesc(it.M, (S + 1 - pa) * it.N);
         const uint32_t aslice16 = (uint32_t)((it.mrows + 7) >> 3) * 16u;   // A slice stride in 16-byte units
-        const int nf = it.kind == 1 ? 1 : it.fam_end - it.fam_begin;
+        const int nf = it.fam_end - it.fam_begin;
         for (int f = 0; f < nf && ok; ++f) {
-          const int nkb = it.kind == 1 ? it.nkb : p.fams[it.fam_begin + f].nkb;
+          const int nkb = p.fams[it.fam_begin + f].nkb;
           const uint32_t buf = famc & 1u, use = famc >> 1;
           if (!oz_wait(oz_smem(&tempty_bar[buf]), (use & 1u) ^ 1u, &abort_sh)) {
             if (!abort_sh) oz_fail(&abort_sh, p.err);
@@ -508,66 +486,24 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       }
       if (!__shfl_sync(0xffffffffu, good, 0)) break;
       OzMeta<BN> &m = meta[slot];
-      if (it.kind == 1) {
-        // stacked runs (at most 16): the run holding each tile row, its P
-        // destination and the tau scale of the X column it came from
-        const int np = it.fam_end - it.fam_begin;
-        OzStack sk{};
-        int ng = 0;
-        if (lane < np) {
-          sk = p.stacks[it.fam_begin + lane];
-          ng = sk.a_ng;
-        }
-        int incl = ng * 8;
-        for (int o = 1; o < 32; o <<= 1) {
-          const int t = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += t;
-        }
-        const int start = incl - ng * 8;
-        for (int j = lane; j < it.ncols; j += 32) m.cs[0][j] = oz_pow2_of(p.scales[it.cs_idx + j]);
-        int64_t rdst[4] = {-1, -1, -1, -1}, ridx[4] = {0, 0, 0, 0};
-        for (int q = 0; q < np; ++q) {
-          const int s0 = __shfl_sync(0xffffffffu, start, q);
-          const int e0 = s0 + 8 * __shfl_sync(0xffffffffu, ng, q);
-          const int64_t d0 = __shfl_sync(0xffffffffu, sk.dst_off, q);
-          const int64_t x0 = __shfl_sync(0xffffffffu, sk.rs_idx, q);
-          const int ld = __shfl_sync(0xffffffffu, sk.dst_ld, q);
-          const int nc = __shfl_sync(0xffffffffu, sk.ncols, q);
-#pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            const int r = lane + 32 * t;
-            if (r >= s0 && r < e0 && r - s0 < nc) {
-              rdst[t] = d0 + (int64_t)(r - s0) * ld + it.col0;
-              ridx[t] = x0 + (r - s0);
-            }
-          }
-        }
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const int r = lane + 32 * t;
-          m.dst[r] = rdst[t];
-          m.rs[0][r] = rdst[t] >= 0 ? oz_pow2_of(p.scales[ridx[t]]) : 0.0;
-        }
-      } else {
-        const int nf = it.fam_end - it.fam_begin;   // at most 2 (checked by the plan)
-        for (int f = 0; f < nf; ++f) {
-          const OzFam fm = p.fams[it.fam_begin + f];
-          for (int j = lane; j < it.ncols; j += 32) m.cs[f][j] = oz_pow2_of(p.scales[fm.cs_idx + it.col0 + j]);
-          for (int r = lane; r < it.mrows; r += 32) m.rs[f][r] = oz_pow2_of(p.scales[fm.rs_idx + it.row0 + r]);
-        }
-        const OzCell c = p.cells[it.cell];
-        const int na = it.init ? c.a_end - c.a_begin : 0;
-        if (lane == 0) {
-          m.c_off = c.off + it.row0 + (int64_t)it.col0 * c.ld;
-          m.c_ld = c.ld;
-          m.na = na;
-        }
-        if (lane < min(na, OZ_META_AX)) {
-          const Task t = p.tasks[c.a_begin + lane];
-          m.ax_coef[lane] = t.coef;
-          m.ax_off[lane] = t.L.off + (int64_t)it.col0 * t.L.ld + it.row0;
-          m.ax_ld[lane] = t.L.ld;
-        }
+      const int nf = it.fam_end - it.fam_begin;   // at most 2 (checked by the plan)
+      for (int f = 0; f < nf; ++f) {
+        const OzFam fm = p.fams[it.fam_begin + f];
+        for (int j = lane; j < it.ncols; j += 32) m.cs[f][j] = oz_pow2_of(p.scales[fm.cs_idx + it.col0 + j]);
+        for (int r = lane; r < it.mrows; r += 32) m.rs[f][r] = oz_pow2_of(p.scales[fm.rs_idx + it.row0 + r]);
+      }
+      const OzCell c = p.cells[it.cell];
+      const int na = it.init ? c.a_end - c.a_begin : 0;
+      if (lane == 0) {
+        m.c_off = c.off + it.row0 + (int64_t)it.col0 * c.ld;
+        m.c_ld = c.ld;
+        m.na = na;
+      }
+      if (lane < min(na, OZ_META_AX)) {
+        const Task t = p.tasks[c.a_begin + lane];
+        m.ax_coef[lane] = t.coef;
+        m.ax_off[lane] = t.L.off + (int64_t)it.col0 * t.L.ld + it.row0;
+        m.ax_ld[lane] = t.L.ld;
       }
       oz_arrive(oz_smem(&meta_full[slot]));   // every lane: release of its own writes
     }
@@ -607,11 +543,10 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
         r = quarter * 16 + lane;
         rv = lane < 16 && r < it.mrows;
       }
-      const int rr = min(r, 127);
       // this half's 8-column chunks: [c0, c0 + nchh)
       const int nch = it.N >> 3, hch = (nch + 1) >> 1;
       const int c0 = half * hch, nchh = min(hch, nch - c0);
-      const int nf = it.kind == 1 ? 1 : it.fam_end - it.fam_begin;
+      const int nf = it.fam_end - it.fam_begin;
       const int slot = (int)(icount % OZ_META);
       if (!oz_wait(oz_smem(&meta_full[slot]), (icount / OZ_META) & 1u, &abort_sh)) {
         if (!abort_sh) oz_fail(&abort_sh, p.err);
@@ -619,16 +554,14 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
         break;
       }
       const OzMeta<BN> &m = meta[slot];
-      double *dst = nullptr;
-      int64_t cstride = 1;
+      double *const dst = (it.kind == 0 ? p.out : p.scr) + m.c_off + r;
+      const int64_t cstride = m.c_ld;
       // the values the tile is added to, loaded before the accumulators are
       // waited for: the old H*psi (cells of launch 2) or the axpy terms (init)
       double old[HCH * 8];
 #pragma unroll
       for (int j = 0; j < HCH * 8; ++j) old[j] = 0.0;
       if (it.kind == 0) {
-        dst = p.out + m.c_off + r;
-        cstride = m.c_ld;
         const int na = m.na;
         if (rv) {
 #pragma unroll
@@ -668,10 +601,6 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
             }
           }
         }
-      } else {
-        const int64_t d = m.dst[rr];
-        rv = rv && d >= 0;
-        dst = rv ? p.scr + d : nullptr;
       }
       // this half of the tile row, summed over the item's families
       double accv[HCH * 8];
@@ -679,7 +608,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       for (int j = 0; j < HCH * 8; ++j) accv[j] = 0.0;
       for (int f = 0; f < nf; ++f) {
         const uint32_t buf = famc & 1u, use = famc >> 1;
-        const double rscale = rv ? m.rs[f][rr] : 0.0;
+        const double rscale = rv ? m.rs[f][r] : 0.0;
         if (!oz_wait(oz_smem(&tfull_bar[buf]), use & 1u, &abort_sh)) {
           if (!abort_sh) oz_fail(&abort_sh, p.err);
           ok = false;
@@ -720,7 +649,8 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       }
       if (!ok) break;
       oz_arrive(oz_smem(&meta_empty[slot]));   // the slot's data is in registers now
-      // store this half of the tile row
+      // store this half of the tile row (products: and raise pi with the row's maximum)
+      double rmax = 0.0;
 #pragma unroll
       for (int cl = 0; cl < HCH; ++cl) {
         const int col = (c0 + cl) * 8;
@@ -729,14 +659,15 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
           for (int jj = 0; jj < 8; ++jj) {
             const int n = col + jj;
             if (n < it.ncols) {
-              if (it.kind == 0)
-                dst[(int64_t)n * cstride] = old[cl * 8 + jj] + accv[cl * 8 + jj];
-              else
-                dst[n] = accv[cl * 8 + jj];
+              const double v = old[cl * 8 + jj] + accv[cl * 8 + jj];
+              dst[(int64_t)n * cstride] = v;
+              rmax = fmax(rmax, fabs(v));
             }
           }
         }
       }
+      if (it.kind == 1 && rmax > 0.0)
+        atomicMax((unsigned long long *)&p.scales[it.pi_idx + r], (unsigned long long)__double_as_longlong(rmax));
     }
   }
   __syncthreads();
@@ -777,11 +708,11 @@ static cudaError_t launch_gemm_t(const OzGemmParams &p, int ncta, cudaStream_t s
 }
 
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
-                           const OzStack *stacks, const OzCell *cells, const Task *tasks, const uint8_t *pack,
+                           const OzCell *cells, const Task *tasks, const uint8_t *pack,
                            double *scales, const double *psi, double *scr, double *out, int *err, int s,
                            cudaStream_t st) {
   if (ncta <= 0) return cudaSuccess;
-  OzGemmParams p{items, cta, segs, fams, stacks, cells, tasks, pack, scales, psi, scr, out, err};
+  OzGemmParams p{items, cta, segs, fams, cells, tasks, pack, scales, psi, scr, out, err};
   switch (s) {
     case 3: return launch_gemm_t<3, 48>(p, ncta, st);
     case 4: return launch_gemm_t<4, 48>(p, ncta, st);

@@ -23,9 +23,11 @@
 //                                             scaled per sys basis state (pi)
 //                                          B: per-cell concat (static)
 //
-// Phase-1 products P_t = op(A_t) X_t are computed first with the rows of
-// P_t^T (columns of X_t, scale tau) stacked across products that share
-// op(A_t); their epilogue stores P in FP64 and raises pi.
+// Phase-1 products P_t = op(A_t) X_t are computed first, each as a family of
+// one segment: A = the split of op(A_t) (static, own row scales, shared by
+// every product of the operator), B = the column split of X_t (tau, shared
+// with the left families); their epilogue stores P in FP64 and raises pi,
+// the row maxima of P per sys basis state, with one atomic maximum per row.
 //
 // Split storage ("pack" pools, bytes): a split of `rows` x K is cut into
 // tiles of R rows (R = 128 for an A operand, R = BN for a B operand) and
@@ -92,39 +94,30 @@ struct OzFam {
   int32_t pad;
 };
 
-// A run of stacked rows of a product tile: rows of P^T = columns
-// [8*a_g0, 8*a_g0 + ncols) of X_t, held as a_ng row groups of the tile's
-// stack split (written there by a split job of X_t's columns).
-struct OzStack {
-  int64_t dst_off;          // P_t(0, 8*a_g0) in the product space
-  int64_t rs_idx;           // tau index of X_t's column 8*a_g0
-  int32_t a_g0, a_ng;
-  int32_t dst_ld;
-  int32_t ncols;            // valid rows of this run
-};
-
 // A work item: the output tile rows [row0, row0 + M) x cols [col0, col0 + N)
-//   kind 0 (cell):  of phase-2 cell `cell`; families [fam_begin, fam_end);
-//                   init = 1: the tile is written (axpy terms or zero), then
-//                   every family is added; init = 0: families are added
-//   kind 1 (stack): of the products stacked in [fam_begin, fam_end) of the
-//                   stack list; segment `seg` pairs the tile's stack split
-//                   (A) with the shared operator's split (B)
+// of cell `cell` (an entry of the cell list), families [fam_begin, fam_end)
+// (at most two):
+//   kind 0 (H*psi cell):  init = 1: the tile is written (axpy terms or
+//                         zero), then every family is added; init = 0: the
+//                         families are added to the tile
+//   kind 1 (product P_t): the tile is stored, and the maximum |P| of each
+//                         tile row raises the pi scale scales[pi_idx + row]
 struct OzItem {
   int32_t kind, cell;
   int32_t row0, col0;
   int32_t M, N;             // M in {64, 128}; N multiple of 16, <= oz_bn(s)
   int32_t mrows, ncols;     // valid rows / columns
   int32_t fam_begin, fam_end;
-  int32_t seg;              // kind 1: the segment of the shared operator
+  int32_t pad1;
   int32_t init;
-  int64_t cs_idx;           // kind 1: scale index of the operator's row 0
+  int64_t pi_idx;           // kind 1: pi index of tile row 0
   int32_t nkb;              // k-blocks of all its families
   int32_t pad2;
   int64_t cost;             // issued int8 MACs (for ordering)
 };
 
-// Output cell of kind-0 items (phase-2 cell) with its axpy tasks.
+// Output cell of the items: a phase-2 cell of H*psi (in the output vector)
+// with its axpy tasks, or a phase-1 product (in the product space, no axpy).
 struct OzCell {
   int64_t off;
   int32_t ld, M, N;
@@ -160,7 +153,6 @@ struct OzPlan {
   // GEMM tables
   std::vector<OzSeg> segs;
   std::vector<OzFam> fams;
-  std::vector<OzStack> stacks;
   std::vector<OzCell> cells;
   std::vector<OzItem> items1, items2;      // launch 1 (products, left, right), launch 2 (two-sided)
   // static schedule: CTA b of a launch runs items [cta[b], cta[b+1]) in order
@@ -181,7 +173,7 @@ void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans
 void launch_oz_split(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
                      const double *psi, const double *scr, const double *scales, uint8_t *pack, int s, cudaStream_t st);
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
-                           const OzStack *stacks, const OzCell *cells, const Task *tasks, const uint8_t *pack,
+                           const OzCell *cells, const Task *tasks, const uint8_t *pack,
                            double *scales, const double *psi, double *scr, double *out, int *err, int s,
                            cudaStream_t st);
 

@@ -5,9 +5,10 @@
 //   once per step   sta_jobs: operator splits (phase-1 operators, per-cell
 //                   concatenations of coef * op(.)), with their own row scales
 //   per H*psi       zero rho/tau/pi; psi_jobs (max, then split): psi column
-//                   splits (tau) and row splits (rho); launch 1 (products,
-//                   left and right families); prod_jobs: product row splits
-//                   (pi, raised by launch 1); launch 2 (two-sided families)
+//                   splits (tau) and row splits (rho), one of each per psi
+//                   cell; launch 1 (products, left and right families; the
+//                   product epilogue raises pi); prod_jobs: product row
+//                   splits; launch 2 (two-sided families)
 #include <algorithm>
 #include <cstring>
 #include <map>
@@ -122,19 +123,6 @@ struct Builder {
     if (it == psi_cell.end()) throw std::runtime_error("psi operand is not a cell");
     return it->second;
   }
-  // tau of psi cell c's columns: from its column split's job, or from a
-  // maximum-only job when the cell is only stacked (one job per cell)
-  std::vector<char> tau_job;
-  void tau_of(int c) {
-    if (tau_job[c]) return;
-    tau_job[c] = 1;
-    const Cell &x = hp.cells2[c];
-    const Tiling t = tiling(x.N, x.M, true);
-    OzJob j = job(SP_PSI, x.off, x.ld, 1, x.N, x.M, 1.0, 0, t, 0, t.gsum, 0, hp.cell2_col_state[c], true);
-    j.want_split = 0;
-    dyn_psi.push_back(j);
-    dyn_psi_rel.push_back(REL_TAU);
-  }
   // psi cell c as a B operand: rows = its columns (scale tau), K = its rows
   int64_t psi_col(int c) {
     if (colsplit[c] < 0) {
@@ -142,9 +130,8 @@ struct Builder {
       const Tiling t = tiling(x.N, x.M, true);
       colsplit[c] = alloc_dyn(t);
       dyn_psi.push_back(job(SP_PSI, x.off, x.ld, 1, x.N, x.M, 1.0, colsplit[c], t, 0, t.gsum, 0,
-                            hp.cell2_col_state[c], !tau_job[c]));
+                            hp.cell2_col_state[c], true));
       dyn_psi_rel.push_back(REL_TAU);
-      tau_job[c] = 1;
     }
     return colsplit[c];
   }
@@ -160,14 +147,15 @@ struct Builder {
     }
     return rowsplit[c];
   }
-  // phase-1 product p as an A operand: rows = its rows (scale pi), K = its columns
+  // phase-1 product p as an A operand: rows = its rows (scale pi, raised by
+  // the product's epilogue in launch 1), K = its columns
   int64_t prod_row(int p) {
     if (prodsplit[p] < 0) {
       const Cell &P = hp.cells1[p];
       const Tiling t = tiling(P.M, P.N, false);
       prodsplit[p] = alloc_dyn(t);
       dyn_prod.push_back(job(SP_SCR, P.off, 1, P.ld, P.M, P.N, 1.0, prodsplit[p], t, 0, t.gsum, 0,
-                             hp.cell1_row_state[p], true));
+                             hp.cell1_row_state[p], false));
     }
     return prodsplit[p];
   }
@@ -176,9 +164,10 @@ struct Builder {
     return (int64_t)it.M * it.N * 32 * kbs * (S * (S + 1) / 2);
   }
 
-  // Phase-1 products P_t = op(A_t) X_t, grouped by operator: the columns of
-  // the X_t (rows of P_t^T, scale tau) are stacked into 128-row tiles, each
-  // tile a split of its own written by one job per run.
+  // Phase-1 products P_t = op(A_t) X_t: per operator one static split of
+  // op(A_t) (A role, own row scales), shared by all its products; each
+  // product is a family of one segment with the column split of X_t (B role,
+  // tau) and its own output cell (the product in the scratch space).
   void products() {
     const int BN = oz.bn;
     std::map<std::pair<int64_t, int>, std::vector<int>> by_op;
@@ -196,17 +185,10 @@ struct Builder {
       const int32_t Mop = c0.M, K = t0.K;
       int32_t rs, ks;
       strides(t0.L, 0, rs, ks);
-      const Tiling tb = tiling(Mop, K, true);
-      const int64_t pk = alloc_sta(tb);
+      const Tiling ta = tiling(Mop, K, false);
+      const int64_t pk = alloc_sta(ta);
       const int64_t sc = alloc_scales(Mop);
-      oz.sta_jobs.push_back(job(SP_OPS, t0.L.off, rs, ks, Mop, K, 1.0, pk, tb, 0, tb.gsum, 0, sc, true));
-      // runs of <= 16 row groups: columns of the operands
-      struct Run {
-        OzStack st;
-        int x;   // psi cell
-        int p;   // product
-      };
-      std::vector<Run> runs;
+      oz.sta_jobs.push_back(job(SP_OPS, t0.L.off, rs, ks, Mop, K, 1.0, pk, ta, 0, ta.gsum, 0, sc, true));
       for (int p : prods) {
         const Cell &c = hp.cells1[p];
         const Task &t = hp.tasks1[c.t_begin];
@@ -214,73 +196,51 @@ struct Builder {
         const int x = psi_index(t.R);
         const Cell &X = hp.cells2[x];
         if (X.M != K || X.N != c.N) throw std::runtime_error("product operand shape");
-        const int32_t G = cdiv(X.N, 8);
-        for (int32_t g0 = 0; g0 < G; g0 += 16) {
-          Run r;
-          std::memset(&r.st, 0, sizeof r.st);
-          r.x = x;
-          r.p = p;
-          r.st.a_g0 = g0;
-          r.st.a_ng = std::min(16, G - g0);
-          r.st.dst_off = c.off + (int64_t)8 * g0 * c.ld;
-          r.st.dst_ld = c.ld;
-          r.st.ncols = std::min(8 * r.st.a_ng, X.N - 8 * g0);
-          r.st.rs_idx = hp.cell2_col_state[x] + 8 * g0;   // tau-relative
-          runs.push_back(r);
-        }
-      }
-      size_t i = 0;
-      while (i < runs.size()) {
-        int32_t groups = 0;
-        size_t e = i;
-        while (e < runs.size() && groups + runs[e].st.a_ng <= 16) groups += runs[e++].st.a_ng;
-        // the tile's stack split (one 128-row tile) and the jobs that fill it
-        const Tiling ta = tiling(8 * groups, K, false);
-        const int64_t sk = alloc_dyn(ta);
-        const int fb = (int)oz.stacks.size();
-        int32_t off = 0;
-        for (size_t q = i; q < e; ++q) {
-          const Run &r = runs[q];
-          const Cell &X = hp.cells2[r.x];
-          oz.stacks.push_back(r.st);
-          // tau of X's columns comes from X's own maximum job (tau_of)
-          dyn_psi.push_back(job(SP_PSI, X.off + (int64_t)8 * r.st.a_g0 * X.ld, X.ld, 1, r.st.ncols, K, 1.0, sk, ta,
-                                8 * off, r.st.a_ng, 0, hp.cell2_col_state[r.x] + 8 * r.st.a_g0, false));
-          dyn_psi_rel.push_back(REL_TAU);
-          tau_of(r.x);
-          off += r.st.a_ng;
-        }
-        const int fe = (int)oz.stacks.size();
-        i = e;
         OzSeg sg;
         std::memset(&sg, 0, sizeof sg);
-        sg.a_base = sk;
+        sg.a_base = pk;
         sg.a_nkb = ta.nkb;
-        sg.b_base = pk;
-        sg.b_nkb = tb.nkb;
-        sg.nkb = tb.nkb;
-        const int seg = (int)oz.segs.size();
-        seg_dyn_a.push_back(seg);
+        sg.b_base = psi_col(x);
+        sg.b_nkb = cdiv(K, 32);
+        sg.nkb = cdiv(K, 32);
+        OzFam f;
+        std::memset(&f, 0, sizeof f);
+        f.seg_begin = (int)oz.segs.size();
+        seg_dyn_b.push_back((int)oz.segs.size());
         oz.segs.push_back(sg);
-        for (int32_t n0 = 0; n0 < Mop; n0 += BN) {
-          OzItem it;
-          std::memset(&it, 0, sizeof it);
-          it.kind = 1;
-          it.cell = -1;
-          it.row0 = 0;
-          it.col0 = n0;
-          it.mrows = groups * 8;
-          it.M = it.mrows <= 64 ? 64 : 128;
-          it.ncols = std::min(BN, Mop - n0);
-          it.N = std::min(BN, (it.ncols + 15) / 16 * 16);
-          it.fam_begin = fb;
-          it.fam_end = fe;
-          it.seg = seg;
-          it.init = 1;
-          it.cs_idx = sc + n0;
-          it.cost = item_cost(it, sg.nkb);
-          oz.items1.push_back(it);
-        }
+        f.seg_end = (int)oz.segs.size();
+        f.rs_idx = sc;
+        f.cs_idx = hp.cell2_col_state[x];
+        const int fi = (int)oz.fams.size();
+        famrel.push_back({fi, REL_NONE, REL_TAU});
+        oz.fams.push_back(f);
+        OzCell oc;
+        std::memset(&oc, 0, sizeof oc);
+        oc.off = c.off;
+        oc.ld = c.ld;
+        oc.M = c.M;
+        oc.N = c.N;
+        const int cell_idx = (int)oz.cells.size();
+        oz.cells.push_back(oc);
+        for (int32_t r0 = 0; r0 < Mop; r0 += 128)
+          for (int32_t n0 = 0; n0 < c.N; n0 += BN) {
+            OzItem it;
+            std::memset(&it, 0, sizeof it);
+            it.kind = 1;
+            it.cell = cell_idx;
+            it.row0 = r0;
+            it.col0 = n0;
+            it.mrows = std::min(128, Mop - r0);
+            it.M = it.mrows <= 64 ? 64 : 128;
+            it.ncols = std::min(BN, c.N - n0);
+            it.N = std::min(BN, (it.ncols + 15) / 16 * 16);
+            it.fam_begin = fi;
+            it.fam_end = fi + 1;
+            it.init = 0;
+            it.pi_idx = hp.cell1_row_state[p] + r0;   // made absolute in finish()
+            it.cost = item_cost(it, sg.nkb);
+            oz.items1.push_back(it);
+          }
       }
     }
   }
@@ -397,7 +357,7 @@ struct Builder {
         it.N = std::min(BN, (it.ncols + 15) / 16 * 16);
         it.fam_begin = fb;
         it.fam_end = fe;
-        it.seg = -1;
+        it.pad1 = 0;
         it.init = init;
         it.cost = item_cost(it, kbs);
         dst.push_back(it);
@@ -463,7 +423,8 @@ struct Builder {
     const int64_t base[3] = {oz.rho0, oz.tau0, oz.pi0};
     for (size_t i = 0; i < dyn_psi.size(); ++i) dyn_psi[i].scale_idx += base[dyn_psi_rel[i]];
     for (OzJob &j : dyn_prod) j.scale_idx += oz.pi0;
-    for (OzStack &r : oz.stacks) r.rs_idx += oz.tau0;
+    for (OzItem &it : oz.items1)
+      if (it.kind == 1) it.pi_idx += oz.pi0;
     for (const FamRel &fr : famrel) {
       OzFam &f = oz.fams[fr.fam];
       if (fr.rs_rel != REL_NONE) f.rs_idx += base[fr.rs_rel];
@@ -477,9 +438,7 @@ struct Builder {
     for (std::vector<OzItem> *v : {&oz.items1, &oz.items2})
       for (OzItem &it : *v) {
         it.nkb = 0;
-        if (it.kind == 1) it.nkb = oz.segs[it.seg].nkb;
-        else
-          for (int f = it.fam_begin; f < it.fam_end; ++f) it.nkb += oz.fams[f].nkb;
+        for (int f = it.fam_begin; f < it.fam_end; ++f) it.nkb += oz.fams[f].nkb;
       }
     // maximum jobs and split jobs in lists of their own, so that no kernel
     // walks over jobs it has nothing to do for
@@ -522,12 +481,12 @@ struct Builder {
         if (t.R.space == SP_NONE) continue;
         (t.L.space == SP_SCR ? oz.flops2 : oz.flops1) += 2.0 * c.M * c.N * (double)t.K;
       }
-    // the epilogue stages at most two families of a cell item and 16 stacked
-    // runs of a product item
+    // the epilogue stages at most two families of an item (an initialising
+    // cell item may have none: it writes its axpy terms or zeros)
     for (const std::vector<OzItem> *v : {&oz.items1, &oz.items2})
       for (const OzItem &it : *v)
-        if ((it.kind == 0 && it.fam_end - it.fam_begin > 2) || (it.kind == 1 && it.fam_end - it.fam_begin > 16))
-          throw std::runtime_error("work item with too many families or stacked runs");
+        if (it.fam_end - it.fam_begin > 2 || (it.fam_end <= it.fam_begin && !(it.kind == 0 && it.init)))
+          throw std::runtime_error("work item with no family to add or with more than two");
     // exact int32 accumulation: a diagonal sums <= s slice products of 127^2 per k
     if ((double)kmax * S * 127.0 * 127.0 >= 2147483647.0)
       throw std::runtime_error("inner dimension too large for int32 accumulation");
@@ -591,7 +550,6 @@ struct Builder {
     for (size_t p = 0; p < hp.cells1.size(); ++p) prod_of[hp.cells1[p].off] = (int)p;
     colsplit.assign(npsi, -1);
     rowsplit.assign(npsi, -1);
-    tau_job.assign(npsi, 0);
     prodsplit.assign(hp.cells1.size(), -1);
     products();
     cells();
@@ -614,7 +572,6 @@ void build_ozaki_plan(const HpsiPlan &hp, int s, int nsm, OzPlan &oz) {
 static_assert(sizeof(OzJob) == sizeof(tj_oz_job), "job layout");
 static_assert(sizeof(OzSeg) == sizeof(tj_oz_seg), "segment layout");
 static_assert(sizeof(OzFam) == sizeof(tj_oz_fam), "family layout");
-static_assert(sizeof(OzStack) == sizeof(tj_oz_stack), "stack layout");
 static_assert(sizeof(OzItem) == sizeof(tj_oz_item), "item layout");
 static_assert(sizeof(OzCell) == sizeof(tj_oz_cell), "cell layout");
 
@@ -654,7 +611,6 @@ extern "C" int tj_ozaki_plan_export(const tj_lattice *lat, const tj_model *sys, 
   put(out->prod_jobs, oz.prod_jobs, out->n_prod_jobs);
   put(out->segs, oz.segs, out->n_segs);
   put(out->fams, oz.fams, out->n_fams);
-  put(out->stacks, oz.stacks, out->n_stacks);
   put(out->cells, oz.cells, out->n_cells);
   put(out->items1, oz.items1, out->n_items1);
   put(out->items2, oz.items2, out->n_items2);

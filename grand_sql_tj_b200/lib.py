@@ -91,15 +91,10 @@ class OzFamC(C.Structure):
                 ("nkb", C.c_int32), ("pad_", C.c_int32)]
 
 
-class OzStackC(C.Structure):
-    _fields_ = [("dst_off", C.c_int64), ("rs_idx", C.c_int64)] + \
-               [(n, C.c_int32) for n in ("a_g0", "a_ng", "dst_ld", "ncols")]
-
-
 class OzItemC(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("kind", "cell", "row0", "col0", "M", "N", "mrows", "ncols", "fam_begin",
-                                         "fam_end", "seg", "init")] + \
-               [("cs_idx", C.c_int64), ("nkb", C.c_int32), ("pad2_", C.c_int32), ("cost", C.c_int64)]
+                                         "fam_end", "pad1_", "init")] + \
+               [("pi_idx", C.c_int64), ("nkb", C.c_int32), ("pad2_", C.c_int32), ("cost", C.c_int64)]
 
 
 class OzCellC(C.Structure):
@@ -107,7 +102,7 @@ class OzCellC(C.Structure):
 
 
 _OZ_ARRAYS = [("sta_jobs", OzJobC), ("psi_jobs", OzJobC), ("prod_jobs", OzJobC), ("segs", OzSegC),
-              ("fams", OzFamC), ("stacks", OzStackC), ("cells", OzCellC), ("items1", OzItemC), ("items2", OzItemC)]
+              ("fams", OzFamC), ("cells", OzCellC), ("items1", OzItemC), ("items2", OzItemC)]
 
 
 class OzExport(C.Structure):

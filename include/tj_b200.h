@@ -335,9 +335,9 @@ int tj_cor_plan_export(int kind, const tj_block *a, const tj_block *b, const tj_
  * |value|; want_max: the job raises it).  A segment pairs k-blocks of an A
  * split and a B split; a family sums its segments and scales by
  * scales[rs_idx + row] * scales[cs_idx + col]; an item is one output tile
- * (kind 0: of cell `cell`, families [fam_begin, fam_end); kind 1: phase-1
- * products stacked in [fam_begin, fam_end) of the stack list, segment
- * `seg`).  The plan schedules the items of each launch statically over 148
+ * of cell `cell` with families [fam_begin, fam_end) (kind 0: a cell of H*psi,
+ * added to; kind 1: a phase-1 product, stored, its row maxima raising the pi
+ * scales from scales[pi_idx]).  The plan schedules the items of each launch statically over 148
  * CTAs (the export's device-independent choice).  Two-call pattern as
  * above. */
 typedef struct tj_oz_job {
@@ -348,13 +348,9 @@ typedef struct tj_oz_job {
 } tj_oz_job;
 typedef struct tj_oz_seg { int64_t a_base, b_base; int32_t a_nkb, b_nkb, a_kb0, b_kb0, nkb, pad_; } tj_oz_seg;
 typedef struct tj_oz_fam { int32_t seg_begin, seg_end; int64_t rs_idx, cs_idx; int32_t nkb, pad_; } tj_oz_fam;
-typedef struct tj_oz_stack {
-  int64_t dst_off, rs_idx;
-  int32_t a_g0, a_ng, dst_ld, ncols;
-} tj_oz_stack;
 typedef struct tj_oz_item {
-  int32_t kind, cell, row0, col0, M, N, mrows, ncols, fam_begin, fam_end, seg, init;
-  int64_t cs_idx;
+  int32_t kind, cell, row0, col0, M, N, mrows, ncols, fam_begin, fam_end, pad1_, init;
+  int64_t pi_idx;
   int32_t nkb, pad2_;
   int64_t cost;
 } tj_oz_item;
@@ -363,11 +359,10 @@ typedef struct tj_ozaki_export {
   int32_t slices, tile_n;
   int64_t sta_pack, dyn_pack, n_scales, rho0, tau0, pi0;
   double int8_ops;
-  int64_t n_sta_jobs, n_psi_jobs, n_prod_jobs, n_segs, n_fams, n_stacks, n_cells, n_items1, n_items2;
+  int64_t n_sta_jobs, n_psi_jobs, n_prod_jobs, n_segs, n_fams, n_cells, n_items1, n_items2;
   tj_oz_job *sta_jobs, *psi_jobs, *prod_jobs;
   tj_oz_seg *segs;
   tj_oz_fam *fams;
-  tj_oz_stack *stacks;
   tj_oz_cell *cells;
   tj_oz_item *items1, *items2;
   int64_t n_cta1, n_cta2;     /* CTA b of launch k runs items [cta_k[b], cta_k[b+1]) */

@@ -116,26 +116,36 @@ class _Machine:
 
     def run_items(self, items, n, covered):
         oz = self.oz
-        S = self.S
         for ii in range(n):
             it = items[ii]
-            ga, gb = -(-it.mrows // 8), it.N // 8
             assert it.M in (64, 128) and it.mrows <= it.M and it.N % 16 == 0 and it.ncols <= it.N <= self.BN
+            assert it.fam_end - it.fam_begin <= 2
             ta, tb = it.row0 // 128, it.col0 // self.BN
+            ga, gb = -(-it.mrows // 8), it.N // 8
 
             def operands(sg):
                 A = self.tile_digits(sg.a_base, sg.a_nkb, 16, ta, ga, sg.a_kb0, sg.nkb)
                 B = self.tile_digits(sg.b_base, sg.b_nkb, self.BN // 8, tb, gb, sg.b_kb0, sg.nkb)
                 return A, B
 
+            c = oz["cells"][it.cell]
+            key = (it.cell, it.row0, it.col0)
+            assert key not in covered
+            covered.add(key)
+            rows = it.row0 + np.arange(it.mrows)
+            cols = it.col0 + np.arange(it.ncols)
+            idx = c.off + rows[:, None] + cols[None, :] * c.ld
+            tot = np.zeros((it.mrows, it.ncols))
+            for f in range(it.fam_begin, it.fam_end):
+                fm = oz["fams"][f]
+                As, Bs = zip(*[operands(oz["segs"][sgi]) for sgi in range(fm.seg_begin, fm.seg_end)])
+                A = np.concatenate(As, axis=2)[:, :it.mrows]
+                B = np.concatenate(Bs, axis=2)[:, :it.ncols]
+                acc = self.accum(A, B)
+                rs = _pow2_of(self.scales[fm.rs_idx + rows])
+                cs = _pow2_of(self.scales[fm.cs_idx + cols])
+                tot = tot + (acc * rs[:, None]) * cs[None, :]
             if it.kind == 0:
-                c = oz["cells"][it.cell]
-                key = (it.cell, it.row0, it.col0)
-                assert key not in covered
-                covered.add(key)
-                rows = it.row0 + np.arange(it.mrows)
-                cols = it.col0 + np.arange(it.ncols)
-                idx = c.off + rows[:, None] + cols[None, :] * c.ld
                 if it.init:
                     old = np.zeros((it.mrows, it.ncols))
                     tasks = self.plan["tasks2"]
@@ -145,35 +155,13 @@ class _Machine:
                         old = old + t.coef * b[t.L.off + cols[None, :] * t.L.ld + rows[:, None]]
                 else:
                     old = self.out[idx]
-                tot = np.zeros((it.mrows, it.ncols))
-                for f in range(it.fam_begin, it.fam_end):
-                    fm = oz["fams"][f]
-                    As, Bs = zip(*[operands(oz["segs"][sgi]) for sgi in range(fm.seg_begin, fm.seg_end)])
-                    A = np.concatenate(As, axis=2)[:, :it.mrows]
-                    B = np.concatenate(Bs, axis=2)[:, :it.ncols]
-                    acc = self.accum(A, B)
-                    rs = _pow2_of(self.scales[fm.rs_idx + rows])
-                    cs = _pow2_of(self.scales[fm.cs_idx + cols])
-                    tot = tot + (acc * rs[:, None]) * cs[None, :]
                 self.out[idx] = old + tot
             else:
-                A, B = operands(oz["segs"][it.seg])
-                B = B[:, :it.ncols]
-                acc = self.accum(A, B)
-                cs = _pow2_of(self.scales[it.cs_idx + np.arange(it.ncols)])
-                r0 = 0
-                for si in range(it.fam_begin, it.fam_end):
-                    sk = oz["stacks"][si]
-                    jl = np.arange(sk.ncols)
-                    rs = _pow2_of(self.scales[sk.rs_idx + jl])
-                    val = (acc[r0:r0 + sk.ncols] * rs[:, None]) * cs[None, :]
-                    # P(i = col0 + n, j = 8*a_g0 + jl)
-                    idx = sk.dst_off + jl[:, None] * sk.dst_ld + it.col0 + np.arange(it.ncols)[None, :]
-                    key = ("p", int(sk.dst_off), it.col0)
-                    assert key not in covered
-                    covered.add(key)
-                    self.scr[idx] = val
-                    r0 += sk.a_ng * 8
+                # a phase-1 product tile: stored, and pi raised by each row's maximum
+                assert it.fam_end - it.fam_begin == 1 and not it.init
+                self.scr[idx] = tot
+                pi = it.pi_idx + np.arange(it.mrows)
+                self.scales[pi] = np.maximum(self.scales[pi], np.max(np.abs(tot), axis=1))
 
 
 def execute_ozaki(plan, oz, psi):

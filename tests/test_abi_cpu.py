@@ -26,7 +26,7 @@ MIRRORS = {
     "tj_plan_operand": L.PlanOperand, "tj_plan_task": L.PlanTask, "tj_plan_cell": L.PlanCell,
     "tj_plan_upload": L.PlanUpload, "tj_plan_merge": L.PlanMerge, "tj_plan_item": L.PlanItem,
     "tj_plan_reduce": L.PlanReduce, "tj_plan_export": L.PlanExport,
-    "tj_oz_job": L.OzJobC, "tj_oz_seg": L.OzSegC, "tj_oz_fam": L.OzFamC, "tj_oz_stack": L.OzStackC,
+    "tj_oz_job": L.OzJobC, "tj_oz_seg": L.OzSegC, "tj_oz_fam": L.OzFamC,
     "tj_oz_item": L.OzItemC, "tj_oz_cell": L.OzCellC, "tj_ozaki_export": L.OzExport,
 }
 
