@@ -492,7 +492,7 @@ extern "C" int tj_lanczos_memo_new(tj_ctx *ctx, const tj_lattice *lat, const tj_
   if ((rc = prepare_hpsi(ctx, lat, sys, env, sys_bs, env_bs, eigvec))) return rc;
   const int64_t D = eigvec->dim;
   const int64_t ld = (D + 31) / 32 * 32;
-  if ((rc = ctx->lanV.reserve(sizeof(double) * ld * (LOOP_IN + 2)))) return rc;
+  if ((rc = ctx->lanV.reserve(sizeof(double) * ld * (LOOP_IN + 4)))) return rc;
   const int nblk = dot_blocks(D);
   const int mdb = (int)((D + 256 * 8 - 1) / (256 * 8));
   if ((rc = ctx->lanScal.reserve(sizeof(double) * 1024))) return rc;
@@ -501,8 +501,10 @@ extern "C" int tj_lanczos_memo_new(tj_ctx *ctx, const tj_lattice *lat, const tj_
   double *V = ctx->lanV.d();
   double *S = ctx->lanScal.d();   // [0..127] alpha, [128..255] beta, [256..383] uu, [384..511] coef, [512] lam, [513] nrm, [600..727] dz
   double *alpha = S, *beta = S + 128, *uu = S + 256, *coef = S + 384, *lam = S + 512, *nrm = S + 513, *dz = S + 600;
+  int *itd = (int *)(S + 1000);   // the iteration's step L, read by the captured kernels
   double *part = ctx->lanPart.d(), *mpart = part + nblk;
   auto vec = [&](int j) { return V + (int64_t)(j - 1) * ld; };   // tempvec(j), 1-based
+  double *X = vec(LOOP_IN + 3), *Y = vec(LOOP_IN + 4);         // H*psi input and output of an iteration
   auto norm_into = [&](const double *x, double *res) {
     launch_dot(x, x, D, part, nblk, ctx->stream);
     launch_sum(part, nblk, res, 1, ctx->stream);
@@ -517,44 +519,66 @@ extern "C" int tj_lanczos_memo_new(tj_ctx *ctx, const tj_lattice *lat, const tj_
     return TJ_OK;
   };
   const auto t0 = std::chrono::steady_clock::now();
-  CK(cudaMemsetAsync(S, 0, sizeof(double) * 1024, ctx->stream));
-  CK(cudaMemcpyAsync(vec(1), eigvec->data, sizeof(double) * D, cudaMemcpyHostToDevice, ctx->stream));
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemsetAsync(S, 0, sizeof(double) * 1024, st));
+  CK(cudaMemcpyAsync(vec(1), eigvec->data, sizeof(double) * D, cudaMemcpyHostToDevice, st));
   norm_into(vec(1), nrm);
-  launch_scale_inv(vec(1), nrm, D, ctx->stream);
+  launch_scale_inv(vec(1), nrm, D, st);
   dot_into(vec(1), vec(1), uu + 1);
   const int64_t h0 = ctx->n_hpsi;
-  if ((rc = run_hpsi(ctx, vec(1), vec(2), false))) return rc;
-  dot_into(vec(1), vec(2), alpha + 1);
+  if ((rc = run_hpsi(ctx, vec(1), Y, false))) return rc;
+  dot_into(vec(1), Y, alpha + 1);
   double ritzmin = 0, hb = 0, hl = 0;
   if ((rc = fetch(alpha + 1, &ritzmin))) return rc;
   int last = 1;
-  // One host synchronisation per iteration: beta(last) and the new Ritz value
-  // are read together at its end.  The reference stops before normalising
-  // the next vector when |beta| <= lanzero (eigen.f90); here that vector and
-  // its H*psi are computed speculatively and dropped, with `last` restored,
-  // so the result is the same.
+  const int one = 1;
+  CK(cudaMemcpyAsync(itd, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+  // One iteration (block.f90:2515-2551 and eigen.f90:60-150), captured once
+  // as a CUDA graph and launched per step; every kernel reads the step L from
+  // *itd, and the last one publishes beta(L) and the Ritz value to page-locked
+  // host memory and advances L.  The reference stops before normalising the
+  // next vector when |beta| <= lanzero; here that vector and its H*psi are
+  // computed speculatively and dropped, with `last` restored, so the result
+  // is the same.
+  auto ref = [&](int off) { return LzRef{V, ld, itd, off, nullptr}; };
+  const LzRef yref{nullptr, 0, nullptr, 0, Y};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+  launch_lz_update(ref(1), Y, ref(0), ref(-1), S, itd, D, st);                  // vec(L+1) = H vec(L) - ...
+  launch_lz_norm(ref(1), D, part, nblk, S, itd, 128, 1, st);                    // beta(L)
+  launch_lz_scale(ref(1), S, itd, 128, nullptr, D, st);
+  launch_lz_gram_schmidt(V, ld, itd, ref(1), D, mpart, mdb, 128, uu + 1, coef, st);
+  launch_lz_norm(ref(1), D, part, nblk, S, nullptr, 513, 1, st);
+  launch_lz_scale(ref(1), S, nullptr, 513, X, D, st);                           // and X = vec(L+1)
+  launch_lz_norm(ref(1), D, part, nblk, S, itd, 257, 0, st);                    // uu(L+1)
+  rc = run_hpsi(ctx, X, Y, false);
+  if (!rc) {
+    launch_lz_dot(ref(1), yref, D, part, nblk, S, itd, 1, st);                  // alpha(L+1)
+    launch_lz_tridiag(alpha + 1, beta + 1, itd, 1, lam, st);
+    launch_lz_publish(S, itd, ctx->pinned, st);
+  }
+  const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+  --ctx->n_hpsi;   // the captured H*psi ran nothing
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (ce != cudaSuccess) return set_err(TJ_ERR_CUDA, std::string("Lanczos graph capture: ") + cudaGetErrorString(ce));
+  cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) return set_err(TJ_ERR_CUDA, std::string("Lanczos graph: ") + cudaGetErrorString(ie));
+  struct ExecGuard {
+    cudaGraphExec_t e;
+    ~ExecGuard() { cudaGraphExecDestroy(e); }
+  } guard{exec};
   while (last < LOOP_IN) {
-    launch_lanczos_update(vec(last + 1), vec(last), last >= 2 ? vec(last - 1) : nullptr, alpha + last,
-                          beta + last - 1, D, ctx->stream);
-    norm_into(vec(last + 1), beta + last);
-    CK(cudaMemcpyAsync(ctx->pinned, beta + last, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    launch_scale_inv(vec(last + 1), beta + last, D, ctx->stream);
-    // Gram_Schmidt_process (block.f90:2515-2551)
-    launch_multi_dot(V, ld, last, vec(last + 1), D, mpart, mdb, 128, ctx->stream);
-    launch_multi_sum(mpart, mdb, last, 128, uu + 1, coef, ctx->stream);
-    launch_combine(V, ld, last, coef, vec(last + 1), D, 0, ctx->stream);
-    norm_into(vec(last + 1), nrm);
-    launch_scale_inv(vec(last + 1), nrm, D, ctx->stream);
-    ++last;
-    dot_into(vec(last), vec(last), uu + last);
-    if ((rc = run_hpsi(ctx, vec(last), vec(last + 1), false))) return rc;
-    dot_into(vec(last), vec(last + 1), alpha + last);
-    launch_tridiag_min(alpha + 1, beta + 1, last, lam, nullptr, 0, ctx->stream);
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(ctx->pinned + 1, lam, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaGraphLaunch(exec, st));
+    CK(cudaStreamSynchronize(st));
+    ++ctx->n_hpsi;
     hb = ctx->pinned[0];
     hl = ctx->pinned[1];
+    ++last;
     if (!std::isfinite(hb)) return set_err(TJ_ERR_NUMERIC, "Lanczos: non-finite beta");
     if (std::fabs(hb) <= lanzero) {
       --last;

@@ -368,7 +368,7 @@ __device__ __forceinline__ int sturm_count(const double *a, const double *b, int
 // point per lane: five bits per pass) finished by bisection, then inverse
 // iteration with a pivoted tridiagonal solve on one thread.  n is at most the
 // Lanczos depth.
-__global__ void tridiag_min_kernel(const double *a, const double *b, int n, double *lam, double *vec, int want_vec) {
+__device__ void tridiag_min_body(const double *a, const double *b, int n, double *lam, double *vec, int want_vec) {
   if (blockIdx.x != 0 || threadIdx.x >= 32) return;
   const int lane = threadIdx.x;
   double lo = 0.0, hi = 0.0;
@@ -464,9 +464,155 @@ __global__ void tridiag_min_kernel(const double *a, const double *b, int n, doub
     if (x[i] != 0.0) { sgn = x[i] > 0 ? 1.0 : -1.0; break; }
   for (int i = 0; i < n; ++i) vec[i] = sgn * x[i];
 }
+__global__ void tridiag_min_kernel(const double *a, const double *b, int n, double *lam, double *vec, int want_vec) {
+  tridiag_min_body(a, b, n, lam, vec, want_vec);
+}
 void launch_tridiag_min(const double *a, const double *b, int n, double *lam, double *vec, int want_vec,
                         cudaStream_t s) {
   tridiag_min_kernel<<<1, 32, 0, s>>>(a, b, n, lam, vec, want_vec);
+}
+
+// ---- one Lanczos iteration with its step read from device memory (*it), so
+// that the same launches -- captured once as a CUDA graph -- serve every
+// iteration.  S holds alpha (0..127), beta (128..255), uu (256..383), the
+// Gram-Schmidt coefficients (384..511), the Ritz value (512) and a norm (513).
+__device__ __forceinline__ double *lz_ptr(const LzRef &r) {
+  return r.fixed ? r.fixed : r.V + (int64_t)(*r.it + r.off - 1) * r.ld;
+}
+
+__global__ void lz_update_kernel(LzRef dst, const double *__restrict__ src, LzRef x1, LzRef x2, const double *S,
+                                 const int *it, int64_t n) {
+  const int L = *it;
+  const double av = S[L], bv = L >= 2 ? S[128 + L - 1] : 0.0;
+  double *y = lz_ptr(dst);
+  const double *p1 = lz_ptr(x1), *p2 = L >= 2 ? lz_ptr(x2) : nullptr;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double v = src[i] - av * p1[i];
+    if (p2) v = v - bv * p2[i];
+    y[i] = v;
+  }
+}
+
+__global__ void lz_dot_kernel(LzRef x, LzRef y, int64_t n, double *partials) {
+  __shared__ double sh[VT / 32];
+  const double *__restrict__ px = lz_ptr(x), *__restrict__ py = lz_ptr(y);
+  double s = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    s += px[i] * py[i];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void lz_sum_kernel(const double *partials, int nblk, double *S, const int *it, int idx, int sqrt_flag) {
+  __shared__ double sh[VT / 32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) s += partials[i];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) S[idx + (it ? *it : 0)] = sqrt_flag ? sqrt(s) : s;
+}
+
+__global__ void lz_scale_kernel(LzRef x, const double *S, const int *it, int idx, double *copy, int64_t n) {
+  const double d = S[idx + (it ? *it : 0)];
+  double *px = lz_ptr(x);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double v = px[i] / d;
+    px[i] = v;
+    if (copy) copy[i] = v;
+  }
+}
+
+__global__ void lz_multi_dot_kernel(const double *__restrict__ V, int64_t ld, const int *it, LzRef wr_, int64_t n,
+                                    double *partials, int kmax) {
+  __shared__ double sh[VT / 32];
+  const int k = *it;
+  const double *__restrict__ w = lz_ptr(wr_);
+  const int64_t base = (int64_t)blockIdx.x * VT * MD_PER + threadIdx.x;
+  double wr[MD_PER];
+#pragma unroll
+  for (int i = 0; i < MD_PER; ++i) {
+    const int64_t e = base + (int64_t)i * VT;
+    wr[i] = e < n ? w[e] : 0.0;
+  }
+  for (int j = 0; j < k; ++j) {
+    const double *v = V + (int64_t)j * ld;
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < MD_PER; ++i) {
+      const int64_t e = base + (int64_t)i * VT;
+      if (e < n) s += v[e] * wr[i];
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) partials[(int64_t)blockIdx.x * kmax + j] = s;
+  }
+}
+
+__global__ void lz_multi_sum_kernel(const double *partials, int nblk, int kmax, const double *uu, double *coef,
+                                    const int *it) {
+  __shared__ double sh[VT / 32];
+  const int j = blockIdx.x;
+  if (j >= *it) return;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += partials[(int64_t)b * kmax + j];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) coef[j] = s / uu[j];
+}
+
+__global__ void lz_combine_kernel(const double *__restrict__ V, int64_t ld, const int *it,
+                                  const double *__restrict__ coef, LzRef wr_, int64_t n) {
+  __shared__ double c[128];
+  const int k = *it;
+  double *w = lz_ptr(wr_);
+  for (int j = threadIdx.x; j < k && j < 128; j += blockDim.x) c[j] = coef[j];
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double t = 0.0;
+    for (int j = 0; j < k; ++j) t = t + c[j] * V[(int64_t)j * ld + i];
+    w[i] = w[i] - t;
+  }
+}
+
+__global__ void lz_tridiag_kernel(const double *a, const double *b, const int *it, int noff, double *lam) {
+  tridiag_min_body(a, b, *it + noff, lam, nullptr, 0);
+}
+
+// beta(L) and the Ritz value to page-locked host memory; the step advances
+__global__ void lz_publish_kernel(const double *S, int *it, double *host) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int L = *it;
+  host[0] = S[128 + L];
+  host[1] = S[512];
+  __threadfence_system();
+  *it = L + 1;
+}
+
+void launch_lz_update(LzRef dst, const double *src, LzRef x1, LzRef x2, const double *S, const int *it, int64_t n,
+                      cudaStream_t s) {
+  lz_update_kernel<<<vgrid(n), VT, 0, s>>>(dst, src, x1, x2, S, it, n);
+}
+void launch_lz_norm(LzRef x, int64_t n, double *partials, int nblk, double *S, const int *it, int idx, int sqrt_flag,
+                    cudaStream_t s) {
+  lz_dot_kernel<<<nblk, VT, 0, s>>>(x, x, n, partials);
+  lz_sum_kernel<<<1, VT, 0, s>>>(partials, nblk, S, it, idx, sqrt_flag);
+}
+void launch_lz_dot(LzRef x, LzRef y, int64_t n, double *partials, int nblk, double *S, const int *it, int idx,
+                   cudaStream_t s) {
+  lz_dot_kernel<<<nblk, VT, 0, s>>>(x, y, n, partials);
+  lz_sum_kernel<<<1, VT, 0, s>>>(partials, nblk, S, it, idx, 0);
+}
+void launch_lz_scale(LzRef x, const double *S, const int *it, int idx, double *copy, int64_t n, cudaStream_t s) {
+  lz_scale_kernel<<<vgrid(n), VT, 0, s>>>(x, S, it, idx, copy, n);
+}
+void launch_lz_gram_schmidt(const double *V, int64_t ld, const int *it, LzRef w, int64_t n, double *partials,
+                            int nblk, int kmax, const double *uu, double *coef, cudaStream_t s) {
+  lz_multi_dot_kernel<<<nblk, VT, 0, s>>>(V, ld, it, w, n, partials, kmax);
+  lz_multi_sum_kernel<<<kmax, VT, 0, s>>>(partials, nblk, kmax, uu, coef, it);
+  lz_combine_kernel<<<vgrid(n), VT, 0, s>>>(V, ld, it, coef, w, n);
+}
+void launch_lz_tridiag(const double *a, const double *b, const int *it, int noff, double *lam, cudaStream_t s) {
+  lz_tridiag_kernel<<<1, 32, 0, s>>>(a, b, it, noff, lam);
+}
+void launch_lz_publish(const double *S, int *it, double *host, cudaStream_t s) {
+  lz_publish_kernel<<<1, 32, 0, s>>>(S, it, host);
 }
 
 __global__ void copy_kernel(double *dst, const double *src, int64_t n) {

@@ -57,4 +57,31 @@ void launch_tridiag_min(const double *a, const double *b, int n, double *lam, do
 // out = sum of a device array of n doubles into res (deterministic)
 void launch_copy(double *dst, const double *src, int64_t n, cudaStream_t s);
 
+// ---- Lanczos iteration with the step L read from device memory (*it) ----
+// A vector chosen when the kernel runs: vec(*it + off) = V + (*it + off - 1) * ld, or `fixed`.
+struct LzRef {
+  double *V;
+  int64_t ld;
+  const int *it;
+  int off;
+  double *fixed;
+};
+// dst = src - alpha(L) x1 - beta(L-1) x2 (x2 only for L >= 2)
+void launch_lz_update(LzRef dst, const double *src, LzRef x1, LzRef x2, const double *S, const int *it, int64_t n,
+                      cudaStream_t s);
+// S[idx + L] = ||x|| (sqrt_flag) or x.x ; it == nullptr: S[idx]
+void launch_lz_norm(LzRef x, int64_t n, double *partials, int nblk, double *S, const int *it, int idx, int sqrt_flag,
+                    cudaStream_t s);
+void launch_lz_dot(LzRef x, LzRef y, int64_t n, double *partials, int nblk, double *S, const int *it, int idx,
+                   cudaStream_t s);
+// x /= S[idx + L] (it == nullptr: S[idx]); copy (if not null) receives the result too
+void launch_lz_scale(LzRef x, const double *S, const int *it, int idx, double *copy, int64_t n, cudaStream_t s);
+// w -= sum_{j < L} (V_j . w / uu[j]) V_j   (classical Gram-Schmidt against the first L vectors)
+void launch_lz_gram_schmidt(const double *V, int64_t ld, const int *it, LzRef w, int64_t n, double *partials,
+                            int nblk, int kmax, const double *uu, double *coef, cudaStream_t s);
+// lowest eigenvalue of the leading (L + noff) x (L + noff) tridiagonal
+void launch_lz_tridiag(const double *a, const double *b, const int *it, int noff, double *lam, cudaStream_t s);
+// host[0] = beta(L), host[1] = Ritz value (page-locked host memory); then L += 1
+void launch_lz_publish(const double *S, int *it, double *host, cudaStream_t s);
+
 }  // namespace tjb
