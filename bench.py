@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end Lanczos leg (profiling runs)")
     ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default tiling)")
+    ap.add_argument("--no-microbench", action="store_true", help="skip the grouped block-GEMM microbenchmark")
     return ap.parse_args()
 
 
@@ -280,6 +282,13 @@ def main():
         ctxoz = Context(local)
         ctxoz.set_precision(TJ_PREC_OZAKI, args.slices)
     head = ctxoz if mixed else ctx64
+    # the autotuner's tiling for this superblock, in both precisions (untimed)
+    tune = {}
+    if not args.no_tune:
+        if mixed:
+            tune["mixed"] = ctxoz.autotune(sb).as_dict()
+        if args.precision != "ozaki":
+            tune["fp64"] = ctx64.autotune(sb).as_dict()
     # untimed legs first: the other precision (for the speed-up) and warm-up
     ms64 = st64 = None
     if args.precision == "mixed":
@@ -340,6 +349,22 @@ def main():
         del kept
         pinned.close()
 
+    micro = None
+    if rank == 0 and not args.no_microbench:
+        # grouped block-GEMM microbenchmark: 400 sector pairs, dims log-uniform in
+        # [8, 1024], 4..16 terms each; one persistent grouped launch (autotuned
+        # tiling) against one launch per block GEMM
+        from grand_sql_tj_b200 import gg
+        gb = gg.make_batch(n_cells=400, seed=args.seed)
+        g_ms, g_out, g_fl, g_tr = ctx64.grouped_gemm_bench(gb, 2, reps=3)
+        p_ms, p_out, _, _ = ctx64.grouped_gemm_bench(gb, 1, reps=1)
+        micro = {**gb.spec, "flops": g_fl, "grouped_ms": g_ms, "grouped_tflops": g_fl / (g_ms * 1e-3) / 1e12,
+                 "per_block_ms": p_ms, "per_block_launches": gb.spec["terms"],
+                 "per_block_tflops": g_fl / (p_ms * 1e-3) / 1e12, "grouped_speedup": p_ms / g_ms,
+                 "max_diff_rel": float(np.max(np.abs(g_out - p_out)) / max(np.max(np.abs(p_out)), 1e-300)),
+                 "tuned": g_tr.as_dict() if g_tr is not None else None, "dtype": "f64"}
+        del gb, g_out, p_out
+
     peaks = measured_peaks()
     fp64 = fp64_peak_tflops(local) if rank == 0 else None
     if mixed:
@@ -397,6 +422,10 @@ def main():
             line["accuracy"] = accuracy
         if step is not None:
             line["sweep"] = step
+        if tune:
+            line["autotune"] = tune
+        if micro is not None:
+            line["grouped_gemm_microbench"] = micro
         print(json.dumps(line), flush=True)
     ctx64.close()
     if ctxoz is not None:

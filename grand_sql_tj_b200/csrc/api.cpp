@@ -179,7 +179,8 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   h = key_basis(h, env_bs);
   h = fnv(h, wave->sub, sizeof(tj_wave_sub) * wave->num);
   h = fnv(h, &ctx->prec_mode, sizeof ctx->prec_mode);
-  if (ctx->plan_valid && ctx->plan_key == h) return TJ_OK;
+  h = fnv(h, &ctx->slices, sizeof ctx->slices);
+  if (ctx->plan_valid && ctx->plan_key == h && tune_is_current(ctx)) return TJ_OK;
   ctx->plan_valid = false;
   CK(cudaSetDevice(ctx->device));
   using clk = std::chrono::steady_clock;
@@ -189,6 +190,13 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   std::string msg;
   int rc = build_hpsi_plan(lat, sys, env, sys_bs, env_bs, wave, *P, msg);
   if (rc) return set_err(rc, "H*psi plan: " + msg);
+  // tiling choices: the autotuner's for this block-size histogram, when known
+  ctx->hist_key = plan_hist_key(*P, ctx->prec_mode, ctx->slices);
+  if (!ctx->tuning && ctx->autotune != TJ_TUNE_OFF) tune_lookup(ctx->hist_key, ctx->tune);
+  if (!(ctx->tune == TuneParams())) {
+    split_tiles(P->cells1, P->tasks1, P->tiles1, P->red1, P->nslots1, false, ctx->tune);
+    split_tiles(P->cells2, P->tasks2, P->tiles2, P->red2, P->nslots2, false, ctx->tune);
+  }
   const double plan_ms = ms_since(t_start);
   const auto t_up = clk::now();
   // operators: one copy per input block, then the merged sums on the device
@@ -234,7 +242,7 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
     try {
       int nsm = 148;
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
-      build_ozaki_plan(*P, ctx->slices, nsm, *oz);
+      build_ozaki_plan(*P, ctx->slices, nsm, *oz, ctx->tune);
     } catch (const std::exception &e) {
       return set_err(TJ_ERR_ARG, std::string("split-precision plan: ") + e.what());
     }
@@ -296,7 +304,10 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   }
   ctx->plan = std::move(P);
   ctx->plan_key = h;
+  ctx->plan_tune = ctx->tune;
   ctx->plan_valid = true;
+  if (!ctx->tuning && ctx->autotune == TJ_TUNE_ON_MISS && !tune_lookup(ctx->hist_key, ctx->tune))
+    return autotune_plan(ctx, lat, sys, env, sys_bs, env_bs, wave, nullptr);
   return TJ_OK;
 }
 
@@ -318,7 +329,7 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
   CK(launch_oz_gemm((const OzItem *)ctx->ozItems1.p, (const int32_t *)ctx->ozCta1.p, (int)oz.cta1.size() - 1,
                     (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzCell *)ctx->ozCells.p,
-                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, st));
+                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, oz.bn, st));
   if (timed) CK(cudaEventRecord(ctx->ev[2], st));
   launch_oz_max((const OzJob *)ctx->ozProdMJobs.p, (int)oz.prod_mjobs.size(), (const OzSpan *)ctx->ozProdMSpans.p,
                 (int)oz.prod_mspans.size(), ctx->ops.d(), in, ctx->scr.d(), scales, st);
@@ -328,7 +339,7 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
   CK(launch_oz_gemm((const OzItem *)ctx->ozItems2.p, (const int32_t *)ctx->ozCta2.p, (int)oz.cta2.size() - 1,
                     (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzCell *)ctx->ozCells.p,
-                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, st));
+                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, oz.bn, st));
   if (timed) CK(cudaEventRecord(ctx->ev[4], st));
   CK(cudaGetLastError());
   ++ctx->n_hpsi;
@@ -367,7 +378,7 @@ int tjb::run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed) {
   g.ntiles = (int)P.tiles1.size();
   g.counter = cnt;
   g.slots = ctx->slots.d();
-  launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles), ctx->stream);
+  launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles, ctx->tune.ctas_per_sm), ctx->stream);
   launch_reduce(g, (const Reduce *)ctx->red1.p, (int)P.red1.size(), ctx->stream);
   if (timed) {
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
@@ -379,7 +390,7 @@ int tjb::run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed) {
   g.tiles = (const Tile *)ctx->tiles2.p;
   g.ntiles = (int)P.tiles2.size();
   g.counter = cnt + 1;
-  launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles), ctx->stream);
+  launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles, ctx->tune.ctas_per_sm), ctx->stream);
   launch_reduce(g, (const Reduce *)ctx->red2.p, (int)P.red2.size(), ctx->stream);
   if (timed) CK(cudaEventRecord(ctx->ev[4], ctx->stream));
   CK(cudaGetLastError());

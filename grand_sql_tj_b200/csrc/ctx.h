@@ -39,6 +39,12 @@ struct tj_ctx {
   // launch, 3 after the product splits, 4 end (FP64: 1 = 0 and 3 = 2)
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   int prec_mode = TJ_PREC_FP64, slices = 6;
+  // tiling / schedule choices in use, and how they are chosen (TJ_TUNE_*)
+  tjb::TuneParams tune;
+  int autotune = TJ_TUNE_CACHED;
+  bool tuning = false;        // inside tj_autotune (prepare_hpsi must not recurse)
+  uint64_t hist_key = 0;      // block-size histogram of the current plan
+  tjb::TuneParams plan_tune;  // the choices the current plan was built with
   // compiled H*psi of the current step
   std::unique_ptr<tjb::HpsiPlan> plan;
   uint64_t plan_key = 0;
@@ -52,6 +58,7 @@ struct tj_ctx {
   tjb::DevBuf lanV, lanScal, lanPart;
   tjb::DevBuf trA, trB, trC, trD, trE;          // truncation
   tjb::DevBuf corCells, corTasks, corTiles, corOps, corScr, corPsi;   // correlators
+  tjb::DevBuf ggPool, ggOut, ggTab, ggSlots;                          // grouped block-GEMM benchmark
   // split-precision H*psi
   std::unique_ptr<tjb::OzPlan> oz;
   tjb::DevBuf ozPack, ozScales, ozStaJobs, ozPsiJobs, ozProdJobs, ozSegs, ozFams, ozCells, ozItems1,
@@ -60,7 +67,8 @@ struct tj_ctx {
   std::vector<tjb::DevBuf *> all_bufs() {
     return {&ops, &scr, &vin, &vout, &counters, &partials, &cells1, &cells2, &tasks1, &tasks2, &tiles1,
             &tiles2, &red1, &red2, &slots, &m_dst, &m_n, &m_sb, &m_se, &m_src, &m_coef, &lanV, &lanScal, &lanPart, &trA, &trB,
-            &trC, &trD, &trE, &corCells, &corTasks, &corTiles, &corOps, &corScr, &corPsi, &ozPack, &ozScales,
+            &trC, &trD, &trE, &corCells, &corTasks, &corTiles, &corOps, &corScr, &corPsi, &ggPool, &ggOut, &ggTab,
+            &ggSlots, &ozPack, &ozScales,
             &ozStaJobs, &ozPsiJobs, &ozProdJobs, &ozSegs, &ozFams, &ozCells, &ozItems1, &ozItems2,
             &ozCta1, &ozCta2, &ozStaSpans, &ozPsiSpans, &ozProdSpans, &ozStaMSpans,
             &ozPsiMSpans, &ozProdMSpans, &ozStaMJobs, &ozPsiMJobs, &ozProdMJobs, &ozMisc};
@@ -73,4 +81,18 @@ int prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const 
                  const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave);
 int run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed);
 int check_device_flags(tj_ctx *ctx);
+
+// autotuning (tune.cpp)
+// key of the plan's block-size histogram: GEMM tasks counted by
+// (log2 M, log2 N, log2 K), with the precision mode and slice count
+uint64_t plan_hist_key(const HpsiPlan &P, int prec_mode, int slices);
+// process-wide table of tuned choices per histogram key
+bool tune_lookup(uint64_t key, TuneParams &tp);
+void tune_store(uint64_t key, const TuneParams &tp);
+// whether the current plan was built with the choices that would be used now
+bool tune_is_current(tj_ctx *ctx);
+// searches the choices for the superblock by timing H*psi, stores them and
+// leaves the plan prepared with the best
+int autotune_plan(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const tj_model *env,
+                  const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave, tj_tune_result *out);
 }  // namespace tjb

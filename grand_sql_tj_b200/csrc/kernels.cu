@@ -2,6 +2,7 @@
 // merged-operator sums (hmerge), and the Lanczos vector operations.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "kernels.cuh"
@@ -160,11 +161,11 @@ __global__ void __launch_bounds__(GEMM_THREADS, 4) grouped_gemm_f64(GemmParams p
   }
 }
 
-int grouped_gemm_grid(int ntiles) {
+int grouped_gemm_grid(int ntiles, int ctas_per_sm) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int g = sms * 4;
+  int g = sms * std::min(4, std::max(1, ctas_per_sm));
   return ntiles < g ? (ntiles > 0 ? ntiles : 1) : g;
 }
 

@@ -26,7 +26,7 @@ struct GemmParams {
 void launch_grouped_gemm(const GemmParams &p, int grid, cudaStream_t s);
 // out tile = sum of its partial slots (in slot order) + its axpy tasks
 void launch_reduce(const GemmParams &p, const Reduce *red, int nred, cudaStream_t s);
-int grouped_gemm_grid(int ntiles);
+int grouped_gemm_grid(int ntiles, int ctas_per_sm = 4);
 
 // merged operators: dst[e] = sum_j coef_j * src_j[e]
 void launch_merge(double *ops, const int64_t *dst, const int64_t *n, const int32_t *sb, const int32_t *se,

@@ -709,9 +709,13 @@ static cudaError_t launch_gemm_t(const OzGemmParams &p, int ncta, cudaStream_t s
 
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
                            const OzCell *cells, const Task *tasks, const uint8_t *pack,
-                           double *scales, const double *psi, double *scr, double *out, int *err, int s,
+                           double *scales, const double *psi, double *scr, double *out, int *err, int s, int bn,
                            cudaStream_t st) {
   if (ncta <= 0) return cudaSuccess;
+  if (s == 5 && bn == 32) return launch_gemm_t<5, 32>(OzGemmParams{items, cta, segs, fams, cells, tasks, pack, scales,
+                                                                   psi, scr, out, err},
+                                                      ncta, st);
+  if (bn != oz_bn(s)) return cudaErrorInvalidValue;
   OzGemmParams p{items, cta, segs, fams, cells, tasks, pack, scales, psi, scr, out, err};
   switch (s) {
     case 3: return launch_gemm_t<3, 48>(p, ncta, st);

@@ -164,8 +164,10 @@ struct OzPlan {
   double flops1 = 0, flops2 = 0;           // FP64-equivalent flops of each launch
 };
 
-// Builds the split-precision form of an H*psi plan (host).
-void build_ozaki_plan(const HpsiPlan &hp, int s, int nsm, OzPlan &oz);
+// Builds the split-precision form of an H*psi plan (host); tp.oz_bn picks
+// the N tile (0: oz_bn(s); 32 is also available for s = 5) and
+// tp.oz_item_cost the per-item cost of the static schedule.
+void build_ozaki_plan(const HpsiPlan &hp, int s, int nsm, OzPlan &oz, const TuneParams &tp = TuneParams());
 
 // device launches (ozaki.cu)
 void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
@@ -174,7 +176,7 @@ void launch_oz_split(const OzJob *jobs, int njobs, const OzSpan *spans, int nspa
                      const double *psi, const double *scr, const double *scales, uint8_t *pack, int s, cudaStream_t st);
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
                            const OzCell *cells, const Task *tasks, const uint8_t *pack,
-                           double *scales, const double *psi, double *scr, double *out, int *err, int s,
+                           double *scales, const double *psi, double *scr, double *out, int *err, int s, int bn,
                            cudaStream_t st);
 
 }  // namespace tjb

@@ -48,6 +48,7 @@ struct Builder {
   struct FamRel { int fam, rs_rel, cs_rel; };
   std::vector<FamRel> famrel;
 
+  int sched_item_cost = 4;   // fixed per-item cost of the schedule, in k-blocks
   Builder(const HpsiPlan &h, OzPlan &o, int s) : hp(h), oz(o), S(s) {}
 
   // A operands are tiled by 128 rows; B operands by the N tile, each tile a
@@ -523,7 +524,8 @@ struct Builder {
       return;
     }
     const int nb = std::min(oz.nsm, n);
-    auto est = [](const OzItem &it) { return (int64_t)it.nkb + 4; };
+    const int64_t fixed = sched_item_cost;
+    auto est = [fixed](const OzItem &it) { return (int64_t)it.nkb + fixed; };
     std::stable_sort(v.begin(), v.end(), [&](const OzItem &a, const OzItem &b) { return est(a) > est(b); });
     std::vector<int64_t> load(nb, 0);
     std::vector<std::vector<int>> bins(nb);
@@ -559,13 +561,16 @@ struct Builder {
 
 }  // namespace
 
-void build_ozaki_plan(const HpsiPlan &hp, int s, int nsm, OzPlan &oz) {
+void build_ozaki_plan(const HpsiPlan &hp, int s, int nsm, OzPlan &oz, const TuneParams &tp) {
   if (s < 3 || s > OZ_MAX_S) throw std::runtime_error("slices must be in 3..8");
+  if (tp.oz_bn != 0 && tp.oz_bn != oz_bn(s) && !(s == 5 && tp.oz_bn == 32))
+    throw std::runtime_error("N tile not available for this slice count");
   oz = OzPlan();
   oz.s = s;
   oz.nsm = std::max(1, nsm);
-  oz.bn = oz_bn(s);
+  oz.bn = tp.oz_bn ? tp.oz_bn : oz_bn(s);
   Builder b(hp, oz, s);
+  b.sched_item_cost = std::max(0, tp.oz_item_cost);
   b.build();
 }
 

@@ -182,7 +182,7 @@ static inline double m1pow(int n) { return (n % 2) ? -1.0 : 1.0; }
 // partial dot products are simply summed).  Items are ordered by decreasing
 // work so that the dynamic scheduler finishes with the small ones.
 void split_tiles(const std::vector<Cell> &cells, const std::vector<Task> &tasks, std::vector<Tile> &tiles,
-                 std::vector<Reduce> &red, int64_t &nslots, bool dot_mode) {
+                 std::vector<Reduce> &red, int64_t &nslots, bool dot_mode, const TuneParams &tp) {
   tiles.clear();
   red.clear();
   nslots = 0;
@@ -195,8 +195,10 @@ void split_tiles(const std::vector<Cell> &cells, const std::vector<Task> &tasks,
     total += k * nt;
     ntile += nt;
   }
-  // aim at ~6 items per resident CTA (148 SMs x 4), never below 256 k-steps per item
-  const double target = std::max(256.0, total / (148.0 * 4 * 6));
+  // aim at tp.items_per_cta items per resident CTA (148 SMs x tp.ctas_per_sm),
+  // never below tp.min_ksteps k-steps per item
+  const double target =
+      std::max((double)tp.min_ksteps, total / (148.0 * std::max(1, tp.ctas_per_sm) * std::max(1, tp.items_per_cta)));
   std::vector<std::pair<double, Tile>> w;
   for (int ci = 0; ci < (int)cells.size(); ++ci) {
     const Cell &c = cells[ci];

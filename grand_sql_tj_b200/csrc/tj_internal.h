@@ -99,9 +99,23 @@ struct HpsiPlan {
 // Tile shape of the grouped FP64 kernel.
 constexpr int BM = 64, BN = 64, BK = 16;
 
+// Tiling and scheduling choices the autotuner searches (defaults: the values
+// set by hand for the 4x24 m = 2000 superblock).
+struct TuneParams {
+  int items_per_cta = 6;    // FP64: split-K aims at this many items per resident CTA ...
+  int min_ksteps = 256;     // ... never cutting an item below this many inner-dimension steps
+  int ctas_per_sm = 4;      // FP64: resident CTAs per SM of the grouped kernel (1..4)
+  int oz_bn = 0;            // split precision: N tile (0: the default of the slice count)
+  int oz_item_cost = 4;     // split precision: per-item cost, in k-blocks, of the static schedule
+  bool operator==(const TuneParams &o) const {
+    return items_per_cta == o.items_per_cta && min_ksteps == o.min_ksteps && ctas_per_sm == o.ctas_per_sm &&
+           oz_bn == o.oz_bn && oz_item_cost == o.oz_item_cost;
+  }
+};
+
 // Work items (and Reduce records) of one grouped-GEMM pass over `cells`.
 void split_tiles(const std::vector<Cell> &cells, const std::vector<Task> &tasks, std::vector<Tile> &tiles,
-                 std::vector<Reduce> &red, int64_t &nslots, bool dot_mode);
+                 std::vector<Reduce> &red, int64_t &nslots, bool dot_mode, const TuneParams &tp = TuneParams());
 
 // Builds the plan (host).  Returns TJ_OK or an error code with msg set.
 int build_hpsi_plan(const tj_lattice *lat, const tj_model *sys, const tj_model *env,

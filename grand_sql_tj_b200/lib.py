@@ -13,13 +13,14 @@ from typing import Optional, Tuple
 
 import numpy as np
 
-from .structs import (Block, TjBasis, TjBlock, TjBlockSub, TjHpsiStats, TjLattice, TjModel,
-                      TjTruncResult, TjWave, Wave, block_from_c_result)
+from .structs import (Block, TjBasis, TjBlock, TjBlockSub, TjGgCell, TjGgTerm, TjHpsiStats, TjLattice, TjModel,
+                      TjTruncResult, TjTuneResult, TjWave, Wave, block_from_c_result)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtjb200.so")
 
 TJ_PREC_FP64, TJ_PREC_OZAKI = 0, 1
+TJ_TUNE_OFF, TJ_TUNE_CACHED, TJ_TUNE_ON_MISS = 0, 1, 2
 
 
 class TjError(RuntimeError):
@@ -173,6 +174,12 @@ def lib():
         L.tj_truncation.argtypes = [C.c_void_p, P(TjWave), C.c_int, C.c_int, C.c_int, C.c_double,
                                     P(TjTruncResult)]
         L.tj_hpsi_stats_get.argtypes = [C.c_void_p, P(TjHpsiStats)]
+        L.tj_set_autotune.argtypes = [C.c_void_p, C.c_int]
+        L.tj_autotune.argtypes = [C.c_void_p, P(TjLattice), P(TjModel), P(TjModel), P(TjBasis), P(TjBasis),
+                                  P(TjWave), P(TjTuneResult)]
+        L.tj_grouped_gemm_bench.argtypes = [C.c_void_p, P(TjGgCell), C.c_int, P(TjGgTerm), C.c_int,
+                                            P(C.c_double), C.c_int64, C.c_int64, C.c_int, C.c_int,
+                                            P(C.c_double), P(C.c_double), P(C.c_double), P(TjTuneResult)]
         L.tj_hpsi_plan_export.argtypes = [P(TjLattice), P(TjModel), P(TjModel), P(TjBasis), P(TjBasis),
                                           P(TjWave), P(PlanExport)]
         L.tj_cor_plan_export.argtypes = [C.c_int, P(TjBlock), P(TjBlock), P(TjBasis), P(TjBasis), P(TjWave),
@@ -227,6 +234,28 @@ class Context:
         s = TjHpsiStats()
         _chk(lib().tj_hpsi_stats_get(self.h, C.byref(s)))
         return s
+
+    def set_autotune(self, mode: int):
+        _chk(lib().tj_set_autotune(self.h, mode))
+
+    def autotune(self, sb, packed=None) -> TjTuneResult:
+        """tj_autotune: searches the tiling choices for this superblock's block-size histogram."""
+        ps, pe, bs, be = packed if packed is not None else pack_superblock(sb)
+        r = TjTuneResult()
+        _chk(lib().tj_autotune(self.h, C.byref(sb.lat.c), C.byref(ps.c), C.byref(pe.c), C.byref(bs.c),
+                               C.byref(be.c), C.byref(sb.wave.c), C.byref(r)))
+        return r
+
+    def grouped_gemm_bench(self, batch, mode: int, reps: int = 3):
+        """tj_grouped_gemm_bench on a GgBatch: (ms per repetition, output, flops, tune result or None)."""
+        out = np.zeros(batch.out_len)
+        ms, fl = C.c_double(), C.c_double()
+        tr = TjTuneResult()
+        _chk(lib().tj_grouped_gemm_bench(self.h, batch.cells, len(batch.cells), batch.terms, len(batch.terms),
+                                         batch.pool.ctypes.data_as(C.POINTER(C.c_double)), batch.pool.size,
+                                         batch.out_len, mode, reps, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                         C.byref(ms), C.byref(fl), C.byref(tr)))
+        return ms.value, out, fl.value, (tr if mode == 2 else None)
 
     # --------------------------------------------------------- hot path
     def model_wave(self, sb, invec: Optional[Wave] = None) -> Wave:

@@ -97,6 +97,27 @@ class TjHpsiStats(C.Structure):
                 ("ozplan_ms", C.c_double), ("lanczos_ms", C.c_double)]
 
 
+class TjTuneResult(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("items_per_cta", "min_ksteps", "ctas_per_sm", "oz_bn", "oz_item_cost",
+                                         "evaluated")] + \
+               [("default_ms", C.c_double), ("tuned_ms", C.c_double), ("tuning_ms", C.c_double),
+                ("hist_key", C.c_uint64)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class TjGgCell(C.Structure):
+    _fields_ = [("out_off", C.c_int64), ("M", C.c_int32), ("N", C.c_int32), ("t_begin", C.c_int32),
+                ("t_end", C.c_int32)]
+
+
+class TjGgTerm(C.Structure):
+    _fields_ = [("l_off", C.c_int64), ("r_off", C.c_int64)] + \
+               [(n, C.c_int32) for n in ("l_ld", "r_ld", "K", "l_trans", "r_trans", "pad_")] + \
+               [("coef", C.c_double)]
+
+
 def _dptr(a: np.ndarray):
     return a.ctypes.data_as(c_double_p)
 

@@ -246,6 +246,55 @@ typedef struct tj_hpsi_stats {
 } tj_hpsi_stats;
 int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st);
 
+/* ------------------------------------------------------------ autotuning */
+/* No counterpart in the reference.  The tiling of the grouped FP64 GEMM
+ * (split-K granularity: items per resident CTA and minimum inner-dimension
+ * steps per item; resident CTAs per SM) and of the split-precision GEMM (N
+ * tile, per-item cost of its static schedule) is chosen per block-size
+ * histogram of the H*psi plan -- its GEMM tasks counted by (log2 M, log2 N,
+ * log2 K) -- by timing H*psi with each candidate (coordinate descent from the
+ * defaults; a change is kept when it is at least 2 % faster).  The choices
+ * are kept in a process-wide table; TJ_TUNE_CACHED (default) uses a stored
+ * choice when the histogram matches, TJ_TUNE_ON_MISS also runs the search
+ * the first time a histogram is seen, TJ_TUNE_OFF always uses the defaults. */
+enum { TJ_TUNE_OFF = 0, TJ_TUNE_CACHED = 1, TJ_TUNE_ON_MISS = 2 };
+typedef struct tj_tune_result {
+  int32_t items_per_cta, min_ksteps, ctas_per_sm, oz_bn, oz_item_cost;
+  int32_t evaluated;            /* candidates timed                                   */
+  double default_ms, tuned_ms;  /* device time of one H*psi with the defaults / chosen */
+  double tuning_ms;             /* host wall time of the search                       */
+  uint64_t hist_key;
+} tj_tune_result;
+int tj_set_autotune(tj_ctx *ctx, int mode);
+/* Runs the search for this superblock (in the context's precision mode)
+ * whatever the mode, stores the choice and leaves the plan prepared with it. */
+int tj_autotune(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const tj_model *env,
+                const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave, tj_tune_result *out);
+
+/* ------------------------------------------- grouped block-GEMM benchmark */
+/* No counterpart in the reference.  The batched block-GEMM pattern of H*psi
+ * on synthetic data: output cell c (M x N, column-major, ld = M, at
+ * out[out_off]) = sum over its terms t in [t_begin, t_end) of
+ * coef * op(L) op(R), op(L) M x K, op(R) K x N, both windows of one operand
+ * pool (l_off / r_off, leading dimensions l_ld / r_ld, transposed when
+ * l_trans / r_trans).  mode 0: one persistent grouped launch (the H*psi FP64
+ * kernel, split-K tiling from the context's choices); mode 1: one launch per
+ * term (block GEMM), each adding to its cell; mode 2: mode 0 after the
+ * autotuner's search of the tiling for this batch (reported in *tuned when
+ * not NULL; the context's own choices are left as they were).  The pool is
+ * uploaded once; `reps` timed repetitions (CUDA events) after one warm-up
+ * give *ms per repetition; out (out_len doubles) receives the result and
+ * *flops the algorithmic 2 M N K sum. */
+typedef struct tj_gg_cell { int64_t out_off; int32_t M, N, t_begin, t_end; } tj_gg_cell;
+typedef struct tj_gg_term {
+  int64_t l_off, r_off;
+  int32_t l_ld, r_ld, K, l_trans, r_trans, pad_;
+  double coef;
+} tj_gg_term;
+int tj_grouped_gemm_bench(tj_ctx *ctx, const tj_gg_cell *cells, int ncells, const tj_gg_term *terms, int nterms,
+                          const double *pool, int64_t pool_len, int64_t out_len, int mode, int reps,
+                          double *out, double *ms, double *flops, tj_tune_result *tuned);
+
 /* Device-resident benchmarking helper: uploads invec once, then runs `reps`
  * H*psi products back to back on the device (inputs resident in HBM), with
  * CUDA events around the whole loop; *ms is the mean device time per H*psi.

@@ -22,7 +22,8 @@ MIRRORS = {
     "tj_block_sub": S.TjBlockSub, "tj_block": S.TjBlock, "tj_block_set": S.TjBlockSet, "tj_model": S.TjModel,
     "tj_basis_sub": S.TjBasisSub, "tj_basis_map": S.TjBasisMap, "tj_basis": S.TjBasis,
     "tj_wave_sub": S.TjWaveSub, "tj_wave": S.TjWave, "tj_lattice": S.TjLattice,
-    "tj_trunc_result": S.TjTruncResult, "tj_hpsi_stats": S.TjHpsiStats,
+    "tj_trunc_result": S.TjTruncResult, "tj_hpsi_stats": S.TjHpsiStats, "tj_tune_result": S.TjTuneResult,
+    "tj_gg_cell": S.TjGgCell, "tj_gg_term": S.TjGgTerm,
     "tj_plan_operand": L.PlanOperand, "tj_plan_task": L.PlanTask, "tj_plan_cell": L.PlanCell,
     "tj_plan_upload": L.PlanUpload, "tj_plan_merge": L.PlanMerge, "tj_plan_item": L.PlanItem,
     "tj_plan_reduce": L.PlanReduce, "tj_plan_export": L.PlanExport,
@@ -41,7 +42,7 @@ def declared_functions():
 def test_header_declares_the_hot_path():
     names = declared_functions()
     for must in ("tj_model_wave", "tj_lanczos_memo_new", "tj_truncation", "tj_model_wave_noalloc",
-                 "tj_sys_site_env_site_cor_ndia", "tj_host_register"):
+                 "tj_sys_site_env_site_cor_ndia", "tj_host_register", "tj_autotune", "tj_grouped_gemm_bench"):
         assert must in names
 
 
