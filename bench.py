@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default tiling)")
     ap.add_argument("--no-microbench", action="store_true", help="skip the grouped block-GEMM microbenchmark")
+    ap.add_argument("--instances", type=int, default=1,
+                    help="K > 1: also time K independent superblocks (dopings 1/12, 1/10, 1/8, 1/6, ...) in shared "
+                         "launches against the same K run one after another")
     return ap.parse_args()
 
 
@@ -349,6 +352,25 @@ def main():
         del kept
         pinned.close()
 
+    shared = None
+    if args.instances > 1:
+        # independent instances of the same lattice at several dopings, one set of launches
+        geo = {"cyl4x24_m2000": (24, 4, 47, 47, 2000, {}), "cyl4x24_m500": (24, 4, 47, 47, 500, {}),
+               "cyl6x24_m6000": (24, 6, 71, 71, 6000, {"t2": -0.2})}[args.workload]
+        nx, ny, ls, le, m, kw = geo
+        dop = [1 / 12, 1 / 10, 1 / 8, 1 / 6, 1 / 14, 1 / 5, 1 / 16, 1 / 4][:args.instances]
+        ns = nx * ny
+        sbs = [synth.make_superblock(nx, ny, ls, le, m, ns - 2 * int(round(d * ns / 2)), args.seed + i, **kw)
+               for i, d in enumerate(dop)]
+        outs, ms_shared = head.model_wave_multi(sbs, reps=20)
+        sep = [head.model_wave_bench(s_, 20)[0] for s_ in sbs]
+        shared = {"instances": len(sbs), "dopings": dop, "holes": [ns - s_.tot_num_up if s_.tot_num_up else None
+                                                                   for s_ in sbs],
+                  "psi_dims": [s_.wave.dim for s_ in sbs], "shared_ms": ms_shared, "separate_ms": sep,
+                  "separate_ms_sum": sum(sep), "shared_speedup": sum(sep) / ms_shared,
+                  "hpsi_per_s_shared": len(sbs) * 1000.0 / ms_shared}
+        del sbs, outs
+
     micro = None
     if rank == 0 and not args.no_microbench:
         # grouped block-GEMM microbenchmark: 400 sector pairs, dims log-uniform in
@@ -426,6 +448,8 @@ def main():
             line["autotune"] = tune
         if micro is not None:
             line["grouped_gemm_microbench"] = micro
+        if shared is not None:
+            line["shared_launch"] = shared
         print(json.dumps(line), flush=True)
     ctx64.close()
     if ctxoz is not None:

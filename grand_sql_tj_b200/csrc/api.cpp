@@ -165,31 +165,47 @@ static uint64_t key_lattice(uint64_t h, const tj_lattice *L) {
   return fnv(h, L->esite, sizeof(double) * ns1);
 }
 
+static uint64_t instance_key(uint64_t h, const tj_lattice *lat, const tj_model *sys, const tj_model *env,
+                             const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave) {
+  h = key_lattice(h, lat);
+  h = key_model(h, sys);
+  h = key_model(h, env);
+  h = key_basis(h, sys_bs);
+  h = key_basis(h, env_bs);
+  return fnv(h, wave->sub, sizeof(tj_wave_sub) * wave->num);
+}
+
 // Compiles (or reuses) the plan of H*psi and uploads operators and work lists.
 int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const tj_model *env,
                       const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave) {
   if (!ctx || !lat || !sys || !env || !sys_bs || !env_bs || !wave) return set_err(TJ_ERR_ARG, "null argument");
   if (!lat->neib || !lat->nleg11 || !lat->jt || !sys->sub || !env->sub || !sys_bs->sub || !env_bs->sub || !wave->sub)
     return set_err(TJ_ERR_ARG, "null table in the inputs");
-  uint64_t h = 1469598103934665603ull;
-  h = key_lattice(h, lat);
-  h = key_model(h, sys);
-  h = key_model(h, env);
-  h = key_basis(h, sys_bs);
-  h = key_basis(h, env_bs);
-  h = fnv(h, wave->sub, sizeof(tj_wave_sub) * wave->num);
+  uint64_t h = instance_key(1469598103934665603ull, lat, sys, env, sys_bs, env_bs, wave);
   h = fnv(h, &ctx->prec_mode, sizeof ctx->prec_mode);
   h = fnv(h, &ctx->slices, sizeof ctx->slices);
   if (ctx->plan_valid && ctx->plan_key == h && tune_is_current(ctx)) return TJ_OK;
   ctx->plan_valid = false;
   CK(cudaSetDevice(ctx->device));
-  using clk = std::chrono::steady_clock;
-  auto ms_since = [](clk::time_point a) { return std::chrono::duration<double, std::milli>(clk::now() - a).count(); };
-  const auto t_start = clk::now();
+  const auto t_start = std::chrono::steady_clock::now();
   std::unique_ptr<HpsiPlan> P(new HpsiPlan());
   std::string msg;
   int rc = build_hpsi_plan(lat, sys, env, sys_bs, env_bs, wave, *P, msg);
   if (rc) return set_err(rc, "H*psi plan: " + msg);
+  if ((rc = install_plan(ctx, std::move(P), h, t_start))) return rc;
+  if (!ctx->tuning && ctx->autotune == TJ_TUNE_ON_MISS && !tune_lookup(ctx->hist_key, ctx->tune))
+    return autotune_plan(ctx, lat, sys, env, sys_bs, env_bs, wave, nullptr);
+  return TJ_OK;
+}
+
+// Installs a compiled plan: tiling choices, operator upload and hmerge, work
+// lists, and (split precision) the split-precision plan with the operator
+// splits of this step.
+int tjb::install_plan(tj_ctx *ctx, std::unique_ptr<HpsiPlan> P, uint64_t h,
+                      std::chrono::steady_clock::time_point t_start) {
+  using clk = std::chrono::steady_clock;
+  auto ms_since = [](clk::time_point a) { return std::chrono::duration<double, std::milli>(clk::now() - a).count(); };
+  int rc;
   // tiling choices: the autotuner's for this block-size histogram, when known
   ctx->hist_key = plan_hist_key(*P, ctx->prec_mode, ctx->slices);
   if (!ctx->tuning && ctx->autotune != TJ_TUNE_OFF) tune_lookup(ctx->hist_key, ctx->tune);
@@ -306,8 +322,6 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   ctx->plan_key = h;
   ctx->plan_tune = ctx->tune;
   ctx->plan_valid = true;
-  if (!ctx->tuning && ctx->autotune == TJ_TUNE_ON_MISS && !tune_lookup(ctx->hist_key, ctx->tune))
-    return autotune_plan(ctx, lat, sys, env, sys_bs, env_bs, wave, nullptr);
   return TJ_OK;
 }
 
@@ -449,6 +463,67 @@ extern "C" int tj_model_wave(tj_ctx *ctx, const tj_lattice *lat, const tj_model 
   ctx->stats.last_ms_phase2 = t[2];
   ctx->stats.last_ms = t[3];
   return TJ_OK;
+}
+
+extern "C" int tj_model_wave_multi(tj_ctx *ctx, int n, const tj_lattice *const *lat, const tj_model *const *sys,
+                                   const tj_model *const *env, const tj_basis *const *sys_bs,
+                                   const tj_basis *const *env_bs, const tj_wave *const *invec,
+                                   tj_wave *const *outvec, int reps, double *ms) {
+  int rc;
+  if (!ctx || n < 1 || !lat || !sys || !env || !sys_bs || !env_bs || !invec || !outvec)
+    return set_err(TJ_ERR_ARG, "tj_model_wave_multi: null argument");
+  if (reps < 0 || (reps > 0 && !ms)) return set_err(TJ_ERR_ARG, "tj_model_wave_multi: bad reps");
+  uint64_t h = 1469598103934665603ull;
+  for (int i = 0; i < n; ++i) {
+    if (!lat[i] || !sys[i] || !env[i] || !sys_bs[i] || !env_bs[i]) return set_err(TJ_ERR_ARG, "null instance input");
+    if (!lat[i]->neib || !lat[i]->nleg11 || !lat[i]->jt || !sys[i]->sub || !env[i]->sub || !sys_bs[i]->sub ||
+        !env_bs[i]->sub)
+      return set_err(TJ_ERR_ARG, "null table in the inputs");
+    if ((rc = check_wave(invec[i])) || (rc = check_wave(outvec[i]))) return rc;
+    if (!same_layout(invec[i], outvec[i])) return set_err(TJ_ERR_ARG, "outvec must have invec's sector layout");
+    h = instance_key(h, lat[i], sys[i], env[i], sys_bs[i], env_bs[i], invec[i]);
+  }
+  h = fnv(h, &n, sizeof n);
+  h = fnv(h, &ctx->prec_mode, sizeof ctx->prec_mode);
+  h = fnv(h, &ctx->slices, sizeof ctx->slices);
+  CK(cudaSetDevice(ctx->device));
+  if (!(ctx->plan_valid && ctx->plan_key == h && tune_is_current(ctx) && (int)ctx->multi_off.size() == n)) {
+    ctx->plan_valid = false;
+    const auto t_start = std::chrono::steady_clock::now();
+    std::vector<HpsiPlan> parts(n);
+    std::vector<const HpsiPlan *> pp;
+    for (int i = 0; i < n; ++i) {
+      std::string msg;
+      rc = build_hpsi_plan(lat[i], sys[i], env[i], sys_bs[i], env_bs[i], invec[i], parts[i], msg);
+      if (rc) return set_err(rc, "H*psi plan of instance " + std::to_string(i) + ": " + msg);
+      pp.push_back(&parts[i]);
+    }
+    std::unique_ptr<HpsiPlan> P(new HpsiPlan());
+    merge_plans(pp, *P, ctx->multi_off);
+    if ((rc = install_plan(ctx, std::move(P), h, t_start))) return rc;
+  }
+  const int64_t D = ctx->plan->psi_len;
+  if ((rc = ctx->vin.reserve(sizeof(double) * (D + 4))) || (rc = ctx->vout.reserve(sizeof(double) * (D + 4))))
+    return rc;
+  for (int i = 0; i < n; ++i)
+    CK(cudaMemcpyAsync(ctx->vin.d() + ctx->multi_off[i], invec[i]->data, sizeof(double) * invec[i]->dim,
+                       cudaMemcpyHostToDevice, ctx->stream));
+  if ((rc = run_hpsi(ctx, ctx->vin.d(), ctx->vout.d(), true))) return rc;
+  if (reps > 0) {
+    CK(cudaEventRecord(ctx->ev[5], ctx->stream));
+    for (int r = 0; r < reps; ++r)
+      if ((rc = run_hpsi(ctx, ctx->vin.d(), ctx->vout.d(), false))) return rc;
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    CK(cudaEventSynchronize(ctx->ev[0]));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, ctx->ev[5], ctx->ev[0]));
+    *ms = t / reps;
+  }
+  for (int i = 0; i < n; ++i)
+    CK(cudaMemcpyAsync(outvec[i]->data, ctx->vout.d() + ctx->multi_off[i], sizeof(double) * outvec[i]->dim,
+                       cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return check_device_flags(ctx);
 }
 
 extern "C" int tj_model_wave_bench(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const tj_model *env,

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <memory>
 #include <string>
 #include <vector>
@@ -45,6 +46,7 @@ struct tj_ctx {
   bool tuning = false;        // inside tj_autotune (prepare_hpsi must not recurse)
   uint64_t hist_key = 0;      // block-size histogram of the current plan
   tjb::TuneParams plan_tune;  // the choices the current plan was built with
+  std::vector<int64_t> multi_off;   // shared-launch plan: offset of each instance's vector
   // compiled H*psi of the current step
   std::unique_ptr<tjb::HpsiPlan> plan;
   uint64_t plan_key = 0;
@@ -81,6 +83,7 @@ int prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const 
                  const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave);
 int run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed);
 int check_device_flags(tj_ctx *ctx);
+int install_plan(tj_ctx *ctx, std::unique_ptr<HpsiPlan> P, uint64_t key, std::chrono::steady_clock::time_point t0);
 
 // autotuning (tune.cpp)
 // key of the plan's block-size histogram: GEMM tasks counted by

@@ -1750,3 +1750,78 @@ extern "C" int tj_cor_plan_export(int kind, const tj_block *a, const tj_block *b
   if (rc) return tjb_set_err(rc, "correlator plan: " + msg);
   return export_plan(P, out);
 }
+
+namespace tjb {
+
+// Independent superblocks in one plan: instance i's operators, input and
+// output vector, phase-1 products and basis-state indices are placed after
+// those of the instances before it, and the work items are cut again over
+// the union, so that one set of launches computes every instance's H*psi.
+void merge_plans(const std::vector<const HpsiPlan *> &parts, HpsiPlan &out, std::vector<int64_t> &psi_off,
+                 const TuneParams &tp) {
+  out = HpsiPlan();
+  psi_off.clear();
+  for (const HpsiPlan *p : parts) {
+    const int64_t ob = out.ops_len, pb = out.psi_len, sb = out.scratch_len;
+    const int t1 = (int)out.tasks1.size(), t2 = (int)out.tasks2.size();
+    const int mb = (int)out.merge_src.size();
+    const int32_t ss = out.n_sys_states, es = out.n_env_states;
+    psi_off.push_back(pb);
+    auto shift = [&](Operand &o) {
+      if (o.space == SP_OPS) o.off += ob;
+      else if (o.space == SP_PSI) o.off += pb;
+      else if (o.space == SP_SCR) o.off += sb;
+    };
+    for (HpsiPlan::Upload u : p->uploads) {
+      u.dst += ob;
+      out.uploads.push_back(u);
+    }
+    for (HpsiPlan::Merge m : p->merges) {
+      m.dst += ob;
+      m.s_begin += mb;
+      m.s_end += mb;
+      out.merges.push_back(m);
+    }
+    for (int64_t s : p->merge_src) out.merge_src.push_back(s + ob);
+    out.merge_coef.insert(out.merge_coef.end(), p->merge_coef.begin(), p->merge_coef.end());
+    for (auto e : p->sub_extent) out.sub_extent.push_back({e.first + ob, e.second});
+    for (Task t : p->tasks1) {
+      shift(t.L);
+      shift(t.R);
+      out.tasks1.push_back(t);
+    }
+    for (Task t : p->tasks2) {
+      shift(t.L);
+      shift(t.R);
+      out.tasks2.push_back(t);
+    }
+    for (Cell c : p->cells1) {
+      c.off += sb;
+      c.t_begin += t1;
+      c.t_end += t1;
+      out.cells1.push_back(c);
+    }
+    for (Cell c : p->cells2) {
+      c.off += pb;
+      c.t_begin += t2;
+      c.t_end += t2;
+      out.cells2.push_back(c);
+    }
+    for (int32_t s : p->cell2_row_state) out.cell2_row_state.push_back(s + ss);
+    for (int32_t s : p->cell2_col_state) out.cell2_col_state.push_back(s + es);
+    for (int32_t s : p->cell1_row_state) out.cell1_row_state.push_back(s + ss);
+    out.n_sys_states += p->n_sys_states;
+    out.n_env_states += p->n_env_states;
+    out.ops_len += p->ops_len;
+    out.psi_len += p->psi_len;
+    out.scratch_len += p->scratch_len;
+    out.flops += p->flops;
+    out.flops_ref += p->flops_ref;
+    out.bytes += p->bytes;
+    out.key += p->key;
+  }
+  split_tiles(out.cells1, out.tasks1, out.tiles1, out.red1, out.nslots1, false, tp);
+  split_tiles(out.cells2, out.tasks2, out.tiles2, out.red2, out.nslots2, false, tp);
+}
+
+}  // namespace tjb

@@ -122,6 +122,11 @@ int build_hpsi_plan(const tj_lattice *lat, const tj_model *sys, const tj_model *
                     const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave,
                     HpsiPlan &plan, std::string &msg);
 
+// Independent superblocks in one plan (shared launches); psi_off[i]: offset of
+// instance i's vector in the concatenated input / output vector.
+void merge_plans(const std::vector<const HpsiPlan *> &parts, HpsiPlan &out, std::vector<int64_t> &psi_off,
+                 const TuneParams &tp = TuneParams());
+
 // Racah 6j symbol on doubled spins (host); same formula as the reference's W6JS.
 double w6j(int j1, int j2, int j3, int l1, int l2, int l3);
 

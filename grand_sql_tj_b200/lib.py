@@ -175,6 +175,9 @@ def lib():
                                     P(TjTruncResult)]
         L.tj_hpsi_stats_get.argtypes = [C.c_void_p, P(TjHpsiStats)]
         L.tj_set_autotune.argtypes = [C.c_void_p, C.c_int]
+        L.tj_model_wave_multi.argtypes = [C.c_void_p, C.c_int, P(P(TjLattice)), P(P(TjModel)), P(P(TjModel)),
+                                          P(P(TjBasis)), P(P(TjBasis)), P(P(TjWave)), P(P(TjWave)), C.c_int,
+                                          P(C.c_double)]
         L.tj_autotune.argtypes = [C.c_void_p, P(TjLattice), P(TjModel), P(TjModel), P(TjBasis), P(TjBasis),
                                   P(TjWave), P(TjTuneResult)]
         L.tj_grouped_gemm_bench.argtypes = [C.c_void_p, P(TjGgCell), C.c_int, P(TjGgTerm), C.c_int,
@@ -234,6 +237,26 @@ class Context:
         s = TjHpsiStats()
         _chk(lib().tj_hpsi_stats_get(self.h, C.byref(s)))
         return s
+
+    def model_wave_multi(self, sbs, reps: int = 0, invecs=None):
+        """tj_model_wave_multi: H*psi of independent superblocks in shared launches.
+        Returns (outputs, ms of one shared product when reps > 0)."""
+        P = C.POINTER
+        n = len(sbs)
+        invecs = [sb.wave for sb in sbs] if invecs is None else invecs
+        packs = [pack_superblock(sb) for sb in sbs]
+        outs = [w.like() for w in invecs]
+        arr = lambda t, xs: (P(t) * n)(*[C.pointer(x) for x in xs])
+        lat = arr(TjLattice, [sb.lat.c for sb in sbs])
+        sysm = arr(TjModel, [p[0].c for p in packs])
+        envm = arr(TjModel, [p[1].c for p in packs])
+        sbs_ = arr(TjBasis, [p[2].c for p in packs])
+        ebs_ = arr(TjBasis, [p[3].c for p in packs])
+        ins = arr(TjWave, [w.c for w in invecs])
+        ous = arr(TjWave, [w.c for w in outs])
+        ms = C.c_double()
+        _chk(lib().tj_model_wave_multi(self.h, n, lat, sysm, envm, sbs_, ebs_, ins, ous, reps, C.byref(ms)))
+        return outs, (ms.value if reps > 0 else None)
 
     def set_autotune(self, mode: int):
         _chk(lib().tj_set_autotune(self.h, mode))

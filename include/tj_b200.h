@@ -246,6 +246,20 @@ typedef struct tj_hpsi_stats {
 } tj_hpsi_stats;
 int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st);
 
+/* ---------------------------------------------- independent instances */
+/* No counterpart in the reference.  model_wave (with hmerge) of n
+ * independent superblocks -- several DMRG runs at different dopings or J/t,
+ * each with its own lattice, models, bases and wavefunction -- in shared
+ * launches: the instances' plans are merged into one (operators, vectors,
+ * products and basis-state scales placed one after another) so that one set
+ * of kernels computes every outvec[i] = H_i invec[i].  The merged plan is
+ * cached like the single one.  reps > 0: after the product, `reps` more
+ * products of all instances are timed on the device and *ms receives the
+ * mean time of one. */
+int tj_model_wave_multi(tj_ctx *ctx, int n, const tj_lattice *const *lat, const tj_model *const *sys,
+                        const tj_model *const *env, const tj_basis *const *sys_bs, const tj_basis *const *env_bs,
+                        const tj_wave *const *invec, tj_wave *const *outvec, int reps, double *ms);
+
 /* ------------------------------------------------------------ autotuning */
 /* No counterpart in the reference.  The tiling of the grouped FP64 GEMM
  * (split-K granularity: items per resident CTA and minimum inner-dimension
