@@ -264,6 +264,10 @@ struct OzCfg {
   static constexpr int STAGES = STAGES_RAW > 8 ? 8 : STAGES_RAW;
   static constexpr int SMEM = STAGES * STAGE;
   static_assert(S * BN <= 256, "diagonal accumulators exceed one TMEM buffer");
+  // k-blocks one TMEM accumulation may take: a diagonal sums at most S slice
+  // products of 127^2 per k, and must stay below 2^31; longer families are
+  // accumulated in pieces and the pieces added in FP64
+  static constexpr int KB_PIECE = (int)(2147483647LL / (32LL * S * 127 * 127));
   static_assert(STAGES >= 2, "too few pipeline stages");
 };
 
@@ -276,6 +280,7 @@ template <int BN>
 struct OzMeta {
   double cs[2][BN];
   double rs[2][128];
+  int32_t npiece[2];             // accumulations of each family (pieces of at most OzCfg::KB_PIECE k-blocks)
   int64_t c_off;                 // offset of the tile's (row0, col0) in out (cells) or scr (products)
   int32_t c_ld, na;              // cells: leading dimension; axpy terms (init items)
   double ax_coef[OZ_META_AX];
@@ -426,7 +431,9 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
         const uint32_t aslice16 = (uint32_t)((it.mrows + 7) >> 3) * 16u;   // A slice stride in 16-byte units
         const int nf = it.fam_end - it.fam_begin;
         for (int f = 0; f < nf && ok; ++f) {
-          const int nkb = p.fams[it.fam_begin + f].nkb;
+          const int nkb_f = p.fams[it.fam_begin + f].nkb;
+          for (int k0 = 0; k0 < nkb_f && ok; k0 += C::KB_PIECE) {
+          const int nkb = min(C::KB_PIECE, nkb_f - k0);
           const uint32_t buf = famc & 1u, use = famc >> 1;
           if (!oz_wait(oz_smem(&tempty_bar[buf]), (use & 1u) ^ 1u, &abort_sh)) {
             if (!abort_sh) oz_fail(&abort_sh, p.err);
@@ -464,6 +471,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
           if (!ok) break;
           oz_commit(oz_smem(&tfull_bar[buf]));
           ++famc;
+          }
         }
       }
       if (issued) {
@@ -489,6 +497,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       const int nf = it.fam_end - it.fam_begin;   // at most 2 (checked by the plan)
       for (int f = 0; f < nf; ++f) {
         const OzFam fm = p.fams[it.fam_begin + f];
+        if (lane == 0) m.npiece[f] = (fm.nkb + C::KB_PIECE - 1) / C::KB_PIECE;
         for (int j = lane; j < it.ncols; j += 32) m.cs[f][j] = oz_pow2_of(p.scales[fm.cs_idx + it.col0 + j]);
         for (int r = lane; r < it.mrows; r += 32) m.rs[f][r] = oz_pow2_of(p.scales[fm.rs_idx + it.row0 + r]);
       }
@@ -606,7 +615,8 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       double accv[HCH * 8];
 #pragma unroll
       for (int j = 0; j < HCH * 8; ++j) accv[j] = 0.0;
-      for (int f = 0; f < nf; ++f) {
+      for (int f = 0; f < nf && ok; ++f)
+      for (int pc = 0; pc < m.npiece[f]; ++pc) {
         const uint32_t buf = famc & 1u, use = famc >> 1;
         const double rscale = rv ? m.rs[f][r] : 0.0;
         if (!oz_wait(oz_smem(&tfull_bar[buf]), use & 1u, &abort_sh)) {

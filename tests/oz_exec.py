@@ -141,7 +141,9 @@ class _Machine:
                 As, Bs = zip(*[operands(oz["segs"][sgi]) for sgi in range(fm.seg_begin, fm.seg_end)])
                 A = np.concatenate(As, axis=2)[:, :it.mrows]
                 B = np.concatenate(Bs, axis=2)[:, :it.ncols]
-                acc = self.accum(A, B)
+                # the device accumulates at most kb_piece k-blocks in int32, then adds the pieces
+                kp = 32 * ((2 ** 31 - 1) // (32 * self.S * 127 * 127))
+                acc = sum(self.accum(A[:, :, k0:k0 + kp], B[:, :, k0:k0 + kp]) for k0 in range(0, A.shape[2], kp))
                 rs = _pow2_of(self.scales[fm.rs_idx + rows])
                 cs = _pow2_of(self.scales[fm.cs_idx + cols])
                 tot = tot + (acc * rs[:, None]) * cs[None, :]

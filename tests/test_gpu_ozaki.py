@@ -77,3 +77,20 @@ def test_ozaki_lanczos_energy_per_site(ctx, product_lib):
     nsite = sb.geo.num_site
     assert abs(e - e64) / nsite <= 1e-9, (e, e64)
     assert abs(float(np.dot(w.data, w64.data))) >= 1 - 1e-7
+
+
+def test_ozaki_long_families_in_pieces(product_lib):
+    """6x24 m=6000: families longer than one int32 accumulation (about 26k
+    inner dimension at 5 slices) are accumulated in pieces; 7 slices must
+    reproduce the FP64 device result to 1e-12 of max|H psi|."""
+    from grand_sql_tj_b200.lib import TJ_PREC_OZAKI, Context
+    sb = synth.workload("cyl6x24_m6000", seed=8)
+    f, o = Context(0), Context(0)
+    try:
+        o.set_precision(TJ_PREC_OZAKI, 7)
+        ref = f.model_wave(sb).data
+        got = o.model_wave(sb).data
+    finally:
+        f.close()
+        o.close()
+    assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
