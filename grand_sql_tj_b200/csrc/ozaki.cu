@@ -188,20 +188,26 @@ __device__ __forceinline__ uint64_t oz_now_ns() {
 
 constexpr uint64_t OZ_WAIT_NS = 2000000000ull;
 
+__device__ __forceinline__ bool oz_try(uint32_t mbar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 // Waits for the phase of the given parity; false after ~2 s or when another
-// role has aborted (*abort != 0).
+// role has aborted (*abort != 0).  The clock is read only once the first try
+// has failed (a phase that has already completed costs one try).
 __device__ __forceinline__ bool oz_wait(uint32_t mbar, uint32_t parity, volatile int *abort) {
+  if (oz_try(mbar, parity)) return true;
   const uint64_t t0 = oz_now_ns();
   for (;;) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, P1;\n\t}"
-        : "=r"(ok)
-        : "r"(mbar), "r"(parity)
-        : "memory");
-    if (ok) return true;
+    if (oz_try(mbar, parity)) return true;
     if (abort && *abort) return false;
     if (oz_now_ns() - t0 > OZ_WAIT_NS) return false;
   }
