@@ -263,8 +263,14 @@ __device__ __forceinline__ void oz_commit(uint32_t mbar) {
 
 template <int S, int BN>
 struct OzCfg {
-  static constexpr int A_BYTES = S * 16 * 256;          // 128 rows x 32 k, s slices
-  static constexpr int B_BYTES = S * (BN / 8) * 256;
+  // a stage holds KPS consecutive k-blocks of an item's family: the cost of a
+  // stage (barriers, copies, MMA issue) is nearly fixed, so fewer, larger
+  // stages go faster
+  static constexpr int KPS = 2;
+  static constexpr int A_KB = S * 16 * 256;             // one k-block: 128 rows x 32 k, s slices
+  static constexpr int B_KB = S * (BN / 8) * 256;
+  static constexpr int A_BYTES = KPS * A_KB;
+  static constexpr int B_BYTES = KPS * B_KB;
   static constexpr int STAGE = A_BYTES + B_BYTES;
   static constexpr int STAGES_RAW = (200 * 1024) / STAGE;
   static constexpr int STAGES = STAGES_RAW > 8 ? 8 : STAGES_RAW;
@@ -273,7 +279,7 @@ struct OzCfg {
   // k-blocks one TMEM accumulation may take: a diagonal sums at most S slice
   // products of 127^2 per k, and must stay below 2^31; longer families are
   // accumulated in pieces and the pieces added in FP64
-  static constexpr int KB_PIECE = (int)(2147483647LL / (32LL * S * 127 * 127));
+  static constexpr int KB_PIECE = (int)(2147483647LL / (32LL * S * 127 * 127)) / KPS * KPS;
   static_assert(STAGES >= 2, "too few pipeline stages");
 };
 
@@ -380,10 +386,15 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       // tiles of this item: A row tile ta (ga groups), B column tile tb (gb groups)
       const uint32_t ga = (uint32_t)((it.mrows + 7) >> 3), gb = (uint32_t)(it.N >> 3);
       const int64_t ta = it.row0 / 128, tb = it.col0 / BN;
-      const uint32_t bytes = (ga + gb) * GB;
+      const uint32_t bytes1 = (ga + gb) * GB;   // one k-block of both operands
       for (int f = it.fam_begin; f < it.fam_end && ok; ++f) {
         const OzFam fm = p.fams[f];
         const int sb = fm.seg_begin, se = fm.seg_end;
+        // the family's k-blocks, segment after segment, fill stages of up to
+        // KPS k-blocks (a stage may hold the end of one segment and the start
+        // of the next; stage boundaries fall every KPS k-blocks of the family)
+        int done = 0, in_stage = 0;
+        uint32_t sa = 0, sbb = 0, fbar = 0;
         for (int s0 = sb; s0 < se && ok; s0 += 32) {
           // the next <= 32 segments, one per lane
           OzSeg mine;
@@ -400,15 +411,23 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
             const uint8_t *asrc = p.pack + a_base + ta * a_nkb * (int64_t)(16 * GB) + (int64_t)a_kb0 * ga * GB;
             const uint8_t *bsrc = p.pack + b_base + tb * b_nkb * (int64_t)((BN / 8) * GB) + (int64_t)b_kb0 * gb * GB;
             for (int kb = 0; kb < nkb; ++kb) {
-              if (!acquire(bytes)) {
-                ok = false;
-                break;
+              if (in_stage == 0) {
+                const int n = min(C::KPS, fm.nkb - done);
+                if (!acquire((uint32_t)n * bytes1)) {
+                  ok = false;
+                  break;
+                }
+                sa = smem0 + (uint32_t)(stage * C::STAGE);
+                sbb = sa + C::A_BYTES;
+                fbar = oz_smem(&full_bar[stage]);
               }
-              const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE), sbb = sa + C::A_BYTES;
-              const uint32_t fbar = oz_smem(&full_bar[stage]);
-              if (lane == 0) oz_bulk_g2s(sa, asrc + (int64_t)kb * ga * GB, ga * GB, fbar);
-              if (lane == 1) oz_bulk_g2s(sbb, bsrc + (int64_t)kb * gb * GB, gb * GB, fbar);
-              if (++stage == ST) stage = 0, ph ^= 1u;
+              if (lane == 0) oz_bulk_g2s(sa + in_stage * ga * GB, asrc + (int64_t)kb * ga * GB, ga * GB, fbar);
+              if (lane == 1) oz_bulk_g2s(sbb + in_stage * gb * GB, bsrc + (int64_t)kb * gb * GB, gb * GB, fbar);
+              ++done;
+              if (++in_stage == C::KPS || done == fm.nkb) {
+                in_stage = 0;
+                if (++stage == ST) stage = 0, ph ^= 1u;
+              }
             }
           }
         }
@@ -435,6 +454,8 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
 #pragma unroll
         for (int pa = 1; pa <= S; ++pa) idesc[pa - 1] = oz_idesc(it.M, (S + 1 - pa) * it.N);
         const uint32_t aslice16 = (uint32_t)((it.mrows + 7) >> 3) * 16u;   // A slice stride in 16-byte units
+        const uint32_t ga_gb = (uint32_t)((it.mrows + 7) >> 3) * GB;       // bytes of one A k-block
+        const uint32_t gb_gb = (uint32_t)(it.N >> 3) * GB;                 // bytes of one B k-block
         const int nf = it.fam_end - it.fam_begin;
         for (int f = 0; f < nf && ok; ++f) {
           const int nkb_f = p.fams[it.fam_begin + f].nkb;
@@ -448,7 +469,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
           }
           asm volatile("tcgen05.fence::after_thread_sync;");
           const uint32_t dt = tmem + buf * 256u;
-          for (int kb = 0; kb < nkb; ++kb) {
+          for (int kb = 0; kb < nkb; kb += C::KPS) {
             if (!oz_wait(oz_smem(&full_bar[stage]), ph, &abort_sh)) {
               if (!abort_sh) oz_fail(&abort_sh, p.err);
               ok = false;
@@ -456,19 +477,23 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
             const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE);
-            const uint64_t da0 = dbase + (uint64_t)(sa >> 4);
-            const uint64_t db = dbase + (uint64_t)((sa + C::A_BYTES) >> 4);
+            const int n = min(C::KPS, nkb - kb);   // k-blocks in this stage
+            for (int j = 0; j < n; ++j) {
+              // k-block j of the stage: A at sa + j ga GB, B at sa + A_BYTES + j gb GB
+              const uint64_t da0 = dbase + (uint64_t)((sa + (uint32_t)j * ga_gb) >> 4);
+              const uint64_t db = dbase + (uint64_t)((sa + C::A_BYTES + (uint32_t)j * gb_gb) >> 4);
 #pragma unroll
-            for (int pa = 1; pa <= S; ++pa) {
-              const uint64_t da = da0 + (uint64_t)((pa - 1) * aslice16);   // A slices ga groups apart
-              const uint32_t d = dt + (uint32_t)((pa - 1) * it.N);
-              const uint32_t acc = (kb == 0 && pa == 1) ? 0u : 1u;
-              asm volatile(
-                  "{\n\t.reg .pred p;\n\t"
-                  "setp.ne.b32 p, %4, 0;\n\t"
-                  "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-                  :
-                  : "r"(d), "l"(da), "l"(db), "r"(idesc[pa - 1]), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+              for (int pa = 1; pa <= S; ++pa) {
+                const uint64_t da = da0 + (uint64_t)((pa - 1) * aslice16);   // A slices ga groups apart
+                const uint32_t d = dt + (uint32_t)((pa - 1) * it.N);
+                const uint32_t acc = (kb == 0 && j == 0 && pa == 1) ? 0u : 1u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                    :
+                    : "r"(d), "l"(da), "l"(db), "r"(idesc[pa - 1]), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+              }
             }
             issued = true;
             oz_commit(oz_smem(&empty_bar[stage]));   // frees the stage when these MMAs finish
