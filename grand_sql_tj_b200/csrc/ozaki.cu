@@ -410,7 +410,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
             const int32_t nkb = __shfl_sync(0xffffffffu, mine.nkb, j);
             const uint8_t *asrc = p.pack + a_base + ta * a_nkb * (int64_t)(16 * GB) + (int64_t)a_kb0 * ga * GB;
             const uint8_t *bsrc = p.pack + b_base + tb * b_nkb * (int64_t)((BN / 8) * GB) + (int64_t)b_kb0 * gb * GB;
-            for (int kb = 0; kb < nkb; ++kb) {
+            for (int kb = 0; kb < nkb;) {
               if (in_stage == 0) {
                 const int n = min(C::KPS, fm.nkb - done);
                 if (!acquire((uint32_t)n * bytes1)) {
@@ -421,10 +421,17 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
                 sbb = sa + C::A_BYTES;
                 fbar = oz_smem(&full_bar[stage]);
               }
-              if (lane == 0) oz_bulk_g2s(sa + in_stage * ga * GB, asrc + (int64_t)kb * ga * GB, ga * GB, fbar);
-              if (lane == 1) oz_bulk_g2s(sbb + in_stage * gb * GB, bsrc + (int64_t)kb * gb * GB, gb * GB, fbar);
-              ++done;
-              if (++in_stage == C::KPS || done == fm.nkb) {
+              // the k-blocks of this segment that go into the current stage are
+              // contiguous in the split and in the stage: one copy per operand
+              const int take = min(nkb - kb, C::KPS - in_stage);
+              if (lane == 0)
+                oz_bulk_g2s(sa + in_stage * ga * GB, asrc + (int64_t)kb * ga * GB, (uint32_t)take * ga * GB, fbar);
+              if (lane == 1)
+                oz_bulk_g2s(sbb + in_stage * gb * GB, bsrc + (int64_t)kb * gb * GB, (uint32_t)take * gb * GB, fbar);
+              kb += take;
+              done += take;
+              in_stage += take;
+              if (in_stage == C::KPS || done == fm.nkb) {
                 in_stage = 0;
                 if (++stage == ST) stage = 0, ph ^= 1u;
               }

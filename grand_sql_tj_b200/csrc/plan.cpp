@@ -10,6 +10,8 @@
 // operators (block_transfer_trans, block.f90:1676-1706) are never copied: a
 // transposed view only flips the operand's transpose flag.
 #include <algorithm>
+#include <functional>
+#include <unordered_set>
 #include <array>
 #include <climits>
 #include <cmath>
@@ -77,6 +79,7 @@ struct OSub {
   int num_up, num_down, down_dif, row_dim, sdim;
   int64_t off;   // device offset of the stored matrix
   bool zero;     // structurally zero (merged sub-block without contributions)
+  mutable bool touched = false;   // read by some task of the plan being built
 };
 struct OBlk {
   int len = 0, up_dif = 0, down_dif = 0;
@@ -199,12 +202,19 @@ void split_tiles(const std::vector<Cell> &cells, const std::vector<Task> &tasks,
   // never below tp.min_ksteps k-steps per item
   const double target =
       std::max((double)tp.min_ksteps, total / (148.0 * std::max(1, tp.ctas_per_sm) * std::max(1, tp.items_per_cta)));
-  std::vector<std::pair<double, Tile>> w;
+  // tiles in emission order with their weights; sorted below by weight,
+  // heaviest first, ties kept in emission order
+  std::vector<Tile> all;
+  std::vector<std::pair<double, int64_t>> w;
+  all.reserve((size_t)ntile + cells.size());
+  w.reserve((size_t)ntile + cells.size());
+  std::vector<double> chunk_w;
+  std::vector<std::pair<int, int>> chunks;
   for (int ci = 0; ci < (int)cells.size(); ++ci) {
     const Cell &c = cells[ci];
     int gb = c.t_begin, ge = c.t_begin;   // GEMM tasks [gb, ge), axpys [ge, t_end)
     while (ge < c.t_end && tasks[ge].R.space != SP_NONE) ++ge;
-    std::vector<std::pair<int, int>> chunks;
+    chunks.clear();
     double acc = 0;
     int start = gb;
     for (int t = gb; t < ge; ++t) {
@@ -217,6 +227,9 @@ void split_tiles(const std::vector<Cell> &cells, const std::vector<Task> &tasks,
     }
     chunks.push_back({start, ge});
     const bool split = chunks.size() > 1 && !dot_mode;
+    chunk_w.assign(chunks.size(), 1.0);
+    for (size_t k = 0; k < chunks.size(); ++k)
+      for (int t = chunks[k].first; t < chunks[k].second; ++t) chunk_w[k] += tasks[t].K;
     for (int r = 0; r < c.M; r += BM)
       for (int q = 0; q < c.N; q += BN) {
         int slot0 = -1;
@@ -226,8 +239,6 @@ void split_tiles(const std::vector<Cell> &cells, const std::vector<Task> &tasks,
           red.push_back(Reduce{ci, r, q, slot0, (int)chunks.size(), ge, c.t_end, 0});
         }
         for (size_t k = 0; k < chunks.size(); ++k) {
-          double kw = 1;
-          for (int t = chunks[k].first; t < chunks[k].second; ++t) kw += tasks[t].K;
           Tile t;
           t.cell = ci;
           t.row0 = r;
@@ -238,14 +249,26 @@ void split_tiles(const std::vector<Cell> &cells, const std::vector<Task> &tasks,
           t.ab = ge;
           t.ae = (!split && k == 0) ? c.t_end : ge;
           t.slot = split ? slot0 + (int)k : -1;
-          w.push_back({kw, t});
+          w.push_back({chunk_w[k], (int64_t)all.size()});
+          all.push_back(t);
         }
       }
   }
-  std::stable_sort(w.begin(), w.end(), [](const std::pair<double, Tile> &a, const std::pair<double, Tile> &b) {
-    return a.first > b.first;
-  });
-  for (auto &p : w) tiles.push_back(p.second);
+  // the weights take few distinct values: a stable counting sort over their
+  // ranks (heaviest first) gives the order of a stable sort by weight
+  std::unordered_set<double> distinct;
+  for (auto &p : w) distinct.insert(p.first);
+  std::vector<double> uniq(distinct.begin(), distinct.end());
+  std::sort(uniq.begin(), uniq.end(), std::greater<double>());
+  std::vector<int64_t> start(uniq.size() + 1, 0);
+  std::vector<int32_t> rank(w.size());
+  for (size_t j = 0; j < w.size(); ++j) {
+    rank[j] = (int32_t)(std::lower_bound(uniq.begin(), uniq.end(), w[j].first, std::greater<double>()) - uniq.begin());
+    ++start[rank[j] + 1];
+  }
+  for (size_t r = 0; r < uniq.size(); ++r) start[r + 1] += start[r];
+  tiles.resize(all.size());
+  for (size_t j = 0; j < w.size(); ++j) tiles[start[rank[j]]++] = all[w[j].second];
 }
 
 namespace {
@@ -263,9 +286,23 @@ struct Builder {
   int ncells = 0;
   std::map<std::tuple<int, int, int, int>, int> sec_of;   // first sector with the labels
   // tasks
-  std::vector<std::vector<Task>> cell_tasks;
-  std::unordered_map<std::string, int> prod_id;
-  std::vector<int64_t> op_touched;
+  std::vector<Task> out_tasks;      // phase-2 tasks in emission order
+  std::vector<int32_t> out_cell;    // and the output cell of each
+  // phase-1 products op(A) * X already emitted: key (operator offset, transpose, psi cell)
+  struct ProdKey {
+    int64_t off;
+    int32_t xc;
+    int32_t trans;
+    bool operator==(const ProdKey &o) const { return off == o.off && xc == o.xc && trans == o.trans; }
+  };
+  struct ProdKeyHash {
+    size_t operator()(const ProdKey &k) const {
+      uint64_t h = (uint64_t)k.off * 0x9e3779b97f4a7c15ull;
+      h ^= ((uint64_t)(uint32_t)k.xc << 1 | (uint64_t)(k.trans & 1)) + 0x632be59bd9b4e019ull + (h << 6) + (h >> 2);
+      return (size_t)h;
+    }
+  };
+  std::unordered_map<ProdKey, int, ProdKeyHash> prod_id;
   bool dedup = true;
   bool cor_mode = false;   // correlators: keep only the cells that have tasks
 
@@ -339,7 +376,8 @@ struct Builder {
           cell_N[c] = b.sdim;
         }
     }
-    cell_tasks.assign(ncells, {});
+    out_tasks.clear();
+    out_cell.clear();
   }
   int cell(int i, int m, int n) const { return cell_base[i] + m * ebs->sub[sec_y[i]].num + n; }
   int find_sec(int su, int sd, int eu, int ed) const {
@@ -360,8 +398,10 @@ struct Builder {
     std::memset(&o, 0, sizeof o);
     return o;
   }
-  void touch(const Operand &o) {
-    if (o.space == SP_OPS) op_touched.push_back(o.off);
+  static void touch(const OView &V, int k) { V.b->sub[k].touched = true; }
+  void add_task(int oc, const Task &t) {
+    out_tasks.push_back(t);
+    out_cell.push_back(oc);
   }
 
   // out(oc) += coef * op(A) * X(xc); op(A) is (rows x K)
@@ -376,8 +416,8 @@ struct Builder {
     t.coef = coef;
     t.K = K;
     t.pad = 0;
-    touch(t.L);
-    cell_tasks[oc].push_back(t);
+    touch(A, ka);
+    add_task(oc, t);
     const double f = 2.0 * rows * cell_N[oc] * (double)K;
     plan.flops += f;
     plan.flops_ref += f + ref_extra;
@@ -394,8 +434,8 @@ struct Builder {
     t.coef = coef;
     t.K = K;
     t.pad = 0;
-    touch(t.R);
-    cell_tasks[oc].push_back(t);
+    touch(B, kb);
+    add_task(oc, t);
     const double f = 2.0 * cell_M[oc] * cols * (double)K;
     plan.flops += f;
     plan.flops_ref += f;
@@ -411,7 +451,7 @@ struct Builder {
     t.coef = coef;
     t.K = 0;
     t.pad = 0;
-    cell_tasks[oc].push_back(t);
+    add_task(oc, t);
     plan.flops += 2.0 * cell_M[oc] * cell_N[oc];
     plan.flops_ref += 2.0 * cell_M[oc] * cell_N[oc];
   }
@@ -423,8 +463,7 @@ struct Builder {
     if (M != cell_M[oc] || N != cell_N[oc] || K1 != cell_M[xc] || K2 != cell_N[xc])
       throw PlanError(TJ_ERR_ARG, "operator sub-block does not match the basis dimensions");
     Operand a = A.mat(ka, at);
-    char key[64];
-    std::snprintf(key, sizeof key, "%lld:%d:%d", (long long)a.off, (int)a.trans, xc);
+    const ProdKey key{a.off, xc, (int32_t)a.trans};
     int pid;
     auto it = dedup ? prod_id.find(key) : prod_id.end();
     if (it != prod_id.end()) {
@@ -450,7 +489,7 @@ struct Builder {
       t.coef = 1.0;
       t.K = K1;
       t.pad = 0;
-      touch(t.L);
+      touch(A, ka);
       plan.tasks1.push_back(t);
       plan.flops += 2.0 * M * K2 * (double)K1;
     }
@@ -464,8 +503,8 @@ struct Builder {
     t.coef = coef;
     t.K = K2;
     t.pad = 0;
-    touch(t.R);
-    cell_tasks[oc].push_back(t);
+    touch(B, kb);
+    add_task(oc, t);
     plan.flops += 2.0 * M * N * (double)K2;
     plan.flops_ref += 2.0 * M * K2 * (double)K1 + 2.0 * M * N * (double)K2;
   }
@@ -515,23 +554,39 @@ struct Builder {
       }
     }
   }
+  // sectors of a basis with the labels (new_num_up, new_num_down), in index
+  // order; built on first use
+  struct SecIndex {
+    std::unordered_map<uint64_t, std::vector<int>> by_lab;
+    bool ready = false;
+  };
+  mutable SecIndex sys_idx, env_idx;
+  static const std::vector<int> *sectors_with(const tj_basis *b, SecIndex &ix, int nu, int nd) {
+    auto key = [](int u, int d) { return (uint64_t)(uint32_t)u << 32 | (uint32_t)d; };
+    if (!ix.ready) {
+      for (int k = 0; k < b->num; ++k) ix.by_lab[key(b->sub[k].new_num_up, b->sub[k].new_num_down)].push_back(k);
+      ix.ready = true;
+    }
+    auto it = ix.by_lab.find(key(nu, nd));
+    return it == ix.by_lab.end() ? nullptr : &it->second;
+  }
   // locate the system sub-block of the sector with labels (nu, nd) satisfying pred
   template <class P>
   bool find_sys(int nu, int nd, P pred, int &xk, int &l) const {
-    for (int k = 0; k < sbs->num; ++k) {
-      if (sbs->sub[k].new_num_up != nu || sbs->sub[k].new_num_down != nd) continue;
+    const std::vector<int> *ks = sectors_with(sbs, sys_idx, nu, nd);
+    if (!ks) return false;
+    for (int k : *ks)
       for (int q = 0; q < sbs->sub[k].num; ++q)
         if (pred(SM(k, q))) { xk = k; l = q; return true; }
-    }
     return false;
   }
   template <class P>
   bool find_env(int nu, int nd, P pred, int &yk, int &l) const {
-    for (int k = 0; k < ebs->num; ++k) {
-      if (ebs->sub[k].new_num_up != nu || ebs->sub[k].new_num_down != nd) continue;
+    const std::vector<int> *ks = sectors_with(ebs, env_idx, nu, nd);
+    if (!ks) return false;
+    for (int k : *ks)
       for (int q = 0; q < ebs->sub[k].num; ++q)
         if (pred(EM(k, q))) { yk = k; l = q; return true; }
-    }
     return false;
   }
   // sub-block index l of map x, as a cell row/column index of sector ko
@@ -849,51 +904,89 @@ struct Builder {
   void block_vec_block_ndia(const OView &sbl, const OView &ebl, char fel, double coef) {
     const int up = sbl.up_dif(), d1 = sbl.down_dif();
     if (up != ebl.up_dif() || d1 != ebl.down_dif()) throw PlanError(TJ_ERR_QN, "Quantum number error in block_vec_block");
+    // The operator sub-block, the target basis sub-block and the 6j symbol of
+    // each side depend on one side's sub-block, its spin step dd and the new
+    // sector spin nsd only, so they are tabulated once per sector; the loops
+    // below visit (m, n, dd, edd, nsd) in the order of the Fortran loops and
+    // do the same floating-point operations.
+    const int nq = d1 + 1;  // dd = -d1, -d1 + 2, ..., d1
+    struct Half { int k, blk, l, hs; double w; };
+    std::vector<Half> st, et;
     for (int i = 0; i < wave->num; ++i) {
       const tj_wave_sub &w = wave->sub[i];
       const int su = w.sys_num_up, sd = w.sys_num_down, eu = w.env_num_up, ed = w.env_num_down;
-      const int x = sec_x[i], y = sec_y[i];
-      for (int m = 0; m < sbs->sub[x].num; ++m)
-        for (int n = 0; n < ebs->sub[y].num; ++n) {
-          const tj_basis_sub &ms = SM(x, m), &me = EM(y, n);
-          for (int dd = -d1; dd <= d1; dd += 2) {
-            const int ks = sbl.find(ms.bl_num_up, ms.bl_num_down, dd, true);
-            const int nsb_up = ms.bl_num_up + up, nsb_dn = ms.bl_num_down + dd;
-            for (int edd = -d1; edd <= d1; edd += 2) {
-              const int neb_up = me.bl_num_up - up, neb_dn = me.bl_num_down - edd;
-              const int ke = ebl.find(neb_up, neb_dn, edd, true);
-              if (ks < 0 || ke < 0) continue;
-              for (int nsd = std::abs(sd - d1); nsd <= sd + d1; nsd += 2) {
-                const int nsu = su + up, neu = eu - up, ned = nsd;
-                int xk, ls, yk, le;
-                if (!find_sys(nsu, nsd, [&](const tj_basis_sub &q) {
-                      return q.bl_num_up == nsb_up && q.bl_num_down == nsb_dn && q.st_num_down == ms.st_num_down &&
-                             q.st_num_up == ms.st_num_up; }, xk, ls))
-                  continue;
-                if (!find_env(neu, ned, [&](const tj_basis_sub &q) {
-                      return q.bl_num_up == neb_up && q.bl_num_down == neb_dn && q.st_num_down == me.st_num_down &&
-                             q.st_num_up == me.st_num_up; }, yk, le))
-                  continue;
-                const int ko = find_sec(nsu, nsd, neu, ned);
-                if (ko < 0) continue;
-                const int j1 = nsd, j2 = d1, j3 = sd, j4 = ms.bl_num_down, j5 = ms.st_num_down, j6 = nsb_dn;
-                const int j11 = ned, j22 = d1, j33 = ed, j44 = me.bl_num_down, j55 = me.st_num_down, j66 = neb_dn;
-                double c1 = w6j(j1, j2, j3, j4, j5, j6);
+      const int x = sec_x[i], y = sec_y[i], nm = sbs->sub[x].num, nn = ebs->sub[y].num;
+      const int nsd0 = std::abs(sd - d1), nt = (sd + d1 - nsd0) / 2 + 1;
+      const int nsu = su + up, neu = eu - up;
+      int ko[8];
+      if (nt > 8) throw PlanError(TJ_ERR_QN, "operator spin step too large in block_vec_block");
+      for (int t = 0; t < nt; ++t) ko[t] = find_sec(nsu, nsd0 + 2 * t, neu, nsd0 + 2 * t);
+      st.assign((size_t)nm * nq * nt, Half{-1, -1, -1, 0, 0.0});
+      et.assign((size_t)nn * nq * nt, Half{-1, -1, -1, 0, 0.0});
+      for (int m = 0; m < nm; ++m) {
+        const tj_basis_sub &ms = SM(x, m);
+        for (int q = 0; q < nq; ++q) {
+          const int dd = -d1 + 2 * q;
+          const int ks = sbl.find(ms.bl_num_up, ms.bl_num_down, dd, true);
+          const int nsb_up = ms.bl_num_up + up, nsb_dn = ms.bl_num_down + dd;
+          for (int t = 0; t < nt; ++t) {
+            Half &h = st[((size_t)m * nq + q) * nt + t];
+            h.k = ks;
+            if (ks < 0) continue;
+            const int nsd = nsd0 + 2 * t;
+            if (!find_sys(nsu, nsd, [&](const tj_basis_sub &b) {
+                  return b.bl_num_up == nsb_up && b.bl_num_down == nsb_dn && b.st_num_down == ms.st_num_down &&
+                         b.st_num_up == ms.st_num_up; }, h.blk, h.l))
+              continue;
+            h.w = w6j(nsd, d1, sd, ms.bl_num_down, ms.st_num_down, nsb_dn);
+            h.hs = (nsb_dn + ms.st_num_down + sd + d1) / 2;
+          }
+        }
+      }
+      for (int n = 0; n < nn; ++n) {
+        const tj_basis_sub &me = EM(y, n);
+        for (int q = 0; q < nq; ++q) {
+          const int edd = -d1 + 2 * q;
+          const int neb_up = me.bl_num_up - up, neb_dn = me.bl_num_down - edd;
+          const int ke = ebl.find(neb_up, neb_dn, edd, true);
+          for (int t = 0; t < nt; ++t) {
+            Half &h = et[((size_t)n * nq + q) * nt + t];
+            h.k = ke;
+            if (ke < 0) continue;
+            const int ned = nsd0 + 2 * t;
+            if (!find_env(neu, ned, [&](const tj_basis_sub &b) {
+                  return b.bl_num_up == neb_up && b.bl_num_down == neb_dn && b.st_num_down == me.st_num_down &&
+                         b.st_num_up == me.st_num_up; }, h.blk, h.l))
+              continue;
+            h.w = w6j(ned, d1, ed, me.bl_num_down, me.st_num_down, neb_dn);
+            h.hs = (neb_dn + me.st_num_down + ed + d1) / 2;
+          }
+        }
+      }
+      for (int m = 0; m < nm; ++m)
+        for (int n = 0; n < nn; ++n) {
+          const tj_basis_sub &me = EM(y, n);
+          const int xc = cell(i, m, n);
+          const double sg = sgn(fel, sd + me.st_num_down);
+          for (int q = 0; q < nq; ++q)
+            for (int eq = 0; eq < nq; ++eq)
+              for (int t = 0; t < nt; ++t) {
+                const Half &hs = st[((size_t)m * nq + q) * nt + t], &he = et[((size_t)n * nq + eq) * nt + t];
+                if (hs.k < 0 || he.k < 0 || hs.blk < 0 || he.blk < 0 || ko[t] < 0) continue;
+                double c1 = hs.w;
                 if (c1 == 0.0) continue;
-                const double c11 = w6j(j11, j22, j33, j44, j55, j66);
+                const double c11 = he.w;
                 if (c11 == 0.0) continue;
                 c1 *= c11;
                 if (c1 == 0.0) continue;
-                c1 *= std::sqrt((1.0 + j11) * (1.0 + j33) / (1.0 + d1));
-                if (((j6 + j5 + j3 + j2) / 2 + (j66 + j55 + j33 + j22) / 2) % 2 == 1) c1 = -c1;
-                const double ct = sgn(fel, sd + me.st_num_down) * coef * c1;
-                const int oc = cell(ko, sys_index_in(ko, xk, ls), env_index_in(ko, yk, le));
-                const int xc = cell(i, m, n);
-                emit2(oc, sbl, ks, false, xc, ebl, ke, false, ct);
-                if (d1 == 1) emit2(xc, sbl, ks, true, oc, ebl, ke, true, ct);
+                const int nsd = nsd0 + 2 * t;
+                c1 *= std::sqrt((1.0 + nsd) * (1.0 + ed) / (1.0 + d1));
+                if ((hs.hs + he.hs) % 2 == 1) c1 = -c1;
+                const double ct = sg * coef * c1;
+                const int oc = cell(ko[t], sys_index_in(ko[t], hs.blk, hs.l), env_index_in(ko[t], he.blk, he.l));
+                emit2(oc, sbl, hs.k, false, xc, ebl, he.k, false, ct);
+                if (d1 == 1) emit2(xc, sbl, hs.k, true, oc, ebl, he.k, true, ct);
               }
-            }
-          }
         }
     }
   }
@@ -918,11 +1011,17 @@ struct Builder {
 
   // -------------------------------------------------------------- finalise
   void finalize() {
-    // phase-2 cells: every cell of the output vector
+    // phase-2 cells: every cell of the output vector, its GEMM tasks first and
+    // its axpy tasks last (the kernel applies axpys in its epilogue), each
+    // group in emission order
+    std::vector<int32_t> pg(ncells, 0), pa(ncells, 0);
+    for (size_t j = 0; j < out_tasks.size(); ++j) ++(out_tasks[j].R.space != SP_NONE ? pg : pa)[out_cell[j]];
     plan.cells2.clear();
     plan.tasks2.clear();
+    int32_t pos = 0;
     for (int c = 0; c < ncells; ++c) {
-      if (cor_mode && cell_tasks[c].empty()) continue;
+      const int32_t ng = pg[c], na = pa[c];
+      if (cor_mode && ng + na == 0) continue;
       Cell cl;
       std::memset(&cl, 0, sizeof cl);
       cl.off = cell_off[c];
@@ -930,16 +1029,19 @@ struct Builder {
       cl.M = cell_M[c];
       cl.N = cell_N[c];
       cl.space = SP_PSI;
-      cl.t_begin = (int)plan.tasks2.size();
-      // GEMM tasks first, axpy tasks last (the kernel applies axpys in its epilogue)
-      for (const Task &t : cell_tasks[c])
-        if (t.R.space != SP_NONE) plan.tasks2.push_back(t);
-      for (const Task &t : cell_tasks[c])
-        if (t.R.space == SP_NONE) plan.tasks2.push_back(t);
-      cl.t_end = (int)plan.tasks2.size();
+      cl.t_begin = pos;
+      pg[c] = pos;
+      pa[c] = pos + ng;
+      pos += ng + na;
+      cl.t_end = pos;
       plan.cells2.push_back(cl);
       plan.cell2_row_state.push_back(cell_rs[c]);
       plan.cell2_col_state.push_back(cell_cs[c]);
+    }
+    plan.tasks2.resize(pos);
+    for (size_t j = 0; j < out_tasks.size(); ++j) {
+      const Task &t = out_tasks[j];
+      plan.tasks2[t.R.space != SP_NONE ? pg[out_cell[j]]++ : pa[out_cell[j]]++] = t;
     }
     auto make_tiles = [&](const std::vector<Cell> &cells, const std::vector<Task> &tasks,
                           std::vector<Tile> &tiles, std::vector<Reduce> &red, int64_t &nslots) {
@@ -947,8 +1049,6 @@ struct Builder {
     };
     make_tiles(plan.cells1, plan.tasks1, plan.tiles1, plan.red1, plan.nslots1);
     make_tiles(plan.cells2, plan.tasks2, plan.tiles2, plan.red2, plan.nslots2);
-    std::sort(op_touched.begin(), op_touched.end());
-    op_touched.erase(std::unique(op_touched.begin(), op_touched.end()), op_touched.end());
   }
 };
 
@@ -1265,10 +1365,15 @@ int build_hpsi_plan(const tj_lattice *lat, const tj_model *sysm, const tj_model 
     B.finalize();
     // algorithmic bytes: every operator sub-block touched once, psi read, output read-modify-write
     double opb = 0;
-    {
-      std::unordered_map<int64_t, int64_t> sz;
-      for (const auto &e : plan.sub_extent) sz[e.first] = e.second;
-      for (int64_t off : B.op_touched) opb += (double)sz[off];
+    auto add_touched = [&](const OBlk &b) {
+      for (const OSub &s : b.sub)
+        if (s.touched) opb += (double)s.row_dim * s.sdim;
+    };
+    for (const Model *m : {&sys, &env}) {
+      add_touched(m->ham);
+      for (const auto &a : m->sub) for (const OBlk &b : a) add_touched(b);
+      for (const auto &a : m->snc) for (const OBlk &b : a) add_touched(b);
+      for (const auto &a : m->sub_s) for (const OBlk &b : a) add_touched(b);
     }
     plan.bytes = 8.0 * (opb + 3.0 * (double)wave->dim);
     return TJ_OK;
