@@ -11,7 +11,9 @@
 //                   splits; launch 2 (two-sided families)
 #include <algorithm>
 #include <cstring>
+#include <functional>
 #include <map>
+#include <queue>
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
@@ -367,6 +369,7 @@ struct Builder {
 
   void cells() {
     const int64_t npsi = (int64_t)hp.cells2.size();
+    std::vector<int> left, right, two;
     for (int64_t ci = 0; ci < npsi; ++ci) {
       const Cell &c = hp.cells2[ci];
       OzCell oc;
@@ -376,7 +379,9 @@ struct Builder {
       oc.M = c.M;
       oc.N = c.N;
       oc.a_begin = oc.a_end = c.t_end;
-      std::vector<int> left, right, two;
+      left.clear();
+      right.clear();
+      two.clear();
       for (int ti = c.t_begin; ti < c.t_end; ++ti) {
         const Task &t = hp.tasks2[ti];
         if (t.R.space == SP_NONE) {
@@ -444,13 +449,16 @@ struct Builder {
     // maximum jobs and split jobs in lists of their own, so that no kernel
     // walks over jobs it has nothing to do for
     auto part = [](std::vector<OzJob> &all, std::vector<OzJob> &mx) {
+      size_t nm = 0;
+      for (const OzJob &j : all) nm += j.want_max ? 1 : 0;
       mx.clear();
-      std::vector<OzJob> sp;
-      for (const OzJob &j : all) {
-        if (j.want_max) mx.push_back(j);
-        if (j.want_split) sp.push_back(j);
+      mx.reserve(nm);
+      size_t w = 0;
+      for (size_t i = 0; i < all.size(); ++i) {
+        if (all[i].want_max) mx.push_back(all[i]);
+        if (all[i].want_split) all[w++] = all[i];
       }
-      all.swap(sp);
+      all.resize(w);
     };
     part(oz.sta_jobs, oz.sta_mjobs);
     part(dyn_psi, oz.psi_mjobs);
@@ -505,6 +513,7 @@ struct Builder {
     spans.clear();
     std::vector<int64_t> st(jobs.size() + 1, 0);
     for (size_t j = 0; j < jobs.size(); ++j) st[j + 1] = st[j] + job_units(jobs[j], max_units);
+    spans.reserve((size_t)((st.back() + OZ_SPLIT_THREADS - 1) / OZ_SPLIT_THREADS));
     size_t j = 0;
     for (int64_t g = 0; g < st.back(); g += OZ_SPLIT_THREADS) {
       while (st[j + 1] <= g) ++j;
@@ -527,21 +536,31 @@ struct Builder {
     const int nb = std::min(oz.nsm, n);
     const int64_t fixed = sched_item_cost;
     auto est = [fixed](const OzItem &it) { return (int64_t)it.nkb + fixed; };
-    std::stable_sort(v.begin(), v.end(), [&](const OzItem &a, const OzItem &b) { return est(a) > est(b); });
-    std::vector<int64_t> load(nb, 0);
-    std::vector<std::vector<int>> bins(nb);
-    for (int i = 0; i < n; ++i) {
-      int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-      load[b] += est(v[i]);
-      bins[b].push_back(i);
-    }
-    std::vector<OzItem> out;
-    out.reserve(n);
+    // items by decreasing estimate, ties in list order (a stable counting sort)
+    int64_t emax = 0;
+    for (const OzItem &it : v) emax = std::max(emax, est(it));
+    std::vector<int32_t> start((size_t)emax + 2, 0), order(n);
+    for (const OzItem &it : v) ++start[(size_t)(emax - est(it)) + 1];
+    for (size_t e = 0; e + 1 < start.size(); ++e) start[e + 1] += start[e];
+    for (int i = 0; i < n; ++i) order[start[(size_t)(emax - est(v[i]))]++] = i;
+    // each to the least loaded CTA, the lowest-numbered among equals
+    using Load = std::pair<int64_t, int32_t>;
+    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+    for (int b = 0; b < nb; ++b) heap.push({0, b});
+    std::vector<int32_t> bin(n);
     cta.assign(nb + 1, 0);
-    for (int b = 0; b < nb; ++b) {
-      for (int i : bins[b]) out.push_back(v[i]);
-      cta[b + 1] = (int32_t)out.size();
+    for (int i = 0; i < n; ++i) {
+      Load l = heap.top();
+      heap.pop();
+      bin[i] = l.second;
+      ++cta[l.second + 1];
+      l.first += est(v[order[i]]);
+      heap.push(l);
     }
+    for (int b = 0; b < nb; ++b) cta[b + 1] += cta[b];
+    std::vector<int32_t> fill(cta.begin(), cta.end() - 1);
+    std::vector<OzItem> out(n);
+    for (int i = 0; i < n; ++i) out[fill[bin[i]]++] = v[order[i]];
     v.swap(out);
   }
 
@@ -554,6 +573,23 @@ struct Builder {
     colsplit.assign(npsi, -1);
     rowsplit.assign(npsi, -1);
     prodsplit.assign(hp.cells1.size(), -1);
+    // capacities: one static job and one segment per product and per phase-2
+    // GEMM task, up to three families and one work-item row per tile
+    const size_t n1 = hp.cells1.size(), n2 = (size_t)npsi, nt = hp.tasks2.size();
+    size_t ntiles = 0;
+    for (const Cell &c : hp.cells1) ntiles += (size_t)cdiv(c.M, 128) * cdiv(c.N, oz.bn);
+    for (const Cell &c : hp.cells2) ntiles += (size_t)cdiv(c.M, 128) * cdiv(c.N, oz.bn);
+    oz.sta_jobs.reserve(n1 + nt);
+    oz.segs.reserve(n1 + nt);
+    seg_dyn_a.reserve(nt);
+    seg_dyn_b.reserve(n1 + nt);
+    oz.fams.reserve(n1 + 3 * n2);
+    famrel.reserve(n1 + 3 * n2);
+    oz.cells.reserve(n1 + n2);
+    oz.items1.reserve(ntiles);
+    dyn_psi.reserve(2 * n2);
+    dyn_psi_rel.reserve(2 * n2);
+    dyn_prod.reserve(n1);
     products();
     cells();
     finish();
