@@ -582,13 +582,15 @@ extern "C" int tj_lanczos_memo_new(tj_ctx *ctx, const tj_lattice *lat, const tj_
   const int nblk = dot_blocks(D);
   const int mdb = (int)((D + 256 * 8 - 1) / (256 * 8));
   if ((rc = ctx->lanScal.reserve(sizeof(double) * 1024))) return rc;
-  if ((rc = ctx->lanPart.reserve(sizeof(double) * ((size_t)std::max(nblk, 1) + (size_t)std::max(mdb, 1) * 128 + 256))))
+  const int npart = std::max(nblk, lz_blocks(D));
+  if ((rc = ctx->lanPart.reserve(sizeof(double) * ((size_t)std::max(npart, 1) + (size_t)std::max(mdb, 1) * 128 + 256))))
     return rc;
   double *V = ctx->lanV.d();
   double *S = ctx->lanScal.d();   // [0..127] alpha, [128..255] beta, [256..383] uu, [384..511] coef, [512] lam, [513] nrm, [600..727] dz
   double *alpha = S, *beta = S + 128, *uu = S + 256, *coef = S + 384, *lam = S + 512, *nrm = S + 513, *dz = S + 600;
   int *itd = (int *)(S + 1000);   // the iteration's step L, read by the captured kernels
-  double *part = ctx->lanPart.d(), *mpart = part + nblk;
+  int *cnt = (int *)(S + 1002);   // block counter of the kernels that end in a grid-wide sum
+  double *part = ctx->lanPart.d(), *mpart = part + npart;
   auto vec = [&](int j) { return V + (int64_t)(j - 1) * ld; };   // tempvec(j), 1-based
   double *X = vec(LOOP_IN + 3), *Y = vec(LOOP_IN + 4);         // H*psi input and output of an iteration
   auto norm_into = [&](const double *x, double *res) {
@@ -627,22 +629,16 @@ extern "C" int tj_lanczos_memo_new(tj_ctx *ctx, const tj_lattice *lat, const tj_
   // computed speculatively and dropped, with `last` restored, so the result
   // is the same.
   auto ref = [&](int off) { return LzRef{V, ld, itd, off, nullptr}; };
-  const LzRef yref{nullptr, 0, nullptr, 0, Y};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
-  launch_lz_update(ref(1), Y, ref(0), ref(-1), S, itd, D, st);                  // vec(L+1) = H vec(L) - ...
-  launch_lz_norm(ref(1), D, part, nblk, S, itd, 128, 1, st);                    // beta(L)
-  launch_lz_scale(ref(1), S, itd, 128, nullptr, D, st);
-  launch_lz_gram_schmidt(V, ld, itd, ref(1), D, mpart, mdb, 128, uu + 1, coef, st);
-  launch_lz_norm(ref(1), D, part, nblk, S, nullptr, 513, 1, st);
-  launch_lz_scale(ref(1), S, nullptr, 513, X, D, st);                           // and X = vec(L+1)
-  launch_lz_norm(ref(1), D, part, nblk, S, itd, 257, 0, st);                    // uu(L+1)
+  launch_lz_update_norm(ref(1), Y, ref(0), ref(-1), S, itd, D, part, cnt, st);   // vec(L+1), beta(L)
+  launch_lz_gram_schmidt(V, ld, itd, ref(1), D, S, mpart, mdb, 128, uu + 1, coef, part, cnt, st);
+  launch_lz_scale_norm(ref(1), X, D, S, itd, part, cnt, st);                    // X = vec(L+1), uu(L+1)
   rc = run_hpsi(ctx, X, Y, false);
   if (!rc) {
-    launch_lz_dot(ref(1), yref, D, part, nblk, S, itd, 1, st);                  // alpha(L+1)
-    launch_lz_tridiag(alpha + 1, beta + 1, itd, 1, lam, st);
-    launch_lz_publish(S, itd, ctx->pinned, st);
+    launch_lz_dot(ref(1), Y, D, S, itd, part, cnt, st);                         // alpha(L+1)
+    launch_lz_tridiag_publish(S, itd, ctx->pinned, st);
   }
   const cudaError_t ce = cudaStreamEndCapture(st, &graph);
   --ctx->n_hpsi;   // the captured H*psi ran nothing

@@ -349,61 +349,139 @@ void launch_combine(const double *V, int64_t ld, int k, const double *coef, doub
   combine_kernel<<<vgrid(n), VT, 0, s>>>(V, ld, k, coef, w, n, assign);
 }
 
-// Number of eigenvalues of the tridiagonal (a, b) below x (Sturm count).
-__device__ __forceinline__ int sturm_count(const double *a, const double *b, int n, double x) {
+// Number of eigenvalues of the tridiagonal (a, b2 = b*b) below x (Sturm count).
+__device__ __forceinline__ int sturm_count(const double *a, const double *b2, int n, double x) {
   const double tiny = 1e-300;
   int cnt = 0;
   double q = a[0] - x;
   if (q < 0) ++cnt;
   for (int i = 1; i < n; ++i) {
     if (fabs(q) < tiny) q = -tiny;
-    q = (a[i] - x) - b[i - 1] * b[i - 1] / q;
+    q = (a[i] - x) - b2[i - 1] / q;
     if (q < 0) ++cnt;
   }
   return cnt;
 }
 
+// Ordered integer image of a double: monotone in the value, with +0 and -0
+// both at 0, so that consecutive integers are adjacent doubles.
+__device__ __forceinline__ int64_t ord_of(double x) {
+  const int64_t bits = __double_as_longlong(x);
+  return bits >= 0 ? bits : -(bits & 0x7fffffffffffffffLL);
+}
+__device__ __forceinline__ double val_of(int64_t k) {
+  return k >= 0 ? __longlong_as_double(k) : __longlong_as_double((-k) | (int64_t)0x8000000000000000ULL);
+}
+
+constexpr int TRI_THREADS = 256;   // threads (multisection points) of the tridiagonal eigenvalue kernels
+
 // Lowest eigenpair of a symmetric tridiagonal matrix (n <= 128): the lowest
 // eigenvalue to full precision -- the pair of adjacent doubles where the
-// Sturm count turns from 0 to 1 -- by 32-point multisection (one warp, one
-// point per lane: five bits per pass) finished by bisection, then inverse
-// iteration with a pivoted tridiagonal solve on one thread.  n is at most the
-// Lanczos depth.
-__device__ void tridiag_min_body(const double *a, const double *b, int n, double *lam, double *vec, int want_vec) {
-  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
-  const int lane = threadIdx.x;
-  double lo = 0.0, hi = 0.0;
-  for (int i = 0; i < n; ++i) {
+// Sturm count turns from 0 to 1 -- by multisection over the ordered integer
+// images of the doubles (TRI_THREADS points per pass, one per thread, about
+// eight bits per pass; the last pass places its points on consecutive
+// doubles), then inverse iteration with a pivoted tridiagonal solve on one
+// thread.  n is at most the Lanczos depth.  Runs on one block of TRI_THREADS
+// threads; every thread returns the same bracket [lo, hi] of adjacent doubles.
+// hint (if finite): an upper estimate of the eigenvalue, such as the lowest
+// eigenvalue of the leading (n-1) x (n-1) matrix, which is never below it
+// (Cauchy interlacing).  The first pass then places its points at
+// geometrically growing distances below the hint (and one just above it), so
+// that the bracket it leaves is a fraction of the eigenvalue's distance from
+// the hint wide; the bracket at the end is the same either way.
+__device__ void tridiag_min_bracket(const double *a, const double *b, int n, double hint, double &lo_out,
+                                    double &hi_out) {
+  __shared__ double sa[128], sb2[128], slo[TRI_THREADS / 32], shi[TRI_THREADS / 32];
+  __shared__ unsigned sv[TRI_THREADS / 32], su[TRI_THREADS / 32];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  // the matrix to shared memory, and its Gershgorin bounds (a block-wide min
+  // and max of a[i] -+ (|b[i-1]| + |b[i]|), exact in any order)
+  double lo = INFINITY, hi = -INFINITY;
+  for (int i = t; i < n; i += blockDim.x) {
+    sa[i] = a[i];
+    sb2[i] = i < n - 1 ? b[i] * b[i] : 0.0;
     const double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i < n - 1 ? fabs(b[i]) : 0.0);
-    const double l = a[i] - r, h = a[i] + r;
-    if (i == 0 || l < lo) lo = l;
-    if (i == 0 || h > hi) hi = h;
+    lo = fmin(lo, a[i] - r);
+    hi = fmax(hi, a[i] + r);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if (lane == 0) {
+    slo[w] = lo;
+    shi[w] = hi;
+  }
+  __syncthreads();
+  lo = slo[0];
+  hi = shi[0];
+  for (int q = 1; q < TRI_THREADS / 32; ++q) {
+    lo = fmin(lo, slo[q]);
+    hi = fmax(hi, shi[q]);
   }
   // invariant: count(lo) = 0 < count(hi) (Gershgorin bounds)
-  for (int pass = 0; pass < 64; ++pass) {
-    const double x = lo + (hi - lo) * ((double)(lane + 1) / 33.0);
-    const bool valid = x > lo && x < hi;
-    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-    if (vmask == 0) break;
-    const int cnt = valid ? sturm_count(a, b, n, x) : 0;
-    const unsigned up = __ballot_sync(0xffffffffu, valid && cnt >= 1);
-    if (up == 0) {
-      lo = __shfl_sync(0xffffffffu, x, 31 - __clz(vmask));   // the highest valid point
-    } else {
-      const int f = __ffs(up) - 1;
-      const double xf = __shfl_sync(0xffffffffu, x, f);
-      const double xp = __shfl_sync(0xffffffffu, x, f > 0 ? f - 1 : 0);
-      if (f > 0 && ((vmask >> (f - 1)) & 1u)) lo = xp;
-      hi = xf;
+  // images lie in (-2^63, 2^63), so their distance can exceed the int64
+  // range: spans and offsets are taken modulo 2^64, where they are exact
+  int64_t klo = ord_of(lo), khi = ord_of(hi);
+  auto dist = [](int64_t kl, int64_t kh) -> uint64_t { return (uint64_t)kh - (uint64_t)kl; };
+  auto point = [&](int j, int64_t kl, int64_t kh) -> int64_t {
+    const uint64_t span = dist(kl, kh);
+    if (span <= (uint64_t)TRI_THREADS + 1) return (int64_t)((uint64_t)kl + (uint64_t)(j + 1));
+    return (int64_t)((uint64_t)kl +
+                     (uint64_t)((double)span * ((double)(j + 1) / (double)(TRI_THREADS + 1))));
+  };
+  // first-pass points from the hint: point j = khint + 1 - (g - 1) with
+  // g = below^((T-1-j)/(T-1)), below = khint + 1 - klo; non-decreasing in j,
+  // the last one just above the hint
+  const bool use_hint = isfinite(hint) && hint > lo && hint < hi;
+  const int64_t khint = use_hint ? ord_of(hint) : 0;
+  auto hint_point = [&](int j, int64_t kl) -> int64_t {
+    const double below = (double)(dist(kl, khint) + 1);
+    const double g = exp2((double)(TRI_THREADS - 1 - j) * log2(below) / (double)(TRI_THREADS - 1));
+    const uint64_t off = g >= below ? dist(kl, khint) + 1 : (uint64_t)g;   // 1 .. below
+    return (int64_t)((uint64_t)khint + 1 - (off - 1));
+  };
+  for (int pass = 0; pass < 64 && khi > klo && dist(klo, khi) > 1; ++pass) {
+    const bool geo = use_hint && pass == 0;
+    auto pt = [&](int j) { return geo ? hint_point(j, klo) : point(j, klo, khi); };
+    const int64_t kx = pt(t);
+    const bool valid = kx > klo && kx < khi;
+    const bool up = valid && sturm_count(sa, sb2, n, val_of(kx)) >= 1;
+    const unsigned vm = __ballot_sync(0xffffffffu, valid), um = __ballot_sync(0xffffffffu, up);
+    if (lane == 0) {
+      sv[w] = vm;
+      su[w] = um;
     }
+    __syncthreads();
+    // f: the first point with a count of at least one; the new lo is the
+    // highest valid point below it (all of them have a count of zero)
+    int f = -1, g = -1;
+    for (int q = 0; q < TRI_THREADS / 32 && f < 0; ++q)
+      if (su[q]) f = q * 32 + __ffs(su[q]) - 1;
+    const int lim = f < 0 ? TRI_THREADS : f;
+    for (int q = (lim - 1) >> 5; q >= 0 && g < 0 && lim > 0; --q) {
+      unsigned m = sv[q];
+      const int top = lim - q * 32;
+      if (top < 32) m &= (1u << top) - 1u;
+      if (m) g = q * 32 + 31 - __clz(m);
+    }
+    const int64_t nlo = g >= 0 ? pt(g) : klo, nhi = f >= 0 ? pt(f) : khi;
+    __syncthreads();
+    if (nlo == klo && nhi == khi) break;   // no valid point: lo and hi are adjacent
+    klo = nlo;
+    khi = nhi;
   }
-  for (int it = 0; it < 200; ++it) {
-    const double mid = 0.5 * (lo + hi);
-    if (mid <= lo || mid >= hi) break;
-    if (sturm_count(a, b, n, mid) >= 1) hi = mid; else lo = mid;
-  }
+  lo_out = val_of(klo);
+  hi_out = val_of(khi);
+}
+
+__device__ void tridiag_min_body(const double *a, const double *b, int n, double *lam, double *vec, int want_vec) {
+  if (blockIdx.x != 0) return;
+  double lo, hi;
+  tridiag_min_bracket(a, b, n, __longlong_as_double(0x7FF8000000000000LL), lo, hi);
   const double l = 0.5 * (lo + hi);
-  if (lane != 0) return;
+  if (threadIdx.x != 0) return;
   *lam = l;
   if (!want_vec) return;
   // inverse iteration on (T - l I) with partial pivoting
@@ -470,69 +548,88 @@ __global__ void tridiag_min_kernel(const double *a, const double *b, int n, doub
 }
 void launch_tridiag_min(const double *a, const double *b, int n, double *lam, double *vec, int want_vec,
                         cudaStream_t s) {
-  tridiag_min_kernel<<<1, 32, 0, s>>>(a, b, n, lam, vec, want_vec);
+  tridiag_min_kernel<<<1, TRI_THREADS, 0, s>>>(a, b, n, lam, vec, want_vec);
 }
 
 // ---- one Lanczos iteration with its step read from device memory (*it), so
 // that the same launches -- captured once as a CUDA graph -- serve every
 // iteration.  S holds alpha (0..127), beta (128..255), uu (256..383), the
 // Gram-Schmidt coefficients (384..511), the Ritz value (512) and a norm (513).
+// Each norm or dot product is folded into the kernel that produces its
+// vector (one pass over the vector instead of two, one launch instead of
+// three): every block reduces its share of the squares or products, and the
+// last block to finish adds the block partials in a fixed order, so the
+// result does not depend on the order the blocks run in.
 __device__ __forceinline__ double *lz_ptr(const LzRef &r) {
   return r.fixed ? r.fixed : r.V + (int64_t)(*r.it + r.off - 1) * r.ld;
 }
 
-__global__ void lz_update_kernel(LzRef dst, const double *__restrict__ src, LzRef x1, LzRef x2, const double *S,
-                                 const int *it, int64_t n) {
+// The block partial s (valid in thread 0) to partials[blockIdx.x]; the last
+// block to arrive (counted on *cnt, which it resets for the next kernel) adds
+// the partials, thread i taking i, i + blockDim.x, ..., then the block tree,
+// and stores the total (or its square root) at *res.
+__device__ void lz_grid_sum(double s, double *partials, int *cnt, double *res, int sqrt_flag, double *sh) {
+  __shared__ int last;
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = s;
+    __threadfence();
+    last = atomicAdd(cnt, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double t = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) t += __ldcg(partials + i);
+  t = block_sum(t, sh);
+  if (threadIdx.x == 0) {
+    *res = sqrt_flag ? sqrt(t) : t;
+    *cnt = 0;
+  }
+}
+
+// vec(L+1) = H vec(L) - alpha(L) vec(L) - beta(L-1) vec(L-1); beta(L) = |vec(L+1)|
+__global__ void lz_update_norm_kernel(LzRef dst, const double *__restrict__ src, LzRef x1, LzRef x2, double *S,
+                                      const int *it, int64_t n, double *partials, int *cnt) {
+  __shared__ double sh[VT / 32];
   const int L = *it;
   const double av = S[L], bv = L >= 2 ? S[128 + L - 1] : 0.0;
-  double *y = lz_ptr(dst);
-  const double *p1 = lz_ptr(x1), *p2 = L >= 2 ? lz_ptr(x2) : nullptr;
+  double *__restrict__ y = lz_ptr(dst);
+  const double *__restrict__ p1 = lz_ptr(x1);
+  const double *__restrict__ p2 = L >= 2 ? lz_ptr(x2) : nullptr;
+  double s = 0.0;
+#pragma unroll 4
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double v = src[i] - av * p1[i];
     if (p2) v = v - bv * p2[i];
     y[i] = v;
+    s += v * v;
   }
-}
-
-__global__ void lz_dot_kernel(LzRef x, LzRef y, int64_t n, double *partials) {
-  __shared__ double sh[VT / 32];
-  const double *__restrict__ px = lz_ptr(x), *__restrict__ py = lz_ptr(y);
-  double s = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    s += px[i] * py[i];
   s = block_sum(s, sh);
-  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  lz_grid_sum(s, partials, cnt, S + 128 + L, 1, sh);
 }
 
-__global__ void lz_sum_kernel(const double *partials, int nblk, double *S, const int *it, int idx, int sqrt_flag) {
+// Projections of w / beta(L) on vec(1..L), with w scaled in place: each block
+// keeps its slice of w in registers and streams the L vectors past it (the
+// kernel is bound by those reads: L vectors of n doubles).  Five resident
+// blocks per SM put the grid (one block per VT * MD_PER elements: 685 for
+// 1.4M) in one wave on 148 SMs.
+__global__ void __launch_bounds__(VT, 5) lz_multi_dot_kernel(const double *__restrict__ V, int64_t ld, const int *it, LzRef wr_, int64_t n,
+                                    const double *S, double *partials, int kmax) {
   __shared__ double sh[VT / 32];
-  double s = 0.0;
-  for (int i = threadIdx.x; i < nblk; i += blockDim.x) s += partials[i];
-  s = block_sum(s, sh);
-  if (threadIdx.x == 0) S[idx + (it ? *it : 0)] = sqrt_flag ? sqrt(s) : s;
-}
-
-__global__ void lz_scale_kernel(LzRef x, const double *S, const int *it, int idx, double *copy, int64_t n) {
-  const double d = S[idx + (it ? *it : 0)];
-  double *px = lz_ptr(x);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double v = px[i] / d;
-    px[i] = v;
-    if (copy) copy[i] = v;
-  }
-}
-
-__global__ void lz_multi_dot_kernel(const double *__restrict__ V, int64_t ld, const int *it, LzRef wr_, int64_t n,
-                                    double *partials, int kmax) {
-  __shared__ double sh[VT / 32];
-  const int k = *it;
-  const double *__restrict__ w = lz_ptr(wr_);
+  const int L = *it;
+  const int k = min(L, kmax);
+  const double d = S[128 + L];
+  double *__restrict__ w = lz_ptr(wr_);
   const int64_t base = (int64_t)blockIdx.x * VT * MD_PER + threadIdx.x;
   double wr[MD_PER];
 #pragma unroll
   for (int i = 0; i < MD_PER; ++i) {
     const int64_t e = base + (int64_t)i * VT;
-    wr[i] = e < n ? w[e] : 0.0;
+    wr[i] = 0.0;
+    if (e < n) {
+      wr[i] = w[e] / d;
+      w[e] = wr[i];
+    }
   }
   for (int j = 0; j < k; ++j) {
     const double *v = V + (int64_t)j * ld;
@@ -547,6 +644,7 @@ __global__ void lz_multi_dot_kernel(const double *__restrict__ V, int64_t ld, co
   }
 }
 
+// coef(j) = (sum of the block projections) / uu(j), one block per vector
 __global__ void lz_multi_sum_kernel(const double *partials, int nblk, int kmax, const double *uu, double *coef,
                                     const int *it) {
   __shared__ double sh[VT / 32];
@@ -558,62 +656,102 @@ __global__ void lz_multi_sum_kernel(const double *partials, int nblk, int kmax, 
   if (threadIdx.x == 0) coef[j] = s / uu[j];
 }
 
-__global__ void lz_combine_kernel(const double *__restrict__ V, int64_t ld, const int *it,
-                                  const double *__restrict__ coef, LzRef wr_, int64_t n) {
-  __shared__ double c[128];
-  const int k = *it;
-  double *w = lz_ptr(wr_);
-  for (int j = threadIdx.x; j < k && j < 128; j += blockDim.x) c[j] = coef[j];
+// w -= sum_j coef(j) vec(j); S[513] = |w|
+constexpr int LZ_KMAX = 128;
+__global__ void lz_combine_norm_kernel(const double *__restrict__ V, int64_t ld, const int *it,
+                                       const double *__restrict__ coef, LzRef wr_, int64_t n, double *S,
+                                       double *partials, int *cnt) {
+  __shared__ double c[LZ_KMAX];
+  __shared__ double sh[VT / 32];
+  const int k = min(*it, LZ_KMAX);
+  double *__restrict__ w = lz_ptr(wr_);
+  for (int j = threadIdx.x; j < k; j += blockDim.x) c[j] = coef[j];
   __syncthreads();
+  double s = 0.0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double t = 0.0;
     for (int j = 0; j < k; ++j) t = t + c[j] * V[(int64_t)j * ld + i];
-    w[i] = w[i] - t;
+    const double v = w[i] - t;
+    w[i] = v;
+    s += v * v;
   }
+  s = block_sum(s, sh);
+  lz_grid_sum(s, partials, cnt, S + 513, 1, sh);
 }
 
-__global__ void lz_tridiag_kernel(const double *a, const double *b, const int *it, int noff, double *lam) {
-  tridiag_min_body(a, b, *it + noff, lam, nullptr, 0);
-}
-
-// beta(L) and the Ritz value to page-locked host memory; the step advances
-__global__ void lz_publish_kernel(const double *S, int *it, double *host) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// w /= S[513], copied to x; uu(L+1) = w . w
+__global__ void lz_scale_norm_kernel(LzRef wr_, double *__restrict__ x, int64_t n, double *S, const int *it,
+                                     double *partials, int *cnt) {
+  __shared__ double sh[VT / 32];
   const int L = *it;
+  const double d = S[513];
+  double *__restrict__ w = lz_ptr(wr_);
+  double s = 0.0;
+#pragma unroll 4
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double v = w[i] / d;
+    w[i] = v;
+    x[i] = v;
+    s += v * v;
+  }
+  s = block_sum(s, sh);
+  lz_grid_sum(s, partials, cnt, S + 257 + L, 0, sh);
+}
+
+// alpha(L+1) = vec(L+1) . y
+__global__ void lz_dot_kernel(LzRef xr, const double *__restrict__ y, int64_t n, double *S, const int *it,
+                              double *partials, int *cnt) {
+  __shared__ double sh[VT / 32];
+  const int L = *it;
+  const double *__restrict__ x = lz_ptr(xr);
+  double s = 0.0;
+#pragma unroll 4
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    s += x[i] * y[i];
+  s = block_sum(s, sh);
+  lz_grid_sum(s, partials, cnt, S + 1 + L, 0, sh);
+}
+
+// The Ritz value of T(L+1); beta(L) and the Ritz value to page-locked host
+// memory; the step advances.
+__global__ void lz_tridiag_publish_kernel(double *S, int *it, double *host) {
+  const int L = *it;
+  double lo, hi;
+  // from the second step on, S[512] holds the Ritz value of the step before
+  tridiag_min_bracket(S + 1, S + 129, L + 1, L >= 2 ? S[512] : __longlong_as_double(0x7FF8000000000000LL), lo, hi);
+  if (threadIdx.x != 0) return;
+  S[512] = 0.5 * (lo + hi);
   host[0] = S[128 + L];
   host[1] = S[512];
   __threadfence_system();
   *it = L + 1;
 }
 
-void launch_lz_update(LzRef dst, const double *src, LzRef x1, LzRef x2, const double *S, const int *it, int64_t n,
-                      cudaStream_t s) {
-  lz_update_kernel<<<vgrid(n), VT, 0, s>>>(dst, src, x1, x2, S, it, n);
+// the elementwise kernels with a fused norm run on the grid of a dot product
+// (fewer partials for the last block to add); the Gram-Schmidt combination,
+// which streams L vectors per element, on the wider vector grid
+int lz_blocks(int64_t n) { return std::max(vgrid(n), dot_blocks(n)); }
+void launch_lz_update_norm(LzRef dst, const double *src, LzRef x1, LzRef x2, double *S, const int *it, int64_t n,
+                           double *partials, int *cnt, cudaStream_t s) {
+  lz_update_norm_kernel<<<dot_blocks(n), VT, 0, s>>>(dst, src, x1, x2, S, it, n, partials, cnt);
 }
-void launch_lz_norm(LzRef x, int64_t n, double *partials, int nblk, double *S, const int *it, int idx, int sqrt_flag,
-                    cudaStream_t s) {
-  lz_dot_kernel<<<nblk, VT, 0, s>>>(x, x, n, partials);
-  lz_sum_kernel<<<1, VT, 0, s>>>(partials, nblk, S, it, idx, sqrt_flag);
+void launch_lz_gram_schmidt(const double *V, int64_t ld, const int *it, LzRef w, int64_t n, double *S,
+                            double *mpartials, int mdb, int kmax, const double *uu, double *coef, double *partials,
+                            int *cnt, cudaStream_t s) {
+  lz_multi_dot_kernel<<<mdb, VT, 0, s>>>(V, ld, it, w, n, S, mpartials, kmax);
+  lz_multi_sum_kernel<<<kmax, VT, 0, s>>>(mpartials, mdb, kmax, uu, coef, it);
+  lz_combine_norm_kernel<<<vgrid(n), VT, 0, s>>>(V, ld, it, coef, w, n, S, partials, cnt);
 }
-void launch_lz_dot(LzRef x, LzRef y, int64_t n, double *partials, int nblk, double *S, const int *it, int idx,
+void launch_lz_scale_norm(LzRef w, double *x, int64_t n, double *S, const int *it, double *partials, int *cnt,
+                          cudaStream_t s) {
+  lz_scale_norm_kernel<<<dot_blocks(n), VT, 0, s>>>(w, x, n, S, it, partials, cnt);
+}
+void launch_lz_dot(LzRef x, const double *y, int64_t n, double *S, const int *it, double *partials, int *cnt,
                    cudaStream_t s) {
-  lz_dot_kernel<<<nblk, VT, 0, s>>>(x, y, n, partials);
-  lz_sum_kernel<<<1, VT, 0, s>>>(partials, nblk, S, it, idx, 0);
+  lz_dot_kernel<<<dot_blocks(n), VT, 0, s>>>(x, y, n, S, it, partials, cnt);
 }
-void launch_lz_scale(LzRef x, const double *S, const int *it, int idx, double *copy, int64_t n, cudaStream_t s) {
-  lz_scale_kernel<<<vgrid(n), VT, 0, s>>>(x, S, it, idx, copy, n);
-}
-void launch_lz_gram_schmidt(const double *V, int64_t ld, const int *it, LzRef w, int64_t n, double *partials,
-                            int nblk, int kmax, const double *uu, double *coef, cudaStream_t s) {
-  lz_multi_dot_kernel<<<nblk, VT, 0, s>>>(V, ld, it, w, n, partials, kmax);
-  lz_multi_sum_kernel<<<kmax, VT, 0, s>>>(partials, nblk, kmax, uu, coef, it);
-  lz_combine_kernel<<<vgrid(n), VT, 0, s>>>(V, ld, it, coef, w, n);
-}
-void launch_lz_tridiag(const double *a, const double *b, const int *it, int noff, double *lam, cudaStream_t s) {
-  lz_tridiag_kernel<<<1, 32, 0, s>>>(a, b, it, noff, lam);
-}
-void launch_lz_publish(const double *S, int *it, double *host, cudaStream_t s) {
-  lz_publish_kernel<<<1, 32, 0, s>>>(S, it, host);
+void launch_lz_tridiag_publish(double *S, int *it, double *host, cudaStream_t s) {
+  lz_tridiag_publish_kernel<<<1, TRI_THREADS, 0, s>>>(S, it, host);
 }
 
 __global__ void copy_kernel(double *dst, const double *src, int64_t n) {

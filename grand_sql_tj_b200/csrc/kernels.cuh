@@ -66,22 +66,27 @@ struct LzRef {
   int off;
   double *fixed;
 };
-// dst = src - alpha(L) x1 - beta(L-1) x2 (x2 only for L >= 2)
-void launch_lz_update(LzRef dst, const double *src, LzRef x1, LzRef x2, const double *S, const int *it, int64_t n,
-                      cudaStream_t s);
-// S[idx + L] = ||x|| (sqrt_flag) or x.x ; it == nullptr: S[idx]
-void launch_lz_norm(LzRef x, int64_t n, double *partials, int nblk, double *S, const int *it, int idx, int sqrt_flag,
-                    cudaStream_t s);
-void launch_lz_dot(LzRef x, LzRef y, int64_t n, double *partials, int nblk, double *S, const int *it, int idx,
+// S: alpha(j) at S[j], beta(j) at S[128 + j], uu(j) at S[256 + j], the Ritz
+// value at S[512], a norm at S[513]; cnt: a zeroed int the kernels that end in
+// a grid-wide sum count their blocks on (the last block resets it); partials:
+// lz_blocks(n) doubles.
+int lz_blocks(int64_t n);
+// dst = src - alpha(L) x1 - beta(L-1) x2 (x2 only for L >= 2); beta(L) = |dst|
+void launch_lz_update_norm(LzRef dst, const double *src, LzRef x1, LzRef x2, double *S, const int *it, int64_t n,
+                           double *partials, int *cnt, cudaStream_t s);
+// w /= beta(L); w -= sum_{j < L} (V_j . w / uu[j]) V_j (classical Gram-Schmidt
+// against the first L vectors); S[513] = |w|.  mpartials: mdb * kmax doubles.
+void launch_lz_gram_schmidt(const double *V, int64_t ld, const int *it, LzRef w, int64_t n, double *S,
+                            double *mpartials, int mdb, int kmax, const double *uu, double *coef, double *partials,
+                            int *cnt, cudaStream_t s);
+// w /= S[513], copied to x; uu(L + 1) = w . w
+void launch_lz_scale_norm(LzRef w, double *x, int64_t n, double *S, const int *it, double *partials, int *cnt,
+                          cudaStream_t s);
+// alpha(L + 1) = x . y
+void launch_lz_dot(LzRef x, const double *y, int64_t n, double *S, const int *it, double *partials, int *cnt,
                    cudaStream_t s);
-// x /= S[idx + L] (it == nullptr: S[idx]); copy (if not null) receives the result too
-void launch_lz_scale(LzRef x, const double *S, const int *it, int idx, double *copy, int64_t n, cudaStream_t s);
-// w -= sum_{j < L} (V_j . w / uu[j]) V_j   (classical Gram-Schmidt against the first L vectors)
-void launch_lz_gram_schmidt(const double *V, int64_t ld, const int *it, LzRef w, int64_t n, double *partials,
-                            int nblk, int kmax, const double *uu, double *coef, cudaStream_t s);
-// lowest eigenvalue of the leading (L + noff) x (L + noff) tridiagonal
-void launch_lz_tridiag(const double *a, const double *b, const int *it, int noff, double *lam, cudaStream_t s);
-// host[0] = beta(L), host[1] = Ritz value (page-locked host memory); then L += 1
-void launch_lz_publish(const double *S, int *it, double *host, cudaStream_t s);
+// S[512] = lowest eigenvalue of the leading (L + 1) x (L + 1) tridiagonal;
+// host[0] = beta(L), host[1] = S[512] (page-locked host memory); then L += 1
+void launch_lz_tridiag_publish(double *S, int *it, double *host, cudaStream_t s);
 
 }  // namespace tjb

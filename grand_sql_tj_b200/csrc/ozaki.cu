@@ -98,19 +98,36 @@ __global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_max_kernel(const OzJob *j
   }
   if (r < 0) return;
   const double *row = oz_space(J.space, ops, psi, scr) + J.src_off + (int64_t)r * J.rs;
-  const int k0 = c * OZ_MAX_CHUNK, k1 = min(J.K, k0 + OZ_MAX_CHUNK);
-  double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
-  int kk = k0;
-  for (; kk + 4 <= k1; kk += 4) {
-    m0 = fmax(m0, fabs(row[(int64_t)kk * J.ks]));
-    m1 = fmax(m1, fabs(row[(int64_t)(kk + 1) * J.ks]));
-    m2 = fmax(m2, fabs(row[(int64_t)(kk + 2) * J.ks]));
-    m3 = fmax(m3, fabs(row[(int64_t)(kk + 3) * J.ks]));
-  }
-  for (; kk < k1; ++kk) m0 = fmax(m0, fabs(row[(int64_t)kk * J.ks]));
-  const double m = fabs(J.coef) * fmax(fmax(m0, m1), fmax(m2, m3));
+  // all OZ_MAX_CHUNK loads of the unit in flight at once (the kernel is bound
+  // by the loads in flight, not by the instructions)
+  const int k0 = c * OZ_MAX_CHUNK;
+  double x[OZ_MAX_CHUNK];
+#pragma unroll
+  for (int q = 0; q < OZ_MAX_CHUNK; ++q) x[q] = k0 + q < J.K ? fabs(row[(int64_t)(k0 + q) * J.ks]) : 0.0;
+#pragma unroll
+  for (int w = OZ_MAX_CHUNK / 2; w > 0; w >>= 1)
+#pragma unroll
+    for (int q = 0; q < w; ++q) x[q] = fmax(x[q], x[q + w]);
+  const double m = fabs(J.coef) * x[0];
   if (m > 0.0)
     atomicMax((unsigned long long *)&scales[J.scale_idx + r], (unsigned long long)__double_as_longlong(m));
+}
+
+// The radix-128 digits of y (|y| < 1) truncated toward zero -- digit q is
+// sign(y) * (floor(|y| * 128^(q+1)) mod 128), what S rounds of "multiply by
+// 128, truncate, subtract" give (every step of those is exact) -- are the
+// 7-bit groups of floor(|y| * 2^(7S)), read here from the exponent and
+// mantissa bits with integer shifts instead of 2S floating-point conversions.
+// Zero, subnormal (no digit reaches 2^-1022) and non-finite inputs give 0.
+template <int S>
+__device__ __forceinline__ uint64_t oz_fixed(double y) {
+  const uint64_t b = (uint64_t)__double_as_longlong(y);
+  const int e = (int)((b >> 52) & 0x7FFu);
+  if (e == 0 || e >= 1023) return 0;   // |y| < 2^-1022, or not below 1
+  const uint64_t m = (b & 0xFFFFFFFFFFFFFull) | 0x10000000000000ull;   // |y| = m * 2^(e - 1075)
+  const int sh = 1075 - 7 * S - e;   // >= 53 - 7S >= -3 for S <= 8
+  if (sh >= 64) return 0;
+  return sh >= 0 ? m >> sh : m << (-sh);
 }
 
 // Scaled, truncated radix-128 digits: s 16-byte digit rows per unit.
@@ -139,13 +156,13 @@ __global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_split_kernel(const OzJob 
       }
 #pragma unroll
       for (int kk = 0; kk < 16; ++kk) {
-        double t = (J.coef * x[kk]) * inv;
+        const double t = (J.coef * x[kk]) * inv;
+        const uint64_t f = oz_fixed<S>(t);
+        const bool neg = __double_as_longlong(t) < 0;
 #pragma unroll
         for (int q = 0; q < S; ++q) {
-          t *= 128.0;
-          const double a = trunc(t);
-          t -= a;
-          dig[q][kk >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)a) << (8 * (kk & 3));
+          const int a = (int)((f >> (7 * (S - 1 - q))) & 127u);
+          dig[q][kk >> 2] |= ((uint32_t)(uint8_t)(neg ? -a : a)) << (8 * (kk & 3));
         }
       }
     }

@@ -132,7 +132,7 @@ struct OzSpan {
   int32_t job, u0;
 };
 constexpr int OZ_SPLIT_THREADS = 128;
-constexpr int OZ_MAX_CHUNK = 64;
+constexpr int OZ_MAX_CHUNK = 16;
 
 struct OzPlan {
   int s = 5;
