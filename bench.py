@@ -316,7 +316,13 @@ def main():
         from grand_sql_tj_b200.lib import PinnedHost, pack_superblock, packed_arrays
         packed = pack_superblock(sb)
         pinned = PinnedHost(packed_arrays(packed))
-        e0, iters, w, e2e_wall, st2 = lanczos_leg(head, sb, lz, packed)
+        # one untimed solve (first-use costs: graph instantiation, lazy module
+        # loads), then the median of three timed solves
+        lanczos_leg(head, sb, lz, packed)
+        runs = sorted((lanczos_leg(head, sb, lz, packed) for _ in range(3)), key=lambda r: r[3])
+        e0, iters, w, e2e_wall, st2 = runs[1]
+        e2e_walls = [r[3] for r in runs]
+        del runs
         nh = max(int(st2.lanczos_hpsi), 1)
         e2e_wall = allmax(pg, e2e_wall, args.impl)
         ops_bytes = 0
@@ -329,6 +335,7 @@ def main():
                "pinned host memory + %d H*psi + Ritz vector download)" % nh,
                "h2d_bytes_per_step": int((ops_bytes + 8 * sb.wave.dim) / nh),
                "d2h_bytes_per_step": int(8 * sb.wave.dim / nh), "lanczos_iters": iters, "E0": e0,
+               "timed_solves_s": e2e_walls, "statistic": "median of 3 solves after 1 untimed",
                "breakdown_ms": {"prepare": st2.prepare_ms, "plan_compile": st2.plan_ms,
                                 "operator_upload": st2.upload_ms, "split_plan": st2.ozplan_ms,
                                 "lanczos_iterations": st2.lanczos_ms}}
