@@ -187,6 +187,7 @@ struct OzGemmParams {
   const OzSeg *segs;
   const OzFam *fams;
   const OzCell *cells;
+  const OzProdRow *prows;
   const Task *tasks;
   const uint8_t *pack;
   double *scales;
@@ -315,6 +316,11 @@ struct OzMeta {
   double ax_coef[OZ_META_AX];
   int64_t ax_off[OZ_META_AX];    // psi offset of the axpy operand's (row0, col0)
   int32_t ax_ld[OZ_META_AX];
+  // product stacks (kind 1): per tile row, the product-space offset of its
+  // column 0 (-1: a padding row of the stack), its column stride and its pi
+  int64_t row_off[128];
+  int64_t row_pi[128];
+  int32_t row_ld[128];
 };
 
 // 8 epilogue warps (two column halves of the tile x four TMEM lane quarters),
@@ -569,6 +575,41 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
         m.ax_off[lane] = t.L.off + (int64_t)it.col0 * t.L.ld + it.row0;
         m.ax_ld[lane] = t.L.ld;
       }
+      if (it.kind == 1) {
+        // a product stack: lane l resolves tile rows l, l + 32, l + 64, l + 96
+        // against the stack's products, taken 32 at a time, one per lane
+        int64_t ro[4], rp[4];
+        int32_t rl[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ro[q] = -1, rp[q] = 0, rl[q] = 0;
+        for (int s0 = c.a_begin; s0 < c.a_end; s0 += 32) {
+          OzProdRow pr;
+          if (s0 + lane < c.a_end) pr = p.prows[s0 + lane];
+          const int cnt = min(32, c.a_end - s0);
+          for (int j = 0; j < cnt; ++j) {
+            const int32_t rb = __shfl_sync(0xffffffffu, pr.row_begin, j);
+            const int32_t nr = __shfl_sync(0xffffffffu, pr.rows, j);
+            const int32_t ld = __shfl_sync(0xffffffffu, pr.ld, j);
+            const int64_t off = __shfl_sync(0xffffffffu, pr.off, j);
+            const int64_t pi = __shfl_sync(0xffffffffu, pr.pi, j);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int32_t R = it.row0 + lane + 32 * q;
+              if (R >= rb && R < rb + nr) {
+                ro[q] = off + (R - rb) + (int64_t)it.col0 * ld;
+                rp[q] = pi + (R - rb);
+                rl[q] = ld;
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          m.row_off[lane + 32 * q] = ro[q];
+          m.row_pi[lane + 32 * q] = rp[q];
+          m.row_ld[lane + 32 * q] = rl[q];
+        }
+      }
       oz_arrive(oz_smem(&meta_full[slot]));   // every lane: release of its own writes
     }
     __syncwarp();
@@ -618,8 +659,20 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
         break;
       }
       const OzMeta<BN> &m = meta[slot];
-      double *const dst = (it.kind == 0 ? p.out : p.scr) + m.c_off + r;
-      const int64_t cstride = m.c_ld;
+      // the tile row's destination: an H*psi cell, or (product stacks) the
+      // product the row belongs to (none for the stack's padding rows)
+      double *dst;
+      int64_t cstride, pi_r = 0;
+      if (it.kind == 1) {
+        const int64_t ro = rv ? m.row_off[r] : -1;
+        rv = ro >= 0;
+        dst = p.scr + (rv ? ro : 0);
+        cstride = rv ? m.row_ld[r] : 0;
+        pi_r = rv ? m.row_pi[r] : 0;
+      } else {
+        dst = p.out + m.c_off + r;
+        cstride = m.c_ld;
+      }
       // the values the tile is added to, loaded before the accumulators are
       // waited for: the old H*psi (cells of launch 2) or the axpy terms (init)
       double old[HCH * 8];
@@ -731,8 +784,8 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
           }
         }
       }
-      if (it.kind == 1 && rmax > 0.0)
-        atomicMax((unsigned long long *)&p.scales[it.pi_idx + r], (unsigned long long)__double_as_longlong(rmax));
+      if (it.kind == 1 && rv && rmax > 0.0)
+        atomicMax((unsigned long long *)&p.scales[pi_r], (unsigned long long)__double_as_longlong(rmax));
     }
   }
   __syncthreads();
@@ -773,15 +826,13 @@ static cudaError_t launch_gemm_t(const OzGemmParams &p, int ncta, cudaStream_t s
 }
 
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
-                           const OzCell *cells, const Task *tasks, const uint8_t *pack,
+                           const OzCell *cells, const OzProdRow *prows, const Task *tasks, const uint8_t *pack,
                            double *scales, const double *psi, double *scr, double *out, int *err, int s, int bn,
                            cudaStream_t st) {
   if (ncta <= 0) return cudaSuccess;
-  if (s == 5 && bn == 32) return launch_gemm_t<5, 32>(OzGemmParams{items, cta, segs, fams, cells, tasks, pack, scales,
-                                                                   psi, scr, out, err},
-                                                      ncta, st);
+  const OzGemmParams p{items, cta, segs, fams, cells, prows, tasks, pack, scales, psi, scr, out, err};
+  if (s == 5 && bn == 32) return launch_gemm_t<5, 32>(p, ncta, st);
   if (bn != oz_bn(s)) return cudaErrorInvalidValue;
-  OzGemmParams p{items, cta, segs, fams, cells, tasks, pack, scales, psi, scr, out, err};
   switch (s) {
     case 3: return launch_gemm_t<3, 48>(p, ncta, st);
     case 4: return launch_gemm_t<4, 48>(p, ncta, st);

@@ -100,8 +100,11 @@ struct OzFam {
 //   kind 0 (H*psi cell):  init = 1: the tile is written (axpy terms or
 //                         zero), then every family is added; init = 0: the
 //                         families are added to the tile
-//   kind 1 (product P_t): the tile is stored, and the maximum |P| of each
-//                         tile row raises the pi scale scales[pi_idx + row]
+//   kind 1 (products):    rows [row0, row0 + M) of a product stack (the
+//                         phase-1 products P_t = op(A_t) X of one psi cell
+//                         X, their operators' rows stacked): each tile row
+//                         is stored to its product and its maximum |P|
+//                         raises that product row's pi scale (OzProdRow)
 struct OzItem {
   int32_t kind, cell;
   int32_t row0, col0;
@@ -110,19 +113,28 @@ struct OzItem {
   int32_t fam_begin, fam_end;
   int32_t pad1;
   int32_t init;
-  int64_t pi_idx;           // kind 1: pi index of tile row 0
+  int64_t pi_idx;           // unused (0): product rows carry their pi in OzProdRow
   int32_t nkb;              // k-blocks of all its families
   int32_t pad2;
   int64_t cost;             // issued int8 MACs (for ordering)
 };
 
 // Output cell of the items: a phase-2 cell of H*psi (in the output vector)
-// with its axpy tasks, or a phase-1 product (in the product space, no axpy).
+// with its axpy tasks [a_begin, a_end), or a product stack (M stacked rows,
+// N columns) whose products are prod_rows [a_begin, a_end).
 struct OzCell {
   int64_t off;
   int32_t ld, M, N;
-  int32_t a_begin, a_end;   // axpy tasks in the phase-2 task list
+  int32_t a_begin, a_end;
   int32_t pad;
+};
+
+// One product of a stack: stack rows [row_begin, row_begin + rows) are its
+// rows 0..rows-1, stored at off + row + col * ld in the product space; the
+// pi scale of its row r is scales[pi + r].  Products start on 8-row groups.
+struct OzProdRow {
+  int32_t row_begin, rows, ld, pad;
+  int64_t off, pi;
 };
 
 // Work split of a job list over 128-thread CTAs: CTA b starts at unit u0 of
@@ -154,6 +166,7 @@ struct OzPlan {
   std::vector<OzSeg> segs;
   std::vector<OzFam> fams;
   std::vector<OzCell> cells;
+  std::vector<OzProdRow> prod_rows;        // products of the stacks (kind-1 cells)
   std::vector<OzItem> items1, items2;      // launch 1 (products, left, right), launch 2 (two-sided)
   // static schedule: CTA b of a launch runs items [cta[b], cta[b+1]) in order
   // (longest-processing-time-first assignment over nsm CTAs)
@@ -175,7 +188,7 @@ void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans
 void launch_oz_split(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
                      const double *psi, const double *scr, const double *scales, uint8_t *pack, int s, cudaStream_t st);
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
-                           const OzCell *cells, const Task *tasks, const uint8_t *pack,
+                           const OzCell *cells, const OzProdRow *prows, const Task *tasks, const uint8_t *pack,
                            double *scales, const double *psi, double *scr, double *out, int *err, int s, int bn,
                            cudaStream_t st);
 

@@ -167,84 +167,103 @@ struct Builder {
     return (int64_t)it.M * it.N * 32 * kbs * (S * (S + 1) / 2);
   }
 
-  // Phase-1 products P_t = op(A_t) X_t: per operator one static split of
-  // op(A_t) (A role, own row scales), shared by all its products; each
-  // product is a family of one segment with the column split of X_t (B role,
-  // tau) and its own output cell (the product in the scratch space).
+  // Phase-1 products P_t = op(A_t) X_t, stacked per psi cell X: the products
+  // of one X share their B operand (the canonical column split of X, scale
+  // tau) and their inner dimension, so their operators' rows are stacked
+  // into one static split (A role, 128-row tiles, each product starting on
+  // an 8-row group, row scales of their own) and the stack is one family of
+  // one segment.  Its items are 128-row x N tiles of the stack; the epilogue
+  // stores each row to its product (prod_rows) and raises that row's pi.
   void products() {
     const int BN = oz.bn;
-    std::map<std::pair<int64_t, int>, std::vector<int>> by_op;
+    std::map<int, std::vector<int>> by_x;
     for (size_t p = 0; p < hp.cells1.size(); ++p) {
       const Cell &c = hp.cells1[p];
       if (c.t_end != c.t_begin + 1) throw std::runtime_error("phase-1 cell with more than one task");
       const Task &t = hp.tasks1[c.t_begin];
       if (t.L.space != SP_OPS || t.coef != 1.0) throw std::runtime_error("unexpected phase-1 task");
-      by_op[{t.L.off, (int)t.L.trans}].push_back((int)p);
+      by_x[psi_index(t.R)].push_back((int)p);
     }
-    for (auto &kv : by_op) {
+    for (auto &kv : by_x) {
+      const int x = kv.first;
       const std::vector<int> &prods = kv.second;
-      const Cell &c0 = hp.cells1[prods[0]];
-      const Task &t0 = hp.tasks1[c0.t_begin];
-      const int32_t Mop = c0.M, K = t0.K;
-      int32_t rs, ks;
-      strides(t0.L, 0, rs, ks);
-      const Tiling ta = tiling(Mop, K, false);
+      const Cell &X = hp.cells2[x];
+      const int32_t K = X.M;
+      // the stack's rows: each product's rows from an 8-row boundary
+      int32_t rows = 0;
+      std::vector<int32_t> rb(prods.size());
+      for (size_t i = 0; i < prods.size(); ++i) {
+        const Cell &c = hp.cells1[prods[i]];
+        const Task &t = hp.tasks1[c.t_begin];
+        if (t.K != K || c.N != X.N) throw std::runtime_error("product operand shape");
+        rb[i] = rows;
+        rows += (c.M + 7) / 8 * 8;
+      }
+      const Tiling ta = tiling(rows, K, false);
       const int64_t pk = alloc_sta(ta);
-      const int64_t sc = alloc_scales(Mop);
-      oz.sta_jobs.push_back(job(SP_OPS, t0.L.off, rs, ks, Mop, K, 1.0, pk, ta, 0, ta.gsum, 0, sc, true));
-      for (int p : prods) {
+      const int64_t sc = alloc_scales(rows);
+      OzCell oc;
+      std::memset(&oc, 0, sizeof oc);
+      oc.M = rows;
+      oc.N = X.N;
+      oc.a_begin = (int32_t)oz.prod_rows.size();
+      for (size_t i = 0; i < prods.size(); ++i) {
+        const int p = prods[i];
         const Cell &c = hp.cells1[p];
         const Task &t = hp.tasks1[c.t_begin];
-        if (c.M != Mop || t.K != K) throw std::runtime_error("products of one operator differ in shape");
-        const int x = psi_index(t.R);
-        const Cell &X = hp.cells2[x];
-        if (X.M != K || X.N != c.N) throw std::runtime_error("product operand shape");
-        OzSeg sg;
-        std::memset(&sg, 0, sizeof sg);
-        sg.a_base = pk;
-        sg.a_nkb = ta.nkb;
-        sg.b_base = psi_col(x);
-        sg.b_nkb = cdiv(K, 32);
-        sg.nkb = cdiv(K, 32);
-        OzFam f;
-        std::memset(&f, 0, sizeof f);
-        f.seg_begin = (int)oz.segs.size();
-        seg_dyn_b.push_back((int)oz.segs.size());
-        oz.segs.push_back(sg);
-        f.seg_end = (int)oz.segs.size();
-        f.rs_idx = sc;
-        f.cs_idx = hp.cell2_col_state[x];
-        const int fi = (int)oz.fams.size();
-        famrel.push_back({fi, REL_NONE, REL_TAU});
-        oz.fams.push_back(f);
-        OzCell oc;
-        std::memset(&oc, 0, sizeof oc);
-        oc.off = c.off;
-        oc.ld = c.ld;
-        oc.M = c.M;
-        oc.N = c.N;
-        const int cell_idx = (int)oz.cells.size();
-        oz.cells.push_back(oc);
-        for (int32_t r0 = 0; r0 < Mop; r0 += 128)
-          for (int32_t n0 = 0; n0 < c.N; n0 += BN) {
-            OzItem it;
-            std::memset(&it, 0, sizeof it);
-            it.kind = 1;
-            it.cell = cell_idx;
-            it.row0 = r0;
-            it.col0 = n0;
-            it.mrows = std::min(128, Mop - r0);
-            it.M = it.mrows <= 64 ? 64 : 128;
-            it.ncols = std::min(BN, c.N - n0);
-            it.N = std::min(BN, (it.ncols + 15) / 16 * 16);
-            it.fam_begin = fi;
-            it.fam_end = fi + 1;
-            it.init = 0;
-            it.pi_idx = hp.cell1_row_state[p] + r0;   // made absolute in finish()
-            it.cost = item_cost(it, sg.nkb);
-            oz.items1.push_back(it);
-          }
+        int32_t rs, ks;
+        strides(t.L, 0, rs, ks);
+        oz.sta_jobs.push_back(job(SP_OPS, t.L.off, rs, ks, c.M, K, 1.0, pk, ta, rb[i], (c.M + 7) / 8, 0,
+                                  sc + rb[i], true));
+        OzProdRow pr;
+        std::memset(&pr, 0, sizeof pr);
+        pr.row_begin = rb[i];
+        pr.rows = c.M;
+        pr.ld = c.ld;
+        pr.off = c.off;
+        pr.pi = hp.cell1_row_state[p];   // made absolute in finish()
+        oz.prod_rows.push_back(pr);
       }
+      oc.a_end = (int32_t)oz.prod_rows.size();
+      OzSeg sg;
+      std::memset(&sg, 0, sizeof sg);
+      sg.a_base = pk;
+      sg.a_nkb = ta.nkb;
+      sg.b_base = psi_col(x);
+      sg.b_nkb = cdiv(K, 32);
+      sg.nkb = cdiv(K, 32);
+      OzFam f;
+      std::memset(&f, 0, sizeof f);
+      f.seg_begin = (int)oz.segs.size();
+      seg_dyn_b.push_back((int)oz.segs.size());
+      oz.segs.push_back(sg);
+      f.seg_end = (int)oz.segs.size();
+      f.rs_idx = sc;
+      f.cs_idx = hp.cell2_col_state[x];
+      const int fi = (int)oz.fams.size();
+      famrel.push_back({fi, REL_NONE, REL_TAU});
+      oz.fams.push_back(f);
+      const int cell_idx = (int)oz.cells.size();
+      oz.cells.push_back(oc);
+      for (int32_t r0 = 0; r0 < rows; r0 += 128)
+        for (int32_t n0 = 0; n0 < X.N; n0 += BN) {
+          OzItem it;
+          std::memset(&it, 0, sizeof it);
+          it.kind = 1;
+          it.cell = cell_idx;
+          it.row0 = r0;
+          it.col0 = n0;
+          it.mrows = std::min(128, rows - r0);
+          it.M = it.mrows <= 64 ? 64 : 128;
+          it.ncols = std::min(BN, X.N - n0);
+          it.N = std::min(BN, (it.ncols + 15) / 16 * 16);
+          it.fam_begin = fi;
+          it.fam_end = fi + 1;
+          it.init = 0;
+          it.pi_idx = 0;
+          it.cost = item_cost(it, sg.nkb);
+          oz.items1.push_back(it);
+        }
     }
   }
 
@@ -429,8 +448,7 @@ struct Builder {
     const int64_t base[3] = {oz.rho0, oz.tau0, oz.pi0};
     for (size_t i = 0; i < dyn_psi.size(); ++i) dyn_psi[i].scale_idx += base[dyn_psi_rel[i]];
     for (OzJob &j : dyn_prod) j.scale_idx += oz.pi0;
-    for (OzItem &it : oz.items1)
-      if (it.kind == 1) it.pi_idx += oz.pi0;
+    for (OzProdRow &pr : oz.prod_rows) pr.pi += oz.pi0;
     for (const FamRel &fr : famrel) {
       OzFam &f = oz.fams[fr.fam];
       if (fr.rs_rel != REL_NONE) f.rs_idx += base[fr.rs_rel];
@@ -586,6 +604,7 @@ struct Builder {
     oz.fams.reserve(n1 + 3 * n2);
     famrel.reserve(n1 + 3 * n2);
     oz.cells.reserve(n1 + n2);
+    oz.prod_rows.reserve(n1);
     oz.items1.reserve(ntiles);
     dyn_psi.reserve(2 * n2);
     dyn_psi_rel.reserve(2 * n2);
@@ -616,6 +635,7 @@ static_assert(sizeof(OzSeg) == sizeof(tj_oz_seg), "segment layout");
 static_assert(sizeof(OzFam) == sizeof(tj_oz_fam), "family layout");
 static_assert(sizeof(OzItem) == sizeof(tj_oz_item), "item layout");
 static_assert(sizeof(OzCell) == sizeof(tj_oz_cell), "cell layout");
+static_assert(sizeof(OzProdRow) == sizeof(tj_oz_prow), "product row layout");
 
 }  // namespace tjb
 
@@ -661,5 +681,6 @@ extern "C" int tj_ozaki_plan_export(const tj_lattice *lat, const tj_model *sys, 
   put(out->sta_mjobs, oz.sta_mjobs, out->n_sta_mjobs);
   put(out->psi_mjobs, oz.psi_mjobs, out->n_psi_mjobs);
   put(out->prod_mjobs, oz.prod_mjobs, out->n_prod_mjobs);
+  put(out->prod_rows, oz.prod_rows, out->n_prod_rows);
   return TJ_OK;
 }

@@ -102,6 +102,10 @@ class OzCellC(C.Structure):
     _fields_ = [("off", C.c_int64)] + [(n, C.c_int32) for n in ("ld", "M", "N", "a_begin", "a_end", "pad_")]
 
 
+class OzProwC(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("row_begin", "rows", "ld", "pad_")] + [("off", C.c_int64), ("pi", C.c_int64)]
+
+
 _OZ_ARRAYS = [("sta_jobs", OzJobC), ("psi_jobs", OzJobC), ("prod_jobs", OzJobC), ("segs", OzSegC),
               ("fams", OzFamC), ("cells", OzCellC), ("items1", OzItemC), ("items2", OzItemC)]
 
@@ -115,7 +119,7 @@ class OzExport(C.Structure):
                 [("n_cta1", C.c_int64), ("n_cta2", C.c_int64), ("cta1", C.POINTER(C.c_int32)),
                  ("cta2", C.POINTER(C.c_int32)), ("n_sta_mjobs", C.c_int64), ("n_psi_mjobs", C.c_int64),
                  ("n_prod_mjobs", C.c_int64), ("sta_mjobs", C.POINTER(OzJobC)), ("psi_mjobs", C.POINTER(OzJobC)),
-                 ("prod_mjobs", C.POINTER(OzJobC))])
+                 ("prod_mjobs", C.POINTER(OzJobC)), ("n_prod_rows", C.c_int64), ("prod_rows", C.POINTER(OzProwC))])
 
 
 _lib = None
@@ -453,6 +457,7 @@ def ozaki_plan_export(sb, slices: int = 5, invec: Optional[Wave] = None) -> dict
     arrs["cta2"] = (C.c_int32 * max(ex.n_cta2, 1))()
     for n in ("sta_mjobs", "psi_mjobs", "prod_mjobs"):
         arrs[n] = (OzJobC * max(getattr(ex, "n_" + n), 1))()
+    arrs["prod_rows"] = (OzProwC * max(ex.n_prod_rows, 1))()
     for k, a in arrs.items():
         setattr(ex, k, C.cast(a, type(getattr(ex, k))))
     _chk(call(C.byref(ex)))

@@ -399,8 +399,10 @@ int tj_cor_plan_export(int kind, const tj_block *a, const tj_block *b, const tj_
  * split and a B split; a family sums its segments and scales by
  * scales[rs_idx + row] * scales[cs_idx + col]; an item is one output tile
  * of cell `cell` with families [fam_begin, fam_end) (kind 0: a cell of H*psi,
- * added to; kind 1: a phase-1 product, stored, its row maxima raising the pi
- * scales from scales[pi_idx]).  The plan schedules the items of each launch statically over 148
+ * added to; kind 1: a tile of a product stack -- the phase-1 products of one
+ * input cell, their operators' rows stacked -- whose rows are stored to their
+ * products and raise their pi scales as prod_rows say; pi_idx is unused).
+ * The plan schedules the items of each launch statically over 148
  * CTAs (the export's device-independent choice).  Two-call pattern as
  * above. */
 typedef struct tj_oz_job {
@@ -418,6 +420,9 @@ typedef struct tj_oz_item {
   int64_t cost;
 } tj_oz_item;
 typedef struct tj_oz_cell { int64_t off; int32_t ld, M, N, a_begin, a_end, pad_; } tj_oz_cell;
+/* a product of a product stack (kind-1 cell): stack rows [row_begin, row_begin + rows) are stored at
+   off + row + col * ld of the product space; pi scale of its row r: pi + r */
+typedef struct tj_oz_prow { int32_t row_begin, rows, ld, pad_; int64_t off, pi; } tj_oz_prow;
 typedef struct tj_ozaki_export {
   int32_t slices, tile_n;
   int64_t sta_pack, dyn_pack, n_scales, rho0, tau0, pi0;
@@ -433,6 +438,9 @@ typedef struct tj_ozaki_export {
   /* the maximum jobs (row scales) of the three lists, run before their splits */
   int64_t n_sta_mjobs, n_psi_mjobs, n_prod_mjobs;
   tj_oz_job *sta_mjobs, *psi_mjobs, *prod_mjobs;
+  /* the products of the product stacks (cells of kind-1 items: prod_rows[a_begin, a_end)) */
+  int64_t n_prod_rows;
+  tj_oz_prow *prod_rows;
 } tj_ozaki_export;
 int tj_ozaki_plan_export(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
                          const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave, int slices,

@@ -159,11 +159,20 @@ class _Machine:
                     old = self.out[idx]
                 self.out[idx] = old + tot
             else:
-                # a phase-1 product tile: stored, and pi raised by each row's maximum
+                # a tile of a product stack: each row stored to the product it
+                # belongs to, and that row's pi raised by its maximum; the
+                # stack's padding rows (products start on 8-row groups) are zero
                 assert it.fam_end - it.fam_begin == 1 and not it.init
-                self.scr[idx] = tot
-                pi = it.pi_idx + np.arange(it.mrows)
-                self.scales[pi] = np.maximum(self.scales[pi], np.max(np.abs(tot), axis=1))
+                prods = [oz["prod_rows"][k] for k in range(c.a_begin, c.a_end)]
+                for i, R in enumerate(rows):
+                    hit = [q for q in prods if q.row_begin <= R < q.row_begin + q.rows]
+                    if not hit:
+                        assert np.all(tot[i] == 0.0)
+                        continue
+                    q = hit[0]
+                    rr = int(R - q.row_begin)
+                    self.scr[q.off + rr + cols * q.ld] = tot[i]
+                    self.scales[q.pi + rr] = max(self.scales[q.pi + rr], float(np.max(np.abs(tot[i]))))
 
 
 def execute_ozaki(plan, oz, psi):
