@@ -116,20 +116,11 @@ __global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_max_kernel(const OzJob *j
 // The radix-128 digits of y (|y| < 1) truncated toward zero -- digit q is
 // sign(y) * (floor(|y| * 128^(q+1)) mod 128), what S rounds of "multiply by
 // 128, truncate, subtract" give (every step of those is exact) -- are the
-// 7-bit groups of floor(|y| * 2^(7S)), read here from the exponent and
-// mantissa bits with integer shifts instead of 2S floating-point conversions.
-// Zero, subnormal (no digit reaches 2^-1022) and non-finite inputs give 0.
-template <int S>
-__device__ __forceinline__ uint64_t oz_fixed(double y) {
-  const uint64_t b = (uint64_t)__double_as_longlong(y);
-  const int e = (int)((b >> 52) & 0x7FFu);
-  if (e == 0 || e >= 1023) return 0;   // |y| < 2^-1022, or not below 1
-  const uint64_t m = (b & 0xFFFFFFFFFFFFFull) | 0x10000000000000ull;   // |y| = m * 2^(e - 1075)
-  const int sh = 1075 - 7 * S - e;   // >= 53 - 7S >= -3 for S <= 8
-  if (sh >= 64) return 0;
-  return sh >= 0 ? m >> sh : m << (-sh);
-}
-
+// 7-bit groups of F = floor(|y| * 2^(7S)) with the sign of y.  F comes from
+// one truncating conversion (|y| * 2^(7S) is exact: a power-of-two scaling),
+// the groups are packed four elements to a word per slice, and the words of
+// negative elements are negated bytewise at the end: (w ^ m) - m per byte,
+// m = 0xFF in the bytes of negative elements.  Non-finite inputs give 0.
 // Scaled, truncated radix-128 digits: s 16-byte digit rows per unit.
 template <int S>
 __global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_split_kernel(const OzJob *jobs, int njobs, const OzSpan *spans,
@@ -154,17 +145,22 @@ __global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_split_kernel(const OzJob 
         const int k = c16 * 16 + kk;
         x[kk] = k < J.K ? row[(int64_t)k * J.ks] : 0.0;
       }
+      constexpr double P2 = (double)(1ull << (7 * S));
+      uint32_t negm[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
       for (int kk = 0; kk < 16; ++kk) {
         const double t = (J.coef * x[kk]) * inv;
-        const uint64_t f = oz_fixed<S>(t);
-        const bool neg = __double_as_longlong(t) < 0;
+        const double a = fabs(t);
+        const uint64_t f = a < 1.0 ? __double2ull_rz(a * P2) : 0ull;
+        if (__double_as_longlong(t) < 0) negm[kk >> 2] |= 0xFFu << (8 * (kk & 3));
 #pragma unroll
-        for (int q = 0; q < S; ++q) {
-          const int a = (int)((f >> (7 * (S - 1 - q))) & 127u);
-          dig[q][kk >> 2] |= ((uint32_t)(uint8_t)(neg ? -a : a)) << (8 * (kk & 3));
-        }
+        for (int q = 0; q < S; ++q)
+          dig[q][kk >> 2] |= ((uint32_t)(f >> (7 * (S - 1 - q))) & 127u) << (8 * (kk & 3));
       }
+#pragma unroll
+      for (int q = 0; q < S; ++q)
+#pragma unroll
+        for (int w = 0; w < 4; ++w) dig[q][w] = __vsub4(dig[q][w] ^ negm[w], negm[w]);
     }
   }
   // split row -> tile, group within the tile
