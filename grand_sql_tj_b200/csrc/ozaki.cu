@@ -286,7 +286,7 @@ struct OzCfg {
   static constexpr int A_BYTES = KPS * A_KB;
   static constexpr int B_BYTES = KPS * B_KB;
   static constexpr int STAGE = A_BYTES + B_BYTES;
-  static constexpr int STAGES_RAW = (200 * 1024) / STAGE;
+  static constexpr int STAGES_RAW = (192 * 1024) / STAGE;
   static constexpr int STAGES = STAGES_RAW > 8 ? 8 : STAGES_RAW;
   static constexpr int SMEM = STAGES * STAGE;
   static_assert(S * BN <= 256, "diagonal accumulators exceed one TMEM buffer");
@@ -304,9 +304,9 @@ constexpr int OZ_META = 4;       // ring slots
 constexpr int OZ_META_AX = 4;    // axpy terms held per cell (more are read from global memory)
 template <int BN>
 struct OzMeta {
-  double cs[2][BN];
-  double rs[2][128];
-  int32_t npiece[2];             // accumulations of each family (pieces of at most OzCfg::KB_PIECE k-blocks)
+  double cs[OZ_MAX_FAM][BN];
+  double rs[OZ_MAX_FAM][128];
+  int32_t npiece[OZ_MAX_FAM];    // accumulations of each family (pieces of at most OzCfg::KB_PIECE k-blocks)
   int64_t c_off;                 // offset of the tile's (row0, col0) in out (cells) or scr (products)
   int32_t c_ld, na;              // cells: leading dimension; axpy terms (init items)
   double ax_coef[OZ_META_AX];
@@ -551,7 +551,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       }
       if (!__shfl_sync(0xffffffffu, good, 0)) break;
       OzMeta<BN> &m = meta[slot];
-      const int nf = it.fam_end - it.fam_begin;   // at most 2 (checked by the plan)
+      const int nf = it.fam_end - it.fam_begin;   // at most OZ_MAX_FAM (checked by the plan)
       for (int f = 0; f < nf; ++f) {
         const OzFam fm = p.fams[it.fam_begin + f];
         if (lane == 0) m.npiece[f] = (fm.nkb + C::KB_PIECE - 1) / C::KB_PIECE;

@@ -144,6 +144,7 @@ struct OzSpan {
   int32_t job, u0;
 };
 constexpr int OZ_SPLIT_THREADS = 128;
+constexpr int OZ_MAX_FAM = 3;   // families of one work item (a cell's left, right and two-sided sums)
 constexpr int OZ_MAX_CHUNK = 16;
 
 struct OzPlan {
@@ -167,7 +168,7 @@ struct OzPlan {
   std::vector<OzFam> fams;
   std::vector<OzCell> cells;
   std::vector<OzProdRow> prod_rows;        // products of the stacks (kind-1 cells)
-  std::vector<OzItem> items1, items2;      // launch 1 (products, left, right), launch 2 (two-sided)
+  std::vector<OzItem> items1, items2;      // launch 1 (product stacks), launch 2 (cells: left, right, two-sided)
   // static schedule: CTA b of a launch runs items [cta[b], cta[b+1]) in order
   // (longest-processing-time-first assignment over nsm CTAs)
   std::vector<int32_t> cta1, cta2;

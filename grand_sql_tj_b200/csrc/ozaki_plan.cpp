@@ -420,14 +420,16 @@ struct Builder {
       const int fl = left.empty() ? -1 : left_family(c, ci, left);
       const int fr = right.empty() ? -1 : right_family(c, ci, right, false);
       const int f2 = two.empty() ? -1 : right_family(c, ci, two, true);
-      // launch 1: the left and right families (adjacent in the list) or none
+      // launch 2 (after the products and their splits): one item per tile
+      // with all of the cell's families (adjacent in the list: left, right,
+      // two-sided), written once with its axpy terms
       int fb = 0, fe = 0;
-      if (fl >= 0 || fr >= 0) {
-        fb = fl >= 0 ? fl : fr;
-        fe = (fr >= 0 ? fr : fl) + 1;
-      }
-      add_items(oz.items1, c, cell_idx, fb, fe, 1);
-      if (f2 >= 0) add_items(oz.items2, c, cell_idx, f2, f2 + 1, 0);
+      for (int f : {fl, fr, f2})
+        if (f >= 0) {
+          if (fe == 0) fb = f;
+          fe = f + 1;
+        }
+      add_items(oz.items2, c, cell_idx, fb, fe, 1);
     }
   }
 
@@ -499,21 +501,21 @@ struct Builder {
         (v == &oz.items1 ? oz.issued1 : oz.issued2) += 2.0 * it.cost;
         kmax = std::max<int64_t>(kmax, it.cost / ((int64_t)it.M * it.N * (S * (S + 1) / 2)));
       }
-    // FP64-equivalent work: products and one-sided tasks in launch 1, two-sided tasks in launch 2
+    // FP64-equivalent work: the products in launch 1, the cells' tasks in launch 2
     oz.flops1 = oz.flops2 = 0;
     for (const Cell &c : hp.cells1) oz.flops1 += 2.0 * c.M * c.N * (double)hp.tasks1[c.t_begin].K;
     for (const Cell &c : hp.cells2)
       for (int ti = c.t_begin; ti < c.t_end; ++ti) {
         const Task &t = hp.tasks2[ti];
         if (t.R.space == SP_NONE) continue;
-        (t.L.space == SP_SCR ? oz.flops2 : oz.flops1) += 2.0 * c.M * c.N * (double)t.K;
+        oz.flops2 += 2.0 * c.M * c.N * (double)t.K;
       }
     // the epilogue stages at most two families of an item (an initialising
     // cell item may have none: it writes its axpy terms or zeros)
     for (const std::vector<OzItem> *v : {&oz.items1, &oz.items2})
       for (const OzItem &it : *v)
-        if (it.fam_end - it.fam_begin > 2 || (it.fam_end <= it.fam_begin && !(it.kind == 0 && it.init)))
-          throw std::runtime_error("work item with no family to add or with more than two");
+        if (it.fam_end - it.fam_begin > OZ_MAX_FAM || (it.fam_end <= it.fam_begin && !(it.kind == 0 && it.init)))
+          throw std::runtime_error("work item with no family to add or with more than three");
     // exact int32 accumulation: the GEMM accumulates a family in pieces of
     // at most floor((2^31 - 1) / (32 s 127^2)) k-blocks, so only one k-block
     // has to fit (it always does: 32 s 127^2 < 2^31 for s <= 8)

@@ -119,7 +119,7 @@ class _Machine:
         for ii in range(n):
             it = items[ii]
             assert it.M in (64, 128) and it.mrows <= it.M and it.N % 16 == 0 and it.ncols <= it.N <= self.BN
-            assert it.fam_end - it.fam_begin <= 2
+            assert it.fam_end - it.fam_begin <= 3
             ta, tb = it.row0 // 128, it.col0 // self.BN
             ga, gb = -(-it.mrows // 8), it.N // 8
 
