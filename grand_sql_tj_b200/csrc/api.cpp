@@ -220,6 +220,24 @@ int tjb::install_plan(tj_ctx *ctx, std::unique_ptr<HpsiPlan> P, uint64_t h,
   for (const auto &u : P->uploads)
     if (u.n > 0)
       CK(cudaMemcpyAsync(ctx->ops.d() + u.dst, u.src, sizeof(double) * u.n, cudaMemcpyHostToDevice, ctx->stream));
+  // the split-precision plan is built on the host while those copies run
+  // (from page-locked memory they return at once; the table uploads below,
+  // from pageable memory, wait for the stream to reach them)
+  double ozplan_ms = 0;
+  std::unique_ptr<OzPlan> oz;
+  if (ctx->prec_mode == TJ_PREC_OZAKI) {
+    const auto t_oz = clk::now();
+    oz.reset(new OzPlan());
+    try {
+      int nsm = 148;
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+      build_ozaki_plan(*P, ctx->slices, nsm, *oz, ctx->tune);
+    } catch (const std::exception &e) {
+      cudaStreamSynchronize(ctx->stream);   // the copies above still read the caller's buffers
+      return set_err(TJ_ERR_ARG, std::string("split-precision plan: ") + e.what());
+    }
+    ozplan_ms = ms_since(t_oz);
+  }
   {
     std::vector<int64_t> dst, n;
     std::vector<int32_t> sb, se;
@@ -248,21 +266,10 @@ int tjb::install_plan(tj_ctx *ctx, std::unique_ptr<HpsiPlan> P, uint64_t h,
   if ((rc = ctx->counters.reserve(64))) return rc;
   if ((rc = ctx->partials.reserve(sizeof(double) * (std::max(P->tiles2.size(), P->tiles1.size()) + 4096))))
     return rc;
-  const double upload_ms = ms_since(t_up);
-  double ozplan_ms = 0;
+  const double upload_ms = ms_since(t_up) - ozplan_ms;   // host time of the uploads themselves
   ctx->oz.reset();
-  if (ctx->prec_mode == TJ_PREC_OZAKI) {
-    // split-precision form: regroup the tasks, split the operators once for this step
-    const auto t_oz = clk::now();
-    std::unique_ptr<OzPlan> oz(new OzPlan());
-    try {
-      int nsm = 148;
-      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
-      build_ozaki_plan(*P, ctx->slices, nsm, *oz, ctx->tune);
-    } catch (const std::exception &e) {
-      return set_err(TJ_ERR_ARG, std::string("split-precision plan: ") + e.what());
-    }
-    ozplan_ms = ms_since(t_oz);
+  if (oz) {
+    // split-precision form: its tables, then the operators' splits (once per step)
     if ((rc = upload_vec(ctx, ctx->ozStaJobs, oz->sta_jobs)) || (rc = upload_vec(ctx, ctx->ozPsiJobs, oz->psi_jobs)) ||
         (rc = upload_vec(ctx, ctx->ozProdJobs, oz->prod_jobs)) || (rc = upload_vec(ctx, ctx->ozSegs, oz->segs)) ||
         (rc = upload_vec(ctx, ctx->ozFams, oz->fams)) ||
