@@ -354,9 +354,12 @@ __global__ void inverse_iter_kernel(const double *dall, const double *eall, cons
 }
 
 // One kept block (grp = {sector, first job, count}): classical Gram-Schmidt
-// applied twice to its vectors in descending eigenvalue order, so that the
-// dominant states are the least changed; inverse iteration leaves vectors of
-// close eigenvalues only approximately orthogonal (to about eps ||T|| / gap).
+// on its vectors in descending eigenvalue order, so that the dominant states
+// are the least changed; inverse iteration leaves vectors of close
+// eigenvalues only approximately orthogonal (to about eps ||T|| / gap).  The
+// projection is repeated only when the first one removed more than half of
+// the vector's squared norm ("twice is enough": after one pass that keeps
+// the norm above 1/sqrt(2), the vector is orthogonal to working accuracy).
 // status bit 1: a vector lost more than 0.999 of its norm to the projection.
 __global__ void __launch_bounds__(ORTH_THREADS) orthonormalize_kernel(const int *grp, const int *dims, double *Y,
                                                                       int ldy, int *status) {
@@ -387,6 +390,7 @@ __global__ void __launch_bounds__(ORTH_THREADS) orthonormalize_kernel(const int 
       const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
       for (int i = tid; i < n; i += blockDim.x) y[i] *= inv;
       __syncthreads();
+      if (nrm > 0.7071067811865476) break;   // the vector entered with unit norm
     }
   }
 }
