@@ -273,7 +273,7 @@ int tjb::install_plan(tj_ctx *ctx, std::unique_ptr<HpsiPlan> P, uint64_t h,
     if ((rc = upload_vec(ctx, ctx->ozStaJobs, oz->sta_jobs)) || (rc = upload_vec(ctx, ctx->ozPsiJobs, oz->psi_jobs)) ||
         (rc = upload_vec(ctx, ctx->ozProdJobs, oz->prod_jobs)) || (rc = upload_vec(ctx, ctx->ozSegs, oz->segs)) ||
         (rc = upload_vec(ctx, ctx->ozFams, oz->fams)) ||
-        (rc = upload_vec(ctx, ctx->ozCells, oz->cells)) || (rc = upload_vec(ctx, ctx->ozProdRows, oz->prod_rows)) ||
+        (rc = upload_vec(ctx, ctx->ozCells, oz->cells)) || (rc = upload_vec(ctx, ctx->ozStackRows, oz->stack_rows)) ||
         (rc = upload_vec(ctx, ctx->ozItems1, oz->items1)) ||
         (rc = upload_vec(ctx, ctx->ozItems2, oz->items2)) || (rc = upload_vec(ctx, ctx->ozCta1, oz->cta1)) ||
         (rc = upload_vec(ctx, ctx->ozCta2, oz->cta2)) || (rc = upload_vec(ctx, ctx->ozStaSpans, oz->sta_spans)) ||
@@ -351,7 +351,7 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
   CK(launch_oz_gemm((const OzItem *)ctx->ozItems1.p, (const int32_t *)ctx->ozCta1.p, (int)oz.cta1.size() - 1,
                     (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzCell *)ctx->ozCells.p,
-                    (const OzProdRow *)ctx->ozProdRows.p,
+                    (const OzStackRow *)ctx->ozStackRows.p,
                     (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, oz.bn, st));
   if (timed) CK(cudaEventRecord(ctx->ev[2], st));
   launch_oz_max((const OzJob *)ctx->ozProdMJobs.p, (int)oz.prod_mjobs.size(), (const OzSpan *)ctx->ozProdMSpans.p,
@@ -362,7 +362,7 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
   CK(launch_oz_gemm((const OzItem *)ctx->ozItems2.p, (const int32_t *)ctx->ozCta2.p, (int)oz.cta2.size() - 1,
                     (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzCell *)ctx->ozCells.p,
-                    (const OzProdRow *)ctx->ozProdRows.p,
+                    (const OzStackRow *)ctx->ozStackRows.p,
                     (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, oz.bn, st));
   if (timed) CK(cudaEventRecord(ctx->ev[4], st));
   CK(cudaGetLastError());

@@ -183,7 +183,7 @@ struct OzGemmParams {
   const OzSeg *segs;
   const OzFam *fams;
   const OzCell *cells;
-  const OzProdRow *prows;
+  const OzStackRow *srows;
   const Task *tasks;
   const uint8_t *pack;
   double *scales;
@@ -540,9 +540,61 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
     __syncwarp();
   } else if (warp == OZ_EPI_THREADS / 32 + 2) {
     // ------------------------------------------------ metadata (whole warp): one ring slot per item
+    // An item's static records (its families, its cell) are loaded one item
+    // ahead, and all of its own loads (the families' scales, the stack rows
+    // or the axpy terms) are issued before its ring slot is waited for, so
+    // that an item costs about one round of global loads, not a chain.
+    constexpr int CQ = (BN + 31) / 32, RQ = 128 / 32;   // loads per lane: columns, rows
+    struct FamS { int64_t rs, cs; int32_t nkb; };
+    struct CellS { int64_t off; int32_t ld, a_begin, a_end; };
+    FamS fn[OZ_MAX_FAM];
+    CellS cn;
+    auto load_static = [&](int ii) {
+      const OzItem it = get_item(ii);
+      const int nf = it.fam_end - it.fam_begin;
+#pragma unroll
+      for (int f = 0; f < OZ_MAX_FAM; ++f)
+        if (f < nf) {
+          const OzFam fm = p.fams[it.fam_begin + f];
+          fn[f] = FamS{fm.rs_idx, fm.cs_idx, fm.nkb};
+        }
+      const OzCell c = p.cells[it.cell];
+      cn = CellS{c.off, c.ld, c.a_begin, c.a_end};
+    };
+    if (ib < ie_cta) load_static(ib);
     uint32_t icount = 0;
     for (int ii = ib; ii < ie_cta; ++ii, ++icount) {
       const OzItem it = get_item(ii);
+      FamS fc[OZ_MAX_FAM];
+#pragma unroll
+      for (int f = 0; f < OZ_MAX_FAM; ++f) fc[f] = fn[f];
+      const CellS c = cn;
+      if (ii + 1 < ie_cta) load_static(ii + 1);
+      const int nf = it.fam_end - it.fam_begin;   // at most OZ_MAX_FAM (checked by the plan)
+      const int na = it.init ? c.a_end - c.a_begin : 0;
+      double csv[OZ_MAX_FAM][CQ], rsv[OZ_MAX_FAM][RQ];
+#pragma unroll
+      for (int f = 0; f < OZ_MAX_FAM; ++f) {
+#pragma unroll
+        for (int q = 0; q < CQ; ++q) {
+          const int j = lane + 32 * q;
+          csv[f][q] = f < nf && j < it.ncols ? p.scales[fc[f].cs + it.col0 + j] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < RQ; ++q) {
+          const int r = lane + 32 * q;
+          rsv[f][q] = f < nf && r < it.mrows ? p.scales[fc[f].rs + it.row0 + r] : 0.0;
+        }
+      }
+      Task tk;
+      if (lane < min(na, OZ_META_AX)) tk = p.tasks[c.a_begin + lane];
+      OzStackRow sr[RQ];
+#pragma unroll
+      for (int q = 0; q < RQ; ++q) {
+        const int r = lane + 32 * q;
+        sr[q] = OzStackRow{-1, 0, 0, 0};
+        if (it.kind == 1 && r < it.mrows) sr[q] = p.srows[c.off + it.row0 + r];
+      }
       const int slot = (int)(icount % OZ_META);
       int good = 1;
       if (lane == 0 && !oz_wait(oz_smem(&meta_empty[slot]), ((icount / OZ_META) & 1u) ^ 1u, &abort_sh)) {
@@ -551,59 +603,37 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       }
       if (!__shfl_sync(0xffffffffu, good, 0)) break;
       OzMeta<BN> &m = meta[slot];
-      const int nf = it.fam_end - it.fam_begin;   // at most OZ_MAX_FAM (checked by the plan)
-      for (int f = 0; f < nf; ++f) {
-        const OzFam fm = p.fams[it.fam_begin + f];
-        if (lane == 0) m.npiece[f] = (fm.nkb + C::KB_PIECE - 1) / C::KB_PIECE;
-        for (int j = lane; j < it.ncols; j += 32) m.cs[f][j] = oz_pow2_of(p.scales[fm.cs_idx + it.col0 + j]);
-        for (int r = lane; r < it.mrows; r += 32) m.rs[f][r] = oz_pow2_of(p.scales[fm.rs_idx + it.row0 + r]);
+#pragma unroll
+      for (int f = 0; f < OZ_MAX_FAM; ++f) {
+        if (f < nf) {
+          if (lane == 0) m.npiece[f] = (fc[f].nkb + C::KB_PIECE - 1) / C::KB_PIECE;
+#pragma unroll
+          for (int q = 0; q < CQ; ++q)
+            if (lane + 32 * q < it.ncols) m.cs[f][lane + 32 * q] = oz_pow2_of(csv[f][q]);
+#pragma unroll
+          for (int q = 0; q < RQ; ++q)
+            if (lane + 32 * q < it.mrows) m.rs[f][lane + 32 * q] = oz_pow2_of(rsv[f][q]);
+        }
       }
-      const OzCell c = p.cells[it.cell];
-      const int na = it.init ? c.a_end - c.a_begin : 0;
       if (lane == 0) {
         m.c_off = c.off + it.row0 + (int64_t)it.col0 * c.ld;
         m.c_ld = c.ld;
         m.na = na;
       }
       if (lane < min(na, OZ_META_AX)) {
-        const Task t = p.tasks[c.a_begin + lane];
-        m.ax_coef[lane] = t.coef;
-        m.ax_off[lane] = t.L.off + (int64_t)it.col0 * t.L.ld + it.row0;
-        m.ax_ld[lane] = t.L.ld;
+        m.ax_coef[lane] = tk.coef;
+        m.ax_off[lane] = tk.L.off + (int64_t)it.col0 * tk.L.ld + it.row0;
+        m.ax_ld[lane] = tk.L.ld;
       }
       if (it.kind == 1) {
-        // a product stack: lane l resolves tile rows l, l + 32, l + 64, l + 96
-        // against the stack's products, taken 32 at a time, one per lane
-        int64_t ro[4], rp[4];
-        int32_t rl[4];
+        // a product stack: tile row r is stack row row0 + r, whose product
+        // the stack-row table names
 #pragma unroll
-        for (int q = 0; q < 4; ++q) ro[q] = -1, rp[q] = 0, rl[q] = 0;
-        for (int s0 = c.a_begin; s0 < c.a_end; s0 += 32) {
-          OzProdRow pr;
-          if (s0 + lane < c.a_end) pr = p.prows[s0 + lane];
-          const int cnt = min(32, c.a_end - s0);
-          for (int j = 0; j < cnt; ++j) {
-            const int32_t rb = __shfl_sync(0xffffffffu, pr.row_begin, j);
-            const int32_t nr = __shfl_sync(0xffffffffu, pr.rows, j);
-            const int32_t ld = __shfl_sync(0xffffffffu, pr.ld, j);
-            const int64_t off = __shfl_sync(0xffffffffu, pr.off, j);
-            const int64_t pi = __shfl_sync(0xffffffffu, pr.pi, j);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const int32_t R = it.row0 + lane + 32 * q;
-              if (R >= rb && R < rb + nr) {
-                ro[q] = off + (R - rb) + (int64_t)it.col0 * ld;
-                rp[q] = pi + (R - rb);
-                rl[q] = ld;
-              }
-            }
-          }
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          m.row_off[lane + 32 * q] = ro[q];
-          m.row_pi[lane + 32 * q] = rp[q];
-          m.row_ld[lane + 32 * q] = rl[q];
+        for (int q = 0; q < RQ; ++q) {
+          const int r = lane + 32 * q;
+          m.row_off[r] = sr[q].off >= 0 ? sr[q].off + (int64_t)it.col0 * sr[q].ld : -1;
+          m.row_pi[r] = sr[q].pi;
+          m.row_ld[r] = sr[q].ld;
         }
       }
       oz_arrive(oz_smem(&meta_full[slot]));   // every lane: release of its own writes
@@ -822,11 +852,11 @@ static cudaError_t launch_gemm_t(const OzGemmParams &p, int ncta, cudaStream_t s
 }
 
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
-                           const OzCell *cells, const OzProdRow *prows, const Task *tasks, const uint8_t *pack,
+                           const OzCell *cells, const OzStackRow *srows, const Task *tasks, const uint8_t *pack,
                            double *scales, const double *psi, double *scr, double *out, int *err, int s, int bn,
                            cudaStream_t st) {
   if (ncta <= 0) return cudaSuccess;
-  const OzGemmParams p{items, cta, segs, fams, cells, prows, tasks, pack, scales, psi, scr, out, err};
+  const OzGemmParams p{items, cta, segs, fams, cells, srows, tasks, pack, scales, psi, scr, out, err};
   if (s == 5 && bn == 32) return launch_gemm_t<5, 32>(p, ncta, st);
   if (bn != oz_bn(s)) return cudaErrorInvalidValue;
   switch (s) {

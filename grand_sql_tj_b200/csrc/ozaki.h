@@ -137,6 +137,14 @@ struct OzProdRow {
   int64_t off, pi;
 };
 
+// The same per stack row, for the GEMM (derived from OzProdRow): the
+// product-space offset of the row's column 0 (-1: a padding row), its pi
+// scale index and its column stride.  A stack's rows start at its cell's off.
+struct OzStackRow {
+  int64_t off, pi;
+  int32_t ld, pad;
+};
+
 // Work split of a job list over 128-thread CTAs: CTA b starts at unit u0 of
 // job `job`.  Split units: one row (rows padded to whole groups) x 16 k;
 // maximum units: one row x OZ_MAX_CHUNK k.
@@ -168,6 +176,7 @@ struct OzPlan {
   std::vector<OzFam> fams;
   std::vector<OzCell> cells;
   std::vector<OzProdRow> prod_rows;        // products of the stacks (kind-1 cells)
+  std::vector<OzStackRow> stack_rows;      // every stack row (kind-1 cell c: rows from cells[c].off)
   std::vector<OzItem> items1, items2;      // launch 1 (product stacks), launch 2 (cells: left, right, two-sided)
   // static schedule: CTA b of a launch runs items [cta[b], cta[b+1]) in order
   // (longest-processing-time-first assignment over nsm CTAs)
@@ -189,7 +198,7 @@ void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans
 void launch_oz_split(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
                      const double *psi, const double *scr, const double *scales, uint8_t *pack, int s, cudaStream_t st);
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
-                           const OzCell *cells, const OzProdRow *prows, const Task *tasks, const uint8_t *pack,
+                           const OzCell *cells, const OzStackRow *srows, const Task *tasks, const uint8_t *pack,
                            double *scales, const double *psi, double *scr, double *out, int *err, int s, int bn,
                            cudaStream_t st);
 
