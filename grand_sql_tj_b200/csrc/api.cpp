@@ -273,7 +273,8 @@ int tjb::install_plan(tj_ctx *ctx, std::unique_ptr<HpsiPlan> P, uint64_t h,
     if ((rc = upload_vec(ctx, ctx->ozStaJobs, oz->sta_jobs)) || (rc = upload_vec(ctx, ctx->ozPsiJobs, oz->psi_jobs)) ||
         (rc = upload_vec(ctx, ctx->ozProdJobs, oz->prod_jobs)) || (rc = upload_vec(ctx, ctx->ozSegs, oz->segs)) ||
         (rc = upload_vec(ctx, ctx->ozFams, oz->fams)) ||
-        (rc = upload_vec(ctx, ctx->ozCells, oz->cells)) || (rc = upload_vec(ctx, ctx->ozStackRows, oz->stack_rows)) ||
+        (rc = upload_vec(ctx, ctx->ozCells, oz->cells)) || (rc = upload_vec(ctx, ctx->ozProdRows, oz->prod_rows)) ||
+        (rc = ctx->ozStackRows.reserve(sizeof(OzStackRow) * (oz->n_stack_rows + 1))) ||
         (rc = upload_vec(ctx, ctx->ozItems1, oz->items1)) ||
         (rc = upload_vec(ctx, ctx->ozItems2, oz->items2)) || (rc = upload_vec(ctx, ctx->ozCta1, oz->cta1)) ||
         (rc = upload_vec(ctx, ctx->ozCta2, oz->cta2)) || (rc = upload_vec(ctx, ctx->ozStaSpans, oz->sta_spans)) ||
@@ -287,6 +288,8 @@ int tjb::install_plan(tj_ctx *ctx, std::unique_ptr<HpsiPlan> P, uint64_t h,
         (rc = ctx->ozScales.reserve(sizeof(double) * (oz->n_scales + 4))) || (rc = ctx->ozMisc.reserve(256)))
       return rc;
     CK(cudaMemsetAsync(ctx->ozMisc.p, 0, 256, ctx->stream));
+    launch_oz_stack_rows((const OzCell *)ctx->ozCells.p, (int)oz->cells.size(), (const OzProdRow *)ctx->ozProdRows.p,
+                         (OzStackRow *)ctx->ozStackRows.p, oz->n_stack_rows, ctx->stream);
     CK(cudaMemsetAsync(ctx->ozScales.p, 0, sizeof(double) * (oz->n_scales + 4), ctx->stream));
     // operator splits: once per step
     launch_oz_max((const OzJob *)ctx->ozStaMJobs.p, (int)oz->sta_mjobs.size(), (const OzSpan *)ctx->ozStaMSpans.p,

@@ -63,7 +63,7 @@ struct tj_ctx {
   tjb::DevBuf ggPool, ggOut, ggTab, ggSlots;                          // grouped block-GEMM benchmark
   // split-precision H*psi
   std::unique_ptr<tjb::OzPlan> oz;
-  tjb::DevBuf ozPack, ozScales, ozStaJobs, ozPsiJobs, ozProdJobs, ozSegs, ozFams, ozCells, ozStackRows, ozItems1,
+  tjb::DevBuf ozPack, ozScales, ozStaJobs, ozPsiJobs, ozProdJobs, ozSegs, ozFams, ozCells, ozProdRows, ozStackRows, ozItems1,
       ozItems2, ozCta1, ozCta2, ozStaSpans, ozPsiSpans, ozProdSpans, ozStaMSpans,
       ozPsiMSpans, ozProdMSpans, ozStaMJobs, ozPsiMJobs, ozProdMJobs, ozMisc;
   std::vector<tjb::DevBuf *> all_bufs() {
@@ -71,7 +71,7 @@ struct tj_ctx {
             &tiles2, &red1, &red2, &slots, &m_dst, &m_n, &m_sb, &m_se, &m_src, &m_coef, &lanV, &lanScal, &lanPart, &trA, &trB,
             &trC, &trD, &trE, &corCells, &corTasks, &corTiles, &corOps, &corScr, &corPsi, &ggPool, &ggOut, &ggTab,
             &ggSlots, &ozPack, &ozScales,
-            &ozStaJobs, &ozPsiJobs, &ozProdJobs, &ozSegs, &ozFams, &ozCells, &ozStackRows, &ozItems1, &ozItems2,
+            &ozStaJobs, &ozPsiJobs, &ozProdJobs, &ozSegs, &ozFams, &ozCells, &ozProdRows, &ozStackRows, &ozItems1, &ozItems2,
             &ozCta1, &ozCta2, &ozStaSpans, &ozPsiSpans, &ozProdSpans, &ozStaMSpans,
             &ozPsiMSpans, &ozProdMSpans, &ozStaMJobs, &ozPsiMJobs, &ozProdMJobs, &ozMisc};
   }

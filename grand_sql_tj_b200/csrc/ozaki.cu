@@ -819,7 +819,26 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
 }
 
+// The stack-row table: one CTA per cell; a product stack's products write
+// their rows (the table was set to 0xFF bytes, off = -1, for padding rows).
+__global__ void oz_stack_rows_kernel(const OzCell *cells, const OzProdRow *prows, OzStackRow *srows) {
+  const OzCell c = cells[blockIdx.x];
+  if (c.ld != 0 || c.a_end <= c.a_begin) return;   // not a product stack
+  for (int k = c.a_begin; k < c.a_end; ++k) {
+    const OzProdRow pr = prows[k];
+    for (int r = threadIdx.x; r < pr.rows; r += blockDim.x)
+      srows[c.off + pr.row_begin + r] = OzStackRow{pr.off + r, pr.pi + r, pr.ld, 0};
+  }
+}
+
 // ------------------------------------------------------------ host launches
+void launch_oz_stack_rows(const OzCell *cells, int ncells, const OzProdRow *prows, OzStackRow *srows, int64_t n,
+                          cudaStream_t st) {
+  if (ncells <= 0 || n <= 0) return;
+  cudaMemsetAsync(srows, 0xFF, sizeof(OzStackRow) * (size_t)n, st);
+  oz_stack_rows_kernel<<<ncells, 128, 0, st>>>(cells, prows, srows);
+}
+
 void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
                    const double *psi, const double *scr, double *scales, cudaStream_t st) {
   if (njobs <= 0 || nspans <= 0) return;

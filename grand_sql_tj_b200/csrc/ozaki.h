@@ -137,9 +137,10 @@ struct OzProdRow {
   int64_t off, pi;
 };
 
-// The same per stack row, for the GEMM (derived from OzProdRow): the
-// product-space offset of the row's column 0 (-1: a padding row), its pi
-// scale index and its column stride.  A stack's rows start at its cell's off.
+// The same per stack row, for the GEMM (filled on the device from OzProdRow
+// by launch_oz_stack_rows): the product-space offset of the row's column 0
+// (-1: a padding row), its pi scale index and its column stride.  A stack's
+// rows start at its cell's off.
 struct OzStackRow {
   int64_t off, pi;
   int32_t ld, pad;
@@ -176,7 +177,7 @@ struct OzPlan {
   std::vector<OzFam> fams;
   std::vector<OzCell> cells;
   std::vector<OzProdRow> prod_rows;        // products of the stacks (kind-1 cells)
-  std::vector<OzStackRow> stack_rows;      // every stack row (kind-1 cell c: rows from cells[c].off)
+  int64_t n_stack_rows = 0;                // rows of the stack-row table (kind-1 cell c: from cells[c].off)
   std::vector<OzItem> items1, items2;      // launch 1 (product stacks), launch 2 (cells: left, right, two-sided)
   // static schedule: CTA b of a launch runs items [cta[b], cta[b+1]) in order
   // (longest-processing-time-first assignment over nsm CTAs)
@@ -193,6 +194,9 @@ struct OzPlan {
 void build_ozaki_plan(const HpsiPlan &hp, int s, int nsm, OzPlan &oz, const TuneParams &tp = TuneParams());
 
 // device launches (ozaki.cu)
+// the stack-row table (n rows) from the stacks' products; padding rows get off = -1
+void launch_oz_stack_rows(const OzCell *cells, int ncells, const OzProdRow *prows, OzStackRow *srows, int64_t n,
+                          cudaStream_t st);
 void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
                    const double *psi, const double *scr, double *scales, cudaStream_t st);
 void launch_oz_split(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,

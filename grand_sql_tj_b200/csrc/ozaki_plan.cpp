@@ -451,17 +451,13 @@ struct Builder {
     for (size_t i = 0; i < dyn_psi.size(); ++i) dyn_psi[i].scale_idx += base[dyn_psi_rel[i]];
     for (OzJob &j : dyn_prod) j.scale_idx += oz.pi0;
     for (OzProdRow &pr : oz.prod_rows) pr.pi += oz.pi0;
-    // the per-row table of the stacks, read by the GEMM's metadata warp
-    oz.stack_rows.clear();
+    // the stacks' places in the per-row table the GEMM's metadata warp reads
+    // (the table itself is filled on the device)
+    oz.n_stack_rows = 0;
     for (OzCell &c : oz.cells) {
       if (c.a_end <= c.a_begin || c.ld != 0) continue;   // H*psi cells have ld > 0
-      c.off = (int64_t)oz.stack_rows.size();
-      oz.stack_rows.resize(oz.stack_rows.size() + c.M, OzStackRow{-1, 0, 0, 0});
-      for (int k = c.a_begin; k < c.a_end; ++k) {
-        const OzProdRow &pr = oz.prod_rows[k];
-        for (int32_t r = 0; r < pr.rows; ++r)
-          oz.stack_rows[c.off + pr.row_begin + r] = OzStackRow{pr.off + r, pr.pi + r, pr.ld, 0};
-      }
+      c.off = oz.n_stack_rows;
+      oz.n_stack_rows += c.M;
     }
     for (const FamRel &fr : famrel) {
       OzFam &f = oz.fams[fr.fam];
