@@ -80,6 +80,7 @@ struct OSub {
   int64_t off;   // device offset of the stored matrix
   bool zero;     // structurally zero (merged sub-block without contributions)
   mutable bool touched = false;   // read by some task of the plan being built
+  int32_t merge = -1;             // merged sub-blocks (hmerge): index of its merge record
 };
 struct OBlk {
   int len = 0, up_dif = 0, down_dif = 0;
@@ -1110,6 +1111,7 @@ static void pass_info(const OBlk &old, OBlk &nw, HpsiPlan &plan) {
     s.off = plan.ops_len;
     s.zero = true;
     plan.sub_extent.push_back({s.off, n});
+    s.merge = (int32_t)plan.merges.size();
     plan.merges.push_back({s.off, n, (int32_t)plan.merge_src.size(), (int32_t)plan.merge_src.size()});
     plan.ops_len += align4(n);
   }
@@ -1124,21 +1126,22 @@ static void add_two(const OBlk &b1, double coef, OBlk &nw, HpsiPlan &plan) {
         x1 = x + 1;
         if ((int64_t)q.row_dim * q.sdim != (int64_t)s.row_dim * s.sdim)
           throw PlanError(TJ_ERR_ARG, "hmerge: operator sub-blocks of different size");
-        // find the merge record of s (its destination offset)
-        for (auto it = plan.merges.rbegin(); it != plan.merges.rend(); ++it)
-          if (it->dst == s.off) {
-            // sources of one destination are contiguous: append by moving this record last
-            HpsiPlan::Merge m = *it;
-            std::vector<int64_t> src(plan.merge_src.begin() + m.s_begin, plan.merge_src.begin() + m.s_end);
-            std::vector<double> cf(plan.merge_coef.begin() + m.s_begin, plan.merge_coef.begin() + m.s_end);
-            src.push_back(q.off);
-            cf.push_back(coef);
-            it->s_begin = (int32_t)plan.merge_src.size();
-            plan.merge_src.insert(plan.merge_src.end(), src.begin(), src.end());
-            plan.merge_coef.insert(plan.merge_coef.end(), cf.begin(), cf.end());
-            it->s_end = (int32_t)plan.merge_src.size();
-            break;
-          }
+        // the merge record of s (one per merged sub-block, made by pass_info)
+        if (s.merge < 0 || plan.merges[s.merge].dst != s.off)
+          throw PlanError(TJ_ERR_ARG, "hmerge: merged sub-block without its merge record");
+        HpsiPlan::Merge &mr = plan.merges[s.merge];
+        // sources of one destination are contiguous: append by moving them last
+        const int32_t b = mr.s_begin, e = mr.s_end;
+        mr.s_begin = (int32_t)plan.merge_src.size();
+        for (int32_t k = b; k < e; ++k) {
+          const int64_t src = plan.merge_src[k];
+          const double cf = plan.merge_coef[k];
+          plan.merge_src.push_back(src);
+          plan.merge_coef.push_back(cf);
+        }
+        plan.merge_src.push_back(q.off);
+        plan.merge_coef.push_back(coef);
+        mr.s_end = (int32_t)plan.merge_src.size();
         s.zero = false;
         break;
       }
