@@ -77,7 +77,11 @@ __device__ __forceinline__ bool oz_unit(const OzJob *jobs, int njobs, const OzSp
 
 // Row maxima of |coef * M| (a list of maximum jobs): one unit = one row x
 // OZ_MAX_CHUNK k, consecutive threads on consecutive rows, one atomic max
-// per unit.
+// per unit.  Jobs with want_max = 2 (a psi cell split both ways) also raise
+// the column maxima, scales[dst + k]: their rows are padded to whole warps
+// and they come first in the list, so a warp holds 32 rows of one job and
+// one chunk, and each column's maximum is reduced across the warp and
+// raised by one lane.
 __global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_max_kernel(const OzJob *jobs, int njobs, const OzSpan *spans,
                                                                   const double *ops, const double *psi,
                                                                   const double *scr, double *scales) {
@@ -88,28 +92,42 @@ __global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_max_kernel(const OzJob *j
   for (int j = sp.job; j < njobs; ++j) {
     J = jobs[j];
     const int nc = (J.K + OZ_MAX_CHUNK - 1) / OZ_MAX_CHUNK;
-    const int64_t units = (int64_t)J.nrows * nc;
+    const int rows = J.want_max == 2 ? (J.nrows + 31) / 32 * 32 : J.nrows;
+    const int64_t units = (int64_t)rows * nc;
     if (k < units) {
-      r = (int)(k % J.nrows);
-      c = (int)(k / J.nrows);
+      r = (int)(k % rows);
+      c = (int)(k / rows);
       break;
     }
     k -= units;
   }
   if (r < 0) return;
-  const double *row = oz_space(J.space, ops, psi, scr) + J.src_off + (int64_t)r * J.rs;
+  const bool valid = r < J.nrows;
+  const double *row = oz_space(J.space, ops, psi, scr) + J.src_off + (int64_t)(valid ? r : 0) * J.rs;
   // all OZ_MAX_CHUNK loads of the unit in flight at once (the kernel is bound
   // by the loads in flight, not by the instructions)
   const int k0 = c * OZ_MAX_CHUNK;
   double x[OZ_MAX_CHUNK];
 #pragma unroll
-  for (int q = 0; q < OZ_MAX_CHUNK; ++q) x[q] = k0 + q < J.K ? fabs(row[(int64_t)(k0 + q) * J.ks]) : 0.0;
+  for (int q = 0; q < OZ_MAX_CHUNK; ++q) x[q] = valid && k0 + q < J.K ? fabs(row[(int64_t)(k0 + q) * J.ks]) : 0.0;
+  if (J.want_max == 2) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int q = 0; q < OZ_MAX_CHUNK; ++q) {
+      double cm = x[q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+      cm *= fabs(J.coef);
+      if (lane == q && k0 + q < J.K && cm > 0.0)
+        atomicMax((unsigned long long *)&scales[J.dst + k0 + q], (unsigned long long)__double_as_longlong(cm));
+    }
+  }
 #pragma unroll
   for (int w = OZ_MAX_CHUNK / 2; w > 0; w >>= 1)
 #pragma unroll
     for (int q = 0; q < w; ++q) x[q] = fmax(x[q], x[q + w]);
   const double m = fabs(J.coef) * x[0];
-  if (m > 0.0)
+  if (valid && m > 0.0)
     atomicMax((unsigned long long *)&scales[J.scale_idx + r], (unsigned long long)__double_as_longlong(m));
 }
 

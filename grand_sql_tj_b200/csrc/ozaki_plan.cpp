@@ -42,6 +42,7 @@ struct Builder {
   int64_t sta_bytes = 0, dyn_bytes = 0;
   std::vector<OzJob> dyn_psi, dyn_prod;
   std::vector<int> dyn_psi_rel;                 // REL_RHO / REL_TAU per psi job
+  std::vector<int> row_job, col_job;            // per psi cell: its row / column split job in dyn_psi, or -1
   std::unordered_map<int64_t, int> psi_cell;    // psi offset -> phase-2 cell
   std::unordered_map<int64_t, int> prod_of;     // scratch offset -> product
   std::vector<int64_t> colsplit, rowsplit;      // per psi cell: dynamic pack offset or -1
@@ -134,6 +135,7 @@ struct Builder {
       colsplit[c] = alloc_dyn(t);
       dyn_psi.push_back(job(SP_PSI, x.off, x.ld, 1, x.N, x.M, 1.0, colsplit[c], t, 0, t.gsum, 0,
                             hp.cell2_col_state[c], true));
+      col_job[c] = (int)dyn_psi.size() - 1;
       dyn_psi_rel.push_back(REL_TAU);
     }
     return colsplit[c];
@@ -146,6 +148,7 @@ struct Builder {
       rowsplit[c] = alloc_dyn(t);
       dyn_psi.push_back(job(SP_PSI, x.off, 1, x.ld, x.M, x.N, 1.0, rowsplit[c], t, 0, t.gsum, 0,
                             hp.cell2_row_state[c], true));
+      row_job[c] = (int)dyn_psi.size() - 1;
       dyn_psi_rel.push_back(REL_RHO);
     }
     return rowsplit[c];
@@ -489,7 +492,28 @@ struct Builder {
       all.resize(w);
     };
     part(oz.sta_jobs, oz.sta_mjobs);
-    part(dyn_psi, oz.psi_mjobs);
+    // a psi cell split both ways gets one maximum job for its rows (rho) and
+    // its columns (tau, base in the job's dst): want_max = 2, rows padded to
+    // warps; those jobs go first, so that no warp of the maximum kernel
+    // straddles two of them or a job of another kind
+    {
+      std::vector<OzJob> comb, rest;
+      std::vector<char> merged(dyn_psi.size(), 0);
+      for (size_t c = 0; c < row_job.size(); ++c)
+        if (row_job[c] >= 0 && col_job[c] >= 0) {
+          OzJob j = dyn_psi[row_job[c]];
+          j.want_max = 2;
+          j.dst = dyn_psi[col_job[c]].scale_idx;
+          comb.push_back(j);
+          merged[row_job[c]] = merged[col_job[c]] = 1;
+        }
+      for (size_t i = 0; i < dyn_psi.size(); ++i)
+        if (!merged[i] && dyn_psi[i].want_max) rest.push_back(dyn_psi[i]);
+      std::vector<OzJob> splits;
+      part(dyn_psi, splits);   // the split list (want_split), in creation order
+      oz.psi_mjobs = std::move(comb);
+      oz.psi_mjobs.insert(oz.psi_mjobs.end(), rest.begin(), rest.end());
+    }
     part(dyn_prod, oz.prod_mjobs);
     oz.psi_jobs = std::move(dyn_psi);
     oz.prod_jobs = std::move(dyn_prod);
@@ -534,7 +558,7 @@ struct Builder {
   // global units [b*T, (b+1)*T), starting inside job `job` at unit u0.
   // Split units cover gtot*8 rows x K/16; maximum units nrows x K/OZ_MAX_CHUNK.
   static int64_t job_units(const OzJob &j, bool max_units) {
-    if (max_units) return (int64_t)j.nrows * cdiv(j.K, OZ_MAX_CHUNK);
+    if (max_units) return (int64_t)(j.want_max == 2 ? (j.nrows + 31) / 32 * 32 : j.nrows) * cdiv(j.K, OZ_MAX_CHUNK);
     return (int64_t)j.gtot * 8 * (cdiv(j.K, 32) * 2);
   }
   static void make_spans(const std::vector<OzJob> &jobs, std::vector<OzSpan> &spans, bool max_units) {
@@ -600,6 +624,8 @@ struct Builder {
     for (size_t p = 0; p < hp.cells1.size(); ++p) prod_of[hp.cells1[p].off] = (int)p;
     colsplit.assign(npsi, -1);
     rowsplit.assign(npsi, -1);
+    row_job.assign(npsi, -1);
+    col_job.assign(npsi, -1);
     prodsplit.assign(hp.cells1.size(), -1);
     // capacities: one static job and one segment per product and per phase-2
     // GEMM task, up to three families and one work-item row per tile

@@ -48,9 +48,14 @@ class _Machine:
             j = jobs[i]
             if not j.want_max:
                 continue
-            m = np.max(np.abs(self._matrix(j)), axis=1)
+            A = np.abs(self._matrix(j))
+            m = np.max(A, axis=1)
             idx = j.scale_idx + np.arange(j.nrows)
             self.scales[idx] = np.maximum(self.scales[idx], m)
+            if j.want_max == 2:
+                # a psi cell split both ways: its column maxima too, from dst
+                cidx = j.dst + np.arange(j.K)
+                self.scales[cidx] = np.maximum(self.scales[cidx], np.max(A, axis=0))
 
     def run_split(self, jobs, n):
         S = self.S
