@@ -190,7 +190,8 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   const auto t_start = std::chrono::steady_clock::now();
   std::unique_ptr<HpsiPlan> P(new HpsiPlan());
   std::string msg;
-  int rc = build_hpsi_plan(lat, sys, env, sys_bs, env_bs, wave, *P, msg);
+  // the FP64 work lists only for the FP64 path
+  int rc = build_hpsi_plan(lat, sys, env, sys_bs, env_bs, wave, *P, msg, ctx->prec_mode == TJ_PREC_FP64);
   if (rc) return set_err(rc, "H*psi plan: " + msg);
   if ((rc = install_plan(ctx, std::move(P), h, t_start))) return rc;
   if (!ctx->tuning && ctx->autotune == TJ_TUNE_ON_MISS && !tune_lookup(ctx->hist_key, ctx->tune))
@@ -209,7 +210,7 @@ int tjb::install_plan(tj_ctx *ctx, std::unique_ptr<HpsiPlan> P, uint64_t h,
   // tiling choices: the autotuner's for this block-size histogram, when known
   ctx->hist_key = plan_hist_key(*P, ctx->prec_mode, ctx->slices);
   if (!ctx->tuning && ctx->autotune != TJ_TUNE_OFF) tune_lookup(ctx->hist_key, ctx->tune);
-  if (!(ctx->tune == TuneParams())) {
+  if (!(ctx->tune == TuneParams()) && ctx->prec_mode == TJ_PREC_FP64) {
     split_tiles(P->cells1, P->tasks1, P->tiles1, P->red1, P->nslots1, false, ctx->tune);
     split_tiles(P->cells2, P->tasks2, P->tiles2, P->red2, P->nslots2, false, ctx->tune);
   }

@@ -306,6 +306,7 @@ struct Builder {
   std::unordered_map<ProdKey, int, ProdKeyHash> prod_id;
   bool dedup = true;
   bool cor_mode = false;   // correlators: keep only the cells that have tasks
+  bool want_tiles = true;  // make the FP64 work lists
 
   Builder(const tj_basis *s, const tj_basis *e, const tj_wave *w, HpsiPlan &p) : sbs(s), ebs(e), wave(w), plan(p) {}
 
@@ -1048,8 +1049,10 @@ struct Builder {
                           std::vector<Tile> &tiles, std::vector<Reduce> &red, int64_t &nslots) {
       split_tiles(cells, tasks, tiles, red, nslots, cor_mode);
     };
-    make_tiles(plan.cells1, plan.tasks1, plan.tiles1, plan.red1, plan.nslots1);
-    make_tiles(plan.cells2, plan.tasks2, plan.tiles2, plan.red2, plan.nslots2);
+    if (want_tiles) {
+      make_tiles(plan.cells1, plan.tasks1, plan.tiles1, plan.red1, plan.nslots1);
+      make_tiles(plan.cells2, plan.tasks2, plan.tiles2, plan.red2, plan.nslots2);
+    }
   }
 };
 
@@ -1294,7 +1297,7 @@ static void check_lattice(const tj_lattice *L) {
 }  // namespace
 
 int build_hpsi_plan(const tj_lattice *lat, const tj_model *sysm, const tj_model *envm, const tj_basis *sys_bs,
-                    const tj_basis *env_bs, const tj_wave *wave, HpsiPlan &plan, std::string &msg) {
+                    const tj_basis *env_bs, const tj_wave *wave, HpsiPlan &plan, std::string &msg, bool tiles) {
   try {
     check_lattice(lat);
     if (!sys_bs || !env_bs || !wave || !sys_bs->sub || !env_bs->sub || (wave->num > 0 && !wave->sub))
@@ -1311,6 +1314,7 @@ int build_hpsi_plan(const tj_lattice *lat, const tj_model *sysm, const tj_model 
     hmerge(g, sys, env, plan);
     const SiteOps so = make_site_ops(lat->up_bias);
     Builder B(sys_bs, env_bs, wave, plan);
+    B.want_tiles = tiles;
     B.init_cells();
     plan.psi_len = wave->dim;
     // model_wave, add_op = 1 (get_sys.f90:4157-4239)

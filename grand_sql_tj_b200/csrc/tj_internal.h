@@ -118,9 +118,11 @@ void split_tiles(const std::vector<Cell> &cells, const std::vector<Task> &tasks,
                  std::vector<Reduce> &red, int64_t &nslots, bool dot_mode, const TuneParams &tp = TuneParams());
 
 // Builds the plan (host).  Returns TJ_OK or an error code with msg set.
+// tiles = false: the FP64 work lists (tiles, reduce records) are not made
+// (the split-precision path runs its own)
 int build_hpsi_plan(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
                     const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave,
-                    HpsiPlan &plan, std::string &msg);
+                    HpsiPlan &plan, std::string &msg, bool tiles = true);
 
 // Independent superblocks in one plan (shared launches); psi_off[i]: offset of
 // instance i's vector in the concatenated input / output vector.
