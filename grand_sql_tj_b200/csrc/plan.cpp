@@ -380,6 +380,14 @@ struct Builder {
     }
     out_tasks.clear();
     out_cell.clear();
+    // capacities from the cell count (a cell has a few terms of each kind),
+    // so that the lists are not regrown and rehashed while the terms are emitted
+    out_tasks.reserve((size_t)ncells * 4);
+    out_cell.reserve((size_t)ncells * 4);
+    prod_id.reserve((size_t)ncells * 2);
+    plan.cells1.reserve((size_t)ncells * 2);
+    plan.tasks1.reserve((size_t)ncells * 2);
+    plan.cell1_row_state.reserve((size_t)ncells * 2);
   }
   int cell(int i, int m, int n) const { return cell_base[i] + m * ebs->sub[sec_y[i]].num + n; }
   int find_sec(int su, int sd, int eu, int ed) const {
