@@ -81,6 +81,11 @@ class Clocks:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the timed region can be shorter than nvidia-smi's start-up: wait
+            # (up to 3 s) for its first sample, so that the region is covered
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
