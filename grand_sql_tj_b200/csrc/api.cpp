@@ -426,7 +426,7 @@ int tjb::run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed) {
   return TJ_OK;
 }
 
-static int check_wave(const tj_wave *w) {
+int tjb::check_wave(const tj_wave *w) {
   if (!w || w->num < 0 || (w->num > 0 && (!w->sub || !w->data)) || w->dim < 0)
     return set_err(TJ_ERR_ARG, "bad wavefunction");
   int64_t d = 0;
@@ -437,7 +437,7 @@ static int check_wave(const tj_wave *w) {
   if (d > w->dim) return set_err(TJ_ERR_ARG, "sector extends past wave->dim");
   return TJ_OK;
 }
-static bool same_layout(const tj_wave *a, const tj_wave *b) {
+bool tjb::same_layout(const tj_wave *a, const tj_wave *b) {
   if (a->num != b->num || a->dim != b->dim) return false;
   return std::memcmp(a->sub, b->sub, sizeof(tj_wave_sub) * a->num) == 0;
 }

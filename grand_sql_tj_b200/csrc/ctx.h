@@ -83,6 +83,11 @@ int prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const 
                  const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave);
 int run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed);
 int check_device_flags(tj_ctx *ctx);
+// wavefunction table checks shared by every entry point that takes a tj_wave:
+// null tables, negative sizes or offsets, a sector past wave->dim
+int check_wave(const tj_wave *w);
+// same sector table (outvec must have invec's layout)
+bool same_layout(const tj_wave *a, const tj_wave *b);
 int install_plan(tj_ctx *ctx, std::unique_ptr<HpsiPlan> P, uint64_t key, std::chrono::steady_clock::time_point t0);
 
 // autotuning (tune.cpp)

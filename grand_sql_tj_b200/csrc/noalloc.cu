@@ -71,16 +71,25 @@ extern "C" int tj_model_wave_noalloc(const tj_lattice *lat, const tj_model *sys,
   using namespace tjb;
   if (!lat || !sys || !env || !sys_bs || !env_bs || !invec || !outvec)
     return set_err(TJ_ERR_ARG, "tj_model_wave_noalloc: null argument");
+  int rc;
+  if ((rc = check_wave(invec)) || (rc = check_wave(outvec))) return rc;
   if (!invec->data || !outvec->data || misaligned(invec->data) || misaligned(outvec->data))
     return set_err(TJ_ERR_ARG, "tj_model_wave_noalloc: wave data must be 8-byte aligned device pointers");
-  if (invec->num != outvec->num || invec->dim != outvec->dim ||
-      (invec->num > 0 && std::memcmp(invec->sub, outvec->sub, sizeof(tj_wave_sub) * invec->num) != 0))
+  if (!same_layout(invec, outvec))
     return set_err(TJ_ERR_ARG, "tj_model_wave_noalloc: outvec must have invec's sector layout");
+  {
+    // the second GEMM pass reads psi while other tiles already write H*psi:
+    // the two vectors must not share memory
+    const uintptr_t a0 = (uintptr_t)invec->data, a1 = a0 + sizeof(double) * (uintptr_t)invec->dim;
+    const uintptr_t b0 = (uintptr_t)outvec->data, b1 = b0 + sizeof(double) * (uintptr_t)outvec->dim;
+    if (invec->dim > 0 && a0 < b1 && b0 < a1)
+      return set_err(TJ_ERR_ARG, "tj_model_wave_noalloc: invec and outvec data overlap (in-place H*psi is not supported)");
+  }
   cudaStream_t s = (cudaStream_t)stream;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return set_err(TJ_ERR_NODEV, "tj_model_wave_noalloc: no CUDA device");
   double *base = nullptr;
-  int rc = scratch_address(dev, &base);
+  rc = scratch_address(dev, &base);
   if (rc) return rc;
 
   HpsiPlan P;
@@ -93,15 +102,26 @@ extern "C" int tj_model_wave_noalloc(const tj_lattice *lat, const tj_model *sys,
   // them; merged blocks go to the start of the scratch array.
   int64_t merged0 = P.ops_len;
   for (const auto &m : P.merges) merged0 = std::min(merged0, m.dst);
-  std::vector<HpsiPlan::Upload> ups = P.uploads;
-  for (const auto &u : ups)
-    if (u.n > 0 && misaligned(u.src))
-      return set_err(TJ_ERR_ARG, "tj_model_wave_noalloc: operator data must be 8-byte aligned device pointers");
+  // a block whose sub-blocks are all empty has an upload of length 0 at the
+  // same offset as the next block's; it is dropped so that the offset search
+  // below can only land on the block that holds the offset
+  std::vector<HpsiPlan::Upload> ups;
+  for (const auto &u : P.uploads)
+    if (u.n > 0) {
+      if (!u.src || misaligned(u.src))
+        return set_err(TJ_ERR_ARG, "tj_model_wave_noalloc: operator data must be 8-byte aligned device pointers");
+      ups.push_back(u);
+    }
   std::sort(ups.begin(), ups.end(), [](const HpsiPlan::Upload &a, const HpsiPlan::Upload &b) { return a.dst < b.dst; });
+  bool unmapped = false;
   auto remap = [&](int64_t v) -> int64_t {
     if (v >= merged0) return v - merged0;
     auto it = std::upper_bound(ups.begin(), ups.end(), v,
                                [](int64_t x, const HpsiPlan::Upload &u) { return x < u.dst; });
+    if (it == ups.begin() || v >= (it - 1)->dst + (it - 1)->n) {
+      unmapped = true;   // not inside any operator block the caller passed
+      return 0;
+    }
     const HpsiPlan::Upload &u = *(it - 1);
     return (int64_t)(((intptr_t)u.src - (intptr_t)base) / (intptr_t)sizeof(double)) + (v - u.dst);
   };
@@ -119,6 +139,7 @@ extern "C" int tj_model_wave_noalloc(const tj_lattice *lat, const tj_model *sys,
     mse.push_back(m.s_end);
   }
   for (int64_t &x : msrc) x = remap(x);
+  if (unmapped) return set_err(TJ_ERR_ARG, "tj_model_wave_noalloc: an operand lies outside every operator block");
 
   // scratch layout: merged operators | phase-1 products | partial tiles | work lists | counters
   int64_t cursor = up256(P.ops_len - merged0);

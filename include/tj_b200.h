@@ -330,11 +330,16 @@ int tj_model_wave_bench(tj_ctx *ctx, const tj_lattice *lat,
  * that the library declares; every GPU that loads the library holds it until
  * the process exits.  The call allocates nothing (no cudaMalloc/cudaFree),
  * runs on `stream` (a cudaStream_t, NULL for the default stream) and returns
- * after the stream has synchronised.  A superblock needing more scratch than
- * the array holds is rejected with TJ_ERR_LIMIT.  The first call on a device
- * looks up the array's device address, so make that first call before any
- * stream capture.  All calls share the one array: calls that overlap on the
- * GPU (other threads, other streams) race and must not be issued. */
+ * after the stream has synchronised.  It always computes in FP64 (the grouped
+ * FP64 GEMM): the split-precision mode of a tj_ctx does not apply to it.
+ * invec and outvec must not share memory (TJ_ERR_ARG otherwise).  A
+ * superblock needing more scratch than the array holds is rejected with
+ * TJ_ERR_LIMIT.  The first call on a device looks up the array's device
+ * address and keeps it for the life of the process, so make that first call
+ * before any stream capture, and do not call this entry point on a device
+ * after resetting it (cudaDeviceReset): the kept address would be stale.  All
+ * calls share the one array: calls that overlap on the GPU (other threads,
+ * other streams) race and must not be issued. */
 #define TJ_NOALLOC_SCRATCH_BYTES (64ull << 20)
 int tj_model_wave_noalloc(const tj_lattice *lat, const tj_model *sys, const tj_model *env,
                           const tj_basis *sys_bs, const tj_basis *env_bs,

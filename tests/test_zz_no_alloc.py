@@ -70,3 +70,30 @@ def test_model_wave_noalloc_matches_model_wave(product_lib):
         assert np.all(np.isfinite(got)), "call %d left unwritten entries" % call
         err = np.max(np.abs(got - expected)) / scale
         assert err < 1e-12, (call, err)
+
+
+def test_model_wave_noalloc_rejects_overlapping_vectors(product_lib):
+    """The second GEMM pass reads psi while other tiles already write H*psi, so
+    an in-place call (outvec sharing invec's memory) would silently give wrong
+    numbers; the entry point refuses it with TJ_ERR_ARG before any GPU work."""
+    import torch
+    from grand_sql_tj_b200.lib import lib
+    L = lib()
+    L.tj_model_wave_noalloc.argtypes = [C.c_void_p] * 7 + [C.c_void_p]
+    sb = synth.workload("tiny", seed=5)
+    keep = []
+    ps, pe = sb.sys.pack(), sb.env.pack()
+    bs, be = sb.sys_bs.pack(), sb.env_bs.pack()
+    dsys, denv = _dev_model(ps, keep), _dev_model(pe, keep)
+    x = torch.from_numpy(np.concatenate([sb.wave.data, sb.wave.data])).cuda()
+    torch.cuda.synchronize()
+    w = sb.wave.c
+    base = x.data_ptr()
+    for shift in (0, 8 * max(w.dim // 2, 1)):   # same buffer, and a partial overlap
+        win = TjWave(w.sys_len, w.env_len, w.num, 0, w.dim, w.sub, C.cast(C.c_void_p(base), c_double_p))
+        wout = TjWave(w.sys_len, w.env_len, w.num, 0, w.dim, w.sub, C.cast(C.c_void_p(base + shift), c_double_p))
+        rc = L.tj_model_wave_noalloc(C.addressof(sb.lat.c), C.addressof(dsys), C.addressof(denv),
+                                     C.addressof(bs.c), C.addressof(be.c), C.addressof(win),
+                                     C.addressof(wout), None)
+        assert rc == 1, (shift, rc)
+        assert "overlap" in L.tj_last_error().decode()
