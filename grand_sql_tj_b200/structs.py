@@ -84,6 +84,12 @@ class TjTruncResult(C.Structure):
                 ("entropys", C.c_double), ("sub", C.POINTER(TjBlockSub)), ("data", c_double_p)]
 
 
+class TjModelResult(C.Structure):
+    _fields_ = [("len", C.c_int32), ("nsub", C.c_int32), ("n_subs", C.c_int32), ("pad_", C.c_int32),
+                ("data_len", C.c_int64), ("sets", C.POINTER(TjBlockSet)), ("subs", C.POINTER(TjBlockSub)),
+                ("data", c_double_p), ("model", TjModel)]
+
+
 class TjHpsiStats(C.Structure):
     _fields_ = [("flops", C.c_double), ("flops_ref", C.c_double), ("bytes", C.c_double),
                 ("n_products", C.c_int64), ("n_tasks", C.c_int64), ("n_tiles_p1", C.c_int64),
@@ -322,6 +328,44 @@ def block_transfer_trans(b: Block) -> Block:
     subs = [SubBlock(s.num_up + b.up_dif, s.num_down + s.down_dif, -s.down_dif, np.asfortranarray(s.mat.T))
             for s in b.subs]
     return Block(b.len, -b.up_dif, b.down_dif, subs)
+
+
+def call_model_result(call):
+    """Runs a two-call model-result entry point `call(res_ptr) -> rc` and
+    returns the new Model (copied out of the result arrays)."""
+    res = TjModelResult()
+    rc = call(C.byref(res))
+    if rc:
+        return rc, None
+    sets = (TjBlockSet * max(res.nsub, 1))()
+    subs = (TjBlockSub * max(res.n_subs, 1))()
+    data = np.zeros(max(res.data_len, 1))
+    res.sets = C.cast(sets, C.POINTER(TjBlockSet))
+    res.subs = C.cast(subs, C.POINTER(TjBlockSub))
+    res.data = data.ctypes.data_as(c_double_p)
+    rc = call(C.byref(res))
+    if rc:
+        return rc, None
+    return 0, model_from_c(res.model, data)
+
+
+def _block_from_c(b: TjBlock, data: np.ndarray) -> Block:
+    subs = []
+    for i in range(b.num):
+        s = b.sub[i]
+        n = s.row_dim * s.sdim
+        subs.append(SubBlock(s.num_up, s.num_down, s.down_dif,
+                             data[s.off:s.off + n].reshape((s.row_dim, s.sdim), order="F").copy()))
+    return Block(b.len, b.up_dif, b.down_dif, subs)
+
+
+def model_from_c(m: TjModel, data: np.ndarray) -> Model:
+    """A tj_model whose blocks all point into `data` -> a numpy-side Model."""
+    sets = []
+    for i in range(m.nsub):
+        bs = m.sub[i]
+        sets.append(BlockSet(*[_block_from_c(getattr(bs, k), data) for k in OPS]))
+    return Model(m.len, _block_from_c(m.ham, data), sets)
 
 
 def block_from_c_result(res: TjTruncResult, length: int) -> Block:

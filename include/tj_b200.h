@@ -220,6 +220,50 @@ int tj_sys_site_env_site_cor_ndia(tj_ctx *ctx, const tj_block *sys_st, const tj_
                                   const tj_basis *sys_bs, const tj_basis *env_bs,
                                   const tj_wave *wave, char flag, double *value); /* :5709-5924 */
 
+/* ------------------------------------------------ operator renormalisation */
+
+/* A block model written by the library: Total_Model (code/tjsq/common.f90:
+ * 144-149) with ham and sub(1:nsub).  Two-call pattern, as tj_trunc_result:
+ * with sets, subs or data NULL only the sizes are filled; then the caller
+ * allocates sets[nsub], subs[n_subs] and data[data_len] and calls again, and
+ * `model` is filled with blocks that point into those arrays (every block's
+ * data pointer is `data`; its sub-blocks' offsets are counted from there).
+ * Sub-block records follow the order ham, then sets 1..nsub, each set in the
+ * order elec_up, elec_down, spin_sd, spin_sz, num_sn; a block's records are
+ * in the order the reference's update_trun_dia / update_trun_ndia create
+ * them (code/tjsq/block.f90:1311-1503), their matrices back to back. */
+typedef struct tj_model_result {
+  int32_t len, nsub;            /* new block length, operator sets nleg11(len)          */
+  int32_t n_subs, pad_;         /* sub-block records of ham and every operator           */
+  int64_t data_len;             /* doubles of all their matrices                         */
+  tj_block_set *sets;           /* caller-allocated, nsub entries (or NULL)              */
+  tj_block_sub *subs;           /* caller-allocated, n_subs entries (or NULL)            */
+  double *data;                 /* caller-allocated, data_len doubles (or NULL)          */
+  tj_model model;               /* second call: the new model                            */
+} tj_model_result;
+
+/* Get_Hamiltonian_Sys(pre,next,basis,trun)  (code/tjsq/get_sys.f90:4-239)
+ * for side = 0, Get_Hamiltonian_Env  (code/tjsq/get_sys.f90:245-480) for
+ * side = 1: the block `pre` (length L) is enlarged by one site into the
+ * basis `basis` (Get_basis of pre, length L + 1) -- its Hamiltonian with the
+ * new bonds (update_block_dia, Get_hamiltonian_ndia, Get_hamiltonian_dia,
+ * the site's chemical potential) and the operator sets of the sites that
+ * still have bonds outside the block (update_block_ndia_sys/env,
+ * update_site_ndia_sys/env, update_block_dia, update_site_dia;
+ * code/tjsq/block.f90:382-1306), reordered as the reference reorders them
+ * -- and every operator is truncated with `trun`: U^T O U per sector pair
+ * (update_trun_dia / update_trun_ndia, code/tjsq/block.f90:1311-1503).  trun
+ * is the truncation operator of tj_truncation (sub-block (num_up, num_down),
+ * row_dim = the sector's dimension in `basis`, sdim = kept states); the
+ * reference's untruncated steps pass the identity (block_transfer_basis with
+ * unit matrices, code/tjsq/dmrg_sub.f90:659-667, 678-686).  mshift is the reference's global
+ * of the same name, read by the environment side only (the superblock's
+ * system-block length + 1).  The new model (length L + 1, spin_sz left
+ * empty as in the reference, whose loop over operator kinds skips it) is
+ * returned through `out`. */
+int tj_get_hamiltonian(tj_ctx *ctx, const tj_lattice *lat, int side, int mshift, const tj_model *pre,
+                       const tj_basis *basis, const tj_block *trun, tj_model_result *out);
+
 /* --------------------------------------------------- measurement support */
 
 /* Statistics of the H*psi task list compiled for the last tj_model_wave /

@@ -14,8 +14,8 @@ import subprocess
 
 import numpy as np
 
-from grand_sql_tj_b200.structs import (TjBasis, TjBlock, TjLattice, TjModel, TjTruncResult,
-                                       TjWave, TjBlockSub, Block, block_from_c_result)
+from grand_sql_tj_b200.structs import (TjBasis, TjBlock, TjLattice, TjModel, TjModelResult, TjTruncResult,
+                                       TjWave, TjBlockSub, Block, block_from_c_result, call_model_result)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle_tj.so")
@@ -71,6 +71,8 @@ def lib(threads: int = 1):
         for n in ("ora_sys_block_site_cor_ndia", "ora_env_block_site_cor_ndia"):
             getattr(L, n).argtypes = [P(TjBlock), P(TjBlock), P(TjBasis), P(TjWave), C.c_char,
                                       P(C.c_double)]
+        L.ora_get_hamiltonian.argtypes = [P(TjLattice), C.c_int, C.c_int, P(TjModel), P(TjBasis), P(TjBlock),
+                                          P(TjModelResult)]
         L.ora_site_operator.argtypes = [C.c_int, C.c_int, P(TjBlock), P(TjBlockSub), P(C.c_double)]
         rc = L.ora_init(openblas_path().encode(), threads)
         if rc:
@@ -171,3 +173,41 @@ def correlator(name: str, a, b, sys_bs, env_bs, wave, flag: str = "B") -> float:
     else:
         _chk(fn(C.byref(pa.c), C.byref(pb.c), C.byref(ps.c), C.byref(pe.c), C.byref(wave.c), f, C.byref(v)))
     return v.value
+
+
+def get_hamiltonian(lat, side: int, mshift: int, pre, basis, trun):
+    """Get_Hamiltonian_Sys (side 0) / Get_Hamiltonian_Env (side 1): the block
+    `pre` enlarged into `basis` and truncated with the Block `trun`; returns the
+    new Model."""
+    L = lib()
+    pp, pb, pt = pre.pack(), basis.pack(), trun.pack()
+    rc, m = call_model_result(lambda r: L.ora_get_hamiltonian(C.byref(lat.c), side, mshift, C.byref(pp.c),
+                                                              C.byref(pb.c), C.byref(pt.c), r))
+    _chk(rc)
+    return m
+
+
+def lanczos_parts(lat, sys, env, sys_bs, env_bs, wave, lanzero: float):
+    """lanczos_memo_new on explicit models and bases; `wave` is the start vector (copied)."""
+    L = lib()
+    w = wave.copy()
+    ps, pe = sys.pack(), env.pack()
+    bs, be = sys_bs.pack(), env_bs.pack()
+    e, it = C.c_double(), C.c_int()
+    _chk(L.ora_lanczos(C.byref(lat.c), C.byref(ps.c), C.byref(pe.c), C.byref(bs.c), C.byref(be.c),
+                       C.byref(w.c), lanzero, C.byref(e), C.byref(it)))
+    return e.value, it.value, w
+
+
+class OracleBackend:
+    """The hot-path calls of grand_sql_tj_b200.sweep.Dmrg on the oracle (CPU)."""
+
+    def lanczos(self, lat, sys, env, sys_bs, env_bs, wave, lanzero):
+        return lanczos_parts(lat, sys, env, sys_bs, env_bs, wave, lanzero)
+
+    def truncation(self, wave, side, kept_min, kept_max, trun_err):
+        r, trun, _ = truncation(wave, side, kept_min, kept_max, trun_err)
+        return r, trun
+
+    def get_hamiltonian(self, lat, side, mshift, pre, basis, trun):
+        return get_hamiltonian(lat, side, mshift, pre, basis, trun)

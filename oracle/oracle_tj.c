@@ -2058,3 +2058,459 @@ int ora_sys_site_env_site_cor_ndia(const tj_block *stb, const tj_block *st2b, co
   *value = v;
   return 0;
 }
+
+/* ============================================ operator renormalisation */
+/* Get_Hamiltonian_Sys / Get_Hamiltonian_Env (get_sys.f90:4-480) with the
+ * block-update routines they call (block.f90:382-1503).  Every routine builds
+ * its new block as a dense sub-block per sector (pair), as the reference
+ * does, and the truncation is the reference's pair of DGEMMs per sub-block. */
+
+static OSub *osub_alloc(int n) { return (OSub *)calloc(n > 0 ? n : 1, sizeof(OSub)); }
+static double *mat_zero(int r, int c) { return (double *)calloc((size_t)r * c + 1, sizeof(double)); }
+static void blk_new(OBlk *o, int len, int num, int up_dif, int down_dif) {
+  memset(o, 0, sizeof *o);
+  o->len = len; o->num = num; o->up_dif = up_dif; o->down_dif = down_dif;
+  o->sub = osub_alloc(num);
+  o->owns = 1;
+}
+/* block_transfer (block.f90:1708-1735): a deep copy */
+static void blk_copy(const OBlk *in, OBlk *out) {
+  blk_new(out, in->len, in->num, in->up_dif, in->down_dif);
+  out->dim = in->dim;
+  for (int i = 0; i < in->num; i++) {
+    out->sub[i] = in->sub[i];
+    size_t n = (size_t)in->sub[i].row_dim * in->sub[i].sdim;
+    out->sub[i].mat = (double *)malloc((n + 1) * sizeof(double));
+    memcpy(out->sub[i].mat, in->sub[i].mat, n * sizeof(double));
+  }
+}
+/* mat(r0.., c0..) += a * src(0.., 0..) over nr x nc (src leading dimension lds) */
+static void mat_axpy(double *m, int ldm, int r0, int c0, double a, const double *src, int lds, int nr, int nc) {
+  for (int c = 0; c < nc; c++)
+    for (int r = 0; r < nr; r++) m[(size_t)(c0 + c) * ldm + r0 + r] += a * src[(size_t)c * lds + r];
+}
+
+/* update_block_dia (block.f90:382-433) */
+static void upd_block_dia(const OBlk *blk, const tj_basis *bs, OBlk *nb) {
+  blk_new(nb, bs->len, bs->num, 0, 0);
+  nb->dim = bs->dim;
+  for (int i = 0; i < bs->num; i++) {
+    int d = bs->sub[i].dim;
+    nb->sub[i] = (OSub){bs->sub[i].new_num_up, bs->sub[i].new_num_down, 0, d, d, mat_zero(d, d)};
+  }
+  for (int k = 0; k < nb->num; k++)
+    for (int x = 0; x < bs->sub[k].num; x++) {
+      const tj_basis_sub *m = BM(bs, k, x);
+      for (int i = 0; i < blk->num; i++) {
+        if (blk->sub[i].num_up != m->bl_num_up || blk->sub[i].num_down != m->bl_num_down) continue;
+        double c1 = sqrt((1.0 + nb->sub[k].num_down) / (1.0 + blk->sub[i].num_down));
+        mat_axpy(nb->sub[k].mat, nb->sub[k].row_dim, m->spos, m->spos, c1, blk->sub[i].mat, blk->sub[i].row_dim,
+                 m->sdim, m->sdim);
+        break;
+      }
+    }
+}
+/* update_site_dia (block.f90:439-494) */
+static void upd_site_dia(const OBlk *site, const tj_basis *bs, OBlk *nb) {
+  blk_new(nb, bs->len, bs->num, 0, 0);
+  nb->dim = bs->dim;
+  for (int i = 0; i < bs->num; i++) {
+    int d = bs->sub[i].dim;
+    nb->sub[i] = (OSub){bs->sub[i].new_num_up, bs->sub[i].new_num_down, 0, d, d, mat_zero(d, d)};
+  }
+  for (int k = 0; k < nb->num; k++)
+    for (int x = 0; x < bs->sub[k].num; x++) {
+      const tj_basis_sub *m = BM(bs, k, x);
+      for (int i = 0; i < site->num; i++) {
+        if (site->sub[i].num_up != m->st_num_up || site->sub[i].num_down != m->st_num_down) continue;
+        double c1 = sqrt((1.0 + nb->sub[k].num_down) / (1.0 + site->sub[i].num_down));
+        double v = site->sub[i].mat[0] * c1;
+        for (int y = 0; y < m->sdim; y++) nb->sub[k].mat[(size_t)(m->spos + y) * nb->sub[k].row_dim + m->spos + y] += v;
+        break;
+      }
+    }
+}
+/* The sub-block structure shared by update_block_ndia_sys/env and
+ * update_site_ndia_sys/env (steps <1>-<2>): one sub-block per basis sector x
+ * and spin transfer down_dif in -d..d (step su = 2) whose target sector
+ * exists, in that loop order. */
+static void ndia_structure(const tj_basis *bs, int len, int up_dif, int d1, OBlk *nb) {
+  int num = 0;
+  for (int x = 0; x < bs->num; x++)
+    for (int dd = -d1; dd <= d1; dd += 2)
+      if (find_bs(bs, bs->sub[x].new_num_up + up_dif, bs->sub[x].new_num_down + dd) >= 0) num++;
+  blk_new(nb, len, num, up_dif, d1);
+  int id = 0;
+  for (int x = 0; x < bs->num; x++)
+    for (int dd = -d1; dd <= d1; dd += 2) {
+      int y = find_bs(bs, bs->sub[x].new_num_up + up_dif, bs->sub[x].new_num_down + dd);
+      if (y < 0) continue;
+      int ld = bs->sub[y].dim, rd = bs->sub[x].dim;
+      nb->dim += rd;
+      nb->sub[id++] = (OSub){bs->sub[x].new_num_up, bs->sub[x].new_num_down, dd, ld, rd, mat_zero(ld, rd)};
+    }
+}
+/* update_block_ndia_sys (block.f90:497-690), env_side = 0, and
+ * update_block_ndia_env (block.f90:695-881), env_side = 1 (fermion sign
+ * from the parity of the site's 2S) */
+static void upd_block_ndia(const OBlk *blk, const tj_basis *bs, OBlk *nb, int env_side, char flag) {
+  const int up_dif = blk->up_dif, d1 = blk->down_dif;
+  ndia_structure(bs, bs->len, up_dif, d1, nb);
+  for (int i = 0; i < nb->num; i++) {
+    int rnu = nb->sub[i].num_up, rnd = nb->sub[i].num_down, dd = nb->sub[i].down_dif;
+    int rid = find_bs(bs, rnu, rnd), lid = find_bs(bs, rnu + up_dif, rnd + dd);
+    if (rid < 0 || lid < 0) continue;
+    int lnd = rnd + dd;
+    for (int x = 0; x < bs->sub[rid].num; x++) {
+      const tj_basis_sub *m = BM(bs, rid, x);
+      for (int sdd = -d1; sdd <= d1; sdd += 2) {
+        int bid = find_sub(blk, m->bl_num_up, m->bl_num_down, sdd, 1);
+        if (bid < 0) continue;
+        int lsnu = m->bl_num_up + up_dif, lsnd = m->bl_num_down + sdd;
+        const tj_basis_sub *ml = NULL;
+        for (int y = 0; y < bs->sub[lid].num; y++) {
+          const tj_basis_sub *q = BM(bs, lid, y);
+          if (q->bl_num_up == lsnu && q->bl_num_down == lsnd && q->st_num_down == m->st_num_down) {
+            ml = q;
+            break;
+          }
+        }
+        if (!ml) continue;
+        double signs = 1.0;
+        if (env_side) signs = sgn_flag(flag, m->st_num_down);
+        int j1 = lnd, j2 = d1, j3 = rnd, j4 = m->bl_num_down, j5 = m->st_num_down, j6 = lsnd;
+        double coef = W6(j1, j2, j3, j4, j5, j6) * sqrt((1.0 + j1) * (1.0 + j3)) * ipow_m1((j6 + j5 + j3 + j2) / 2);
+        if (coef == 0.0) continue;
+        coef *= signs;
+        mat_axpy(nb->sub[i].mat, nb->sub[i].row_dim, ml->spos, m->spos, coef, blk->sub[bid].mat, blk->sub[bid].row_dim,
+                 ml->sdim, m->sdim);
+      }
+    }
+  }
+}
+/* update_site_ndia_sys (block.f90:888-1105), env_side = 0 (fermion sign from
+ * the parity of the block's 2S), and update_site_ndia_env (block.f90:1107-
+ * 1306), env_side = 1 (no sign) */
+static void upd_site_ndia(const OBlk *site, const tj_basis *bs, OBlk *nb, int env_side, char flag) {
+  const int up_dif = site->up_dif, d1 = site->down_dif;
+  ndia_structure(bs, bs->len, up_dif, d1, nb);
+  for (int i = 0; i < nb->num; i++) {
+    int rnu = nb->sub[i].num_up, rnd = nb->sub[i].num_down, dd = nb->sub[i].down_dif;
+    int rid = find_bs(bs, rnu, rnd), lid = find_bs(bs, rnu + up_dif, rnd + dd);
+    if (rid < 0 || lid < 0) continue;
+    int lnd = rnd + dd;
+    for (int x = 0; x < bs->sub[rid].num; x++) {
+      const tj_basis_sub *m = BM(bs, rid, x);
+      for (int sdd = -d1; sdd <= d1; sdd += 2) {
+        int sid = find_sub(site, m->st_num_up, m->st_num_down, sdd, 1);
+        if (sid < 0) continue;
+        int lsnu = m->st_num_up + up_dif, lsnd = m->st_num_down + sdd;
+        const tj_basis_sub *ml = NULL;
+        for (int y = 0; y < bs->sub[lid].num; y++) {
+          const tj_basis_sub *q = BM(bs, lid, y);
+          if (q->st_num_up == lsnu && q->st_num_down == lsnd && q->bl_num_down == m->bl_num_down) {
+            ml = q;
+            break;
+          }
+        }
+        if (!ml) continue;
+        double signs = env_side ? 1.0 : sgn_flag(flag, m->bl_num_down);
+        int j1 = lnd, j2 = d1, j3 = rnd, j4 = m->st_num_down, j5 = m->bl_num_down, j6 = lsnd;
+        double coef = W6(j1, j2, j3, j4, j5, j6) * ipow_m1((j5 + j4 + j1 + j2) / 2) * sqrt((1.0 + j1) * (1.0 + j3));
+        if (coef == 0.0) continue;
+        coef *= signs;
+        double v = coef * site->sub[sid].mat[0];
+        for (int y = 0; y < m->sdim; y++)
+          nb->sub[i].mat[(size_t)(m->spos + y) * nb->sub[i].row_dim + ml->spos + y] += v;
+      }
+    }
+  }
+}
+/* Get_hamiltonian_ndia (get_sys.f90:578-759): coef * [block x site^T + h.c.]
+ * added into the enlarged Hamiltonian; sys_side = 1 for Flags = 'S' */
+static void ham_ndia(const OBlk *blk, const OBlk *site, const tj_basis *bs, double coef, OBlk *ham, char flagsign,
+                     int sys_side) {
+  const int up_dif = blk->up_dif, d1 = blk->down_dif;
+  for (int i = 0; i < ham->num; i++) {
+    int rnu = ham->sub[i].num_up, rnd = ham->sub[i].num_down;
+    int rid = find_bs(bs, rnu, rnd), lid = find_bs(bs, rnu, rnd + ham->sub[i].down_dif);
+    if (rid < 0 || lid < 0) continue;
+    for (int x = 0; x < bs->sub[rid].num; x++) {
+      const tj_basis_sub *m = BM(bs, rid, x);
+      for (int sdd = -d1; sdd <= d1; sdd += 2) {
+        int bid = find_sub(blk, m->bl_num_up, m->bl_num_down, sdd, 1);
+        if (bid < 0) continue;
+        int lsnu = m->bl_num_up + up_dif, lsnd = m->bl_num_down + sdd;
+        for (int nsd = abs(m->st_num_down - site->down_dif); nsd <= m->st_num_down + site->down_dif; nsd += 2) {
+          int st_dd = m->st_num_down - nsd, nsu = m->st_num_up - site->up_dif;
+          int sid = find_sub(site, nsu, nsd, st_dd, 1);
+          const tj_basis_sub *ml = NULL;
+          for (int y = 0; y < bs->sub[lid].num; y++) {
+            const tj_basis_sub *q = BM(bs, lid, y);
+            if (q->bl_num_up == lsnu && q->bl_num_down == lsnd && q->st_num_down == nsd) {
+              ml = q;
+              break;
+            }
+          }
+          if (!ml || sid < 0) continue;
+          int j1 = lsnd, j2 = m->bl_num_down, j3 = d1, j4 = m->st_num_down, j5 = nsd, j6 = rnd;
+          double c1 = W6(j1, j2, j3, j4, j5, j6);
+          c1 = c1 * sqrt((1.0 + j6) / (1.0 + j3)) * ipow_m1((j2 + j5 + j3 + j6) / 2) * site->sub[sid].mat[0];
+          double sign = 1.0;
+          if (sys_side && flagsign == 'F') {
+            if (m->bl_num_up % 2 == 1) sign = -1.0;
+            if (m->bl_num_down % 2 == 1) sign = -1.0;
+          }
+          if (c1 == 0.0) continue;
+          c1 = c1 * coef * sign;
+          const OSub *b = &blk->sub[bid];
+          mat_axpy(ham->sub[i].mat, ham->sub[i].row_dim, ml->spos, m->spos, c1, b->mat, b->row_dim, ml->sdim, m->sdim);
+          if (site->down_dif == 1) {
+            for (int c = 0; c < ml->sdim; c++)
+              for (int r = 0; r < m->sdim; r++)
+                ham->sub[i].mat[(size_t)(ml->spos + c) * ham->sub[i].row_dim + m->spos + r] +=
+                    c1 * b->mat[(size_t)r * b->row_dim + c];
+          }
+        }
+      }
+    }
+  }
+}
+/* Get_hamiltonian_dia (get_sys.f90:507-565) with Flag1 = Flag2 = 'N' and no
+ * conjugate part, as Get_Hamiltonian_Sys/Env call it */
+static void ham_dia(const OBlk *o1, const OBlk *o2, double coef, OBlk *ham) {
+  for (int i = 0; i < ham->num; i++) {
+    int nu = ham->sub[i].num_up, nd = ham->sub[i].num_down, sd = ham->sub[i].sdim;
+    int a = find_sub(o1, nu, nd, 0, 0), b = find_sub(o2, nu, nd, 0, 0);
+    if (a < 0 || b < 0) continue;
+    double c1 = coef / sqrt(1.0 + nd);
+    dg('N', 'N', sd, sd, sd, c1, o1->sub[a].mat, sd, o2->sub[b].mat, sd, 1.0, ham->sub[i].mat, sd);
+  }
+}
+/* update_trun_dia (block.f90:1311-1362) */
+static void upd_trun_dia(const OBlk *ori, const OBlk *trun, OBlk *eff) {
+  blk_new(eff, ori->len, trun->num, ori->up_dif, ori->down_dif);
+  eff->dim = trun->dim;
+  for (int i = 0; i < trun->num; i++) {
+    int k = trun->sub[i].sdim;
+    eff->sub[i] = (OSub){trun->sub[i].num_up, trun->sub[i].num_down, 0, k, k, mat_zero(k, k)};
+  }
+  for (int i = 0; i < eff->num; i++) {
+    int ed = eff->sub[i].sdim;
+    int x = find_sub(ori, eff->sub[i].num_up, eff->sub[i].num_down, 0, 0);
+    if (x < 0) continue;
+    int od = ori->sub[x].row_dim;
+    double *mid = mat_zero(od, ed);
+    dg('N', 'N', od, ed, od, 1.0, ori->sub[x].mat, od, trun->sub[i].mat, od, 0.0, mid, od);
+    dg('T', 'N', ed, ed, od, 1.0, trun->sub[i].mat, od, mid, od, 0.0, eff->sub[i].mat, ed);
+    free(mid);
+  }
+}
+/* update_trun_ndia (block.f90:1365-1503) */
+static void upd_trun_ndia(const OBlk *ori, const OBlk *trun, OBlk *eff) {
+  const int up_dif = ori->up_dif, d1 = ori->down_dif;
+  int num = 0;
+  for (int x = 0; x < trun->num; x++)
+    for (int dd = -d1; dd <= d1; dd += 2)
+      if (find_sub(trun, trun->sub[x].num_up + up_dif, trun->sub[x].num_down + dd, 0, 0) >= 0) num++;
+  blk_new(eff, ori->len, num, up_dif, d1);
+  int id = 0;
+  for (int x = 0; x < trun->num; x++)
+    for (int dd = -d1; dd <= d1; dd += 2) {
+      int y = find_sub(trun, trun->sub[x].num_up + up_dif, trun->sub[x].num_down + dd, 0, 0);
+      if (y < 0) continue;
+      int ld = trun->sub[y].sdim, rd = trun->sub[x].sdim;
+      eff->dim += rd;
+      eff->sub[id++] = (OSub){trun->sub[x].num_up, trun->sub[x].num_down, dd, ld, rd, mat_zero(ld, rd)};
+    }
+  for (int i = 0; i < eff->num; i++) {
+    int rnu = eff->sub[i].num_up, rnd = eff->sub[i].num_down, dd = eff->sub[i].down_dif;
+    int rid = find_sub(trun, rnu, rnd, 0, 0), lid = find_sub(trun, rnu + up_dif, rnd + dd, 0, 0);
+    int oid = find_sub(ori, rnu, rnd, dd, 1);
+    if (rid < 0 || lid < 0 || oid < 0) continue;
+    int orow = ori->sub[oid].row_dim, ocol = ori->sub[oid].sdim;
+    int rd = trun->sub[rid].sdim, ld = trun->sub[lid].sdim;
+    double *mid = mat_zero(orow, rd);
+    dg('N', 'N', orow, rd, ocol, 1.0, ori->sub[oid].mat, orow, trun->sub[rid].mat, ocol, 0.0, mid, orow);
+    dg('T', 'N', ld, rd, orow, 1.0, trun->sub[lid].mat, orow, mid, orow, 0.0, eff->sub[i].mat, ld);
+    free(mid);
+  }
+}
+
+/* Writes a model into the two-call result (layout of tj_model_result). */
+static void put_block(const OBlk *b, tj_model_result *out, int *ns, int64_t *nd, tj_block *dst) {
+  const int write = out->sets && out->subs && out->data;
+  if (write) {
+    *dst = (tj_block){b->len, b->num, b->dim, b->up_dif, b->down_dif, 0, out->subs + *ns, out->data};
+  }
+  for (int i = 0; i < b->num; i++) {
+    const OSub *s = &b->sub[i];
+    const int64_t n = (int64_t)s->row_dim * s->sdim;
+    if (write) {
+      out->subs[*ns + i] = (tj_block_sub){s->num_up, s->num_down, s->down_dif, s->row_dim, s->sdim, 0, *nd};
+      memcpy(out->data + *nd, s->mat, (size_t)n * sizeof(double));
+    }
+    *nd += n;
+  }
+  *ns += b->num;
+}
+
+/* Get_Hamiltonian_Sys (get_sys.f90:4-239), side 0, and Get_Hamiltonian_Env
+ * (get_sys.f90:245-480), side 1. */
+int ora_get_hamiltonian(const tj_lattice *lat, int side, int mshift, const tj_model *prem, const tj_basis *basis,
+                        const tj_block *trunb, tj_model_result *out) {
+  if (!p_dgemm) return fail(TJ_ERR_ARG, "oracle not initialised (ora_init)");
+  if (!lat || !prem || !basis || !trunb || !out) return fail(TJ_ERR_ARG, "ora_get_hamiltonian: null argument");
+  Geo g;
+  memset(&g, 0, sizeof g);
+  g.L = lat;
+  g.ns1 = lat->num_site + 1;
+  const int neibt = lat->neibt, len0 = prem->len, env = side != 0;
+  SiteOps so;
+  site_ops_build(lat->up_bias, &so);
+  OModel pre;
+  model_view(prem, &pre, 0);
+  OBlk trun;
+  blk_view(trunb, &trun);
+  const int nl0 = NLEG11(&g, len0), nl1 = NLEG11(&g, len0 + 1);
+  const int nslot = (nl0 > nl1 ? nl0 : nl1) + 1;
+  OSet *next = (OSet *)calloc(nslot, sizeof(OSet));   /* next%sub(1:...) */
+  OSet *res = (OSet *)calloc(nl1 > 0 ? nl1 : 1, sizeof(OSet));
+  OBlk next_ham, tmp, tmp1, new_ham;
+  memset(&tmp, 0, sizeof tmp);
+  memset(&tmp1, 0, sizeof tmp1);
+  int rc = 0;
+  if (pre.nsub < nl0) {
+    rc = fail(TJ_ERR_ARG, "ora_get_hamiltonian: pre has fewer operator sets than nleg11(len)");
+    goto done;
+  }
+  upd_block_dia(&pre.ham, basis, &next_ham);
+  /* the new site J, the block site II it bonds to, and the coupling row */
+  for (int ij = 1; ij <= 5; ij += 2) {
+    const int J = env ? len0 + 1 + mshift : len0 + 1;
+    const int jl = env ? NPOSI_LAT(&g, J) : J;   /* lattice index of the new site */
+    for (int k = 1; k <= neibt; k++) {
+      int I = NEIB(&g, jl, k);
+      int II = env ? NPOSI_DM(&g, I) - mshift : I;
+      if (!(II <= len0 && II > 0)) continue;
+      int i1 = INB1(&g, II, len0);
+      if (!(i1 > 0 && i1 <= nl0)) continue;
+      double coefx = JT(&g, k, jl), coefsd = JD(&g, k, jl);
+      if (ij == 1 && coefx != 0.0)
+        ham_ndia(&pre.sub[i1 - 1].op[EU], &so.eu, basis, coefx, &next_ham, 'F', !env);
+      if (ij == 3 && coefsd != 0.0)
+        ham_ndia(&pre.sub[i1 - 1].op[SD], &so.sd, basis, coefsd, &next_ham, 'B', !env);
+    }
+    for (int y = 1; y <= len0; y++) {
+      int i1 = INB1(&g, y, len0);
+      if (i1 > nl0 || i1 < 1) continue;
+      OSet *p = &pre.sub[i1 - 1], *n = &next[i1];
+      if (ij == 1) {
+        blk_free(&n->op[EU]);
+        blk_free(&n->op[ED]);
+        upd_block_ndia(&p->op[EU], basis, &n->op[EU], env, 'F');
+        upd_block_ndia(&p->op[ED], basis, &n->op[ED], env, 'F');
+      } else if (ij == 3) {
+        blk_free(&n->op[SD]);
+        upd_block_ndia(&p->op[SD], basis, &n->op[SD], env, 'B');
+      } else {
+        blk_free(&n->op[SN]);
+        upd_block_dia(&p->op[SN], basis, &n->op[SN]);
+      }
+    }
+    blk_free(&tmp);
+    blk_free(&tmp1);
+    if (ij == 1) {
+      upd_site_ndia(&so.eu, basis, &tmp, env, 'F');
+      upd_site_ndia(&so.ed, basis, &tmp1, env, 'F');
+    } else if (ij == 3) {
+      upd_site_ndia(&so.sd, basis, &tmp, env, 'B');
+    } else {
+      upd_site_dia(&so.ne, basis, &tmp);
+    }
+    if (ij == 5) {
+      for (int k = 1; k <= neibt; k++) {
+        int I = NEIB(&g, jl, k);
+        int II = env ? NPOSI_DM(&g, I) - mshift : I;
+        if (!(II <= len0 && II > 0)) continue;
+        int i1 = INB1(&g, II, len0);
+        if (!(i1 > 0 && i1 <= nl0)) continue;
+        ham_dia(&next[i1].op[SN], &tmp, JN(&g, k), &next_ham);
+      }
+      if (ESITE(&g, jl) != 0.0) blk_add_two(&tmp, ESITE(&g, jl), &next_ham);
+    }
+    /* reorder: operators of the sites that keep bonds, then the new site */
+    const int kind[2] = {ij == 1 ? EU : ij == 3 ? SD : SN, ED};
+    const int nk = ij == 1 ? 2 : 1;
+    for (int I = 1; I <= len0; I++) {
+      int i1 = INB1(&g, I, len0), j = INB1(&g, I, len0 + 1);
+      if (j <= nl1 && j != i1)
+        for (int q = 0; q < nk; q++) {
+          blk_free(&next[j].op[kind[q]]);
+          blk_copy(&next[i1].op[kind[q]], &next[j].op[kind[q]]);
+        }
+    }
+    {
+      int j = INB1(&g, len0 + 1, len0 + 1);
+      if (j < 1 || j >= nslot) {
+        rc = fail(TJ_ERR_ARG, "ora_get_hamiltonian: new site has no operator slot");
+        goto done;
+      }
+      blk_free(&next[j].op[kind[0]]);
+      blk_copy(&tmp, &next[j].op[kind[0]]);
+      if (ij == 1) {
+        blk_free(&next[j].op[ED]);
+        blk_copy(&tmp1, &next[j].op[ED]);
+      }
+    }
+    for (int ii = 1; ii <= nl1; ii++)
+      for (int q = 0; q < nk; q++) {
+        if (ij == 5)
+          upd_trun_dia(&next[ii].op[SN], &trun, &res[ii - 1].op[SN]);
+        else
+          upd_trun_ndia(&next[ii].op[kind[q]], &trun, &res[ii - 1].op[kind[q]]);
+      }
+  }
+  upd_trun_dia(&next_ham, &trun, &new_ham);
+  {
+    /* result: ham, then sets 1..nl1 (elec_up, elec_down, spin_sd, spin_sz (empty), num_sn) */
+    int ns = 0;
+    int64_t nd = 0;
+    tj_block tb;
+    put_block(&new_ham, out, &ns, &nd, &tb);
+    if (out->sets && out->subs && out->data) out->model.ham = tb;
+    for (int ii = 0; ii < nl1; ii++) {
+      OBlk empty;
+      blk_new(&empty, len0 + 1, 0, 0, 0);
+      const OBlk *ops[5] = {&res[ii].op[EU], &res[ii].op[ED], &res[ii].op[SD], &empty, &res[ii].op[SN]};
+      tj_block b5[5];
+      for (int q = 0; q < 5; q++) put_block(ops[q], out, &ns, &nd, &b5[q]);
+      if (out->sets && out->subs && out->data)
+        out->sets[ii] = (tj_block_set){b5[0], b5[1], b5[2], b5[3], b5[4]};
+      blk_free(&empty);
+    }
+    out->len = len0 + 1;
+    out->nsub = nl1;
+    out->n_subs = ns;
+    out->data_len = nd;
+    if (out->sets && out->subs && out->data) {
+      out->model.len = len0 + 1;
+      out->model.nsub = nl1;
+      out->model.sub = out->sets;
+    }
+  }
+  blk_free(&new_ham);
+done:
+  blk_free(&next_ham);
+  blk_free(&tmp);
+  blk_free(&tmp1);
+  for (int i = 0; i < nslot; i++)
+    for (int q = 0; q < 5; q++) blk_free(&next[i].op[q]);
+  for (int i = 0; i < (nl1 > 0 ? nl1 : 1); i++)
+    for (int q = 0; q < 5; q++) blk_free(&res[i].op[q]);
+  free(next);
+  free(res);
+  blk_free(&trun);
+  model_free(&pre);
+  return rc;
+}

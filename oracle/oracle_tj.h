@@ -69,6 +69,15 @@ int ora_sys_site_env_block_cor_ndia(const tj_block *st, const tj_block *b, const
 int ora_sys_site_env_site_cor_ndia(const tj_block *st, const tj_block *st2, const tj_basis *sbs,
                                    const tj_basis *ebs, const tj_wave *w, char flag, double *v);
 
+/* Get_Hamiltonian_Sys (side 0, code/tjsq/get_sys.f90:4-239) and
+ * Get_Hamiltonian_Env (side 1, get_sys.f90:245-480) with update_block_dia,
+ * update_site_dia, update_block_ndia_sys/env, update_site_ndia_sys/env,
+ * Get_hamiltonian_ndia, Get_hamiltonian_dia and update_trun_dia/ndia
+ * (block.f90:382-1503, get_sys.f90:507-759); same arguments and two-call
+ * result as tj_get_hamiltonian. */
+int ora_get_hamiltonian(const tj_lattice *lat, int side, int mshift, const tj_model *pre, const tj_basis *basis,
+                        const tj_block *trun, tj_model_result *out);
+
 /* Site operators of Get_site_operator_su2_U0 (code/tjsq/dmrg_sub.f90:370-473):
  * which = 0 st_elec_up, 1 st_elec_down, 2 num_elec, 3 st_sd, 4 st_si.
  * Writes at most 2 sub-blocks and 2 doubles; returns the sub count. */
