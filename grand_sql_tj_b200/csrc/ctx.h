@@ -6,6 +6,7 @@
 
 #include <chrono>
 #include <memory>
+#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -31,6 +32,12 @@ struct DevBuf {
 };
 
 }  // namespace tjb
+
+// compiled operator renormalisation of the last tj_get_hamiltonian call (renorm.cpp)
+struct tj_renorm_state;
+namespace tjb {
+std::shared_ptr<tj_renorm_state> new_renorm_state();
+}
 
 struct tj_ctx {
   int device = 0;
@@ -61,6 +68,9 @@ struct tj_ctx {
   tjb::DevBuf trA, trB, trC, trD, trE;          // truncation
   tjb::DevBuf corCells, corTasks, corTiles, corOps, corScr, corPsi;   // correlators
   tjb::DevBuf ggPool, ggOut, ggTab, ggSlots;                          // grouped block-GEMM benchmark
+  tjb::DevBuf rnOps, rnTrun, rnScr, rnOut, rnSlots, rnTab;             // operator renormalisation
+  tjb::DevBuf wtOps, wtOld, wtNew, wtScr, wtSlots, wtTab;              // wavefunction prediction
+  std::shared_ptr<tj_renorm_state> renorm;
   // split-precision H*psi
   std::unique_ptr<tjb::OzPlan> oz;
   tjb::DevBuf ozPack, ozScales, ozStaJobs, ozPsiJobs, ozProdJobs, ozSegs, ozFams, ozCells, ozProdRows, ozStackRows, ozItems1,
@@ -70,7 +80,8 @@ struct tj_ctx {
     return {&ops, &scr, &vin, &vout, &counters, &partials, &cells1, &cells2, &tasks1, &tasks2, &tiles1,
             &tiles2, &red1, &red2, &slots, &m_dst, &m_n, &m_sb, &m_se, &m_src, &m_coef, &lanV, &lanScal, &lanPart, &trA, &trB,
             &trC, &trD, &trE, &corCells, &corTasks, &corTiles, &corOps, &corScr, &corPsi, &ggPool, &ggOut, &ggTab,
-            &ggSlots, &ozPack, &ozScales,
+            &ggSlots, &rnOps, &rnTrun, &rnScr, &rnOut, &rnSlots, &rnTab, &wtOps, &wtOld, &wtNew, &wtScr,
+            &wtSlots, &wtTab, &ozPack, &ozScales,
             &ozStaJobs, &ozPsiJobs, &ozProdJobs, &ozSegs, &ozFams, &ozCells, &ozProdRows, &ozStackRows, &ozItems1, &ozItems2,
             &ozCta1, &ozCta2, &ozStaSpans, &ozPsiSpans, &ozProdSpans, &ozStaMSpans,
             &ozPsiMSpans, &ozProdMSpans, &ozStaMJobs, &ozPsiMJobs, &ozProdMJobs, &ozMisc};

@@ -1815,7 +1815,7 @@ static_assert(sizeof(Reduce) == sizeof(tj_plan_reduce), "reduce layout");
 
 }  // namespace tjb
 
-static int export_plan(tjb::HpsiPlan &P, tj_plan_export *out) {
+int tjb::export_hpsi_plan(const tjb::HpsiPlan &P, tj_plan_export *out) {
   out->ops_len = P.ops_len;
   out->scratch_len = P.scratch_len;
   out->psi_len = P.psi_len;
@@ -1857,7 +1857,7 @@ extern "C" int tj_hpsi_plan_export(const tj_lattice *lat, const tj_model *sys, c
   std::string msg;
   int rc = tjb::build_hpsi_plan(lat, sys, env, sys_bs, env_bs, wave, P, msg);
   if (rc) return tjb_set_err(rc, "H*psi plan: " + msg);
-  return export_plan(P, out);
+  return tjb::export_hpsi_plan(P, out);
 }
 
 extern "C" int tj_cor_plan_export(int kind, const tj_block *a, const tj_block *b, const tj_basis *sys_bs,
@@ -1868,7 +1868,7 @@ extern "C" int tj_cor_plan_export(int kind, const tj_block *a, const tj_block *b
   std::string msg;
   int rc = tjb::build_cor_plan((tjb::CorKind)kind, a, b, sys_bs, env_bs, wave, flag, P, msg);
   if (rc) return tjb_set_err(rc, "correlator plan: " + msg);
-  return export_plan(P, out);
+  return tjb::export_hpsi_plan(P, out);
 }
 
 namespace tjb {

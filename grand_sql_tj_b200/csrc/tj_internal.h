@@ -141,4 +141,7 @@ int build_cor_plan(CorKind kind, const tj_block *a, const tj_block *b, const tj_
                    const tj_basis *env_bs, const tj_wave *wave, char flag, HpsiPlan &plan,
                    std::string &msg);
 
+// Copies a plan into the caller's arrays of tj_plan_export (two-call pattern).
+int export_hpsi_plan(const HpsiPlan &P, tj_plan_export *out);
+
 }  // namespace tjb

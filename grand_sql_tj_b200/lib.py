@@ -13,8 +13,9 @@ from typing import Optional, Tuple
 
 import numpy as np
 
-from .structs import (Block, TjBasis, TjBlock, TjBlockSub, TjGgCell, TjGgTerm, TjHpsiStats, TjLattice, TjModel,
-                      TjTruncResult, TjTuneResult, TjWave, Wave, block_from_c_result)
+from .structs import (Block, TjBasis, TjBlock, TjBlockSet, TjBlockSub, TjGgCell, TjGgTerm, TjHpsiStats, TjLattice,
+                      TjModel, TjModelResult, TjTruncResult, TjTuneResult, TjWave, Wave, block_from_c_result,
+                      call_model_result)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtjb200.so")
@@ -193,6 +194,14 @@ def lib():
                                          C.c_char, P(PlanExport)]
         L.tj_ozaki_plan_export.argtypes = [P(TjLattice), P(TjModel), P(TjModel), P(TjBasis), P(TjBasis),
                                            P(TjWave), C.c_int, P(OzExport)]
+        L.tj_get_hamiltonian.argtypes = [C.c_void_p, P(TjLattice), C.c_int, C.c_int, P(TjModel), P(TjBasis),
+                                         P(TjBlock), P(TjModelResult)]
+        L.tj_renorm_plan_export.argtypes = [P(TjLattice), C.c_int, C.c_int, P(TjModel), P(TjBasis), P(TjBlock),
+                                            P(PlanExport), P(TjModelResult)]
+        L.tj_wave_trans.argtypes = [C.c_void_p, C.c_int, P(TjBasis), P(TjBasis), P(TjBlock), P(TjBlock), P(TjWave),
+                                    P(TjWave)]
+        L.tj_wave_trans_plan_export.argtypes = [C.c_int, P(TjBasis), P(TjBasis), P(TjBlock), P(TjBlock), P(TjWave),
+                                                P(TjWave), P(PlanExport)]
         for n in ("tj_measure_sys_block", "tj_measure_env_block"):
             getattr(L, n).argtypes = [C.c_void_p, P(TjBlock), P(TjBasis), P(TjWave), P(C.c_double)]
         L.tj_sys_block_env_block_cor_dia.argtypes = [C.c_void_p, P(TjBlock), P(TjBlock), P(TjBasis),
@@ -319,6 +328,33 @@ class Context:
                                        C.byref(be.c), C.byref(w.c), 1, lanzero, e, C.byref(it)))
         return e[0], it.value, w
 
+    def lanczos(self, lat, sys, env, sys_bs, env_bs, wave: Wave, lanzero: float):
+        """lanczos_memo_new on explicit models and bases: returns (E0, iterations, Ritz vector)."""
+        w = wave.copy()
+        ps, pe, bs, be = sys.pack(), env.pack(), sys_bs.pack(), env_bs.pack()
+        e, it = (C.c_double * 1)(), C.c_int()
+        _chk(lib().tj_lanczos_memo_new(self.h, C.byref(lat.c), C.byref(ps.c), C.byref(pe.c), C.byref(bs.c),
+                                       C.byref(be.c), C.byref(w.c), 1, lanzero, e, C.byref(it)))
+        return e[0], it.value, w
+
+    def get_hamiltonian(self, lat, side: int, mshift: int, pre, basis, trun: Block):
+        """Get_Hamiltonian_Sys (side 0) / Get_Hamiltonian_Env (side 1) (get_sys.f90:4-480):
+        the Model `pre` enlarged into `basis` and truncated with `trun`; returns the new Model."""
+        pp, pb, pt = pre.pack(), basis.pack(), trun.pack()
+        rc, m = call_model_result(lambda r: lib().tj_get_hamiltonian(self.h, C.byref(lat.c), side, mshift,
+                                                                     C.byref(pp.c), C.byref(pb.c), C.byref(pt.c), r))
+        _chk(rc)
+        return m
+
+    def wave_trans(self, direction: int, sys_bs, env_bs, sys_trun: Block, env_trun: Block, old: Wave,
+                   new_wave: Wave) -> Wave:
+        """wave_trans_LR (direction 0) / wave_trans_RL (direction 1) (dmrg_sub.f90:1093-1384):
+        fills `new_wave` (the next superblock's sectors) and returns it."""
+        pb, pe, ps, pt = sys_bs.pack(), env_bs.pack(), sys_trun.pack(), env_trun.pack()
+        _chk(lib().tj_wave_trans(self.h, direction, C.byref(pb.c), C.byref(pe.c), C.byref(ps.c), C.byref(pt.c),
+                                 C.byref(old.c), C.byref(new_wave.c)))
+        return new_wave
+
     def truncation(self, wave: Wave, side: int, kept_min: int, kept_max: int, trun_err: float):
         """Get_density_matrix_{sys,env}_new + Get_truncation_operator (den_mat.f90)."""
         r = TjTruncResult()
@@ -380,6 +416,55 @@ def _export(call) -> dict:
         src = np.ctypeslib.as_array(C.cast(u.src, C.POINTER(C.c_double)), shape=(u.n,))
         ops[u.dst:u.dst + u.n] = src
     return {"ex": ex, "ops": ops, **arrs}
+
+
+def renorm_plan_export(lat, side: int, mshift: int, pre, basis, trun: Block) -> dict:
+    """Compiled task lists of tj_get_hamiltonian (no GPU needed), with the
+    result's records: {"ex", "ops", ..., "trun": trun data, "res": TjModelResult}."""
+    L = lib()
+    pp, pb, pt = pre.pack(), basis.pack(), trun.pack()
+    res = TjModelResult()
+    _chk(L.tj_renorm_plan_export(C.byref(lat.c), side, mshift, C.byref(pp.c), C.byref(pb.c), C.byref(pt.c),
+                                 C.byref(PlanExport()), C.byref(res)))
+    sets = (TjBlockSet * max(res.nsub, 1))()
+    subs = (TjBlockSub * max(res.n_subs, 1))()
+    dummy = np.zeros(1)
+    res.sets = C.cast(sets, C.POINTER(TjBlockSet))
+    res.subs = C.cast(subs, C.POINTER(TjBlockSub))
+    res.data = dummy.ctypes.data_as(C.POINTER(C.c_double))
+    d = _export(lambda ex: L.tj_renorm_plan_export(C.byref(lat.c), side, mshift, C.byref(pp.c), C.byref(pb.c),
+                                                    C.byref(pt.c), ex, C.byref(res)))
+    lo = min((pt.subs[i].off for i in range(len(trun.subs))), default=0)
+    d.update(trun=pt.data[lo:].copy(), res=res, res_arrays=(sets, subs, dummy))
+    return d
+
+
+def wave_trans_plan_export(direction: int, sys_bs, env_bs, sys_trun: Block, env_trun: Block, old: Wave,
+                           new_wave: Wave) -> dict:
+    """Compiled task lists of tj_wave_trans (no GPU needed)."""
+    L = lib()
+    pb, pe, ps, pt = sys_bs.pack(), env_bs.pack(), sys_trun.pack(), env_trun.pack()
+    return _export(lambda ex: L.tj_wave_trans_plan_export(direction, C.byref(pb.c), C.byref(pe.c), C.byref(ps.c),
+                                                           C.byref(pt.c), C.byref(old.c), C.byref(new_wave.c), ex))
+
+
+class DeviceBackend:
+    """The hot-path calls of grand_sql_tj_b200.sweep.Dmrg on the B200, through the C ABI."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def lanczos(self, lat, sys, env, sys_bs, env_bs, wave, lanzero):
+        return self.ctx.lanczos(lat, sys, env, sys_bs, env_bs, wave, lanzero)
+
+    def truncation(self, wave, side, kept_min, kept_max, trun_err):
+        return self.ctx.truncation(wave, side, kept_min, kept_max, trun_err)
+
+    def get_hamiltonian(self, lat, side, mshift, pre, basis, trun):
+        return self.ctx.get_hamiltonian(lat, side, mshift, pre, basis, trun)
+
+    def wave_trans(self, direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave):
+        return self.ctx.wave_trans(direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave)
 
 
 def pack_superblock(sb):

@@ -100,7 +100,9 @@ class TjHpsiStats(C.Structure):
                 ("flops_launch1", C.c_double), ("flops_launch2", C.c_double),
                 ("int8_ops_launch1", C.c_double), ("int8_ops_launch2", C.c_double),
                 ("prepare_ms", C.c_double), ("plan_ms", C.c_double), ("upload_ms", C.c_double),
-                ("ozplan_ms", C.c_double), ("lanczos_ms", C.c_double)]
+                ("ozplan_ms", C.c_double), ("lanczos_ms", C.c_double),
+                ("renorm_plan_ms", C.c_double), ("renorm_ms", C.c_double), ("renorm_e2e_ms", C.c_double),
+                ("renorm_flops", C.c_double)]
 
 
 class TjTuneResult(C.Structure):

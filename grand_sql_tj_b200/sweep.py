@@ -15,7 +15,7 @@ Every hot-path call goes through a backend object with the methods
   lanczos(lat, sys, env, sys_bs, env_bs, wave, lanzero) -> (E0, iters, wave)
   truncation(wave, side, kept_min, kept_max, trun_err) -> (info, trun Block)
   get_hamiltonian(lat, side, mshift, pre, basis, trun) -> Model
-  wave_trans(direction, sys_bs, env_bs, sys_trun, env_trun, old, new_sectors) -> Wave
+  wave_trans(direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave) -> new_wave
 
 `DeviceBackend` (grand_sql_tj_b200.lib) runs them on the B200 through the C
 ABI.
@@ -179,3 +179,129 @@ class Dmrg:
             self.records.append(r)
             label += 1
         return out
+
+    # ------------------------------------------------------------ sweeps
+    def _start_wave(self, secs, sys_len, env_len, restart: bool, direction: int, trans_args):
+        """The initial vector of a sweep's first step (dmrg_sub.f90:763-788 /
+        945-971): random for a fresh start, else the last step's vector, carried
+        to this superblock when its lengths differ."""
+        new = Wave(sys_len, env_len, secs)
+        if not restart or self.wave is None:
+            wave_initialize(new, self.rng)
+            return new
+        if self.wave.sys_len != sys_len:
+            return self.be.wave_trans(direction, *trans_args(), self.wave, new)
+        new.data[:new.dim] = self.wave.data[:self.wave.dim]
+        return new
+
+    def left_to_right(self, bg_id: int, end_id: int, restart: bool = True, lanzero: Optional[float] = None,
+                      trun_err: Optional[float] = None, phase: str = "L->R") -> List[StepRecord]:
+        """left_to_right (dmrg_sub.f90:729-907): the system block grows from
+        length bg_id to end_id - 1 + 1, each step truncated by its density
+        matrix, the wavefunction carried from step to step by wave_trans_LR."""
+        p, geo, N = self.p, self.geo, self.N
+        lanzero = p.lanzero if lanzero is None else lanzero
+        trun_err = p.trun_err if trun_err is None else trun_err
+        tot_up = p.n_elec if self.up_bias else 0
+        label = bg_id
+        sys = self.sysblocks[label]
+        env = self.envblocks[N - label - 2]
+        out = []
+        sys_trun = None
+        first = True
+        while first or label + 1 <= end_id:
+            t0 = time.perf_counter()
+            lat = geo.lattice(sys.len, env.len)
+            sys_bs = self._basis(sys)
+            env_bs = self._basis(env) if first else self.envbs[N - label - 1]
+            secs = get_super_basis(sys_bs, env_bs, tot_up, p.tot_num_down)
+            if first:
+                wave = self._start_wave(secs, sys_bs.len, env_bs.len, restart, 0,
+                                        lambda: (sys_bs, self.envbs[N - label], self.systruns[label],
+                                                 self.envtruns[N - label - 1]))
+            else:
+                wave = self.be.wave_trans(0, sys_bs, self.envbs[N - label], sys_trun, self.envtruns[N - label - 1],
+                                          self.wave, Wave(sys_bs.len, env_bs.len, secs))
+            tp = time.perf_counter()
+            e, it, wave = self._lanczos(lat, sys, env, sys_bs, env_bs, wave, lanzero)
+            t1 = time.perf_counter()
+            info, sys_trun = self.be.truncation(wave, 0, p.kept_min, p.kept_max, trun_err)
+            t2 = time.perf_counter()
+            sys = self.be.get_hamiltonian(lat, 0, 0, sys, sys_bs, sys_trun)
+            t3 = time.perf_counter()
+            self.sysblocks[label + 1], self.systruns[label + 1], self.sysbs[label + 1] = sys, sys_trun, sys_bs
+            self.wave = wave
+            r = StepRecord(phase, sys_bs.len - 1, env_bs.len - 1, e, it, wave.dim, float(info.trunc_err),
+                           int(info.num_state), t3 - t0, t1 - tp, t2 - t1, t3 - t2, tp - t0)
+            out.append(r)
+            self.records.append(r)
+            label += 1
+            first = False
+            if label + 1 <= end_id:
+                env = self.envblocks[N - label - 2]
+        return out
+
+    def right_to_left(self, bg_id: int, end_id: int, restart: bool = True, lanzero: Optional[float] = None,
+                      trun_err: Optional[float] = None, phase: str = "R->L") -> List[StepRecord]:
+        """right_to_left (dmrg_sub.f90:911-1087): the environment block grows
+        while the system block shrinks from length bg_id - 1 to end_id - 1,
+        the wavefunction carried by wave_trans_RL."""
+        p, geo, N = self.p, self.geo, self.N
+        lanzero = p.lanzero if lanzero is None else lanzero
+        trun_err = p.trun_err if trun_err is None else trun_err
+        tot_up = p.n_elec if self.up_bias else 0
+        label = bg_id
+        sys = self.sysblocks[label - 1]
+        env = self.envblocks[N - label - 1]
+        out = []
+        env_trun = None
+        first = True
+        while first or label - 1 >= end_id:
+            t0 = time.perf_counter()
+            lat = geo.lattice(sys.len, env.len)
+            sys_bs = self._basis(sys) if first else self.sysbs[label]
+            env_bs = self._basis(env)
+            secs = get_super_basis(sys_bs, env_bs, tot_up, p.tot_num_down)
+            if first:
+                wave = self._start_wave(secs, sys_bs.len, env_bs.len, restart, 1,
+                                        lambda: (self.sysbs[label + 1], env_bs, self.systruns[label],
+                                                 self.envtruns[N - label - 1]))
+            else:
+                wave = self.be.wave_trans(1, self.sysbs[label + 1], env_bs, self.systruns[label], env_trun,
+                                          self.wave, Wave(sys_bs.len, env_bs.len, secs))
+            tp = time.perf_counter()
+            e, it, wave = self._lanczos(lat, sys, env, sys_bs, env_bs, wave, lanzero)
+            t1 = time.perf_counter()
+            info, env_trun = self.be.truncation(wave, 1, p.kept_min, p.kept_max, trun_err)
+            t2 = time.perf_counter()
+            env = self.be.get_hamiltonian(lat, 1, sys.len + 1, env, env_bs, env_trun)
+            t3 = time.perf_counter()
+            self.envblocks[N - label], self.envtruns[N - label], self.envbs[N - label] = env, env_trun, env_bs
+            self.wave = wave
+            r = StepRecord(phase, sys_bs.len - 1, env_bs.len - 1, e, it, wave.dim, float(info.trunc_err),
+                           int(info.num_state), t3 - t0, t1 - tp, t2 - t1, t3 - t2, tp - t0)
+            out.append(r)
+            self.records.append(r)
+            label -= 1
+            first = False
+            if label - 1 >= end_id:
+                sys = self.sysblocks[label - 1]
+        return out
+
+    def ground_state(self, sweeps: int, final_half: bool = False) -> List[StepRecord]:
+        """Get_Ground_State (main.f90:96-187) for a fresh start: warm-up to
+        half the lattice, a left-to-right half-sweep from a random vector, a
+        right-to-left half-sweep, then `sweeps` full sweeps (left to right and
+        back) at the sweep thresholds; kept_max and the thresholds as given in
+        the parameters (the reference's kept-state schedule is left to the
+        caller)."""
+        N = self.N
+        self.warm_up()
+        self.left_to_right(N // 2 - 1, N - 2, restart=False, phase="L->R0")
+        self.right_to_left(N - 2, 1, restart=True, phase="R->L0")
+        for s in range(sweeps):
+            self.left_to_right(1, N - 2, restart=True, phase="L->R%d" % (s + 1))
+            self.right_to_left(N - 2, 1, restart=True, phase="R->L%d" % (s + 1))
+        if final_half:
+            self.left_to_right(1, N // 2 + 3, restart=True, phase="final")
+        return self.records

@@ -231,3 +231,41 @@ def workload(name: str, seed: int = 1234) -> Superblock:
     if name == "cyl6x24_m6000":   # 6x24 cylinder, t'=-0.2, 18 holes, m=6000
         return make_superblock(24, 6, 71, 71, 6000, 126, seed, t2=-0.2)
     raise KeyError(name)
+
+
+@dataclass
+class RenormCase:
+    """Inputs of one operator renormalisation (Get_Hamiltonian_Sys/Env)."""
+    lat: Lattice
+    side: int
+    mshift: int
+    pre: Model
+    basis: Basis
+    trun: Block
+
+
+def random_trun(basis: Basis, kept: int, rng) -> Block:
+    """A truncation operator keeping about `kept` states of `basis`: per sector
+    a column-orthonormal matrix (row_dim = the sector's dimension) with the
+    sector's share of the kept states (at least one)."""
+    subs = []
+    for m in basis.maps:
+        k = max(1, min(m.dim, int(round(kept * m.dim / basis.dim))))
+        q, _ = np.linalg.qr(rng.standard_normal((m.dim, k)))
+        subs.append(SubBlock(m.new_num_up, m.new_num_down, 0, np.asfortranarray(q)))
+    return Block(basis.len, 0, 0, subs)
+
+
+def renorm_case(name: str, side: int = 0, seed: int = 1234) -> RenormCase:
+    """The renormalisation of the system (side 0) or environment (side 1)
+    block of a named superblock: the block is enlarged by its centre site and
+    truncated back to about m states."""
+    sb = workload(name, seed=seed)
+    rng = np.random.default_rng(seed + 17)
+    ms = {"tiny": 6, "small": 24, "small_gc": 24, "cyl4": 64, "ladder16_m256": 256, "cyl4x24_m2000": 2000,
+          "cyl4x24_m500": 500, "cyl6x24_m6000": 6000}[name]
+    pre = sb.sys if side == 0 else sb.env
+    basis = sb.sys_bs if side == 0 else sb.env_bs
+    trun = random_trun(basis, ms, rng)
+    mshift = 0 if side == 0 else sb.sys.len + 1
+    return RenormCase(sb.lat, side, mshift, pre, basis, trun)

@@ -264,6 +264,26 @@ typedef struct tj_model_result {
 int tj_get_hamiltonian(tj_ctx *ctx, const tj_lattice *lat, int side, int mshift, const tj_model *pre,
                        const tj_basis *basis, const tj_block *trun, tj_model_result *out);
 
+
+/* ------------------------------------------------ wavefunction prediction */
+
+/* wave_trans_LR(sys_bs,env_bs,sys_trun,env_trun,old_wave,new_wave)
+ * (code/tjsq/dmrg_sub.f90:1093-1238) for direction = 0 and wave_trans_RL
+ * (code/tjsq/dmrg_sub.f90:1242-1384) for direction = 1: the converged
+ * wavefunction of the last DMRG step carried to the next superblock of a
+ * sweep, as the reference's left_to_right / right_to_left call them
+ * (dmrg_sub.f90:778, 845, 960, 1026).  Arguments as in the reference:
+ * direction 0 -- sys_bs is the new system block's enlarged basis, env_bs the
+ * environment basis of the last step, sys_trun the truncation just computed,
+ * env_trun the one that built the last step's environment block; direction
+ * 1 -- the mirror image.  new_wave's sector table is the caller's
+ * (allocate_wave of the new super basis); its data is overwritten by the
+ * carried vector, normalised (wave_normalize).  TJ_ERR_NUMERIC if the
+ * carried vector is zero. */
+int tj_wave_trans(tj_ctx *ctx, int direction, const tj_basis *sys_bs, const tj_basis *env_bs,
+                  const tj_block *sys_trun, const tj_block *env_trun, const tj_wave *old_wave,
+                  tj_wave *new_wave);
+
 /* --------------------------------------------------- measurement support */
 
 /* Statistics of the H*psi task list compiled for the last tj_model_wave /
@@ -287,6 +307,10 @@ typedef struct tj_hpsi_stats {
    * plan compile, operator upload + hmerge + work-list upload, the
    * split-precision plan, and the last tj_lanczos_memo_new after it */
   double prepare_ms, plan_ms, upload_ms, ozplan_ms, lanczos_ms;
+  /* the last tj_get_hamiltonian: host time of its plan (ms), device time of
+   * its two GEMM launches (ms), the whole call from the first upload to the
+   * end of the download (ms), and its FP64 flops */
+  double renorm_plan_ms, renorm_ms, renorm_e2e_ms, renorm_flops;
 } tj_hpsi_stats;
 int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st);
 
@@ -432,6 +456,25 @@ int tj_hpsi_plan_export(const tj_lattice *lat, const tj_model *sys, const tj_mod
  * matching entry point (NULL for a basis or operator it does not take). */
 int tj_cor_plan_export(int kind, const tj_block *a, const tj_block *b, const tj_basis *sys_bs,
                        const tj_basis *env_bs, const tj_wave *wave, char flag, tj_plan_export *out);
+/* The compiled form of tj_get_hamiltonian for checks on the CPU (no GPU, no
+ * arithmetic): the two grouped-GEMM passes as in tj_hpsi_plan_export, with
+ * space 1 = the blocks of `pre`, space 2 = trun's data from its lowest
+ * sub-block offset, and the cells of the second pass writing the new
+ * operators in the result's layout (psi_len = the result's data_len).  `res`
+ * (optional) receives the result's sizes, and with its arrays set its
+ * records and blocks, as tj_get_hamiltonian would give them (data left
+ * unwritten). */
+int tj_renorm_plan_export(const tj_lattice *lat, int side, int mshift, const tj_model *pre,
+                          const tj_basis *basis, const tj_block *trun, tj_plan_export *out,
+                          tj_model_result *res);
+/* The compiled form of tj_wave_trans for checks on the CPU: space 1 = the
+ * data of sys_trun then of env_trun (each from its lowest sub-block offset,
+ * as the uploads say), space 2 = old_wave's data, the cells of the second
+ * pass writing new_wave's layout before the normalisation (psi_len =
+ * new_wave->dim). */
+int tj_wave_trans_plan_export(int direction, const tj_basis *sys_bs, const tj_basis *env_bs,
+                              const tj_block *sys_trun, const tj_block *env_trun, const tj_wave *old_wave,
+                              const tj_wave *new_wave, tj_plan_export *out);
 
 /* The split-precision form of the same H*psi (TJ_PREC_OZAKI with `slices`
  * int8 slices), for CPU checks of its tables.  A split stores `rows` x K of

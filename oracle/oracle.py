@@ -73,6 +73,7 @@ def lib(threads: int = 1):
                                       P(C.c_double)]
         L.ora_get_hamiltonian.argtypes = [P(TjLattice), C.c_int, C.c_int, P(TjModel), P(TjBasis), P(TjBlock),
                                           P(TjModelResult)]
+        L.ora_wave_trans.argtypes = [C.c_int, P(TjBasis), P(TjBasis), P(TjBlock), P(TjBlock), P(TjWave), P(TjWave)]
         L.ora_site_operator.argtypes = [C.c_int, C.c_int, P(TjBlock), P(TjBlockSub), P(C.c_double)]
         rc = L.ora_init(openblas_path().encode(), threads)
         if rc:
@@ -199,6 +200,16 @@ def lanczos_parts(lat, sys, env, sys_bs, env_bs, wave, lanzero: float):
     return e.value, it.value, w
 
 
+def wave_trans(direction: int, sys_bs, env_bs, sys_trun, env_trun, old, new_wave):
+    """wave_trans_LR (direction 0) / wave_trans_RL (direction 1): fills and returns
+    `new_wave` (a Wave with the next superblock's sectors)."""
+    L = lib()
+    pb, pe, ps, pt = sys_bs.pack(), env_bs.pack(), sys_trun.pack(), env_trun.pack()
+    _chk(L.ora_wave_trans(direction, C.byref(pb.c), C.byref(pe.c), C.byref(ps.c), C.byref(pt.c), C.byref(old.c),
+                          C.byref(new_wave.c)))
+    return new_wave
+
+
 class OracleBackend:
     """The hot-path calls of grand_sql_tj_b200.sweep.Dmrg on the oracle (CPU)."""
 
@@ -211,3 +222,6 @@ class OracleBackend:
 
     def get_hamiltonian(self, lat, side, mshift, pre, basis, trun):
         return get_hamiltonian(lat, side, mshift, pre, basis, trun)
+
+    def wave_trans(self, direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave):
+        return wave_trans(direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave)

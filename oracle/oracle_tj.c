@@ -2514,3 +2514,112 @@ done:
   model_free(&pre);
   return rc;
 }
+
+/* ============================================ wavefunction prediction */
+static void wave_norm_scale(tj_wave *w) {
+  double s = wave_product(w, w->data, w->data);
+  wave_scale(w->dim, w->data, sqrt(s));   /* divides by the norm */
+}
+/* wave_trans_LR (dmrg_sub.f90:1093-1238), direction 0, and wave_trans_RL
+ * (dmrg_sub.f90:1242-1384), direction 1 */
+int ora_wave_trans(int direction, const tj_basis *sys_bs, const tj_basis *env_bs, const tj_block *sys_trunb,
+                   const tj_block *env_trunb, const tj_wave *old, tj_wave *nw) {
+  if (!p_dgemm) return fail(TJ_ERR_ARG, "oracle not initialised (ora_init)");
+  if (!sys_bs || !env_bs || !sys_trunb || !env_trunb || !old || !nw) return fail(TJ_ERR_ARG, "ora_wave_trans: null");
+  OBlk st, et;
+  blk_view(sys_trunb, &st);
+  blk_view(env_trunb, &et);
+  memset(nw->data, 0, (size_t)nw->dim * sizeof(double));
+  for (int i = 0; i < old->num; i++) {
+    const int snu = old->sub[i].sys_num_up, snd = old->sub[i].sys_num_down;
+    const int enu = old->sub[i].env_num_up, end = old->sub[i].env_num_down;
+    const int osd = old->sub[i].sys_dim, oed = old->sub[i].env_dim;
+    if (direction == 0) {
+      const int tid = find_sub(&st, snu, snd, 0, 0);
+      if (tid < 0) continue;
+      for (int k = 0; k < env_bs->num; k++) {
+        if (env_bs->sub[k].new_num_up != enu || env_bs->sub[k].new_num_down != end) continue;
+        for (int x = 0; x < env_bs->sub[k].num; x++) {
+          const tj_basis_sub *m = BM(env_bs, k, x);
+          const int stu = m->st_num_up, std_ = m->st_num_down, neu = m->bl_num_up, ned = m->bl_num_down;
+          const int opos = m->spos, osub = m->sdim;
+          const int eid = find_sub(&et, neu, ned, 0, 0);
+          for (int nsd = abs(snd - std_); nsd <= snd + std_; nsd += 2) {
+            const int nsu = snu + stu;
+            int bid = -1, bsub = -1;
+            for (int y = 0; y < sys_bs->num && bid < 0; y++) {
+              if (sys_bs->sub[y].new_num_up != nsu || sys_bs->sub[y].new_num_down != nsd) continue;
+              for (int z = 0; z < sys_bs->sub[y].num; z++) {
+                const tj_basis_sub *q = BM(sys_bs, y, z);
+                if (q->bl_num_up == snu && q->bl_num_down == snd && q->st_num_up == stu && q->st_num_down == std_) {
+                  bid = y;
+                  bsub = z;
+                  break;
+                }
+              }
+            }
+            const int wid = find_out(nw, nsu, nsd, neu, ned);
+            if (eid < 0 || bid < 0 || wid < 0) continue;
+            const int nedim = nw->sub[wid].env_dim;
+            const int npos = BM(sys_bs, bid, bsub)->spos, nsub = BM(sys_bs, bid, bsub)->sdim;
+            const int j12 = snd, j3 = std_, j4 = ned, j123 = nsd, j34 = end;
+            double c1 = ipow_m1((j12 + j3 + j123) / 2) / sqrt((1.0 + j12) * (1.0 + j123));
+            c1 *= sqrt((1.0 + j123) * (j34 + 1.0));
+            if (((j12 + j3 + j4) / 2) % 2 != 0) c1 = -c1;
+            if (((j3 + j4 - j34) / 2) % 2 != 0) c1 = -c1;
+            double *sub = mat_zero(nsub, osub);
+            dg('T', 'N', nsub, osub, osd, c1, st.sub[tid].mat, osd, WP(old, i, 0, opos), LD(old, i), 0.0, sub, nsub);
+            dg('N', 'T', nsub, nedim, osub, 1.0, sub, nsub, et.sub[eid].mat, nedim, 1.0, WP(nw, wid, npos, 0),
+               LD(nw, wid));
+            free(sub);
+          }
+        }
+      }
+    } else {
+      const int tid = find_sub(&et, enu, end, 0, 0);
+      if (tid < 0) continue;
+      for (int k = 0; k < sys_bs->num; k++) {
+        if (sys_bs->sub[k].new_num_up != snu || sys_bs->sub[k].new_num_down != snd) continue;
+        for (int x = 0; x < sys_bs->sub[k].num; x++) {
+          const tj_basis_sub *m = BM(sys_bs, k, x);
+          const int stu = m->st_num_up, std_ = m->st_num_down, nsu = m->bl_num_up, nsd = m->bl_num_down;
+          for (int ned = abs(end - std_); ned <= end + std_; ned += 2) {
+            const int neu = enu + stu;
+            const int opos = m->spos, osub = m->sdim;
+            const int sid = find_sub(&st, nsu, nsd, 0, 0);
+            int bid = -1, bsub = -1;
+            for (int y = 0; y < env_bs->num && bid < 0; y++) {
+              if (env_bs->sub[y].new_num_up != neu || env_bs->sub[y].new_num_down != ned) continue;
+              for (int z = 0; z < env_bs->sub[y].num; z++) {
+                const tj_basis_sub *q = BM(env_bs, y, z);
+                if (q->bl_num_up == enu && q->bl_num_down == end && q->st_num_up == stu && q->st_num_down == std_) {
+                  bid = y;
+                  bsub = z;
+                  break;
+                }
+              }
+            }
+            const int wid = find_out(nw, nsu, nsd, neu, ned);
+            if (sid < 0 || bid < 0 || wid < 0) continue;
+            const int nsdim = nw->sub[wid].sys_dim;
+            const int npos = BM(env_bs, bid, bsub)->spos, nsub = BM(env_bs, bid, bsub)->sdim;
+            const int j12 = end, j3 = std_, j4 = nsd, j123 = ned, j34 = snd;
+            double c1 = ipow_m1((j34 + j4 + j3) / 2) / sqrt((1.0 + j12) * (1.0 + j4));
+            c1 *= sqrt((1.0 + j123) * (j34 + 1.0));
+            if (((j4 + j3 + j12) / 2) % 2 != 0) c1 = -c1;
+            if (((j12 + j3 - j123) / 2) % 2 != 0) c1 = -c1;
+            double *sub = mat_zero(nsdim, oed);
+            dg('N', 'N', nsdim, oed, osub, c1, st.sub[sid].mat, nsdim, WP(old, i, opos, 0), LD(old, i), 0.0, sub,
+               nsdim);
+            dg('N', 'N', nsdim, nsub, oed, 1.0, sub, nsdim, et.sub[tid].mat, oed, 1.0, WP(nw, wid, 0, npos), LD(nw, wid));
+            free(sub);
+          }
+        }
+      }
+    }
+  }
+  wave_norm_scale(nw);
+  blk_free(&st);
+  blk_free(&et);
+  return 0;
+}

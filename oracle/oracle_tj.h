@@ -78,6 +78,13 @@ int ora_sys_site_env_site_cor_ndia(const tj_block *st, const tj_block *st2, cons
 int ora_get_hamiltonian(const tj_lattice *lat, int side, int mshift, const tj_model *pre, const tj_basis *basis,
                         const tj_block *trun, tj_model_result *out);
 
+/* wave_trans_LR (direction 0, code/tjsq/dmrg_sub.f90:1093-1238) and
+ * wave_trans_RL (direction 1, dmrg_sub.f90:1242-1384): the wavefunction of
+ * the last step carried to the next superblock; new_wave's sectors are set
+ * by the caller (allocate_wave), its data is overwritten and normalised. */
+int ora_wave_trans(int direction, const tj_basis *sys_bs, const tj_basis *env_bs, const tj_block *sys_trun,
+                   const tj_block *env_trun, const tj_wave *old_wave, tj_wave *new_wave);
+
 /* Site operators of Get_site_operator_su2_U0 (code/tjsq/dmrg_sub.f90:370-473):
  * which = 0 st_elec_up, 1 st_elec_down, 2 num_elec, 3 st_sd, 4 st_si.
  * Writes at most 2 sub-blocks and 2 doubles; returns the sub count. */
