@@ -473,12 +473,13 @@ def pack_superblock(sb):
 
 
 def packed_arrays(packed):
-    """Every operator data array of pack_superblock's models."""
-    out = []
+    """Every operator data array of pack_superblock's models (each array once)."""
+    out, seen = [], set()
     for m in packed[:2]:
-        out.append(m.ham.data)
-        for sets in m.sets:
-            out.extend(p.data for p in sets)
+        for a in [m.ham.data] + [p.data for sets in m.sets for p in sets]:
+            if id(a) not in seen:
+                seen.add(id(a))
+                out.append(a)
     return out
 
 

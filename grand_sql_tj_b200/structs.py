@@ -198,7 +198,9 @@ class Model:
     sub: List[BlockSet]
 
     def pack(self) -> "PackedModel":
-        return PackedModel(self)
+        # a model the library returned keeps its result arrays: packed without a copy
+        pk = getattr(self, "_packed", None)
+        return pk if pk is not None else PackedModel(self)
 
 
 class PackedModel:
@@ -348,26 +350,47 @@ def call_model_result(call):
     rc = call(C.byref(res))
     if rc:
         return rc, None
-    return 0, model_from_c(res.model, data)
+    return 0, model_from_c(res.model, data, keep=(res, sets, subs, data))
 
 
 def _block_from_c(b: TjBlock, data: np.ndarray) -> Block:
+    """Sub-blocks as column-major views into `data` (no copy)."""
     subs = []
     for i in range(b.num):
         s = b.sub[i]
         n = s.row_dim * s.sdim
         subs.append(SubBlock(s.num_up, s.num_down, s.down_dif,
-                             data[s.off:s.off + n].reshape((s.row_dim, s.sdim), order="F").copy()))
+                             data[s.off:s.off + n].reshape((s.row_dim, s.sdim), order="F")))
     return Block(b.len, b.up_dif, b.down_dif, subs)
 
 
-def model_from_c(m: TjModel, data: np.ndarray) -> Model:
-    """A tj_model whose blocks all point into `data` -> a numpy-side Model."""
+class _ResultPack:
+    """The packed form of a model the library wrote: its own result arrays."""
+
+    class _P:
+        def __init__(self, c, data):
+            self.c, self.data = c, data
+
+    def __init__(self, m: TjModel, data: np.ndarray, keep):
+        self.c = m
+        self.keep = keep
+        self.ham = self._P(m.ham, data)
+        self.sets = [[self._P(getattr(m.sub[i], k), data) for k in OPS] for i in range(m.nsub)]
+        self.data = data
+
+
+def model_from_c(m: TjModel, data: np.ndarray, keep=None) -> Model:
+    """A tj_model whose blocks all point into `data` -> a numpy-side Model whose
+    sub-blocks are views into `data`; `keep` holds the arrays the C structs
+    point into, so that the Model packs without a copy."""
     sets = []
     for i in range(m.nsub):
         bs = m.sub[i]
         sets.append(BlockSet(*[_block_from_c(getattr(bs, k), data) for k in OPS]))
-    return Model(m.len, _block_from_c(m.ham, data), sets)
+    out = Model(m.len, _block_from_c(m.ham, data), sets)
+    if keep is not None:
+        out._packed = _ResultPack(m, data, keep)
+    return out
 
 
 def block_from_c_result(res: TjTruncResult, length: int) -> Block:
