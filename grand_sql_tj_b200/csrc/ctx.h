@@ -35,8 +35,11 @@ struct DevBuf {
 
 // compiled operator renormalisation of the last tj_get_hamiltonian call (renorm.cpp)
 struct tj_renorm_state;
+// device-resident result of the last measurement-operator call (renorm.cpp)
+struct tj_meas_state;
 namespace tjb {
 std::shared_ptr<tj_renorm_state> new_renorm_state();
+std::shared_ptr<tj_meas_state> new_meas_state();
 }
 
 struct tj_ctx {
@@ -71,6 +74,7 @@ struct tj_ctx {
   tjb::DevBuf rnOps, rnTrun, rnScr, rnOut, rnSlots, rnTab;             // operator renormalisation
   tjb::DevBuf wtOps, wtOld, wtNew, wtScr, wtSlots, wtTab;              // wavefunction prediction
   std::shared_ptr<tj_renorm_state> renorm;
+  std::shared_ptr<tj_meas_state> meas;
   // split-precision H*psi
   std::unique_ptr<tjb::OzPlan> oz;
   tjb::DevBuf ozPack, ozScales, ozStaJobs, ozPsiJobs, ozProdJobs, ozSegs, ozFams, ozCells, ozProdRows, ozStackRows, ozItems1,

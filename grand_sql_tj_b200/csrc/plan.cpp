@@ -37,6 +37,39 @@ static double g_fact[302];
 static bool g_fact_ready = false;
 static inline double fct(int i) { return (i >= 0 && i <= 301) ? g_fact[i] : 0.0; }
 
+static void fact_init() {
+  if (g_fact_ready) return;
+  std::fill(g_fact, g_fact + 302, 0.0);
+  g_fact[0] = 1.0;
+  for (int i = 1; i <= 142; ++i) g_fact[i] = g_fact[i - 1] * (double)(float)i;
+  g_fact_ready = true;
+}
+
+// Wigner 3j symbol on doubled spins and projections, by the Racah sum:
+// (j1 j2 j3; m1 m2 m3) = (-1)^(j1-j2-m3) sqrt(D(j1 j2 j3) prod (j_i+m_i)!(j_i-m_i)!)
+//   sum_k (-1)^k / [k! (j3-j2+m1+k)! (j3-j1-m2+k)! (j1+j2-j3-k)! (j1-m1-k)! (j2+m2-k)!],
+// D = (j1+j2-j3)!(j1-j2+j3)!(j2+j3-j1)!/(j1+j2+j3+1)!  (all arguments halved here).
+double w3j(int j1, int j2, int j3, int m1, int m2, int m3) {
+  fact_init();
+  if (m1 + m2 + m3 != 0) return 0.0;
+  if (j3 > j1 + j2 || j3 < std::abs(j1 - j2)) return 0.0;
+  if (std::abs(m1) > j1 || std::abs(m2) > j2 || std::abs(m3) > j3) return 0.0;
+  if (((j1 + j2 + j3) & 1) || ((j1 + m1) & 1) || ((j2 + m2) & 1) || ((j3 + m3) & 1)) return 0.0;
+  const int a = j3 - j2 + m1, b = j3 - j1 - m2, c = j1 + j2 - j3, d = j1 - m1, e = j2 + m2;
+  const int kmin = std::max(0, std::max(-a, -b)), kmax = std::min(c, std::min(d, e));
+  double sum = 0.0;
+  for (int k = kmin; k <= kmax; k += 2) {
+    double den = fct(k / 2) * fct((a + k) / 2) * fct((b + k) / 2) * fct((c - k) / 2) * fct((d - k) / 2) *
+                 fct((e - k) / 2);
+    sum += ((k / 2) % 2 ? -1.0 : 1.0) / den;
+  }
+  const double tri = fct(c / 2) * fct((j1 - j2 + j3) / 2) * fct((j2 + j3 - j1) / 2) / fct((j1 + j2 + j3) / 2 + 1);
+  const double mf = fct((j1 + m1) / 2) * fct((j1 - m1) / 2) * fct((j2 + m2) / 2) * fct((j2 - m2) / 2) *
+                    fct((j3 + m3) / 2) * fct((j3 - m3) / 2);
+  const int ph = (j1 - j2 - m3) / 2;
+  return ((ph % 2) ? -1.0 : 1.0) * std::sqrt(tri * mf) * sum;
+}
+
 double w6j(int j1, int j2, int j3, int l1, int l2, int l3) {
   if (!g_fact_ready) {
     std::fill(g_fact, g_fact + 302, 0.0);
@@ -1945,3 +1978,6 @@ void merge_plans(const std::vector<const HpsiPlan *> &parts, HpsiPlan &out, std:
 }
 
 }  // namespace tjb
+
+extern "C" double tj_w6js(int j1, int j2, int j3, int l1, int l2, int l3) { return tjb::w6j(j1, j2, j3, l1, l2, l3); }
+extern "C" double tj_w3js(int j1, int j2, int j3, int m1, int m2, int m3) { return tjb::w3j(j1, j2, j3, m1, m2, m3); }

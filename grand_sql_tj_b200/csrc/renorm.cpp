@@ -24,6 +24,7 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
@@ -862,4 +863,557 @@ extern "C" int tj_renorm_plan_export(const tj_lattice *lat, int side, int mshift
   R.P.psi_len = R.out_len;
   if (res) fill_result(R, res);
   return export_hpsi_plan(R.P, out);
+}
+
+// ================================================= measurement operators
+// Get_*_oper_* / Change_*_oper_* (code/tjsq/get_sys.f90:764-1238): an
+// operator carried through the stored bases and truncations of one side,
+// one step per block length -- each step the same enlarge-and-truncate pass
+// as the renormalisation above, with the operator staying on the device
+// between steps -- and block_mul_block_ndia / update_trun on their own.
+namespace tjb {
+namespace {
+
+// a block operator resident on the device: structure on the host, matrices in buf
+struct DevOp {
+  RBlk b;
+  int dim = 0;
+  DevBuf buf;
+  DevOp() = default;
+  DevOp(const DevOp &) = delete;
+  DevOp &operator=(const DevOp &) = delete;
+  ~DevOp() { buf.release(); }
+};
+
+// the two grouped-GEMM passes of a plan whose operand spaces are on the device
+int exec_passes(tj_ctx *ctx, const HpsiPlan &P, const double *ops, const double *psi, double *out) {
+  cudaStream_t st = ctx->stream;
+  int rc;
+  if ((rc = ctx->rnScr.reserve(sizeof(double) * (P.scratch_len + 4))) ||
+      (rc = ctx->rnSlots.reserve(sizeof(double) * (std::max(P.nslots1, P.nslots2) * BM * BN + 4))))
+    return rc;
+  std::vector<char> tab;
+  auto add = [&](const void *p, size_t n) {
+    size_t at = (tab.size() + 255) / 256 * 256;
+    tab.resize(at + n + 1);
+    if (n && p) std::memcpy(tab.data() + at, p, n);
+    return at;
+  };
+  const size_t o_c1 = add(P.cells1.data(), P.cells1.size() * sizeof(Cell));
+  const size_t o_t1 = add(P.tasks1.data(), P.tasks1.size() * sizeof(Task));
+  const size_t o_l1 = add(P.tiles1.data(), P.tiles1.size() * sizeof(Tile));
+  const size_t o_r1 = add(P.red1.data(), P.red1.size() * sizeof(Reduce));
+  const size_t o_c2 = add(P.cells2.data(), P.cells2.size() * sizeof(Cell));
+  const size_t o_t2 = add(P.tasks2.data(), P.tasks2.size() * sizeof(Task));
+  const size_t o_l2 = add(P.tiles2.data(), P.tiles2.size() * sizeof(Tile));
+  const size_t o_r2 = add(P.red2.data(), P.red2.size() * sizeof(Reduce));
+  const size_t o_cnt = add(nullptr, 16);
+  std::memset(tab.data() + o_cnt, 0, 16);
+  if ((rc = ctx->rnTab.reserve(tab.size() + 256))) return rc;
+  CKR(cudaMemcpyAsync(ctx->rnTab.p, tab.data(), tab.size(), cudaMemcpyHostToDevice, st));
+  char *tb = (char *)ctx->rnTab.p;
+  GemmParams g;
+  std::memset(&g, 0, sizeof g);
+  g.ops = ops;
+  g.psi = psi;
+  g.scr = ctx->rnScr.d();
+  g.out = ctx->rnScr.d();
+  g.cells = (const Cell *)(tb + o_c1);
+  g.tasks = (const Task *)(tb + o_t1);
+  g.tiles = (const Tile *)(tb + o_l1);
+  g.ntiles = (int)P.tiles1.size();
+  g.counter = (unsigned int *)(tb + o_cnt);
+  g.slots = ctx->rnSlots.d();
+  launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles), st);
+  launch_reduce(g, (const Reduce *)(tb + o_r1), (int)P.red1.size(), st);
+  g.out = out;
+  g.cells = (const Cell *)(tb + o_c2);
+  g.tasks = (const Task *)(tb + o_t2);
+  g.tiles = (const Tile *)(tb + o_l2);
+  g.ntiles = (int)P.tiles2.size();
+  g.counter = (unsigned int *)(tb + o_cnt) + 1;
+  launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles), st);
+  launch_reduce(g, (const Reduce *)(tb + o_r2), (int)P.red2.size(), st);
+  CKR(cudaGetLastError());
+  // the tables and the truncation buffer are rewritten by the next pass: wait for this one
+  CKR(cudaStreamSynchronize(st));
+  return TJ_OK;
+}
+
+// a host block uploaded into a device operator
+int upload_op(tj_ctx *ctx, const tj_block &b, DevOp &d) {
+  HpsiPlan P;
+  load_block(b, d.b, P);
+  d.dim = b.dim;
+  int rc = d.buf.reserve(sizeof(double) * (P.ops_len + 4));
+  if (rc) return rc;
+  for (const auto &u : P.uploads)
+    if (u.n > 0) CKR(cudaMemcpyAsync(d.buf.d() + u.dst, u.src, sizeof(double) * u.n, cudaMemcpyHostToDevice, ctx->stream));
+  return TJ_OK;
+}
+
+// host storage of a truncation operator made of unit matrices (block_transfer_basis)
+struct IdTrun {
+  std::vector<tj_block_sub> subs;
+  std::vector<double> data;
+  tj_block blk;
+  explicit IdTrun(const tj_basis *bs) {
+    int64_t off = 0;
+    for (int i = 0; i < bs->num; ++i) {
+      const int d = bs->sub[i].dim;
+      tj_block_sub s;
+      std::memset(&s, 0, sizeof s);
+      s.num_up = bs->sub[i].new_num_up;
+      s.num_down = bs->sub[i].new_num_down;
+      s.row_dim = d;
+      s.sdim = d;
+      s.off = off;
+      subs.push_back(s);
+      off += (int64_t)d * d;
+    }
+    data.assign(std::max<int64_t>(off, 1), 0.0);
+    for (const auto &s : subs)
+      for (int k = 0; k < s.row_dim; ++k) data[s.off + (int64_t)k * s.row_dim + k] = 1.0;
+    std::memset(&blk, 0, sizeof blk);
+    blk.len = bs->len;
+    blk.num = (int32_t)subs.size();
+    blk.dim = bs->dim;
+    blk.sub = subs.data();
+    blk.data = data.data();
+  }
+};
+
+// U^T E U of an enlarged operator (pieces over the device operator `in_dev`):
+// the truncation operator trun is uploaded, one plan, two passes -> out
+int trunc_step(tj_ctx *ctx, const EBlk &e, bool dia, int len, const tj_block &trun, const tj_basis *basis,
+               const double *in_dev, DevOp &out, std::string &msg) {
+  if (trun.num < 1 || !trun.sub || !trun.data) {
+    msg = "empty truncation operator";
+    return TJ_ERR_ARG;
+  }
+  HpsiPlan P;
+  Builder B(nullptr, basis, P);
+  int64_t lo = LLONG_MAX, hi = 0;
+  for (int k = 0; k < trun.num; ++k) {
+    const tj_block_sub &s = trun.sub[k];
+    if (s.row_dim < 0 || s.sdim < 0 || s.off < 0) {
+      msg = "bad truncation sub-block";
+      return TJ_ERR_ARG;
+    }
+    lo = std::min(lo, (int64_t)s.off);
+    hi = std::max(hi, (int64_t)s.off + (int64_t)s.row_dim * s.sdim);
+  }
+  for (int k = 0; k < trun.num; ++k) {
+    const tj_block_sub &s = trun.sub[k];
+    B.trun.sec.push_back(TSec{s.num_up, s.num_down, s.row_dim, s.sdim, s.off - lo});
+  }
+  B.trun_dim = trun.dim;
+  try {
+    B.truncate(e, dia, len);
+  } catch (const RenormError &er) {
+    msg = er.what();
+    return er.code;
+  }
+  {   // tasks sorted by cell (the cells were emitted in record order)
+    std::vector<int32_t> cnt(P.cells2.size() + 1, 0);
+    for (int32_t c : B.t2cell) cnt[c + 1]++;
+    for (size_t i = 0; i < P.cells2.size(); ++i) cnt[i + 1] += cnt[i];
+    P.tasks2.resize(B.t2.size());
+    std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1);
+    for (size_t t = 0; t < B.t2.size(); ++t) P.tasks2[pos[B.t2cell[t]]++] = B.t2[t];
+    std::vector<Cell> kept;
+    for (size_t i = 0; i < P.cells2.size(); ++i) {
+      if (cnt[i + 1] == cnt[i]) continue;
+      Cell cl = P.cells2[i];
+      cl.t_begin = cnt[i];
+      cl.t_end = cnt[i + 1];
+      kept.push_back(cl);
+    }
+    P.cells2.swap(kept);
+  }
+  split_tiles(P.cells1, P.tasks1, P.tiles1, P.red1, P.nslots1, false);
+  split_tiles(P.cells2, P.tasks2, P.tiles2, P.red2, P.nslots2, false);
+  int rc;
+  if ((rc = ctx->rnTrun.reserve(sizeof(double) * (hi - lo + 4))) ||
+      (rc = out.buf.reserve(sizeof(double) * (B.out_len + 4))))
+    return rc;
+  CKR(cudaMemcpyAsync(ctx->rnTrun.d(), trun.data + lo, sizeof(double) * (hi - lo), cudaMemcpyHostToDevice,
+                      ctx->stream));
+  CKR(cudaMemsetAsync(out.buf.p, 0, sizeof(double) * (B.out_len + 4), ctx->stream));
+  if ((rc = exec_passes(ctx, P, in_dev, ctx->rnTrun.d(), out.buf.d()))) return rc;
+  const OutBlk &ob = B.blocks[0];
+  out.b.len = len;
+  out.b.up_dif = ob.up_dif;
+  out.b.down_dif = ob.down_dif;
+  out.dim = ob.dim;
+  out.b.sub.clear();
+  for (int i = 0; i < ob.num; ++i) {
+    const tj_block_sub &r = B.recs[ob.first + i];
+    out.b.sub.push_back(RSub{r.num_up, r.num_down, r.down_dif, r.row_dim, r.sdim, r.off});
+  }
+  return TJ_OK;
+}
+
+// the enlargement of a device operator into a basis (update_block_dia /
+// update_block_ndia_sys/env) or of a one-site operator (update_site_*)
+EBlk enlarge(const tj_basis *bs, const RBlk *blk, const SiteOp *site, bool dia, int side, char types) {
+  Ctx c;
+  c.bs = bs;
+  if (dia) return enl_dia(c, blk, site);
+  return enl_ndia(c, blk, site, side == 1, types);
+}
+
+// a device operator whose pieces are its own sub-blocks (no enlargement), to be truncated
+EBlk as_pieces(const DevOp &d) {
+  EBlk e;
+  e.len = d.b.len;
+  e.up_dif = d.b.up_dif;
+  e.down_dif = d.b.down_dif;
+  e.set = true;
+  for (const RSub &s : d.b.sub) {
+    ESub q{s.num_up, s.num_down, s.down_dif, -1, -1, {}};
+    q.p.push_back(Piece{0, s.row_dim, 0, s.sdim, s.off, s.row_dim, 0, 0, 1.0});
+    e.sub.push_back(std::move(q));
+  }
+  return e;
+}
+
+SiteOp site_of(const tj_block &b) {
+  SiteOp s;
+  s.up_dif = b.up_dif;
+  s.down_dif = b.down_dif;
+  if (b.num > 0 && (!b.sub || !b.data)) throw RenormError(TJ_ERR_ARG, "site operator with null sub/data");
+  for (int k = 0; k < b.num; ++k) {
+    const tj_block_sub &q = b.sub[k];
+    if (q.row_dim != 1 || q.sdim != 1) throw RenormError(TJ_ERR_ARG, "site operator sub-blocks must be 1x1");
+    s.sub.push_back(SiteOp::S{q.num_up, q.num_down, q.down_dif, b.data[q.off]});
+  }
+  return s;
+}
+
+// result (two-call) of the last measurement-operator call, kept on the device
+struct LastOp {
+  uint64_t key = 0;
+  bool valid = false;
+  DevOp op;
+};
+
+int finish(tj_ctx *ctx, DevOp &d, tj_block_result *out) {
+  int64_t n = 0;
+  for (const RSub &s : d.b.sub) n = std::max(n, s.off + (int64_t)s.row_dim * s.sdim);
+  out->num = (int32_t)d.b.sub.size();
+  out->data_len = n;
+  if (!out->subs || !out->data) return TJ_OK;
+  for (size_t i = 0; i < d.b.sub.size(); ++i) {
+    const RSub &s = d.b.sub[i];
+    tj_block_sub r;
+    std::memset(&r, 0, sizeof r);
+    r.num_up = s.num_up;
+    r.num_down = s.num_down;
+    r.down_dif = s.down_dif;
+    r.row_dim = s.row_dim;
+    r.sdim = s.sdim;
+    r.off = s.off;
+    out->subs[i] = r;
+  }
+  if (n > 0) CKR(cudaMemcpyAsync(out->data, d.buf.d(), sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  CKR(cudaStreamSynchronize(ctx->stream));
+  std::memset(&out->block, 0, sizeof out->block);
+  out->block.len = d.b.len;
+  out->block.num = out->num;
+  out->block.dim = d.dim;
+  out->block.up_dif = d.b.up_dif;
+  out->block.down_dif = d.b.down_dif;
+  out->block.sub = out->subs;
+  out->block.data = out->data;
+  return TJ_OK;
+}
+
+// The loop shared by Get_*_oper_* and Change_*_oper_* (get_sys.f90:764-1238):
+// `cur` (block length idx) enlarged into bsm(idx+1) and truncated by its
+// truncation, up to length idx_two - 1; then enlarged into bsm(idx_two), and
+// truncated there when truns.
+int carry_dev(tj_ctx *ctx, const tj_chain *ch, int side, bool dia, char types, DevOp &cur, int idx, int idx_two,
+              bool truns, DevOp &res, std::string &msg) {
+  DevOp tmp;
+  auto chain_ok = [&](int i) { return i >= 1 && i <= ch->n; };
+  while (idx + 1 <= idx_two - 1) {
+    if (!chain_ok(idx + 1)) {
+      msg = "chain index out of range";
+      return TJ_ERR_ARG;
+    }
+    const tj_basis *bs = &ch->bsm[idx];
+    EBlk e = enlarge(bs, &cur.b, nullptr, dia, side, types);
+    ++idx;
+    int rc;
+    if (idx <= ch->trun_idx) {
+      IdTrun id(bs);
+      rc = trunc_step(ctx, e, dia, bs->len, id.blk, bs, cur.buf.d(), tmp, msg);
+    } else {
+      rc = trunc_step(ctx, e, dia, bs->len, ch->truns[idx - 1], bs, cur.buf.d(), tmp, msg);
+    }
+    if (rc) return rc;
+    std::swap(cur.b, tmp.b);
+    std::swap(cur.buf, tmp.buf);
+    cur.dim = tmp.dim;
+  }
+  if (!chain_ok(idx + 1) || !chain_ok(idx_two)) {
+    msg = "chain index out of range";
+    return TJ_ERR_ARG;
+  }
+  const tj_basis *bs = &ch->bsm[idx];
+  EBlk e = enlarge(bs, &cur.b, nullptr, dia, side, types);
+  if (truns) return trunc_step(ctx, e, dia, bs->len, ch->truns[idx_two - 1], bs, cur.buf.d(), res, msg);
+  IdTrun id(bs);
+  return trunc_step(ctx, e, dia, bs->len, id.blk, bs, cur.buf.d(), res, msg);
+}
+
+uint64_t key_chain(uint64_t h, const tj_chain *ch) {
+  h = fnv(h, ch, sizeof *ch);
+  if (ch->bsm && ch->n > 0) h = fnv(h, ch->bsm, sizeof(tj_basis) * ch->n);
+  if (ch->truns && ch->n > 0) h = fnv(h, ch->truns, sizeof(tj_block) * ch->n);
+  return h;
+}
+
+}  // namespace
+}  // namespace tjb
+
+struct tj_meas_state {
+  tjb::LastOp last;
+};
+std::shared_ptr<tj_meas_state> tjb::new_meas_state() { return std::make_shared<tj_meas_state>(); }
+
+static int meas_call(tj_ctx *ctx, uint64_t key, tj_block_result *out,
+                     const std::function<int(tjb::DevOp &, std::string &)> &compute, const char *what) {
+  using namespace tjb;
+  if (!ctx || !out) return set_err(TJ_ERR_ARG, std::string(what) + ": null argument");
+  CKR(cudaSetDevice(ctx->device));
+  if (!ctx->meas) ctx->meas = new_meas_state();
+  LastOp &L = ctx->meas->last;
+  if (!(L.valid && L.key == key)) {
+    L.valid = false;
+    std::string msg;
+    int rc;
+    try {
+      rc = compute(L.op, msg);
+    } catch (const std::exception &e) {
+      rc = TJ_ERR_ARG;
+      msg = e.what();
+    }
+    if (rc) return set_err(rc, std::string(what) + ": " + msg);
+    L.key = key;
+    L.valid = true;
+  }
+  return finish(ctx, L.op, out);
+}
+
+extern "C" int tj_get_oper(tj_ctx *ctx, int side, int dia, const tj_chain *chain, const tj_block *st_oper, int old_idx,
+                           int new_idx, int truns, char types, tj_block_result *out) {
+  using namespace tjb;
+  if (!chain || !st_oper || (side != 0 && side != 1) || (chain->n > 0 && (!chain->bsm || !chain->truns)))
+    return set_err(TJ_ERR_ARG, "tj_get_oper: bad argument");
+  uint64_t h = 1469598103934665603ull;
+  const int args[6] = {1, side, dia, old_idx, new_idx, truns};
+  h = fnv(h, args, sizeof args);
+  h = fnv(h, &types, 1);
+  h = key_block(h, *st_oper);
+  h = key_chain(h, chain);
+  return meas_call(ctx, h, out, [&](DevOp &res, std::string &msg) -> int {
+    const int i1 = std::min(old_idx, new_idx), i2 = std::max(old_idx, new_idx);
+    const SiteOp site = site_of(*st_oper);
+    auto chain_ok = [&](int i) { return i >= 1 && i <= chain->n; };
+    DevOp cur;
+    int rc;
+    if (i1 <= i2 - 1) {
+      if (i1 <= 1) {
+        if ((rc = upload_op(ctx, *st_oper, cur))) return rc;
+      } else {
+        if (!chain_ok(i1)) {
+          msg = "chain index out of range";
+          return TJ_ERR_ARG;
+        }
+        const tj_basis *bs = &chain->bsm[i1 - 1];
+        EBlk e = enlarge(bs, nullptr, &site, dia != 0, side, types);
+        if (i1 <= chain->trun_idx) {
+          IdTrun id(bs);
+          rc = trunc_step(ctx, e, dia != 0, bs->len, id.blk, bs, nullptr, cur, msg);
+        } else {
+          rc = trunc_step(ctx, e, dia != 0, bs->len, chain->truns[i1 - 1], bs, nullptr, cur, msg);
+        }
+        if (rc) return rc;
+      }
+      return carry_dev(ctx, chain, side, dia != 0, types, cur, i1, i2, truns != 0, res, msg);
+    }
+    if (!chain_ok(i2) && !(i1 <= 1 && !truns)) {
+      msg = "chain index out of range";
+      return TJ_ERR_ARG;
+    }
+    if (i1 <= 1) {   // block_transfer(st_oper), then the optional truncation
+      if (!truns) return upload_op(ctx, *st_oper, res);
+      if ((rc = upload_op(ctx, *st_oper, cur))) return rc;
+      return trunc_step(ctx, as_pieces(cur), dia != 0, cur.b.len, chain->truns[i2 - 1], &chain->bsm[i2 - 1],
+                        cur.buf.d(), res, msg);
+    }
+    const tj_basis *bs = &chain->bsm[i2 - 1];
+    EBlk e = enlarge(bs, nullptr, &site, dia != 0, side, types);
+    if (truns) return trunc_step(ctx, e, dia != 0, bs->len, chain->truns[i2 - 1], bs, nullptr, res, msg);
+    IdTrun id(bs);
+    return trunc_step(ctx, e, dia != 0, bs->len, id.blk, bs, nullptr, res, msg);
+  }, "tj_get_oper");
+}
+
+extern "C" int tj_change_oper(tj_ctx *ctx, int side, int dia, const tj_chain *chain, const tj_block *old_oper,
+                              int old_idx, int new_idx, int truns, char types, tj_block_result *out) {
+  using namespace tjb;
+  if (!chain || !old_oper || (side != 0 && side != 1) || (chain->n > 0 && (!chain->bsm || !chain->truns)))
+    return set_err(TJ_ERR_ARG, "tj_change_oper: bad argument");
+  uint64_t h = 1469598103934665603ull;
+  const int args[6] = {2, side, dia, old_idx, new_idx, truns};
+  h = fnv(h, args, sizeof args);
+  h = fnv(h, &types, 1);
+  h = key_block(h, *old_oper);
+  h = key_chain(h, chain);
+  return meas_call(ctx, h, out, [&](DevOp &res, std::string &msg) -> int {
+    const int i1 = std::min(old_idx, new_idx), i2 = std::max(old_idx, new_idx);
+    int rc;
+    if (i1 <= i2 - 1) {
+      DevOp cur;
+      if ((rc = upload_op(ctx, *old_oper, cur))) return rc;
+      return carry_dev(ctx, chain, side, dia != 0, types, cur, i1, i2, truns != 0, res, msg);
+    }
+    return upload_op(ctx, *old_oper, res);
+  }, "tj_change_oper");
+}
+
+extern "C" int tj_update_trun(tj_ctx *ctx, int dia, const tj_block *ori, const tj_block *trun, tj_block_result *out) {
+  using namespace tjb;
+  if (!ori || !trun) return set_err(TJ_ERR_ARG, "tj_update_trun: null argument");
+  uint64_t h = 1469598103934665603ull;
+  const int args[2] = {3, dia};
+  h = fnv(h, args, sizeof args);
+  h = key_block(key_block(h, *ori), *trun);
+  return meas_call(ctx, h, out, [&](DevOp &res, std::string &msg) -> int {
+    DevOp cur;
+    int rc;
+    if ((rc = upload_op(ctx, *ori, cur))) return rc;
+    tj_basis none;   // the truncation reads trun's sectors only
+    std::memset(&none, 0, sizeof none);
+    return trunc_step(ctx, as_pieces(cur), dia != 0, ori->len, *trun, &none, cur.buf.d(), res, msg);
+  }, "tj_update_trun");
+}
+
+extern "C" int tj_block_mul_block_ndia(tj_ctx *ctx, const tj_block *oper1, char flag1, const tj_block *oper2,
+                                       char flag2, double coef, int down_dif, const tj_basis *basis,
+                                       tj_block_result *out) {
+  using namespace tjb;
+  if (!oper1 || !oper2 || !basis || !basis->sub) return set_err(TJ_ERR_ARG, "tj_block_mul_block_ndia: null argument");
+  if ((flag1 != 'N' && flag1 != 'T') || (flag2 != 'N' && flag2 != 'T'))
+    return set_err(TJ_ERR_ARG, "tj_block_mul_block_ndia: flags must be 'N' or 'T'");
+  uint64_t h = 1469598103934665603ull;
+  const int args[2] = {4, down_dif};
+  h = fnv(h, args, sizeof args);
+  h = fnv(h, &flag1, 1);
+  h = fnv(h, &flag2, 1);
+  h = fnv(h, &coef, sizeof coef);
+  h = key_block(key_block(h, *oper1), *oper2);
+  h = fnv(h, basis, sizeof *basis);
+  h = fnv(h, basis->sub, sizeof(tj_basis_map) * basis->num);
+  return meas_call(ctx, h, out, [&](DevOp &res, std::string &msg) -> int {
+    HpsiPlan P;
+    RBlk a, b;
+    load_block(*oper1, a, P);
+    load_block(*oper2, b, P);
+    int rc;
+    DevOp src;
+    if ((rc = src.buf.reserve(sizeof(double) * (P.ops_len + 4)))) return rc;
+    for (const auto &u : P.uploads)
+      if (u.n > 0)
+        CKR(cudaMemcpyAsync(src.buf.d() + u.dst, u.src, sizeof(double) * u.n, cudaMemcpyHostToDevice, ctx->stream));
+    auto find_bs = [&](int nu, int nd) {
+      for (int x = 0; x < basis->num; ++x)
+        if (basis->sub[x].new_num_up == nu && basis->sub[x].new_num_down == nd) return x;
+      return -1;
+    };
+    const int up1 = flag1 == 'N' ? a.up_dif : -a.up_dif, up2 = flag2 == 'N' ? b.up_dif : -b.up_dif;
+    const int up_dif = up1 + up2, d2 = b.down_dif;
+    res.b.len = basis->len;
+    res.b.up_dif = up_dif;
+    res.b.down_dif = down_dif;
+    res.b.sub.clear();
+    res.dim = 0;
+    int64_t out_len = 0;
+    for (int i = 0; i < basis->num; ++i) {
+      const int nu = basis->sub[i].new_num_up, nd = basis->sub[i].new_num_down, nnu = nu + up_dif;
+      for (int nnd = std::abs(nd - down_dif); nnd <= nd + down_dif; nnd += 2) {
+        const int x = find_bs(nnu, nnd);
+        if (x < 0) continue;
+        const int old_dim = basis->sub[i].dim, new_dim = basis->sub[x].dim;
+        res.b.sub.push_back(RSub{nu, nd, nnd - nd, new_dim, old_dim, out_len});
+        res.dim += old_dim;
+        Cell cl;
+        std::memset(&cl, 0, sizeof cl);
+        cl.off = out_len;
+        cl.ld = std::max(1, new_dim);
+        cl.M = new_dim;
+        cl.N = old_dim;
+        cl.space = SP_PSI;
+        cl.t_begin = (int32_t)P.tasks2.size();
+        // the coupled product's 3j normalisation (block.f90:2138-2145), with the
+        // operator's total transfer down_dif (new_oper%down_dif)
+        const int kq = nnd - nd;
+        const double c11 = w3j(nnd, down_dif, nd, -nnd, kq, nd);
+        for (int mnd = std::abs(nd - d2); mnd <= nd + d2; mnd += 2) {
+          const int m2u = flag2 == 'N' ? nu : nu + up2, m2d = flag2 == 'N' ? nd : mnd;
+          const int dd22 = flag2 == 'N' ? mnd - nd : nd - mnd;
+          const int m1u = flag1 == 'N' ? nu + up2 : nnu, m1d = flag1 == 'N' ? mnd : nnd;
+          const int dd11 = flag1 == 'N' ? nnd - mnd : mnd - nnd;
+          const int i2 = b.find(m2u, m2d, dd22, true), i1 = a.find(m1u, m1d, dd11, true);
+          if (i1 < 0 || i2 < 0) continue;
+          if (c11 == 0.0) {
+            msg = "vanishing 3j normalisation";
+            return TJ_ERR_NUMERIC;
+          }
+          double c1 = 0.0;
+          for (int jj6 = -mnd; jj6 <= mnd; jj6 += 2) {
+            const int a5 = nnd - jj6, b5 = jj6 - nd;
+            double c12 = w3j(nnd, a.down_dif, mnd, -nnd, a5, jj6);
+            c12 *= w3j(mnd, b.down_dif, nd, -jj6, b5, nd) * m1((mnd - jj6) / 2);
+            c12 *= w3j(a.down_dif, b.down_dif, down_dif, a5, b5, -kq) * m1((-a.down_dif + b.down_dif + kq) / 2) *
+                   std::sqrt(down_dif + 1.0);
+            c1 += c12;
+          }
+          if (c1 == 0.0) continue;
+          c1 = coef * c1 / c11;
+          const RSub &A = a.sub[i1], &Bq = b.sub[i2];
+          const int mid = flag1 == 'N' ? A.sdim : A.row_dim;
+          if ((flag1 == 'N' ? A.row_dim : A.sdim) != new_dim || (flag2 == 'N' ? Bq.sdim : Bq.row_dim) != old_dim ||
+              (flag2 == 'N' ? Bq.row_dim : Bq.sdim) != mid) {
+            msg = "operator dimensions disagree with the basis";
+            return TJ_ERR_QN;
+          }
+          Task t;
+          std::memset(&t, 0, sizeof t);
+          t.L.off = A.off;
+          t.L.ld = std::max(1, A.row_dim);
+          t.L.space = SP_OPS;
+          t.L.trans = flag1 == 'T';
+          t.R.off = Bq.off;
+          t.R.ld = std::max(1, Bq.row_dim);
+          t.R.space = SP_OPS;
+          t.R.trans = flag2 == 'T';
+          t.coef = c1;
+          t.K = mid;
+          P.tasks2.push_back(t);
+          P.flops += 2.0 * new_dim * old_dim * (double)mid;
+        }
+        cl.t_end = (int32_t)P.tasks2.size();
+        if (cl.t_end > cl.t_begin && new_dim > 0 && old_dim > 0) P.cells2.push_back(cl);
+        out_len += (int64_t)new_dim * old_dim;
+      }
+    }
+    split_tiles(P.cells2, P.tasks2, P.tiles2, P.red2, P.nslots2, false);
+    if ((rc = res.buf.reserve(sizeof(double) * (out_len + 4)))) return rc;
+    CKR(cudaMemsetAsync(res.buf.p, 0, sizeof(double) * (out_len + 4), ctx->stream));
+    return exec_passes(ctx, P, src.buf.d(), nullptr, res.buf.d());
+  }, "tj_block_mul_block_ndia");
 }

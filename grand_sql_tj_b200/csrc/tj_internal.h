@@ -131,6 +131,8 @@ void merge_plans(const std::vector<const HpsiPlan *> &parts, HpsiPlan &out, std:
 
 // Racah 6j symbol on doubled spins (host); same formula as the reference's W6JS.
 double w6j(int j1, int j2, int j3, int l1, int l2, int l3);
+// Wigner 3j symbol on doubled spins and projections (Racah's sum)
+double w3j(int j1, int j2, int j3, int m1, int m2, int m3);
 
 // Correlator plans: one cell list whose epilogue dots with psi instead of storing.
 enum CorKind {

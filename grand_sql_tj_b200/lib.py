@@ -13,9 +13,9 @@ from typing import Optional, Tuple
 
 import numpy as np
 
-from .structs import (Block, TjBasis, TjBlock, TjBlockSet, TjBlockSub, TjGgCell, TjGgTerm, TjHpsiStats, TjLattice,
-                      TjModel, TjModelResult, TjTruncResult, TjTuneResult, TjWave, Wave, block_from_c_result,
-                      call_model_result)
+from .structs import (Block, TjBasis, TjBlock, TjBlockResult, TjBlockSet, TjBlockSub, TjChain, TjGgCell, TjGgTerm,
+                      TjHpsiStats, TjLattice, TjModel, TjModelResult, TjTruncResult, TjTuneResult, TjWave, Wave,
+                      block_from_c_result, call_block_result, call_model_result)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtjb200.so")
@@ -202,6 +202,16 @@ def lib():
                                     P(TjWave)]
         L.tj_wave_trans_plan_export.argtypes = [C.c_int, P(TjBasis), P(TjBasis), P(TjBlock), P(TjBlock), P(TjWave),
                                                 P(TjWave), P(PlanExport)]
+        L.tj_get_oper.argtypes = [C.c_void_p, C.c_int, C.c_int, P(TjChain), P(TjBlock), C.c_int, C.c_int, C.c_int,
+                                  C.c_char, P(TjBlockResult)]
+        L.tj_change_oper.argtypes = L.tj_get_oper.argtypes
+        L.tj_update_trun.argtypes = [C.c_void_p, C.c_int, P(TjBlock), P(TjBlock), P(TjBlockResult)]
+        L.tj_block_mul_block_ndia.argtypes = [C.c_void_p, P(TjBlock), C.c_char, P(TjBlock), C.c_char, C.c_double,
+                                              C.c_int, P(TjBasis), P(TjBlockResult)]
+        L.tj_w6js.restype = C.c_double
+        L.tj_w6js.argtypes = [C.c_int] * 6
+        L.tj_w3js.restype = C.c_double
+        L.tj_w3js.argtypes = [C.c_int] * 6
         for n in ("tj_measure_sys_block", "tj_measure_env_block"):
             getattr(L, n).argtypes = [C.c_void_p, P(TjBlock), P(TjBasis), P(TjWave), P(C.c_double)]
         L.tj_sys_block_env_block_cor_dia.argtypes = [C.c_void_p, P(TjBlock), P(TjBlock), P(TjBasis),
@@ -355,6 +365,41 @@ class Context:
                                  C.byref(old.c), C.byref(new_wave.c)))
         return new_wave
 
+    def get_oper(self, side: int, dia: int, chain, st_oper: Block, old_idx: int, new_idx: int, truns: bool,
+                 types: str = "B") -> Block:
+        """Get_{sys,env}_oper_{dia,ndia} (get_sys.f90:764-1130); chain: structs.PackedChain."""
+        ps = st_oper.pack()
+        rc, b = call_block_result(lambda r: lib().tj_get_oper(self.h, side, int(dia), C.byref(chain.c), C.byref(ps.c),
+                                                              old_idx, new_idx, int(truns), types.encode(), r))
+        _chk(rc)
+        return b
+
+    def change_oper(self, side: int, dia: int, chain, old_oper: Block, old_idx: int, new_idx: int, truns: bool,
+                    types: str = "B") -> Block:
+        """Change_{sys,env}_oper_{dia,ndia} (get_sys.f90:893-1238)."""
+        ps = old_oper.pack()
+        rc, b = call_block_result(lambda r: lib().tj_change_oper(self.h, side, int(dia), C.byref(chain.c),
+                                                                 C.byref(ps.c), old_idx, new_idx, int(truns),
+                                                                 types.encode(), r))
+        _chk(rc)
+        return b
+
+    def update_trun(self, dia: int, ori: Block, trun: Block) -> Block:
+        """update_trun_dia / update_trun_ndia (block.f90:1311-1503)."""
+        po, pt = ori.pack(), trun.pack()
+        rc, b = call_block_result(lambda r: lib().tj_update_trun(self.h, int(dia), C.byref(po.c), C.byref(pt.c), r))
+        _chk(rc)
+        return b
+
+    def block_mul_block_ndia(self, o1: Block, f1: str, o2: Block, f2: str, coef: float, down_dif: int, basis) -> Block:
+        """block_mul_block_ndia (block.f90:1956-2197)."""
+        p1, p2, pb = o1.pack(), o2.pack(), basis.pack()
+        rc, b = call_block_result(lambda r: lib().tj_block_mul_block_ndia(self.h, C.byref(p1.c), f1.encode(),
+                                                                          C.byref(p2.c), f2.encode(), coef, down_dif,
+                                                                          C.byref(pb.c), r))
+        _chk(rc)
+        return b
+
     def truncation(self, wave: Wave, side: int, kept_min: int, kept_max: int, trun_err: float):
         """Get_density_matrix_{sys,env}_new + Get_truncation_operator (den_mat.f90)."""
         r = TjTruncResult()
@@ -465,6 +510,21 @@ class DeviceBackend:
 
     def wave_trans(self, direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave):
         return self.ctx.wave_trans(direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave)
+
+    def get_oper(self, side, dia, chain, st_oper, old_idx, new_idx, truns, types="B"):
+        return self.ctx.get_oper(side, dia, chain, st_oper, old_idx, new_idx, truns, types)
+
+    def change_oper(self, side, dia, chain, old_oper, old_idx, new_idx, truns, types="B"):
+        return self.ctx.change_oper(side, dia, chain, old_oper, old_idx, new_idx, truns, types)
+
+    def update_trun(self, dia, ori, trun):
+        return self.ctx.update_trun(dia, ori, trun)
+
+    def block_mul_block_ndia(self, o1, f1, o2, f2, coef, down_dif, basis):
+        return self.ctx.block_mul_block_ndia(o1, f1, o2, f2, coef, down_dif, basis)
+
+    def correlator(self, name, a, b, sys_bs, env_bs, wave, flag="B"):
+        return self.ctx.correlator(name, a, b, sys_bs, env_bs, wave, flag)
 
 
 def pack_superblock(sb):

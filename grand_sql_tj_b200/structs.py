@@ -90,6 +90,16 @@ class TjModelResult(C.Structure):
                 ("data", c_double_p), ("model", TjModel)]
 
 
+class TjBlockResult(C.Structure):
+    _fields_ = [("num", C.c_int32), ("pad_", C.c_int32), ("data_len", C.c_int64),
+                ("subs", C.POINTER(TjBlockSub)), ("data", c_double_p), ("block", TjBlock)]
+
+
+class TjChain(C.Structure):
+    _fields_ = [("n", C.c_int32), ("trun_idx", C.c_int32), ("bsm", C.POINTER(TjBasis)),
+                ("truns", C.POINTER(TjBlock))]
+
+
 class TjHpsiStats(C.Structure):
     _fields_ = [("flops", C.c_double), ("flops_ref", C.c_double), ("bytes", C.c_double),
                 ("n_products", C.c_int64), ("n_tasks", C.c_int64), ("n_tiles_p1", C.c_int64),
@@ -391,6 +401,42 @@ def model_from_c(m: TjModel, data: np.ndarray, keep=None) -> Model:
     if keep is not None:
         out._packed = _ResultPack(m, data, keep)
     return out
+
+
+def call_block_result(call):
+    """Runs a two-call block-result entry point `call(res_ptr) -> rc`; returns (rc, Block)."""
+    res = TjBlockResult()
+    rc = call(C.byref(res))
+    if rc:
+        return rc, None
+    subs = (TjBlockSub * max(res.num, 1))()
+    data = np.zeros(max(res.data_len, 1))
+    res.subs = C.cast(subs, C.POINTER(TjBlockSub))
+    res.data = data.ctypes.data_as(c_double_p)
+    rc = call(C.byref(res))
+    if rc:
+        return rc, None
+    return 0, _block_from_c(res.block, data)
+
+
+class PackedChain:
+    """tj_chain of one side's measurement tables: bases[i] / truns[i] for block
+    length i (dicts keyed by length, as the sweep driver stores them)."""
+
+    def __init__(self, n: int, bases: dict, truns: dict, trun_idx: int = 1):
+        self.bsm = (TjBasis * max(n, 1))()
+        self.truns = (TjBlock * max(n, 1))()
+        self.keep = []
+        for i in range(2, n + 1):
+            if i in bases:
+                pb = bases[i].pack()
+                self.keep.append(pb)
+                self.bsm[i - 1] = pb.c
+            if i in truns and i > trun_idx:
+                pt = truns[i].pack()
+                self.keep.append(pt)
+                self.truns[i - 1] = pt.c
+        self.c = TjChain(n, trun_idx, C.cast(self.bsm, C.POINTER(TjBasis)), C.cast(self.truns, C.POINTER(TjBlock)))
 
 
 def block_from_c_result(res: TjTruncResult, length: int) -> Block:

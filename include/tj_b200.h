@@ -161,6 +161,12 @@ const char *tj_last_error(void);
 int tj_host_register(void *p, size_t bytes);
 int tj_host_unregister(void *p);
 
+/* W6JS / W3JS (code/tjsq/block.f90:1564-1615, 1522-1561): the Wigner 6j and
+ * 3j symbols on doubled spins (and doubled projections), as the library's
+ * coefficient tables compute them on the host. */
+double tj_w6js(int j1, int j2, int j3, int l1, int l2, int l3);
+double tj_w3js(int j1, int j2, int j3, int m1, int m2, int m3);
+
 /* ------------------------------------------------------- hot-path calls */
 
 /* model_wave(sys,env,sys_bs,env_bs,invec,outvec)  (code/tjsq/get_sys.f90:4127-4381),
@@ -264,6 +270,58 @@ typedef struct tj_model_result {
 int tj_get_hamiltonian(tj_ctx *ctx, const tj_lattice *lat, int side, int mshift, const tj_model *pre,
                        const tj_basis *basis, const tj_block *trun, tj_model_result *out);
 
+
+/* ------------------------------------------------- measurement operators */
+
+/* A block operator written by the library, two-call pattern as above: with
+ * subs or data NULL only num and data_len are filled; then the caller
+ * allocates subs[num] and data[data_len] and calls again, and `block` is
+ * filled (its sub points to subs, its data to data). */
+typedef struct tj_block_result {
+  int32_t num, pad_;
+  int64_t data_len;
+  tj_block_sub *subs;          /* caller-allocated, num entries (or NULL)  */
+  double *data;                /* caller-allocated, data_len doubles       */
+  tj_block block;              /* second call: the operator                */
+} tj_block_result;
+
+/* The measurement chain of one side: the module arrays sys_bsm(:) /
+ * systruns(:) (or env_bsm / envtruns) that the reference's Measurement reads
+ * from disk (code/tjsq/main.f90:225-240).  bsm[i - 1] is the enlarged basis
+ * of block length i (i = 2..n; bsm[0] is not read) and truns[i - 1] its
+ * truncation operator (read for i > trun_idx; lengths <= trun_idx are kept
+ * untruncated, as the reference's trun_idx). */
+typedef struct tj_chain {
+  int32_t n, trun_idx;
+  const tj_basis *bsm;
+  const tj_block *truns;
+} tj_chain;
+
+/* Get_sys_oper_dia / Get_env_oper_dia / Get_sys_oper_ndia / Get_env_oper_ndia
+ * (code/tjsq/get_sys.f90:764-891, 998-1130): the one-site operator st_oper
+ * placed at site old_idx (counted from the block's open end) and carried
+ * through the chain to a block of length new_idx (the enlarged basis of
+ * length new_idx; with truns != 0 truncated by its truncation operator).
+ * side 0: system chain, 1: environment chain; dia != 0: the _dia routines
+ * (down_dif = 0 operators), else the _ndia routines with types 'F' or 'B'.
+ * Each step of the chain (enlarge by one site, truncate) is one pair of
+ * grouped-GEMM launches; the operator stays on the device between steps. */
+int tj_get_oper(tj_ctx *ctx, int side, int dia, const tj_chain *chain, const tj_block *st_oper, int old_idx,
+                int new_idx, int truns, char types, tj_block_result *out);
+/* Change_sys_oper_dia / Change_env_oper_dia / Change_sys_oper_ndia /
+ * Change_env_oper_ndia (code/tjsq/get_sys.f90:893-996, 1134-1238): a block
+ * operator of block length old_idx carried to block length new_idx. */
+int tj_change_oper(tj_ctx *ctx, int side, int dia, const tj_chain *chain, const tj_block *old_oper, int old_idx,
+                   int new_idx, int truns, char types, tj_block_result *out);
+/* block_mul_block_ndia(oper1,Flag1,oper2,Flag2,coef,new_oper,basis)
+ * (code/tjsq/block.f90:1956-2197): the product of two operators of one block
+ * coupled to total spin transfer down_dif (the caller's new_oper%down_dif),
+ * with the Wigner 3j recoupling; flag 'N' or 'T' per operand. */
+int tj_block_mul_block_ndia(tj_ctx *ctx, const tj_block *oper1, char flag1, const tj_block *oper2, char flag2,
+                            double coef, int down_dif, const tj_basis *basis, tj_block_result *out);
+/* update_trun_dia (dia != 0) / update_trun_ndia (code/tjsq/block.f90:1311-
+ * 1503): U^T O U of a block operator by a truncation operator. */
+int tj_update_trun(tj_ctx *ctx, int dia, const tj_block *ori, const tj_block *trun, tj_block_result *out);
 
 /* ------------------------------------------------ wavefunction prediction */
 

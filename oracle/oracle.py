@@ -14,8 +14,9 @@ import subprocess
 
 import numpy as np
 
-from grand_sql_tj_b200.structs import (TjBasis, TjBlock, TjLattice, TjModel, TjModelResult, TjTruncResult,
-                                       TjWave, TjBlockSub, Block, block_from_c_result, call_model_result)
+from grand_sql_tj_b200.structs import (TjBasis, TjBlock, TjBlockResult, TjChain, TjLattice, TjModel, TjModelResult,
+                                       TjTruncResult, TjWave, TjBlockSub, Block, block_from_c_result,
+                                       call_block_result, call_model_result)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle_tj.so")
@@ -74,6 +75,12 @@ def lib(threads: int = 1):
         L.ora_get_hamiltonian.argtypes = [P(TjLattice), C.c_int, C.c_int, P(TjModel), P(TjBasis), P(TjBlock),
                                           P(TjModelResult)]
         L.ora_wave_trans.argtypes = [C.c_int, P(TjBasis), P(TjBasis), P(TjBlock), P(TjBlock), P(TjWave), P(TjWave)]
+        L.ora_get_oper.argtypes = [C.c_int, C.c_int, P(TjChain), P(TjBlock), C.c_int, C.c_int, C.c_int, C.c_char,
+                                   P(TjBlockResult)]
+        L.ora_change_oper.argtypes = L.ora_get_oper.argtypes
+        L.ora_block_mul_block_ndia.argtypes = [P(TjBlock), C.c_char, P(TjBlock), C.c_char, C.c_double, C.c_int,
+                                               P(TjBasis), P(TjBlockResult)]
+        L.ora_update_trun.argtypes = [C.c_int, P(TjBlock), P(TjBlock), P(TjBlockResult)]
         L.ora_site_operator.argtypes = [C.c_int, C.c_int, P(TjBlock), P(TjBlockSub), P(C.c_double)]
         rc = L.ora_init(openblas_path().encode(), threads)
         if rc:
@@ -210,6 +217,43 @@ def wave_trans(direction: int, sys_bs, env_bs, sys_trun, env_trun, old, new_wave
     return new_wave
 
 
+def get_oper(side, dia, chain, st_oper, old_idx, new_idx, truns, types="B"):
+    """Get_{sys,env}_oper_{dia,ndia}: chain is a structs.PackedChain."""
+    L = lib()
+    ps = st_oper.pack()
+    rc, b = call_block_result(lambda r: L.ora_get_oper(side, int(dia), C.byref(chain.c), C.byref(ps.c), old_idx,
+                                                       new_idx, int(truns), types.encode(), r))
+    _chk(rc)
+    return b
+
+
+def change_oper(side, dia, chain, old_oper, old_idx, new_idx, truns, types="B"):
+    """Change_{sys,env}_oper_{dia,ndia}."""
+    L = lib()
+    ps = old_oper.pack()
+    rc, b = call_block_result(lambda r: L.ora_change_oper(side, int(dia), C.byref(chain.c), C.byref(ps.c), old_idx,
+                                                          new_idx, int(truns), types.encode(), r))
+    _chk(rc)
+    return b
+
+
+def block_mul_block_ndia(o1, f1, o2, f2, coef, down_dif, basis):
+    L = lib()
+    p1, p2, pb = o1.pack(), o2.pack(), basis.pack()
+    rc, b = call_block_result(lambda r: L.ora_block_mul_block_ndia(C.byref(p1.c), f1.encode(), C.byref(p2.c),
+                                                                   f2.encode(), coef, down_dif, C.byref(pb.c), r))
+    _chk(rc)
+    return b
+
+
+def update_trun(dia, ori, trun):
+    L = lib()
+    po, pt = ori.pack(), trun.pack()
+    rc, b = call_block_result(lambda r: L.ora_update_trun(int(dia), C.byref(po.c), C.byref(pt.c), r))
+    _chk(rc)
+    return b
+
+
 class OracleBackend:
     """The hot-path calls of grand_sql_tj_b200.sweep.Dmrg on the oracle (CPU)."""
 
@@ -225,3 +269,18 @@ class OracleBackend:
 
     def wave_trans(self, direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave):
         return wave_trans(direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave)
+
+    def get_oper(self, side, dia, chain, st_oper, old_idx, new_idx, truns, types="B"):
+        return get_oper(side, dia, chain, st_oper, old_idx, new_idx, truns, types)
+
+    def change_oper(self, side, dia, chain, old_oper, old_idx, new_idx, truns, types="B"):
+        return change_oper(side, dia, chain, old_oper, old_idx, new_idx, truns, types)
+
+    def block_mul_block_ndia(self, o1, f1, o2, f2, coef, down_dif, basis):
+        return block_mul_block_ndia(o1, f1, o2, f2, coef, down_dif, basis)
+
+    def update_trun(self, dia, ori, trun):
+        return update_trun(dia, ori, trun)
+
+    def correlator(self, name, a, b, sys_bs, env_bs, wave, flag="B"):
+        return correlator(name, a, b, sys_bs, env_bs, wave, flag)

@@ -2623,3 +2623,254 @@ int ora_wave_trans(int direction, const tj_basis *sys_bs, const tj_basis *env_bs
   blk_free(&et);
   return 0;
 }
+
+/* ============================================ measurement operators */
+static void put_block_result(const OBlk *b, tj_block_result *out) {
+  out->num = b->num;
+  int64_t n = 0;
+  for (int i = 0; i < b->num; i++) n += (int64_t)b->sub[i].row_dim * b->sub[i].sdim;
+  out->data_len = n;
+  if (!out->subs || !out->data) return;
+  int64_t off = 0;
+  for (int i = 0; i < b->num; i++) {
+    const OSub *s = &b->sub[i];
+    const int64_t m = (int64_t)s->row_dim * s->sdim;
+    out->subs[i] = (tj_block_sub){s->num_up, s->num_down, s->down_dif, s->row_dim, s->sdim, 0, off};
+    memcpy(out->data + off, s->mat, (size_t)m * sizeof(double));
+    off += m;
+  }
+  out->block = (tj_block){b->len, b->num, b->dim, b->up_dif, b->down_dif, 0, out->subs, out->data};
+}
+/* one enlargement of a block operator (update_block_dia / update_block_ndia_sys/env) */
+static void enlarge_block(const OBlk *o, const tj_basis *bs, int side, int dia, char types, OBlk *out) {
+  if (dia)
+    upd_block_dia(o, bs, out);
+  else
+    upd_block_ndia(o, bs, out, side, types);
+}
+static void truncate_op(const OBlk *o, const OBlk *trun, int dia, OBlk *out) {
+  if (dia)
+    upd_trun_dia(o, trun, out);
+  else
+    upd_trun_ndia(o, trun, out);
+}
+static int chain_check(const tj_chain *ch, int idx) {
+  if (!ch || idx < 1 || idx > ch->n || !ch->bsm || !ch->truns) return fail(TJ_ERR_ARG, "chain index out of range");
+  return 0;
+}
+/* the loop shared by Get_*_oper_* and Change_*_oper_*: from a block operator
+ * of length idx carried (enlarge, then truncate unless idx <= trun_idx) to
+ * the enlarged basis of length idx_two, truncated there when truns */
+static int carry(const tj_chain *ch, int side, int dia, char types, OBlk *op, int idx, int idx_two, int truns,
+                 OBlk *res) {
+  while (idx + 1 <= idx_two - 1) {
+    if (chain_check(ch, idx + 1)) return TJ_ERR_ARG;
+    OBlk mid;
+    enlarge_block(op, &ch->bsm[idx], side, dia, types, &mid);
+    blk_free(op);
+    idx++;
+    if (idx <= ch->trun_idx) {
+      *op = mid;
+    } else {
+      OBlk t;
+      blk_view(&ch->truns[idx - 1], &t);
+      truncate_op(&mid, &t, dia, op);
+      blk_free(&t);
+      blk_free(&mid);
+    }
+  }
+  if (chain_check(ch, idx + 1)) return TJ_ERR_ARG;
+  enlarge_block(op, &ch->bsm[idx], side, dia, types, res);
+  blk_free(op);
+  if (truns) {
+    OBlk t, r2;
+    blk_view(&ch->truns[idx_two - 1], &t);
+    truncate_op(res, &t, dia, &r2);
+    blk_free(&t);
+    blk_free(res);
+    *res = r2;
+  }
+  return 0;
+}
+/* Get_sys_oper_dia / Get_env_oper_dia / Get_sys_oper_ndia / Get_env_oper_ndia
+ * (get_sys.f90:764-891, 998-1130) */
+int ora_get_oper(int side, int dia, const tj_chain *ch, const tj_block *st_oper, int old_idx, int new_idx,
+                 int truns, char types, tj_block_result *out) {
+  if (!p_dgemm) return fail(TJ_ERR_ARG, "oracle not initialised (ora_init)");
+  const int i1 = old_idx < new_idx ? old_idx : new_idx, i2 = old_idx < new_idx ? new_idx : old_idx;
+  OBlk st, op, res;
+  memset(&res, 0, sizeof res);
+  blk_view(st_oper, &st);
+  int rc = 0;
+  if (i1 <= i2 - 1) {
+    if (i1 <= 1) {
+      blk_copy(&st, &op);
+    } else {
+      if ((rc = chain_check(ch, i1))) goto out;
+      OBlk mid;
+      if (dia) upd_site_dia(&st, &ch->bsm[i1 - 1], &mid);
+      else upd_site_ndia(&st, &ch->bsm[i1 - 1], &mid, side, types);
+      if (i1 <= ch->trun_idx) {
+        op = mid;
+      } else {
+        OBlk t;
+        blk_view(&ch->truns[i1 - 1], &t);
+        truncate_op(&mid, &t, dia, &op);
+        blk_free(&t);
+        blk_free(&mid);
+      }
+    }
+    rc = carry(ch, side, dia, types, &op, i1, i2, truns, &res);
+    if (rc) goto out;
+  } else {
+    if (i1 <= 1) {
+      blk_copy(&st, &res);
+    } else {
+      if ((rc = chain_check(ch, i2))) goto out;
+      if (dia) upd_site_dia(&st, &ch->bsm[i2 - 1], &res);
+      else upd_site_ndia(&st, &ch->bsm[i2 - 1], &res, side, types);
+    }
+    if (truns) {
+      if ((rc = chain_check(ch, i2))) goto out;
+      OBlk t, r2;
+      blk_view(&ch->truns[i2 - 1], &t);
+      truncate_op(&res, &t, dia, &r2);
+      blk_free(&t);
+      blk_free(&res);
+      res = r2;
+    }
+  }
+  put_block_result(&res, out);
+out:
+  blk_free(&res);
+  blk_free(&st);
+  return rc;
+}
+/* Change_sys_oper_dia / Change_env_oper_dia / Change_sys_oper_ndia /
+ * Change_env_oper_ndia (get_sys.f90:893-996, 1134-1238) */
+int ora_change_oper(int side, int dia, const tj_chain *ch, const tj_block *old_oper, int old_idx, int new_idx,
+                    int truns, char types, tj_block_result *out) {
+  if (!p_dgemm) return fail(TJ_ERR_ARG, "oracle not initialised (ora_init)");
+  const int i1 = old_idx < new_idx ? old_idx : new_idx, i2 = old_idx < new_idx ? new_idx : old_idx;
+  OBlk in, op, res;
+  memset(&res, 0, sizeof res);
+  blk_view(old_oper, &in);
+  int rc = 0;
+  if (i1 <= i2 - 1) {
+    blk_copy(&in, &op);
+    rc = carry(ch, side, dia, types, &op, i1, i2, truns, &res);
+    if (rc) goto out;
+  } else {
+    blk_copy(&in, &res);
+  }
+  put_block_result(&res, out);
+out:
+  blk_free(&res);
+  blk_free(&in);
+  return rc;
+}
+/* block_mul_block_ndia (block.f90:1956-2197) */
+int ora_block_mul_block_ndia(const tj_block *o1b, char f1, const tj_block *o2b, char f2, double coef, int down_dif,
+                             const tj_basis *bs, tj_block_result *out) {
+  if (!p_dgemm) return fail(TJ_ERR_ARG, "oracle not initialised (ora_init)");
+  OBlk o1, o2;
+  blk_view(o1b, &o1);
+  blk_view(o2b, &o2);
+  const int up1 = f1 == 'N' ? o1.up_dif : -o1.up_dif, up2 = f2 == 'N' ? o2.up_dif : -o2.up_dif;
+  const int d2 = o2.down_dif;
+  const int up_dif = up1 + up2;
+  int num = 0;
+  for (int i = 0; i < bs->num; i++) {
+    int nu = bs->sub[i].new_num_up, nd = bs->sub[i].new_num_down;
+    for (int nnd = abs(nd - down_dif); nnd <= nd + down_dif; nnd += 2)
+      if (find_bs(bs, nu + up_dif, nnd) >= 0) num++;
+  }
+  OBlk nb;
+  blk_new(&nb, bs->len, num, up_dif, down_dif);
+  int id = 0;
+  for (int i = 0; i < bs->num; i++) {
+    const int nu = bs->sub[i].new_num_up, nd = bs->sub[i].new_num_down, nnu = nu + up_dif;
+    for (int nnd = abs(nd - down_dif); nnd <= nd + down_dif; nnd += 2) {
+      const int x = find_bs(bs, nnu, nnd);
+      if (x < 0) continue;
+      const int old_dim = bs->sub[i].dim, new_dim = bs->sub[x].dim;
+      OSub *S = &nb.sub[id++];
+      *S = (OSub){nu, nd, nnd - nd, new_dim, old_dim, mat_zero(new_dim, old_dim)};
+      nb.dim += old_dim;
+      for (int mnd = abs(nd - d2); mnd <= nd + d2; mnd += 2) {
+        int m2u, m2d, dd22;
+        if (f2 == 'N') {
+          m2u = nu;
+          m2d = nd;
+          dd22 = mnd - nd;
+        } else {
+          m2u = nu + up2;
+          m2d = mnd;
+          dd22 = nd - mnd;
+        }
+        const int idx2 = find_sub(&o2, m2u, m2d, dd22, 1);
+        int m1u, m1d, dd11;
+        if (f1 == 'N') {
+          m1u = nu + up2;
+          m1d = mnd;
+          dd11 = nnd - mnd;
+        } else {
+          m1u = nnu;
+          m1d = nnd;
+          dd11 = mnd - nnd;
+        }
+        const int idx1 = find_sub(&o1, m1u, m1d, dd11, 1);
+        if (idx1 < 0 || idx2 < 0) continue;
+        int mid_dim, lda, ldb;
+        if (f1 == 'N') {
+          mid_dim = o1.sub[idx1].sdim;
+          lda = new_dim;
+        } else {
+          mid_dim = o1.sub[idx1].row_dim;
+          lda = mid_dim;
+        }
+        ldb = f2 == 'N' ? mid_dim : old_dim;
+        int j1 = nnd, j4 = -j1, j3 = nd, j6 = j3, j2 = nb.down_dif, j5 = -j4 - j6;   /* new_oper%down_dif */
+        const int kq = j5;
+        const double c11 = ora_w3js(j1, j2, j3, j4, j5, j6);
+        if (c11 == 0.0) {
+          blk_free(&nb);
+          blk_free(&o1);
+          blk_free(&o2);
+          return fail(TJ_ERR_NUMERIC, "block_mul_block_ndia: vanishing 3j normalisation");
+        }
+        double c1 = 0.0;
+        for (int jj6 = -mnd; jj6 <= mnd; jj6 += 2) {
+          const int a1 = nnd, a4 = -a1, a2 = o1.down_dif, a3 = mnd, a5 = -a4 - jj6;
+          double c12 = ora_w3js(a1, a2, a3, a4, a5, jj6);
+          const int b1 = mnd, b4 = -jj6, b2 = o2.down_dif, b3 = nd, b6 = b3, b5 = -b4 - b6;
+          c12 *= ora_w3js(b1, b2, b3, b4, b5, b6) * ipow_m1((b1 + b4) / 2);
+          const int i1 = o1.down_dif, i2 = o2.down_dif, i3 = down_dif, i4 = a5, i5 = b5, i6 = -kq;
+          c12 *= ora_w3js(i1, i2, i3, i4, i5, i6) * ipow_m1((-i1 + i2 + kq) / 2) * sqrt(i3 + 1.0);
+          c1 += c12;
+        }
+        if (c1 == 0.0) continue;
+        c1 = coef * c1 / c11;
+        dg(f1, f2, new_dim, old_dim, mid_dim, c1, o1.sub[idx1].mat, lda, o2.sub[idx2].mat, ldb, 1.0, S->mat, new_dim);
+      }
+    }
+  }
+  put_block_result(&nb, out);
+  blk_free(&nb);
+  blk_free(&o1);
+  blk_free(&o2);
+  return 0;
+}
+/* update_trun_dia / update_trun_ndia (block.f90:1311-1503) on their own */
+int ora_update_trun(int dia, const tj_block *ori, const tj_block *trunb, tj_block_result *out) {
+  if (!p_dgemm) return fail(TJ_ERR_ARG, "oracle not initialised (ora_init)");
+  OBlk o, t, r;
+  blk_view(ori, &o);
+  blk_view(trunb, &t);
+  truncate_op(&o, &t, dia, &r);
+  put_block_result(&r, out);
+  blk_free(&r);
+  blk_free(&o);
+  blk_free(&t);
+  return 0;
+}

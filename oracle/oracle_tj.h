@@ -85,6 +85,19 @@ int ora_get_hamiltonian(const tj_lattice *lat, int side, int mshift, const tj_mo
 int ora_wave_trans(int direction, const tj_basis *sys_bs, const tj_basis *env_bs, const tj_block *sys_trun,
                    const tj_block *env_trun, const tj_wave *old_wave, tj_wave *new_wave);
 
+/* Get_{sys,env}_oper_{dia,ndia} (code/tjsq/get_sys.f90:764-891, 998-1130),
+ * Change_{sys,env}_oper_{dia,ndia} (get_sys.f90:893-996, 1134-1238),
+ * block_mul_block_ndia (block.f90:1956-2197) and update_trun_dia / ndia
+ * (block.f90:1311-1503); arguments and two-call results as tj_get_oper,
+ * tj_change_oper, tj_block_mul_block_ndia and tj_update_trun. */
+int ora_get_oper(int side, int dia, const tj_chain *ch, const tj_block *st_oper, int old_idx, int new_idx,
+                 int truns, char types, tj_block_result *out);
+int ora_change_oper(int side, int dia, const tj_chain *ch, const tj_block *old_oper, int old_idx, int new_idx,
+                    int truns, char types, tj_block_result *out);
+int ora_block_mul_block_ndia(const tj_block *o1, char f1, const tj_block *o2, char f2, double coef, int down_dif,
+                             const tj_basis *basis, tj_block_result *out);
+int ora_update_trun(int dia, const tj_block *ori, const tj_block *trun, tj_block_result *out);
+
 /* Site operators of Get_site_operator_su2_U0 (code/tjsq/dmrg_sub.f90:370-473):
  * which = 0 st_elec_up, 1 st_elec_down, 2 num_elec, 3 st_sd, 4 st_si.
  * Writes at most 2 sub-blocks and 2 doubles; returns the sub count. */

@@ -208,3 +208,10 @@ def grand_canonical_ground_energy(geo):
             e, _, _ = ground_energy(geo, n)
         best = e if best is None else min(best, e)
     return best
+
+
+def density_correlation(cl, psi, i, j):
+    """<psi| n_i n_j |psi> (0-based sites i != j)."""
+    occ = cl.up | cl.dn
+    both = ((occ >> i) & 1) & ((occ >> j) & 1)
+    return float(np.sum(psi[both == 1] ** 2))

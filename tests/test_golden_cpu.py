@@ -79,3 +79,13 @@ def test_oracle_matches_frozen_results(oracle_lib, name, seed, kmin, kmax):
     assert r.num_state == int(t[0])
     assert np.allclose([r.trunc_err, r.entropy1, r.entropy2, r.entropys], t[1:], rtol=0, atol=1e-10)
     assert np.max(np.abs(np.sort(ev) - np.sort(g["rho_eigs"]))) <= 1e-12
+
+
+def test_product_w6j_w3j_exact(product_lib, symbols):
+    """The library's own 6j and 3j (the coefficient tables of every plan; the
+    3j of block_mul_block_ndia) against the same exact rational values."""
+    from grand_sql_tj_b200.lib import lib
+    L = lib()
+    w6 = max(abs(L.tj_w6js(*j) - v) / abs(v) for *j, v in symbols["w6j"])
+    w3 = max(abs(L.tj_w3js(*j) - v) / abs(v) for *j, v in symbols["w3j"])
+    assert w6 <= 1e-13 and w3 <= 1e-13, (w6, w3)
