@@ -86,6 +86,13 @@ extern "C" int tj_set_precision(tj_ctx *ctx, int mode, int slices) {
   return TJ_OK;
 }
 
+extern "C" int tj_set_wait_limit(tj_ctx *ctx, double seconds) {
+  if (!ctx) return set_err(TJ_ERR_ARG, "null context");
+  if (!(seconds >= 0.0) || seconds > 60.0) return set_err(TJ_ERR_ARG, "wait limit must be within [0, 60] seconds");
+  ctx->wait_s = seconds;
+  return TJ_OK;
+}
+
 extern "C" int tj_step_begin(tj_ctx *ctx) {
   if (!ctx) return set_err(TJ_ERR_ARG, "null context");
   ctx->plan_valid = false;
@@ -184,7 +191,7 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   uint64_t h = instance_key(1469598103934665603ull, lat, sys, env, sys_bs, env_bs, wave);
   h = fnv(h, &ctx->prec_mode, sizeof ctx->prec_mode);
   h = fnv(h, &ctx->slices, sizeof ctx->slices);
-  if (ctx->plan_valid && ctx->plan_key == h && tune_is_current(ctx)) return TJ_OK;
+  if (ctx->plan_valid && ctx->plan_key == h && tune_is_current(ctx)) return reset_device_flags(ctx);
   ctx->plan_valid = false;
   CK(cudaSetDevice(ctx->device));
   const auto t_start = std::chrono::steady_clock::now();
@@ -195,8 +202,8 @@ int tjb::prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, c
   if (rc) return set_err(rc, "H*psi plan: " + msg);
   if ((rc = install_plan(ctx, std::move(P), h, t_start))) return rc;
   if (!ctx->tuning && ctx->autotune == TJ_TUNE_ON_MISS && !tune_lookup(ctx->hist_key, ctx->tune))
-    return autotune_plan(ctx, lat, sys, env, sys_bs, env_bs, wave, nullptr);
-  return TJ_OK;
+    if ((rc = autotune_plan(ctx, lat, sys, env, sys_bs, env_bs, wave, nullptr))) return rc;
+  return reset_device_flags(ctx);
 }
 
 // Installs a compiled plan: tiling choices, operator upload and hmerge, work
@@ -294,7 +301,8 @@ int tjb::install_plan(tj_ctx *ctx, std::unique_ptr<HpsiPlan> P, uint64_t h,
     CK(cudaMemsetAsync(ctx->ozScales.p, 0, sizeof(double) * (oz->n_scales + 4), ctx->stream));
     // operator splits: once per step
     launch_oz_max((const OzJob *)ctx->ozStaMJobs.p, (int)oz->sta_mjobs.size(), (const OzSpan *)ctx->ozStaMSpans.p,
-                  (int)oz->sta_mspans.size(), ctx->ops.d(), nullptr, nullptr, ctx->ozScales.d(), ctx->stream);
+                  (int)oz->sta_mspans.size(), ctx->ops.d(), nullptr, nullptr, ctx->ozScales.d(),
+                  (int *)((char *)ctx->ozMisc.p + 64), ctx->stream);
     launch_oz_split((const OzJob *)ctx->ozStaJobs.p, (int)oz->sta_jobs.size(), (const OzSpan *)ctx->ozStaSpans.p,
                     (int)oz->sta_spans.size(), ctx->ops.d(), nullptr, nullptr, ctx->ozScales.d(),
                     (uint8_t *)ctx->ozPack.p, oz->s, ctx->stream);
@@ -302,6 +310,15 @@ int tjb::install_plan(tj_ctx *ctx, std::unique_ptr<HpsiPlan> P, uint64_t h,
     ctx->oz = std::move(oz);
   }
   CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->oz) {
+    // the operators' own splits: a non-finite operator entry is reported now
+    int flag = 0;
+    CK(cudaMemcpy(&flag, (char *)ctx->ozMisc.p + 64, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag & 2) {
+      ctx->oz.reset();
+      return set_err(TJ_ERR_NUMERIC, "split-precision H*psi: an operator holds a NaN or an infinity");
+    }
+  }
   ctx->stats = tj_hpsi_stats();
   ctx->stats.prepare_ms = ms_since(t_start);
   ctx->stats.plan_ms = plan_ms;
@@ -343,12 +360,13 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
   const OzPlan &oz = *ctx->oz;
   cudaStream_t st = ctx->stream;
   int *err = (int *)((char *)ctx->ozMisc.p + 64);
+  const uint64_t wait_ns = (uint64_t)(ctx->wait_s * 1e9);
   double *scales = ctx->ozScales.d();
   uint8_t *pack = (uint8_t *)ctx->ozPack.p;
   CK(cudaMemsetAsync(scales + oz.dyn_scale_begin, 0, sizeof(double) * (oz.n_scales - oz.dyn_scale_begin), st));
   if (timed) CK(cudaEventRecord(ctx->ev[0], st));
   launch_oz_max((const OzJob *)ctx->ozPsiMJobs.p, (int)oz.psi_mjobs.size(), (const OzSpan *)ctx->ozPsiMSpans.p,
-                (int)oz.psi_mspans.size(), ctx->ops.d(), in, ctx->scr.d(), scales, st);
+                (int)oz.psi_mspans.size(), ctx->ops.d(), in, ctx->scr.d(), scales, err, st);
   launch_oz_split((const OzJob *)ctx->ozPsiJobs.p, (int)oz.psi_jobs.size(), (const OzSpan *)ctx->ozPsiSpans.p,
                   (int)oz.psi_spans.size(), ctx->ops.d(), in, ctx->scr.d(), scales, pack, oz.s, st);
   if (timed) CK(cudaEventRecord(ctx->ev[1], st));
@@ -356,10 +374,10 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
                     (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzCell *)ctx->ozCells.p,
                     (const OzStackRow *)ctx->ozStackRows.p,
-                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, oz.bn, st));
+                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, oz.bn, wait_ns, st));
   if (timed) CK(cudaEventRecord(ctx->ev[2], st));
   launch_oz_max((const OzJob *)ctx->ozProdMJobs.p, (int)oz.prod_mjobs.size(), (const OzSpan *)ctx->ozProdMSpans.p,
-                (int)oz.prod_mspans.size(), ctx->ops.d(), in, ctx->scr.d(), scales, st);
+                (int)oz.prod_mspans.size(), ctx->ops.d(), in, ctx->scr.d(), scales, err, st);
   launch_oz_split((const OzJob *)ctx->ozProdJobs.p, (int)oz.prod_jobs.size(), (const OzSpan *)ctx->ozProdSpans.p,
                   (int)oz.prod_spans.size(), ctx->ops.d(), in, ctx->scr.d(), scales, pack, oz.s, st);
   if (timed) CK(cudaEventRecord(ctx->ev[3], st));
@@ -367,7 +385,7 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
                     (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzCell *)ctx->ozCells.p,
                     (const OzStackRow *)ctx->ozStackRows.p,
-                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, oz.bn, st));
+                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, oz.bn, wait_ns, st));
   if (timed) CK(cudaEventRecord(ctx->ev[4], st));
   CK(cudaGetLastError());
   ++ctx->n_hpsi;
@@ -380,7 +398,17 @@ int tjb::check_device_flags(tj_ctx *ctx) {
   int flag = 0;
   CK(cudaMemcpyAsync(&flag, (char *)ctx->ozMisc.p + 64, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  if (flag) return set_err(TJ_ERR_TIMEOUT, "split-precision GEMM: a bounded tensor-core wait timed out");
+  if (flag & 2)
+    return set_err(TJ_ERR_NUMERIC, "split-precision H*psi: the input vector (or a product) holds a NaN or an infinity");
+  if (flag & 1) return set_err(TJ_ERR_TIMEOUT, "split-precision GEMM: a bounded tensor-core wait timed out");
+  return TJ_OK;
+}
+
+// Clears the split-precision kernels' error flags at the start of a call, so
+// that each call reports its own failures.
+int tjb::reset_device_flags(tj_ctx *ctx) {
+  if (!ctx->oz) return TJ_OK;
+  CK(cudaMemsetAsync((char *)ctx->ozMisc.p + 64, 0, sizeof(int), ctx->stream));
   return TJ_OK;
 }
 
@@ -516,6 +544,7 @@ extern "C" int tj_model_wave_multi(tj_ctx *ctx, int n, const tj_lattice *const *
     merge_plans(pp, *P, ctx->multi_off);
     if ((rc = install_plan(ctx, std::move(P), h, t_start))) return rc;
   }
+  if ((rc = reset_device_flags(ctx))) return rc;
   const int64_t D = ctx->plan->psi_len;
   if ((rc = ctx->vin.reserve(sizeof(double) * (D + 4))) || (rc = ctx->vout.reserve(sizeof(double) * (D + 4))))
     return rc;

@@ -50,6 +50,7 @@ struct tj_ctx {
   // launch, 3 after the product splits, 4 end (FP64: 1 = 0 and 3 = 2)
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   int prec_mode = TJ_PREC_FP64, slices = 6;
+  double wait_s = 2.0;        // limit of the split-precision GEMM's pipeline waits (tj_set_wait_limit)
   // tiling / schedule choices in use, and how they are chosen (TJ_TUNE_*)
   tjb::TuneParams tune;
   int autotune = TJ_TUNE_CACHED;
@@ -98,6 +99,7 @@ int prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const 
                  const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave);
 int run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed);
 int check_device_flags(tj_ctx *ctx);
+int reset_device_flags(tj_ctx *ctx);
 // wavefunction table checks shared by every entry point that takes a tj_wave:
 // null tables, negative sizes or offsets, a sector past wave->dim
 int check_wave(const tj_wave *w);

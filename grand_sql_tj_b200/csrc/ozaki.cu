@@ -20,6 +20,7 @@
 //                  Every wait is bounded by wall time: on timeout the kernel
 //                  raises *err, lets the other roles drop out, waits (bounded)
 //                  for its copies and MMAs in flight, frees TMEM and returns.
+//                  Where all lanes of a warp wait, the warp decides together.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -84,7 +85,7 @@ __device__ __forceinline__ bool oz_unit(const OzJob *jobs, int njobs, const OzSp
 // raised by one lane.
 __global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_max_kernel(const OzJob *jobs, int njobs, const OzSpan *spans,
                                                                   const double *ops, const double *psi,
-                                                                  const double *scr, double *scales) {
+                                                                  const double *scr, double *scales, int *err) {
   const OzSpan sp = spans[blockIdx.x];
   int64_t k = (int64_t)sp.u0 + threadIdx.x;
   OzJob J;
@@ -110,6 +111,12 @@ __global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_max_kernel(const OzJob *j
   double x[OZ_MAX_CHUNK];
 #pragma unroll
   for (int q = 0; q < OZ_MAX_CHUNK; ++q) x[q] = valid && k0 + q < J.K ? fabs(row[(int64_t)(k0 + q) * J.ks]) : 0.0;
+  // a NaN or an infinity cannot be split (its scale and digits are undefined):
+  // the host reports it instead of returning a silently wrong product
+  bool bad = false;
+#pragma unroll
+  for (int q = 0; q < OZ_MAX_CHUNK; ++q) bad |= !isfinite(x[q]);
+  if (bad) atomicOr(err, 2);
   if (J.want_max == 2) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -208,6 +215,7 @@ struct OzGemmParams {
   const double *psi;
   double *scr, *out;
   int *err;
+  uint64_t wait_ns;   // limit of the pipeline's waits
 };
 
 __device__ __forceinline__ uint32_t oz_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -232,22 +240,27 @@ __device__ __forceinline__ bool oz_try(uint32_t mbar, uint32_t parity) {
   return ok != 0;
 }
 
-// Waits for the phase of the given parity; false after ~2 s or when another
-// role has aborted (*abort != 0).  The clock is read only once the first try
-// has failed (a phase that has already completed costs one try).
-__device__ __forceinline__ bool oz_wait(uint32_t mbar, uint32_t parity, volatile int *abort) {
+// Waits for the phase of the given parity; false after limit_ns or when
+// another role has aborted (*abort != 0).  The clock is read only once the
+// first try has failed (a phase that has already completed costs one try).
+// The pipeline's waits use the caller's limit (OzGemmParams::wait_ns); the
+// drain waits before the CTA exits always use OZ_WAIT_NS, so that no CTA
+// leaves with bulk copies or MMAs in flight.
+__device__ __forceinline__ bool oz_wait(uint32_t mbar, uint32_t parity, volatile int *abort,
+                                        uint64_t limit_ns = OZ_WAIT_NS) {
   if (oz_try(mbar, parity)) return true;
   const uint64_t t0 = oz_now_ns();
   for (;;) {
     if (oz_try(mbar, parity)) return true;
     if (abort && *abort) return false;
-    if (oz_now_ns() - t0 > OZ_WAIT_NS) return false;
+    if (oz_now_ns() - t0 > limit_ns) return false;
   }
 }
 
+// *err bits: 1 a bounded wait gave up, 2 a non-finite value entered a split
 __device__ __forceinline__ void oz_fail(volatile int *abort, int *err) {
   *abort = 1;
-  atomicExch(err, 1);
+  atomicOr(err, 1);
 }
 
 // K-major, no-swizzle UMMA shared-memory descriptor (core matrices of 8 rows x
@@ -403,7 +416,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
     auto acquire = [&](uint32_t bytes) -> bool {
       int good = 1;
       if (lane == 0) {
-        if (!oz_wait(oz_smem(&empty_bar[stage]), ph ^ 1u, &abort_sh)) {
+        if (!oz_wait(oz_smem(&empty_bar[stage]), ph ^ 1u, &abort_sh, p.wait_ns)) {
           if (!abort_sh) oz_fail(&abort_sh, p.err);
           good = 0;
         } else {
@@ -506,7 +519,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
           for (int k0 = 0; k0 < nkb_f && ok; k0 += C::KB_PIECE) {
           const int nkb = min(C::KB_PIECE, nkb_f - k0);
           const uint32_t buf = famc & 1u, use = famc >> 1;
-          if (!oz_wait(oz_smem(&tempty_bar[buf]), (use & 1u) ^ 1u, &abort_sh)) {
+          if (!oz_wait(oz_smem(&tempty_bar[buf]), (use & 1u) ^ 1u, &abort_sh, p.wait_ns)) {
             if (!abort_sh) oz_fail(&abort_sh, p.err);
             ok = false;
             break;
@@ -514,7 +527,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
           asm volatile("tcgen05.fence::after_thread_sync;");
           const uint32_t dt = tmem + buf * 256u;
           for (int kb = 0; kb < nkb; kb += C::KPS) {
-            if (!oz_wait(oz_smem(&full_bar[stage]), ph, &abort_sh)) {
+            if (!oz_wait(oz_smem(&full_bar[stage]), ph, &abort_sh, p.wait_ns)) {
               if (!abort_sh) oz_fail(&abort_sh, p.err);
               ok = false;
               break;
@@ -615,7 +628,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       }
       const int slot = (int)(icount % OZ_META);
       int good = 1;
-      if (lane == 0 && !oz_wait(oz_smem(&meta_empty[slot]), ((icount / OZ_META) & 1u) ^ 1u, &abort_sh)) {
+      if (lane == 0 && !oz_wait(oz_smem(&meta_empty[slot]), ((icount / OZ_META) & 1u) ^ 1u, &abort_sh, p.wait_ns)) {
         if (!abort_sh) oz_fail(&abort_sh, p.err);
         good = 0;
       }
@@ -697,7 +710,11 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       const int c0 = half * hch, nchh = min(hch, nch - c0);
       const int nf = it.fam_end - it.fam_begin;
       const int slot = (int)(icount % OZ_META);
-      if (!oz_wait(oz_smem(&meta_full[slot]), (icount / OZ_META) & 1u, &abort_sh)) {
+      // every lane waits (acquiring the slot's data) and the warp decides
+      // together, so that the warp-collective TMEM reads below are never
+      // reached by part of a warp
+      if (!__all_sync(0xffffffffu, oz_wait(oz_smem(&meta_full[slot]), (icount / OZ_META) & 1u, &abort_sh,
+                                           p.wait_ns))) {
         if (!abort_sh) oz_fail(&abort_sh, p.err);
         ok = false;
         break;
@@ -771,7 +788,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       for (int pc = 0; pc < m.npiece[f]; ++pc) {
         const uint32_t buf = famc & 1u, use = famc >> 1;
         const double rscale = rv ? m.rs[f][r] : 0.0;
-        if (!oz_wait(oz_smem(&tfull_bar[buf]), use & 1u, &abort_sh)) {
+        if (!__all_sync(0xffffffffu, oz_wait(oz_smem(&tfull_bar[buf]), use & 1u, &abort_sh, p.wait_ns))) {
           if (!abort_sh) oz_fail(&abort_sh, p.err);
           ok = false;
           break;
@@ -858,9 +875,9 @@ void launch_oz_stack_rows(const OzCell *cells, int ncells, const OzProdRow *prow
 }
 
 void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
-                   const double *psi, const double *scr, double *scales, cudaStream_t st) {
+                   const double *psi, const double *scr, double *scales, int *err, cudaStream_t st) {
   if (njobs <= 0 || nspans <= 0) return;
-  oz_max_kernel<<<nspans, OZ_SPLIT_THREADS, 0, st>>>(jobs, njobs, spans, ops, psi, scr, scales);
+  oz_max_kernel<<<nspans, OZ_SPLIT_THREADS, 0, st>>>(jobs, njobs, spans, ops, psi, scr, scales, err);
 }
 
 void launch_oz_split(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
@@ -891,9 +908,9 @@ static cudaError_t launch_gemm_t(const OzGemmParams &p, int ncta, cudaStream_t s
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
                            const OzCell *cells, const OzStackRow *srows, const Task *tasks, const uint8_t *pack,
                            double *scales, const double *psi, double *scr, double *out, int *err, int s, int bn,
-                           cudaStream_t st) {
+                           uint64_t wait_ns, cudaStream_t st) {
   if (ncta <= 0) return cudaSuccess;
-  const OzGemmParams p{items, cta, segs, fams, cells, srows, tasks, pack, scales, psi, scr, out, err};
+  const OzGemmParams p{items, cta, segs, fams, cells, srows, tasks, pack, scales, psi, scr, out, err, wait_ns};
   if (s == 5 && bn == 32) return launch_gemm_t<5, 32>(p, ncta, st);
   if (bn != oz_bn(s)) return cudaErrorInvalidValue;
   switch (s) {

@@ -197,13 +197,14 @@ void build_ozaki_plan(const HpsiPlan &hp, int s, int nsm, OzPlan &oz, const Tune
 // the stack-row table (n rows) from the stacks' products; padding rows get off = -1
 void launch_oz_stack_rows(const OzCell *cells, int ncells, const OzProdRow *prows, OzStackRow *srows, int64_t n,
                           cudaStream_t st);
+// raises bit 2 of *err when a value it reads is not finite
 void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
-                   const double *psi, const double *scr, double *scales, cudaStream_t st);
+                   const double *psi, const double *scr, double *scales, int *err, cudaStream_t st);
 void launch_oz_split(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
                      const double *psi, const double *scr, const double *scales, uint8_t *pack, int s, cudaStream_t st);
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
                            const OzCell *cells, const OzStackRow *srows, const Task *tasks, const uint8_t *pack,
                            double *scales, const double *psi, double *scr, double *out, int *err, int s, int bn,
-                           cudaStream_t st);
+                           uint64_t wait_ns, cudaStream_t st);
 
 }  // namespace tjb

@@ -170,6 +170,7 @@ def lib():
         L.tj_ctx_destroy.argtypes = [C.c_void_p]
         L.tj_set_precision.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.tj_step_begin.argtypes = [C.c_void_p]
+        L.tj_set_wait_limit.argtypes = [C.c_void_p, C.c_double]
         L.tj_host_register.argtypes = [C.c_void_p, C.c_size_t]
         L.tj_host_unregister.argtypes = [C.c_void_p]
         hp = [C.c_void_p, P(TjLattice), P(TjModel), P(TjModel), P(TjBasis), P(TjBasis)]
@@ -255,6 +256,9 @@ class Context:
 
     def step_begin(self):
         _chk(lib().tj_step_begin(self.h))
+
+    def set_wait_limit(self, seconds: float):
+        _chk(lib().tj_set_wait_limit(self.h, seconds))
 
     def stats(self) -> TjHpsiStats:
         s = TjHpsiStats()

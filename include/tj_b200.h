@@ -149,6 +149,13 @@ int tj_ctx_destroy(tj_ctx *ctx);
 /* Arithmetic of the block GEMMs of H*psi: TJ_PREC_FP64, or TJ_PREC_OZAKI with
  * `slices` int8 slices per operand (3..8). */
 int tj_set_precision(tj_ctx *ctx, int mode, int slices);
+/* No counterpart in the reference.  Every wait inside the split-precision
+ * GEMM's pipeline (a stage's copies, the MMAs of a family, an item's
+ * metadata) gives up after `seconds` (default 2): the kernel then lets its
+ * other roles stop, waits for its copies and MMAs in flight (with their own
+ * 2 s bound), releases its tensor memory and returns, and the call returns
+ * TJ_ERR_TIMEOUT; the context stays usable.  seconds in [0, 60]. */
+int tj_set_wait_limit(tj_ctx *ctx, double seconds);
 /* Invalidates the operators and task lists cached for the current DMRG step. */
 int tj_step_begin(tj_ctx *ctx);
 const char *tj_last_error(void);
