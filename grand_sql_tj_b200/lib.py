@@ -13,7 +13,7 @@ from typing import Optional, Tuple
 
 import numpy as np
 
-from .structs import (Block, TjBasis, TjBlock, TjBlockResult, TjBlockSet, TjBlockSub, TjChain, TjGgCell, TjGgTerm,
+from .structs import (Basis, BasisMap, Block, TjBasis, TjBasisMap, TjBasisResult, TjBasisSub, TjBlock, TjBlockResult, TjBlockSet, TjBlockSub, TjChain, TjGgCell, TjGgTerm,
                       TjHpsiStats, TjLattice, TjModel, TjModelResult, TjTruncResult, TjTuneResult, TjWave, Wave,
                       block_from_c_result, call_block_result, call_model_result)
 
@@ -209,6 +209,15 @@ def lib():
         L.tj_update_trun.argtypes = [C.c_void_p, C.c_int, P(TjBlock), P(TjBlock), P(TjBlockResult)]
         L.tj_block_mul_block_ndia.argtypes = [C.c_void_p, P(TjBlock), C.c_char, P(TjBlock), C.c_char, C.c_double,
                                               C.c_int, P(TjBasis), P(TjBlockResult)]
+        L.tj_disk_name.argtypes = [C.c_int, C.c_int, C.c_char_p, C.c_int]
+        L.tj_wave_to_disk.argtypes = [C.c_char_p, P(TjWave)]
+        L.tj_wave_from_disk.argtypes = [C.c_char_p, P(TjWave), C.c_void_p, C.c_void_p]
+        L.tj_block_to_disk.argtypes = [C.c_char_p, P(TjBlock)]
+        L.tj_block_from_disk.argtypes = [C.c_char_p, P(TjBlockResult)]
+        L.tj_model_to_disk.argtypes = [C.c_char_p, P(TjModel)]
+        L.tj_model_from_disk.argtypes = [C.c_char_p, P(TjModelResult)]
+        L.tj_basis_to_disk.argtypes = [C.c_char_p, P(TjBasis)]
+        L.tj_basis_from_disk.argtypes = [C.c_char_p, P(TjBasisResult)]
         L.tj_w6js.restype = C.c_double
         L.tj_w6js.argtypes = [C.c_int] * 6
         L.tj_w3js.restype = C.c_double
@@ -529,6 +538,76 @@ class DeviceBackend:
 
     def correlator(self, name, a, b, sys_bs, env_bs, wave, flag="B"):
         return self.ctx.correlator(name, a, b, sys_bs, env_bs, wave, flag)
+
+
+# ------------------------------------------------------------ checkpoint files
+def disk_name(kind: int, idx: int) -> str:
+    """The reference's file name: kind 0 sysblocks, 1 systruns, 2 sysbs, 3 envblocks, 4 envtruns, 5 envbs, 6 eigvec."""
+    buf = C.create_string_buffer(64)
+    _chk(lib().tj_disk_name(kind, idx, buf, 64))
+    return buf.value.decode()
+
+
+def wave_to_disk(path: str, wave: Wave):
+    _chk(lib().tj_wave_to_disk(path.encode(), C.byref(wave.c)))
+
+
+def wave_from_disk(path: str) -> Wave:
+    from .structs import TjWaveSub, WaveSector
+    L = lib()
+    hdr = TjWave()
+    _chk(L.tj_wave_from_disk(path.encode(), C.byref(hdr), None, None))
+    subs = (TjWaveSub * max(hdr.num, 1))()
+    data = np.zeros(max(hdr.dim, 1))
+    _chk(L.tj_wave_from_disk(path.encode(), C.byref(hdr), C.cast(subs, C.c_void_p), data.ctypes.data))
+    secs = [WaveSector(s.sys_num_up, s.sys_num_down, s.env_num_up, s.env_num_down, s.sys_dim, s.env_dim)
+            for s in subs[:hdr.num]]
+    return Wave(hdr.sys_len, hdr.env_len, secs, data)
+
+
+def block_to_disk(path: str, block: Block):
+    pb = block.pack()
+    _chk(lib().tj_block_to_disk(path.encode(), C.byref(pb.c)))
+
+
+def block_from_disk(path: str) -> Block:
+    rc, b = call_block_result(lambda r: lib().tj_block_from_disk(path.encode(), r))
+    _chk(rc)
+    return b
+
+
+def model_to_disk(path: str, model):
+    pm = model.pack()
+    _chk(lib().tj_model_to_disk(path.encode(), C.byref(pm.c)))
+
+
+def model_from_disk(path: str):
+    rc, m = call_model_result(lambda r: lib().tj_model_from_disk(path.encode(), r))
+    _chk(rc)
+    return m
+
+
+def basis_to_disk(path: str, basis: Basis):
+    pb = basis.pack()
+    _chk(lib().tj_basis_to_disk(path.encode(), C.byref(pb.c)))
+
+
+def basis_from_disk(path: str) -> Basis:
+    L = lib()
+    r = TjBasisResult()
+    _chk(L.tj_basis_from_disk(path.encode(), C.byref(r)))
+    sub = (TjBasisMap * max(r.num, 1))()
+    maps = (TjBasisSub * max(r.nmaps, 1))()
+    r.sub = C.cast(sub, C.POINTER(TjBasisMap))
+    r.maps = C.cast(maps, C.POINTER(TjBasisSub))
+    _chk(L.tj_basis_from_disk(path.encode(), C.byref(r)))
+    out = []
+    for i in range(r.num):
+        m = sub[i]
+        out.append(BasisMap(m.new_num_up, m.new_num_down,
+                            [(q.spos, q.sdim, q.bl_num_up, q.bl_num_down, q.st_num_up, q.st_num_down)
+                             for q in maps[m.first:m.first + m.num]]))
+    return Basis(r.len, out)
 
 
 def pack_superblock(sb):

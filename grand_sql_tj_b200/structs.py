@@ -100,6 +100,11 @@ class TjChain(C.Structure):
                 ("truns", C.POINTER(TjBlock))]
 
 
+class TjBasisResult(C.Structure):
+    _fields_ = [("len", C.c_int32), ("num", C.c_int32), ("dim", C.c_int32), ("nmaps", C.c_int32),
+                ("sub", C.POINTER(TjBasisMap)), ("maps", C.POINTER(TjBasisSub)), ("basis", TjBasis)]
+
+
 class TjHpsiStats(C.Structure):
     _fields_ = [("flops", C.c_double), ("flops_ref", C.c_double), ("bytes", C.c_double),
                 ("n_products", C.c_int64), ("n_tasks", C.c_int64), ("n_tiles_p1", C.c_int64),

@@ -349,6 +349,50 @@ int tj_wave_trans(tj_ctx *ctx, int direction, const tj_basis *sys_bs, const tj_b
                   const tj_block *sys_trun, const tj_block *env_trun, const tj_wave *old_wave,
                   tj_wave *new_wave);
 
+/* ------------------------------------------------------- checkpoint files */
+
+/* The reference's files (code/tjsq/block.f90:2760-3097), read and written on
+ * the host.  Binary files are Fortran sequential unformatted files as
+ * gfortran and ifort write them: each WRITE statement is one record framed by
+ * its byte length as a 4-byte little-endian integer before and after (a
+ * record above 2^31 - 9 bytes as subrecords with negative markers), default
+ * integers of 4 bytes, REAL(8) of 8, matrices column-major.  Basis files are
+ * the formatted text of basis_to_disk.  The reference names them sysblocks<i>,
+ * systruns<i>, sysbs<i> (and env...) and eigvec<i> (Get_model_name,
+ * Get_wave_name, code/tjsq/dmrg_sub.f90:294-346); tj_disk_name builds them:
+ * kind 0 sysblocks, 1 systruns, 2 sysbs, 3 envblocks, 4 envtruns, 5 envbs,
+ * 6 eigvec. */
+int tj_disk_name(int kind, int idx, char *buf, int buflen);
+/* wave_to_disk (block.f90:2760-2787) */
+int tj_wave_to_disk(const char *path, const tj_wave *wave);
+/* wave_from_disk (block.f90:2791-2821), two-call: with subs or data NULL
+ * only hdr's sys_len, env_len, num and dim are filled; then the caller
+ * allocates subs[num] and data[dim] and calls again (hdr->sub and hdr->data
+ * are set to them, sectors back to back from offset 0). */
+int tj_wave_from_disk(const char *path, tj_wave *hdr, tj_wave_sub *subs, double *data);
+/* truns_to_disk / truns_from_disk (block_to_disk / block_from_disk;
+ * block.f90:2826-2870, 2956-2996): one block per file; two-call result. */
+int tj_block_to_disk(const char *path, const tj_block *block);
+int tj_block_from_disk(const char *path, tj_block_result *out);
+/* model_to_disk (block.f90:2873-2906): len, ham, then per operator set (the
+ * caller's nsub = nleg11(len)) elec_up, elec_down, spin_sd, num_sn.
+ * model_from_disk (block.f90:2910-2952), two-call as tj_model_result, nsub
+ * from the number of blocks stored, spin_sz empty (it is not stored); the
+ * reference's deletion of the next block file is left to the caller. */
+int tj_model_to_disk(const char *path, const tj_model *model);
+int tj_model_from_disk(const char *path, tj_model_result *out);
+/* basis_to_disk / basis_from_disk (block.f90:3000-3097), formatted text.
+ * Two-call: with sub or maps NULL the sizes are filled; then the caller
+ * allocates sub[num] and maps[nmaps] and calls again. */
+typedef struct tj_basis_result {
+  int32_t len, num, dim, nmaps;
+  tj_basis_map *sub;           /* caller-allocated, num entries (or NULL)   */
+  tj_basis_sub *maps;          /* caller-allocated, nmaps entries (or NULL) */
+  tj_basis basis;              /* second call: the basis                    */
+} tj_basis_result;
+int tj_basis_to_disk(const char *path, const tj_basis *basis);
+int tj_basis_from_disk(const char *path, tj_basis_result *out);
+
 /* --------------------------------------------------- measurement support */
 
 /* Statistics of the H*psi task list compiled for the last tj_model_wave /
