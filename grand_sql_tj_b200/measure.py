@@ -85,3 +85,87 @@ def density_cor(be, ch: Chains, wave, oper1, oper2, flag: str, sid1: int, ny: in
             value = be.correlator("sys_block_env_block_cor_ndia", sys_oper, env_oper, sys_bs, env_bs, wave, flag)
         out[(sid1, sid3)] = value * scale
     return out
+
+
+def get_sys_two(be, ch: Chains, idx1: int, idx2: int, ops):
+    """Get_sys_two (measure.f90:3798-3832): the singlet pair c+_idx1 c+_idx2
+    (block_mul_block_ndia coupled to total spin 0) on the block of length idx2."""
+    n1 = be.get_oper(0, 0, ch.sys, ops["elec_up"], idx1, idx2, False, "F")
+    n2 = be.get_oper(0, 0, ch.sys, ops["elec_up"], idx2, idx2, False, "F")
+    new = be.block_mul_block_ndia(n1, "N", n2, "N", 1.0, 0, ch.sys_bases[idx2])
+    return be.update_trun(0, new, ch.sys_truns[idx2]) if idx2 > ch.trun_idx else new
+
+
+def get_sys_two1(be, ch: Chains, idx2: int, idx3: int, idx4: int, pair, ops):
+    """Get_sys_two1 (measure.f90:3835-3889): the pair operator of block length
+    idx2 times c_idx3 (coupled to spin 1/2) times c_idx4 (coupled to spin 0),
+    carried to the system block."""
+    new = be.change_oper(0, 0, ch.sys, pair, idx2, idx3, False, "B")
+    n1 = be.get_oper(0, 0, ch.sys, ops["elec_down"], idx3, idx3, False, "F")
+    n2 = be.block_mul_block_ndia(new, "N", n1, "N", 1.0, 1, ch.sys_bases[idx3])
+    n1 = be.update_trun(0, n2, ch.sys_truns[idx3]) if idx3 > ch.trun_idx else n2
+    n12 = be.change_oper(0, 0, ch.sys, n1, idx3, idx4, False, "F")
+    n2 = be.get_oper(0, 0, ch.sys, ops["elec_down"], idx4, idx4, False, "F")
+    n3 = be.block_mul_block_ndia(n12, "N", n2, "N", 1.0, 0, ch.sys_bases[idx4])
+    n1 = be.update_trun(1, n3, ch.sys_truns[idx4]) if idx4 > ch.trun_idx else n3
+    return be.change_oper(0, 1, ch.sys, n1, idx4, ch.sys_len - 1, True, "B")
+
+
+def get_scop_operator_env(be, ch: Chains, idx1: int, idx2: int, new_idx: int, truns: bool, ops):
+    """Get_SCOP_Operator_Env (measure.f90:6211-6263), singlet 'S0': the pair
+    c+_idx1 c+_idx2 of the environment chain, carried to length new_idx."""
+    n1 = be.get_oper(1, 0, ch.env, ops["elec_up"], idx1, idx2, False, "F")
+    n2 = be.get_oper(1, 0, ch.env, ops["elec_up"], idx2, idx2, False, "F")
+    new = be.block_mul_block_ndia(n1, "N", n2, "N", 1.0, 0, ch.env_bases[idx2])
+    env = be.update_trun(0, new, ch.env_truns[idx2]) if idx2 > ch.trun_idx else new
+    return be.change_oper(1, 0, ch.env, env, idx2, new_idx, truns, "B")
+
+
+def pairing_cor(be, ch: Chains, wave, ops, neib, xc1: int, xc2: int, ij: int, ny: int,
+                num_site: int) -> Dict[Tuple[int, int, int], float]:
+    """Get_mSCOP_Operator_Cor0(wave, trun_idx, 'S0', ..., xc1, xc2, ij, ij1)
+    (measure.f90:3377-3507): the singlet pair correlation <D+_(sid1,sid2)
+    D_(sid3,sid4)> for the bond (sid1, sid2 = neib(sid1, ij)) and the bonds
+    (sid3, sid4 = neib(sid3, j)), j = 1, 3, 5, of the sites sid3 of sid1's
+    row, in the system block (four operators of one block) and in the
+    environment block (a pair on each side).  neib(i, k) is the lattice's
+    neighbour table.  Returns {(sid1, sid3, j): value}; the reference's file
+    output and its column of disconnected products are left out."""
+    sys_len, env_len = ch.sys_len, ch.env_len
+    sys_bs, env_bs = ch.sys_bases[sys_len], ch.env_bases[env_len]
+    out = {}
+
+    def env_part(sid1, sid2, sys_oper, sid3_range):
+        for sid3 in sid3_range:
+            if (sid3 - sid1) % ny != 0:
+                continue
+            eid1 = num_site - sid3 + 1
+            for j in (1, 3, 5):
+                sid4 = int(neib(sid3, j))
+                eid2 = num_site - sid4 + 1
+                if max(eid1, eid2) <= env_len - 1:
+                    env_oper = get_scop_operator_env(be, ch, min(eid1, eid2), max(eid1, eid2), env_len - 1, True, ops)
+                    out[(sid1, sid3, j)] = be.correlator("sys_block_env_block_cor_ndia", sys_oper, env_oper, sys_bs,
+                                                         env_bs, wave, "B")
+
+    for sid11 in range(xc1, xc2 + 1, ny):
+        sid1 = sid11
+        sid2 = int(neib(sid1, ij))
+        pair = get_sys_two(be, ch, min(sid1, sid2), max(sid1, sid2), ops)
+        for sid3 in range(sid1 + ny, sys_len - 3 + 1, ny):
+            for j in (1, 3, 5):
+                sid4 = int(neib(sid3, j))
+                if min(sid4, sid3) <= max(sid1, sid2):
+                    continue
+                if max(sid3, sid4) <= sys_len - 1:
+                    four = get_sys_two1(be, ch, max(sid1, sid2), min(sid3, sid4), max(sid3, sid4), pair, ops)
+                    out[(sid1, sid3, j)] = be.correlator("measure_sys_block", four, None, sys_bs, None, wave)
+        if ny >= 6:
+            s1 = sid11 + 4
+            s2 = int(neib(s1, ij))
+            p1 = get_sys_two(be, ch, min(s1, s2), max(s1, s2), ops)
+            sys_oper = be.change_oper(0, 0, ch.sys, p1, s2, sys_len - 1, True, "B")
+            env_part(s1, s2, sys_oper, range(sys_len + 2, sys_len + ny + 2))
+        sys_oper = be.change_oper(0, 0, ch.sys, pair, sid2, sys_len - 1, True, "B")
+        env_part(sid1, sid2, sys_oper, range(sys_len + 2, num_site - ny + 1))
+    return out

@@ -44,9 +44,9 @@ def bonds_of(geo):
     return out
 
 
-def _states(n, n_elec):
+def _states(n, n_elec, n_up=None):
     ups, dns = [], []
-    nu = n_elec // 2
+    nu = n_elec // 2 if n_up is None else n_up
     for occ in itertools.combinations(range(n), n_elec):
         for upset in itertools.combinations(occ, nu):
             u = 0
@@ -70,10 +70,10 @@ def _popcount(x):
 
 
 class TJCluster:
-    def __init__(self, n_site, bonds, esite, n_elec):
-        assert n_elec % 2 == 0
+    def __init__(self, n_site, bonds, esite, n_elec, n_up=None):
+        assert n_up is not None or n_elec % 2 == 0
         self.n, self.bonds, self.N = n_site, bonds, n_elec
-        self.up, self.dn = _states(n_site, n_elec)
+        self.up, self.dn = _states(n_site, n_elec, n_up)
         self.key = (self.up << n_site) | self.dn
         order = np.argsort(self.key)
         self.up, self.dn, self.key = self.up[order], self.dn[order], self.key[order]
@@ -215,3 +215,42 @@ def density_correlation(cl, psi, i, j):
     occ = cl.up | cl.dn
     both = ((occ >> i) & 1) & ((occ >> j) & 1)
     return float(np.sum(psi[both == 1] ** 2))
+
+
+def annihilate(cl, vec, site, spin, target):
+    """c_(site, spin) |vec> as a vector of the cluster `target` (one electron
+    less).  Fermion order: modes by site, up (spin 0) before down (spin 1) on a
+    site -- the order whose string the hopping of TJCluster.hamiltonian counts
+    (electrons on the sites between the two ends)."""
+    src = cl.up if spin == 0 else cl.dn
+    b = 1 << site
+    ok = (src & b) != 0
+    up, dn = cl.up[ok], cl.dn[ok]
+    below = b - 1
+    # occupied modes before (site, spin): every electron on a lower site, and
+    # the up electron of this site when a down electron is removed
+    nbefore = _popcount(up & below) + _popcount(dn & below) + (spin == 1) * ((up & b) != 0)
+    if spin == 0:
+        up = up ^ b
+    else:
+        dn = dn ^ b
+    out = np.zeros(target.dim)
+    out[target._index(up, dn)] = vec[ok] * np.where(nbefore % 2 == 0, 1.0, -1.0)
+    return out
+
+
+def singlet_pair_correlation(cl, psi, a, b, c, d):
+    """<psi| D+_(a,b) D_(c,d) |psi> with D_(i,j) = (c_(j,dn) c_(i,up) - c_(j,up) c_(i,dn)) / sqrt(2),
+    the annihilator of the singlet pair (c+_(i,up) c+_(j,dn) - c+_(i,dn) c+_(j,up)) / sqrt(2)."""
+    n, N = cl.n, cl.N
+    nu = N // 2
+    m_up = TJCluster(n, [], np.zeros(n), N - 1, nu - 1)    # after removing an up electron
+    m_dn = TJCluster(n, [], np.zeros(n), N - 1, nu)        # after removing a down electron
+    two = TJCluster(n, [], np.zeros(n), N - 2, nu - 1)
+
+    def pair(i, j):
+        x = annihilate(m_up, annihilate(cl, psi, i, 0, m_up), j, 1, two)
+        y = annihilate(m_dn, annihilate(cl, psi, i, 1, m_dn), j, 0, two)
+        return (x - y) / np.sqrt(2.0)
+
+    return float(pair(a, b) @ pair(c, d))

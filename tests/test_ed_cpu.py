@@ -60,3 +60,17 @@ def test_ed_helper_two_site_values():
     H = cl.hamiltonian().toarray()
     assert np.allclose(H, H.T)
     assert np.linalg.eigvalsh(H)[0] < -1.0 / 3.0
+
+
+def test_ed_pair_operator_known_answers():
+    """The ED singlet pair operator on two sites with two electrons: the
+    ground state of J > 0 is the singlet, <D+ D> = 1; the Sz = 0 triplet
+    gives 0."""
+    import numpy as np
+    from tests import ed
+    cl = ed.TJCluster(2, [(0, 1, 0.0, 1.0)], np.zeros(2), 2)
+    w, v = np.linalg.eigh(cl.hamiltonian().toarray())
+    assert abs(ed.singlet_pair_correlation(cl, v[:, 0], 0, 1, 0, 1) - 1.0) <= 1e-14
+    assert abs(ed.singlet_pair_correlation(cl, v[:, 1], 0, 1, 0, 1)) <= 1e-14
+    # D_(i,j) = D_(j,i) for the singlet
+    assert abs(ed.singlet_pair_correlation(cl, v[:, 0], 0, 1, 1, 0) - 1.0) <= 1e-14

@@ -5,6 +5,8 @@ tj_update_trun, tj_block_mul_block_ndia) and the correlations they give.
     on the device and on the oracle with the same inputs, on a truncated
     2x8 ladder: identical sub-block records, entries within 1e-12 of the
     largest; the correlations within 1e-10;
+  * the same for every call of the restated Get_mSCOP_Operator_Cor0 (the
+    singlet pair correlation, bonds along and across the ladder);
   * <S_i . S_j> from an untruncated device run on a 2x6 ladder against
     exact diagonalisation (3e-8, the convergence of the Lanczos vector).
 """
@@ -12,7 +14,7 @@ import numpy as np
 import pytest
 
 from grand_sql_tj_b200.lattice import Geometry
-from grand_sql_tj_b200.measure import Chains, density_cor
+from grand_sql_tj_b200.measure import Chains, density_cor, pairing_cor
 from grand_sql_tj_b200.sweep import Dmrg, DmrgParams, site_block_ops
 
 pytestmark = pytest.mark.gpu
@@ -73,6 +75,12 @@ def test_measurement_calls_match_oracle(ctx, oracle_lib):
         density_cor(be, ch, d.wave, ops["st_sd"], ops["st_sd"], "B", sid1, 2, n)
     density_cor(be, ch, d.wave, ops["elec_up"], ops["elec_down"], "F", 1, 2, n)
     assert be.calls > 20
+    geo.setup(d.wave.sys_len - 1, d.wave.env_len - 1)
+    before = be.calls
+    for ij in (1, 3):
+        res = pairing_cor(be, ch, d.wave, ops, lambda i, k: int(geo.neib[i, k]), 1, 3, ij, 2, n)
+        assert len(res) >= 3
+    assert be.calls > before + 30
 
 
 def test_device_spin_correlation_equals_ed(ctx):
