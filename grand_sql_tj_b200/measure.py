@@ -169,3 +169,34 @@ def pairing_cor(be, ch: Chains, wave, ops, neib, xc1: int, xc2: int, ij: int, ny
         sys_oper = be.change_oper(0, 0, ch.sys, pair, sid2, sys_len - 1, True, "B")
         env_part(sid1, sid2, sys_oper, range(sys_len + 2, num_site - ny + 1))
     return out
+
+
+def measurement(be, dmrg, ops=None) -> Dict[str, Dict[tuple, float]]:
+    """The correlator part of Measurement (main.f90:191-332) for the
+    wavefunction `dmrg.wave` left by Get_Ground_State's last half-sweep: the
+    reference site xc1 = (Nx / 6) ny - ny + 1, then
+      pair_y  Get_mSCOP_Operator_Cor0(..., 'S0', xc1, xc1, 1, 0)  (main.f90:257)
+      pair_x  Get_mSCOP_Operator_Cor0(..., 'S0', xc1, xc1, 3, 0)  (main.f90:258)
+      density Get_density_cor(num_elec, num_elec, 'B', xc1)        (main.f90:274)
+      spin    Get_density_cor(st_sd, st_sd, 'B', xc1)              (main.f90:286)
+      elec    Get_density_cor(st_elec_up, st_elec_down, 'F', xc1)  (main.f90:299)
+    each as {site tuple: value}; the files the reference writes are left out."""
+    from .sweep import site_block_ops
+    geo, wave = dmrg.geo, dmrg.wave
+    ops = site_block_ops(dmrg.up_bias) if ops is None else ops
+    ny, n = geo.ny, dmrg.N
+    xc1 = (geo.nx // 6) * ny - ny + 1
+    ch = Chains(dmrg, wave)
+    geo.setup(wave.sys_len - 1, wave.env_len - 1)
+    neib_tab = geo.neib.copy()
+
+    def neib(i, k):
+        return int(neib_tab[i, k])
+
+    return {
+        "pair_y": pairing_cor(be, ch, wave, ops, neib, xc1, xc1, 1, ny, n),
+        "pair_x": pairing_cor(be, ch, wave, ops, neib, xc1, xc1, 3, ny, n),
+        "density": density_cor(be, ch, wave, ops["num_elec"], ops["num_elec"], "B", xc1, ny, n),
+        "spin": density_cor(be, ch, wave, ops["st_sd"], ops["st_sd"], "B", xc1, ny, n),
+        "elec": density_cor(be, ch, wave, ops["elec_up"], ops["elec_down"], "F", xc1, ny, n),
+    }

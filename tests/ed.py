@@ -239,14 +239,25 @@ def annihilate(cl, vec, site, spin, target):
     return out
 
 
+_SECTORS = {}
+
+
+def _sector(n, n_elec, n_up):
+    """The basis of n sites with n_elec electrons, n_up of them up (memoised)."""
+    key = (n, n_elec, n_up)
+    if key not in _SECTORS:
+        _SECTORS[key] = TJCluster(n, [], np.zeros(n), n_elec, n_up)
+    return _SECTORS[key]
+
+
 def singlet_pair_correlation(cl, psi, a, b, c, d):
     """<psi| D+_(a,b) D_(c,d) |psi> with D_(i,j) = (c_(j,dn) c_(i,up) - c_(j,up) c_(i,dn)) / sqrt(2),
     the annihilator of the singlet pair (c+_(i,up) c+_(j,dn) - c+_(i,dn) c+_(j,up)) / sqrt(2)."""
     n, N = cl.n, cl.N
     nu = N // 2
-    m_up = TJCluster(n, [], np.zeros(n), N - 1, nu - 1)    # after removing an up electron
-    m_dn = TJCluster(n, [], np.zeros(n), N - 1, nu)        # after removing a down electron
-    two = TJCluster(n, [], np.zeros(n), N - 2, nu - 1)
+    m_up = _sector(n, N - 1, nu - 1)    # after removing an up electron
+    m_dn = _sector(n, N - 1, nu)        # after removing a down electron
+    two = _sector(n, N - 2, nu - 1)
 
     def pair(i, j):
         x = annihilate(m_up, annihilate(cl, psi, i, 0, m_up), j, 1, two)
@@ -254,3 +265,13 @@ def singlet_pair_correlation(cl, psi, a, b, c, d):
         return (x - y) / np.sqrt(2.0)
 
     return float(pair(a, b) @ pair(c, d))
+
+
+def hopping_correlation(cl, psi, i, j):
+    """<psi| sum_s c+_(i,s) c_(j,s) |psi>, i != j."""
+    total = 0.0
+    for spin in (0, 1):
+        nu = cl.N // 2
+        m = _sector(cl.n, cl.N - 1, nu - 1 if spin == 0 else nu)
+        total += float(annihilate(cl, psi, i, spin, m) @ annihilate(cl, psi, j, spin, m))
+    return total

@@ -11,13 +11,15 @@ The singlet pair correlation <D+_(i,j) D_(k,l)> of the restated
 Get_mSCOP_Operator_Cor0 (measure.f90:3377-3507) is checked the same way, on
 the ladder (pairs in the system block and across the blocks) and on a
 6-leg cylinder of two columns (the branch the reference takes for ny >= 6).
+Finally the restated Measurement (main.f90:191-332) gives all five families (spin, density, single-particle
+sum_s <c+_is c_js>, pairs along y and x) equal to exact diagonalisation.
 Tolerance 3e-8 absolute: the Lanczos vector is converged on its Ritz value
 (1e-14), which leaves the vector itself accurate to about 1e-7.
 """
 import pytest
 
 from grand_sql_tj_b200.lattice import Geometry
-from grand_sql_tj_b200.measure import Chains, density_cor, pairing_cor
+from grand_sql_tj_b200.measure import Chains, density_cor, measurement, pairing_cor
 from grand_sql_tj_b200.sweep import Dmrg, DmrgParams, site_block_ops
 
 
@@ -96,3 +98,18 @@ def test_pairing_six_leg_branch_equals_ed(oracle_lib):
     res = pairing_cor(be, Chains(d, d.wave), d.wave, site_block_ops(1), neib, 1, 1, 1, 6, n)
     assert (5, 11, 1) in res
     _check_pairs(res, neib, 1, cl, psi)
+
+
+def test_measurement_driver_equals_ed(run):
+    from tests import ed
+    be, d, ch, psi, cl = run
+    m = measurement(be, d)
+    exact = {"spin": ed.spin_correlation, "density": ed.density_correlation, "elec": ed.hopping_correlation}
+    for name, f in exact.items():
+        assert len(m[name]) >= 5
+        for (i, j), v in m[name].items():
+            assert abs(v - f(cl, psi, i - 1, j - 1)) <= 3e-8, (name, i, j, v)
+    neib = _neib(d.geo, d.wave)
+    _check_pairs(m["pair_y"], neib, 1, cl, psi)
+    _check_pairs(m["pair_x"], neib, 3, cl, psi)
+    assert len(m["pair_y"]) >= 6 and len(m["pair_x"]) >= 3
