@@ -360,38 +360,77 @@ __global__ void inverse_iter_kernel(const double *dall, const double *eall, cons
 // projection is repeated only when the first one removed more than half of
 // the vector's squared norm ("twice is enough": after one pass that keeps
 // the norm above 1/sqrt(2), the vector is orthogonal to working accuracy).
-// status bit 1: a vector lost more than 0.999 of its norm to the projection.
-__global__ void __launch_bounds__(ORTH_THREADS) orthonormalize_kernel(const int *grp, const int *dims, double *Y,
-                                                                      int ldy, int *status) {
+//
+// A vector that loses more than 0.999 of its norm to the projection depends
+// on the accepted ones.  That happens for a cluster of eigenvalues closer
+// than the pivot floor eps ||T||, where inverse iteration amplifies one
+// direction of the cluster far above the others -- in practice the null
+// space of a rank-deficient density matrix (a sector with fewer environment
+// than system states, or one of tiny weight), all of whose states the keep
+// rule may keep.  When the vector's eigenvalue lies within 1e4 eps ||T|| of
+// the sector's smallest, the cluster is the bottom of the spectrum, every
+// eigenvector above it has been accepted (kept vectors are the largest of
+// their sector), and the complement of the accepted vectors is the rest of
+// the cluster: a pseudo-random vector projected off the accepted ones is then
+// an eigenvector to working accuracy (residual <= the cluster's width), as
+// good as any basis DSYEV returns for it.  Up to four such vectors are tried.
+// status bit 1: a vector stayed dependent (or its cluster is not at the
+// bottom of the spectrum).
+__global__ void __launch_bounds__(ORTH_THREADS) orthonormalize_kernel(const int *grp, const int *dims,
+                                                                      const int64_t *eoff, const double *evals,
+                                                                      const double *info, const int *job_k,
+                                                                      double *Y, int ldy, int *status) {
   extern __shared__ double h[];
   __shared__ double red[32];
   const int s = grp[4 * blockIdx.x], j0 = grp[4 * blockIdx.x + 1], cnt = grp[4 * blockIdx.x + 2];
   const int n = dims[s], tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const double lam_min = evals[eoff[s]], cluster = 1e4 * EIG_EPS * info[4 * s + 2];
   for (int t = 1; t < cnt; ++t) {
-    double *y = Y + (size_t)(j0 + cnt - 1 - t) * ldy;
-    for (int pass = 0; pass < 2; ++pass) {
-      for (int q = warp; q < t; q += nw) {
-        const double *z = Y + (size_t)(j0 + cnt - 1 - q) * ldy;
-        double acc = 0.0;
-        for (int i = lane; i < n; i += 32) acc += z[i] * y[i];
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) h[q] = acc;
+    const int jt = j0 + cnt - 1 - t;
+    double *y = Y + (size_t)jt * ldy;
+    bool ok = false;
+    for (int attempt = 0; attempt < 5 && !ok; ++attempt) {
+      if (attempt > 0) {   // a fresh pseudo-random unit vector (k + 4096 a never repeats a start)
+        double ss = 0.0;
+        for (int i = tid; i < n; i += blockDim.x) {
+          const double v = start_entry(s, job_k[jt] + 4096 * attempt, i);
+          y[i] = v;
+          ss += v * v;
+        }
+        const double inv = 1.0 / sqrt(block_sum(ss, red));
+        for (int i = tid; i < n; i += blockDim.x) y[i] *= inv;
+        __syncthreads();
       }
-      __syncthreads();
-      double ss = 0.0;
-      for (int i = tid; i < n; i += blockDim.x) {
-        double acc = y[i];
-        for (int q = 0; q < t; ++q) acc -= h[q] * Y[(size_t)(j0 + cnt - 1 - q) * ldy + i];
-        y[i] = acc;
-        ss += acc * acc;
+      ok = true;
+      for (int pass = 0; pass < 2; ++pass) {
+        for (int q = warp; q < t; q += nw) {
+          const double *z = Y + (size_t)(j0 + cnt - 1 - q) * ldy;
+          double acc = 0.0;
+          for (int i = lane; i < n; i += 32) acc += z[i] * y[i];
+          for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+          if (lane == 0) h[q] = acc;
+        }
+        __syncthreads();
+        double ss = 0.0;
+        for (int i = tid; i < n; i += blockDim.x) {
+          double acc = y[i];
+          for (int q = 0; q < t; ++q) acc -= h[q] * Y[(size_t)(j0 + cnt - 1 - q) * ldy + i];
+          y[i] = acc;
+          ss += acc * acc;
+        }
+        const double nrm = sqrt(block_sum(ss, red));   // the same value in every thread
+        if (pass == 0 && !(nrm >= 1e-3)) {
+          ok = false;
+          break;
+        }
+        const double inv = 1.0 / nrm;
+        for (int i = tid; i < n; i += blockDim.x) y[i] *= inv;
+        __syncthreads();
+        if (nrm > 0.7071067811865476) break;   // the vector entered with unit norm
       }
-      const double nrm = sqrt(block_sum(ss, red));
-      if (pass == 0 && nrm < 1e-3 && tid == 0) atomicOr(status, 2);
-      const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
-      for (int i = tid; i < n; i += blockDim.x) y[i] *= inv;
-      __syncthreads();
-      if (nrm > 0.7071067811865476) break;   // the vector entered with unit norm
+      if (!ok && attempt == 0 && !(evals[eoff[s] + job_k[jt]] - lam_min <= cluster)) break;
     }
+    if (!ok && tid == 0) atomicOr(status, 2);
   }
 }
 
@@ -739,8 +778,8 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
                                                             maxn, (double *)(cb + p_work),
                                                             (unsigned char *)(cb + p_piv), Y, ldy, d_status);
       CKT(cudaGetLastError());
-      orthonormalize_kernel<<<ngrp, ORTH_THREADS, sizeof(double) * maxn, st>>>((const int *)(ab + q_grp), d_dims, Y,
-                                                                               ldy, d_status);
+      orthonormalize_kernel<<<ngrp, ORTH_THREADS, sizeof(double) * maxn, st>>>(
+          (const int *)(ab + q_grp), d_dims, d_eoff, dev, dinfo, (const int *)(ab + q_k), Y, ldy, d_status);
       CKT(cudaGetLastError());
       const size_t bsm = sizeof(double) * (size_t)W * ldy;
       CKT(cudaFuncSetAttribute(backtransform_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
@@ -763,7 +802,9 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
         return set_err(TJ_ERR_NUMERIC, buf);
       }
       if (status[0] & 2)
-        return set_err(TJ_ERR_NUMERIC, "tj_truncation: inverse iteration gave linearly dependent eigenvectors");
+        return set_err(TJ_ERR_NUMERIC,
+                       "tj_truncation: inverse iteration gave linearly dependent eigenvectors for a cluster of "
+                       "eigenvalues above the bottom of its sector's spectrum");
     }
     std::memset(&tc.res, 0, sizeof tc.res);
     tc.res.num_state = num_state;

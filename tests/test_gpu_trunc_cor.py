@@ -82,6 +82,56 @@ def test_truncation(ctx, oracle_lib, wl, side, kmin, kmax):
     assert r2.num_state == r1.num_state and all(np.array_equal(a.mat, b.mat) for a, b in zip(t1.subs, t2.subs))
 
 
+def test_truncation_rank_deficient(ctx, oracle_lib):
+    """Density matrices with large null spaces -- the truncations of an
+    untruncated 2x6 ladder run, system block much longer than the
+    environment -- with every state kept: the columns are orthonormal, each
+    spans an invariant subspace of its rho (residual <= 1e-13 ||rho||), and
+    the spectrum summaries equal the oracle's (DSYEV)."""
+    from grand_sql_tj_b200.lattice import Geometry
+    from grand_sql_tj_b200.sweep import Dmrg, DmrgParams
+    from oracle.oracle import OracleBackend
+
+    class Rec:
+        def __init__(self):
+            self.o, self.waves = OracleBackend(), []
+
+        def __getattr__(self, k):
+            return getattr(self.o, k)
+
+        def truncation(self, wave, side, kmin, kmax, err):
+            self.waves.append((wave.copy(), side))
+            return self.o.truncation(wave, side, kmin, kmax, err)
+
+    geo = Geometry(6, 2, t=1.0, J=1.0 / 3.0, esite=-0.1, up_bias=1)
+    be = Rec()
+    d = Dmrg(geo, be, DmrgParams(n_elec=10, kept_min=10 ** 5, kept_max=10 ** 6, lanzero=1e-12, lanzero_warm=1e-12,
+                                 seed=3))
+    d.warm_up()
+    d.left_to_right(5, 10, restart=False)
+    from oracle import oracle
+    checked = 0
+    for w, side in be.waves[-3:]:
+        r0, _, _ = oracle.truncation(w, side, 10 ** 5, 10 ** 6, 1e-18)
+        r1, t1 = ctx.truncation(w, side, 10 ** 5, 10 ** 6, 1e-18)
+        assert r1.num_state == r0.num_state
+        for k in ("trunc_err", "entropy1", "entropy2", "entropys"):
+            assert abs(getattr(r1, k) - getattr(r0, k)) <= 1e-10, k
+        nrm2 = float(w.data[:w.dim] @ w.data[:w.dim])
+        for sub in t1.subs:
+            q = sub.mat
+            assert np.max(np.abs(q.T @ q - np.eye(q.shape[1]))) <= 1e-12
+            assert side == 0
+            i = next(i for i, sc in enumerate(w.sectors) if (sc.sys_num_up, sc.sys_num_down) == (sub.num_up, sub.num_down))
+            x = w.sector(i)
+            rho = (x @ x.T) / nrm2
+            lam = np.einsum("ij,ij->j", q, rho @ q)
+            res = np.max(np.abs(rho @ q - q * lam))
+            assert res <= 1e-13 * max(np.max(np.abs(rho)), 1e-300), (sub.num_up, sub.num_down, res)
+            checked += q.shape[1]
+    assert checked > 500
+
+
 @pytest.mark.parametrize("wl", ["small", "small_gc", "cyl4"])
 def test_correlators(ctx, oracle_lib, wl):
     from oracle import oracle
