@@ -294,7 +294,8 @@ def sweep_leg(ctx64, ctxoz, name: str, prep: str, seed: int):
             setattr(d, k, dict(v))
         d.wave = snap[1].copy()
         d.rng.bit_generator.state = snap[2]
-        d.be = DeviceBackend(ctx)
+        trace = []
+        d.be = DeviceBackend(ctx, trace)
         n0 = len(d.records)
         t = time.perf_counter()
         d.left_to_right(1, N - 2, restart=True, phase="L->R")
@@ -306,6 +307,19 @@ def sweep_leg(ctx64, ctxoz, name: str, prep: str, seed: int):
                     "E_end": recs[-1].energy, "E_min": min(r.energy for r in recs),
                     "max_trunc_err": max(r.trunc_err for r in recs), "max_psi_dim": max(r.dim for r in recs),
                     "seconds": {k[2:]: v for k, v in agg.items()}}
+        tr = [st for name, st in trace if name == "truncation"]
+        stages = ("rho", "tridiag", "eig", "select", "vec", "orth", "back", "total")
+        out[tag]["truncation_ms"] = {k: sum(getattr(st, "trunc_ms_" + k) for st in tr) for k in stages}
+        out[tag]["truncation_ms"]["max_sector"] = max(st.trunc_max_n for st in tr)
+        out[tag]["truncation_ms"]["max_kept_block"] = max(st.trunc_max_kept for st in tr)
+        rn = [st for name, st in trace if name == "get_hamiltonian"]
+        out[tag]["renorm_ms"] = {"plan": sum(st.renorm_plan_ms for st in rn), "gemm": sum(st.renorm_ms for st in rn),
+                                 "call": sum(st.renorm_e2e_ms for st in rn),
+                                 "tflops": sum(st.renorm_flops for st in rn) / max(sum(st.renorm_ms for st in rn), 1e-9) / 1e9}
+        lz = [st for name, st in trace if name == "lanczos"]
+        out[tag]["lanczos_ms"] = {"prepare": sum(st.prepare_ms for st in lz), "plan": sum(st.plan_ms for st in lz),
+                                  "split_plan": sum(st.ozplan_ms for st in lz),
+                                  "iterations": sum(st.lanczos_ms for st in lz)}
         return recs
 
     r64 = one(ctx64, "fp64")

@@ -48,6 +48,8 @@ tj_ctx::~tj_ctx() {
   for (DevBuf *b : all_bufs()) b->release();
   for (auto &e : ev)
     if (e) cudaEventDestroy(e);
+  for (auto &e : tev)
+    if (e) cudaEventDestroy(e);
   if (stream) cudaStreamDestroy(stream);
   if (pinned) cudaFreeHost(pinned);
 }
@@ -67,6 +69,7 @@ extern "C" int tj_ctx_create(tj_ctx **out, int device) {
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   CK(cudaMallocHost((void **)&c->pinned, 32 * sizeof(double)));
   for (auto &e : c->ev) CK(cudaEventCreate(&e));
+  for (auto &e : c->tev) CK(cudaEventCreate(&e));
   *out = c.release();
   return TJ_OK;
 }

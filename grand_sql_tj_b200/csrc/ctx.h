@@ -49,6 +49,7 @@ struct tj_ctx {
   // H*psi timing: 0 start, 1 after the splits of psi, 2 after the first GEMM
   // launch, 3 after the product splits, 4 end (FP64: 1 = 0 and 3 = 2)
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t tev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};   // truncation stages
   int prec_mode = TJ_PREC_FP64, slices = 6;
   double wait_s = 2.0;        // limit of the split-precision GEMM's pipeline waits (tj_set_wait_limit)
   // tiling / schedule choices in use, and how they are chosen (TJ_TUNE_*)

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -544,6 +545,8 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
   if (!hit) {
     CKT(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
+    const auto wall0 = std::chrono::steady_clock::now();
+    CKT(cudaEventRecord(ctx->tev[0], st));
     // psi on the device and its norm
     int rc;
     if ((rc = ctx->trA.reserve(sizeof(double) * (D + 4)))) return rc;
@@ -642,12 +645,14 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     g.counter = (unsigned int *)(tbase + p_cnt);
     launch_grouped_gemm(g, grouped_gemm_grid(g.ntiles), st);
     CKT(cudaGetLastError());
+    CKT(cudaEventRecord(ctx->tev[1], st));
     // tridiagonal reduction, then all eigenvalues
     const size_t tsm = sizeof(double) * (3 * (size_t)maxn + std::max(maxn, EIG_THREADS));
     CKT(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
     tridiag_kernel<<<nsec, EIG_THREADS, tsm, st>>>(ctx->trB.d(), d_roff, d_dims, d_eoff,
                                                    (const int *)(tbase + p_order), dd, de, dtau, dinfo);
     CKT(cudaGetLastError());
+    CKT(cudaEventRecord(ctx->tev[2], st));
     if (etot) {
       bisect_kernel<<<(unsigned)((etot + 127) / 128), 128, 0, st>>>(dd, de, d_eoff, d_dims, dinfo,
                                                                     (const int *)(tbase + p_esec), (int)etot, dev);
@@ -655,7 +660,13 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     }
     std::vector<double> ev(etot);
     CKT(cudaMemcpyAsync(ev.data(), dev, sizeof(double) * etot, cudaMemcpyDeviceToHost, st));
+    CKT(cudaEventRecord(ctx->tev[3], st));
     CKT(cudaStreamSynchronize(st));
+    const auto sel0 = std::chrono::steady_clock::now();
+    float stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < 3; ++i) CKT(cudaEventElapsedTime(&stage_ms[i], ctx->tev[i], ctx->tev[i + 1]));
+    double select_ms = 0;
+    int max_kept = 0;
 
     // ---- selection (den_mat.f90:201-330) ----
     std::vector<int> qnu(nsec), qnd(nsec);
@@ -773,14 +784,19 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       CKT(cudaMemcpyAsync(ab + q_grp, grp.data(), grp.size() * 4, cudaMemcpyHostToDevice, st));
       CKT(cudaMemcpyAsync(ab + q_slab, slab.data(), slab.size() * 4, cudaMemcpyHostToDevice, st));
       double *Y = (double *)(cb + p_y), *d_out = (double *)(ab + q_out);
+      for (int b = 0; b < ngrp; ++b) max_kept = std::max(max_kept, grp[4 * b + 2]);
+      select_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - sel0).count();
+      CKT(cudaEventRecord(ctx->tev[4], st));
       inverse_iter_kernel<<<(njobs + 63) / 64, 64, 0, st>>>(dd, de, d_eoff, d_dims, dinfo, dev,
                                                             (const int *)(ab + q_sec), (const int *)(ab + q_k), njobs,
                                                             maxn, (double *)(cb + p_work),
                                                             (unsigned char *)(cb + p_piv), Y, ldy, d_status);
       CKT(cudaGetLastError());
+      CKT(cudaEventRecord(ctx->tev[5], st));
       orthonormalize_kernel<<<ngrp, ORTH_THREADS, sizeof(double) * maxn, st>>>(
           (const int *)(ab + q_grp), d_dims, d_eoff, dev, dinfo, (const int *)(ab + q_k), Y, ldy, d_status);
       CKT(cudaGetLastError());
+      CKT(cudaEventRecord(ctx->tev[6], st));
       const size_t bsm = sizeof(double) * (size_t)W * ldy;
       CKT(cudaFuncSetAttribute(backtransform_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
       backtransform_kernel<<<nslab, 32 * W, bsm, st>>>(ctx->trB.d(), d_roff, dtau, d_eoff, d_dims,
@@ -790,7 +806,9 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       int status[16] = {0};
       CKT(cudaMemcpyAsync(tc.mats.data(), d_out, sizeof(double) * dpos, cudaMemcpyDeviceToHost, st));
       CKT(cudaMemcpyAsync(status, d_status, sizeof status, cudaMemcpyDeviceToHost, st));
+      CKT(cudaEventRecord(ctx->tev[7], st));
       CKT(cudaStreamSynchronize(st));
+      for (int i = 4; i < 7; ++i) CKT(cudaEventElapsedTime(&stage_ms[i - 1], ctx->tev[i], ctx->tev[i + 1]));
       if (status[0] & 1) {
         double dg[6];
         std::memcpy(dg, status + 4, sizeof dg);
@@ -805,6 +823,19 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
         return set_err(TJ_ERR_NUMERIC,
                        "tj_truncation: inverse iteration gave linearly dependent eigenvectors for a cluster of "
                        "eigenvalues above the bottom of its sector's spectrum");
+    }
+    {
+      tj_hpsi_stats &S = ctx->stats;
+      S.trunc_ms_rho = stage_ms[0];
+      S.trunc_ms_tridiag = stage_ms[1];
+      S.trunc_ms_eig = stage_ms[2];
+      S.trunc_ms_select = select_ms;
+      S.trunc_ms_vec = stage_ms[3];
+      S.trunc_ms_orth = stage_ms[4];
+      S.trunc_ms_back = stage_ms[5];
+      S.trunc_ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
+      S.trunc_max_n = maxn;
+      S.trunc_max_kept = max_kept;
     }
     std::memset(&tc.res, 0, sizeof tc.res);
     tc.res.num_state = num_state;

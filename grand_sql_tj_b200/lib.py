@@ -509,17 +509,23 @@ def wave_trans_plan_export(direction: int, sys_bs, env_bs, sys_trun: Block, env_
 class DeviceBackend:
     """The hot-path calls of grand_sql_tj_b200.sweep.Dmrg on the B200, through the C ABI."""
 
-    def __init__(self, ctx: Context):
+    def __init__(self, ctx: Context, trace: Optional[list] = None):
         self.ctx = ctx
+        self.trace = trace   # if a list: (call, the context's statistics after it) per step call
+
+    def _traced(self, name, r):
+        if self.trace is not None:
+            self.trace.append((name, self.ctx.stats()))
+        return r
 
     def lanczos(self, lat, sys, env, sys_bs, env_bs, wave, lanzero):
-        return self.ctx.lanczos(lat, sys, env, sys_bs, env_bs, wave, lanzero)
+        return self._traced("lanczos", self.ctx.lanczos(lat, sys, env, sys_bs, env_bs, wave, lanzero))
 
     def truncation(self, wave, side, kept_min, kept_max, trun_err):
-        return self.ctx.truncation(wave, side, kept_min, kept_max, trun_err)
+        return self._traced("truncation", self.ctx.truncation(wave, side, kept_min, kept_max, trun_err))
 
     def get_hamiltonian(self, lat, side, mshift, pre, basis, trun):
-        return self.ctx.get_hamiltonian(lat, side, mshift, pre, basis, trun)
+        return self._traced("get_hamiltonian", self.ctx.get_hamiltonian(lat, side, mshift, pre, basis, trun))
 
     def wave_trans(self, direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave):
         return self.ctx.wave_trans(direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave)

@@ -117,7 +117,11 @@ class TjHpsiStats(C.Structure):
                 ("prepare_ms", C.c_double), ("plan_ms", C.c_double), ("upload_ms", C.c_double),
                 ("ozplan_ms", C.c_double), ("lanczos_ms", C.c_double),
                 ("renorm_plan_ms", C.c_double), ("renorm_ms", C.c_double), ("renorm_e2e_ms", C.c_double),
-                ("renorm_flops", C.c_double)]
+                ("renorm_flops", C.c_double),
+                ("trunc_ms_rho", C.c_double), ("trunc_ms_tridiag", C.c_double), ("trunc_ms_eig", C.c_double),
+                ("trunc_ms_select", C.c_double), ("trunc_ms_vec", C.c_double), ("trunc_ms_orth", C.c_double),
+                ("trunc_ms_back", C.c_double), ("trunc_ms_total", C.c_double),
+                ("trunc_max_n", C.c_int64), ("trunc_max_kept", C.c_int64)]
 
 
 class TjTuneResult(C.Structure):

@@ -420,6 +420,16 @@ typedef struct tj_hpsi_stats {
    * its two GEMM launches (ms), the whole call from the first upload to the
    * end of the download (ms), and its FP64 flops */
   double renorm_plan_ms, renorm_ms, renorm_e2e_ms, renorm_flops;
+  /* the last tj_truncation that computed (not the cached second call):
+   * device time (ms) of psi's upload and the density matrices, the
+   * tridiagonal reductions, the eigenvalues (with their download), the host
+   * keep rule, inverse iteration of the kept vectors, their
+   * orthonormalisation, the back-transformation and download; the whole
+   * call (host wall time); the largest density-matrix sector and the largest
+   * kept block */
+  double trunc_ms_rho, trunc_ms_tridiag, trunc_ms_eig, trunc_ms_select, trunc_ms_vec, trunc_ms_orth,
+      trunc_ms_back, trunc_ms_total;
+  int64_t trunc_max_n, trunc_max_kept;
 } tj_hpsi_stats;
 int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st);
 

