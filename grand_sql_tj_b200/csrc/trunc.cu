@@ -28,7 +28,11 @@
 #include <string>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "ctx.h"
+
+namespace cg = cooperative_groups;
 
 namespace tjb {
 
@@ -37,6 +41,8 @@ constexpr int EIG_MAX_N = 4096;
 constexpr double EIG_EPS = 2.220446049250313e-16;        // 2^-52
 constexpr double EIG_SAFMIN = 2.2250738585072014e-308;   // smallest normal FP64
 constexpr int ORTH_THREADS = 512;
+constexpr int TD_CL = 8;          // CTAs of a tridiagonalisation cluster
+constexpr int TD_BIG = 320;       // sectors of at least this many states are reduced by a whole cluster
 
 // Sum of one value per thread over the block, in a fixed order; every thread
 // receives it.  red holds 32 doubles of shared memory.
@@ -60,14 +66,26 @@ __device__ __forceinline__ double block_sum(double x, double *red) {
 // the Sturm-count pivot floor.  The rank-2 update of step k,
 // A <- A - v w^T - w v^T, is applied lazily inside the matrix-vector product
 // p = A v of step k+1, so each step reads and writes the trailing block once.
-// One CTA per sector; order[] lists the sectors largest first.
-__global__ void __launch_bounds__(EIG_THREADS) tridiag_kernel(double *Aall, const int64_t *off, const int *dims,
-                                                             const int64_t *eoff, const int *order, double *dall,
-                                                             double *eall, double *tauall, double *info) {
-  extern __shared__ double sm[];
-  __shared__ double red[32];
-  __shared__ double sh_tau, sh_scl;
-  const int s = order[blockIdx.x], n = dims[s], tid = threadIdx.x, nt = blockDim.x;
+// One CTA per sector (tridiag_one) or one cluster per large sector
+// (tridiag_coop).
+__device__ __forceinline__ void tridiag_info(int s, int n, const double *d, const double *e, double *info) {
+  double gl = 1e308, gu = -1e308, emax2 = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double el = i > 0 ? fabs(e[i - 1]) : 0.0, er = i + 1 < n ? fabs(e[i]) : 0.0;
+    gl = fmin(gl, d[i] - el - er);
+    gu = fmax(gu, d[i] + el + er);
+    if (i + 1 < n) emax2 = fmax(emax2, e[i] * e[i]);
+  }
+  info[4 * s + 0] = gl;
+  info[4 * s + 1] = gu;
+  info[4 * s + 2] = fmax(fabs(gl), fabs(gu));
+  info[4 * s + 3] = EIG_SAFMIN * fmax(1.0, emax2);
+}
+
+__device__ void tridiag_one(int s, double *Aall, const int64_t *off, const int *dims, const int64_t *eoff,
+                            double *dall, double *eall, double *tauall, double *info, double *sm, double *red,
+                            double &sh_tau, double &sh_scl) {
+  const int n = dims[s], tid = threadIdx.x, nt = blockDim.x;
   double *A = Aall + off[s];
   double *d = dall + eoff[s], *e = eall + eoff[s], *tau = tauall + eoff[s];
   double *vp = sm, *wp = vp + n, *v = wp + n, *part = v + n;   // part: max(n, nt) entries
@@ -154,17 +172,138 @@ __global__ void __launch_bounds__(EIG_THREADS) tridiag_kernel(double *Aall, cons
   if (tid == 0) {
     d[n - 1] = A[(int64_t)(n - 1) * n + (n - 1)];
     if (n >= 1) tau[n - 1] = 0.0;
-    double gl = 1e308, gu = -1e308, emax2 = 0.0;
-    for (int i = 0; i < n; ++i) {
-      const double el = i > 0 ? fabs(e[i - 1]) : 0.0, er = i + 1 < n ? fabs(e[i]) : 0.0;
-      gl = fmin(gl, d[i] - el - er);
-      gu = fmax(gu, d[i] + el + er);
-      if (i + 1 < n) emax2 = fmax(emax2, e[i] * e[i]);
+    tridiag_info(s, n, d, e, info);
+  }
+}
+
+// The same reduction of one large sector by the TD_CL CTAs of a thread-block
+// cluster.  Every CTA forms column k itself (the pending update applied; the
+// same arithmetic in the same order, so the same reflector everywhere); CTA
+// c owns the trailing columns j = c (mod TD_CL), applies the pending rank-2
+// update to them and forms its part of p = A v; the parts meet in shared
+// memory across the cluster (distributed shared memory, two buffers
+// alternating by step) and every CTA sums them in rank order.  One cluster
+// barrier per step orders the owners' column writes (global memory) and the
+// parts before they are read.  The owner of column k stores its reflector
+// there only after that barrier, when no CTA reads the column any more.
+__device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aall, const int64_t *off,
+                             const int *dims, const int64_t *eoff, double *dall, double *eall, double *tauall,
+                             double *info, double *sm, double *red, double &sh_tau, double &sh_scl) {
+  const int n = dims[s], tid = threadIdx.x, nt = blockDim.x;
+  double *A = Aall + off[s];
+  double *d = dall + eoff[s], *e = eall + eoff[s], *tau = tauall + eoff[s];
+  // vp, wp, v: n each; part: max(n, nt); cp: the cluster parts, 2 x n
+  double *vp = sm, *wp = vp + n, *v = wp + n, *part = v + n, *cp = part + max(n, nt);
+  bool pending = false;
+  for (int k = 0; k + 1 < n; ++k) {
+    const int k1 = k + 1, m = n - k1;
+    const bool owner = (k % TD_CL) == rank;
+    double *colk = A + (int64_t)k * n;
+    double ss = 0.0;
+    for (int i = k + tid; i < n; i += nt) {
+      double a = colk[i];
+      if (pending) a -= vp[i] * wp[k] + wp[i] * vp[k];
+      v[i] = a;
+      if (i > k1) ss += a * a;
     }
-    info[4 * s + 0] = gl;
-    info[4 * s + 1] = gu;
-    info[4 * s + 2] = fmax(fabs(gl), fabs(gu));
-    info[4 * s + 3] = EIG_SAFMIN * fmax(1.0, emax2);
+    const double sigma2 = block_sum(ss, red);
+    if (tid == 0) {
+      const double alpha = v[k1];
+      double beta = alpha, t = 0.0, scl = 0.0;
+      if (sigma2 > 0.0) {
+        const double nr = sqrt(alpha * alpha + sigma2);
+        beta = alpha >= 0.0 ? -nr : nr;
+        t = (beta - alpha) / beta;
+        scl = 1.0 / (alpha - beta);
+      }
+      if (owner) {
+        d[k] = v[k];
+        e[k] = beta;
+        tau[k] = t;
+      }
+      sh_tau = t;
+      sh_scl = scl;
+    }
+    __syncthreads();
+    const double t = sh_tau, scl = sh_scl;
+    for (int i = k1 + tid; i < n; i += nt) v[i] = i == k1 ? 1.0 : v[i] * scl;
+    __syncthreads();
+    // owned trailing columns j0, j0 + TD_CL, ...
+    const int j0 = k1 + ((rank - k1) % TD_CL + TD_CL) % TD_CL;
+    const int mloc = j0 < n ? (n - 1 - j0) / TD_CL + 1 : 0;
+    const int R = min((m + 31) & ~31, nt), G = nt / R;
+    const int g = tid / R, r = tid - g * R;
+    if (g < G) {
+      for (int ii = r; ii < m; ii += R) {
+        const int i = k1 + ii;
+        const double vpi = pending ? vp[i] : 0.0, wpi = pending ? wp[i] : 0.0;
+        double acc = 0.0;
+        for (int q = g; q < mloc; q += G) {
+          const int j = j0 + q * TD_CL;
+          double *a = A + (int64_t)j * n + i;
+          double x = *a;
+          if (pending) {
+            x -= vpi * wp[j] + wpi * vp[j];
+            *a = x;
+          }
+          acc += x * v[j];
+        }
+        part[g * m + ii] = acc;
+      }
+    }
+    __syncthreads();
+    double *mine = cp + (k & 1) * n;
+    for (int ii = tid; ii < m; ii += nt) {
+      double p = 0.0;
+      for (int q = 0; q < G; ++q) p += part[q * m + ii];
+      mine[ii] = p;
+    }
+    __threadfence();
+    cl.sync();
+    if (owner)
+      for (int i = k1 + tid; i < n; i += nt) colk[i] = v[i];
+    double pv = 0.0;
+    for (int ii = tid; ii < m; ii += nt) {
+      double p = 0.0;
+      for (int c = 0; c < TD_CL; ++c) p += cl.map_shared_rank(mine, c)[ii];
+      p *= t;
+      part[ii] = p;
+      pv += p * v[k1 + ii];
+    }
+    const double K = 0.5 * t * block_sum(pv, red);
+    for (int ii = tid; ii < m; ii += nt) {
+      const int i = k1 + ii;
+      wp[i] = part[ii] - K * v[i];
+      vp[i] = v[i];
+    }
+    pending = true;
+    __syncthreads();
+  }
+  __threadfence();
+  cl.sync();   // the last parts are read; every owner's writes are visible
+  if (rank == 0 && tid == 0) {
+    d[n - 1] = A[(int64_t)(n - 1) * n + (n - 1)];
+    tau[n - 1] = 0.0;
+    tridiag_info(s, n, d, e, info);
+  }
+}
+
+// One cluster of TD_CL CTAs per entry of the cluster list: a large sector
+// shared by all of them (tbig), or up to TD_CL small sectors, one per CTA
+// (tsec[cluster * TD_CL + rank], -1 for none).  Sectors largest first.
+__global__ void __cluster_dims__(TD_CL, 1, 1) __launch_bounds__(EIG_THREADS)
+    tridiag_kernel(double *Aall, const int64_t *off, const int *dims, const int64_t *eoff, const int *tsec,
+                   const int *tbig, double *dall, double *eall, double *tauall, double *info) {
+  extern __shared__ double sm[];
+  __shared__ double red[32];
+  __shared__ double sh_tau, sh_scl;
+  cg::cluster_group cl = cg::this_cluster();
+  const int b = blockIdx.x / TD_CL, rank = (int)cl.block_rank();
+  const int s = tsec[blockIdx.x];
+  if (tbig[b]) {
+    tridiag_coop(cl, rank, s, Aall, off, dims, eoff, dall, eall, tauall, info, sm, red, sh_tau, sh_scl);
+  } else if (s >= 0 && dims[s] > 0) {
+    tridiag_one(s, Aall, off, dims, eoff, dall, eall, tauall, info, sm, red, sh_tau, sh_scl);
   }
 }
 
@@ -616,7 +755,26 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     const size_t p_roff = pos; pos += al256(ob);
     const size_t p_eoff = pos; pos += al256(ob);
     const size_t p_dims = pos; pos += al256(db);
-    const size_t p_order = pos; pos += al256(db);
+    // clusters of the tridiagonal reduction: one per large sector, then the
+    // small sectors TD_CL at a time (largest first)
+    std::vector<int> tsec, tbig;
+    {
+      size_t q = 0;
+      for (; q < order.size() && dims[order[q]] >= TD_BIG; ++q) {
+        tsec.insert(tsec.end(), TD_CL, order[q]);
+        tbig.push_back(1);
+      }
+      std::vector<int> small;
+      for (; q < order.size(); ++q)
+        if (dims[order[q]] > 0) small.push_back(order[q]);
+      for (size_t i = 0; i < small.size(); i += TD_CL) {
+        for (int r = 0; r < TD_CL; ++r) tsec.push_back(i + r < small.size() ? small[i + r] : -1);
+        tbig.push_back(0);
+      }
+    }
+    const int nclus = (int)tbig.size();
+    const size_t p_tsec = pos; pos += al256(sizeof(int) * std::max<size_t>(tsec.size(), 1));
+    const size_t p_tbig = pos; pos += al256(sizeof(int) * std::max<size_t>(tbig.size(), 1));
     const size_t p_esec = pos; pos += al256(sizeof(int) * (size_t)std::max<int64_t>(etot, 1));
     const size_t p_cnt = pos; pos += 256;
     if ((rc = ctx->trE.reserve(pos))) return rc;
@@ -627,7 +785,10 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     CKT(cudaMemcpyAsync(tbase + p_roff, roff.data(), ob, cudaMemcpyHostToDevice, st));
     CKT(cudaMemcpyAsync(tbase + p_eoff, eoff.data(), ob, cudaMemcpyHostToDevice, st));
     CKT(cudaMemcpyAsync(tbase + p_dims, dims.data(), db, cudaMemcpyHostToDevice, st));
-    CKT(cudaMemcpyAsync(tbase + p_order, order.data(), db, cudaMemcpyHostToDevice, st));
+    if (nclus) {
+      CKT(cudaMemcpyAsync(tbase + p_tsec, tsec.data(), sizeof(int) * tsec.size(), cudaMemcpyHostToDevice, st));
+      CKT(cudaMemcpyAsync(tbase + p_tbig, tbig.data(), sizeof(int) * tbig.size(), cudaMemcpyHostToDevice, st));
+    }
     if (etot) CKT(cudaMemcpyAsync(tbase + p_esec, esec.data(), sizeof(int) * etot, cudaMemcpyHostToDevice, st));
     CKT(cudaMemsetAsync(tbase + p_cnt, 0, 256, st));
     const int64_t *d_roff = (const int64_t *)(tbase + p_roff), *d_eoff = (const int64_t *)(tbase + p_eoff);
@@ -647,11 +808,14 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     CKT(cudaGetLastError());
     CKT(cudaEventRecord(ctx->tev[1], st));
     // tridiagonal reduction, then all eigenvalues
-    const size_t tsm = sizeof(double) * (3 * (size_t)maxn + std::max(maxn, EIG_THREADS));
-    CKT(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
-    tridiag_kernel<<<nsec, EIG_THREADS, tsm, st>>>(ctx->trB.d(), d_roff, d_dims, d_eoff,
-                                                   (const int *)(tbase + p_order), dd, de, dtau, dinfo);
-    CKT(cudaGetLastError());
+    const size_t tsm = sizeof(double) * (5 * (size_t)maxn + std::max(maxn, EIG_THREADS));
+    if (nclus) {
+      CKT(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+      tridiag_kernel<<<nclus * TD_CL, EIG_THREADS, tsm, st>>>(ctx->trB.d(), d_roff, d_dims, d_eoff,
+                                                              (const int *)(tbase + p_tsec),
+                                                              (const int *)(tbase + p_tbig), dd, de, dtau, dinfo);
+      CKT(cudaGetLastError());
+    }
     CKT(cudaEventRecord(ctx->tev[2], st));
     if (etot) {
       bisect_kernel<<<(unsigned)((etot + 127) / 128), 128, 0, st>>>(dd, de, d_eoff, d_dims, dinfo,
