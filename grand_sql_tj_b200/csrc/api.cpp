@@ -45,6 +45,7 @@ int tjb::dev_reserve(void **p, size_t *cap, size_t bytes) {
 
 tj_ctx::~tj_ctx() {
   cudaSetDevice(device);
+  tjb::res_clear(this);
   for (DevBuf *b : all_bufs()) b->release();
   for (auto &e : ev)
     if (e) cudaEventDestroy(e);
@@ -230,7 +231,7 @@ int tjb::install_plan(tj_ctx *ctx, std::unique_ptr<HpsiPlan> P, uint64_t h,
   if ((rc = ctx->ops.reserve(sizeof(double) * (P->ops_len + 4)))) return rc;
   for (const auto &u : P->uploads)
     if (u.n > 0)
-      CK(cudaMemcpyAsync(ctx->ops.d() + u.dst, u.src, sizeof(double) * u.n, cudaMemcpyHostToDevice, ctx->stream));
+      CK(upload(ctx, ctx->ops.d() + u.dst, u.src, u.n, ctx->stream));
   // the split-precision plan is built on the host while those copies run
   // (from page-locked memory they return at once; the table uploads below,
   // from pageable memory, wait for the stream to reach them)

@@ -31,6 +31,15 @@ struct DevBuf {
   }
 };
 
+// a block kept on the device for the caller's array [host, host + n)
+// (resident.cpp)
+struct ResEntry {
+  const double *host = nullptr;
+  int64_t n = 0;
+  double *dev = nullptr;
+  uint64_t stamp = 0, sample = 0;
+};
+
 }  // namespace tjb
 
 // compiled operator renormalisation of the last tj_get_hamiltonian call (renorm.cpp)
@@ -75,6 +84,10 @@ struct tj_ctx {
   tjb::DevBuf ggPool, ggOut, ggTab, ggSlots;                          // grouped block-GEMM benchmark
   tjb::DevBuf rnOps, rnTrun, rnScr, rnOut, rnSlots, rnTab;             // operator renormalisation
   tjb::DevBuf wtOps, wtOld, wtNew, wtScr, wtSlots, wtTab;              // wavefunction prediction
+  // device-resident blocks (tj_set_residency): budget in bytes (0: off)
+  std::vector<tjb::ResEntry> resident;
+  size_t res_budget = 0, res_bytes = 0;
+  uint64_t res_clock = 0;
   std::shared_ptr<tj_renorm_state> renorm;
   std::shared_ptr<tj_meas_state> meas;
   // split-precision H*psi
@@ -100,6 +113,13 @@ int prepare_hpsi(tj_ctx *ctx, const tj_lattice *lat, const tj_model *sys, const 
                  const tj_basis *sys_bs, const tj_basis *env_bs, const tj_wave *wave);
 int run_hpsi(tj_ctx *ctx, const double *in, double *out, bool timed);
 int check_device_flags(tj_ctx *ctx);
+// residency (resident.cpp): the device copy of host [p, p + n) if kept, else
+// null; keep the device copy dev_src of a host array the library filled;
+// drop all; an upload that reads the kept copy when there is one
+const double *res_find(tj_ctx *ctx, const double *p, int64_t n);
+int res_keep(tj_ctx *ctx, const double *host, int64_t n, const double *dev_src, cudaStream_t st);
+void res_clear(tj_ctx *ctx);
+cudaError_t upload(tj_ctx *ctx, double *dst, const double *src, int64_t n, cudaStream_t st);
 int reset_device_flags(tj_ctx *ctx);
 // wavefunction table checks shared by every entry point that takes a tj_wave:
 // null tables, negative sizes or offsets, a sector past wave->dim

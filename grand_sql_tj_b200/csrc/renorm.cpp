@@ -780,7 +780,7 @@ extern "C" int tj_get_hamiltonian(tj_ctx *ctx, const tj_lattice *lat, int side, 
     return rc;
   CKR(cudaEventRecord(ctx->ev[5], st));
   for (const auto &u : P.uploads)
-    if (u.n > 0) CKR(cudaMemcpyAsync(ctx->rnOps.d() + u.dst, u.src, sizeof(double) * u.n, cudaMemcpyHostToDevice, st));
+    if (u.n > 0) CKR(upload(ctx, ctx->rnOps.d() + u.dst, u.src, u.n, st));
   {
     int64_t lo = LLONG_MAX;
     for (int k = 0; k < trun->num; ++k) lo = std::min(lo, (int64_t)trun->sub[k].off);
@@ -842,6 +842,7 @@ extern "C" int tj_get_hamiltonian(tj_ctx *ctx, const tj_lattice *lat, int side, 
   ctx->stats.renorm_e2e_ms = all_ms;
   ctx->stats.renorm_flops = P.flops;
   fill_result(R, out);
+  if ((rc = res_keep(ctx, out->data, R.out_len, ctx->rnOut.d(), st))) return rc;
   return TJ_OK;
 }
 
@@ -948,7 +949,7 @@ int upload_op(tj_ctx *ctx, const tj_block &b, DevOp &d) {
   int rc = d.buf.reserve(sizeof(double) * (P.ops_len + 4));
   if (rc) return rc;
   for (const auto &u : P.uploads)
-    if (u.n > 0) CKR(cudaMemcpyAsync(d.buf.d() + u.dst, u.src, sizeof(double) * u.n, cudaMemcpyHostToDevice, ctx->stream));
+    if (u.n > 0) CKR(upload(ctx, d.buf.d() + u.dst, u.src, u.n, ctx->stream));
   return TJ_OK;
 }
 
@@ -1328,7 +1329,7 @@ extern "C" int tj_block_mul_block_ndia(tj_ctx *ctx, const tj_block *oper1, char 
     if ((rc = src.buf.reserve(sizeof(double) * (P.ops_len + 4)))) return rc;
     for (const auto &u : P.uploads)
       if (u.n > 0)
-        CKR(cudaMemcpyAsync(src.buf.d() + u.dst, u.src, sizeof(double) * u.n, cudaMemcpyHostToDevice, ctx->stream));
+        CKR(upload(ctx, src.buf.d() + u.dst, u.src, u.n, ctx->stream));
     auto find_bs = [&](int nu, int nd) {
       for (int x = 0; x < basis->num; ++x)
         if (basis->sub[x].new_num_up == nu && basis->sub[x].new_num_down == nd) return x;

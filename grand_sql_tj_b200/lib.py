@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 from typing import Optional, Tuple
 
 import numpy as np
@@ -171,6 +172,8 @@ def lib():
         L.tj_set_precision.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.tj_step_begin.argtypes = [C.c_void_p]
         L.tj_set_wait_limit.argtypes = [C.c_void_p, C.c_double]
+        L.tj_set_residency.argtypes = [C.c_void_p, C.c_double]
+        L.tj_residency_forget.argtypes = [C.c_void_p, C.c_void_p]
         L.tj_host_register.argtypes = [C.c_void_p, C.c_size_t]
         L.tj_host_unregister.argtypes = [C.c_void_p]
         hp = [C.c_void_p, P(TjLattice), P(TjModel), P(TjModel), P(TjBasis), P(TjBasis)]
@@ -247,7 +250,25 @@ class Context:
 
     def __init__(self, device: int = 0):
         self.h = C.c_void_p()
+        self.resident = False
         _chk(lib().tj_ctx_create(C.byref(self.h), device))
+
+    def set_residency(self, gigabytes: float):
+        """tj_set_residency: keep the blocks get_hamiltonian returns on the device
+        (budget in GB; 0 turns it off).  Each returned Model's array is dropped
+        from the device when the Model is freed."""
+        _chk(lib().tj_set_residency(self.h, float(gigabytes)))
+        self.resident = gigabytes > 0
+
+    def _forget_when_freed(self, arr: np.ndarray):
+        ref = weakref.ref(self)
+        ptr = arr.ctypes.data
+
+        def forget():
+            c = ref()
+            if c is not None and c.h:
+                lib().tj_residency_forget(c.h, C.c_void_p(ptr))
+        weakref.finalize(arr, forget)
 
     def close(self):
         if self.h:
@@ -367,6 +388,8 @@ class Context:
         rc, m = call_model_result(lambda r: lib().tj_get_hamiltonian(self.h, C.byref(lat.c), side, mshift,
                                                                      C.byref(pp.c), C.byref(pb.c), C.byref(pt.c), r))
         _chk(rc)
+        if self.resident:
+            self._forget_when_freed(m._packed.data)
         return m
 
     def wave_trans(self, direction: int, sys_bs, env_bs, sys_trun: Block, env_trun: Block, old: Wave,

@@ -158,6 +158,17 @@ int tj_set_precision(tj_ctx *ctx, int mode, int slices);
 int tj_set_wait_limit(tj_ctx *ctx, double seconds);
 /* Invalidates the operators and task lists cached for the current DMRG step. */
 int tj_step_begin(tj_ctx *ctx);
+/* No counterpart in the reference.  Keeps on the device, within a budget of
+ * `gigabytes` (0, the default: off), the blocks tj_get_hamiltonian writes
+ * into caller arrays; later uploads from inside such an array (tj_model_wave,
+ * tj_lanczos_memo_new, tj_get_hamiltonian, the measurement operators) copy
+ * the kept device data instead.  The caller must not modify a filled array
+ * while it is kept: tj_residency_forget(ctx, p) drops the array containing
+ * p (do so before freeing or reusing it).  A fingerprint of 64 values of
+ * each array, checked at every use, drops an entry whose array changed
+ * there; least recently used entries go first when the budget is full. */
+int tj_set_residency(tj_ctx *ctx, double gigabytes);
+int tj_residency_forget(tj_ctx *ctx, const void *host);
 const char *tj_last_error(void);
 /* No counterpart in the reference.  Page-locks (pins) `bytes` of the caller's
  * host memory at `p` for the lifetime of the registration, so that the
@@ -430,6 +441,10 @@ typedef struct tj_hpsi_stats {
   double trunc_ms_rho, trunc_ms_tridiag, trunc_ms_eig, trunc_ms_select, trunc_ms_vec, trunc_ms_orth,
       trunc_ms_back, trunc_ms_total;
   int64_t trunc_max_n, trunc_max_kept;
+  /* residency (tj_set_residency): uploads served from kept device copies
+   * since the context was created, and their bytes */
+  int64_t res_hits;
+  double res_hit_bytes;
 } tj_hpsi_stats;
 int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st);
 

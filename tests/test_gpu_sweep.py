@@ -102,3 +102,37 @@ def test_device_run_matches_oracle_run(ctx, oracle_lib):
         assert a.num_state == b.num_state
         if max(a.trunc_err, b.trunc_err) > 1e-13:
             assert abs(a.trunc_err - b.trunc_err) <= 0.1 * max(a.trunc_err, b.trunc_err)
+
+
+def test_residency_gives_the_same_run(product_lib):
+    """Blocks kept on the device (tj_set_residency) give the same run as
+    uploads from the host arrays, bit for bit, with uploads served from the
+    kept copies; a kept array that the caller changes where its fingerprint
+    looks is dropped and read from the host again."""
+    from grand_sql_tj_b200.lib import Context, DeviceBackend
+    p = DmrgParams(n_elec=14, kept_min=32, kept_max=48, seed=11, lanzero=1e-10, lanzero_warm=1e-10)
+    c0, c1 = Context(0), Context(0)
+    try:
+        c1.set_residency(2.0)
+        geo = Geometry(8, 2, t=1.0, J=1.0 / 3.0, esite=0.0, up_bias=1)
+        ref = Dmrg(Geometry(8, 2, t=1.0, J=1.0 / 3.0, esite=0.0, up_bias=1), DeviceBackend(c0), p).ground_state(1)
+        d = Dmrg(geo, DeviceBackend(c1), p)
+        got = d.ground_state(1)
+        assert c1.stats().res_hits > 20 and c0.stats().res_hits == 0
+        assert [r.energy for r in got] == [r.energy for r in ref]
+        assert [r.trunc_err for r in got] == [r.trunc_err for r in ref]
+        L = 5
+        lat = geo.lattice(L, geo.num_site - L - 2)
+        pre = d.sysblocks[L]
+        a = c1.get_hamiltonian(lat, 0, 0, pre, d.sysbs[L + 1], d.systruns[L + 1])
+        b = c0.get_hamiltonian(lat, 0, 0, pre, d.sysbs[L + 1], d.systruns[L + 1])
+        assert np.array_equal(a._packed.data, b._packed.data)
+        hits = c1.stats().res_hits
+        pre._packed.data[0] += 1.0
+        a = c1.get_hamiltonian(lat, 0, 0, pre, d.sysbs[L + 1], d.systruns[L + 1])
+        b = c0.get_hamiltonian(lat, 0, 0, pre, d.sysbs[L + 1], d.systruns[L + 1])
+        assert np.array_equal(a._packed.data, b._packed.data)
+        assert c1.stats().res_hits == hits
+    finally:
+        c0.close()
+        c1.close()
