@@ -118,6 +118,8 @@ extern "C" int tj_host_unregister(void *p) {
 extern "C" int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st) {
   if (!ctx || !st) return set_err(TJ_ERR_ARG, "null argument");
   *st = ctx->stats;
+  st->res_hits = ctx->res_hits;
+  st->res_hit_bytes = ctx->res_hit_bytes;
   return TJ_OK;
 }
 

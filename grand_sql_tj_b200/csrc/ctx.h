@@ -88,6 +88,8 @@ struct tj_ctx {
   std::vector<tjb::ResEntry> resident;
   size_t res_budget = 0, res_bytes = 0;
   uint64_t res_clock = 0;
+  int64_t res_hits = 0;       // uploads served from kept copies since creation
+  double res_hit_bytes = 0;
   std::shared_ptr<tj_renorm_state> renorm;
   std::shared_ptr<tj_meas_state> meas;
   // split-precision H*psi

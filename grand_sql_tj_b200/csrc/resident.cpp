@@ -59,8 +59,8 @@ const double *res_find(tj_ctx *ctx, const double *p, int64_t n) {
       return nullptr;
     }
     e.stamp = ++ctx->res_clock;
-    ++ctx->stats.res_hits;
-    ctx->stats.res_hit_bytes += 8.0 * (double)n;
+    ++ctx->res_hits;
+    ctx->res_hit_bytes += 8.0 * (double)n;
     return e.dev + (p - e.host);
   }
   return nullptr;

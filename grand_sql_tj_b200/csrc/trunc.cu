@@ -516,13 +516,10 @@ __global__ void inverse_iter_kernel(const double *dall, const double *eall, cons
 // good as any basis DSYEV returns for it.  Up to four such vectors are tried.
 // status bit 1: a vector stayed dependent (or its cluster is not at the
 // bottom of the spectrum).
-__global__ void __launch_bounds__(ORTH_THREADS) orthonormalize_kernel(const int *grp, const int *dims,
-                                                                      const int64_t *eoff, const double *evals,
-                                                                      const double *info, const int *job_k,
-                                                                      double *Y, int ldy, int *status) {
-  extern __shared__ double h[];
-  __shared__ double red[32];
-  const int s = grp[4 * blockIdx.x], j0 = grp[4 * blockIdx.x + 1], cnt = grp[4 * blockIdx.x + 2];
+__device__ void ortho_one(int blk, const int *grp, const int *dims, const int64_t *eoff, const double *evals,
+                          const double *info, const int *job_k, double *Y, int ldy, int *status, double *h,
+                          double *red) {
+  const int s = grp[4 * blk], j0 = grp[4 * blk + 1], cnt = grp[4 * blk + 2];
   const int n = dims[s], tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   const double lam_min = evals[eoff[s]], cluster = 1e4 * EIG_EPS * info[4 * s + 2];
   for (int t = 1; t < cnt; ++t) {
@@ -572,6 +569,118 @@ __global__ void __launch_bounds__(ORTH_THREADS) orthonormalize_kernel(const int 
     }
     if (!ok && tid == 0) atomicOr(status, 2);
   }
+}
+
+// The same orthonormalisation of one large kept block by the TD_CL CTAs of a
+// cluster: CTA c owns a slice of rows of every vector.  Per projection pass
+// each CTA forms its part of the dot products with the accepted vectors, the
+// parts meet through distributed shared memory, every CTA sums them in rank
+// order (so every CTA holds the same coefficients and takes the same
+// decisions), subtracts on its own rows, and the squared norm is summed the
+// same way.  Each exchange uses the buffer of its parity and ends with one
+// cluster barrier; a buffer is written again only two exchanges later, after
+// every CTA has passed the barrier that follows its reads.  A CTA reads and
+// writes only its own rows of the vectors in global memory.
+__device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *grp, const int *dims,
+                           const int64_t *eoff, const double *evals, const double *info, const int *job_k, double *Y,
+                           int ldy, int *status, double *sm, double *red) {
+  const int s = grp[4 * blk], j0 = grp[4 * blk + 1], cnt = grp[4 * blk + 2];
+  const int n = dims[s], tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  const double lam_min = evals[eoff[s]], cluster = 1e4 * EIG_EPS * info[4 * s + 2];
+  const int per = (n + TD_CL - 1) / TD_CL, r0 = min(n, rank * per), r1 = min(n, r0 + per), nr = r1 - r0;
+  // hp: parts of the dots (2 x cnt), h: the dots (cnt), ys: own rows of the
+  // vector (per), sl: parts of the squared norm (2)
+  double *hp = sm, *h = hp + 2 * cnt, *ys = h + cnt, *sl = ys + per;
+  unsigned xch = 0;   // exchanges so far (buffer parity)
+  auto cluster_sum = [&](double x) -> double {   // x: the CTA's value, the same in all its threads
+    double *slot = sl + (xch & 1);
+    if (tid == 0) *slot = x;
+    cl.sync();
+    ++xch;
+    double tot = 0.0;
+    for (int c = 0; c < TD_CL; ++c) tot += *cl.map_shared_rank(slot, c);
+    return tot;
+  };
+  auto vec = [&](int q) { return Y + (size_t)(j0 + cnt - 1 - q) * ldy; };   // q-th vector in descending order
+  for (int t = 1; t < cnt; ++t) {
+    double *y = vec(t);
+    const int jt = j0 + cnt - 1 - t;
+    bool ok = false;
+    for (int attempt = 0; attempt < 5 && !ok; ++attempt) {
+      if (attempt == 0) {
+        for (int i = tid; i < nr; i += nt) ys[i] = y[r0 + i];
+        __syncthreads();
+      } else {   // a fresh pseudo-random unit vector (see ortho_one)
+        double ss = 0.0;
+        for (int i = tid; i < nr; i += nt) {
+          const double v = start_entry(s, job_k[jt] + 4096 * attempt, r0 + i);
+          ys[i] = v;
+          ss += v * v;
+        }
+        const double inv = 1.0 / sqrt(cluster_sum(block_sum(ss, red)));
+        for (int i = tid; i < nr; i += nt) ys[i] *= inv;
+        __syncthreads();
+      }
+      ok = true;
+      for (int pass = 0; pass < 2; ++pass) {
+        double *hpw = hp + (xch & 1) * cnt;
+        for (int q = warp; q < t; q += nw) {
+          const double *z = vec(q) + r0;
+          double acc = 0.0;
+          for (int i = lane; i < nr; i += 32) acc += z[i] * ys[i];
+          for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+          if (lane == 0) hpw[q] = acc;
+        }
+        cl.sync();
+        ++xch;
+        for (int q = tid; q < t; q += nt) {
+          double tot = 0.0;
+          for (int c = 0; c < TD_CL; ++c) tot += cl.map_shared_rank(hpw, c)[q];
+          h[q] = tot;
+        }
+        __syncthreads();
+        double ss = 0.0;
+        for (int i = tid; i < nr; i += nt) {
+          double acc = ys[i];
+          for (int q = 0; q < t; ++q) acc -= h[q] * vec(q)[r0 + i];
+          ys[i] = acc;
+          ss += acc * acc;
+        }
+        const double nrm = sqrt(cluster_sum(block_sum(ss, red)));   // the same value in every CTA
+        if (pass == 0 && !(nrm >= 1e-3)) {
+          ok = false;
+          break;
+        }
+        const double inv = 1.0 / nrm;
+        for (int i = tid; i < nr; i += nt) ys[i] *= inv;
+        __syncthreads();
+        if (nrm > 0.7071067811865476) break;
+      }
+      if (!ok && attempt == 0 && !(evals[eoff[s] + job_k[jt]] - lam_min <= cluster)) break;
+    }
+    for (int i = tid; i < nr; i += nt) y[r0 + i] = ys[i];
+    __syncthreads();
+    if (!ok && rank == 0 && tid == 0) atomicOr(status, 2);
+  }
+  cl.sync();   // no CTA leaves while another may still read its buffers
+}
+
+// One cluster of TD_CL CTAs per entry of the cluster list: a large kept block
+// shared by all of them (obig), or up to TD_CL small blocks, one per CTA
+// (oblk[cluster * TD_CL + rank], -1 for none).
+__global__ void __cluster_dims__(TD_CL, 1, 1) __launch_bounds__(ORTH_THREADS)
+    orthonormalize_kernel(const int *oblk, const int *obig, const int *grp, const int *dims, const int64_t *eoff,
+                          const double *evals, const double *info, const int *job_k, double *Y, int ldy,
+                          int *status) {
+  extern __shared__ double sm[];
+  __shared__ double red[32];
+  cg::cluster_group cl = cg::this_cluster();
+  const int b = blockIdx.x / TD_CL, rank = (int)cl.block_rank();
+  const int blk = oblk[blockIdx.x];
+  if (obig[b])
+    ortho_coop(cl, rank, blk, grp, dims, eoff, evals, info, job_k, Y, ldy, status, sm, red);
+  else if (blk >= 0)
+    ortho_one(blk, grp, dims, eoff, evals, info, job_k, Y, ldy, status, sm, red);
 }
 
 // Back-transformation of the kept vectors, one warp per vector and the
@@ -939,6 +1048,27 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       const size_t q_dst = q; q += al256((size_t)njobs * 8);
       const size_t q_grp = q; q += al256(grp.size() * 4);
       const size_t q_slab = q; q += al256(slab.size() * 4);
+      // clusters of the orthonormalisation: one per large kept block (cnt^2 n
+      // above 3e7), then the other blocks TD_CL at a time, largest first
+      std::vector<int> oblk, obig;
+      {
+        std::vector<int> bo(ngrp);
+        std::iota(bo.begin(), bo.end(), 0);
+        auto work = [&](int b) { return (double)grp[4 * b + 2] * grp[4 * b + 2] * dims[grp[4 * b]]; };
+        std::stable_sort(bo.begin(), bo.end(), [&](int a, int b) { return work(a) > work(b); });
+        size_t i = 0;
+        for (; i < bo.size() && work(bo[i]) >= 3e7; ++i) {
+          oblk.insert(oblk.end(), TD_CL, bo[i]);
+          obig.push_back(1);
+        }
+        for (; i < bo.size(); i += TD_CL) {
+          for (int r = 0; r < TD_CL; ++r) oblk.push_back(i + r < bo.size() ? bo[i + r] : -1);
+          obig.push_back(0);
+        }
+      }
+      const int nocl = (int)obig.size();
+      const size_t q_oblk = q; q += al256(oblk.size() * 4);
+      const size_t q_obig = q; q += al256(obig.size() * 4);
       const size_t q_out = q; q += al256((size_t)dpos * 8);
       if ((rc = ctx->trA.reserve(q))) return rc;   // psi is no longer needed
       char *ab = (char *)ctx->trA.p, *cb = (char *)ctx->trC.p;
@@ -947,6 +1077,8 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       CKT(cudaMemcpyAsync(ab + q_dst, job_dst.data(), (size_t)njobs * 8, cudaMemcpyHostToDevice, st));
       CKT(cudaMemcpyAsync(ab + q_grp, grp.data(), grp.size() * 4, cudaMemcpyHostToDevice, st));
       CKT(cudaMemcpyAsync(ab + q_slab, slab.data(), slab.size() * 4, cudaMemcpyHostToDevice, st));
+      CKT(cudaMemcpyAsync(ab + q_oblk, oblk.data(), oblk.size() * 4, cudaMemcpyHostToDevice, st));
+      CKT(cudaMemcpyAsync(ab + q_obig, obig.data(), obig.size() * 4, cudaMemcpyHostToDevice, st));
       double *Y = (double *)(cb + p_y), *d_out = (double *)(ab + q_out);
       for (int b = 0; b < ngrp; ++b) max_kept = std::max(max_kept, grp[4 * b + 2]);
       select_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - sel0).count();
@@ -957,8 +1089,13 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
                                                             (unsigned char *)(cb + p_piv), Y, ldy, d_status);
       CKT(cudaGetLastError());
       CKT(cudaEventRecord(ctx->tev[5], st));
-      orthonormalize_kernel<<<ngrp, ORTH_THREADS, sizeof(double) * maxn, st>>>(
-          (const int *)(ab + q_grp), d_dims, d_eoff, dev, dinfo, (const int *)(ab + q_k), Y, ldy, d_status);
+      {
+        const size_t osm = sizeof(double) * (3 * (size_t)maxn + (maxn + TD_CL - 1) / TD_CL + 8);
+        CKT(cudaFuncSetAttribute(orthonormalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)osm));
+        orthonormalize_kernel<<<nocl * TD_CL, ORTH_THREADS, osm, st>>>(
+            (const int *)(ab + q_oblk), (const int *)(ab + q_obig), (const int *)(ab + q_grp), d_dims, d_eoff, dev,
+            dinfo, (const int *)(ab + q_k), Y, ldy, d_status);
+      }
       CKT(cudaGetLastError());
       CKT(cudaEventRecord(ctx->tev[6], st));
       const size_t bsm = sizeof(double) * (size_t)W * ldy;
