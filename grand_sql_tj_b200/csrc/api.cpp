@@ -46,6 +46,9 @@ int tjb::dev_reserve(void **p, size_t *cap, size_t bytes) {
 tj_ctx::~tj_ctx() {
   cudaSetDevice(device);
   tjb::res_clear(this);
+  if (stage) cudaFreeHost(stage);
+  for (auto &e : sev)
+    if (e) cudaEventDestroy(e);
   for (DevBuf *b : all_bufs()) b->release();
   for (auto &e : ev)
     if (e) cudaEventDestroy(e);
@@ -729,7 +732,7 @@ extern "C" int tj_lanczos_memo_new(tj_ctx *ctx, const tj_lattice *lat, const tj_
   norm_into(ctx->vout.d(), nrm);
   launch_scale_inv(ctx->vout.d(), nrm, D, ctx->stream);
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(eigvec->data, ctx->vout.d(), sizeof(double) * D, cudaMemcpyDeviceToHost, ctx->stream));
+  if ((rc = download(ctx, eigvec->data, ctx->vout.d(), D, ctx->stream))) return rc;
   if ((rc = fetch(lam, &hl))) return rc;
   if ((rc = check_device_flags(ctx))) return rc;
   energies[0] = hl;

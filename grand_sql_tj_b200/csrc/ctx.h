@@ -88,6 +88,8 @@ struct tj_ctx {
   std::vector<tjb::ResEntry> resident;
   size_t res_budget = 0, res_bytes = 0;
   uint64_t res_clock = 0;
+  double *stage = nullptr;    // page-locked staging of large downloads (2 x 8 MB)
+  cudaEvent_t sev[2] = {nullptr, nullptr};
   int64_t res_hits = 0;       // uploads served from kept copies since creation
   double res_hit_bytes = 0;
   std::shared_ptr<tj_renorm_state> renorm;
@@ -122,6 +124,9 @@ const double *res_find(tj_ctx *ctx, const double *p, int64_t n);
 int res_keep(tj_ctx *ctx, const double *host, int64_t n, const double *dev_src, cudaStream_t st);
 void res_clear(tj_ctx *ctx);
 cudaError_t upload(tj_ctx *ctx, double *dst, const double *src, int64_t n, cudaStream_t st);
+// device-to-host copy of n doubles into caller memory, through page-locked
+// staging; returns when dst is filled (the stream is synchronised)
+int download(tj_ctx *ctx, double *dst, const double *src, int64_t n, cudaStream_t st);
 int reset_device_flags(tj_ctx *ctx);
 // wavefunction table checks shared by every entry point that takes a tj_wave:
 // null tables, negative sizes or offsets, a sector past wave->dim

@@ -832,7 +832,7 @@ extern "C" int tj_get_hamiltonian(tj_ctx *ctx, const tj_lattice *lat, int side, 
   launch_reduce(g, (const Reduce *)(tb + o_r2), (int)P.red2.size(), st);
   CKR(cudaEventRecord(ctx->ev[1], st));
   CKR(cudaGetLastError());
-  CKR(cudaMemcpyAsync(out->data, ctx->rnOut.d(), sizeof(double) * R.out_len, cudaMemcpyDeviceToHost, st));
+  if ((rc = download(ctx, out->data, ctx->rnOut.d(), R.out_len, st))) return rc;
   CKR(cudaEventRecord(ctx->ev[2], st));
   CKR(cudaStreamSynchronize(st));
   float gemm_ms = 0, all_ms = 0;
@@ -1117,7 +1117,10 @@ int finish(tj_ctx *ctx, DevOp &d, tj_block_result *out) {
     r.off = s.off;
     out->subs[i] = r;
   }
-  if (n > 0) CKR(cudaMemcpyAsync(out->data, d.buf.d(), sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (n > 0) {
+    const int rc = download(ctx, out->data, d.buf.d(), n, ctx->stream);
+    if (rc) return rc;
+  }
   CKR(cudaStreamSynchronize(ctx->stream));
   std::memset(&out->block, 0, sizeof out->block);
   out->block.len = d.b.len;

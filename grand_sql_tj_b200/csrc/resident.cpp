@@ -21,6 +21,8 @@
 
 #include <cstring>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "ctx.h"
 
@@ -110,6 +112,66 @@ cudaError_t upload(tj_ctx *ctx, double *dst, const double *src, int64_t n, cudaS
   const double *d = res_find(ctx, src, n);
   return cudaMemcpyAsync(dst, d ? d : src, sizeof(double) * n, d ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                          st);
+}
+
+// Device-to-host copy into caller (pageable) memory through two page-locked
+// staging chunks: the DMA of chunk c runs while chunk c - 1 is copied out on
+// the host by several threads.  A copy straight into pageable memory runs
+// at a fraction of the DMA rate, and slower still into pages never touched
+// (each first touch is a page fault inside the copy).  Returns when dst is
+// filled.
+int download(tj_ctx *ctx, double *dst, const double *src, int64_t n, cudaStream_t st) {
+  const size_t chunk = (size_t)8 << 20;
+  const size_t bytes = (size_t)n * 8;
+  if (bytes <= ((size_t)1 << 20)) {
+    if (n > 0 && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      return set_err(TJ_ERR_CUDA, "download: copy failed");
+    if (cudaStreamSynchronize(st) != cudaSuccess) return set_err(TJ_ERR_CUDA, "download: stream failed");
+    return TJ_OK;
+  }
+  if (!ctx->stage) {
+    if (cudaMallocHost((void **)&ctx->stage, 2 * chunk) != cudaSuccess) {
+      ctx->stage = nullptr;
+      return set_err(TJ_ERR_CUDA, "download: no page-locked staging memory");
+    }
+    for (auto &e : ctx->sev)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+        return set_err(TJ_ERR_CUDA, "download: event creation failed");
+  }
+  char *stage = (char *)ctx->stage;
+  const char *s = (const char *)src;
+  char *d = (char *)dst;
+  const size_t nch = (bytes + chunk - 1) / chunk;
+  auto host_copy = [&](char *to, const char *from, size_t len) {
+    const size_t T = len >= ((size_t)4 << 20) ? 4 : 1;
+    if (T == 1) {
+      std::memcpy(to, from, len);
+      return;
+    }
+    std::vector<std::thread> th;
+    const size_t part = (len / T + 4095) / 4096 * 4096;
+    for (size_t t = 1; t < T; ++t) {
+      const size_t a = t * part;
+      if (a >= len) break;
+      th.emplace_back([=] { std::memcpy(to + a, from + a, std::min(part, len - a)); });
+    }
+    std::memcpy(to, from, std::min(part, len));
+    for (auto &x : th) x.join();
+  };
+  for (size_t c = 0; c <= nch; ++c) {
+    if (c < nch) {
+      const size_t off = c * chunk, len = std::min(chunk, bytes - off);
+      if (cudaMemcpyAsync(stage + (c & 1) * chunk, s + off, len, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+          cudaEventRecord(ctx->sev[c & 1], st) != cudaSuccess)
+        return set_err(TJ_ERR_CUDA, "download: copy failed");
+    }
+    if (c > 0) {
+      const size_t p = c - 1, off = p * chunk, len = std::min(chunk, bytes - off);
+      if (cudaEventSynchronize(ctx->sev[p & 1]) != cudaSuccess) return set_err(TJ_ERR_CUDA, "download: copy failed");
+      host_copy(d + off, stage + (p & 1) * chunk, len);
+    }
+  }
+  return TJ_OK;
 }
 
 }  // namespace tjb

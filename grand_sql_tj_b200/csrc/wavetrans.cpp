@@ -390,10 +390,12 @@ extern "C" int tj_wave_trans(tj_ctx *ctx, int direction, const tj_basis *sys_bs,
   launch_sum(part, nblk, nrm, 1, st);
   launch_scale_inv(ctx->wtNew.d(), nrm, D, st);
   CKW(cudaGetLastError());
-  CKW(cudaMemcpyAsync(new_wave->data, ctx->wtNew.d(), sizeof(double) * D, cudaMemcpyDeviceToHost, st));
   double h_nrm = 0;
   CKW(cudaMemcpyAsync(&h_nrm, nrm, sizeof(double), cudaMemcpyDeviceToHost, st));
-  CKW(cudaStreamSynchronize(st));
+  {
+    const int rc = download(ctx, new_wave->data, ctx->wtNew.d(), D, st);
+    if (rc) return rc;
+  }
   if (!(h_nrm > 0.0) || !std::isfinite(h_nrm))
     return set_err(TJ_ERR_NUMERIC, "tj_wave_trans: the carried wavefunction is zero or not finite");
   return TJ_OK;
