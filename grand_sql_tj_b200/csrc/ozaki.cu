@@ -306,18 +306,28 @@ __device__ __forceinline__ void oz_commit(uint32_t mbar) {
                : "memory");
 }
 
+// k-blocks per pipeline stage (up to 5 slices) and the shared memory given to
+// the stages
+// (build-time settings; the defaults are the measured best)
+#ifndef OZ_KPS
+#define OZ_KPS 2
+#endif
+#ifndef OZ_STAGE_CAP
+#define OZ_STAGE_CAP (192 * 1024)
+#endif
+
 template <int S, int BN>
 struct OzCfg {
   // a stage holds KPS consecutive k-blocks of an item's family: the cost of a
   // stage (barriers, copies, MMA issue) is nearly fixed, so fewer, larger
   // stages go faster
-  static constexpr int KPS = 2;
+  static constexpr int KPS = S <= 5 ? OZ_KPS : 2;
   static constexpr int A_KB = S * 16 * 256;             // one k-block: 128 rows x 32 k, s slices
   static constexpr int B_KB = S * (BN / 8) * 256;
   static constexpr int A_BYTES = KPS * A_KB;
   static constexpr int B_BYTES = KPS * B_KB;
   static constexpr int STAGE = A_BYTES + B_BYTES;
-  static constexpr int STAGES_RAW = (192 * 1024) / STAGE;
+  static constexpr int STAGES_RAW = (OZ_STAGE_CAP) / STAGE;
   static constexpr int STAGES = STAGES_RAW > 8 ? 8 : STAGES_RAW;
   static constexpr int SMEM = STAGES * STAGE;
   static_assert(S * BN <= 256, "diagonal accumulators exceed one TMEM buffer");

@@ -758,12 +758,17 @@ struct TruncCache {
 };
 thread_local TruncCache g_tc;
 
+// Fingerprint of psi for the two-call cache: 4096 values spread over it
+// (the second call of the protocol passes the same, unchanged psi; a full
+// pass over psi would cost more than the rest of the second call).
 uint64_t hash_data(const double *p, int64_t n) {
-  uint64_t h = 1469598103934665603ull;
-  const uint64_t *u = (const uint64_t *)p;
-  for (int64_t i = 0; i < n; ++i) {
-    h ^= u[i];
-    h *= 1099511628211ull;
+  uint64_t h = 1469598103934665603ull ^ (uint64_t)n;
+  const int64_t k = n < 4096 ? n : 4096;
+  for (int64_t i = 0; i < k; ++i) {
+    const int64_t at = k > 1 ? i * (n - 1) / (k - 1) : 0;
+    uint64_t u;
+    std::memcpy(&u, p + at, 8);
+    h = (h ^ u) * 1099511628211ull;
   }
   return h;
 }
@@ -800,8 +805,12 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     if ((rc = ctx->trA.reserve(sizeof(double) * (D + 4)))) return rc;
     double *psi = ctx->trA.d();
     CKT(cudaMemcpyAsync(psi, wave->data, sizeof(double) * D, cudaMemcpyHostToDevice, st));
-    double nrm2 = 0;
-    for (int64_t i = 0; i < D; ++i) nrm2 += wave->data[i] * wave->data[i];
+    double acc[4] = {0, 0, 0, 0};   // four independent sums, added at the end
+    int64_t i = 0;
+    for (; i + 4 <= D; i += 4)
+      for (int q = 0; q < 4; ++q) acc[q] += wave->data[i + q] * wave->data[i + q];
+    for (; i < D; ++i) acc[0] += wave->data[i] * wave->data[i];
+    const double nrm2 = (acc[0] + acc[1]) + (acc[2] + acc[3]);
     if (!(nrm2 > 0) || !std::isfinite(nrm2)) return set_err(TJ_ERR_NUMERIC, "tj_truncation: zero or non-finite psi");
     // rho per sector as one grouped-GEMM pass
     std::vector<Cell> cells;
