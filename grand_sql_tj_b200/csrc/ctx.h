@@ -87,6 +87,7 @@ struct tj_ctx {
   // device-resident blocks (tj_set_residency): budget in bytes (0: off)
   std::vector<tjb::ResEntry> resident;
   size_t res_budget = 0, res_bytes = 0;
+  cudaMemPool_t res_pool = nullptr;
   uint64_t res_clock = 0;
   double *stage = nullptr;    // page-locked staging of large downloads (2 x 8 MB)
   cudaEvent_t sev[2] = {nullptr, nullptr};

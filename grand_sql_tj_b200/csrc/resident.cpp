@@ -42,11 +42,30 @@ uint64_t fingerprint(const double *p, int64_t n) {
   return h;
 }
 
+// Kept arrays come from a memory pool of the context's own, freed and
+// allocated in stream order: no device-wide synchronisation per step, and
+// the pool keeps its memory (up to the budget) for the next blocks.
 void drop(tj_ctx *ctx, size_t i) {
   ResEntry &e = ctx->resident[i];
-  if (e.dev) cudaFree(e.dev);
+  if (e.dev) cudaFreeAsync(e.dev, ctx->stream);
   ctx->res_bytes -= (size_t)e.n * 8;
   ctx->resident.erase(ctx->resident.begin() + (long)i);
+}
+
+int ensure_pool(tj_ctx *ctx) {
+  if (ctx->res_pool) return TJ_OK;
+  cudaMemPoolProps props;
+  std::memset(&props, 0, sizeof props);
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = ctx->device;
+  if (cudaMemPoolCreate(&ctx->res_pool, &props) != cudaSuccess) {
+    ctx->res_pool = nullptr;
+    return set_err(TJ_ERR_CUDA, "residency: no memory pool");
+  }
+  uint64_t keep = ~0ull;   // memory stays with the pool between steps
+  cudaMemPoolSetAttribute(ctx->res_pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  return TJ_OK;
 }
 
 }  // namespace
@@ -88,13 +107,15 @@ int res_keep(tj_ctx *ctx, const double *host, int64_t n, const double *dev_src, 
   ResEntry e;
   e.host = host;
   e.n = n;
-  if (cudaMalloc((void **)&e.dev, bytes) != cudaSuccess) {
+  int prc = ensure_pool(ctx);
+  if (prc) return prc;
+  if (cudaMallocFromPoolAsync((void **)&e.dev, bytes, ctx->res_pool, st) != cudaSuccess) {
     cudaGetLastError();
     return TJ_OK;   // no room: the block stays host-only
   }
   cudaError_t rc = cudaMemcpyAsync(e.dev, dev_src, bytes, cudaMemcpyDeviceToDevice, st);
   if (rc != cudaSuccess) {
-    cudaFree(e.dev);
+    cudaFreeAsync(e.dev, st);
     return set_err(TJ_ERR_CUDA, std::string("residency copy: ") + cudaGetErrorString(rc));
   }
   e.sample = fingerprint(host, n);
@@ -106,6 +127,10 @@ int res_keep(tj_ctx *ctx, const double *host, int64_t n, const double *dev_src, 
 
 void res_clear(tj_ctx *ctx) {
   while (!ctx->resident.empty()) drop(ctx, ctx->resident.size() - 1);
+  if (ctx->res_pool) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaMemPoolTrimTo(ctx->res_pool, 0);
+  }
 }
 
 cudaError_t upload(tj_ctx *ctx, double *dst, const double *src, int64_t n, cudaStream_t st) {
@@ -190,11 +215,10 @@ extern "C" int tj_residency_forget(tj_ctx *ctx, const void *host) {
   if (!ctx) return tjb::set_err(TJ_ERR_ARG, "tj_residency_forget: null context");
   const double *p = (const double *)host;
   cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->stream);
   for (size_t i = 0; i < ctx->resident.size();) {
     const tjb::ResEntry &e = ctx->resident[i];
     if (p >= e.host && p < e.host + e.n) {
-      if (e.dev) cudaFree(e.dev);
+      if (e.dev) cudaFreeAsync(e.dev, ctx->stream);
       ctx->res_bytes -= (size_t)e.n * 8;
       ctx->resident.erase(ctx->resident.begin() + (long)i);
     } else {
