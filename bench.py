@@ -61,6 +61,12 @@ def parse():
                     help="real DMRG run whose full sweep is timed (FP64 and split precision from the same state)")
     ap.add_argument("--sweep-prep", default="mixed", choices=["mixed", "fp64"],
                     help="precision of the untimed warm-up and first half-sweeps before the timed sweeps")
+    ap.add_argument("--config5", action="store_true",
+                    help="also run configuration 5's four dopings as real DMRG runs on a 6-leg cylinder, with "
+                         "their pair and density correlators and shared-launch H*psi")
+    ap.add_argument("--config5-nx", type=int, default=12, help="columns of the 6-leg cylinder of --config5")
+    ap.add_argument("--config5-m", type=int, default=500, help="kept multiplets of --config5")
+    ap.add_argument("--config5-sweeps", type=int, default=2, help="full sweeps of each --config5 run")
     ap.add_argument("--instances", type=int, default=1,
                     help="K > 1: also time K independent superblocks (dopings 1/12, 1/10, 1/8, 1/6, ...) in shared "
                          "launches against the same K run one after another")
@@ -346,6 +352,62 @@ def sweep_leg(ctx64, ctxoz, name: str, prep: str, seed: int):
     return out
 
 
+CONFIG5_DOPINGS = (1.0 / 12, 1.0 / 10, 1.0 / 8, 1.0 / 6)
+
+
+def config5_leg(ctx, nx: int, m: int, sweeps: int, seed: int):
+    """Configuration 5 at a size one run can take: the 6-leg cylinder of nx
+    columns (y periodic, x open; t = 1, t' = -0.2, J = 1/3, S = 0) at the four
+    dopings, holes rounded to even numbers.  Each is a DMRG run of the
+    reference's schedule on the device (split-precision H*psi, FP64
+    truncation, renormalisation and prediction; blocks kept resident),
+    followed by the singlet pair (along y and x) and density correlators of
+    Measurement (main.f90:191-332).  Then the H*psi of the four
+    measurement-point superblocks in shared launches (tj_model_wave_multi)
+    against the four one after another, with the two results compared."""
+    import numpy as np
+    from grand_sql_tj_b200.lattice import Geometry
+    from grand_sql_tj_b200.lib import DeviceBackend
+    from grand_sql_tj_b200.measure import measurement
+    from grand_sql_tj_b200.sweep import Dmrg, DmrgParams
+    n = 6 * nx
+    out = {"lattice": "6x%d cylinder (y periodic, x open)" % nx, "t": 1.0, "t2": -0.2, "J": 1.0 / 3.0, "m": m,
+           "sweeps": sweeps, "instances": []}
+    ctx.set_residency(RESIDENCY_GB)
+    lasts = []
+    for delta in CONFIG5_DOPINGS:
+        holes = 2 * int(round(n * delta / 2.0))
+        geo = Geometry(nx, 6, t=1.0, J=1.0 / 3.0, t2=-0.2, esite=0.0, up_bias=1)
+        d = Dmrg(geo, DeviceBackend(ctx), DmrgParams(n_elec=n - holes, kept_min=3 * m // 4, kept_max=m, seed=seed))
+        t0 = time.perf_counter()
+        d.ground_state(sweeps, final_half=True)
+        run_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        cors = measurement(DeviceBackend(ctx), d)
+        meas_s = time.perf_counter() - t0
+        last_sweep = [r for r in d.records if r.phase == "R->L%d" % sweeps]
+        lasts.append(d.last)
+        out["instances"].append({
+            "delta": delta, "holes": holes, "electrons": n - holes, "E_per_site": d.records[-1].energy / n,
+            "max_trunc_err_last_sweep": max(r.trunc_err for r in last_sweep), "run_s": run_s, "steps": len(d.records),
+            "measure_s": meas_s,
+            "pair_y": [[*k, v] for k, v in sorted(cors["pair_y"].items())],
+            "pair_x": [[*k, v] for k, v in sorted(cors["pair_x"].items())],
+            "density": [[*k, v] for k, v in sorted(cors["density"].items())]})
+    outs, ms_shared = ctx.model_wave_multi(lasts, reps=20)
+    ms_seq, diff = 0.0, 0.0
+    for sb, o in zip(lasts, outs):
+        ms1, single = ctx.model_wave_bench(sb, 20)
+        ms_seq += ms1
+        a, b = o.data[:o.dim], single.data[:single.dim]
+        diff = max(diff, float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)))
+    out["shared_launch"] = {"psi_dims": [sb.wave.dim for sb in lasts], "shared_ms": ms_shared,
+                            "sequential_ms": ms_seq, "speedup": ms_seq / ms_shared,
+                            "max_rel_diff_shared_vs_single": diff}
+    ctx.set_residency(0)
+    return out
+
+
 def main():
     args = parse()
     ws, rank, local, pg = dist_init(args)
@@ -485,6 +547,11 @@ def main():
     if args.sweep != "none" and rank == 0 and not args.no_e2e:
         sweep = sweep_leg(ctx64, ctxoz, args.sweep, args.sweep_prep, args.seed)
 
+    config5 = None
+    if args.config5 and rank == 0:
+        config5 = config5_leg(ctxoz if ctxoz is not None else ctx64, args.config5_nx, args.config5_m,
+                              args.config5_sweeps, args.seed)
+
     shared = None
     if args.instances > 1:
         # independent instances of the same lattice at several dopings, one set of launches
@@ -579,6 +646,8 @@ def main():
             line["dmrg_step"] = step
         if sweep is not None:
             line["sweep"] = sweep
+        if config5 is not None:
+            line["config5"] = config5
         if tune:
             line["autotune"] = tune
         if micro is not None:

@@ -91,6 +91,16 @@ class StepRecord:
 
 
 @dataclass
+class LastSuperblock:
+    lat: object
+    sys: Model
+    env: Model
+    sys_bs: Basis
+    env_bs: Basis
+    wave: Wave
+
+
+@dataclass
 class DmrgParams:
     n_elec: int                  # tot_num_up of the canonical run (up_bias = 1); 0 when grand-canonical
     tot_num_down: int = 0        # twice the target total spin
@@ -117,6 +127,7 @@ class Dmrg:
         self.sysbs: Dict[int, Basis] = {}
         self.envbs: Dict[int, Basis] = {}
         self.wave: Optional[Wave] = None
+        self.last: Optional[LastSuperblock] = None
         self.records: List[StepRecord] = []
         self.site = site_sectors(self.up_bias)
 
@@ -132,7 +143,10 @@ class Dmrg:
         return trun, float(info.trunc_err), int(info.num_state)
 
     def _lanczos(self, lat, sys, env, sys_bs, env_bs, wave, lanzero):
-        return self.be.lanczos(lat, sys, env, sys_bs, env_bs, wave, lanzero)
+        e, it, w = self.be.lanczos(lat, sys, env, sys_bs, env_bs, wave, lanzero)
+        # the superblock of the last step (its models, bases and ground state)
+        self.last = LastSuperblock(lat, sys, env, sys_bs, env_bs, w)
+        return e, it, w
 
     # ------------------------------------------------------------ warm-up
     def warm_up(self, end_id: Optional[int] = None, lanzero: Optional[float] = None,

@@ -7,6 +7,9 @@ tj_update_trun, tj_block_mul_block_ndia) and the correlations they give.
     largest; the correlations within 1e-10;
   * the same for every call of the restated Get_mSCOP_Operator_Cor0 (the
     singlet pair correlation, bonds along and across the ladder);
+  * every call of the restated Measurement (main.f90:191-332) on a truncated
+    6x6 cylinder with t' = -0.2 (the six-leg branch of the pair correlator
+    included), device against oracle on the oracle's wavefunction;
   * <S_i . S_j> from an untruncated device run on a 2x6 ladder against
     exact diagonalisation (3e-8, the convergence of the Lanczos vector).
 """
@@ -14,7 +17,7 @@ import numpy as np
 import pytest
 
 from grand_sql_tj_b200.lattice import Geometry
-from grand_sql_tj_b200.measure import Chains, density_cor, pairing_cor
+from grand_sql_tj_b200.measure import Chains, density_cor, measurement, pairing_cor
 from grand_sql_tj_b200.sweep import Dmrg, DmrgParams, site_block_ops
 
 pytestmark = pytest.mark.gpu
@@ -100,3 +103,17 @@ def test_device_spin_correlation_equals_ed(ctx):
     res = density_cor(be, Chains(d, d.wave), d.wave, ops["st_sd"], ops["st_sd"], "B", 1, 2, n)
     for (i, j), v in res.items():
         assert abs(v - ed.spin_correlation(cl, psi, i - 1, j - 1)) <= 3e-8, (i, j, v)
+
+
+def test_six_leg_measurement_matches_oracle(ctx, oracle_lib):
+    from grand_sql_tj_b200.lib import DeviceBackend
+    from oracle.oracle import OracleBackend
+    ora = OracleBackend()
+    geo = Geometry(6, 6, t=1.0, J=1.0 / 3.0, t2=-0.2, esite=0.0, up_bias=1)
+    d = Dmrg(geo, ora, DmrgParams(n_elec=32, kept_min=48, kept_max=64, lanzero=1e-8, lanzero_warm=1e-6, seed=5))
+    d.ground_state(1, final_half=True)
+    be = Pair(DeviceBackend(ctx), ora)
+    res = measurement(be, d)
+    assert any(k[0] == 5 for k in res["pair_y"])   # the six-leg branch (reference bond at site 1 + 4)
+    assert all(len(v) >= 5 for v in res.values())
+    assert be.calls > 60
