@@ -7,8 +7,10 @@ oracle's run of the same schedule from the same seed
 (tests/golden/config1_ladder16_m256.json, made by make_config1.py):
 
   * from the third full sweep on, every step's energy within 1e-10 per site,
-    the same kept multiplets and the truncation error within 10 % (measured:
-    <= 7e-12 per site, 7e-4 relative);
+    the same kept multiplets (unless the discarded weight is rounding noise,
+    where the keep rule's comparison with trun_err = 1e-18 goes either way)
+    and the truncation error within 10 % (measured: <= 7e-12 per site, 7e-4
+    relative);
   * before that, energies within 1e-4 per site: while a block's density
     matrix has fewer nonzero eigenvalues than the states kept (the warm-up
     and the first sweeps), the kept zero-weight states are any basis of the
@@ -56,7 +58,10 @@ def test_config1_steps_match_oracle(device_run):
             assert abs(r.energy - e) / n <= 1e-4, (phase, sl, r.energy, e)
             continue
         assert abs(r.energy - e) / n <= 1e-10, (phase, sl, r.energy, e)
-        assert r.num_state == ns, (phase, sl)
+        # the keep rule compares the discarded weight with trun_err = 1e-18:
+        # where the density matrix has no weight beyond the kept states that
+        # comparison is decided by rounding (in the reference as well)
+        assert r.num_state == ns or max(abs(r.trunc_err), abs(te)) <= 1e-14, (phase, sl, r.num_state, ns)
         if max(abs(r.trunc_err), abs(te)) > 1e-13:
             assert abs(r.trunc_err - te) <= 0.1 * max(abs(r.trunc_err), abs(te)), (phase, sl, r.trunc_err, te)
 
