@@ -328,16 +328,20 @@ def sweep_leg(ctx64, ctxoz, name: str, prep: str, seed: int):
                     "E_end": recs[-1].energy, "E_min": min(r.energy for r in recs),
                     "max_trunc_err": max(r.trunc_err for r in recs), "max_psi_dim": max(r.dim for r in recs),
                     "seconds": {k[2:]: v for k, v in agg.items()}}
-        tr = [st for name, st in trace if name == "truncation"]
+        tr = [st for name, st, _, _ in trace if name == "truncation"]
         stages = ("rho", "tridiag", "eig", "select", "vec", "orth", "back", "total")
         out[tag]["truncation_ms"] = {k: sum(getattr(st, "trunc_ms_" + k) for st in tr) for k in stages}
         out[tag]["truncation_ms"]["max_sector"] = max(st.trunc_max_n for st in tr)
         out[tag]["truncation_ms"]["max_kept_block"] = max(st.trunc_max_kept for st in tr)
-        rn = [st for name, st in trace if name == "get_hamiltonian"]
+        rn = [st for name, st, _, _ in trace if name == "get_hamiltonian"]
+        rh = [h for name, _, _, h in trace if name == "get_hamiltonian"]
         out[tag]["renorm_ms"] = {"plan": sum(st.renorm_plan_ms for st in rn), "gemm": sum(st.renorm_ms for st in rn),
                                  "call": sum(st.renorm_e2e_ms for st in rn),
-                                 "tflops": sum(st.renorm_flops for st in rn) / max(sum(st.renorm_ms for st in rn), 1e-9) / 1e9}
-        lz = [st for name, st in trace if name == "lanczos"]
+                                 "tflops": sum(st.renorm_flops for st in rn) / max(sum(st.renorm_ms for st in rn), 1e-9) / 1e9,
+                                 "wall": 1e3 * sum(w for name, _, w, _ in trace if name == "get_hamiltonian")}
+        for k in ("sizes", "alloc", "fill", "wrap"):
+            out[tag]["renorm_ms"]["host_" + k] = 1e3 * sum(h.get(k, 0.0) for h in rh)
+        lz = [st for name, st, _, _ in trace if name == "lanczos"]
         out[tag]["lanczos_ms"] = {"prepare": sum(st.prepare_ms for st in lz), "plan": sum(st.plan_ms for st in lz),
                                   "split_plan": sum(st.ozplan_ms for st in lz),
                                   "iterations": sum(st.lanczos_ms for st in lz)}
@@ -376,7 +380,7 @@ def config5_leg(ctx, nx: int, m: int, sweeps: int, seed: int):
     ctx.set_residency(RESIDENCY_GB)
     lasts = []
     for delta in CONFIG5_DOPINGS:
-        holes = 2 * int(round(n * delta / 2.0))
+        holes = 2 * int(n * delta / 2.0 + 0.5)   # rounded half up to an even number
         geo = Geometry(nx, 6, t=1.0, J=1.0 / 3.0, t2=-0.2, esite=0.0, up_bias=1)
         d = Dmrg(geo, DeviceBackend(ctx), DmrgParams(n_elec=n - holes, kept_min=3 * m // 4, kept_max=m, seed=seed))
         t0 = time.perf_counter()

@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import time
 import weakref
 from typing import Optional, Tuple
 
@@ -16,7 +17,7 @@ import numpy as np
 
 from .structs import (Basis, BasisMap, Block, TjBasis, TjBasisMap, TjBasisResult, TjBasisSub, TjBlock, TjBlockResult, TjBlockSet, TjBlockSub, TjChain, TjGgCell, TjGgTerm,
                       TjHpsiStats, TjLattice, TjModel, TjModelResult, TjTruncResult, TjTuneResult, TjWave, Wave,
-                      block_from_c_result, call_block_result, call_model_result)
+                      RESULT_HOST_S, block_from_c_result, call_block_result, call_model_result)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtjb200.so")
@@ -536,19 +537,26 @@ class DeviceBackend:
         self.ctx = ctx
         self.trace = trace   # if a list: (call, the context's statistics after it) per step call
 
-    def _traced(self, name, r):
-        if self.trace is not None:
-            self.trace.append((name, self.ctx.stats()))
+    def _traced(self, name, fn):
+        """Runs fn(); with a trace, records (call, the context's statistics
+        after it, its wall time in s, host stage times of a model result)."""
+        if self.trace is None:
+            return fn()
+        t0 = time.perf_counter()
+        r = fn()
+        wall = time.perf_counter() - t0
+        self.trace.append((name, self.ctx.stats(), wall,
+                           dict(RESULT_HOST_S) if name == "get_hamiltonian" else None))
         return r
 
     def lanczos(self, lat, sys, env, sys_bs, env_bs, wave, lanzero):
-        return self._traced("lanczos", self.ctx.lanczos(lat, sys, env, sys_bs, env_bs, wave, lanzero))
+        return self._traced("lanczos", lambda: self.ctx.lanczos(lat, sys, env, sys_bs, env_bs, wave, lanzero))
 
     def truncation(self, wave, side, kept_min, kept_max, trun_err):
-        return self._traced("truncation", self.ctx.truncation(wave, side, kept_min, kept_max, trun_err))
+        return self._traced("truncation", lambda: self.ctx.truncation(wave, side, kept_min, kept_max, trun_err))
 
     def get_hamiltonian(self, lat, side, mshift, pre, basis, trun):
-        return self._traced("get_hamiltonian", self.ctx.get_hamiltonian(lat, side, mshift, pre, basis, trun))
+        return self._traced("get_hamiltonian", lambda: self.ctx.get_hamiltonian(lat, side, mshift, pre, basis, trun))
 
     def wave_trans(self, direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave):
         return self.ctx.wave_trans(direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave)

@@ -10,6 +10,7 @@ for as long as the packed object lives.
 from __future__ import annotations
 
 import ctypes as C
+import time
 from dataclasses import dataclass, field
 from typing import List, Optional, Tuple
 
@@ -354,23 +355,33 @@ def block_transfer_trans(b: Block) -> Block:
     return Block(b.len, -b.up_dif, b.down_dif, subs)
 
 
+# host wall time (s) of the stages of the last call_model_result
+RESULT_HOST_S = {}
+
+
 def call_model_result(call):
     """Runs a two-call model-result entry point `call(res_ptr) -> rc` and
     returns the new Model (copied out of the result arrays)."""
+    t0 = time.perf_counter()
     res = TjModelResult()
     rc = call(C.byref(res))
     if rc:
         return rc, None
+    t1 = time.perf_counter()
     sets = (TjBlockSet * max(res.nsub, 1))()
     subs = (TjBlockSub * max(res.n_subs, 1))()
     data = np.zeros(max(res.data_len, 1))
     res.sets = C.cast(sets, C.POINTER(TjBlockSet))
     res.subs = C.cast(subs, C.POINTER(TjBlockSub))
     res.data = data.ctypes.data_as(c_double_p)
+    t2 = time.perf_counter()
     rc = call(C.byref(res))
     if rc:
         return rc, None
-    return 0, model_from_c(res.model, data, keep=(res, sets, subs, data))
+    t3 = time.perf_counter()
+    m = model_from_c(res.model, data, keep=(res, sets, subs, data))
+    RESULT_HOST_S.update(sizes=t1 - t0, alloc=t2 - t1, fill=t3 - t2, wrap=time.perf_counter() - t3)
+    return 0, m
 
 
 def _block_from_c(b: TjBlock, data: np.ndarray) -> Block:
