@@ -338,7 +338,9 @@ def sweep_leg(ctx64, ctxoz, name: str, prep: str, seed: int):
         out[tag]["renorm_ms"] = {"plan": sum(st.renorm_plan_ms for st in rn), "gemm": sum(st.renorm_ms for st in rn),
                                  "call": sum(st.renorm_e2e_ms for st in rn),
                                  "tflops": sum(st.renorm_flops for st in rn) / max(sum(st.renorm_ms for st in rn), 1e-9) / 1e9,
-                                 "wall": 1e3 * sum(w for name, _, w, _ in trace if name == "get_hamiltonian")}
+                                 "wall": 1e3 * sum(w for name, _, w, _ in trace if name == "get_hamiltonian"),
+                                 "host_pre": sum(st.renorm_pre_ms for st in rn),
+                                 "host_post": sum(st.renorm_post_ms for st in rn)}
         for k in ("sizes", "alloc", "fill", "wrap"):
             out[tag]["renorm_ms"]["host_" + k] = 1e3 * sum(h.get(k, 0.0) for h in rh)
         lz = [st for name, st, _, _ in trace if name == "lanczos"]

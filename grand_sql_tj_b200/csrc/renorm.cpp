@@ -768,6 +768,7 @@ extern "C" int tj_get_hamiltonian(tj_ctx *ctx, const tj_lattice *lat, int side, 
     return TJ_OK;
   }
   // second call: upload, two grouped-GEMM passes, download
+  const auto h0 = std::chrono::steady_clock::now();
   const HpsiPlan &P = R.P;
   CKR(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
@@ -778,6 +779,7 @@ extern "C" int tj_get_hamiltonian(tj_ctx *ctx, const tj_lattice *lat, int side, 
       (rc = ctx->rnOut.reserve(sizeof(double) * (R.out_len + 4))) ||
       (rc = ctx->rnSlots.reserve(sizeof(double) * (std::max(P.nslots1, P.nslots2) * BM * BN + 4))))
     return rc;
+  const double pre_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
   CKR(cudaEventRecord(ctx->ev[5], st));
   for (const auto &u : P.uploads)
     if (u.n > 0) CKR(upload(ctx, ctx->rnOps.d() + u.dst, u.src, u.n, st));
@@ -841,8 +843,11 @@ extern "C" int tj_get_hamiltonian(tj_ctx *ctx, const tj_lattice *lat, int side, 
   ctx->stats.renorm_ms = gemm_ms;
   ctx->stats.renorm_e2e_ms = all_ms;
   ctx->stats.renorm_flops = P.flops;
+  const auto h1 = std::chrono::steady_clock::now();
   fill_result(R, out);
   if ((rc = res_keep(ctx, out->data, R.out_len, ctx->rnOut.d(), st))) return rc;
+  ctx->stats.renorm_pre_ms = pre_ms;
+  ctx->stats.renorm_post_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h1).count();
   return TJ_OK;
 }
 

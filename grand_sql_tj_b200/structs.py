@@ -123,7 +123,8 @@ class TjHpsiStats(C.Structure):
                 ("trunc_ms_select", C.c_double), ("trunc_ms_vec", C.c_double), ("trunc_ms_orth", C.c_double),
                 ("trunc_ms_back", C.c_double), ("trunc_ms_total", C.c_double),
                 ("trunc_max_n", C.c_int64), ("trunc_max_kept", C.c_int64),
-                ("res_hits", C.c_int64), ("res_hit_bytes", C.c_double)]
+                ("res_hits", C.c_int64), ("res_hit_bytes", C.c_double),
+                ("renorm_pre_ms", C.c_double), ("renorm_post_ms", C.c_double)]
 
 
 class TjTuneResult(C.Structure):

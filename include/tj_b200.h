@@ -445,6 +445,9 @@ typedef struct tj_hpsi_stats {
    * since the context was created, and their bytes */
   int64_t res_hits;
   double res_hit_bytes;
+  /* the last tj_get_hamiltonian's second call: host time (ms) before its
+   * first upload and after its download (result tables, residency) */
+  double renorm_pre_ms, renorm_post_ms;
 } tj_hpsi_stats;
 int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st);
 
