@@ -46,10 +46,6 @@ int tjb::dev_reserve(void **p, size_t *cap, size_t bytes) {
 tj_ctx::~tj_ctx() {
   cudaSetDevice(device);
   tjb::res_clear(this);
-  if (res_pool) {
-    cudaStreamSynchronize(stream);
-    cudaMemPoolDestroy(res_pool);
-  }
   if (stage) cudaFreeHost(stage);
   for (auto &e : sev)
     if (e) cudaEventDestroy(e);

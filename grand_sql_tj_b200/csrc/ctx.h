@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <chrono>
+#include <map>
 #include <memory>
 #include <unordered_map>
 #include <string>
@@ -38,6 +39,17 @@ struct ResEntry {
   int64_t n = 0;
   double *dev = nullptr;
   uint64_t stamp = 0, sample = 0;
+};
+
+// device slabs the kept arrays are carved from (resident.cpp): free
+// segments and handed-out segments by address, each with its slab
+struct ResArena {
+  struct Free {
+    size_t size;
+    int slab;
+  };
+  std::vector<char *> slabs;
+  std::map<char *, Free> free, owner;
 };
 
 }  // namespace tjb
@@ -87,7 +99,7 @@ struct tj_ctx {
   // device-resident blocks (tj_set_residency): budget in bytes (0: off)
   std::vector<tjb::ResEntry> resident;
   size_t res_budget = 0, res_bytes = 0;
-  cudaMemPool_t res_pool = nullptr;
+  tjb::ResArena arena;
   uint64_t res_clock = 0;
   double *stage = nullptr;    // page-locked staging of large downloads (2 x 8 MB)
   cudaEvent_t sev[2] = {nullptr, nullptr};

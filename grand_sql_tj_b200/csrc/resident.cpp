@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <iterator>
 #include <string>
 #include <thread>
 #include <vector>
@@ -42,30 +43,76 @@ uint64_t fingerprint(const double *p, int64_t n) {
   return h;
 }
 
-// Kept arrays come from a memory pool of the context's own, freed and
-// allocated in stream order: no device-wide synchronisation per step, and
-// the pool keeps its memory (up to the budget) for the next blocks.
-void drop(tj_ctx *ctx, size_t i) {
-  ResEntry &e = ctx->resident[i];
-  if (e.dev) cudaFreeAsync(e.dev, ctx->stream);
-  ctx->res_bytes -= (size_t)e.n * 8;
-  ctx->resident.erase(ctx->resident.begin() + (long)i);
+// Kept arrays are carved out of large device slabs (4 GB, or the array's
+// size if larger) by a first-fit allocator with coalescing free lists:
+// cudaMalloc runs once per slab, not once per block (growing a memory pool
+// per block cost more than the step's GEMMs).  All uses of kept memory are on
+// the context's stream, so memory freed here and handed out again is only
+// written after the earlier reads have run.
+constexpr size_t SLAB = (size_t)4 << 30;
+
+double *arena_alloc(tj_ctx *ctx, size_t bytes) {
+  bytes = (bytes + 255) / 256 * 256;
+  ResArena &A = ctx->arena;
+  for (auto it = A.free.begin(); it != A.free.end(); ++it) {
+    if (it->second.size < bytes) continue;
+    char *p = it->first;
+    const ResArena::Free f = it->second;
+    A.free.erase(it);
+    if (f.size > bytes) A.free[p + bytes] = ResArena::Free{f.size - bytes, f.slab};
+    A.owner[p] = ResArena::Free{bytes, f.slab};
+    return (double *)p;
+  }
+  const size_t sz = bytes > SLAB ? bytes : SLAB;
+  char *slab = nullptr;
+  if (cudaMalloc((void **)&slab, sz) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  const int id = (int)A.slabs.size();
+  A.slabs.push_back(slab);
+  if (sz > bytes) A.free[slab + bytes] = ResArena::Free{sz - bytes, id};
+  A.owner[slab] = ResArena::Free{bytes, id};
+  return (double *)slab;
 }
 
-int ensure_pool(tj_ctx *ctx) {
-  if (ctx->res_pool) return TJ_OK;
-  cudaMemPoolProps props;
-  std::memset(&props, 0, sizeof props);
-  props.allocType = cudaMemAllocationTypePinned;
-  props.location.type = cudaMemLocationTypeDevice;
-  props.location.id = ctx->device;
-  if (cudaMemPoolCreate(&ctx->res_pool, &props) != cudaSuccess) {
-    ctx->res_pool = nullptr;
-    return set_err(TJ_ERR_CUDA, "residency: no memory pool");
+void arena_free(tj_ctx *ctx, double *ptr) {
+  ResArena &A = ctx->arena;
+  auto o = A.owner.find((char *)ptr);
+  if (o == A.owner.end()) return;
+  char *p = o->first;
+  ResArena::Free f = o->second;
+  A.owner.erase(o);
+  auto next = A.free.lower_bound(p);
+  if (next != A.free.end() && next->first == p + f.size && next->second.slab == f.slab) {
+    f.size += next->second.size;
+    next = A.free.erase(next);
   }
-  uint64_t keep = ~0ull;   // memory stays with the pool between steps
-  cudaMemPoolSetAttribute(ctx->res_pool, cudaMemPoolAttrReleaseThreshold, &keep);
-  return TJ_OK;
+  if (next != A.free.begin()) {
+    auto prev = std::prev(next);
+    if (prev->first + prev->second.size == p && prev->second.slab == f.slab) {
+      prev->second.size += f.size;
+      return;
+    }
+  }
+  A.free[p] = f;
+}
+
+void arena_release(tj_ctx *ctx) {
+  ResArena &A = ctx->arena;
+  if (A.slabs.empty()) return;
+  cudaStreamSynchronize(ctx->stream);
+  for (char *s : A.slabs) cudaFree(s);
+  A.slabs.clear();
+  A.free.clear();
+  A.owner.clear();
+}
+
+void drop(tj_ctx *ctx, size_t i) {
+  ResEntry &e = ctx->resident[i];
+  if (e.dev) arena_free(ctx, e.dev);
+  ctx->res_bytes -= (size_t)e.n * 8;
+  ctx->resident.erase(ctx->resident.begin() + (long)i);
 }
 
 }  // namespace
@@ -107,15 +154,11 @@ int res_keep(tj_ctx *ctx, const double *host, int64_t n, const double *dev_src, 
   ResEntry e;
   e.host = host;
   e.n = n;
-  int prc = ensure_pool(ctx);
-  if (prc) return prc;
-  if (cudaMallocFromPoolAsync((void **)&e.dev, bytes, ctx->res_pool, st) != cudaSuccess) {
-    cudaGetLastError();
-    return TJ_OK;   // no room: the block stays host-only
-  }
+  e.dev = arena_alloc(ctx, bytes);
+  if (!e.dev) return TJ_OK;   // no room: the block stays host-only
   cudaError_t rc = cudaMemcpyAsync(e.dev, dev_src, bytes, cudaMemcpyDeviceToDevice, st);
   if (rc != cudaSuccess) {
-    cudaFreeAsync(e.dev, st);
+    arena_free(ctx, e.dev);
     return set_err(TJ_ERR_CUDA, std::string("residency copy: ") + cudaGetErrorString(rc));
   }
   e.sample = fingerprint(host, n);
@@ -127,10 +170,7 @@ int res_keep(tj_ctx *ctx, const double *host, int64_t n, const double *dev_src, 
 
 void res_clear(tj_ctx *ctx) {
   while (!ctx->resident.empty()) drop(ctx, ctx->resident.size() - 1);
-  if (ctx->res_pool) {
-    cudaStreamSynchronize(ctx->stream);
-    cudaMemPoolTrimTo(ctx->res_pool, 0);
-  }
+  arena_release(ctx);
 }
 
 cudaError_t upload(tj_ctx *ctx, double *dst, const double *src, int64_t n, cudaStream_t st) {
@@ -218,7 +258,7 @@ extern "C" int tj_residency_forget(tj_ctx *ctx, const void *host) {
   for (size_t i = 0; i < ctx->resident.size();) {
     const tjb::ResEntry &e = ctx->resident[i];
     if (p >= e.host && p < e.host + e.n) {
-      if (e.dev) cudaFreeAsync(e.dev, ctx->stream);
+      if (e.dev) tjb::arena_free(ctx, e.dev);
       ctx->res_bytes -= (size_t)e.n * 8;
       ctx->resident.erase(ctx->resident.begin() + (long)i);
     } else {
