@@ -661,7 +661,7 @@ extern "C" int tj_lanczos_memo_new(tj_ctx *ctx, const tj_lattice *lat, const tj_
   const auto t0 = std::chrono::steady_clock::now();
   cudaStream_t st = ctx->stream;
   CK(cudaMemsetAsync(S, 0, sizeof(double) * 1024, st));
-  CK(cudaMemcpyAsync(vec(1), eigvec->data, sizeof(double) * D, cudaMemcpyHostToDevice, st));
+  CK(upload(ctx, vec(1), eigvec->data, D, st));
   norm_into(vec(1), nrm);
   launch_scale_inv(vec(1), nrm, D, st);
   dot_into(vec(1), vec(1), uu + 1);
@@ -733,6 +733,7 @@ extern "C" int tj_lanczos_memo_new(tj_ctx *ctx, const tj_lattice *lat, const tj_
   launch_scale_inv(ctx->vout.d(), nrm, D, ctx->stream);
   CK(cudaGetLastError());
   if ((rc = download(ctx, eigvec->data, ctx->vout.d(), D, ctx->stream))) return rc;
+  if ((rc = res_keep(ctx, eigvec->data, D, ctx->vout.d(), ctx->stream))) return rc;
   if ((rc = fetch(lam, &hl))) return rc;
   if ((rc = check_device_flags(ctx))) return rc;
   energies[0] = hl;

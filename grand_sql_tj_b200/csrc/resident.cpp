@@ -7,8 +7,10 @@
 // block's operators from the caller's (pageable) arrays -- tens of MB per
 // step at m = 2000, more than the GEMMs of the step take.  With residency on
 // (tj_set_residency), tj_get_hamiltonian keeps the device copy of the block
-// it has just written, keyed by the caller's array, and every later upload
-// whose source lies inside a kept array is a device-to-device copy instead.
+// it has just written, keyed by the caller's array (and tj_lanczos_memo_new
+// and tj_wave_trans their wavefunctions, which the next truncation,
+// prediction and Lanczos read), and every later upload whose source lies
+// inside a kept array is a device-to-device copy instead.
 //
 // The caller's side of the contract: an array the library filled is not
 // modified while it is kept (tj_residency_forget drops it first; freeing and

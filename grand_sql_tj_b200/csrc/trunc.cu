@@ -804,7 +804,7 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     int rc;
     if ((rc = ctx->trA.reserve(sizeof(double) * (D + 4)))) return rc;
     double *psi = ctx->trA.d();
-    CKT(cudaMemcpyAsync(psi, wave->data, sizeof(double) * D, cudaMemcpyHostToDevice, st));
+    CKT(upload(ctx, psi, wave->data, D, st));
     double acc[4] = {0, 0, 0, 0};   // four independent sums, added at the end
     int64_t i = 0;
     for (; i + 4 <= D; i += 4)

@@ -337,7 +337,7 @@ extern "C" int tj_wave_trans(tj_ctx *ctx, int direction, const tj_basis *sys_bs,
     return rc;
   for (const auto &u : P.uploads)
     if (u.n > 0) CKW(cudaMemcpyAsync(ctx->wtOps.d() + u.dst, u.src, sizeof(double) * u.n, cudaMemcpyHostToDevice, st));
-  CKW(cudaMemcpyAsync(ctx->wtOld.d(), old_wave->data, sizeof(double) * old_wave->dim, cudaMemcpyHostToDevice, st));
+  CKW(upload(ctx, ctx->wtOld.d(), old_wave->data, old_wave->dim, st));
   std::vector<char> tab;
   auto add = [&](const void *p, size_t n) {
     size_t at = (tab.size() + 255) / 256 * 256;
@@ -393,7 +393,8 @@ extern "C" int tj_wave_trans(tj_ctx *ctx, int direction, const tj_basis *sys_bs,
   double h_nrm = 0;
   CKW(cudaMemcpyAsync(&h_nrm, nrm, sizeof(double), cudaMemcpyDeviceToHost, st));
   {
-    const int rc = download(ctx, new_wave->data, ctx->wtNew.d(), D, st);
+    int rc = download(ctx, new_wave->data, ctx->wtNew.d(), D, st);
+    if (!rc) rc = res_keep(ctx, new_wave->data, D, ctx->wtNew.d(), st);
     if (rc) return rc;
   }
   if (!(h_nrm > 0.0) || !std::isfinite(h_nrm))

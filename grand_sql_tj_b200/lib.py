@@ -371,11 +371,14 @@ class Context:
         e, it = (C.c_double * 1)(), C.c_int()
         _chk(lib().tj_lanczos_memo_new(self.h, C.byref(sb.lat.c), C.byref(ps.c), C.byref(pe.c), C.byref(bs.c),
                                        C.byref(be.c), C.byref(w.c), 1, lanzero, e, C.byref(it)))
+        if self.resident:
+            self._forget_when_freed(w.data)
         return e[0], it.value, w
 
-    def lanczos(self, lat, sys, env, sys_bs, env_bs, wave: Wave, lanzero: float):
-        """lanczos_memo_new on explicit models and bases: returns (E0, iterations, Ritz vector)."""
-        w = wave.copy()
+    def lanczos(self, lat, sys, env, sys_bs, env_bs, wave: Wave, lanzero: float, in_place: bool = False):
+        """lanczos_memo_new on explicit models and bases: returns (E0, iterations, Ritz vector);
+        in_place: the Ritz vector overwrites `wave` (else a copy)."""
+        w = wave if in_place else wave.copy()
         ps, pe, bs, be = sys.pack(), env.pack(), sys_bs.pack(), env_bs.pack()
         e, it = (C.c_double * 1)(), C.c_int()
         _chk(lib().tj_lanczos_memo_new(self.h, C.byref(lat.c), C.byref(ps.c), C.byref(pe.c), C.byref(bs.c),
@@ -400,6 +403,8 @@ class Context:
         pb, pe, ps, pt = sys_bs.pack(), env_bs.pack(), sys_trun.pack(), env_trun.pack()
         _chk(lib().tj_wave_trans(self.h, direction, C.byref(pb.c), C.byref(pe.c), C.byref(ps.c), C.byref(pt.c),
                                  C.byref(old.c), C.byref(new_wave.c)))
+        if self.resident:
+            self._forget_when_freed(new_wave.data)
         return new_wave
 
     def get_oper(self, side: int, dia: int, chain, st_oper: Block, old_idx: int, new_idx: int, truns: bool,
@@ -550,7 +555,9 @@ class DeviceBackend:
         return r
 
     def lanczos(self, lat, sys, env, sys_bs, env_bs, wave, lanzero):
-        return self._traced("lanczos", lambda: self.ctx.lanczos(lat, sys, env, sys_bs, env_bs, wave, lanzero))
+        # the sweep does not reuse its start vector: the Ritz vector overwrites it
+        return self._traced("lanczos", lambda: self.ctx.lanczos(lat, sys, env, sys_bs, env_bs, wave, lanzero,
+                                                                in_place=True))
 
     def truncation(self, wave, side, kept_min, kept_max, trun_err):
         return self._traced("truncation", lambda: self.ctx.truncation(wave, side, kept_min, kept_max, trun_err))

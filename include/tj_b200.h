@@ -159,10 +159,12 @@ int tj_set_wait_limit(tj_ctx *ctx, double seconds);
 /* Invalidates the operators and task lists cached for the current DMRG step. */
 int tj_step_begin(tj_ctx *ctx);
 /* No counterpart in the reference.  Keeps on the device, within a budget of
- * `gigabytes` (0, the default: off), the blocks tj_get_hamiltonian writes
- * into caller arrays; later uploads from inside such an array (tj_model_wave,
- * tj_lanczos_memo_new, tj_get_hamiltonian, the measurement operators) copy
- * the kept device data instead.  The caller must not modify a filled array
+ * `gigabytes` (0, the default: off), the arrays the library writes into
+ * caller memory -- the blocks of tj_get_hamiltonian, the Ritz vector of
+ * tj_lanczos_memo_new, the predicted wavefunction of tj_wave_trans; later
+ * uploads from inside such an array (tj_model_wave, tj_lanczos_memo_new,
+ * tj_truncation, tj_wave_trans, tj_get_hamiltonian, the measurement
+ * operators) copy the kept device data instead.  The caller must not modify a filled array
  * while it is kept: tj_residency_forget(ctx, p) drops the array containing
  * p (do so before freeing or reusing it).  A fingerprint of 64 values of
  * each array, checked at every use, drops an entry whose array changed
