@@ -41,7 +41,6 @@ constexpr int EIG_MAX_N = 4096;
 constexpr double EIG_EPS = 2.220446049250313e-16;        // 2^-52
 constexpr double EIG_SAFMIN = 2.2250738585072014e-308;   // smallest normal FP64
 constexpr int ORTH_THREADS = 512;
-constexpr int TD_CL = 8;          // CTAs of a tridiagonalisation cluster
 constexpr int TD_BIG = 320;       // sectors of at least this many states are reduced by a whole cluster
 
 // Sum of one value per thread over the block, in a fixed order; every thread
@@ -176,16 +175,17 @@ __device__ void tridiag_one(int s, double *Aall, const int64_t *off, const int *
   }
 }
 
-// The same reduction of one large sector by the TD_CL CTAs of a thread-block
+// The same reduction of one large sector by the CL CTAs of a thread-block
 // cluster.  Every CTA forms column k itself (the pending update applied; the
 // same arithmetic in the same order, so the same reflector everywhere); CTA
-// c owns the trailing columns j = c (mod TD_CL), applies the pending rank-2
+// c owns the trailing columns j = c (mod CL), applies the pending rank-2
 // update to them and forms its part of p = A v; the parts meet in shared
 // memory across the cluster (distributed shared memory, two buffers
 // alternating by step) and every CTA sums them in rank order.  One cluster
 // barrier per step orders the owners' column writes (global memory) and the
 // parts before they are read.  The owner of column k stores its reflector
 // there only after that barrier, when no CTA reads the column any more.
+template <int CL>
 __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aall, const int64_t *off,
                              const int *dims, const int64_t *eoff, double *dall, double *eall, double *tauall,
                              double *info, double *sm, double *red, double &sh_tau, double &sh_scl) {
@@ -197,7 +197,7 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
   bool pending = false;
   for (int k = 0; k + 1 < n; ++k) {
     const int k1 = k + 1, m = n - k1;
-    const bool owner = (k % TD_CL) == rank;
+    const bool owner = (k % CL) == rank;
     double *colk = A + (int64_t)k * n;
     double ss = 0.0;
     for (int i = k + tid; i < n; i += nt) {
@@ -228,9 +228,9 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
     const double t = sh_tau, scl = sh_scl;
     for (int i = k1 + tid; i < n; i += nt) v[i] = i == k1 ? 1.0 : v[i] * scl;
     __syncthreads();
-    // owned trailing columns j0, j0 + TD_CL, ...
-    const int j0 = k1 + ((rank - k1) % TD_CL + TD_CL) % TD_CL;
-    const int mloc = j0 < n ? (n - 1 - j0) / TD_CL + 1 : 0;
+    // owned trailing columns j0, j0 + CL, ...
+    const int j0 = k1 + ((rank - k1) % CL + CL) % CL;
+    const int mloc = j0 < n ? (n - 1 - j0) / CL + 1 : 0;
     const int R = min((m + 31) & ~31, nt), G = nt / R;
     const int g = tid / R, r = tid - g * R;
     if (g < G) {
@@ -239,7 +239,7 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
         const double vpi = pending ? vp[i] : 0.0, wpi = pending ? wp[i] : 0.0;
         double acc = 0.0;
         for (int q = g; q < mloc; q += G) {
-          const int j = j0 + q * TD_CL;
+          const int j = j0 + q * CL;
           double *a = A + (int64_t)j * n + i;
           double x = *a;
           if (pending) {
@@ -265,7 +265,7 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
     double pv = 0.0;
     for (int ii = tid; ii < m; ii += nt) {
       double p = 0.0;
-      for (int c = 0; c < TD_CL; ++c) p += cl.map_shared_rank(mine, c)[ii];
+      for (int c = 0; c < CL; ++c) p += cl.map_shared_rank(mine, c)[ii];
       p *= t;
       part[ii] = p;
       pv += p * v[k1 + ii];
@@ -288,20 +288,23 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
   }
 }
 
-// One cluster of TD_CL CTAs per entry of the cluster list: a large sector
-// shared by all of them (tbig), or up to TD_CL small sectors, one per CTA
-// (tsec[cluster * TD_CL + rank], -1 for none).  Sectors largest first.
-__global__ void __cluster_dims__(TD_CL, 1, 1) __launch_bounds__(EIG_THREADS)
+// One cluster of CL CTAs per entry of the cluster list: a large sector
+// shared by all of them (tbig), or up to CL small sectors, one per CTA
+// (tsec[cluster * CL + rank], -1 for none).  Sectors largest first.  CL is
+// 16 where the GPU can schedule clusters of 16 such CTAs (a non-portable
+// size), else 8.
+template <int CL>
+__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(EIG_THREADS)
     tridiag_kernel(double *Aall, const int64_t *off, const int *dims, const int64_t *eoff, const int *tsec,
                    const int *tbig, double *dall, double *eall, double *tauall, double *info) {
   extern __shared__ double sm[];
   __shared__ double red[32];
   __shared__ double sh_tau, sh_scl;
   cg::cluster_group cl = cg::this_cluster();
-  const int b = blockIdx.x / TD_CL, rank = (int)cl.block_rank();
+  const int b = blockIdx.x / CL, rank = (int)cl.block_rank();
   const int s = tsec[blockIdx.x];
   if (tbig[b]) {
-    tridiag_coop(cl, rank, s, Aall, off, dims, eoff, dall, eall, tauall, info, sm, red, sh_tau, sh_scl);
+    tridiag_coop<CL>(cl, rank, s, Aall, off, dims, eoff, dall, eall, tauall, info, sm, red, sh_tau, sh_scl);
   } else if (s >= 0 && dims[s] > 0) {
     tridiag_one(s, Aall, off, dims, eoff, dall, eall, tauall, info, sm, red, sh_tau, sh_scl);
   }
@@ -571,7 +574,7 @@ __device__ void ortho_one(int blk, const int *grp, const int *dims, const int64_
   }
 }
 
-// The same orthonormalisation of one large kept block by the TD_CL CTAs of a
+// The same orthonormalisation of one large kept block by the CL CTAs of a
 // cluster: CTA c owns a slice of rows of every vector.  Per projection pass
 // each CTA forms its part of the dot products with the accepted vectors, the
 // parts meet through distributed shared memory, every CTA sums them in rank
@@ -581,13 +584,14 @@ __device__ void ortho_one(int blk, const int *grp, const int *dims, const int64_
 // cluster barrier; a buffer is written again only two exchanges later, after
 // every CTA has passed the barrier that follows its reads.  A CTA reads and
 // writes only its own rows of the vectors in global memory.
+template <int CL>
 __device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *grp, const int *dims,
                            const int64_t *eoff, const double *evals, const double *info, const int *job_k, double *Y,
                            int ldy, int *status, double *sm, double *red) {
   const int s = grp[4 * blk], j0 = grp[4 * blk + 1], cnt = grp[4 * blk + 2];
   const int n = dims[s], tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   const double lam_min = evals[eoff[s]], cluster = 1e4 * EIG_EPS * info[4 * s + 2];
-  const int per = (n + TD_CL - 1) / TD_CL, r0 = min(n, rank * per), r1 = min(n, r0 + per), nr = r1 - r0;
+  const int per = (n + CL - 1) / CL, r0 = min(n, rank * per), r1 = min(n, r0 + per), nr = r1 - r0;
   // hp: parts of the dots (2 x cnt), h: the dots (cnt), ys: own rows of the
   // vector (per), sl: parts of the squared norm (2)
   double *hp = sm, *h = hp + 2 * cnt, *ys = h + cnt, *sl = ys + per;
@@ -598,7 +602,7 @@ __device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *
     cl.sync();
     ++xch;
     double tot = 0.0;
-    for (int c = 0; c < TD_CL; ++c) tot += *cl.map_shared_rank(slot, c);
+    for (int c = 0; c < CL; ++c) tot += *cl.map_shared_rank(slot, c);
     return tot;
   };
   auto vec = [&](int q) { return Y + (size_t)(j0 + cnt - 1 - q) * ldy; };   // q-th vector in descending order
@@ -635,7 +639,7 @@ __device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *
         ++xch;
         for (int q = tid; q < t; q += nt) {
           double tot = 0.0;
-          for (int c = 0; c < TD_CL; ++c) tot += cl.map_shared_rank(hpw, c)[q];
+          for (int c = 0; c < CL; ++c) tot += cl.map_shared_rank(hpw, c)[q];
           h[q] = tot;
         }
         __syncthreads();
@@ -665,20 +669,21 @@ __device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *
   cl.sync();   // no CTA leaves while another may still read its buffers
 }
 
-// One cluster of TD_CL CTAs per entry of the cluster list: a large kept block
-// shared by all of them (obig), or up to TD_CL small blocks, one per CTA
-// (oblk[cluster * TD_CL + rank], -1 for none).
-__global__ void __cluster_dims__(TD_CL, 1, 1) __launch_bounds__(ORTH_THREADS)
+// One cluster of CL CTAs per entry of the cluster list: a large kept block
+// shared by all of them (obig), or up to CL small blocks, one per CTA
+// (oblk[cluster * CL + rank], -1 for none); CL as for tridiag_kernel.
+template <int CL>
+__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ORTH_THREADS)
     orthonormalize_kernel(const int *oblk, const int *obig, const int *grp, const int *dims, const int64_t *eoff,
                           const double *evals, const double *info, const int *job_k, double *Y, int ldy,
                           int *status) {
   extern __shared__ double sm[];
   __shared__ double red[32];
   cg::cluster_group cl = cg::this_cluster();
-  const int b = blockIdx.x / TD_CL, rank = (int)cl.block_rank();
+  const int b = blockIdx.x / CL, rank = (int)cl.block_rank();
   const int blk = oblk[blockIdx.x];
   if (obig[b])
-    ortho_coop(cl, rank, blk, grp, dims, eoff, evals, info, job_k, Y, ldy, status, sm, red);
+    ortho_coop<CL>(cl, rank, blk, grp, dims, eoff, evals, info, job_k, Y, ldy, status, sm, red);
   else if (blk >= 0)
     ortho_one(blk, grp, dims, eoff, evals, info, job_k, Y, ldy, status, sm, red);
 }
@@ -774,6 +779,37 @@ uint64_t hash_data(const double *p, int64_t n) {
 }
 
 size_t al256(size_t x) { return (x + 255) / 256 * 256; }
+
+// Clusters of 16 CTAs (a non-portable size) where the GPU can schedule one
+// with `threads` threads and `smem` bytes of dynamic shared memory per CTA;
+// otherwise 8.  Asked once per kernel and shared-memory size.
+template <typename K16>
+int cluster_size(K16 kernel16, int threads, size_t smem) {
+  static thread_local std::vector<std::pair<size_t, int>> seen;
+  for (auto &x : seen)
+    if (x.first == smem) return x.second;
+  int cl = 8;
+  if (cudaFuncSetAttribute(kernel16, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess &&
+      cudaFuncSetAttribute(kernel16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess) {
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof cfg);
+    cfg.gridDim = dim3(16, 1, 1);
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = 16;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kernel16, &cfg) == cudaSuccess && n >= 1) cl = 16;
+  }
+  cudaGetLastError();
+  seen.push_back({smem, cl});
+  return cl;
+}
 
 }  // namespace
 
@@ -874,19 +910,21 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     const size_t p_eoff = pos; pos += al256(ob);
     const size_t p_dims = pos; pos += al256(db);
     // clusters of the tridiagonal reduction: one per large sector, then the
-    // small sectors TD_CL at a time (largest first)
+    // small sectors tcl at a time (largest first)
+    const size_t tsm = sizeof(double) * (5 * (size_t)maxn + std::max(maxn, EIG_THREADS));
+    const int tcl = cluster_size(tridiag_kernel<16>, EIG_THREADS, tsm);
     std::vector<int> tsec, tbig;
     {
       size_t q = 0;
       for (; q < order.size() && dims[order[q]] >= TD_BIG; ++q) {
-        tsec.insert(tsec.end(), TD_CL, order[q]);
+        tsec.insert(tsec.end(), tcl, order[q]);
         tbig.push_back(1);
       }
       std::vector<int> small;
       for (; q < order.size(); ++q)
         if (dims[order[q]] > 0) small.push_back(order[q]);
-      for (size_t i = 0; i < small.size(); i += TD_CL) {
-        for (int r = 0; r < TD_CL; ++r) tsec.push_back(i + r < small.size() ? small[i + r] : -1);
+      for (size_t i = 0; i < small.size(); i += tcl) {
+        for (int r = 0; r < tcl; ++r) tsec.push_back(i + r < small.size() ? small[i + r] : -1);
         tbig.push_back(0);
       }
     }
@@ -926,12 +964,17 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     CKT(cudaGetLastError());
     CKT(cudaEventRecord(ctx->tev[1], st));
     // tridiagonal reduction, then all eigenvalues
-    const size_t tsm = sizeof(double) * (5 * (size_t)maxn + std::max(maxn, EIG_THREADS));
     if (nclus) {
-      CKT(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
-      tridiag_kernel<<<nclus * TD_CL, EIG_THREADS, tsm, st>>>(ctx->trB.d(), d_roff, d_dims, d_eoff,
-                                                              (const int *)(tbase + p_tsec),
-                                                              (const int *)(tbase + p_tbig), dd, de, dtau, dinfo);
+      const int *d_tsec = (const int *)(tbase + p_tsec), *d_tbig = (const int *)(tbase + p_tbig);
+      if (tcl == 16) {
+        CKT(cudaFuncSetAttribute(tridiag_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+        tridiag_kernel<16><<<nclus * 16, EIG_THREADS, tsm, st>>>(ctx->trB.d(), d_roff, d_dims, d_eoff, d_tsec, d_tbig,
+                                                                 dd, de, dtau, dinfo);
+      } else {
+        CKT(cudaFuncSetAttribute(tridiag_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+        tridiag_kernel<8><<<nclus * 8, EIG_THREADS, tsm, st>>>(ctx->trB.d(), d_roff, d_dims, d_eoff, d_tsec, d_tbig,
+                                                               dd, de, dtau, dinfo);
+      }
       CKT(cudaGetLastError());
     }
     CKT(cudaEventRecord(ctx->tev[2], st));
@@ -1058,7 +1101,9 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       const size_t q_grp = q; q += al256(grp.size() * 4);
       const size_t q_slab = q; q += al256(slab.size() * 4);
       // clusters of the orthonormalisation: one per large kept block (cnt^2 n
-      // above 3e7), then the other blocks TD_CL at a time, largest first
+      // above 3e7), then the other blocks ocl at a time, largest first
+      const size_t osm = sizeof(double) * (3 * (size_t)maxn + (maxn + 7) / 8 + 8);
+      const int ocl = cluster_size(orthonormalize_kernel<16>, ORTH_THREADS, osm);
       std::vector<int> oblk, obig;
       {
         std::vector<int> bo(ngrp);
@@ -1067,11 +1112,11 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
         std::stable_sort(bo.begin(), bo.end(), [&](int a, int b) { return work(a) > work(b); });
         size_t i = 0;
         for (; i < bo.size() && work(bo[i]) >= 3e7; ++i) {
-          oblk.insert(oblk.end(), TD_CL, bo[i]);
+          oblk.insert(oblk.end(), ocl, bo[i]);
           obig.push_back(1);
         }
-        for (; i < bo.size(); i += TD_CL) {
-          for (int r = 0; r < TD_CL; ++r) oblk.push_back(i + r < bo.size() ? bo[i + r] : -1);
+        for (; i < bo.size(); i += ocl) {
+          for (int r = 0; r < ocl; ++r) oblk.push_back(i + r < bo.size() ? bo[i + r] : -1);
           obig.push_back(0);
         }
       }
@@ -1099,11 +1144,17 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       CKT(cudaGetLastError());
       CKT(cudaEventRecord(ctx->tev[5], st));
       {
-        const size_t osm = sizeof(double) * (3 * (size_t)maxn + (maxn + TD_CL - 1) / TD_CL + 8);
-        CKT(cudaFuncSetAttribute(orthonormalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)osm));
-        orthonormalize_kernel<<<nocl * TD_CL, ORTH_THREADS, osm, st>>>(
-            (const int *)(ab + q_oblk), (const int *)(ab + q_obig), (const int *)(ab + q_grp), d_dims, d_eoff, dev,
-            dinfo, (const int *)(ab + q_k), Y, ldy, d_status);
+        const int *d_oblk = (const int *)(ab + q_oblk), *d_obig = (const int *)(ab + q_obig);
+        const int *d_grp = (const int *)(ab + q_grp), *d_k = (const int *)(ab + q_k);
+        if (ocl == 16) {
+          CKT(cudaFuncSetAttribute(orthonormalize_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)osm));
+          orthonormalize_kernel<16><<<nocl * 16, ORTH_THREADS, osm, st>>>(d_oblk, d_obig, d_grp, d_dims, d_eoff, dev,
+                                                                          dinfo, d_k, Y, ldy, d_status);
+        } else {
+          CKT(cudaFuncSetAttribute(orthonormalize_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)osm));
+          orthonormalize_kernel<8><<<nocl * 8, ORTH_THREADS, osm, st>>>(d_oblk, d_obig, d_grp, d_dims, d_eoff, dev,
+                                                                        dinfo, d_k, Y, ldy, d_status);
+        }
       }
       CKT(cudaGetLastError());
       CKT(cudaEventRecord(ctx->tev[6], st));
