@@ -467,6 +467,14 @@ struct Builder {
       if (fr.rs_rel != REL_NONE) f.rs_idx += base[fr.rs_rel];
       if (fr.cs_rel != REL_NONE) f.cs_idx += base[fr.cs_rel];
     }
+    // The GEMM's producer arms each stage with the bytes of the stage's
+    // k-blocks, counted from the family totals below, and copies each
+    // segment's k-blocks from its two splits: the totals are the sums of the
+    // segments, and every segment's k-blocks must lie inside both splits, or
+    // a stage would wait for bytes that never come (or copy past a split).
+    for (const OzSeg &sg : oz.segs)
+      if (sg.nkb < 1 || sg.a_kb0 < 0 || sg.b_kb0 < 0 || sg.a_kb0 + sg.nkb > sg.a_nkb || sg.b_kb0 + sg.nkb > sg.b_nkb)
+        throw std::runtime_error("split-precision plan: a segment's k-blocks leave its splits");
     for (OzFam &f : oz.fams) {
       f.nkb = 0;
       f.pad = 0;
