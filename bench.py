@@ -278,7 +278,8 @@ def sweep_leg(ctx64, ctxoz, name: str, prep: str, seed: int):
     truncation + operator renormalisation + wavefunction prediction, with
     host buffers in and out (the drop-in's calling pattern) and the blocks
     the library returns also kept on the device (tj_set_residency), so that
-    the next steps read them without a host upload."""
+    the next steps read them without a host upload, and written into
+    page-locked host buffers that are reused (HostPool)."""
     import numpy as np
     from grand_sql_tj_b200.lattice import Geometry
     from grand_sql_tj_b200.lib import DeviceBackend
@@ -292,6 +293,7 @@ def sweep_leg(ctx64, ctxoz, name: str, prep: str, seed: int):
     for c in (ctx64, ctxoz):
         if c is not None:
             c.set_residency(RESIDENCY_GB)
+            c.use_host_pool(True)
     d = Dmrg(geo, DeviceBackend(ctxoz if (prep == "mixed" and ctxoz is not None) else ctx64), p)
     t0 = time.perf_counter()
     d.warm_up()
@@ -380,6 +382,7 @@ def config5_leg(ctx, nx: int, m: int, sweeps: int, seed: int):
     out = {"lattice": "6x%d cylinder (y periodic, x open)" % nx, "t": 1.0, "t2": -0.2, "J": 1.0 / 3.0, "m": m,
            "sweeps": sweeps, "instances": []}
     ctx.set_residency(RESIDENCY_GB)
+    ctx.use_host_pool(True)
     lasts = []
     for delta in CONFIG5_DOPINGS:
         holes = 2 * int(n * delta / 2.0 + 0.5)   # rounded half up to an even number

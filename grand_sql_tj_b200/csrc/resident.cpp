@@ -185,12 +185,15 @@ cudaError_t upload(tj_ctx *ctx, double *dst, const double *src, int64_t n, cudaS
 // staging chunks: the DMA of chunk c runs while chunk c - 1 is copied out on
 // the host by several threads.  A copy straight into pageable memory runs
 // at a fraction of the DMA rate, and slower still into pages never touched
-// (each first touch is a page fault inside the copy).  Returns when dst is
-// filled.
+// (each first touch is a page fault inside the copy); a page-locked
+// destination is written directly.  Returns when dst is filled.
 int download(tj_ctx *ctx, double *dst, const double *src, int64_t n, cudaStream_t st) {
   const size_t chunk = (size_t)8 << 20;
   const size_t bytes = (size_t)n * 8;
-  if (bytes <= ((size_t)1 << 20)) {
+  cudaPointerAttributes pa;
+  const bool locked = cudaPointerGetAttributes(&pa, dst) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  if (locked || bytes <= ((size_t)1 << 20)) {   // page-locked memory takes the DMA directly
     if (n > 0 && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
       return set_err(TJ_ERR_CUDA, "download: copy failed");
     if (cudaStreamSynchronize(st) != cudaSuccess) return set_err(TJ_ERR_CUDA, "download: stream failed");

@@ -246,13 +246,64 @@ def _chk(rc: int):
         raise TjError(rc, lib().tj_last_error().decode())
 
 
+class HostPool:
+    """Page-locked host buffers reused for arrays the library writes (blocks,
+    wavefunctions).  Each buffer is registered once (tj_host_register), so
+    the device writes it by DMA at full rate, and goes back to the pool when
+    the array made from it is freed, so that its pages are not faulted in and
+    pinned again for the next array.  Sizes are rounded up to eight classes
+    per octave."""
+
+    def __init__(self):
+        self.free = {}
+        self.ptrs = []
+
+    @staticmethod
+    def size_class(n: int) -> int:
+        if n <= 1 << 12:
+            return 1 << 12
+        q = 1 << (n.bit_length() - 4)
+        return (n + q - 1) // q * q
+
+    def get(self, n: int) -> np.ndarray:
+        c = self.size_class(n)
+        lst = self.free.get(c)
+        if lst:
+            buf = lst.pop()
+        else:
+            buf = np.empty(c)
+            _chk(lib().tj_host_register(buf.ctypes.data, buf.nbytes))
+            self.ptrs.append(buf.ctypes.data)
+        view = buf[:n]
+        weakref.finalize(view, self._put, c, buf)
+        return view
+
+    def _put(self, c: int, buf: np.ndarray):
+        self.free.setdefault(c, []).append(buf)
+
+    def close(self):
+        for p in self.ptrs:
+            lib().tj_host_unregister(p)
+        self.ptrs, self.free = [], {}
+
+
 class Context:
     """One tj_ctx: a CUDA device, a stream and the cached plan of the current step."""
 
     def __init__(self, device: int = 0):
         self.h = C.c_void_p()
         self.resident = False
+        self.pool: Optional[HostPool] = None
         _chk(lib().tj_ctx_create(C.byref(self.h), device))
+
+    def use_host_pool(self, on: bool = True):
+        """Blocks from get_hamiltonian and the sweep's wavefunctions go into
+        page-locked, reused host buffers (HostPool)."""
+        if on and self.pool is None:
+            self.pool = HostPool()
+        elif not on and self.pool is not None:
+            self.pool.close()
+            self.pool = None
 
     def set_residency(self, gigabytes: float):
         """tj_set_residency: keep the blocks get_hamiltonian returns on the device
@@ -275,6 +326,9 @@ class Context:
         if self.h:
             lib().tj_ctx_destroy(self.h)
             self.h = C.c_void_p()
+        if self.pool is not None:
+            self.pool.close()
+            self.pool = None
 
     def __del__(self):
         try:
@@ -390,7 +444,8 @@ class Context:
         the Model `pre` enlarged into `basis` and truncated with `trun`; returns the new Model."""
         pp, pb, pt = pre.pack(), basis.pack(), trun.pack()
         rc, m = call_model_result(lambda r: lib().tj_get_hamiltonian(self.h, C.byref(lat.c), side, mshift,
-                                                                     C.byref(pp.c), C.byref(pb.c), C.byref(pt.c), r))
+                                                                     C.byref(pp.c), C.byref(pb.c), C.byref(pt.c), r),
+                                  alloc=self.pool.get if self.pool is not None else None)
         _chk(rc)
         if self.resident:
             self._forget_when_freed(m._packed.data)
@@ -566,6 +621,9 @@ class DeviceBackend:
         return self._traced("get_hamiltonian", lambda: self.ctx.get_hamiltonian(lat, side, mshift, pre, basis, trun))
 
     def wave_trans(self, direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave):
+        if self.ctx.pool is not None:   # the predicted vector goes into a pooled page-locked buffer
+            new_wave = Wave(new_wave.sys_len, new_wave.env_len, new_wave.sectors,
+                            self.ctx.pool.get(max(new_wave.dim, 1)))
         return self.ctx.wave_trans(direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave)
 
     def get_oper(self, side, dia, chain, st_oper, old_idx, new_idx, truns, types="B"):

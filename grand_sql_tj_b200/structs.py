@@ -360,9 +360,10 @@ def block_transfer_trans(b: Block) -> Block:
 RESULT_HOST_S = {}
 
 
-def call_model_result(call):
+def call_model_result(call, alloc=None):
     """Runs a two-call model-result entry point `call(res_ptr) -> rc` and
-    returns the new Model (copied out of the result arrays)."""
+    returns the new Model (views into its result arrays); alloc(n) gives the
+    data array of n doubles (default: a new zeroed array)."""
     t0 = time.perf_counter()
     res = TjModelResult()
     rc = call(C.byref(res))
@@ -371,7 +372,7 @@ def call_model_result(call):
     t1 = time.perf_counter()
     sets = (TjBlockSet * max(res.nsub, 1))()
     subs = (TjBlockSub * max(res.n_subs, 1))()
-    data = np.zeros(max(res.data_len, 1))
+    data = np.zeros(max(res.data_len, 1)) if alloc is None else alloc(max(res.data_len, 1))
     res.sets = C.cast(sets, C.POINTER(TjBlockSet))
     res.subs = C.cast(subs, C.POINTER(TjBlockSub))
     res.data = data.ctypes.data_as(c_double_p)

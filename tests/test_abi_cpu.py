@@ -74,3 +74,14 @@ def test_struct_layouts_match_the_header(tmp_path):
         assert got[(cname, "size")] == C.sizeof(cls), cname
         for f in cls._fields_:
             assert got[(cname, f[0])] == getattr(cls, f[0]).offset, (cname, f[0])
+
+
+def test_host_pool_size_classes():
+    """HostPool rounds sizes up to eight classes per octave (at most 1/8 more)."""
+    from grand_sql_tj_b200.lib import HostPool
+    prev = 0
+    for n in list(range(1, 70000, 97)) + [10 ** 6, 3 * 10 ** 6 + 7, 2 ** 24, 2 ** 24 + 1]:
+        c = HostPool.size_class(n)
+        assert c >= n and c >= 4096 and c <= max(4096, n + n // 8 + 1)
+        assert c >= prev
+        prev = c

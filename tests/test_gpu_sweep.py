@@ -105,8 +105,9 @@ def test_device_run_matches_oracle_run(ctx, oracle_lib):
 
 
 def test_residency_gives_the_same_run(product_lib):
-    """Blocks kept on the device (tj_set_residency) give the same run as
-    uploads from the host arrays, bit for bit, with uploads served from the
+    """Blocks kept on the device (tj_set_residency), written into pooled
+    page-locked host buffers, give the same run as uploads from ordinary host
+    arrays, bit for bit, with uploads served from the
     kept copies; a kept array that the caller changes where its fingerprint
     looks is dropped and read from the host again."""
     from grand_sql_tj_b200.lib import Context, DeviceBackend
@@ -114,6 +115,7 @@ def test_residency_gives_the_same_run(product_lib):
     c0, c1 = Context(0), Context(0)
     try:
         c1.set_residency(2.0)
+        c1.use_host_pool(True)
         geo = Geometry(8, 2, t=1.0, J=1.0 / 3.0, esite=0.0, up_bias=1)
         ref = Dmrg(Geometry(8, 2, t=1.0, J=1.0 / 3.0, esite=0.0, up_bias=1), DeviceBackend(c0), p).ground_state(1)
         d = Dmrg(geo, DeviceBackend(c1), p)
