@@ -348,6 +348,8 @@ def sweep_leg(ctx64, ctxoz, name: str, prep: str, seed: int):
         lz = [st for name, st, _, _ in trace if name == "lanczos"]
         out[tag]["lanczos_ms"] = {"prepare": sum(st.prepare_ms for st in lz), "plan": sum(st.plan_ms for st in lz),
                                   "split_plan": sum(st.ozplan_ms for st in lz),
+                                  "upload": sum(st.upload_ms for st in lz),
+                                  "wall": 1e3 * sum(w for name, _, w, _ in trace if name == "lanczos"),
                                   "iterations": sum(st.lanczos_ms for st in lz)}
         return recs
 
