@@ -302,6 +302,13 @@ def sweep_leg(ctx64, ctxoz, name: str, prep: str, seed: int):
     prep_s = time.perf_counter() - t0
     snap = ({k: dict(getattr(d, k)) for k in ("sysblocks", "envblocks", "systruns", "envtruns", "sysbs", "envbs")},
             d.wave.copy(), d.rng.bit_generator.state)
+    # the page-locked pool holds a sweep's worth of buffers before the timed
+    # sweeps (a running DMRG reuses the buffers of the blocks it replaces; the
+    # snapshot above keeps those alive)
+    from grand_sql_tj_b200.lib import HOST_POOL
+    blocks = list(d.sysblocks.values()) + list(d.envblocks.values())
+    HOST_POOL.reserve([m._packed.data.size for m in blocks if getattr(m, "_packed", None) is not None and
+                       hasattr(m._packed, "data")] + [r.dim for r in d.records[-(2 * (N - 3)):]])
     out = {"lattice": "%dx%d" % (ny, nx), "electrons": ne, "m": m, "prep_s": prep_s, "prep_precision": prep,
            "residency_gb": RESIDENCY_GB,
            "steps_per_sweep": 2 * (N - 3)}

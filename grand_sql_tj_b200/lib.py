@@ -246,17 +246,25 @@ def _chk(rc: int):
         raise TjError(rc, lib().tj_last_error().decode())
 
 
+class _PoolView:
+    """The owner of the numpy arrays made from one pool buffer: every view and
+    every slice of them refers to it, so it dies only with the last of them."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 3}
+
+
 class HostPool:
     """Page-locked host buffers reused for arrays the library writes (blocks,
     wavefunctions).  Each buffer is registered once (tj_host_register), so
     the device writes it by DMA at full rate, and goes back to the pool when
-    the array made from it is freed, so that its pages are not faulted in and
-    pinned again for the next array.  Sizes are rounded up to eight classes
-    per octave."""
+    the last array (or slice) made from it is freed, so that its pages are not
+    faulted in and pinned again for the next array.  Sizes are rounded up to
+    eight classes per octave."""
 
     def __init__(self):
         self.free = {}
-        self.ptrs = []
+        self.bufs = []   # every buffer (kept alive here for the process)
 
     @staticmethod
     def size_class(n: int) -> int:
@@ -271,20 +279,25 @@ class HostPool:
         if lst:
             buf = lst.pop()
         else:
-            buf = np.empty(c)
-            _chk(lib().tj_host_register(buf.ctypes.data, buf.nbytes))
-            self.ptrs.append(buf.ctypes.data)
-        view = buf[:n]
-        weakref.finalize(view, self._put, c, buf)
-        return view
+            buf = (C.c_double * c)()
+            _chk(lib().tj_host_register(C.addressof(buf), C.sizeof(buf)))
+            self.bufs.append(buf)
+        owner = _PoolView(C.addressof(buf), n)
+        weakref.finalize(owner, self._put, c, buf)
+        return np.asarray(owner)
 
-    def _put(self, c: int, buf: np.ndarray):
+    def _put(self, c: int, buf):
         self.free.setdefault(c, []).append(buf)
 
-    def close(self):
-        for p in self.ptrs:
-            lib().tj_host_unregister(p)
-        self.ptrs, self.free = [], {}
+    def reserve(self, sizes):
+        """Registers buffers for arrays of the given sizes ahead of use (the
+        registration, not the later use, then carries the pinning cost)."""
+        held = [self.get(n) for n in sizes]
+        del held
+
+
+# One pool per process: page-locked memory serves every context of the device.
+HOST_POOL = HostPool()
 
 
 class Context:
@@ -298,12 +311,8 @@ class Context:
 
     def use_host_pool(self, on: bool = True):
         """Blocks from get_hamiltonian and the sweep's wavefunctions go into
-        page-locked, reused host buffers (HostPool)."""
-        if on and self.pool is None:
-            self.pool = HostPool()
-        elif not on and self.pool is not None:
-            self.pool.close()
-            self.pool = None
+        page-locked, reused host buffers (the process's HostPool)."""
+        self.pool = HOST_POOL if on else None
 
     def set_residency(self, gigabytes: float):
         """tj_set_residency: keep the blocks get_hamiltonian returns on the device
@@ -326,9 +335,7 @@ class Context:
         if self.h:
             lib().tj_ctx_destroy(self.h)
             self.h = C.c_void_p()
-        if self.pool is not None:
-            self.pool.close()
-            self.pool = None
+        self.pool = None
 
     def __del__(self):
         try:
