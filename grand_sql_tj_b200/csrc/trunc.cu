@@ -175,25 +175,46 @@ __device__ void tridiag_one(int s, double *Aall, const int64_t *off, const int *
   }
 }
 
+// Sum of one value per thread over the block with one barrier: each warp's
+// sum goes to its slot of red[2][32] (the half selected by the caller's
+// alternating flag, so that the next sum does not overwrite a half still
+// being read) and every thread adds the slots in the same order.
+__device__ __forceinline__ double block_sum1(double x, double *red, int &half) {
+  for (int k = 16; k > 0; k >>= 1) x += __shfl_xor_sync(0xffffffffu, x, k);
+  double *r = red + 32 * half;
+  half ^= 1;
+  if ((threadIdx.x & 31) == 0) r[threadIdx.x >> 5] = x;
+  __syncthreads();
+  double s = 0.0;
+  const int nw = blockDim.x >> 5;
+  for (int w = 0; w < nw; ++w) s += r[w];
+  return s;
+}
+
 // The same reduction of one large sector by the CL CTAs of a thread-block
 // cluster.  Every CTA forms column k itself (the pending update applied; the
-// same arithmetic in the same order, so the same reflector everywhere); CTA
-// c owns the trailing columns j = c (mod CL), applies the pending rank-2
-// update to them and forms its part of p = A v; the parts meet in shared
-// memory across the cluster (distributed shared memory, two buffers
-// alternating by step) and every CTA sums them in rank order.  One cluster
-// barrier per step orders the owners' column writes (global memory) and the
-// parts before they are read.  The owner of column k stores its reflector
-// there only after that barrier, when no CTA reads the column any more.
+// same arithmetic in the same order, so the same reflector everywhere, and
+// every thread derives beta, tau and the scale from the same sum); CTA c
+// owns the trailing columns j = c (mod CL), applies the pending rank-2 update
+// to them and forms its part of p = A v, one thread per row (the reflector
+// is scaled where it is read); the parts meet in shared memory across the
+// cluster (distributed shared memory, two buffers alternating by step) and
+// every CTA sums them in rank order.  Per step: one cluster barrier, which
+// orders the owners' column writes (global memory) and the parts before they
+// are read, and three CTA barriers.  The owner of column k stores its
+// reflector there only after the cluster barrier, when no CTA reads the
+// column any more.
 template <int CL>
 __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aall, const int64_t *off,
                              const int *dims, const int64_t *eoff, double *dall, double *eall, double *tauall,
-                             double *info, double *sm, double *red, double &sh_tau, double &sh_scl) {
+                             double *info, double *sm, double *red2) {
   const int n = dims[s], tid = threadIdx.x, nt = blockDim.x;
   double *A = Aall + off[s];
   double *d = dall + eoff[s], *e = eall + eoff[s], *tau = tauall + eoff[s];
-  // vp, wp, v: n each; part: max(n, nt); cp: the cluster parts, 2 x n
-  double *vp = sm, *wp = vp + n, *v = wp + n, *part = v + n, *cp = part + max(n, nt);
+  // vp, wp, v: n each; cp: the cluster parts, 2 x n (read by the other CTAs
+  // until the next barrier); pp: the summed p = tau A v, n
+  double *vp = sm, *wp = vp + n, *v = wp + n, *cp = v + n, *pp = cp + 2 * n;
+  int half = 0;
   bool pending = false;
   for (int k = 0; k + 1 < n; ++k) {
     const int k1 = k + 1, m = n - k1;
@@ -206,75 +227,61 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
       v[i] = a;
       if (i > k1) ss += a * a;
     }
-    const double sigma2 = block_sum(ss, red);
-    if (tid == 0) {
-      const double alpha = v[k1];
-      double beta = alpha, t = 0.0, scl = 0.0;
-      if (sigma2 > 0.0) {
-        const double nr = sqrt(alpha * alpha + sigma2);
-        beta = alpha >= 0.0 ? -nr : nr;
-        t = (beta - alpha) / beta;
-        scl = 1.0 / (alpha - beta);
-      }
-      if (owner) {
-        d[k] = v[k];
-        e[k] = beta;
-        tau[k] = t;
-      }
-      sh_tau = t;
-      sh_scl = scl;
+    const double sigma2 = block_sum1(ss, red2, half);   // also the barrier after v
+    const double alpha = v[k1];
+    double beta = alpha, t = 0.0, scl = 0.0;
+    if (sigma2 > 0.0) {
+      const double nr = sqrt(alpha * alpha + sigma2);
+      beta = alpha >= 0.0 ? -nr : nr;
+      t = (beta - alpha) / beta;
+      scl = 1.0 / (alpha - beta);
     }
-    __syncthreads();
-    const double t = sh_tau, scl = sh_scl;
-    for (int i = k1 + tid; i < n; i += nt) v[i] = i == k1 ? 1.0 : v[i] * scl;
-    __syncthreads();
-    // owned trailing columns j0, j0 + CL, ...
+    if (owner && tid == 0) {
+      d[k] = v[k];
+      e[k] = beta;
+      tau[k] = t;
+    }
+    // the scaled reflector: 1 at k1, v[i] * scl below
+    auto rv = [&](int i) { return i == k1 ? 1.0 : v[i] * scl; };
+    // owned trailing columns j0, j0 + CL, ...; one thread per row
     const int j0 = k1 + ((rank - k1) % CL + CL) % CL;
     const int mloc = j0 < n ? (n - 1 - j0) / CL + 1 : 0;
-    const int R = min((m + 31) & ~31, nt), G = nt / R;
-    const int g = tid / R, r = tid - g * R;
-    if (g < G) {
-      for (int ii = r; ii < m; ii += R) {
-        const int i = k1 + ii;
-        const double vpi = pending ? vp[i] : 0.0, wpi = pending ? wp[i] : 0.0;
-        double acc = 0.0;
-        for (int q = g; q < mloc; q += G) {
-          const int j = j0 + q * CL;
-          double *a = A + (int64_t)j * n + i;
-          double x = *a;
-          if (pending) {
-            x -= vpi * wp[j] + wpi * vp[j];
-            *a = x;
-          }
-          acc += x * v[j];
-        }
-        part[g * m + ii] = acc;
-      }
-    }
-    __syncthreads();
     double *mine = cp + (k & 1) * n;
     for (int ii = tid; ii < m; ii += nt) {
-      double p = 0.0;
-      for (int q = 0; q < G; ++q) p += part[q * m + ii];
-      mine[ii] = p;
+      const int i = k1 + ii;
+      const double vpi = pending ? vp[i] : 0.0, wpi = pending ? wp[i] : 0.0;
+      double acc = 0.0;
+      double *a = A + (int64_t)j0 * n + i;
+#pragma unroll 4
+      for (int q = 0; q < mloc; ++q, a += (int64_t)CL * n) {
+        const int j = j0 + q * CL;
+        double x = *a;
+        if (pending) {
+          x -= vpi * wp[j] + wpi * vp[j];
+          *a = x;
+        }
+        acc += x * rv(j);
+      }
+      mine[ii] = acc;
     }
     __threadfence();
     cl.sync();
     if (owner)
-      for (int i = k1 + tid; i < n; i += nt) colk[i] = v[i];
+      for (int i = k1 + tid; i < n; i += nt) colk[i] = rv(i);
     double pv = 0.0;
     for (int ii = tid; ii < m; ii += nt) {
       double p = 0.0;
       for (int c = 0; c < CL; ++c) p += cl.map_shared_rank(mine, c)[ii];
       p *= t;
-      part[ii] = p;
-      pv += p * v[k1 + ii];
+      pp[ii] = p;
+      pv += p * rv(k1 + ii);
     }
-    const double K = 0.5 * t * block_sum(pv, red);
+    const double K = 0.5 * t * block_sum1(pv, red2, half);
     for (int ii = tid; ii < m; ii += nt) {
       const int i = k1 + ii;
-      wp[i] = part[ii] - K * v[i];
-      vp[i] = v[i];
+      const double vi = rv(i);
+      wp[i] = pp[ii] - K * vi;
+      vp[i] = vi;
     }
     pending = true;
     __syncthreads();
@@ -298,13 +305,13 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(EIG_THREADS)
     tridiag_kernel(double *Aall, const int64_t *off, const int *dims, const int64_t *eoff, const int *tsec,
                    const int *tbig, double *dall, double *eall, double *tauall, double *info) {
   extern __shared__ double sm[];
-  __shared__ double red[32];
+  __shared__ double red[64];
   __shared__ double sh_tau, sh_scl;
   cg::cluster_group cl = cg::this_cluster();
   const int b = blockIdx.x / CL, rank = (int)cl.block_rank();
   const int s = tsec[blockIdx.x];
   if (tbig[b]) {
-    tridiag_coop<CL>(cl, rank, s, Aall, off, dims, eoff, dall, eall, tauall, info, sm, red, sh_tau, sh_scl);
+    tridiag_coop<CL>(cl, rank, s, Aall, off, dims, eoff, dall, eall, tauall, info, sm, red);
   } else if (s >= 0 && dims[s] > 0) {
     tridiag_one(s, Aall, off, dims, eoff, dall, eall, tauall, info, sm, red, sh_tau, sh_scl);
   }
@@ -422,20 +429,25 @@ __global__ void inverse_iter_kernel(const double *dall, const double *eall, cons
   for (int i = 0; i < n; ++i) AT(X, i) = start_entry(s, k, i);
   bool bad = false;
   for (int sweep = 0; sweep < 3; ++sweep) {
-    // forward: P and L
+    // forward: P and L.  The running entry stays in a register and the loads
+    // do not depend on it, so the unrolled loop has them in flight ahead of
+    // the arithmetic (the factors are read from L2 at the latency of a load)
+    double cur = AT(X, 0);
+#pragma unroll 8
     for (int i = 0; i + 1 < n; ++i) {
-      const double l = AT(DL, i);
-      if (piv[(size_t)i * st + j]) {
-        const double t = AT(X, i);
-        const double xi = AT(X, i + 1);
-        AT(X, i) = xi;
-        AT(X, i + 1) = t - l * xi;
+      const double l = AT(DL, i), nxt = AT(X, i + 1);
+      if (piv[(size_t)i * st + j]) {   // rows i and i+1 exchanged
+        AT(X, i) = nxt;
+        cur = cur - l * nxt;
       } else {
-        AT(X, i + 1) -= l * AT(X, i);
+        AT(X, i) = cur;
+        cur = nxt - l * cur;
       }
     }
+    AT(X, n - 1) = cur;
     // backward: U, with a rescale of the whole vector if it nears overflow
     double x1 = 0.0, x2 = 0.0;   // x_{i+1}, x_{i+2}
+#pragma unroll 8
     for (int i = n - 1; i >= 0; --i) {
       double xi = (AT(X, i) - AT(DU, i) * x1 - AT(DU2, i) * x2) / AT(U, i);
       if (fabs(xi) > 1e250) {
@@ -581,6 +593,7 @@ __device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *
   // vector (per), sl: parts of the squared norm (2)
   double *hp = sm, *h = hp + 2 * cnt, *ys = h + cnt, *sl = ys + per;
   unsigned xch = 0;   // exchanges so far (buffer parity)
+  int half = 0;       // block_sum1's alternating half of red
   auto cluster_sum = [&](double x) -> double {   // x: the CTA's value, the same in all its threads
     double *slot = sl + (xch & 1);
     if (tid == 0) *slot = x;
@@ -606,7 +619,7 @@ __device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *
           ys[i] = v;
           ss += v * v;
         }
-        const double inv = 1.0 / sqrt(cluster_sum(block_sum(ss, red)));
+        const double inv = 1.0 / sqrt(cluster_sum(block_sum1(ss, red, half)));
         for (int i = tid; i < nr; i += nt) ys[i] *= inv;
         __syncthreads();
       }
@@ -635,7 +648,7 @@ __device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *
           ys[i] = acc;
           ss += acc * acc;
         }
-        const double nrm = sqrt(cluster_sum(block_sum(ss, red)));   // the same value in every CTA
+        const double nrm = sqrt(cluster_sum(block_sum1(ss, red, half)));   // the same value in every CTA
         if (pass == 0 && !(nrm >= 1e-3)) {
           ok = false;
           break;
@@ -663,7 +676,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ORTH_THREADS)
                           const double *evals, const double *info, const int *job_k, double *Y, int ldy,
                           int *status) {
   extern __shared__ double sm[];
-  __shared__ double red[32];
+  __shared__ double red[64];
   cg::cluster_group cl = cg::this_cluster();
   const int b = blockIdx.x / CL, rank = (int)cl.block_rank();
   const int blk = oblk[blockIdx.x];
@@ -896,7 +909,7 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     const size_t p_dims = pos; pos += al256(db);
     // clusters of the tridiagonal reduction: one per large sector, then the
     // small sectors tcl at a time (largest first)
-    const size_t tsm = sizeof(double) * (5 * (size_t)maxn + std::max(maxn, EIG_THREADS));
+    const size_t tsm = sizeof(double) * (6 * (size_t)maxn + std::max(maxn, EIG_THREADS));
     const int tcl = cluster_size(tridiag_kernel<16>, EIG_THREADS, tsm);
     std::vector<int> tsec, tbig;
     {
