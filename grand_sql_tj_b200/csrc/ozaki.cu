@@ -458,17 +458,6 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
         // held: zero times any int8 is zero)
         int done = 0, in_stage = 0;   // granules
         uint32_t sa = 0, sbb = 0, fbar = 0;
-        // a copy continues the pending one of its operand when both its source
-        // and its destination do (the static concatenation of a family is one
-        // run in the split): the pending copy is issued when a piece does not
-        // continue it and when the stage closes
-        uint32_t pa_dst = 0, pa_n = 0, pb_dst = 0, pb_n = 0;
-        const uint8_t *pa_src = nullptr, *pb_src = nullptr;
-        auto flush = [&]() {
-          if (pa_n && lane == 0) oz_bulk_g2s(pa_dst, pa_src, pa_n, fbar);
-          if (pb_n && lane == 1) oz_bulk_g2s(pb_dst, pb_src, pb_n, fbar);
-          pa_n = pb_n = 0;
-        };
         for (int s0 = sb; s0 < se && ok; s0 += 32) {
           // the next <= 32 segments, one per lane
           OzSeg mine;
@@ -501,30 +490,14 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
               // the granules of this segment that go into the current stage are
               // contiguous in the split and in the stage: one copy per operand
               const int take = min(ngr - g, 2 * C::KPS - in_stage);
-              {
-                const uint32_t da = sa + in_stage * ga * GR, na = (uint32_t)take * ga * GR;
-                const uint32_t db = sbb + in_stage * gb * GR, nb = (uint32_t)take * gb * GR;
-                const uint8_t *s_a = asrc + (int64_t)g * ga * GR, *s_b = bsrc + (int64_t)g * gb * GR;
-                const bool cont_a = pa_n && s_a == pa_src + pa_n && da == pa_dst + pa_n;
-                const bool cont_b = pb_n && s_b == pb_src + pb_n && db == pb_dst + pb_n;
-                if (cont_a) {
-                  pa_n += na;
-                } else {
-                  if (pa_n && lane == 0) oz_bulk_g2s(pa_dst, pa_src, pa_n, fbar);
-                  pa_dst = da, pa_src = s_a, pa_n = na;
-                }
-                if (cont_b) {
-                  pb_n += nb;
-                } else {
-                  if (pb_n && lane == 1) oz_bulk_g2s(pb_dst, pb_src, pb_n, fbar);
-                  pb_dst = db, pb_src = s_b, pb_n = nb;
-                }
-              }
+              if (lane == 0)
+                oz_bulk_g2s(sa + in_stage * ga * GR, asrc + (int64_t)g * ga * GR, (uint32_t)take * ga * GR, fbar);
+              if (lane == 1)
+                oz_bulk_g2s(sbb + in_stage * gb * GR, bsrc + (int64_t)g * gb * GR, (uint32_t)take * gb * GR, fbar);
               g += take;
               done += take;
               in_stage += take;
               if (in_stage == 2 * C::KPS || done == fm.ngr) {
-                flush();
                 if ((in_stage & 1) && lane == 0) oz_bulk_g2s(sa + in_stage * ga * GR, p.zeros, ga * GR, fbar);
                 in_stage = 0;
                 if (++stage == ST) stage = 0, ph ^= 1u;
