@@ -301,12 +301,10 @@ int tjb::install_plan(tj_ctx *ctx, std::unique_ptr<HpsiPlan> P, uint64_t h,
         (rc = upload_vec(ctx, ctx->ozStaMJobs, oz->sta_mjobs)) || (rc = upload_vec(ctx, ctx->ozPsiMJobs, oz->psi_mjobs)) ||
         (rc = upload_vec(ctx, ctx->ozProdMJobs, oz->prod_mjobs)))
       return rc;
-    // the pools, then (256-byte aligned) the zero granule of the GEMM's odd families
-    if ((rc = ctx->ozPack.reserve(oz_zero_off(*oz) + OZ_ZERO_BYTES + 256)) ||
+    if ((rc = ctx->ozPack.reserve(oz->sta_pack + oz->dyn_pack + 256)) ||
         (rc = ctx->ozScales.reserve(sizeof(double) * (oz->n_scales + 4))) || (rc = ctx->ozMisc.reserve(256)))
       return rc;
     CK(cudaMemsetAsync(ctx->ozMisc.p, 0, 256, ctx->stream));
-    CK(cudaMemsetAsync((char *)ctx->ozPack.p + oz_zero_off(*oz), 0, OZ_ZERO_BYTES, ctx->stream));
     launch_oz_stack_rows((const OzCell *)ctx->ozCells.p, (int)oz->cells.size(), (const OzProdRow *)ctx->ozProdRows.p,
                          (OzStackRow *)ctx->ozStackRows.p, oz->n_stack_rows, ctx->stream);
     CK(cudaMemsetAsync(ctx->ozScales.p, 0, sizeof(double) * (oz->n_scales + 4), ctx->stream));
@@ -374,7 +372,6 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
   const uint64_t wait_ns = (uint64_t)(ctx->wait_s * 1e9);
   double *scales = ctx->ozScales.d();
   uint8_t *pack = (uint8_t *)ctx->ozPack.p;
-  const uint8_t *zeros = pack + oz_zero_off(oz);
   CK(cudaMemsetAsync(scales + oz.dyn_scale_begin, 0, sizeof(double) * (oz.n_scales - oz.dyn_scale_begin), st));
   if (timed) CK(cudaEventRecord(ctx->ev[0], st));
   launch_oz_max((const OzJob *)ctx->ozPsiMJobs.p, (int)oz.psi_mjobs.size(), (const OzSpan *)ctx->ozPsiMSpans.p,
@@ -386,8 +383,7 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
                     (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzCell *)ctx->ozCells.p,
                     (const OzStackRow *)ctx->ozStackRows.p,
-                    (const Task *)ctx->tasks2.p, pack, zeros, scales, in, ctx->scr.d(), out, err, oz.s, oz.bn, wait_ns,
-                    st));
+                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, oz.bn, wait_ns, st));
   if (timed) CK(cudaEventRecord(ctx->ev[2], st));
   launch_oz_max((const OzJob *)ctx->ozProdMJobs.p, (int)oz.prod_mjobs.size(), (const OzSpan *)ctx->ozProdMSpans.p,
                 (int)oz.prod_mspans.size(), ctx->ops.d(), in, ctx->scr.d(), scales, err, st);
@@ -398,8 +394,7 @@ static int run_hpsi_oz(tj_ctx *ctx, const double *in, double *out, bool timed) {
                     (const OzSeg *)ctx->ozSegs.p,
                     (const OzFam *)ctx->ozFams.p, (const OzCell *)ctx->ozCells.p,
                     (const OzStackRow *)ctx->ozStackRows.p,
-                    (const Task *)ctx->tasks2.p, pack, zeros, scales, in, ctx->scr.d(), out, err, oz.s, oz.bn, wait_ns,
-                    st));
+                    (const Task *)ctx->tasks2.p, pack, scales, in, ctx->scr.d(), out, err, oz.s, oz.bn, wait_ns, st));
   if (timed) CK(cudaEventRecord(ctx->ev[4], st));
   CK(cudaGetLastError());
   ++ctx->n_hpsi;

@@ -61,7 +61,7 @@ __device__ __forceinline__ bool oz_unit(const OzJob *jobs, int njobs, const OzSp
   int64_t k = (int64_t)sp.u0 + threadIdx.x;
   for (; j < njobs; ++j) {
     J = jobs[j];
-    const int rows = J.gtot * 8, nk16 = (J.K + 15) / 16;
+    const int rows = J.gtot * 8, nk16 = (J.K + 31) / 32 * 2;
     const int64_t units = (int64_t)rows * nk16;
     if (k < units) {
       // consecutive threads: consecutive rows, so that the 16-byte digit rows
@@ -192,10 +192,10 @@ __global__ void __launch_bounds__(OZ_SPLIT_THREADS) oz_split_kernel(const OzJob 
   const int sr = J.row0 + r;
   const int t = sr / J.R, rl = sr - t * J.R;
   const int gt = t < J.ntiles - 1 ? J.R / 8 : J.gt_last;
-  const int g = rl >> 3, r8 = rl & 7;
-  const int64_t plane = (int64_t)gt * 128;   // bytes of one slice of one granule of the tile
-  uint8_t *dst = pack + J.dst + (int64_t)t * J.ngr * S * (J.R / 8) * 128 + ((int64_t)(J.gr0 + c16) * S * gt + g) * 128 +
-                 r8 * 16;
+  const int kb = c16 >> 1, c = c16 & 1, g = rl >> 3, r8 = rl & 7;
+  const int64_t plane = (int64_t)gt * 256;   // bytes of one slice of one k-block of the tile
+  uint8_t *dst = pack + J.dst + (int64_t)t * J.nkb * S * (J.R / 8) * 256 + ((int64_t)(J.kb0 + kb) * S * gt + g) * 256 +
+                 c * 128 + r8 * 16;
 #pragma unroll
   for (int q = 0; q < S; ++q)
     *reinterpret_cast<uint4 *>(dst + q * plane) = make_uint4(dig[q][0], dig[q][1], dig[q][2], dig[q][3]);
@@ -211,7 +211,6 @@ struct OzGemmParams {
   const OzStackRow *srows;
   const Task *tasks;
   const uint8_t *pack;
-  const uint8_t *zeros;   // a zero granule (16 groups, all slices): pairs a family's odd last granule
   double *scales;
   const double *psi;
   double *scr, *out;
@@ -369,7 +368,7 @@ template <int S, int BN>
 __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParams p) {
   using C = OzCfg<S, BN>;
   constexpr int ST = C::STAGES;
-  constexpr uint32_t GR = S * 128;   // bytes of one row group (all slices) of one granule
+  constexpr uint32_t GB = S * 256;   // bytes of one row group (all slices) of one k-block
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ __align__(8) uint64_t full_bar[ST], empty_bar[ST], tfull_bar[2], tempty_bar[2], drain_bar;
   __shared__ uint32_t tmem_sh;
@@ -447,16 +446,14 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       // tiles of this item: A row tile ta (ga groups), B column tile tb (gb groups)
       const uint32_t ga = (uint32_t)((it.mrows + 7) >> 3), gb = (uint32_t)(it.N >> 3);
       const int64_t ta = it.row0 / 128, tb = it.col0 / BN;
+      const uint32_t bytes1 = (ga + gb) * GB;   // one k-block of both operands
       for (int f = it.fam_begin; f < it.fam_end && ok; ++f) {
         const OzFam fm = p.fams[f];
         const int sb = fm.seg_begin, se = fm.seg_end;
-        // the family's granules, segment after segment, fill stages of up to
-        // 2 KPS granules (KPS k-blocks); a stage may hold the end of one
-        // segment and the start of the next; stage boundaries fall every 2 KPS
-        // granules of the family, and an odd last granule is paired with a
-        // zero A granule (the B granule it meets is whatever int8 the stage
-        // held: zero times any int8 is zero)
-        int done = 0, in_stage = 0;   // granules
+        // the family's k-blocks, segment after segment, fill stages of up to
+        // KPS k-blocks (a stage may hold the end of one segment and the start
+        // of the next; stage boundaries fall every KPS k-blocks of the family)
+        int done = 0, in_stage = 0;
         uint32_t sa = 0, sbb = 0, fbar = 0;
         for (int s0 = sb; s0 < se && ok; s0 += 32) {
           // the next <= 32 segments, one per lane
@@ -466,20 +463,17 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
           for (int j = 0; j < cnt && ok; ++j) {
             const int64_t a_base = __shfl_sync(0xffffffffu, mine.a_base, j);
             const int64_t b_base = __shfl_sync(0xffffffffu, mine.b_base, j);
-            const int32_t a_ngr = __shfl_sync(0xffffffffu, mine.a_ngr, j);
-            const int32_t b_ngr = __shfl_sync(0xffffffffu, mine.b_ngr, j);
-            const int32_t a_gr0 = __shfl_sync(0xffffffffu, mine.a_gr0, j);
-            const int32_t b_gr0 = __shfl_sync(0xffffffffu, mine.b_gr0, j);
-            const int32_t ngr = __shfl_sync(0xffffffffu, mine.ngr, j);
-            const uint8_t *asrc = p.pack + a_base + ta * a_ngr * (int64_t)(16 * GR) + (int64_t)a_gr0 * ga * GR;
-            const uint8_t *bsrc = p.pack + b_base + tb * b_ngr * (int64_t)((BN / 8) * GR) + (int64_t)b_gr0 * gb * GR;
-            for (int g = 0; g < ngr;) {
+            const int32_t a_nkb = __shfl_sync(0xffffffffu, mine.a_nkb, j);
+            const int32_t b_nkb = __shfl_sync(0xffffffffu, mine.b_nkb, j);
+            const int32_t a_kb0 = __shfl_sync(0xffffffffu, mine.a_kb0, j);
+            const int32_t b_kb0 = __shfl_sync(0xffffffffu, mine.b_kb0, j);
+            const int32_t nkb = __shfl_sync(0xffffffffu, mine.nkb, j);
+            const uint8_t *asrc = p.pack + a_base + ta * a_nkb * (int64_t)(16 * GB) + (int64_t)a_kb0 * ga * GB;
+            const uint8_t *bsrc = p.pack + b_base + tb * b_nkb * (int64_t)((BN / 8) * GB) + (int64_t)b_kb0 * gb * GB;
+            for (int kb = 0; kb < nkb;) {
               if (in_stage == 0) {
-                // the stage's bytes: its real granules of both operands and
-                // the zero A granule when their number is odd
-                const int real = min(2 * C::KPS, fm.ngr - done);
-                const int slots = (real + 1) & ~1;
-                if (!acquire((uint32_t)slots * ga * GR + (uint32_t)real * gb * GR)) {
+                const int n = min(C::KPS, fm.nkb - done);
+                if (!acquire((uint32_t)n * bytes1)) {
                   ok = false;
                   break;
                 }
@@ -487,18 +481,17 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
                 sbb = sa + C::A_BYTES;
                 fbar = oz_smem(&full_bar[stage]);
               }
-              // the granules of this segment that go into the current stage are
+              // the k-blocks of this segment that go into the current stage are
               // contiguous in the split and in the stage: one copy per operand
-              const int take = min(ngr - g, 2 * C::KPS - in_stage);
+              const int take = min(nkb - kb, C::KPS - in_stage);
               if (lane == 0)
-                oz_bulk_g2s(sa + in_stage * ga * GR, asrc + (int64_t)g * ga * GR, (uint32_t)take * ga * GR, fbar);
+                oz_bulk_g2s(sa + in_stage * ga * GB, asrc + (int64_t)kb * ga * GB, (uint32_t)take * ga * GB, fbar);
               if (lane == 1)
-                oz_bulk_g2s(sbb + in_stage * gb * GR, bsrc + (int64_t)g * gb * GR, (uint32_t)take * gb * GR, fbar);
-              g += take;
+                oz_bulk_g2s(sbb + in_stage * gb * GB, bsrc + (int64_t)kb * gb * GB, (uint32_t)take * gb * GB, fbar);
+              kb += take;
               done += take;
               in_stage += take;
-              if (in_stage == 2 * C::KPS || done == fm.ngr) {
-                if ((in_stage & 1) && lane == 0) oz_bulk_g2s(sa + in_stage * ga * GR, p.zeros, ga * GR, fbar);
+              if (in_stage == C::KPS || done == fm.nkb) {
                 in_stage = 0;
                 if (++stage == ST) stage = 0, ph ^= 1u;
               }
@@ -519,7 +512,7 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
       uint32_t ph = 0;
       uint32_t famc = 0;
       bool ok = true, issued = false;
-
+      const uint64_t dbase = oz_desc(0u, 128u, 256u);   // start address added per stage
       for (int ii = p.cta[blockIdx.x], ie = p.cta[blockIdx.x + 1]; ii < ie && ok; ++ii) {
         const OzItem it = get_item(ii);
         // MMA pa multiplies A slice pa with B slices 1..S+1-pa (N' = (S+1-pa) N):
@@ -527,14 +520,9 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
         uint32_t idesc[S];
 #pragma unroll
         for (int pa = 1; pa <= S; ++pa) idesc[pa - 1] = oz_idesc(it.M, (S + 1 - pa) * it.N);
-        // a k-block is two granules side by side: the leading-byte offset
-        // (between the K halves) is one granule of the item's tile, the
-        // stride-byte offset (between row groups) 128; the start address is
-        // added per k-block
-        const uint32_t ga = (uint32_t)((it.mrows + 7) >> 3), gb = (uint32_t)(it.N >> 3);
-        const uint32_t aslice16 = ga * 8u;                 // A slice stride (ga groups) in 16-byte units
-        const uint32_t ga_gr = ga * GR, gb_gr = gb * GR;   // bytes of one A / B granule
-        const uint64_t adesc = oz_desc(0u, ga_gr, 128u), bdesc = oz_desc(0u, gb_gr, 128u);
+        const uint32_t aslice16 = (uint32_t)((it.mrows + 7) >> 3) * 16u;   // A slice stride in 16-byte units
+        const uint32_t ga_gb = (uint32_t)((it.mrows + 7) >> 3) * GB;       // bytes of one A k-block
+        const uint32_t gb_gb = (uint32_t)(it.N >> 3) * GB;                 // bytes of one B k-block
         const int nf = it.fam_end - it.fam_begin;
         for (int f = 0; f < nf && ok; ++f) {
           const int nkb_f = p.fams[it.fam_begin + f].nkb;
@@ -558,9 +546,9 @@ __global__ void __launch_bounds__(OZ_GEMM_THREADS, 1) oz_gemm_kernel(OzGemmParam
             const uint32_t sa = smem0 + (uint32_t)(stage * C::STAGE);
             const int n = min(C::KPS, nkb - kb);   // k-blocks in this stage
             for (int j = 0; j < n; ++j) {
-              // k-block j of the stage: A at sa + 2 j ga_gr, B at sa + A_BYTES + 2 j gb_gr
-              const uint64_t da0 = adesc + (uint64_t)((sa + 2u * (uint32_t)j * ga_gr) >> 4);
-              const uint64_t db = bdesc + (uint64_t)((sa + C::A_BYTES + 2u * (uint32_t)j * gb_gr) >> 4);
+              // k-block j of the stage: A at sa + j ga GB, B at sa + A_BYTES + j gb GB
+              const uint64_t da0 = dbase + (uint64_t)((sa + (uint32_t)j * ga_gb) >> 4);
+              const uint64_t db = dbase + (uint64_t)((sa + C::A_BYTES + (uint32_t)j * gb_gb) >> 4);
 #pragma unroll
               for (int pa = 1; pa <= S; ++pa) {
                 const uint64_t da = da0 + (uint64_t)((pa - 1) * aslice16);   // A slices ga groups apart
@@ -929,10 +917,10 @@ static cudaError_t launch_gemm_t(const OzGemmParams &p, int ncta, cudaStream_t s
 
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
                            const OzCell *cells, const OzStackRow *srows, const Task *tasks, const uint8_t *pack,
-                           const uint8_t *zeros, double *scales, const double *psi, double *scr, double *out,
-                           int *err, int s, int bn, uint64_t wait_ns, cudaStream_t st) {
+                           double *scales, const double *psi, double *scr, double *out, int *err, int s, int bn,
+                           uint64_t wait_ns, cudaStream_t st) {
   if (ncta <= 0) return cudaSuccess;
-  const OzGemmParams p{items, cta, segs, fams, cells, srows, tasks, pack, zeros, scales, psi, scr, out, err, wait_ns};
+  const OzGemmParams p{items, cta, segs, fams, cells, srows, tasks, pack, scales, psi, scr, out, err, wait_ns};
   if (s == 5 && bn == 32) return launch_gemm_t<5, 32>(p, ncta, st);
   if (bn != oz_bn(s)) return cudaErrorInvalidValue;
   switch (s) {

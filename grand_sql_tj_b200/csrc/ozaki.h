@@ -31,19 +31,15 @@
 //
 // Split storage ("pack" pools, bytes): a split of `rows` x K is cut into
 // tiles of R rows (R = 128 for an A operand, R = BN for a B operand) and
-// ceil(K / 16) granules of 16 k.  Tile t holds G_t row groups of 8 rows (R/8
-// for all but the last; the last holds ceil(rem/8) for A, round16(rem)/8 for
-// B, so a B tile is a whole number of 16-row MMA columns), laid out
-//   [tile][granule][slice p][group g < G_t][row r8 (8)][16 bytes]
-// so that one granule of one tile, all slices, is ONE contiguous block of
-// s * G_t * 128 bytes.  Two granules side by side in shared memory are one
-// 32-wide k-block of the MMA in the canonical UMMA K-major, no-swizzle layout
-// (core matrices of 8 rows x 16 bytes; leading-byte offset s * G * 128
-// between the two K halves, stride-byte offset 128 between row groups).
-// A family's tasks are concatenated at the granule, so that a task of inner
-// dimension K costs ceil(K / 16) granules, not ceil(K / 32) k-blocks: the
-// k-blocks of a family are its granules taken in pairs (a last odd granule
-// is paired with zeros).
+// ceil(K / 32) k-blocks.  Tile t holds G_t row groups of 8 rows (R/8 for all
+// but the last; the last holds ceil(rem/8) for A, round16(rem)/8 for B, so a
+// B tile is a whole number of 16-row MMA columns), laid out
+//   [tile][kb][slice p][group g < G_t][c (2)][row r8 (8)][16 bytes]
+// so that one k-block of one tile, all slices, is ONE contiguous block of
+// s * G_t * 256 bytes: it lands in shared memory as s consecutive slices in
+// the canonical UMMA K-major, no-swizzle layout (core matrices of 8 rows x
+// 16 bytes, leading-byte offset 128 between the two K halves, stride-byte
+// offset 256 between row groups).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -60,9 +56,9 @@ constexpr int OZ_MAX_S = 8;
 inline int oz_bn(int s) { return s <= 5 ? 48 : 32; }
 
 // One split job: rows [0, nrows) x k [0, K) of coef * M, M(r, k) =
-// base[src_off + r*rs + k*ks], written as split rows row0 + r, granules
-// [gr0, gr0 + ceil(K/16)) of the split at pack offset `dst` (tiles of R
-// rows, ngr granules in all, ntiles tiles, the last of gt_last groups).  The
+// base[src_off + r*rs + k*ks], written as split rows row0 + r, k-blocks
+// [kb0, kb0 + ceil(K/32)) of the split at pack offset `dst` (tiles of R
+// rows, nkb k-blocks in all, ntiles tiles, the last of gt_last groups).  The
 // job writes gtot groups (rows up to row0 + 8*gtot; rows past nrows and k
 // past K as zero digits).  The row scale is scales[scale_idx + r] (max
 // |value| of the row, made a power of two by the kernels); want_max: the job
@@ -74,18 +70,18 @@ struct OzJob {
   int64_t scale_idx;
   double coef;
   int32_t rs, ks, nrows, K;
-  int32_t gtot, gr0;
-  int32_t R, ngr, ntiles, gt_last, row0;
+  int32_t gtot, kb0;
+  int32_t R, nkb, ntiles, gt_last, row0;
   int8_t space, want_max, want_split;
   int8_t pad;
 };
 
-// One k-range of an operand pair: granules [a_gr0, a_gr0 + ngr) of the A
-// split and [b_gr0, b_gr0 + ngr) of the B split.
+// One k-range of an operand pair: k-blocks [a_kb0, a_kb0 + nkb) of the A
+// split and [b_kb0, b_kb0 + nkb) of the B split.
 struct OzSeg {
   int64_t a_base, b_base;   // pack offsets of the splits
-  int32_t a_ngr, b_ngr;     // their granule counts (tile strides)
-  int32_t a_gr0, b_gr0, ngr;
+  int32_t a_nkb, b_nkb;     // their k-block counts (tile strides)
+  int32_t a_kb0, b_kb0, nkb;
   int32_t pad;
 };
 
@@ -94,8 +90,8 @@ struct OzSeg {
 struct OzFam {
   int32_t seg_begin, seg_end;
   int64_t rs_idx, cs_idx;
-  int32_t nkb;              // k-blocks: its segments' granules in pairs
-  int32_t ngr;              // granules of all its segments
+  int32_t nkb;              // k-blocks of all its segments
+  int32_t pad;
 };
 
 // A work item: the output tile rows [row0, row0 + M) x cols [col0, col0 + N)
@@ -192,10 +188,6 @@ struct OzPlan {
   double flops1 = 0, flops2 = 0;           // FP64-equivalent flops of each launch
 };
 
-// Byte offset of the zero granule in the pack buffer: after the static and
-// dynamic pools, 256-byte aligned.
-inline int64_t oz_zero_off(const OzPlan &oz) { return (oz.sta_pack + oz.dyn_pack + 255) / 256 * 256; }
-
 // Builds the split-precision form of an H*psi plan (host); tp.oz_bn picks
 // the N tile (0: oz_bn(s); 32 is also available for s = 5) and
 // tp.oz_item_cost the per-item cost of the static schedule.
@@ -210,11 +202,9 @@ void launch_oz_max(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans
                    const double *psi, const double *scr, double *scales, int *err, cudaStream_t st);
 void launch_oz_split(const OzJob *jobs, int njobs, const OzSpan *spans, int nspans, const double *ops,
                      const double *psi, const double *scr, const double *scales, uint8_t *pack, int s, cudaStream_t st);
-// zeros: a zero granule of 16 groups, all slices (OZ_ZERO_BYTES), 16-byte aligned
-constexpr int OZ_ZERO_BYTES = 16 * OZ_MAX_S * 128;
 cudaError_t launch_oz_gemm(const OzItem *items, const int32_t *cta, int ncta, const OzSeg *segs, const OzFam *fams,
                            const OzCell *cells, const OzStackRow *srows, const Task *tasks, const uint8_t *pack,
-                           const uint8_t *zeros, double *scales, const double *psi, double *scr, double *out, int *err, int s, int bn,
+                           double *scales, const double *psi, double *scr, double *out, int *err, int s, int bn,
                            uint64_t wait_ns, cudaStream_t st);
 
 }  // namespace tjb

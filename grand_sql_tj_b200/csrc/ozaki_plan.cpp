@@ -30,10 +30,9 @@ inline int32_t cdiv(int64_t a, int64_t b) { return (int32_t)((a + b - 1) / b); }
 // Which dynamic scale pool an index is relative to while building.
 enum { REL_NONE = -1, REL_RHO = 0, REL_TAU = 1, REL_PI = 2 };
 
-// Tiling of a split: tiles of R rows and ngr granules (16 k each); the
-// last tile of gt_last groups.
+// Tiling of a split: tiles of R rows; the last one of gt_last groups.
 struct Tiling {
-  int32_t rows, R, ngr, ntiles, gt_last, gsum;
+  int32_t rows, R, nkb, ntiles, gt_last, gsum;
 };
 
 struct Builder {
@@ -61,14 +60,14 @@ struct Builder {
     Tiling t;
     t.rows = rows;
     t.R = b_role ? oz.bn : 128;
-    t.ngr = cdiv(K, 16);
+    t.nkb = cdiv(K, 32);
     t.ntiles = cdiv(rows, t.R);
     const int32_t rem = rows - (t.ntiles - 1) * t.R;
     t.gt_last = b_role ? (rem + 15) / 16 * 2 : cdiv(rem, 8);
     t.gsum = (t.ntiles - 1) * (t.R / 8) + t.gt_last;
     return t;
   }
-  int64_t split_bytes(const Tiling &t) const { return (int64_t)t.ngr * S * t.gsum * 128; }
+  int64_t split_bytes(const Tiling &t) const { return (int64_t)t.nkb * S * t.gsum * 256; }
   static int64_t align256(int64_t x) { return (x + 255) / 256 * 256; }
   int64_t alloc_sta(const Tiling &t) {
     const int64_t o = sta_bytes;
@@ -87,9 +86,9 @@ struct Builder {
   }
 
   // A job writing rows [row0, row0 + 8*gtot) (gtot groups; the first nrows
-  // from the source) and granules from gr0 of the split at dst.
+  // from the source) and k-blocks from kb0 of the split at dst.
   static OzJob job(int8_t space, int64_t src_off, int32_t rs, int32_t ks, int32_t nrows, int32_t K, double coef,
-                   int64_t dst, const Tiling &t, int32_t row0, int32_t gtot, int32_t gr0, int64_t scale_idx,
+                   int64_t dst, const Tiling &t, int32_t row0, int32_t gtot, int32_t kb0, int64_t scale_idx,
                    bool want_max) {
     if (nrows < 1 || K < 1 || gtot < 1) throw std::runtime_error("empty split");
     OzJob j;
@@ -103,9 +102,9 @@ struct Builder {
     j.nrows = nrows;
     j.K = K;
     j.gtot = gtot;
-    j.gr0 = gr0;
+    j.kb0 = kb0;
     j.R = t.R;
-    j.ngr = t.ngr;
+    j.nkb = t.nkb;
     j.ntiles = t.ntiles;
     j.gt_last = t.gt_last;
     j.row0 = row0;
@@ -232,10 +231,10 @@ struct Builder {
       OzSeg sg;
       std::memset(&sg, 0, sizeof sg);
       sg.a_base = pk;
-      sg.a_ngr = ta.ngr;
+      sg.a_nkb = ta.nkb;
       sg.b_base = psi_col(x);
-      sg.b_ngr = cdiv(K, 16);
-      sg.ngr = cdiv(K, 16);
+      sg.b_nkb = cdiv(K, 32);
+      sg.nkb = cdiv(K, 32);
       OzFam f;
       std::memset(&f, 0, sizeof f);
       f.seg_begin = (int)oz.segs.size();
@@ -265,7 +264,7 @@ struct Builder {
           it.fam_end = fi + 1;
           it.init = 0;
           it.pi_idx = 0;
-          it.cost = item_cost(it, cdiv(sg.ngr, 2));
+          it.cost = item_cost(it, sg.nkb);
           oz.items1.push_back(it);
         }
     }
@@ -274,19 +273,19 @@ struct Builder {
   // A family of tasks that share the B side's concatenation (right: psi rows,
   // two-sided: product rows).
   int right_family(const Cell &c, int64_t ci, const std::vector<int> &tl, bool prods) {
-    int32_t grt = 0;   // granules of the concatenation: each task's K rounded up to 16
-    for (int ti : tl) grt += cdiv(hp.tasks2[ti].K, 16);
-    const Tiling tb = tiling(c.N, 16 * grt, true);
+    int32_t kbt = 0;
+    for (int ti : tl) kbt += cdiv(hp.tasks2[ti].K, 32);
+    const Tiling tb = tiling(c.N, 32 * kbt, true);
     const int64_t pk = alloc_sta(tb);
     const int64_t sc = alloc_scales(c.N);
     OzFam f;
     f.seg_begin = (int)oz.segs.size();
-    int32_t gr = 0;
+    int32_t kb = 0;
     for (int ti : tl) {
       const Task &t = hp.tasks2[ti];
       int32_t rs, ks;
       strides(t.R, 1, rs, ks);
-      oz.sta_jobs.push_back(job(SP_OPS, t.R.off, rs, ks, c.N, t.K, t.coef, pk, tb, 0, tb.gsum, gr, sc, true));
+      oz.sta_jobs.push_back(job(SP_OPS, t.R.off, rs, ks, c.N, t.K, t.coef, pk, tb, 0, tb.gsum, kb, sc, true));
       OzSeg sg;
       std::memset(&sg, 0, sizeof sg);
       if (!prods) {
@@ -305,15 +304,15 @@ struct Builder {
           throw std::runtime_error("two-sided task operand shape");
         sg.a_base = prod_row(p);
       }
-      sg.a_ngr = cdiv(t.K, 16);
-      sg.a_gr0 = 0;
+      sg.a_nkb = cdiv(t.K, 32);
+      sg.a_kb0 = 0;
       sg.b_base = pk;
-      sg.b_ngr = tb.ngr;
-      sg.b_gr0 = gr;
-      sg.ngr = cdiv(t.K, 16);
+      sg.b_nkb = tb.nkb;
+      sg.b_kb0 = kb;
+      sg.nkb = cdiv(t.K, 32);
       seg_dyn_a.push_back((int)oz.segs.size());
       oz.segs.push_back(sg);
-      gr += sg.ngr;
+      kb += sg.nkb;
     }
     f.seg_end = (int)oz.segs.size();
     f.rs_idx = hp.cell2_row_state[ci];
@@ -325,19 +324,19 @@ struct Builder {
   }
 
   int left_family(const Cell &c, int64_t ci, const std::vector<int> &tl) {
-    int32_t grt = 0;   // granules of the concatenation: each task's K rounded up to 16
-    for (int ti : tl) grt += cdiv(hp.tasks2[ti].K, 16);
-    const Tiling ta = tiling(c.M, 16 * grt, false);
+    int32_t kbt = 0;
+    for (int ti : tl) kbt += cdiv(hp.tasks2[ti].K, 32);
+    const Tiling ta = tiling(c.M, 32 * kbt, false);
     const int64_t pk = alloc_sta(ta);
     const int64_t sc = alloc_scales(c.M);
     OzFam f;
     f.seg_begin = (int)oz.segs.size();
-    int32_t gr = 0;
+    int32_t kb = 0;
     for (int ti : tl) {
       const Task &t = hp.tasks2[ti];
       int32_t rs, ks;
       strides(t.L, 0, rs, ks);
-      oz.sta_jobs.push_back(job(SP_OPS, t.L.off, rs, ks, c.M, t.K, t.coef, pk, ta, 0, ta.gsum, gr, sc, true));
+      oz.sta_jobs.push_back(job(SP_OPS, t.L.off, rs, ks, c.M, t.K, t.coef, pk, ta, 0, ta.gsum, kb, sc, true));
       const int x = psi_index(t.R);
       const Cell &X = hp.cells2[x];
       if (X.M != t.K || X.N != c.N || hp.cell2_col_state[x] != hp.cell2_col_state[ci])
@@ -345,15 +344,15 @@ struct Builder {
       OzSeg sg;
       std::memset(&sg, 0, sizeof sg);
       sg.a_base = pk;
-      sg.a_ngr = ta.ngr;
-      sg.a_gr0 = gr;
+      sg.a_nkb = ta.nkb;
+      sg.a_kb0 = kb;
       sg.b_base = psi_col(x);
-      sg.b_ngr = cdiv(t.K, 16);
-      sg.b_gr0 = 0;
-      sg.ngr = cdiv(t.K, 16);
+      sg.b_nkb = cdiv(t.K, 32);
+      sg.b_kb0 = 0;
+      sg.nkb = cdiv(t.K, 32);
       seg_dyn_b.push_back((int)oz.segs.size());
       oz.segs.push_back(sg);
-      gr += sg.ngr;
+      kb += sg.nkb;
     }
     f.seg_end = (int)oz.segs.size();
     f.rs_idx = sc;
@@ -367,11 +366,8 @@ struct Builder {
   void add_items(std::vector<OzItem> &dst, const Cell &c, int cell_idx, int fb, int fe, int init) {
     const int BN = oz.bn;
     int64_t kbs = 0;
-    for (int f = fb; f < fe; ++f) {
-      int64_t gr = 0;   // a family's k-blocks: its granules in pairs
-      for (int sgi = oz.fams[f].seg_begin; sgi < oz.fams[f].seg_end; ++sgi) gr += oz.segs[sgi].ngr;
-      kbs += (gr + 1) / 2;
-    }
+    for (int f = fb; f < fe; ++f)
+      for (int sgi = oz.fams[f].seg_begin; sgi < oz.fams[f].seg_end; ++sgi) kbs += oz.segs[sgi].nkb;
     for (int32_t r0 = 0; r0 < c.M; r0 += 128)
       for (int32_t n0 = 0; n0 < c.N; n0 += BN) {
         OzItem it;
@@ -477,12 +473,12 @@ struct Builder {
     // segments, and every segment's k-blocks must lie inside both splits, or
     // a stage would wait for bytes that never come (or copy past a split).
     for (const OzSeg &sg : oz.segs)
-      if (sg.ngr < 1 || sg.a_gr0 < 0 || sg.b_gr0 < 0 || sg.a_gr0 + sg.ngr > sg.a_ngr || sg.b_gr0 + sg.ngr > sg.b_ngr)
-        throw std::runtime_error("split-precision plan: a segment's granules leave its splits");
+      if (sg.nkb < 1 || sg.a_kb0 < 0 || sg.b_kb0 < 0 || sg.a_kb0 + sg.nkb > sg.a_nkb || sg.b_kb0 + sg.nkb > sg.b_nkb)
+        throw std::runtime_error("split-precision plan: a segment's k-blocks leave its splits");
     for (OzFam &f : oz.fams) {
-      f.ngr = 0;
-      for (int i = f.seg_begin; i < f.seg_end; ++i) f.ngr += oz.segs[i].ngr;
-      f.nkb = (f.ngr + 1) / 2;   // an odd last granule is paired with a zero one
+      f.nkb = 0;
+      f.pad = 0;
+      for (int i = f.seg_begin; i < f.seg_end; ++i) f.nkb += oz.segs[i].nkb;
     }
     for (std::vector<OzItem> *v : {&oz.items1, &oz.items2})
       for (OzItem &it : *v) {
@@ -571,7 +567,7 @@ struct Builder {
   // Split units cover gtot*8 rows x K/16; maximum units nrows x K/OZ_MAX_CHUNK.
   static int64_t job_units(const OzJob &j, bool max_units) {
     if (max_units) return (int64_t)(j.want_max == 2 ? (j.nrows + 31) / 32 * 32 : j.nrows) * cdiv(j.K, OZ_MAX_CHUNK);
-    return (int64_t)j.gtot * 8 * cdiv(j.K, 16);
+    return (int64_t)j.gtot * 8 * (cdiv(j.K, 32) * 2);
   }
   static void make_spans(const std::vector<OzJob> &jobs, std::vector<OzSpan> &spans, bool max_units) {
     spans.clear();

@@ -80,19 +80,19 @@ class PlanExport(C.Structure):
 
 class OzJobC(C.Structure):
     _fields_ = [("src_off", C.c_int64), ("dst", C.c_int64), ("scale_idx", C.c_int64), ("coef", C.c_double)] + \
-               [(n, C.c_int32) for n in ("rs", "ks", "nrows", "K", "gtot", "gr0", "R", "ngr", "ntiles", "gt_last",
+               [(n, C.c_int32) for n in ("rs", "ks", "nrows", "K", "gtot", "kb0", "R", "nkb", "ntiles", "gt_last",
                                          "row0")] + \
                [("space", C.c_int8), ("want_max", C.c_int8), ("want_split", C.c_int8), ("pad_", C.c_int8)]
 
 
 class OzSegC(C.Structure):
     _fields_ = [("a_base", C.c_int64), ("b_base", C.c_int64)] + \
-               [(n, C.c_int32) for n in ("a_ngr", "b_ngr", "a_gr0", "b_gr0", "ngr", "pad_")]
+               [(n, C.c_int32) for n in ("a_nkb", "b_nkb", "a_kb0", "b_kb0", "nkb", "pad_")]
 
 
 class OzFamC(C.Structure):
     _fields_ = [("seg_begin", C.c_int32), ("seg_end", C.c_int32), ("rs_idx", C.c_int64), ("cs_idx", C.c_int64),
-                ("nkb", C.c_int32), ("ngr", C.c_int32)]
+                ("nkb", C.c_int32), ("pad_", C.c_int32)]
 
 
 class OzItemC(C.Structure):

@@ -639,11 +639,11 @@ int tj_wave_trans_plan_export(int direction, const tj_basis *sys_bs, const tj_ba
 typedef struct tj_oz_job {
   int64_t src_off, dst, scale_idx;
   double coef;
-  int32_t rs, ks, nrows, K, gtot, gr0, R, ngr, ntiles, gt_last, row0;
+  int32_t rs, ks, nrows, K, gtot, kb0, R, nkb, ntiles, gt_last, row0;
   int8_t space, want_max, want_split, pad_;
 } tj_oz_job;
-typedef struct tj_oz_seg { int64_t a_base, b_base; int32_t a_ngr, b_ngr, a_gr0, b_gr0, ngr, pad_; } tj_oz_seg;
-typedef struct tj_oz_fam { int32_t seg_begin, seg_end; int64_t rs_idx, cs_idx; int32_t nkb, ngr; } tj_oz_fam;
+typedef struct tj_oz_seg { int64_t a_base, b_base; int32_t a_nkb, b_nkb, a_kb0, b_kb0, nkb, pad_; } tj_oz_seg;
+typedef struct tj_oz_fam { int32_t seg_begin, seg_end; int64_t rs_idx, cs_idx; int32_t nkb, pad_; } tj_oz_fam;
 typedef struct tj_oz_item {
   int32_t kind, cell, row0, col0, M, N, mrows, ncols, fam_begin, fam_end, pad1_, init;
   int64_t pi_idx;

@@ -63,46 +63,46 @@ class _Machine:
             j = jobs[i]
             if not j.want_split:
                 continue
-            ngr = -(-j.K // 16)
+            nkb = -(-j.K // 32)
             rows = j.gtot * 8
-            X = np.zeros((rows, ngr * 16))
+            X = np.zeros((rows, nkb * 32))
             X[:j.nrows, :j.K] = self._matrix(j)
             sc = np.zeros(rows)
             sc[:j.nrows] = _pow2_of(self.scales[j.scale_idx:j.scale_idx + j.nrows])
             with np.errstate(divide="ignore", invalid="ignore"):
                 t = np.where(sc[:, None] > 0, X * np.where(sc > 0, 1.0 / np.where(sc > 0, sc, 1.0), 0.0)[:, None], 0.0)
-            dig = np.zeros((S, rows, ngr * 16), dtype=np.int64)
+            dig = np.zeros((S, rows, nkb * 32), dtype=np.int64)
             for q in range(S):
                 t = t * 128.0
                 a = np.trunc(t)
                 t = t - a
                 dig[q] = a.astype(np.int64)
             assert np.all(np.abs(dig) <= 127)
-            # split row sr -> tile, group; [tile][granule][p][g][r8][16]
+            # split row sr -> tile, group; [tile][kb][p][g][c][r8][16]
             for jr in range(0, rows, 8):
                 sr = j.row0 + jr
                 tt, rl = divmod(sr, j.R)
                 gt = j.R // 8 if tt < j.ntiles - 1 else j.gt_last
                 g = rl // 8
                 assert g < gt
-                tile = j.dst + tt * j.ngr * S * (j.R // 8) * 128
-                for gr in range(ngr):
+                tile = j.dst + tt * j.nkb * S * (j.R // 8) * 256
+                for kb in range(nkb):
                     for q in range(S):
-                        o = tile + ((j.gr0 + gr) * S + q) * gt * 128 + g * 128
-                        assert 0 <= o and o + 128 <= len(self.pack)
-                        blk = dig[q, jr:jr + 8, gr * 16:(gr + 1) * 16]
-                        self.pack[o:o + 128] = blk.reshape(-1).astype(np.int8)
+                        o = tile + ((j.kb0 + kb) * S + q) * gt * 256 + g * 256
+                        assert 0 <= o and o + 256 <= len(self.pack)
+                        blk = dig[q, jr:jr + 8, kb * 32:(kb + 1) * 32].reshape(8, 2, 16).transpose(1, 0, 2)
+                        self.pack[o:o + 256] = blk.reshape(-1).astype(np.int8)
 
-    def tile_digits(self, base, ngr_tot, tile_groups, t, g, gr0, ngr):
-        """Slices (S, 8*g, 16*ngr) of tile t (g groups; full tiles have tile_groups) of a split."""
+    def tile_digits(self, base, nkb_tot, tile_groups, t, g, kb0, nkb):
+        """Slices (S, 8*g, 32*nkb) of tile t (g groups; full tiles have tile_groups) of a split."""
         S = self.S
-        out = np.zeros((S, g * 8, ngr * 16), dtype=np.int64)
-        tb = base + t * ngr_tot * S * tile_groups * 128
-        for gr in range(ngr):
-            o = tb + (gr0 + gr) * S * g * 128
-            assert 0 <= o and o + S * g * 128 <= len(self.pack)
-            b = self.pack[o:o + S * g * 128].astype(np.int64).reshape(S, g, 8, 16)
-            out[:, :, gr * 16:(gr + 1) * 16] = b.reshape(S, g * 8, 16)
+        out = np.zeros((S, g * 8, nkb * 32), dtype=np.int64)
+        tb = base + t * nkb_tot * S * tile_groups * 256
+        for kb in range(nkb):
+            o = tb + (kb0 + kb) * S * g * 256
+            assert 0 <= o and o + S * g * 256 <= len(self.pack)
+            b = self.pack[o:o + S * g * 256].astype(np.int64).reshape(S, g, 2, 8, 16)
+            out[:, :, kb * 32:(kb + 1) * 32] = b.transpose(0, 1, 3, 2, 4).reshape(S, g * 8, 32)
         return out
 
     def accum(self, A, B):
@@ -129,8 +129,8 @@ class _Machine:
             ga, gb = -(-it.mrows // 8), it.N // 8
 
             def operands(sg):
-                A = self.tile_digits(sg.a_base, sg.a_ngr, 16, ta, ga, sg.a_gr0, sg.ngr)
-                B = self.tile_digits(sg.b_base, sg.b_ngr, self.BN // 8, tb, gb, sg.b_gr0, sg.ngr)
+                A = self.tile_digits(sg.a_base, sg.a_nkb, 16, ta, ga, sg.a_kb0, sg.nkb)
+                B = self.tile_digits(sg.b_base, sg.b_nkb, self.BN // 8, tb, gb, sg.b_kb0, sg.nkb)
                 return A, B
 
             c = oz["cells"][it.cell]
@@ -146,8 +146,7 @@ class _Machine:
                 As, Bs = zip(*[operands(oz["segs"][sgi]) for sgi in range(fm.seg_begin, fm.seg_end)])
                 A = np.concatenate(As, axis=2)[:, :it.mrows]
                 B = np.concatenate(Bs, axis=2)[:, :it.ncols]
-                # the family's granules in pairs are its k-blocks; the device
-                # accumulates at most kb_piece k-blocks in int32, then adds the pieces
+                # the device accumulates at most kb_piece k-blocks in int32, then adds the pieces
                 kp = 32 * ((2 ** 31 - 1) // (32 * self.S * 127 * 127))
                 acc = sum(self.accum(A[:, :, k0:k0 + kp], B[:, :, k0:k0 + kp]) for k0 in range(0, A.shape[2], kp))
                 rs = _pow2_of(self.scales[fm.rs_idx + rows])
