@@ -36,7 +36,7 @@ namespace cg = cooperative_groups;
 
 namespace tjb {
 
-constexpr int EIG_THREADS = 1024;
+constexpr int EIG_THREADS = 512;
 constexpr int EIG_MAX_N = 4096;
 constexpr double EIG_EPS = 2.220446049250313e-16;        // 2^-52
 constexpr double EIG_SAFMIN = 2.2250738585072014e-308;   // smallest normal FP64
@@ -264,7 +264,8 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
       }
       mine[ii] = acc;
     }
-    __threadfence();
+    // the cluster barrier's release / acquire order the column writes
+    // (global memory) and the parts (shared memory) for the other CTAs
     cl.sync();
     if (owner)
       for (int i = k1 + tid; i < n; i += nt) colk[i] = rv(i);
@@ -393,7 +394,12 @@ __global__ void inverse_iter_kernel(const double *dall, const double *eall, cons
   const double lam = evals[eoff[s] + k];
   const double pert = fmax(EIG_EPS * info[4 * s + 2], 1e-290);
   const size_t st = (size_t)njobs, pl = (size_t)nmax * st;
-  double *U = work, *DU = work + pl, *DU2 = work + 2 * pl, *DL = work + 3 * pl, *X = work + 4 * pl;
+  // disjoint regions: the loads of the factors may run ahead of the stores to X
+  double *__restrict__ U = work;
+  double *__restrict__ DU = work + pl;
+  double *__restrict__ DU2 = work + 2 * pl;
+  double *__restrict__ DL = work + 3 * pl;
+  double *__restrict__ X = work + 4 * pl;
 #define AT(arr, i) arr[(size_t)(i) * st + j]
   // LU = P (T - lam I): row i of U is (U_i, DU_i, DU2_i) at columns i, i+1, i+2
   double di = d[0] - lam, dui = n > 1 ? e[0] : 0.0;
