@@ -582,8 +582,11 @@ __device__ void ortho_one(int blk, const int *grp, const int *dims, const int64_
 // each CTA forms its part of the dot products with the accepted vectors, the
 // parts meet through distributed shared memory, every CTA sums them in rank
 // order (so every CTA holds the same coefficients and takes the same
-// decisions), subtracts on its own rows, and the squared norm is summed the
-// same way.  Each exchange uses the buffer of its parity and ends with one
+// decisions), subtracts on its own rows; the vector's squared norm travels
+// with the dots, so that when the projection removes less than half of it
+// (the common case: inverse iteration leaves the vectors nearly orthogonal)
+// the new norm needs no second exchange; otherwise it is summed the same way
+// after the subtraction.  Each exchange uses the buffer of its parity and ends with one
 // cluster barrier; a buffer is written again only two exchanges later, after
 // every CTA has passed the barrier that follows its reads.  A CTA reads and
 // writes only its own rows of the vectors in global memory.
@@ -631,9 +634,13 @@ __device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *
       }
       ok = true;
       for (int pass = 0; pass < 2; ++pass) {
+        // one exchange carries the dots with the accepted vectors and the
+        // vector's own squared norm (slot t); when the projection removes
+        // less than half of the squared norm, the new norm is yy - sum h^2
+        // (accurate to rounding there), and no second exchange is needed
         double *hpw = hp + (xch & 1) * cnt;
-        for (int q = warp; q < t; q += nw) {
-          const double *z = vec(q) + r0;
+        for (int q = warp; q <= t; q += nw) {
+          const double *z = q < t ? vec(q) + r0 : ys;
           double acc = 0.0;
           for (int i = lane; i < nr; i += 32) acc += z[i] * ys[i];
           for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -641,12 +648,16 @@ __device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *
         }
         cl.sync();
         ++xch;
-        for (int q = tid; q < t; q += nt) {
+        double hh = 0.0;
+        for (int q = tid; q <= t; q += nt) {
           double tot = 0.0;
           for (int c = 0; c < CL; ++c) tot += cl.map_shared_rank(hpw, c)[q];
           h[q] = tot;
+          if (q < t) hh += tot * tot;
         }
-        __syncthreads();
+        const double s2 = block_sum1(hh, red, half);   // also the barrier after h
+        const double yy = h[t], rest = yy - s2;        // the same values in every CTA
+        const bool fast = rest >= 0.5 * yy && rest > 0.0;
         double ss = 0.0;
         for (int i = tid; i < nr; i += nt) {
           double acc = ys[i];
@@ -654,15 +665,15 @@ __device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *
           ys[i] = acc;
           ss += acc * acc;
         }
-        const double nrm = sqrt(cluster_sum(block_sum1(ss, red, half)));   // the same value in every CTA
+        const double nrm = fast ? sqrt(rest) : sqrt(cluster_sum(block_sum1(ss, red, half)) / yy);
         if (pass == 0 && !(nrm >= 1e-3)) {
           ok = false;
           break;
         }
-        const double inv = 1.0 / nrm;
+        const double inv = fast ? 1.0 / nrm : 1.0 / (nrm * sqrt(yy));
         for (int i = tid; i < nr; i += nt) ys[i] *= inv;
         __syncthreads();
-        if (nrm > 0.7071067811865476) break;
+        if (nrm > 0.7071067811865476) break;   // relative to the norm the vector entered with
       }
       if (!ok && attempt == 0 && !(evals[eoff[s] + job_k[jt]] - lam_min <= cluster)) break;
     }
