@@ -36,8 +36,9 @@ namespace cg = cooperative_groups;
 
 namespace tjb {
 
-constexpr int EIG_THREADS = 512;
+constexpr int EIG_THREADS = 1024;
 constexpr int EIG_MAX_N = 4096;
+static_assert(4 * EIG_THREADS >= EIG_MAX_N, "the cluster reduction holds up to four rows of a column per thread");
 constexpr double EIG_EPS = 2.220446049250313e-16;        // 2^-52
 constexpr double EIG_SAFMIN = 2.2250738585072014e-308;   // smallest normal FP64
 constexpr int ORTH_THREADS = 512;
@@ -134,9 +135,25 @@ __device__ void tridiag_one(int s, double *Aall, const int64_t *off, const int *
         const double vpi = pending ? vp[i] : 0.0, wpi = pending ? wp[i] : 0.0;
         double acc = 0.0;
         double *a = A + (int64_t)(k1 + g) * n + i;
+        const int64_t st = (int64_t)G * n;
         if (pending) {
-#pragma unroll 4
-          for (int jj = g; jj < m; jj += G, a += (int64_t)G * n) {
+          // eight loads issued before the eight stores: a store through a
+          // may alias the next load, so loads and stores interleaved one
+          // column at a time would wait out a full L2 round trip per column
+          int jj = g;
+          for (; jj + 7 * G < m; jj += 8 * G, a += 8 * st) {
+            double x[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) x[u] = a[u * st];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              const int j = k1 + jj + u * G;
+              x[u] -= vpi * wp[j] + wpi * vp[j];
+              a[u * st] = x[u];
+              acc += x[u] * v[j];
+            }
+          }
+          for (; jj < m; jj += G, a += st) {
             const int j = k1 + jj;
             const double x = *a - (vpi * wp[j] + wpi * vp[j]);
             *a = x;
@@ -196,14 +213,17 @@ __device__ __forceinline__ double block_sum1(double x, double *red, int &half) {
 // same arithmetic in the same order, so the same reflector everywhere, and
 // every thread derives beta, tau and the scale from the same sum); CTA c
 // owns the trailing columns j = c (mod CL), applies the pending rank-2 update
-// to them and forms its part of p = A v, one thread per row (the reflector
-// is scaled where it is read); the parts meet in shared memory across the
-// cluster (distributed shared memory, two buffers alternating by step) and
-// every CTA sums them in rank order.  Per step: one cluster barrier, which
-// orders the owners' column writes (global memory) and the parts before they
-// are read, and three CTA barriers.  The owner of column k stores its
-// reflector there only after the cluster barrier, when no CTA reads the
-// column any more.
+// to them and forms its part of p = A v, one thread per row, or, when the
+// CTA's threads outnumber the rows, one per row in each of G groups that
+// split the owned columns (the reflector is scaled where it is read); the
+// parts meet in shared memory across the cluster (distributed shared memory,
+// two buffers alternating by step) and every CTA sums them in rank order.
+// Per step: one cluster barrier, which orders the owners' column writes
+// (global memory) and the parts before they are read, and three CTA barriers
+// (four with column groups).  Column k + 1, complete at that barrier, is
+// loaded into registers there for the next step.  The owner of column k
+// stores its reflector there only after the cluster barrier, when no CTA
+// reads the column any more.
 template <int CL>
 __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aall, const int64_t *off,
                              const int *dims, const int64_t *eoff, double *dall, double *eall, double *tauall,
@@ -213,19 +233,27 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
   double *d = dall + eoff[s], *e = eall + eoff[s], *tau = tauall + eoff[s];
   // vp, wp, v: n each; cp: the cluster parts, 2 x n (read by the other CTAs
   // until the next barrier); pp: the summed p = tau A v, n
-  double *vp = sm, *wp = vp + n, *v = wp + n, *cp = v + n, *pp = cp + 2 * n;
+  // gp: the column groups' parts of A v when a CTA's threads outnumber the
+  // trailing rows (G groups, G * m <= nt entries)
+  double *vp = sm, *wp = vp + n, *v = wp + n, *cp = v + n, *pp = cp + 2 * n, *gp = pp + n;
   int half = 0;
   bool pending = false;
+  // rows k + tid + c nt of column k, loaded during step k - 1 (n <= 4 nt)
+  double nx[4];
   for (int k = 0; k + 1 < n; ++k) {
     const int k1 = k + 1, m = n - k1;
     const bool owner = (k % CL) == rank;
     double *colk = A + (int64_t)k * n;
     double ss = 0.0;
-    for (int i = k + tid; i < n; i += nt) {
-      double a = colk[i];
-      if (pending) a -= vp[i] * wp[k] + wp[i] * vp[k];
-      v[i] = a;
-      if (i > k1) ss += a * a;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int i = k + tid + c * nt;
+      if (i < n) {
+        double a = k == 0 ? colk[i] : nx[c];
+        if (pending) a -= vp[i] * wp[k] + wp[i] * vp[k];
+        v[i] = a;
+        if (i > k1) ss += a * a;
+      }
     }
     const double sigma2 = block_sum1(ss, red2, half);   // also the barrier after v
     const double alpha = v[k1];
@@ -243,30 +271,75 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
     }
     // the scaled reflector: 1 at k1, v[i] * scl below
     auto rv = [&](int i) { return i == k1 ? 1.0 : v[i] * scl; };
-    // owned trailing columns j0, j0 + CL, ...; one thread per row
+    // owned trailing columns j0, j0 + CL, ... (mloc of them): rows r, r + R,
+    // ... by the R threads of each of G column groups, group g taking the
+    // owned columns q = g, g + G, ...
     const int j0 = k1 + ((rank - k1) % CL + CL) % CL;
     const int mloc = j0 < n ? (n - 1 - j0) / CL + 1 : 0;
+    const int R = min((m + 31) & ~31, nt), G = nt / R;
+    const int g = tid / R, r = tid - g * R;
     double *mine = cp + (k & 1) * n;
-    for (int ii = tid; ii < m; ii += nt) {
-      const int i = k1 + ii;
-      const double vpi = pending ? vp[i] : 0.0, wpi = pending ? wp[i] : 0.0;
-      double acc = 0.0;
-      double *a = A + (int64_t)j0 * n + i;
-#pragma unroll 4
-      for (int q = 0; q < mloc; ++q, a += (int64_t)CL * n) {
-        const int j = j0 + q * CL;
-        double x = *a;
+    if (g < G) {
+      const int64_t st = (int64_t)G * CL * n;
+      for (int ii = r; ii < m; ii += R) {
+        const int i = k1 + ii;
+        const double vpi = pending ? vp[i] : 0.0, wpi = pending ? wp[i] : 0.0;
+        double acc = 0.0;
+        double *a = A + (int64_t)(j0 + g * CL) * n + i;
+        int q = g;
         if (pending) {
-          x -= vpi * wp[j] + wpi * vp[j];
-          *a = x;
+          // four loads issued before the four stores (a store through a
+          // may alias the next load: interleaved, every column would wait
+          // out a full L2 round trip; eight would not fit the 64 registers
+          // of a 1024-thread CTA)
+          for (; q + 3 * G < mloc; q += 4 * G, a += 4 * st) {
+            double x[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) x[u] = a[u * st];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int j = j0 + (q + u * G) * CL;
+              x[u] -= vpi * wp[j] + wpi * vp[j];
+              a[u * st] = x[u];
+              acc += x[u] * rv(j);
+            }
+          }
+          for (; q < mloc; q += G, a += st) {
+            const int j = j0 + q * CL;
+            const double x = *a - (vpi * wp[j] + wpi * vp[j]);
+            *a = x;
+            acc += x * rv(j);
+          }
+        } else {
+          for (; q < mloc; q += G, a += st) acc += *a * rv(j0 + q * CL);
         }
-        acc += x * rv(j);
+        if (G == 1)
+          mine[ii] = acc;
+        else
+          gp[g * m + ii] = acc;
       }
-      mine[ii] = acc;
+    }
+    if (G > 1) {
+      __syncthreads();
+      for (int ii = tid; ii < m; ii += nt) {
+        double acc = 0.0;
+        for (int c = 0; c < G; ++c) acc += gp[c * m + ii];
+        mine[ii] = acc;
+      }
     }
     // the cluster barrier's release / acquire order the column writes
     // (global memory) and the parts (shared memory) for the other CTAs
     cl.sync();
+    // column k + 1 is complete now (its owner stored it before the barrier):
+    // its loads for the next step overlap the sums below
+    if (k + 2 < n) {
+      const double *c1 = A + (int64_t)k1 * n;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int i = k1 + tid + c * nt;
+        nx[c] = i < n ? c1[i] : 0.0;
+      }
+    }
     if (owner)
       for (int i = k1 + tid; i < n; i += nt) colk[i] = rv(i);
     double pv = 0.0;
@@ -499,6 +572,76 @@ __global__ void inverse_iter_kernel(const double *dall, const double *eall, cons
 #undef AT
 }
 
+// Dots of y (rows 0..nr-1; shared or global memory) with the vectors zq(q),
+// q = 0..nq-1, into out[q]: each warp takes eight vectors at a time so that
+// their loads are in flight together (one vector at a time, every vector
+// would wait out an L2 round trip: the store of a sum may alias the next
+// vector's loads).  Each dot is summed as lane-strided parts and a shuffle
+// tree, the same for every q.
+template <class ZQ>
+__device__ __forceinline__ void warp_dots8(ZQ zq, int nq, const double *y, int nr, double *out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int q0 = 8 * warp; q0 < nq; q0 += 8 * nw) {
+    double acc[8];
+    const double *z[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      acc[u] = 0.0;
+      z[u] = zq(min(q0 + u, nq - 1));   // past nq: a repeat, discarded
+    }
+    for (int i = lane; i < nr; i += 32) {
+      const double yi = y[i];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc[u] += z[u][i] * yi;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      double a = acc[u];
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+      if (lane == 0 && q0 + u < nq) out[q0 + u] = a;
+    }
+  }
+}
+
+// y <- y - sum_q h[q] zq(q) over rows 0..nr-1, returning the thread's part
+// of the new squared norm.  When the block's threads outnumber the rows, G
+// groups of R threads split the vectors (group g takes q = g, g + G, ...) and
+// their parts (gp: G * nr <= blockDim.x entries) are summed in group order;
+// otherwise one thread per row runs over all of them.  Ends with the block's
+// writes to y complete only for the writing thread (the caller's barrier
+// follows).
+template <class ZQ>
+__device__ __forceinline__ double project_off(ZQ zq, int t, const double *h, double *y, int nr, double *gp) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int R = min(max((nr + 31) & ~31, 32), nt), G = nt / R;
+  double ss = 0.0;
+  if (G == 1) {
+    for (int i = tid; i < nr; i += nt) {
+      double acc = y[i];
+      for (int q = 0; q < t; ++q) acc -= h[q] * zq(q)[i];
+      y[i] = acc;
+      ss += acc * acc;
+    }
+    return ss;
+  }
+  const int g = tid / R, r = tid - g * R;
+  if (g < G && r < nr) {
+    double acc = 0.0;
+#pragma unroll 4
+    for (int q = g; q < t; q += G) acc += h[q] * zq(q)[r];
+    gp[g * nr + r] = acc;
+  }
+  __syncthreads();
+  for (int i = tid; i < nr; i += nt) {
+    double acc = 0.0;
+    for (int c = 0; c < G; ++c) acc += gp[c * nr + i];
+    const double yv = y[i] - acc;
+    y[i] = yv;
+    ss += yv * yv;
+  }
+  return ss;
+}
+
 // One kept block (grp = {sector, first job, count}): classical Gram-Schmidt
 // on its vectors in descending eigenvalue order, so that the dominant states
 // are the least changed; inverse iteration leaves vectors of close
@@ -526,8 +669,10 @@ __device__ void ortho_one(int blk, const int *grp, const int *dims, const int64_
                           const double *info, const int *job_k, double *Y, int ldy, int *status, double *h,
                           double *red) {
   const int s = grp[4 * blk], j0 = grp[4 * blk + 1], cnt = grp[4 * blk + 2];
-  const int n = dims[s], tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int n = dims[s], tid = threadIdx.x;
   const double lam_min = evals[eoff[s]], cluster = 1e4 * EIG_EPS * info[4 * s + 2];
+  double *gp = h + cnt;   // project_off's group parts
+  auto vec = [&](int q) -> const double * { return Y + (size_t)(j0 + cnt - 1 - q) * ldy; };
   for (int t = 1; t < cnt; ++t) {
     const int jt = j0 + cnt - 1 - t;
     double *y = Y + (size_t)jt * ldy;
@@ -546,21 +691,9 @@ __device__ void ortho_one(int blk, const int *grp, const int *dims, const int64_
       }
       ok = true;
       for (int pass = 0; pass < 2; ++pass) {
-        for (int q = warp; q < t; q += nw) {
-          const double *z = Y + (size_t)(j0 + cnt - 1 - q) * ldy;
-          double acc = 0.0;
-          for (int i = lane; i < n; i += 32) acc += z[i] * y[i];
-          for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-          if (lane == 0) h[q] = acc;
-        }
+        warp_dots8(vec, t, y, n, h);
         __syncthreads();
-        double ss = 0.0;
-        for (int i = tid; i < n; i += blockDim.x) {
-          double acc = y[i];
-          for (int q = 0; q < t; ++q) acc -= h[q] * Y[(size_t)(j0 + cnt - 1 - q) * ldy + i];
-          y[i] = acc;
-          ss += acc * acc;
-        }
+        const double ss = project_off(vec, t, h, y, n, gp);
         const double nrm = sqrt(block_sum(ss, red));   // the same value in every thread
         if (pass == 0 && !(nrm >= 1e-3)) {
           ok = false;
@@ -595,12 +728,13 @@ __device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *
                            const int64_t *eoff, const double *evals, const double *info, const int *job_k, double *Y,
                            int ldy, int *status, double *sm, double *red) {
   const int s = grp[4 * blk], j0 = grp[4 * blk + 1], cnt = grp[4 * blk + 2];
-  const int n = dims[s], tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  const int n = dims[s], tid = threadIdx.x, nt = blockDim.x;
   const double lam_min = evals[eoff[s]], cluster = 1e4 * EIG_EPS * info[4 * s + 2];
   const int per = (n + CL - 1) / CL, r0 = min(n, rank * per), r1 = min(n, r0 + per), nr = r1 - r0;
   // hp: parts of the dots (2 x cnt), h: the dots (cnt), ys: own rows of the
-  // vector (per), sl: parts of the squared norm (2)
-  double *hp = sm, *h = hp + 2 * cnt, *ys = h + cnt, *sl = ys + per;
+  // vector (per), sl: parts of the squared norm (2), gp: project_off's group
+  // parts (nt)
+  double *hp = sm, *h = hp + 2 * cnt, *ys = h + cnt, *sl = ys + per, *gp = sl + 2;
   unsigned xch = 0;   // exchanges so far (buffer parity)
   int half = 0;       // block_sum1's alternating half of red
   auto cluster_sum = [&](double x) -> double {   // x: the CTA's value, the same in all its threads
@@ -639,13 +773,7 @@ __device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *
         // less than half of the squared norm, the new norm is yy - sum h^2
         // (accurate to rounding there), and no second exchange is needed
         double *hpw = hp + (xch & 1) * cnt;
-        for (int q = warp; q <= t; q += nw) {
-          const double *z = q < t ? vec(q) + r0 : ys;
-          double acc = 0.0;
-          for (int i = lane; i < nr; i += 32) acc += z[i] * ys[i];
-          for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-          if (lane == 0) hpw[q] = acc;
-        }
+        warp_dots8([&](int q) -> const double * { return q < t ? vec(q) + r0 : ys; }, t + 1, ys, nr, hpw);
         cl.sync();
         ++xch;
         double hh = 0.0;
@@ -658,13 +786,7 @@ __device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *
         const double s2 = block_sum1(hh, red, half);   // also the barrier after h
         const double yy = h[t], rest = yy - s2;        // the same values in every CTA
         const bool fast = rest >= 0.5 * yy && rest > 0.0;
-        double ss = 0.0;
-        for (int i = tid; i < nr; i += nt) {
-          double acc = ys[i];
-          for (int q = 0; q < t; ++q) acc -= h[q] * vec(q)[r0 + i];
-          ys[i] = acc;
-          ss += acc * acc;
-        }
+        const double ss = project_off([&](int q) -> const double * { return vec(q) + r0; }, t, h, ys, nr, gp);
         const double nrm = fast ? sqrt(rest) : sqrt(cluster_sum(block_sum1(ss, red, half)) / yy);
         if (pass == 0 && !(nrm >= 1e-3)) {
           ok = false;
@@ -1117,7 +1239,7 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       const size_t q_slab = q; q += al256(slab.size() * 4);
       // clusters of the orthonormalisation: one per large kept block (cnt^2 n
       // above 3e7), then the other blocks ocl at a time, largest first
-      const size_t osm = sizeof(double) * (3 * (size_t)maxn + (maxn + 7) / 8 + 8);
+      const size_t osm = sizeof(double) * (3 * (size_t)maxn + (maxn + 7) / 8 + 8 + ORTH_THREADS);
       const int ocl = cluster_size(orthonormalize_kernel<16>, ORTH_THREADS, osm);
       std::vector<int> oblk, obig;
       {
