@@ -463,7 +463,8 @@ __global__ void inverse_iter_kernel(const double *dall, const double *eall, cons
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= njobs) return;
   const int s = job_sec[j], k = job_k[j], n = dims[s];
-  const double *d = dall + eoff[s], *e = eall + eoff[s];
+  const double *__restrict__ d = dall + eoff[s];
+  const double *__restrict__ e = eall + eoff[s];
   const double lam = evals[eoff[s] + k];
   const double pert = fmax(EIG_EPS * info[4 * s + 2], 1e-290);
   const size_t st = (size_t)njobs, pl = (size_t)nmax * st;
@@ -506,16 +507,41 @@ __global__ void inverse_iter_kernel(const double *dall, const double *eall, cons
   AT(DU2, n - 1) = 0.0;
   if (n >= 2) AT(DU2, n - 2) = 0.0;
   for (int i = 0; i < n; ++i) AT(X, i) = start_entry(s, k, i);
+  // Each sweep solves with X times `scale` (the previous sweep's rescale to
+  // a largest entry of 1, applied where X is read) and keeps the largest
+  // entry of its result as it goes.  Both passes read eight rows ahead of
+  // their stores: X[i] is stored through the same pointer as the next row's
+  // load, and a load the compiler must keep behind that store would wait out
+  // an L2 round trip per row.
   bool bad = false;
+  double scale = 1.0;
   for (int sweep = 0; sweep < 3; ++sweep) {
-    // forward: P and L.  The running entry stays in a register and the loads
-    // do not depend on it, so the unrolled loop has them in flight ahead of
-    // the arithmetic (the factors are read from L2 at the latency of a load)
-    double cur = AT(X, 0);
-#pragma unroll 8
-    for (int i = 0; i + 1 < n; ++i) {
-      const double l = AT(DL, i), nxt = AT(X, i + 1);
-      if (piv[(size_t)i * st + j]) {   // rows i and i+1 exchanged
+    // forward: P and L
+    double cur = AT(X, 0) * scale;
+    int i = 0;
+    for (; i + 8 < n; i += 8) {   // rows i..i+7; their solves read X[i+1..i+8] as they were
+      double l[8], nx[8];
+      unsigned char pv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        l[u] = AT(DL, i + u);
+        nx[u] = AT(X, i + u + 1) * scale;
+        pv[u] = piv[(size_t)(i + u) * st + j];
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        if (pv[u]) {   // rows i+u and i+u+1 exchanged
+          AT(X, i + u) = nx[u];
+          cur = cur - l[u] * nx[u];
+        } else {
+          AT(X, i + u) = cur;
+          cur = nx[u] - l[u] * cur;
+        }
+      }
+    }
+    for (; i + 1 < n; ++i) {
+      const double l = AT(DL, i), nxt = AT(X, i + 1) * scale;
+      if (piv[(size_t)i * st + j]) {
         AT(X, i) = nxt;
         cur = cur - l * nxt;
       } else {
@@ -525,32 +551,49 @@ __global__ void inverse_iter_kernel(const double *dall, const double *eall, cons
     }
     AT(X, n - 1) = cur;
     // backward: U, with a rescale of the whole vector if it nears overflow
-    double x1 = 0.0, x2 = 0.0;   // x_{i+1}, x_{i+2}
-#pragma unroll 8
-    for (int i = n - 1; i >= 0; --i) {
-      double xi = (AT(X, i) - AT(DU, i) * x1 - AT(DU2, i) * x2) / AT(U, i);
+    // (the rows loaded but not yet solved are rescaled in registers)
+    double x1 = 0.0, x2 = 0.0, mx = 0.0;   // x_{i+1}, x_{i+2}, the largest |x| so far
+    auto row = [&](double xv, double du, double du2, double uu, int at, double *ahead, int nahead) {
+      double xi = (xv - du * x1 - du2 * x2) / uu;
       if (fabs(xi) > 1e250) {
         const double f = 1e-250;
         for (int q = 0; q < n; ++q) AT(X, q) *= f;
+        for (int w = 0; w < nahead; ++w) ahead[w] *= f;
         xi *= f;
         x1 *= f;
         x2 *= f;
+        mx *= f;
       }
-      AT(X, i) = xi;
+      AT(X, at) = xi;
+      mx = fmax(mx, fabs(xi));
       x2 = x1;
       x1 = xi;
+    };
+    i = n - 1;
+    for (; i >= 7; i -= 8) {   // rows i, i-1, ..., i-7
+      double xv[8], du[8], du2[8], uu[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        xv[u] = AT(X, i - u);
+        du[u] = AT(DU, i - u);
+        du2[u] = AT(DU2, i - u);
+        uu[u] = AT(U, i - u);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) row(xv[u], du[u], du2[u], uu[u], i - u, xv + u + 1, 7 - u);
     }
-    double mx = 0.0;
-    for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(AT(X, i)));
+    for (; i >= 0; --i) row(AT(X, i), AT(DU, i), AT(DU2, i), AT(U, i), i, nullptr, 0);
     if (!(mx > 0.0) || !isfinite(mx)) {
       bad = true;
       break;
     }
-    const double inv = 1.0 / mx;
-    for (int i = 0; i < n; ++i) AT(X, i) *= inv;
+    scale = 1.0 / mx;
   }
   double nrm = 0.0;
-  for (int i = 0; i < n; ++i) nrm += AT(X, i) * AT(X, i);
+  for (int i = 0; i < n; ++i) {
+    const double x = AT(X, i) * scale;
+    nrm += x * x;
+  }
   if (bad || !(nrm > 0.0) || !isfinite(nrm)) {
     atomicOr(status, 1);
     // the first failing vector: sector, eigenvalue index, lam, pivot floor, n
@@ -564,10 +607,11 @@ __global__ void inverse_iter_kernel(const double *dall, const double *eall, cons
       diag[5] = nrm;
     }
     nrm = 1.0;
+    scale = 1.0;
   }
   const double inv = 1.0 / sqrt(nrm);
   double *y = Y + (size_t)j * ldy;
-  for (int i = 0; i < n; ++i) y[i] = AT(X, i) * inv;
+  for (int i = 0; i < n; ++i) y[i] = AT(X, i) * scale * inv;
   for (int i = n; i < nmax; ++i) y[i] = 0.0;
 #undef AT
 }
@@ -897,6 +941,10 @@ struct TruncCache {
   tj_trunc_result res{};
   std::vector<tj_block_sub> sub;
   std::vector<double> mats;
+  // the device copy of mats: valid while ctx has computed no other truncation
+  const tj_ctx *ctx = nullptr;
+  uint64_t seq = 0;
+  const double *dev = nullptr;
 };
 thread_local TruncCache g_tc;
 
@@ -972,6 +1020,9 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     CKT(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     const auto wall0 = std::chrono::steady_clock::now();
+    tc.ctx = ctx;
+    tc.seq = ++ctx->trunc_seq;
+    tc.dev = nullptr;
     CKT(cudaEventRecord(ctx->tev[0], st));
     // psi on the device and its norm
     int rc;
@@ -1271,6 +1322,7 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       CKT(cudaMemcpyAsync(ab + q_oblk, oblk.data(), oblk.size() * 4, cudaMemcpyHostToDevice, st));
       CKT(cudaMemcpyAsync(ab + q_obig, obig.data(), obig.size() * 4, cudaMemcpyHostToDevice, st));
       double *Y = (double *)(cb + p_y), *d_out = (double *)(ab + q_out);
+      tc.dev = d_out;
       for (int b = 0; b < ngrp; ++b) max_kept = std::max(max_kept, grp[4 * b + 2]);
       select_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - sel0).count();
       CKT(cudaEventRecord(ctx->tev[4], st));
@@ -1360,6 +1412,15 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
   if (usub && udata) {
     std::memcpy(usub, tc.sub.data(), sizeof(tj_block_sub) * tc.sub.size());
     std::memcpy(udata, tc.mats.data(), sizeof(double) * tc.mats.size());
+    // the renormalisation of this step and the prediction of the next read
+    // the operator again: with residency on, its device copy is kept
+    if (tc.dev && tc.ctx == ctx && tc.seq == ctx->trunc_seq && !tc.mats.empty()) {
+      CKT(cudaSetDevice(ctx->device));
+      // (the copy runs on the context's stream, ahead of anything that
+      // rewrites trA)
+      const int rc = res_keep(ctx, udata, (int64_t)tc.mats.size(), tc.dev, ctx->stream);
+      if (rc) return rc;
+    }
   }
   return TJ_OK;
 }
