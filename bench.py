@@ -352,6 +352,9 @@ def sweep_leg(ctx64, ctxoz, name: str, prep: str, seed: int):
                                   "upload": sum(st.upload_ms for st in lz),
                                   "wall": 1e3 * sum(w for name, _, w, _ in trace if name == "lanczos"),
                                   "iterations": sum(st.lanczos_ms for st in lz)}
+        # the prediction's library call; the rest of `pred` is the driver's
+        # bases of the new superblock
+        out[tag]["wave_trans_ms"] = 1e3 * sum(w for name, _, w, _ in trace if name == "wave_trans")
         return recs
 
     # one untimed sweep from the same state first: a running DMRG reuses the

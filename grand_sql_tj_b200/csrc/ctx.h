@@ -105,6 +105,7 @@ struct tj_ctx {
   cudaEvent_t sev[2] = {nullptr, nullptr};
   int64_t res_hits = 0;       // uploads served from kept copies since creation
   double res_hit_bytes = 0;
+  uint64_t trunc_seq = 0;     // truncations computed (the device operator of the last one stays in trA)
   std::shared_ptr<tj_renorm_state> renorm;
   std::shared_ptr<tj_meas_state> meas;
   // split-precision H*psi

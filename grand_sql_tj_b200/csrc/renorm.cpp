@@ -786,7 +786,7 @@ extern "C" int tj_get_hamiltonian(tj_ctx *ctx, const tj_lattice *lat, int side, 
   {
     int64_t lo = LLONG_MAX;
     for (int k = 0; k < trun->num; ++k) lo = std::min(lo, (int64_t)trun->sub[k].off);
-    CKR(cudaMemcpyAsync(ctx->rnTrun.d(), trun->data + lo, sizeof(double) * P.psi_len, cudaMemcpyHostToDevice, st));
+    CKR(upload(ctx, ctx->rnTrun.d(), trun->data + lo, P.psi_len, st));
   }
   std::vector<char> tab;
   auto add = [&](const void *p, size_t n) {

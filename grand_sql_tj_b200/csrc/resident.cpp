@@ -9,8 +9,10 @@
 // (tj_set_residency), tj_get_hamiltonian keeps the device copy of the block
 // it has just written, keyed by the caller's array (and tj_lanczos_memo_new
 // and tj_wave_trans their wavefunctions, which the next truncation,
-// prediction and Lanczos read), and every later upload whose source lies
-// inside a kept array is a device-to-device copy instead.
+// prediction and Lanczos read, and tj_truncation its operator, which the
+// step's renormalisation and the next step's prediction read), and every
+// later upload whose source lies inside a kept array is a device-to-device
+// copy instead.
 //
 // The caller's side of the contract: an array the library filled is not
 // modified while it is kept (tj_residency_forget drops it first; freeing and

@@ -336,7 +336,7 @@ extern "C" int tj_wave_trans(tj_ctx *ctx, int direction, const tj_basis *sys_bs,
       (rc = ctx->wtSlots.reserve(sizeof(double) * (std::max(P.nslots1, P.nslots2) * BM * BN + 4))))
     return rc;
   for (const auto &u : P.uploads)
-    if (u.n > 0) CKW(cudaMemcpyAsync(ctx->wtOps.d() + u.dst, u.src, sizeof(double) * u.n, cudaMemcpyHostToDevice, st));
+    if (u.n > 0) CKW(upload(ctx, ctx->wtOps.d() + u.dst, u.src, u.n, st));
   CKW(upload(ctx, ctx->wtOld.d(), old_wave->data, old_wave->dim, st));
   std::vector<char> tab;
   auto add = [&](const void *p, size_t n) {

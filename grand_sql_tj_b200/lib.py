@@ -513,6 +513,8 @@ class Context:
         r.sub = C.cast(subs, C.POINTER(TjBlockSub))
         r.data = data.ctypes.data_as(C.POINTER(C.c_double))
         _chk(lib().tj_truncation(self.h, C.byref(wave.c), side, kept_min, kept_max, trun_err, C.byref(r)))
+        if self.resident:
+            self._forget_when_freed(data)
         length = wave.sys_len if side == 0 else wave.env_len
         return r, block_from_c_result(r, length)
 
@@ -631,7 +633,8 @@ class DeviceBackend:
         if self.ctx.pool is not None:   # the predicted vector goes into a pooled page-locked buffer
             new_wave = Wave(new_wave.sys_len, new_wave.env_len, new_wave.sectors,
                             self.ctx.pool.get(max(new_wave.dim, 1)))
-        return self.ctx.wave_trans(direction, sys_bs, env_bs, sys_trun, env_trun, old, new_wave)
+        return self._traced("wave_trans", lambda: self.ctx.wave_trans(direction, sys_bs, env_bs, sys_trun, env_trun,
+                                                                      old, new_wave))
 
     def get_oper(self, side, dia, chain, st_oper, old_idx, new_idx, truns, types="B"):
         return self.ctx.get_oper(side, dia, chain, st_oper, old_idx, new_idx, truns, types)

@@ -161,7 +161,8 @@ int tj_step_begin(tj_ctx *ctx);
 /* No counterpart in the reference.  Keeps on the device, within a budget of
  * `gigabytes` (0, the default: off), the arrays the library writes into
  * caller memory -- the blocks of tj_get_hamiltonian, the Ritz vector of
- * tj_lanczos_memo_new, the predicted wavefunction of tj_wave_trans; later
+ * tj_lanczos_memo_new, the truncation operator of tj_truncation, the
+ * predicted wavefunction of tj_wave_trans; later
  * uploads from inside such an array (tj_model_wave, tj_lanczos_memo_new,
  * tj_truncation, tj_wave_trans, tj_get_hamiltonian, the measurement
  * operators) copy the kept device data instead.  The caller must not modify a filled array
