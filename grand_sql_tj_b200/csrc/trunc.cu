@@ -44,6 +44,16 @@ constexpr double EIG_SAFMIN = 2.2250738585072014e-308;   // smallest normal FP64
 constexpr int ORTH_THREADS = 512;
 constexpr int TD_BIG = 320;       // sectors of at least this many states are reduced by a whole cluster
 
+// Sum of the warps' partial sums r[0..nw-1] by every warp: lane w takes
+// r[w] and a shuffle tree adds them, in the same order in every warp (a
+// serial sum would chain 32 dependent shared-memory loads and adds).
+__device__ __forceinline__ double warp_sum_slots(const double *r) {
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  double s = lane < nw ? r[lane] : 0.0;
+  for (int k = 16; k > 0; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k);
+  return s;
+}
+
 // Sum of one value per thread over the block, in a fixed order; every thread
 // receives it.  red holds 32 doubles of shared memory.
 __device__ __forceinline__ double block_sum(double x, double *red) {
@@ -51,10 +61,7 @@ __device__ __forceinline__ double block_sum(double x, double *red) {
   __syncthreads();
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
   __syncthreads();
-  double s = 0.0;
-  const int nw = blockDim.x >> 5;
-  for (int w = 0; w < nw; ++w) s += red[w];
-  return s;
+  return warp_sum_slots(red);
 }
 
 // Householder reduction of one symmetric sector matrix A (n x n,
@@ -202,10 +209,7 @@ __device__ __forceinline__ double block_sum1(double x, double *red, int &half) {
   half ^= 1;
   if ((threadIdx.x & 31) == 0) r[threadIdx.x >> 5] = x;
   __syncthreads();
-  double s = 0.0;
-  const int nw = blockDim.x >> 5;
-  for (int w = 0; w < nw; ++w) s += r[w];
-  return s;
+  return warp_sum_slots(r);
 }
 
 // The same reduction of one large sector by the CL CTAs of a thread-block
@@ -215,27 +219,46 @@ __device__ __forceinline__ double block_sum1(double x, double *red, int &half) {
 // owns the trailing columns j = c (mod CL), applies the pending rank-2 update
 // to them and forms its part of p = A v, one thread per row, or, when the
 // CTA's threads outnumber the rows, one per row in each of G groups that
-// split the owned columns (the reflector is scaled where it is read); the
-// parts meet in shared memory across the cluster (distributed shared memory,
-// two buffers alternating by step) and every CTA sums them in rank order.
-// Per step: one cluster barrier, which orders the owners' column writes
-// (global memory) and the parts before they are read, and three CTA barriers
-// (four with column groups).  Column k + 1, complete at that barrier, is
-// loaded into registers there for the next step.  The owner of column k
-// stores its reflector there only after the cluster barrier, when no CTA
-// reads the column any more.
+// split the owned columns (the reflector is scaled where it is read).  The
+// parts meet through distributed shared memory as a reduce-scatter and a
+// broadcast, both by remote stores: each CTA stores the parts of rows
+// [o ch, (o + 1) ch) into CTA o's shared memory; after the first cluster
+// barrier CTA o sums them in rank order and stores the sums into every
+// CTA's p; after the second, every CTA reads its own copy.  Per step: two
+// cluster barriers (the first also orders the owners' column writes in
+// global memory before they are read) and three CTA barriers (four with
+// column groups).  Column k + 1, complete at the first barrier, is loaded
+// into registers there for the next step.  The owner of column k stores its
+// reflector there only after the first barrier, when no CTA reads the column
+// any more.
 template <int CL>
 __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aall, const int64_t *off,
                              const int *dims, const int64_t *eoff, double *dall, double *eall, double *tauall,
-                             double *info, double *sm, double *red2) {
+                             double *info, double *sm, int64_t smem_doubles, double *red2, double *pvs) {
   const int n = dims[s], tid = threadIdx.x, nt = blockDim.x;
   double *A = Aall + off[s];
   double *d = dall + eoff[s], *e = eall + eoff[s], *tau = tauall + eoff[s];
-  // vp, wp, v: n each; cp: the cluster parts, 2 x n (read by the other CTAs
-  // until the next barrier); pp: the summed p = tau A v, n
+  // vp, wp, v: n each; cp: the bin of parts of A v sent to this CTA (CL x
+  // ceil(m / CL) <= 2n); pp: p = tau A v, n
   // gp: the column groups' parts of A v when a CTA's threads outnumber the
-  // trailing rows (G groups, G * m <= nt entries)
-  double *vp = sm, *wp = vp + n, *v = wp + n, *cp = v + n, *pp = cp + 2 * n, *gp = pp + n;
+  // trailing rows (G groups, G * m <= nt entries); sl: the CTA's slice of the
+  // trailing block, the rest of the shared memory
+  double *vp = sm, *wp = vp + n, *v = wp + n, *cp = v + n, *pp = cp + 2 * n, *gp = pp + n, *sl = gp + nt;
+  // From step kres on, when the trailing block has mres = n - 1 - kres rows,
+  // each CTA's owned columns (ceil(mres / CL) of them at most) live in its
+  // slice: owned column j >= jr0(c), row i >= kres + 1 at
+  // sl[(j - jr0(c)) / CL * mres + i - kres - 1].  Step kres reads them from
+  // global memory and writes them there; later steps touch only the slice,
+  // and the other CTAs read the next column from its owner's slice.
+  const int64_t cap = smem_doubles - (6 * (int64_t)n + nt);
+  int mres = 0;
+  if (cap > 0) {
+    mres = min(n - 1, (int)sqrt((double)cap * CL));
+    while (mres > 0 && (int64_t)((mres + CL - 1) / CL) * mres > cap) --mres;
+  }
+  const int kres = n - 1 - mres, kr1 = kres + 1;
+  auto jr0 = [&](int c) { return kr1 + ((c - kr1) % CL + CL) % CL; };
+  const int myr0 = jr0(rank);
   int half = 0;
   bool pending = false;
   // rows k + tid + c nt of column k, loaded during step k - 1 (n <= 4 nt)
@@ -278,43 +301,55 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
     const int mloc = j0 < n ? (n - 1 - j0) / CL + 1 : 0;
     const int R = min((m + 31) & ~31, nt), G = nt / R;
     const int g = tid / R, r = tid - g * R;
-    double *mine = cp + (k & 1) * n;
+    // the parts of A v go to the CTA that sums their rows: rows [o ch, (o + 1)
+    // ch) to CTA o, whose bin holds CL rows of ch slots (by sender)
+    const int ch = (m + CL - 1) / CL;
+    auto push = [&](int ii, double val) {
+      const int o = ii / ch;
+      cl.map_shared_rank(cp, o)[rank * ch + (ii - o * ch)] = val;
+    };
+    const bool s_in = k > kres, s_out = k >= kres;   // the owned columns are read / written in the slice
     if (g < G) {
-      const int64_t st = (int64_t)G * CL * n;
+      const int64_t gst = (int64_t)G * CL * n, sst = (int64_t)G * mres;
+      const int64_t ist = s_in ? sst : gst, ost = s_out ? sst : gst;
+      const int jg = j0 + g * CL;   // the group's first column
+      const int64_t sbase = (int64_t)((jg - myr0) / CL) * mres - kr1;
       for (int ii = r; ii < m; ii += R) {
         const int i = k1 + ii;
         const double vpi = pending ? vp[i] : 0.0, wpi = pending ? wp[i] : 0.0;
         double acc = 0.0;
-        double *a = A + (int64_t)(j0 + g * CL) * n + i;
+        const double *ia = s_in ? sl + sbase + i : A + (int64_t)jg * n + i;
+        double *oa = s_out ? sl + sbase + i : A + (int64_t)jg * n + i;
         int q = g;
-        if (pending) {
+        if (pending || s_out != s_in) {
           // four loads issued before the four stores (a store through a
           // may alias the next load: interleaved, every column would wait
           // out a full L2 round trip; eight would not fit the 64 registers
           // of a 1024-thread CTA)
-          for (; q + 3 * G < mloc; q += 4 * G, a += 4 * st) {
+          for (; q + 3 * G < mloc; q += 4 * G, ia += 4 * ist, oa += 4 * ost) {
             double x[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) x[u] = a[u * st];
+            for (int u = 0; u < 4; ++u) x[u] = ia[u * ist];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
               const int j = j0 + (q + u * G) * CL;
-              x[u] -= vpi * wp[j] + wpi * vp[j];
-              a[u * st] = x[u];
+              if (pending) x[u] -= vpi * wp[j] + wpi * vp[j];
+              oa[u * ost] = x[u];
               acc += x[u] * rv(j);
             }
           }
-          for (; q < mloc; q += G, a += st) {
+          for (; q < mloc; q += G, ia += ist, oa += ost) {
             const int j = j0 + q * CL;
-            const double x = *a - (vpi * wp[j] + wpi * vp[j]);
-            *a = x;
+            double x = *ia;
+            if (pending) x -= vpi * wp[j] + wpi * vp[j];
+            *oa = x;
             acc += x * rv(j);
           }
         } else {
-          for (; q < mloc; q += G, a += st) acc += *a * rv(j0 + q * CL);
+          for (; q < mloc; q += G, ia += ist) acc += *ia * rv(j0 + q * CL);
         }
         if (G == 1)
-          mine[ii] = acc;
+          push(ii, acc);
         else
           gp[g * m + ii] = acc;
       }
@@ -324,7 +359,7 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
       for (int ii = tid; ii < m; ii += nt) {
         double acc = 0.0;
         for (int c = 0; c < G; ++c) acc += gp[c * m + ii];
-        mine[ii] = acc;
+        push(ii, acc);
       }
     }
     // the cluster barrier's release / acquire order the column writes
@@ -334,6 +369,10 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
     // its loads for the next step overlap the sums below
     if (k + 2 < n) {
       const double *c1 = A + (int64_t)k1 * n;
+      if (s_out) {   // in the slice of its owner
+        const int ow = k1 % CL;
+        c1 = cl.map_shared_rank(sl, ow) + (int64_t)((k1 - jr0(ow)) / CL) * mres - kr1;
+      }
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         const int i = k1 + tid + c * nt;
@@ -342,15 +381,32 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
     }
     if (owner)
       for (int i = k1 + tid; i < n; i += nt) colk[i] = rv(i);
+    // CTA c sums the parts of its rows from its bin (in sender order), and
+    // stores the sums into every CTA's pp and its part of p.v into every
+    // CTA's pvs[c]; after the second barrier each CTA reads only its own
+    // shared memory.  Every exchange is a store to another CTA's shared
+    // memory: a store does not wait for its reply as a remote load does.
+    // A bin is written again in the next step's product, after its owner
+    // has passed the second barrier; pp and pvs after the next step's first
+    // barrier, which every reader passes after its reads.
+    const int lo = min(m, rank * ch), hi = min(m, lo + ch);
     double pv = 0.0;
-    for (int ii = tid; ii < m; ii += nt) {
+    for (int ii = lo + tid; ii < hi; ii += nt) {
       double p = 0.0;
-      for (int c = 0; c < CL; ++c) p += cl.map_shared_rank(mine, c)[ii];
+#pragma unroll
+      for (int c = 0; c < CL; ++c) p += cp[c * ch + (ii - lo)];
       p *= t;
-      pp[ii] = p;
       pv += p * rv(k1 + ii);
+#pragma unroll
+      for (int c = 0; c < CL; ++c) cl.map_shared_rank(pp, c)[ii] = p;
     }
-    const double K = 0.5 * t * block_sum1(pv, red2, half);
+    pv = block_sum1(pv, red2, half);
+    if (tid < CL) cl.map_shared_rank(pvs, tid)[rank] = pv;
+    cl.sync();
+    double K = 0.0;
+#pragma unroll
+    for (int c = 0; c < CL; ++c) K += pvs[c];
+    K *= 0.5 * t;
     for (int ii = tid; ii < m; ii += nt) {
       const int i = k1 + ii;
       const double vi = rv(i);
@@ -360,10 +416,15 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
     pending = true;
     __syncthreads();
   }
+  // the last diagonal entry, from its owner's slice when the last step
+  // wrote it there
+  const bool last_in_slice = n - 2 >= kres;
+  if (last_in_slice && rank == (n - 1) % CL && tid == 0)
+    d[n - 1] = sl[(int64_t)((n - 1 - myr0) / CL) * mres + (n - 1 - kr1)];
   __threadfence();
   cl.sync();   // the last parts are read; every owner's writes are visible
   if (rank == 0 && tid == 0) {
-    d[n - 1] = A[(int64_t)(n - 1) * n + (n - 1)];
+    if (!last_in_slice) d[n - 1] = A[(int64_t)(n - 1) * n + (n - 1)];
     tau[n - 1] = 0.0;
     tridiag_info(s, n, d, e, info);
   }
@@ -377,15 +438,15 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
 template <int CL>
 __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(EIG_THREADS)
     tridiag_kernel(double *Aall, const int64_t *off, const int *dims, const int64_t *eoff, const int *tsec,
-                   const int *tbig, double *dall, double *eall, double *tauall, double *info) {
+                   const int *tbig, double *dall, double *eall, double *tauall, double *info, int64_t smem_doubles) {
   extern __shared__ double sm[];
   __shared__ double red[64];
-  __shared__ double sh_tau, sh_scl;
+  __shared__ double sh_tau, sh_scl, sh_pvs[16];
   cg::cluster_group cl = cg::this_cluster();
   const int b = blockIdx.x / CL, rank = (int)cl.block_rank();
   const int s = tsec[blockIdx.x];
   if (tbig[b]) {
-    tridiag_coop<CL>(cl, rank, s, Aall, off, dims, eoff, dall, eall, tauall, info, sm, red);
+    tridiag_coop<CL>(cl, rank, s, Aall, off, dims, eoff, dall, eall, tauall, info, sm, smem_doubles, red, sh_pvs);
   } else if (s >= 0 && dims[s] > 0) {
     tridiag_one(s, Aall, off, dims, eoff, dall, eall, tauall, info, sm, red, sh_tau, sh_scl);
   }
@@ -854,7 +915,7 @@ __device__ void ortho_coop(cg::cluster_group &cl, int rank, int blk, const int *
 // shared by all of them (obig), or up to CL small blocks, one per CTA
 // (oblk[cluster * CL + rank], -1 for none); CL as for tridiag_kernel.
 template <int CL>
-__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ORTH_THREADS)
+__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ORTH_THREADS, 1)
     orthonormalize_kernel(const int *oblk, const int *obig, const int *grp, const int *dims, const int64_t *eoff,
                           const double *evals, const double *info, const int *job_k, double *Y, int ldy,
                           int *status) {
@@ -1099,7 +1160,17 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     const size_t p_dims = pos; pos += al256(db);
     // clusters of the tridiagonal reduction: one per large sector, then the
     // small sectors tcl at a time (largest first)
-    const size_t tsm = sizeof(double) * (6 * (size_t)maxn + std::max(maxn, EIG_THREADS));
+    // shared memory: the per-sector vectors, and for a sector reduced by a
+    // cluster as much more as a CTA may have (its slice of the trailing block)
+    size_t tsm = sizeof(double) * (6 * (size_t)maxn + std::max(maxn, EIG_THREADS));
+    if (maxn >= TD_BIG) {
+      int optin = 0;
+      cudaFuncAttributes fa;
+      if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device) == cudaSuccess &&
+          cudaFuncGetAttributes(&fa, tridiag_kernel<16>) == cudaSuccess && optin > (int)fa.sharedSizeBytes + 1024)
+        tsm = std::max(tsm, (size_t)(optin - (int)fa.sharedSizeBytes - 1024) / 256 * 256);
+      cudaGetLastError();
+    }
     const int tcl = cluster_size(tridiag_kernel<16>, EIG_THREADS, tsm);
     std::vector<int> tsec, tbig;
     {
@@ -1157,11 +1228,11 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       if (tcl == 16) {
         CKT(cudaFuncSetAttribute(tridiag_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
         tridiag_kernel<16><<<nclus * 16, EIG_THREADS, tsm, st>>>(ctx->trB.d(), d_roff, d_dims, d_eoff, d_tsec, d_tbig,
-                                                                 dd, de, dtau, dinfo);
+                                                                 dd, de, dtau, dinfo, (int64_t)(tsm / 8));
       } else {
         CKT(cudaFuncSetAttribute(tridiag_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
         tridiag_kernel<8><<<nclus * 8, EIG_THREADS, tsm, st>>>(ctx->trB.d(), d_roff, d_dims, d_eoff, d_tsec, d_tbig,
-                                                               dd, de, dtau, dinfo);
+                                                               dd, de, dtau, dinfo, (int64_t)(tsm / 8));
       }
       CKT(cudaGetLastError());
     }
