@@ -354,7 +354,9 @@ def sweep_leg(ctx64, ctxoz, name: str, prep: str, seed: int):
                                   "iterations": sum(st.lanczos_ms for st in lz)}
         # the prediction's library call; the rest of `pred` is the driver's
         # bases of the new superblock
-        out[tag]["wave_trans_ms"] = 1e3 * sum(w for name, _, w, _ in trace if name == "wave_trans")
+        wt = [st for name, st, _, _ in trace if name == "wave_trans"]
+        out[tag]["wave_trans_ms"] = {"wall": 1e3 * sum(w for name, _, w, _ in trace if name == "wave_trans"),
+                                     "plan": sum(st.wt_plan_ms for st in wt), "device": sum(st.wt_ms for st in wt)}
         return recs
 
     # one untimed sweep from the same state first: a running DMRG reuses the

@@ -324,8 +324,10 @@ extern "C" int tj_wave_trans(tj_ctx *ctx, int direction, const tj_basis *sys_bs,
   if ((rc = check_wave(old_wave)) || (rc = check_wave(new_wave))) return rc;
   HpsiPlan P;
   std::string msg;
+  const auto t0 = std::chrono::steady_clock::now();
   if ((rc = build_wave_trans_plan(direction, sys_bs, env_bs, sys_trun, env_trun, old_wave, new_wave, P, msg)))
     return set_err(rc, "tj_wave_trans: " + msg);
+  ctx->stats.wt_plan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   CKW(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
   const int64_t D = new_wave->dim;
@@ -335,6 +337,7 @@ extern "C" int tj_wave_trans(tj_ctx *ctx, int direction, const tj_basis *sys_bs,
       (rc = ctx->wtScr.reserve(sizeof(double) * (P.scratch_len + 4))) ||
       (rc = ctx->wtSlots.reserve(sizeof(double) * (std::max(P.nslots1, P.nslots2) * BM * BN + 4))))
     return rc;
+  CKW(cudaEventRecord(ctx->ev[5], st));
   for (const auto &u : P.uploads)
     if (u.n > 0) CKW(upload(ctx, ctx->wtOps.d() + u.dst, u.src, u.n, st));
   CKW(upload(ctx, ctx->wtOld.d(), old_wave->data, old_wave->dim, st));
@@ -396,6 +399,11 @@ extern "C" int tj_wave_trans(tj_ctx *ctx, int direction, const tj_basis *sys_bs,
     int rc = download(ctx, new_wave->data, ctx->wtNew.d(), D, st);
     if (!rc) rc = res_keep(ctx, new_wave->data, D, ctx->wtNew.d(), st);
     if (rc) return rc;
+    float ms = 0;
+    if (cudaEventRecord(ctx->ev[2], st) == cudaSuccess && cudaEventSynchronize(ctx->ev[2]) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, ctx->ev[5], ctx->ev[2]) == cudaSuccess)
+      ctx->stats.wt_ms = ms;
+    cudaGetLastError();
   }
   if (!(h_nrm > 0.0) || !std::isfinite(h_nrm))
     return set_err(TJ_ERR_NUMERIC, "tj_wave_trans: the carried wavefunction is zero or not finite");

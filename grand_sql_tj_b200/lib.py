@@ -516,7 +516,7 @@ class Context:
         if self.resident:
             self._forget_when_freed(data)
         length = wave.sys_len if side == 0 else wave.env_len
-        return r, block_from_c_result(r, length)
+        return r, block_from_c_result(r, length, subs, data)
 
     def correlator(self, name: str, a: Block, b: Optional[Block], sys_bs, env_bs, wave: Wave,
                    flag: str = "B") -> float:

@@ -124,7 +124,8 @@ class TjHpsiStats(C.Structure):
                 ("trunc_ms_back", C.c_double), ("trunc_ms_total", C.c_double),
                 ("trunc_max_n", C.c_int64), ("trunc_max_kept", C.c_int64),
                 ("res_hits", C.c_int64), ("res_hit_bytes", C.c_double),
-                ("renorm_pre_ms", C.c_double), ("renorm_post_ms", C.c_double)]
+                ("renorm_pre_ms", C.c_double), ("renorm_post_ms", C.c_double),
+                ("wt_plan_ms", C.c_double), ("wt_ms", C.c_double)]
 
 
 class TjTuneResult(C.Structure):
@@ -181,7 +182,17 @@ class Block:
         return int(sum(s.mat.shape[1] for s in self.subs))
 
     def pack(self) -> "PackedBlock":
-        return PackedBlock(self)
+        # a block the library returned keeps its result arrays: packed without a copy
+        pk = getattr(self, "_packed", None)
+        return pk if pk is not None else PackedBlock(self)
+
+
+class _BlockView:
+    """The packed form of a block the library wrote: its own sub-block table
+    and data array (the sub-blocks of the Block are views into that array)."""
+
+    def __init__(self, c, subs, data):
+        self.c, self.subs, self.data = c, subs, data
 
 
 class PackedBlock:
@@ -439,7 +450,9 @@ def call_block_result(call):
     rc = call(C.byref(res))
     if rc:
         return rc, None
-    return 0, _block_from_c(res.block, data)
+    b = _block_from_c(res.block, data)
+    b._packed = _BlockView(res.block, subs, data)
+    return 0, b
 
 
 class PackedChain:
@@ -462,12 +475,23 @@ class PackedChain:
         self.c = TjChain(n, trun_idx, C.cast(self.bsm, C.POINTER(TjBasis)), C.cast(self.truns, C.POINTER(TjBlock)))
 
 
-def block_from_c_result(res: TjTruncResult, length: int) -> Block:
-    """Turns a filled tj_trunc_result into a Block (trun_op)."""
+def block_from_c_result(res: TjTruncResult, length: int, subs_arr=None, data: Optional[np.ndarray] = None) -> Block:
+    """Turns a filled tj_trunc_result into a Block (trun_op).  Given the
+    sub-block table and data array the result was written into, the
+    sub-blocks are views into `data` and the Block packs to those arrays
+    without a copy; otherwise they are copies."""
     subs = []
     for i in range(res.num):
         s = res.sub[i]
         n = s.row_dim * s.sdim
-        buf = np.ctypeslib.as_array(res.data, shape=(res.data_len,))[s.off:s.off + n]
-        subs.append(SubBlock(s.num_up, s.num_down, 0, buf.reshape((s.row_dim, s.sdim), order="F").copy()))
-    return Block(length, 0, 0, subs)
+        if data is not None:
+            mat = data[s.off:s.off + n].reshape((s.row_dim, s.sdim), order="F")
+        else:
+            buf = np.ctypeslib.as_array(res.data, shape=(res.data_len,))[s.off:s.off + n]
+            mat = buf.reshape((s.row_dim, s.sdim), order="F").copy()
+        subs.append(SubBlock(s.num_up, s.num_down, 0, mat))
+    b = Block(length, 0, 0, subs)
+    if data is not None and subs_arr is not None:
+        b._packed = _BlockView(TjBlock(length, res.num, b.dim, 0, 0, 0, C.cast(subs_arr, C.POINTER(TjBlockSub)),
+                                       _dptr(data)), subs_arr, data)
+    return b

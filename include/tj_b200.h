@@ -451,6 +451,9 @@ typedef struct tj_hpsi_stats {
   /* the last tj_get_hamiltonian's second call: host time (ms) before its
    * first upload and after its download (result tables, residency) */
   double renorm_pre_ms, renorm_post_ms;
+  /* the last tj_wave_trans: host time (ms) of its plan, and device time
+   * from its first upload to the end of its download */
+  double wt_plan_ms, wt_ms;
 } tj_hpsi_stats;
 int tj_hpsi_stats_get(tj_ctx *ctx, tj_hpsi_stats *st);
 

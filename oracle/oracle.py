@@ -143,7 +143,7 @@ def truncation(wave, side: int, kept_min: int, kept_max: int, trun_err: float):
     _chk(L.ora_truncation(C.byref(wave.c), side, kept_min, kept_max, trun_err, C.byref(r),
                           ev.ctypes.data_as(C.POINTER(C.c_double))))
     length = wave.sys_len if side == 0 else wave.env_len
-    return r, block_from_c_result(r, length), ev[:ndim]
+    return r, block_from_c_result(r, length, subs, data), ev[:ndim]
 
 
 def site_operator(which: int, up_bias: int) -> Block:
