@@ -980,6 +980,98 @@ __global__ void backtransform_kernel(const double *Aall, const int64_t *off, con
   for (int i = lane; i < n; i += 32) dst[i] = sg * col[i];
 }
 
+// The same back-transformation with each warp's vector in registers (lane l
+// holds rows l + 32 r, r < RPL) for sectors of up to 32 RPL states: the CTA's
+// BT_WARPS warps (vectors of one kept block, so of one sector) share the
+// reflectors, staged kb at a time in shared memory by one coalesced load of
+// the whole CTA, so that a step waits for no L2 load.  A lane's rows stay
+// fixed (backtransform_kernel's shift with k), so the dot products are
+// grouped differently: the two agree to rounding.  Warps past the block's
+// last vector take part in the loads and barriers only.
+constexpr int BT_WARPS = 8;
+template <int RPL>
+__global__ void __launch_bounds__(32 * BT_WARPS)
+    backtransform_reg_kernel(const double *Aall, const int64_t *off, const double *tauall, const int64_t *eoff,
+                             const int *dims, const int *grp, const int *slab, const double *Y, int ldy,
+                             const int64_t *job_dst, double *out, int kb) {
+  extern __shared__ double sv[];   // kb reflectors of n rows
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nt = blockDim.x;
+  const int g = slab[2 * blockIdx.x], c = slab[2 * blockIdx.x + 1] + warp;
+  const int s = grp[4 * g], j0 = grp[4 * g + 1], cnt = grp[4 * g + 2];
+  const bool active = c < cnt;
+  const int n = dims[s], j = j0 + c;
+  const double *A = Aall + off[s], *tau = tauall + eoff[s];
+  double col[RPL];
+#pragma unroll
+  for (int r = 0; r < RPL; ++r) {
+    const int i = lane + 32 * r;
+    col[r] = active && i < n ? Y[(size_t)j * ldy + i] : 0.0;
+  }
+  for (int k0 = n - 2; k0 >= 0; k0 -= kb) {
+    const int nk = min(kb, k0 + 1);   // reflectors k0, k0 - 1, ..., k0 - nk + 1
+    __syncthreads();                  // the previous chunk is read
+    for (int u = 0; u < nk; ++u) {
+      const int k = k0 - u;
+      const double *v = A + (int64_t)k * n;
+      for (int i = k + 1 + (int)threadIdx.x; i < n; i += nt) sv[(size_t)u * n + i] = v[i];
+    }
+    __syncthreads();
+    if (!active) continue;
+    for (int u = 0; u < nk; ++u) {
+      const int k = k0 - u;
+      const double t = tau[k];
+      if (t == 0.0) continue;
+      const double *v = sv + (size_t)u * n;
+      double acc = 0.0;
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) {
+        const int i = lane + 32 * r;
+        if (i > k && i < n) acc += v[i] * col[r];
+      }
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      const double f = t * acc;
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) {
+        const int i = lane + 32 * r;
+        if (i > k && i < n) col[r] -= f * v[i];
+      }
+    }
+  }
+  if (!active) return;
+  double best = -1.0;
+  int bi = 0;
+#pragma unroll
+  for (int r = 0; r < RPL; ++r) {
+    const int i = lane + 32 * r;
+    if (i < n && fabs(col[r]) > best) {
+      best = fabs(col[r]);
+      bi = i;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ob > best || (ob == best && oi < bi)) {
+      best = ob;
+      bi = oi;
+    }
+  }
+  // the sign of the entry of largest magnitude: the lane holding row bi
+  // broadcasts it
+  double atbi = 0.0;
+#pragma unroll
+  for (int r = 0; r < RPL; ++r)
+    if (lane + 32 * r == bi) atbi = col[r];
+  atbi = __shfl_sync(0xffffffffu, atbi, bi & 31);
+  const double sg = atbi < 0.0 ? -1.0 : 1.0;
+  double *dst = out + job_dst[j];
+#pragma unroll
+  for (int r = 0; r < RPL; ++r) {
+    const int i = lane + 32 * r;
+    if (i < n) dst[i] = sg * col[r];
+  }
+}
+
 }  // namespace tjb
 
 using namespace tjb;
@@ -1343,8 +1435,10 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
     tc.mats.assign(dpos, 0.0);
     const int njobs = (int)job_sec.size(), ngrp = (int)grp.size() / 4;
     if (njobs > 0) {
-      // vectors in shared memory: W warps of one column each per CTA
-      const int W = std::max(1, std::min(32, (int)(196608 / (sizeof(double) * maxn))));
+      // back-transformation: vectors in registers (BT_WARPS to a CTA) for
+      // sectors of up to 32 * 48 states, else in shared memory (W warps)
+      const bool bt_reg = maxn <= 32 * 48;
+      const int W = bt_reg ? BT_WARPS : std::max(1, std::min(32, (int)(196608 / (sizeof(double) * maxn))));
       for (int b = 0; b < ngrp; ++b)
         for (int c0 = 0; c0 < grp[4 * b + 2]; c0 += W) slab.insert(slab.end(), {b, c0});
       const int nslab = (int)slab.size() / 2;
@@ -1418,12 +1512,33 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       }
       CKT(cudaGetLastError());
       CKT(cudaEventRecord(ctx->tev[6], st));
-      const size_t bsm = sizeof(double) * (size_t)W * ldy;
-      CKT(cudaFuncSetAttribute(backtransform_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
-      backtransform_kernel<<<nslab, 32 * W, bsm, st>>>(ctx->trB.d(), d_roff, dtau, d_eoff, d_dims,
-                                                       (const int *)(ab + q_grp), (const int *)(ab + q_slab), Y, ldy,
-                                                       (const int64_t *)(ab + q_dst), d_out);
-      CKT(cudaGetLastError());
+      if (bt_reg) {
+        // eight reflectors per chunk: two CTAs fit an SM for sectors of up to 1536 states
+        const int kb = 8;
+        const size_t bsm = sizeof(double) * (size_t)kb * maxn;
+        const int rpl = (maxn + 31) / 32;
+        auto launch = [&](auto kern) -> cudaError_t {
+          cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm);
+          if (e != cudaSuccess) return e;
+          kern<<<nslab, 32 * BT_WARPS, bsm, st>>>(ctx->trB.d(), d_roff, dtau, d_eoff, d_dims, (const int *)(ab + q_grp),
+                                                 (const int *)(ab + q_slab), Y, ldy, (const int64_t *)(ab + q_dst),
+                                                 d_out, kb);
+          return cudaGetLastError();
+        };
+        if (rpl <= 8) CKT(launch(backtransform_reg_kernel<8>));
+        else if (rpl <= 16) CKT(launch(backtransform_reg_kernel<16>));
+        else if (rpl <= 24) CKT(launch(backtransform_reg_kernel<24>));
+        else if (rpl <= 32) CKT(launch(backtransform_reg_kernel<32>));
+        else if (rpl <= 40) CKT(launch(backtransform_reg_kernel<40>));
+        else CKT(launch(backtransform_reg_kernel<48>));
+      } else {
+        const size_t bsm = sizeof(double) * (size_t)W * ldy;
+        CKT(cudaFuncSetAttribute(backtransform_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
+        backtransform_kernel<<<nslab, 32 * W, bsm, st>>>(ctx->trB.d(), d_roff, dtau, d_eoff, d_dims,
+                                                         (const int *)(ab + q_grp), (const int *)(ab + q_slab), Y,
+                                                         ldy, (const int64_t *)(ab + q_dst), d_out);
+        CKT(cudaGetLastError());
+      }
       int status[16] = {0};
       CKT(cudaMemcpyAsync(tc.mats.data(), d_out, sizeof(double) * dpos, cudaMemcpyDeviceToHost, st));
       CKT(cudaMemcpyAsync(status, d_status, sizeof status, cudaMemcpyDeviceToHost, st));
