@@ -1022,18 +1022,26 @@ __global__ void __launch_bounds__(32 * BT_WARPS)
       const double t = tau[k];
       if (t == 0.0) continue;
       const double *v = sv + (size_t)u * n;
-      double acc = 0.0;
+      // rows 32 r .. 32 r + 31 all at or above k are skipped by the whole
+      // warp; two partial sums (even and odd r) shorten the chain of adds
+      double acc0 = 0.0, acc1 = 0.0;
 #pragma unroll
       for (int r = 0; r < RPL; ++r) {
         const int i = lane + 32 * r;
-        if (i > k && i < n) acc += v[i] * col[r];
+        if (32 * r + 31 > k && i > k && i < n) {
+          if (r & 1)
+            acc1 += v[i] * col[r];
+          else
+            acc0 += v[i] * col[r];
+        }
       }
+      double acc = acc0 + acc1;
       for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
       const double f = t * acc;
 #pragma unroll
       for (int r = 0; r < RPL; ++r) {
         const int i = lane + 32 * r;
-        if (i > k && i < n) col[r] -= f * v[i];
+        if (32 * r + 31 > k && i > k && i < n) col[r] -= f * v[i];
       }
     }
   }
@@ -1093,8 +1101,9 @@ struct TruncCache {
   uint64_t hash = 0;
   tj_trunc_result res{};
   std::vector<tj_block_sub> sub;
-  std::vector<double> mats;
-  // the device copy of mats: valid while ctx has computed no other truncation
+  // the operator stays on the device (trA of ctx) until the second call
+  // copies it out: valid while ctx has computed no other truncation
+  int64_t len = 0;
   const tj_ctx *ctx = nullptr;
   uint64_t seq = 0;
   const double *dev = nullptr;
@@ -1168,14 +1177,17 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
   const uint64_t h = hash_data(wave->data, D);
   TruncCache &tc = g_tc;
   const bool hit = tc.valid && tc.data == wave->data && tc.dim == D && tc.side == side && tc.kept_min == kept_min &&
-                   tc.kept_max == kept_max && tc.trun_err == trun_err && tc.hash == h;
+                   tc.kept_max == kept_max && tc.trun_err == trun_err && tc.hash == h && tc.ctx == ctx &&
+                   tc.seq == ctx->trunc_seq;
   if (!hit) {
     CKT(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     const auto wall0 = std::chrono::steady_clock::now();
+    tc.valid = false;   // until this computation completes
     tc.ctx = ctx;
     tc.seq = ++ctx->trunc_seq;
     tc.dev = nullptr;
+    tc.len = 0;
     CKT(cudaEventRecord(ctx->tev[0], st));
     // psi on the device and its norm
     int rc;
@@ -1432,7 +1444,7 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
       }
       dpos += (int64_t)row * col;
     }
-    tc.mats.assign(dpos, 0.0);
+    tc.len = dpos;
     const int njobs = (int)job_sec.size(), ngrp = (int)grp.size() / 4;
     if (njobs > 0) {
       // back-transformation: vectors in registers (BT_WARPS to a CTA) for
@@ -1540,7 +1552,6 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
         CKT(cudaGetLastError());
       }
       int status[16] = {0};
-      CKT(cudaMemcpyAsync(tc.mats.data(), d_out, sizeof(double) * dpos, cudaMemcpyDeviceToHost, st));
       CKT(cudaMemcpyAsync(status, d_status, sizeof status, cudaMemcpyDeviceToHost, st));
       CKT(cudaEventRecord(ctx->tev[7], st));
       CKT(cudaStreamSynchronize(st));
@@ -1597,14 +1608,18 @@ extern "C" int tj_truncation(tj_ctx *ctx, const tj_wave *wave, int side, int kep
   out->data = udata;
   if (usub && udata) {
     std::memcpy(usub, tc.sub.data(), sizeof(tj_block_sub) * tc.sub.size());
-    std::memcpy(udata, tc.mats.data(), sizeof(double) * tc.mats.size());
-    // the renormalisation of this step and the prediction of the next read
-    // the operator again: with residency on, its device copy is kept
-    if (tc.dev && tc.ctx == ctx && tc.seq == ctx->trunc_seq && !tc.mats.empty()) {
+    if (tc.len > 0) {
+      // straight from the device into the caller's array (the cache hit
+      // above requires the device copy to be intact)
       CKT(cudaSetDevice(ctx->device));
-      // (the copy runs on the context's stream, ahead of anything that
-      // rewrites trA)
-      const int rc = res_keep(ctx, udata, (int64_t)tc.mats.size(), tc.dev, ctx->stream);
+      const int rc = download(ctx, udata, tc.dev, tc.len, ctx->stream);
+      if (rc) return rc;
+    }
+    // the renormalisation of this step and the prediction of the next read
+    // the operator again: with residency on, its device copy is kept (the
+    // copy runs on the context's stream, ahead of anything that rewrites trA)
+    if (tc.len > 0) {
+      const int rc = res_keep(ctx, udata, tc.len, tc.dev, ctx->stream);
       if (rc) return rc;
     }
   }

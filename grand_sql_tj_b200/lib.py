@@ -509,7 +509,8 @@ class Context:
         r = TjTruncResult()
         _chk(lib().tj_truncation(self.h, C.byref(wave.c), side, kept_min, kept_max, trun_err, C.byref(r)))
         subs = (TjBlockSub * max(r.num, 1))()
-        data = np.zeros(max(r.data_len, 1))
+        # the library writes every entry: a pooled page-locked buffer takes the copy at the DMA rate
+        data = self.pool.get(max(r.data_len, 1)) if self.pool is not None else np.zeros(max(r.data_len, 1))
         r.sub = C.cast(subs, C.POINTER(TjBlockSub))
         r.data = data.ctypes.data_as(C.POINTER(C.c_double))
         _chk(lib().tj_truncation(self.h, C.byref(wave.c), side, kept_min, kept_max, trun_err, C.byref(r)))
