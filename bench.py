@@ -274,8 +274,8 @@ def sweep_leg(ctx64, ctxoz, name: str, prep: str, seed: int):
     main.f90:96-187) through the C ABI on the device: warm-up and the first two
     half-sweeps untimed (at the reference's looser thresholds), then one full
     sweep (left to right and back, at lanzero = 2e-5) timed in FP64 and one in
-    split precision, both from the same state (after one untimed sweep from
-    it that fills the page-locked buffer pool).  Every DMRG step is Lanczos +
+    split precision, both from the same state (each after an untimed sweep
+    of its own precision from it that fills the page-locked buffer pool).  Every DMRG step is Lanczos +
     truncation + operator renormalisation + wavefunction prediction, with
     host buffers in and out (the drop-in's calling pattern) and the blocks
     the library returns also kept on the device (tj_set_residency), so that
@@ -359,14 +359,17 @@ def sweep_leg(ctx64, ctxoz, name: str, prep: str, seed: int):
                                      "plan": sum(st.wt_plan_ms for st in wt), "device": sum(st.wt_ms for st in wt)}
         return recs
 
-    # one untimed sweep from the same state first: a running DMRG reuses the
-    # page-locked buffers of the blocks it replaces, and the snapshot keeps
-    # the replaced blocks alive, so the pool is filled once beforehand
-    one(ctxoz if ctxoz is not None else ctx64, "untimed")
-    del out["untimed"]
+    # an untimed sweep from the same state before each timed one: a running
+    # DMRG reuses the page-locked buffers of the blocks it replaces, and the
+    # snapshot keeps the replaced blocks alive, so the pool is filled first
+    # (with the sizes of that precision's run, which differ a little)
+    one(ctx64, "untimed")
     r64 = one(ctx64, "fp64")
     if ctxoz is not None:
+        one(ctxoz, "untimed")
         rmx = one(ctxoz, "mixed")
+    del out["untimed"]
+    if ctxoz is not None:
         out["speedup_vs_fp64"] = out["fp64"]["sweep_s"] / out["mixed"]["sweep_s"]
         out["dE_per_site_end"] = abs(out["fp64"]["E_end"] - out["mixed"]["E_end"]) / N
         out["dE_per_site_max_step"] = max(abs(a.energy - b.energy) for a, b in zip(r64, rmx)) / N
