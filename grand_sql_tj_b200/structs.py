@@ -12,6 +12,7 @@ from __future__ import annotations
 import ctypes as C
 import time
 from dataclasses import dataclass, field
+from collections.abc import Sequence
 from typing import List, Optional, Tuple
 
 import numpy as np
@@ -423,15 +424,40 @@ class _ResultPack:
         self.data = data
 
 
+class _LazySets(Sequence):
+    """Model.sub of a model the library wrote: each BlockSet (its sub-blocks
+    views into the result array) is built when first read -- a sweep reads
+    only the Hamiltonian of the blocks it passes back."""
+
+    def __init__(self, m: TjModel, data: np.ndarray):
+        self._m, self._data = m, data
+        self._sets: List[Optional[BlockSet]] = [None] * m.nsub
+
+    def __len__(self):
+        return len(self._sets)
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self[j] for j in range(*i.indices(len(self)))]
+        if i < 0:
+            i += len(self)
+        if not 0 <= i < len(self):
+            raise IndexError(i)
+        if self._sets[i] is None:
+            bs = self._m.sub[i]
+            self._sets[i] = BlockSet(*[_block_from_c(getattr(bs, k), self._data) for k in OPS])
+        return self._sets[i]
+
+    def __eq__(self, other):
+        return list(self) == list(other)
+
+
 def model_from_c(m: TjModel, data: np.ndarray, keep=None) -> Model:
     """A tj_model whose blocks all point into `data` -> a numpy-side Model whose
-    sub-blocks are views into `data`; `keep` holds the arrays the C structs
-    point into, so that the Model packs without a copy."""
-    sets = []
-    for i in range(m.nsub):
-        bs = m.sub[i]
-        sets.append(BlockSet(*[_block_from_c(getattr(bs, k), data) for k in OPS]))
-    out = Model(m.len, _block_from_c(m.ham, data), sets)
+    sub-blocks are views into `data` (the operator sets built when first
+    read); `keep` holds the arrays the C structs point into, so that the Model
+    packs without a copy."""
+    out = Model(m.len, _block_from_c(m.ham, data), _LazySets(m, data))
     if keep is not None:
         out._packed = _ResultPack(m, data, keep)
     return out
