@@ -36,9 +36,9 @@ namespace cg = cooperative_groups;
 
 namespace tjb {
 
-constexpr int EIG_THREADS = 1024;
+constexpr int EIG_THREADS = 512;
 constexpr int EIG_MAX_N = 4096;
-static_assert(4 * EIG_THREADS >= EIG_MAX_N, "the cluster reduction holds up to four rows of a column per thread");
+constexpr int TD_NX = (EIG_MAX_N + EIG_THREADS - 1) / EIG_THREADS;   // rows of a column per thread
 constexpr double EIG_EPS = 2.220446049250313e-16;        // 2^-52
 constexpr double EIG_SAFMIN = 2.2250738585072014e-308;   // smallest normal FP64
 constexpr int ORTH_THREADS = 512;
@@ -261,15 +261,15 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
   const int myr0 = jr0(rank);
   int half = 0;
   bool pending = false;
-  // rows k + tid + c nt of column k, loaded during step k - 1 (n <= 4 nt)
-  double nx[4];
+  // rows k + tid + c nt of column k, loaded during step k - 1 (n <= TD_NX nt)
+  double nx[TD_NX];
   for (int k = 0; k + 1 < n; ++k) {
     const int k1 = k + 1, m = n - k1;
     const bool owner = (k % CL) == rank;
     double *colk = A + (int64_t)k * n;
     double ss = 0.0;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < TD_NX; ++c) {
       const int i = k + tid + c * nt;
       if (i < n) {
         double a = k == 0 ? colk[i] : nx[c];
@@ -322,16 +322,15 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
         double *oa = s_out ? sl + sbase + i : A + (int64_t)jg * n + i;
         int q = g;
         if (pending || s_out != s_in) {
-          // four loads issued before the four stores (a store through a
+          // eight loads issued before the eight stores (a store through a
           // may alias the next load: interleaved, every column would wait
-          // out a full L2 round trip; eight would not fit the 64 registers
-          // of a 1024-thread CTA)
-          for (; q + 3 * G < mloc; q += 4 * G, ia += 4 * ist, oa += 4 * ost) {
-            double x[4];
+          // out a full L2 round trip)
+          for (; q + 7 * G < mloc; q += 8 * G, ia += 8 * ist, oa += 8 * ost) {
+            double x[8];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) x[u] = ia[u * ist];
+            for (int u = 0; u < 8; ++u) x[u] = ia[u * ist];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < 8; ++u) {
               const int j = j0 + (q + u * G) * CL;
               if (pending) x[u] -= vpi * wp[j] + wpi * vp[j];
               oa[u * ost] = x[u];
@@ -374,7 +373,7 @@ __device__ void tridiag_coop(cg::cluster_group &cl, int rank, int s, double *Aal
         c1 = cl.map_shared_rank(sl, ow) + (int64_t)((k1 - jr0(ow)) / CL) * mres - kr1;
       }
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
+      for (int c = 0; c < TD_NX; ++c) {
         const int i = k1 + tid + c * nt;
         nx[c] = i < n ? c1[i] : 0.0;
       }
