@@ -183,17 +183,30 @@ class Block:
         return int(sum(s.mat.shape[1] for s in self.subs))
 
     def pack(self) -> "PackedBlock":
-        # a block the library returned keeps its result arrays: packed without a copy
+        # a block the library returned keeps its result arrays: packed without
+        # a copy while its sub-blocks are still those views
         pk = getattr(self, "_packed", None)
-        return pk if pk is not None else PackedBlock(self)
+        return pk if pk is not None and pk.matches(self) else PackedBlock(self)
+
+
+def _views(b: "Block"):
+    return [(s.num_up, s.num_down, s.down_dif, s.mat.shape, s.mat.__array_interface__["data"][0],
+             s.mat.flags.f_contiguous) for s in b.subs]
 
 
 class _BlockView:
     """The packed form of a block the library wrote: its own sub-block table
-    and data array (the sub-blocks of the Block are views into that array)."""
+    and data array (the sub-blocks of the Block are views into that array).
+    It stands for the Block while every sub-block is still the view it was
+    made with (matrices changed in place are seen through the views; a
+    replaced sub-block makes pack() copy)."""
 
-    def __init__(self, c, subs, data):
+    def __init__(self, c, subs, data, block: "Block"):
         self.c, self.subs, self.data = c, subs, data
+        self.views = _views(block)
+
+    def matches(self, block: "Block") -> bool:
+        return _views(block) == self.views
 
 
 class PackedBlock:
@@ -232,9 +245,10 @@ class Model:
     sub: List[BlockSet]
 
     def pack(self) -> "PackedModel":
-        # a model the library returned keeps its result arrays: packed without a copy
+        # a model the library returned keeps its result arrays: packed without
+        # a copy while its blocks are still those views
         pk = getattr(self, "_packed", None)
-        return pk if pk is not None else PackedModel(self)
+        return pk if pk is not None and pk.matches(self) else PackedModel(self)
 
 
 class PackedModel:
@@ -416,12 +430,21 @@ class _ResultPack:
         def __init__(self, c, data):
             self.c, self.data = c, data
 
-    def __init__(self, m: TjModel, data: np.ndarray, keep):
+    def __init__(self, m: TjModel, data: np.ndarray, keep, model: "Model"):
         self.c = m
         self.keep = keep
         self.ham = self._P(m.ham, data)
         self.sets = [[self._P(getattr(m.sub[i], k), data) for k in OPS] for i in range(m.nsub)]
         self.data = data
+        self.ham_views = _views(model.ham)
+        self.lazy = model.sub
+
+    def matches(self, model: "Model") -> bool:
+        if model.sub is not self.lazy or _views(model.ham) != self.ham_views:
+            return False
+        # only sets that have been built can have been changed: each against
+        # the views it was built with
+        return all([_views(getattr(bs, k)) for k in OPS] == v for bs, v in self.lazy.built())
 
 
 class _LazySets(Sequence):
@@ -432,6 +455,7 @@ class _LazySets(Sequence):
     def __init__(self, m: TjModel, data: np.ndarray):
         self._m, self._data = m, data
         self._sets: List[Optional[BlockSet]] = [None] * m.nsub
+        self._views: List[Optional[list]] = [None] * m.nsub
 
     def __len__(self):
         return len(self._sets)
@@ -446,10 +470,14 @@ class _LazySets(Sequence):
         if self._sets[i] is None:
             bs = self._m.sub[i]
             self._sets[i] = BlockSet(*[_block_from_c(getattr(bs, k), self._data) for k in OPS])
+            self._views[i] = [_views(getattr(self._sets[i], k)) for k in OPS]
         return self._sets[i]
 
     def __eq__(self, other):
         return list(self) == list(other)
+
+    def built(self):
+        return [(bs, v) for bs, v in zip(self._sets, self._views) if bs is not None]
 
 
 def model_from_c(m: TjModel, data: np.ndarray, keep=None) -> Model:
@@ -459,7 +487,7 @@ def model_from_c(m: TjModel, data: np.ndarray, keep=None) -> Model:
     packs without a copy."""
     out = Model(m.len, _block_from_c(m.ham, data), _LazySets(m, data))
     if keep is not None:
-        out._packed = _ResultPack(m, data, keep)
+        out._packed = _ResultPack(m, data, keep, out)
     return out
 
 
@@ -477,7 +505,7 @@ def call_block_result(call):
     if rc:
         return rc, None
     b = _block_from_c(res.block, data)
-    b._packed = _BlockView(res.block, subs, data)
+    b._packed = _BlockView(res.block, subs, data, b)
     return 0, b
 
 
@@ -519,5 +547,5 @@ def block_from_c_result(res: TjTruncResult, length: int, subs_arr=None, data: Op
     b = Block(length, 0, 0, subs)
     if data is not None and subs_arr is not None:
         b._packed = _BlockView(TjBlock(length, res.num, b.dim, 0, 0, 0, C.cast(subs_arr, C.POINTER(TjBlockSub)),
-                                       _dptr(data)), subs_arr, data)
+                                       _dptr(data)), subs_arr, data, b)
     return b

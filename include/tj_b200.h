@@ -127,7 +127,11 @@ typedef struct tj_lattice {
  * Two-call pattern: call tj_truncation with data == NULL to learn num and
  * the total number of doubles (data_len); allocate sub[num] and
  * data[data_len]; call again to fill them.  trun_op sub-blocks have
- * down_dif = 0, row_dim = sector dimension, sdim = kept columns. */
+ * down_dif = 0, row_dim = sector dimension, sdim = kept columns.  The first
+ * call leaves the operator on the device and the second copies it from
+ * there into data (at the DMA rate when data is page-locked); when another
+ * truncation ran on the same context in between, the second call computes
+ * it again. */
 typedef struct tj_trunc_result {
   int32_t num_state;         /* kept states (Num_state)                             */
   int32_t num;               /* kept sectors (trun_op%num)                          */
