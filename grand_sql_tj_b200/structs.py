@@ -189,9 +189,24 @@ class Block:
         return pk if pk is not None and pk.matches(self) else PackedBlock(self)
 
 
-def _views(b: "Block"):
-    return [(s.num_up, s.num_down, s.down_dif, s.mat.shape, s.mat.__array_interface__["data"][0],
-             s.mat.flags.f_contiguous) for s in b.subs]
+class _Views:
+    """The sub-blocks of a block as made: the matrix objects themselves
+    (held, so that an identity test cannot meet a recycled object) and
+    their sector labels."""
+
+    __slots__ = ("labels", "mats")
+
+    def __init__(self, b: "Block"):
+        self.labels = [(s.num_up, s.num_down, s.down_dif) for s in b.subs]
+        self.mats = [s.mat for s in b.subs]
+
+    def __eq__(self, other: "_Views") -> bool:
+        return (len(self.mats) == len(other.mats) and all(a is b for a, b in zip(self.mats, other.mats))
+                and self.labels == other.labels)
+
+
+def _views(b: "Block") -> _Views:
+    return _Views(b)
 
 
 class _BlockView:
