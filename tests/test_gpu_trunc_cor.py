@@ -82,6 +82,35 @@ def test_truncation(ctx, oracle_lib, wl, side, kmin, kmax):
     assert r2.num_state == r1.num_state and all(np.array_equal(a.mat, b.mat) for a, b in zip(t1.subs, t2.subs))
 
 
+@pytest.mark.parametrize("wl,kmin,kmax", [("cyl4x24_m2000", 3000, 6000), ("cyl6x24_m6000", 2000, 3000)])
+def test_truncation_cluster_sizes(ctx, oracle_lib, wl, kmin, kmax):
+    """Sectors of 320 states and more go to the cluster paths: the reduction
+    by 16 CTAs (from step 0 in shared memory at 359-481 states; moving into
+    shared memory part-way at 900-1524 states) and the cluster
+    orthonormalisation of kept blocks with k^2 d >= 3e7 (full sectors of
+    359-481 states; up to 605 of 1524).  The synthetic wavefunctions of the
+    two headline superblocks, against dsyev in the oracle, with the bounds of
+    test_truncation."""
+    from oracle import oracle
+    psi = synth.workload(wl).wave
+    r0, t0, _ = oracle.truncation(psi, 0, kmin, kmax, 1e-12)
+    r1, t1 = ctx.truncation(psi, 0, kmin, kmax, 1e-12)
+    assert max(s.mat.shape[0] for s in t1.subs) >= 359
+    assert r1.num_state == r0.num_state
+    assert abs(r1.trunc_err - r0.trunc_err) <= 1e-10
+    for k in ("entropy1", "entropy2", "entropys"):
+        assert abs(getattr(r1, k) - getattr(r0, k)) <= 1e-10, k
+    for sb1 in t1.subs:
+        q = sb1.mat
+        assert np.max(np.abs(q.T @ q - np.eye(q.shape[1]))) <= 1e-12
+    p0, p1 = _projectors(t0), _projectors(t1)
+    assert p0.keys() == p1.keys()
+    gaps = _sector_gaps(psi, 0, t0)
+    for k in p0:
+        tol = max(1e-8, 1e-15 / max(gaps[k], 1e-300))
+        assert np.max(np.abs(p0[k] - p1[k])) <= tol, (k, gaps[k])
+
+
 def test_truncation_rank_deficient(ctx, oracle_lib):
     """Density matrices with large null spaces -- the truncations of an
     untruncated 2x6 ladder run, system block much longer than the
