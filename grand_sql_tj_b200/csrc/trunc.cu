@@ -10,13 +10,16 @@
 // Here rho is one more grouped-GEMM pass (one cell per sector).  The
 // eigen-decomposition follows the direct route of DSYEV's first stage and
 // replaces its second: every sector is reduced to tridiagonal form by
-// Householder reflections (one CTA per sector), all eigenvalues come from
-// Sturm-count multisection (one thread per eigenvalue), the host selects the
+// Householder reflections (one CTA per sector, or a thread-block cluster of
+// 8-16 CTAs for sectors of 320 states and more), all eigenvalues come from
+// Sturm-count multisection (one warp per eigenvalue), the host selects the
 // kept states exactly as den_mat.f90 does, and only the kept eigenvectors
 // are computed: inverse iteration on the tridiagonal matrix (one thread per
-// vector), Gram-Schmidt orthonormalisation inside each kept block, and the
-// back-transformation by the stored reflectors, written straight into the
-// truncation operator's layout.  Everything is FP64.
+// vector), Gram-Schmidt orthonormalisation inside each kept block (one CTA,
+// or a cluster for large blocks), and the back-transformation by the stored
+// reflectors, written straight into the truncation operator's layout, which
+// stays on the device until the second call of the two-call protocol copies
+// it out.  Everything is FP64.
 #include <cuda_runtime.h>
 
 #include <algorithm>
