@@ -302,7 +302,15 @@ class Basis:
         return int(sum(m.dim for m in self.maps))
 
     def pack(self) -> "PackedBasis":
-        return PackedBasis(self)
+        # a sweep passes each basis to several calls: the packed form is kept
+        # while the maps read the same (comparing them costs a few
+        # microseconds, packing a few hundred)
+        sig = (self.len, [(m.new_num_up, m.new_num_down, tuple(m.subs)) for m in self.maps])
+        pk = self.__dict__.get("_packed")
+        if pk is None or pk[0] != sig:
+            pk = (sig, PackedBasis(self))
+            self.__dict__["_packed"] = pk
+        return pk[1]
 
 
 class PackedBasis:

@@ -51,3 +51,16 @@ def test_model_operator_sets_built_when_read(oracle_lib):
     assert m.pack() is pk
     getattr(m.sub[0], OPS[0]).subs[0].mat = np.zeros_like(getattr(m.sub[0], OPS[0]).subs[0].mat)
     assert isinstance(m.pack(), PackedModel)
+
+
+def test_basis_pack_kept_while_unchanged():
+    sb = synth.workload("small")
+    b = sb.sys_bs
+    p = b.pack()
+    assert b.pack() is p and p.c.dim == b.dim
+    m = b.maps[0]
+    m.subs.append(m.subs[-1])   # a changed map: packed anew, with the new record
+    p2 = b.pack()
+    assert p2 is not p and p2.c.sub[0].num == len(m.subs)
+    m.subs.pop()
+    assert b.pack().c.sub[0].num == len(m.subs)
